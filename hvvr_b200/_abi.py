@@ -1,0 +1,124 @@
+"""ctypes mirrors of the structs declared in include/hvvr_c.h.
+
+The layouts are byte-compatible with the reference's public types (Sample, ShadingVertex,
+PrecomputedTriangleShade, TopologyNode, SimpleMaterial, LightUnion, transform); numpy
+structured dtypes with the same layout are provided for bulk arrays.
+"""
+import ctypes as C
+
+import numpy as np
+
+HVVR_OK = 0
+HVVR_ERR_INVALID = 1
+HVVR_ERR_NOT_FOUND = 2
+HVVR_ERR_CUDA = 3
+HVVR_ERR_OOM = 4
+HVVR_ERR_OVERFLOW = 5
+HVVR_ERR_TIMEOUT = 6
+HVVR_ERR_STATE = 7
+
+HVVR_LIGHT_NONE, HVVR_LIGHT_DIRECTIONAL, HVVR_LIGHT_POINT, HVVR_LIGHT_SPOT = 0, 1, 2, 3
+HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA = 0, 1
+HVVR_MODE_DEFERRED_MSAA_RESOLVE, HVVR_MODE_FOVEATED_POLAR = 0, 1
+HVVR_FP_FMA, HVVR_FP_STRICT = 0, 1
+HVVR_CAPTURE_HITS = 1
+
+
+class Vec2(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float)]
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class Vec4(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float), ("w", C.c_float)]
+
+
+class FloatRect(C.Structure):
+    _fields_ = [("lower", Vec2), ("upper", Vec2)]
+
+
+class ThinLens(C.Structure):
+    _fields_ = [("radius", C.c_float), ("focal_distance", C.c_float)]
+
+
+class Transform(C.Structure):
+    _fields_ = [("rotation", Vec4), ("translation", Vec3), ("scale", C.c_float)]
+
+
+class LightDirectional(C.Structure):
+    _fields_ = [("direction", Vec3), ("power", Vec3)]
+
+
+class LightPoint(C.Structure):
+    _fields_ = [("position", Vec3), ("falloff_end", C.c_float), ("color", Vec3), ("falloff_scale", C.c_float)]
+
+
+class LightSpot(C.Structure):
+    _fields_ = [("position", Vec3), ("falloff_end", C.c_float), ("direction", Vec3), ("falloff_scale", C.c_float),
+                ("color", Vec3), ("cos_outer_angle", C.c_float), ("cos_angle_scale", C.c_float)]
+
+
+class _LightU(C.Union):
+    _fields_ = [("directional", LightDirectional), ("point", LightPoint), ("spot", LightSpot)]
+
+
+class LightUnion(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("u", _LightU)]
+
+
+class MeshData(C.Structure):
+    _fields_ = [("verts", C.c_void_p), ("vert_count", C.c_uint32),
+                ("tri_shade", C.c_void_p), ("tri_count", C.c_uint32),
+                ("nodes", C.c_void_p), ("node_count", C.c_uint32),
+                ("materials", C.c_void_p), ("material_count", C.c_uint32)]
+
+
+class ImageDesc(C.Structure):
+    _fields_ = [("pixel_format", C.c_uint32), ("memory_type", C.c_uint32), ("data", C.c_void_p),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("stride", C.c_uint64)]
+
+
+class Spec(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("thread_count", C.c_uint32),
+                ("foveated_degree_tracking_error", C.c_float), ("foveated_max_fov_degrees", C.c_float),
+                ("foveated_mar_slope", C.c_float), ("foveated_foveal_mar_degrees", C.c_float),
+                ("output_format", C.c_uint32), ("output_to_3d_api", C.c_uint32),
+                ("fp_mode", C.c_uint32), ("tri_index_capacity", C.c_uint64), ("device", C.c_int)]
+
+
+# numpy layouts of the bulk arrays
+SAMPLE_DTYPE = np.dtype([("pixel", "<u4", 2), ("position", "<f4", 2), ("minor", "<f4", 2), ("major", "<f4")])
+VERTEX_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<u2", 4), ("uv", "<f4", 2), ("pad", "<u4")])
+TRISHADE_DTYPE = np.dtype([("indices", "<u4", 3), ("material", "<u4")])
+TOPO_DTYPE = np.dtype([("leaf_mask", "<u4"), ("data", "<u4", 7)])
+MATERIAL_DTYPE = np.dtype([("emissive", "<f4", 4), ("diffuse", "<f4", 4), ("specular", "<f4", 4),
+                           ("glossiness", "<f4"), ("opacity", "<f4"), ("code", "<u8")])
+NODE_DTYPE = np.dtype([("bounds", "<f4", (6, 4)), ("leaf_mask", "<u4"), ("tri", "<u4", 5), ("pad", "<u4", 2)])
+
+assert SAMPLE_DTYPE.itemsize == 28
+assert VERTEX_DTYPE.itemsize == 32
+assert TRISHADE_DTYPE.itemsize == 16
+assert TOPO_DTYPE.itemsize == 32
+assert MATERIAL_DTYPE.itemsize == 64
+assert NODE_DTYPE.itemsize == 128
+assert C.sizeof(LightUnion) == 56
+assert C.sizeof(Transform) == 32
+
+
+def ptr(a):
+    """ctypes void pointer to a C-contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+def transform(rotation=(0.0, 0.0, 0.0, 1.0), translation=(0.0, 0.0, 0.0), scale=1.0):
+    t = Transform()
+    t.rotation = Vec4(*[float(v) for v in rotation])
+    t.translation = Vec3(*[float(v) for v in translation])
+    t.scale = float(scale)
+    return t

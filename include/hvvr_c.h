@@ -1,0 +1,251 @@
+/*
+ * hvvr_c.h - C ABI of the B200 primary-visibility-and-shading path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (HVVR_OK on success). Nothing here exits the process: failures come back as a
+ * status code plus a message readable through hvvr_last_error().
+ *
+ * Struct layouts are byte-compatible with the reference's public types so that a
+ * caller holding reference data (MeshData arrays, Sample arrays, LightUnion)
+ * can pass it through unchanged. Each declaration names the reference interface
+ * it replaces (paths are relative to the reference project root).
+ */
+#ifndef HVVR_C_H
+#define HVVR_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes
+ * Replaces cutilSafeCall/fail()/assert, which exit the process
+ * (libraries/hvvr/raycaster/cuda_util.h:18-29, libraries/hvvr/shared/debug.cpp:20-34). */
+enum {
+    HVVR_OK = 0,
+    HVVR_ERR_INVALID = 1,   /* bad argument or unsupported configuration */
+    HVVR_ERR_NOT_FOUND = 2, /* destroy of an object this raycaster does not own */
+    HVVR_ERR_CUDA = 3,      /* a CUDA runtime call failed */
+    HVVR_ERR_OOM = 4,       /* device allocation failed */
+    HVVR_ERR_OVERFLOW = 5,  /* a per-frame capacity (triangle-index pool, traversal stack) was exceeded */
+    HVVR_ERR_TIMEOUT = 6,   /* a bounded device-side wait gave up */
+    HVVR_ERR_STATE = 7      /* call made in the wrong state (e.g. read-back before any render) */
+};
+
+/* ---------------------------------------------------------------- plain types */
+typedef struct { float x, y; } hvvr_vec2;
+typedef struct { float x, y, z; } hvvr_vec3;
+typedef struct { float x, y, z, w; } hvvr_vec4;
+
+/* FloatRect (libraries/hvvr/shared/graphics_types.h:27-32) */
+typedef struct { hvvr_vec2 lower, upper; } hvvr_float_rect;
+
+/* ThinLens (libraries/hvvr/shared/graphics_types.h:170-173) */
+typedef struct { float radius, focal_distance; } hvvr_thin_lens;
+
+/* transform {quaternion rotation (x,y,z,w); vector3 translation; float scale}
+ * (libraries/hvvr/shared/vector_math.h:966-969) */
+typedef struct { hvvr_vec4 rotation; hvvr_vec3 translation; float scale; } hvvr_transform;
+
+/* Sample (libraries/hvvr/raycaster/samples.h:17-29), 28 bytes */
+typedef struct {
+    uint32_t pixel_x, pixel_y;
+    hvvr_vec2 position;   /* sample-space position in [0,1]^2 */
+    hvvr_vec2 minor_axis; /* ellipse minor axis */
+    float major_axis_length;
+} hvvr_sample;
+
+/* ShadingVertex (libraries/hvvr/shared/graphics_types.h:83-88), 32 bytes; normal is IEEE half x4 */
+typedef struct { hvvr_vec3 pos; uint16_t normal[4]; hvvr_vec2 uv; uint32_t pad0; } hvvr_shading_vertex;
+
+/* PrecomputedTriangleShade (libraries/hvvr/shared/graphics_types.h:208-211), 16 bytes */
+typedef struct { uint32_t indices[3]; uint32_t material; } hvvr_tri_shade;
+
+/* TopologyNode (libraries/hvvr/shared/graphics_types.h:126-151), 32 bytes.
+ * data[k] / data[k+1] bound leaf k's triangle range; data[1+k] is the relative
+ * child offset for an internal slot k. */
+typedef struct { uint32_t leaf_mask; uint32_t data[7]; } hvvr_topology_node;
+
+/* SimpleMaterial (libraries/hvvr/raycaster/material.h:22-49), 64 bytes */
+typedef struct {
+    hvvr_vec4 emissive, diffuse, specular;
+    float glossiness, opacity;
+    uint64_t texture_ids_and_shading_model;
+} hvvr_material;
+
+/* LightUnion (libraries/hvvr/raycaster/light.h:24-59), 56 bytes */
+enum { HVVR_LIGHT_NONE = 0, HVVR_LIGHT_DIRECTIONAL = 1, HVVR_LIGHT_POINT = 2, HVVR_LIGHT_SPOT = 3 };
+typedef struct { hvvr_vec3 direction; hvvr_vec3 power; } hvvr_light_directional;
+typedef struct { hvvr_vec3 position; float falloff_end; hvvr_vec3 color; float falloff_scale; } hvvr_light_point;
+typedef struct {
+    hvvr_vec3 position; float falloff_end;
+    hvvr_vec3 direction; float falloff_scale;
+    hvvr_vec3 color; float cos_outer_angle; float cos_angle_scale;
+} hvvr_light_spot;
+typedef struct {
+    uint32_t type;
+    union { hvvr_light_directional directional; hvvr_light_point point; hvvr_light_spot spot; } u;
+} hvvr_light_union;
+
+/* MeshData (libraries/hvvr/raycaster/model.h:26-31) as four borrowed arrays.
+ * nodes may be NULL/0: the library then builds the topology itself
+ * (hvvr_generate_topology) on a private copy. */
+typedef struct {
+    const hvvr_shading_vertex* verts; uint32_t vert_count;
+    const hvvr_tri_shade* tri_shade; uint32_t tri_count;
+    const hvvr_topology_node* nodes; uint32_t node_count;
+    const hvvr_material* materials; uint32_t material_count;
+} hvvr_mesh_data;
+
+/* ImageResourceDescriptor (libraries/hvvr/shared/graphics_types.h:56-80).
+ * Only CPU_MEMORY and CUDA_MEMORY exist here (no graphics API on the target). */
+enum { HVVR_PIXEL_RGBA8_SRGB = 0 };
+enum { HVVR_MEMORY_CPU = 0, HVVR_MEMORY_CUDA = 1 };
+typedef struct {
+    uint32_t pixel_format;
+    uint32_t memory_type;
+    void* data;
+    uint32_t width, height;
+    uint64_t stride; /* in pixels */
+} hvvr_image_desc;
+
+/* RayCasterSpecification (libraries/hvvr/raycaster/raycaster_spec.h:22-50) plus
+ * the device-side knobs this implementation adds. */
+enum { HVVR_MODE_DEFERRED_MSAA_RESOLVE = 0, HVVR_MODE_FOVEATED_POLAR = 1 };
+enum { HVVR_FP_FMA = 0, HVVR_FP_STRICT = 1 };
+typedef struct {
+    uint32_t mode;
+    uint32_t thread_count; /* host threads for setup work; 0 = all */
+    float foveated_degree_tracking_error, foveated_max_fov_degrees, foveated_mar_slope, foveated_foveal_mar_degrees;
+    uint32_t output_format;
+    uint32_t output_to_3d_api; /* must be 0: no graphics API here */
+    /* additions */
+    uint32_t fp_mode;             /* HVVR_FP_FMA (reference kernel comments) or HVVR_FP_STRICT (no FMA in edge tests) */
+    uint64_t tri_index_capacity;  /* per-camera triangle-index pool, entries; 0 = default (128M as the reference) */
+    int device;                   /* CUDA device ordinal */
+} hvvr_spec;
+
+typedef struct hvvr_raycaster hvvr_raycaster;
+typedef struct hvvr_camera hvvr_camera;
+typedef struct hvvr_model hvvr_model;
+typedef struct hvvr_light hvvr_light;
+
+/* ---------------------------------------------------------------- errors */
+/* Message of the last failing call on this thread (empty string if none). */
+const char* hvvr_last_error(void);
+/* Library/ABI version: major*10000 + minor*100 + patch. */
+int hvvr_version(void);
+
+/* ---------------------------------------------------------------- raycaster
+ * Raycaster(const RayCasterSpecification&) / ~Raycaster (libraries/hvvr/raycaster/raycaster.h:44-45) */
+void hvvr_spec_default(hvvr_spec* spec);
+int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out);
+int hvvr_raycaster_destroy(hvvr_raycaster* rc);
+/* setSceneDirty (raycaster.h:62) */
+int hvvr_raycaster_set_scene_dirty(hvvr_raycaster* rc);
+/* render(double) (raycaster.h:65; libraries/hvvr/raycaster/render.cpp:204-219).
+ * stream: a cudaStream_t, or NULL for the raycaster's own stream. Returns after the
+ * frame is enqueued; CPU_MEMORY render targets are complete on return. */
+int hvvr_raycaster_render(hvvr_raycaster* rc, double elapsed_time, void* stream);
+/* waits for all work the raycaster enqueued and reports any device-side status flag */
+int hvvr_raycaster_synchronize(hvvr_raycaster* rc);
+
+/* ---------------------------------------------------------------- models
+ * createModel(MeshData&&) / destroyModel (raycaster.h:58-60; libraries/hvvr/raycaster/model.cpp:20-21) */
+int hvvr_model_create(hvvr_raycaster* rc, const hvvr_mesh_data* mesh, hvvr_model** out);
+int hvvr_model_destroy(hvvr_raycaster* rc, hvvr_model* model);
+/* Model::setTransform (model.h:47; model.cpp:25-29): marks the scene dirty */
+int hvvr_model_set_transform(hvvr_model* model, const hvvr_transform* xf);
+/* Replace the model's vertex positions (animation) without rebuilding topology;
+ * the next render refits the BVH in place on the device. count must equal the model's vertex count. */
+int hvvr_model_update_vertices(hvvr_model* model, const hvvr_shading_vertex* verts, uint32_t count);
+
+/* ---------------------------------------------------------------- lights
+ * createLight(const LightUnion&) / destroyLight (raycaster.h:55-56) */
+int hvvr_light_create(hvvr_raycaster* rc, const hvvr_light_union* light, hvvr_light** out);
+int hvvr_light_destroy(hvvr_raycaster* rc, hvvr_light* light);
+
+/* ---------------------------------------------------------------- cameras
+ * createCamera(const FloatRect&, float) / destroyCamera (raycaster.h:49-50) and the
+ * Camera setters (libraries/hvvr/raycaster/camera.h:70-108) */
+int hvvr_camera_create(hvvr_raycaster* rc, const hvvr_float_rect* viewport, float aperture_radius, hvvr_camera** out);
+int hvvr_camera_destroy(hvvr_raycaster* rc, hvvr_camera* cam);
+int hvvr_camera_set_enabled(hvvr_camera* cam, int enabled);
+int hvvr_camera_set_viewport(hvvr_camera* cam, const hvvr_float_rect* viewport);
+int hvvr_camera_set_lens(hvvr_camera* cam, const hvvr_thin_lens* lens);
+int hvvr_camera_set_aperture(hvvr_camera* cam, float radius);
+int hvvr_camera_set_focal_depth(hvvr_camera* cam, float depth);
+int hvvr_camera_set_eye_dir(hvvr_camera* cam, const hvvr_vec3* eye_dir);
+int hvvr_camera_set_spherical_warp(hvvr_camera* cam, float fov_x_degrees, float fov_y_degrees);
+/* setRenderTarget (camera.h:87; camera.cpp:128-133) */
+int hvvr_camera_set_render_target(hvvr_camera* cam, const hvvr_image_desc* target);
+/* setSamples(const Sample*, count, splitColorSamples in {1,2,3}) (camera.h:88; camera.cpp:135-138) */
+int hvvr_camera_set_samples(hvvr_camera* cam, const hvvr_sample* samples, uint32_t count, uint32_t split_color_samples);
+/* setCameraToWorld(const transform&) (camera.h:99; camera.cpp:174-176) */
+int hvvr_camera_set_camera_to_world(hvvr_camera* cam, const hvvr_transform* xf);
+/* MSAA rate in {1,2,4,8,16,32}; the reference fixes it at compile time
+ * (libraries/hvvr/raycaster/raycaster_common.h:27). Default 16. */
+int hvvr_camera_set_msaa(hvvr_camera* cam, uint32_t rate);
+/* getSampleCount (camera.h:95; camera.cpp:162-164): valid (unpadded) sample count */
+int hvvr_camera_get_sample_count(const hvvr_camera* cam, uint32_t* count);
+
+/* ---------------------------------------------------------------- parity read-back
+ * Intermediate results of the last rendered frame, in sorted-sample order (the order
+ * produced by the reference's naiveXYCluster, libraries/hvvr/raycaster/sample_clustering.h:17-49).
+ * Sizes: tiles = blocks*64, padded samples = blocks*8192. */
+enum { HVVR_CAPTURE_HITS = 1 }; /* record per-subsample hit IDs and depth during render */
+int hvvr_camera_set_capture(hvvr_camera* cam, uint32_t flags);
+int hvvr_camera_get_layout(const hvvr_camera* cam, uint32_t* block_count, uint32_t* tile_count,
+                           uint32_t* padded_sample_count, uint32_t* msaa_rate);
+/* Per-tile triangle lists (traverseTiles output, libraries/hvvr/raycaster/traverse_avx.h:412-527):
+ * counts[tile_count]; indices concatenated in tile order; *total receives the total entry count.
+ * Pass indices=NULL to query the total only. */
+int hvvr_camera_read_tile_lists(const hvvr_camera* cam, uint32_t* counts, uint32_t* indices, uint64_t capacity,
+                                uint64_t* total);
+/* Block cull stacks (traverseBlocks + BlockFrame::sort, traverse_avx.h:293-410):
+ * sizes[block_count]; entries[block_count*64] as {float tMin; uint32 mask; uint32 node}. */
+int hvvr_camera_read_block_stacks(const hvvr_camera* cam, uint32_t* sizes, uint32_t* entries);
+/* Per-subsample hit triangle IDs (~0 = miss) and parametric depth (+inf = miss) along the
+ * unnormalised subsample direction; [padded_sample_count * msaa]. Needs HVVR_CAPTURE_HITS. */
+int hvvr_camera_read_hits(const hvvr_camera* cam, uint32_t* tri_ids, float* depth);
+/* Compressed G-buffer (EmitGBuffer, libraries/hvvr/raycaster/intersect.cu:28-89) rebuilt per sample:
+ * for sample s, entries s*msaa .. s*msaa+n-1 hold (tri, mask) pairs sorted by tri, misses last.
+ * n[s] is the pair count. Needs HVVR_CAPTURE_HITS. */
+int hvvr_camera_read_gbuffer(const hvvr_camera* cam, uint32_t* n, uint32_t* tri, uint32_t* mask);
+/* Resolved RGBA8 (sRGB) per sorted sample [padded_sample_count] (ResolveKernel output). */
+int hvvr_camera_read_sample_colors(const hvvr_camera* cam, uint32_t* rgba);
+/* imageLocationToSampleIndex (camera.cpp:57-63) [width*height*split] */
+int hvvr_camera_read_sample_remap(const hvvr_camera* cam, int32_t* remap, uint64_t count);
+/* Camera-space beams of the sorted samples, DirectionalBeam {centerRay,du,dv} x padded samples */
+int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9);
+/* per-frame timing of the last render, device milliseconds (CUDA events):
+ * [0]=scene update/refit, [1]=block cull, [2]=tile cull, [3]=intersect+shade, [4]=remap, [5]=total */
+int hvvr_camera_read_timings(const hvvr_camera* cam, float* ms6);
+/* total triangle-index entries produced by the last frame's tile cull */
+int hvvr_camera_read_list_total(const hvvr_camera* cam, uint64_t* total);
+
+/* ---------------------------------------------------------------- scene state read-back
+ * The refit BVH (GPUSceneState::fetchUpdatedBVH, libraries/hvvr/raycaster/gpu_scene_state.cu:454-467):
+ * node_count*32 floats/uints in the 128-byte BVHNode layout (libraries/hvvr/raycaster/bvh_node.h:17-36). */
+int hvvr_scene_get_counts(const hvvr_raycaster* rc, uint32_t* node_count, uint32_t* tri_count, uint32_t* vert_count);
+int hvvr_scene_read_nodes(hvvr_raycaster* rc, void* nodes128);
+/* PrecomputedTriangleIntersect {v0, edge0, edge1} x tri_count (graphics_types.h:203-207) */
+int hvvr_scene_read_triangles(hvvr_raycaster* rc, float* tris9);
+
+/* ---------------------------------------------------------------- host utilities
+ * GenerateTopology(MeshData&) (libraries/hvvr/shared/bvh.cpp:542-556): SAH BVH2 -> BVH4 -> DFS topology.
+ * Reorders tri_shade and verts in place (triangle IDs everywhere are BVH-order IDs) and writes
+ * node_count nodes into nodes_out (capacity >= (tri_count+1)/2 + 1). */
+int hvvr_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr_tri_shade* tri_shade,
+                           uint32_t tri_count, hvvr_topology_node* nodes_out, uint32_t nodes_capacity,
+                           uint32_t* node_count);
+/* getGridSamples(width, height) (libraries/hvvr/raycaster/samples.cpp:21-42) */
+int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HVVR_C_H */

@@ -1,0 +1,1148 @@
+// hvvr_oracle.cpp - TEST INFRASTRUCTURE ONLY (see hvvr_oracle.h).
+//
+// Scalar restatement of the reference primary-visibility path. Every function cites the
+// reference lines it restates (paths relative to the reference project root; RC/ =
+// libraries/hvvr/raycaster/, SH/ = libraries/hvvr/shared/).
+//
+// Floating point: built with -ffp-contract=off; MXCSR FTZ|DAZ is set for the duration of
+// oracle_render exactly as the reference sets it on its worker threads (RC/raycaster.cpp:21-27).
+// fmaf() appears only where the reference issues an explicit FMA (_mm256_fmadd_ps in
+// RC/traverse_avx.{h,cpp}) or where its kernel comments mark FMA (RC/prim_tests.h:193-229,
+// HVVR_FP_FMA mode).
+
+#include "hvvr_oracle.h"
+
+#include <immintrin.h>
+#include <math.h>
+#include <float.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <vector>
+
+namespace {
+
+enum { kTileSize = 128, kTilesPerBlock = 64, kBlockSize = kTileSize * kTilesPerBlock };
+enum { kBlockStackSize = 64, kTileStackMax = 4096 };
+
+struct V2 { float x, y; };
+struct V3 { float x, y, z; };
+struct V4 { float x, y, z, w; };
+
+inline V3 mk(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 operator+(V3 a, V3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 operator-(V3 a, V3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 operator-(V3 a) { return mk(-a.x, -a.y, -a.z); }
+inline V3 operator*(V3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+inline V3 operator*(V3 a, V3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+// vector3::operator/(float) multiplies by the reciprocal (SH/vector_math.h:210-213)
+inline V3 divs(V3 a, float s) { float inv = 1.0f / s; return mk(a.x * inv, a.y * inv, a.z * inv); }
+// SH/vector_math.h:262-286
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+inline float length(V3 v) { return sqrtf(dot(v, v)); }
+inline V3 normalize(V3 v) { return divs(v, length(v)); }
+// SH/util.h:46-47 (min/max templates)
+inline float tmin(float a, float b) { return a < b ? a : b; }
+inline float tmax(float a, float b) { return a > b ? a : b; }
+inline float sat(float x) { return x > 0.0f ? (x < 1.0f ? x : 1.0f) : 0.0f; } // __saturatef (NaN -> 0)
+
+inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+inline float bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+// denormals-are-zero view of a float, for comparisons the reference makes under MXCSR.DAZ
+inline float daz(float f) { uint32_t u = fbits(f); return (u & 0x7f800000u) == 0 ? bitsf(u & 0x80000000u) : f; }
+
+// column-major matrices (SH/vector_math.h:1003-1133, 1152-1278)
+struct M3 { V3 m0, m1, m2; };
+struct M4 { V4 m0, m1, m2, m3; };
+inline V3 mul(const M3& m, V3 v) {
+    return mk(m.m0.x * v.x + m.m1.x * v.y + m.m2.x * v.z, m.m0.y * v.x + m.m1.y * v.y + m.m2.y * v.z,
+              m.m0.z * v.x + m.m1.z * v.y + m.m2.z * v.z);
+}
+inline V4 mul(const M4& m, V4 v) {
+    return V4{m.m0.x * v.x + m.m1.x * v.y + m.m2.x * v.z + m.m3.x * v.w,
+              m.m0.y * v.x + m.m1.y * v.y + m.m2.y * v.z + m.m3.y * v.w,
+              m.m0.z * v.x + m.m1.z * v.y + m.m2.z * v.z + m.m3.z * v.w,
+              m.m0.w * v.x + m.m1.w * v.y + m.m2.w * v.z + m.m3.w * v.w};
+}
+inline M3 m3of(const M4& m) { return M3{mk(m.m0.x, m.m0.y, m.m0.z), mk(m.m1.x, m.m1.y, m.m1.z), mk(m.m2.x, m.m2.y, m.m2.z)}; }
+
+// matrix4x4(const transform&) = matrix4x4(matrix3x3(rotation) * scale, translation)
+// (SH/vector_math.h:1021-1037 quaternion->matrix, 1158, 1161)
+M4 transformToMatrix(const hvvr_transform& t) {
+    float qx = t.rotation.x, qy = t.rotation.y, qz = t.rotation.z, qw = t.rotation.w;
+    float x2 = qx + qx, y2 = qy + qy, z2 = qz + qz;
+    float xx = qx * x2, yy = qy * y2, zz = qz * z2;
+    float xy = qx * y2, yz = qy * z2, xz = qz * x2;
+    float wx = qw * x2, wy = qw * y2, wz = qw * z2;
+    V3 c0 = mk(1.0f - (yy + zz), xy + wz, xz - wy);
+    V3 c1 = mk(xy - wz, 1.0f - (xx + zz), yz + wx);
+    V3 c2 = mk(xz + wy, yz - wx, 1.0f - (xx + yy));
+    float s = t.scale;
+    c0 = c0 * s; c1 = c1 * s; c2 = c2 * s;
+    return M4{V4{c0.x, c0.y, c0.z, 0.0f}, V4{c1.x, c1.y, c1.z, 0.0f}, V4{c2.x, c2.y, c2.z, 0.0f},
+              V4{t.translation.x, t.translation.y, t.translation.z, 1.0f}};
+}
+
+// ------------------------------------------------------------------ BVH node (RC/bvh_node.h:17-36)
+struct Node {
+    float b[6][4]; // xMax, xNegMin, yMax, yNegMin, zMax, zNegMin
+    uint32_t leafMask;
+    uint32_t tri[5]; // leaf.triIndex[5]; children.offset[k] aliases tri[k+1]
+    uint32_t pad[2];
+};
+static_assert(sizeof(Node) == 128, "node");
+inline uint32_t childOf(const Node* nodes, uint32_t n, int k) { return n + nodes[n].tri[k + 1]; }
+
+struct Tri { V3 v0, e0, e1; };
+
+inline float halfToFloat(uint16_t h) { return _cvtsh_ss(h); }
+inline uint16_t floatToHalf(float f) { return (uint16_t)_cvtss_sh(f, 0); }
+
+// ------------------------------------------------------------------ scene build + refit
+struct Scene {
+    std::vector<Node> nodes;
+    std::vector<hvvr_tri_shade> triShade;
+    std::vector<hvvr_shading_vertex> verts;     // untransformed, merged
+    std::vector<uint32_t> vertModel;
+    std::vector<hvvr_material> materials;
+    std::vector<hvvr_shading_vertex> world;     // transformed
+    std::vector<Tri> tris;
+    uint32_t status = 0;
+};
+
+// Raycaster::buildScene (RC/scene_update.cpp:22-143)
+void buildScene(const oracle_frame_in* in, Scene& s) {
+    uint32_t modelCount = in->model_count;
+    if (modelCount == 0) {
+        s.nodes.assign(1, Node{});
+        s.nodes[0].leafMask = 0xf;
+        return;
+    }
+    uint32_t rootNodeCount = (modelCount + 1) / 3;
+    uint32_t vc = 0, tc = 0, nc = rootNodeCount, mc = 0;
+    for (uint32_t m = 0; m < modelCount; m++) {
+        vc += in->models[m].vert_count; tc += in->models[m].tri_count;
+        nc += in->models[m].node_count; mc += in->models[m].material_count;
+    }
+    s.nodes.assign(nc, Node{});
+    s.triShade.resize(tc);
+    s.verts.resize(vc);
+    s.vertModel.resize(vc);
+    s.materials.resize(mc);
+    std::vector<uint32_t> viewOffsets(modelCount);
+    uint32_t vOff = 0, tOff = 0, mOff = 0, nOff = rootNodeCount;
+    for (uint32_t m = 0; m < modelCount; m++) {
+        const hvvr_mesh_data& md = in->models[m];
+        for (uint32_t i = 0; i < md.material_count; i++) s.materials[mOff + i] = md.materials[i];
+        for (uint32_t i = 0; i < md.tri_count; i++) {
+            hvvr_tri_shade t = md.tri_shade[i];
+            t.indices[0] += vOff; t.indices[1] += vOff; t.indices[2] += vOff;
+            t.material += mOff;
+            s.triShade[tOff + i] = t;
+        }
+        for (uint32_t i = 0; i < md.vert_count; i++) { s.verts[vOff + i] = md.verts[i]; s.vertModel[vOff + i] = m; }
+        viewOffsets[m] = nOff;
+        for (uint32_t i = 0; i < md.node_count; i++) {
+            const hvvr_topology_node& tn = md.nodes[i];
+            Node& n = s.nodes[nOff + i];
+            n.leafMask = tn.leaf_mask;
+            n.tri[0] = tOff + tn.data[0];
+            for (int k = 0; k < 4; k++)
+                n.tri[1 + k] = (tn.leaf_mask & (1u << k)) ? tOff + tn.data[1 + k] : tn.data[1 + k];
+        }
+        vOff += md.vert_count; tOff += md.tri_count; mOff += md.material_count; nOff += md.node_count;
+    }
+    if (rootNodeCount > 0) {
+        // root fix-up nodes: nulls first, then fix-up nodes, then model entry points
+        std::vector<int64_t> children(rootNodeCount * 4);
+        size_t w = 0;
+        for (size_t i = children.size() - modelCount - (rootNodeCount - 1); i != 0; --i) children[w++] = -1;
+        for (uint32_t i = 1; i < rootNodeCount; i++) children[w++] = i;
+        for (uint32_t m = 0; m < modelCount; m++) children[w++] = viewOffsets[m];
+        for (uint32_t i = 0; i < rootNodeCount; i++) {
+            Node& n = s.nodes[i];
+            n.tri[0] = 0;
+            n.leafMask = 0;
+            for (int k = 0; k < 4; k++) {
+                int64_t c = children[4 * i + k];
+                if (c < 0) { n.tri[1 + k] = 0; n.leafMask |= 1u << k; continue; }
+                n.tri[1 + k] = uint32_t(c - i);
+            }
+        }
+    }
+}
+
+// FloatFlip / IFloatFlip (RC/sort.h:13-32)
+inline uint32_t floatFlip(uint32_t f) { uint32_t mask = uint32_t(-int32_t(f >> 31)) | 0x80000000u; return f ^ mask; }
+inline uint32_t ifloatFlip(uint32_t f) { uint32_t mask = ((f & 0x80000000u) == 0) ? 0xffffffffu : 0x80000000u; return f ^ mask; }
+
+// GPUSceneState::update (RC/gpu_scene_state.cu:377-451) and setGeometry's task ordering
+// (RC/gpu_scene_state.cu:469-599). Bounds use the same max operators: atomicMax on
+// float-flipped integers for leaf slots, max(a,b)=a>b?a:b for internal slots.
+void refitScene(const oracle_frame_in* in, Scene& s) {
+    uint32_t modelCount = in->model_count;
+    std::vector<M4> modelToWorld(modelCount);
+    for (uint32_t m = 0; m < modelCount; m++) modelToWorld[m] = transformToMatrix(in->model_xf[m]);
+    // SceneTransformVerticesKernel (RC/gpu_scene_state.cu:88-132)
+    s.world = s.verts;
+    for (size_t i = 0; i < s.verts.size(); i++) {
+        const M4& t = modelToWorld[s.vertModel[i]];
+        const hvvr_shading_vertex& v = s.verts[i];
+        V4 fp = mul(t, V4{v.pos.x, v.pos.y, v.pos.z, 1.0f});
+        V3 p = mk(fp.x, fp.y, fp.z) * (1.0f / fp.w);
+        s.world[i].pos = hvvr_vec3{p.x, p.y, p.z};
+        V3 n = mk(halfToFloat(v.normal[0]), halfToFloat(v.normal[1]), halfToFloat(v.normal[2]));
+        V3 nn = normalize(mul(m3of(t), n));
+        s.world[i].normal[0] = floatToHalf(nn.x);
+        s.world[i].normal[1] = floatToHalf(nn.y);
+        s.world[i].normal[2] = floatToHalf(nn.z);
+        s.world[i].normal[3] = floatToHalf(0.0f);
+    }
+    uint32_t nodeCount = uint32_t(s.nodes.size());
+    uint32_t triCount = uint32_t(s.triShade.size());
+    // triToNodeChild (RC/gpu_scene_state.cu:538-570): nodes back to front, slots 3..0
+    std::vector<uint32_t> triToNodeChild(triCount, 0);
+    for (int64_t n = int64_t(nodeCount) - 1; n >= 0; n--) {
+        const Node& nd = s.nodes[n];
+        for (int k = 3; k >= 0; k--) {
+            if (nd.leafMask & (1u << k)) {
+                for (uint32_t t = nd.tri[k]; t < nd.tri[k + 1]; t++)
+                    if (t < triCount) triToNodeChild[t] = (uint32_t(n) << 2) | uint32_t(k);
+            }
+        }
+    }
+    // SceneRefitPreKernel: bounds := FloatFlip(-inf)
+    std::vector<uint32_t> fb(size_t(nodeCount) * 24, floatFlip(0xff800000u));
+    // ScenePrecomputeTrianglesKernel (RC/gpu_scene_state.cu:167-244)
+    s.tris.resize(triCount);
+    for (uint32_t i = 0; i < triCount; i++) {
+        const hvvr_tri_shade& ts = s.triShade[i];
+        V3 v0 = mk(s.world[ts.indices[0]].pos.x, s.world[ts.indices[0]].pos.y, s.world[ts.indices[0]].pos.z);
+        V3 v1 = mk(s.world[ts.indices[1]].pos.x, s.world[ts.indices[1]].pos.y, s.world[ts.indices[1]].pos.z);
+        V3 v2 = mk(s.world[ts.indices[2]].pos.x, s.world[ts.indices[2]].pos.y, s.world[ts.indices[2]].pos.z);
+        s.tris[i] = Tri{v0, v1 - v0, v2 - v0};
+        float mx[3] = {tmax(v0.x, tmax(v1.x, v2.x)), tmax(v0.y, tmax(v1.y, v2.y)), tmax(v0.z, tmax(v1.z, v2.z))};
+        float nm[3] = {tmax(-v0.x, tmax(-v1.x, -v2.x)), tmax(-v0.y, tmax(-v1.y, -v2.y)), tmax(-v0.z, tmax(-v1.z, -v2.z))};
+        uint32_t nc = triToNodeChild[i];
+        uint32_t parent = nc >> 2, slot = nc & 3;
+        for (int a = 0; a < 3; a++) {
+            uint32_t* pMax = &fb[size_t(parent) * 24 + (2 * a) * 4 + slot];
+            uint32_t* pNeg = &fb[size_t(parent) * 24 + (2 * a + 1) * 4 + slot];
+            *pMax = std::max(*pMax, floatFlip(fbits(mx[a])));
+            *pNeg = std::max(*pNeg, floatFlip(fbits(nm[a])));
+        }
+    }
+    // SceneRefitIntFixupKernel
+    for (uint32_t n = 0; n < nodeCount; n++)
+        for (int j = 0; j < 24; j++) s.nodes[n].b[j / 4][j % 4] = bitsf(ifloatFlip(fb[size_t(n) * 24 + j]));
+    // internal refit, deepest parents first (RC/gpu_scene_state.cu:505-589, 273-375)
+    std::vector<uint32_t> depth(nodeCount, 0);
+    uint32_t maxDepth = 0;
+    for (uint32_t n = 0; n < nodeCount; n++) {
+        const Node& nd = s.nodes[n];
+        for (int k = 3; k >= 0; k--) {
+            if (!(nd.leafMask & (1u << k))) {
+                uint32_t c = n + nd.tri[k + 1];
+                if (c < nodeCount) { depth[c] = depth[n] + 1; maxDepth = std::max(maxDepth, depth[n] + 1); }
+            }
+        }
+    }
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> byDepth(maxDepth + 1);
+    for (uint32_t n = 0; n < nodeCount; n++)
+        for (int k = 0; k < 4; k++)
+            if (!(s.nodes[n].leafMask & (1u << k))) byDepth[depth[n]].push_back({n, uint32_t(k)});
+    for (int64_t d = maxDepth; d >= 0; d--) {
+        for (auto& task : byDepth[d]) {
+            uint32_t c = task.first + s.nodes[task.first].tri[task.second + 1];
+            if (c >= nodeCount) { s.status |= 1; continue; }
+            const Node& ch = s.nodes[c];
+            for (int j = 0; j < 6; j++) {
+                float v = tmax(ch.b[j][0], tmax(ch.b[j][1], tmax(ch.b[j][2], ch.b[j][3])));
+                s.nodes[task.first].b[j][task.second] = v;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ samples (RC/camera.cpp:21-64)
+struct SortedSample { hvvr_sample s; uint32_t channel; };
+
+// naiveXYCluster (RC/sample_clustering.h:17-49)
+void naiveXYCluster(std::vector<SortedSample>& v, size_t k) {
+    size_t yStrata = (size_t)sqrt((double)k);
+    size_t xStrata = (k + yStrata - 1) / yStrata;
+    size_t blockYStrata = (size_t)sqrt((double)kTilesPerBlock);
+    size_t blockXStrata = (kTilesPerBlock + blockYStrata - 1) / blockYStrata;
+    auto yx = [](const SortedSample& a, const SortedSample& b) {
+        return (a.s.position.y < b.s.position.y) || (a.s.position.y == b.s.position.y && a.s.position.x < b.s.position.x);
+    };
+    auto xy = [](const SortedSample& a, const SortedSample& b) {
+        return (a.s.position.x < b.s.position.x) || (a.s.position.x == b.s.position.x && a.s.position.y < b.s.position.y);
+    };
+    size_t n = v.size();
+    std::sort(v.begin(), v.end(), yx);
+    for (size_t i = 0; i < yStrata; ++i)
+        std::sort(v.begin() + (i * kBlockSize * xStrata), v.begin() + std::min((i + 1) * kBlockSize * xStrata, n), xy);
+    for (size_t i = 0; i < k; ++i)
+        std::sort(v.begin() + (i * kBlockSize), v.begin() + std::min((i + 1) * kBlockSize, n), yx);
+    for (size_t i = 0; i < n; i += kTileSize * blockXStrata)
+        std::sort(v.begin() + i, v.begin() + std::min(i + kTileSize * blockXStrata, n), xy);
+}
+
+struct Frustum2D { float d[4]; }; // xMin, -xMax, yMin, -yMax (RC/sample_hierarchy.h:19-58)
+inline void merge2D(Frustum2D& f, float x, float y) {
+    f.d[0] = tmin(f.d[0], x); f.d[1] = tmin(f.d[1], -x); f.d[2] = tmin(f.d[2], y); f.d[3] = tmin(f.d[3], -y);
+}
+
+struct Rays4 { V3 o[4], d[4]; };
+
+// Camera::getSampleToCamera (RC/camera.cpp:167-171)
+M3 sampleToCamera(const hvvr_float_rect& vp) {
+    return M3{mk(vp.upper.x - vp.lower.x, 0, 0), mk(0, vp.lower.y - vp.upper.y, 0), mk(vp.lower.x, vp.upper.y, -1)};
+}
+
+// get3DFrustumFrom2D, perspective mapping (RC/sample_hierarchy.cpp:46-123)
+Rays4 frustumFrom2D(const Frustum2D& f, const M3& S, const hvvr_thin_lens& lens) {
+    const float farPlane = -100.0f;
+    float xMin = f.d[0], xMax = -f.d[1], yMin = f.d[2], yMax = -f.d[3];
+    V3 nearP[4] = {mk(-lens.radius, -lens.radius, 0), mk(+lens.radius, -lens.radius, 0),
+                   mk(+lens.radius, +lens.radius, 0), mk(-lens.radius, +lens.radius, 0)};
+    V3 rd[4] = {mul(S, mk(xMin, yMax, 1)), mul(S, mk(xMax, yMax, 1)), mul(S, mk(xMax, yMin, 1)), mul(S, mk(xMin, yMin, 1))};
+    V3 focus[4];
+    for (int i = 0; i < 4; i++) focus[i] = rd[i] * (lens.focal_distance / -rd[i].z);
+    float fxMax = -INFINITY, fxMin = INFINITY, fyMax = -INFINITY, fyMin = INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        for (int j = 0; j < 4; ++j) {
+            V3 pos = nearP[i];
+            V3 dir = normalize(focus[j] - pos);
+            V3 p = pos + dir * (farPlane / dir.z);
+            fxMax = tmax(fxMax, p.x); fxMin = tmin(fxMin, p.x);
+            fyMax = tmax(fyMax, p.y); fyMin = tmin(fyMin, p.y);
+        }
+    }
+    V3 farP[4] = {mk(fxMin, fyMin, farPlane), mk(fxMax, fyMin, farPlane), mk(fxMax, fyMax, farPlane), mk(fxMin, fyMax, farPlane)};
+    Rays4 r;
+    for (int i = 0; i < 4; i++) { r.o[i] = nearP[i]; r.d[i] = normalize(farP[i] - nearP[i]); }
+    return r;
+}
+
+struct Beam { V3 c, du, dv; };
+
+struct SampleSetup {
+    uint32_t blocks = 0, tiles = 0, padded = 0, valid = 0;
+    std::vector<Rays4> tileRays, blockRays; // camera space
+    std::vector<Beam> beams;
+    std::vector<int32_t> remap;
+};
+
+void setupSamples(const oracle_frame_in* in, SampleSetup& ss) {
+    uint32_t n = in->sample_count;
+    std::vector<SortedSample> sorted(n);
+    for (uint32_t i = 0; i < n; i++) sorted[i] = SortedSample{in->samples[i], i % in->split_color_samples};
+    uint32_t blockCount = (n + kBlockSize - 1) / kBlockSize;
+    naiveXYCluster(sorted, blockCount);
+    ss.blocks = blockCount; ss.tiles = blockCount * kTilesPerBlock; ss.padded = blockCount * kBlockSize; ss.valid = n;
+    M3 S = sampleToCamera(in->viewport);
+    // BeamBatch2D (RC/sample_hierarchy.cpp:154-190); cullRect is +-inf so intersect() is a no-op
+    std::vector<Frustum2D> tile2D(ss.tiles), block2D(blockCount);
+    std::vector<V2> center(ss.padded, V2{0, 0}), major(ss.padded, V2{0, 0}), minor(ss.padded, V2{0, 0});
+    uint32_t maxIndex = n - 1, si = 0;
+    for (uint32_t b = 0; b < blockCount; b++) {
+        Frustum2D bf{{INFINITY, INFINITY, INFINITY, INFINITY}};
+        for (uint32_t t = 0; t < kTilesPerBlock; t++) {
+            Frustum2D tf{{INFINITY, INFINITY, INFINITY, INFINITY}};
+            for (uint32_t k = 0; k < kTileSize; k++) {
+                const hvvr_sample& s = sorted[si].s;
+                float x = s.position.x, y = s.position.y, mj = s.major_axis_length;
+                merge2D(tf, x + mj, y + mj);
+                merge2D(tf, x - mj, y - mj);
+                // unpackSample (RC/samples.cpp:144-159)
+                const float EXT = 0.70710678118f;
+                V2 mn{s.minor_axis.x * EXT, s.minor_axis.y * EXT};
+                float mlen = sqrtf(s.minor_axis.x * s.minor_axis.x + s.minor_axis.y * s.minor_axis.y);
+                float rescale = s.major_axis_length * EXT / mlen;
+                center[si] = V2{s.position.x, s.position.y};
+                minor[si] = mn;
+                major[si] = V2{-mn.y * rescale, mn.x * rescale};
+                si = std::min(si + 1, maxIndex);
+            }
+            for (int j = 0; j < 4; j++) tf.d[j] = tmax(tf.d[j], -INFINITY);
+            tile2D[b * kTilesPerBlock + t] = tf;
+            for (int j = 0; j < 4; j++) bf.d[j] = tmin(bf.d[j], tf.d[j]);
+        }
+        block2D[b] = bf;
+    }
+    // BeamBatch::generateFrom2D (RC/sample_hierarchy.cpp:129-152)
+    ss.tileRays.resize(ss.tiles);
+    ss.blockRays.resize(blockCount);
+    for (uint32_t b = 0; b < blockCount; b++) {
+        for (uint32_t t = 0; t < kTilesPerBlock; t++)
+            ss.tileRays[b * kTilesPerBlock + t] = frustumFrom2D(tile2D[b * kTilesPerBlock + t], S, in->lens);
+        ss.blockRays[b] = frustumFrom2D(block2D[b], S, in->lens);
+    }
+    ss.beams.resize(ss.padded);
+    for (uint32_t i = 0; i < ss.padded; i++) {
+        ss.beams[i].c = mul(S, mk(center[i].x, center[i].y, 1.0f));
+        ss.beams[i].du = mul(S, mk(major[i].x, major[i].y, 0.0f));
+        ss.beams[i].dv = mul(S, mk(minor[i].x, minor[i].y, 0.0f));
+    }
+    uint32_t split = in->split_color_samples;
+    ss.remap.assign(size_t(in->width) * in->height * split, -1);
+    for (uint32_t i = 0; i < n; i++) {
+        const hvvr_sample& s = sorted[i].s;
+        size_t idx = (size_t(s.pixel_y) * in->width + s.pixel_x) * split + sorted[i].channel;
+        if (idx < ss.remap.size()) ss.remap[idx] = int32_t(i);
+    }
+}
+
+// ------------------------------------------------------------------ traversal frustum
+// Frustum::Frustum (RC/traverse_avx.cpp:22-211), lane by lane.
+struct TravFrustum {
+    bool degenerate;
+    int distIdx; // 0..5: xMax, xNegMin, yMax, yNegMin, zMax, zNegMin
+    float tpLo[4][3], tpHi[4][3], w[4];
+    float proj[3][8];
+    float edge[12][3];
+    float minF[12], maxF[12];
+    V3 o[4], d[4];
+};
+
+void buildTravFrustum(const V3* origin, const V3* dir, TravFrustum& f) {
+    V4 plane[4];
+    V3 avg = mk(0, 0, 0);
+    for (int p = 0; p < 4; p++) {
+        f.o[p] = origin[p]; f.d[p] = dir[p];
+        if (isinf(origin[0].x)) {
+            plane[p] = V4{0, 0, 0, -INFINITY};
+        } else {
+            V3 n = cross(dir[p], dir[(p + 1) % 4]);
+            plane[p] = V4{n.x, n.y, n.z, dot(origin[p], n)};
+        }
+        avg = avg + dir[p];
+    }
+    f.degenerate = (plane[0].w == -INFINITY);
+    if (fabsf(avg.x) > fabsf(avg.y)) {
+        if (fabsf(avg.x) > fabsf(avg.z)) f.distIdx = avg.x < 0 ? 0 : 1;
+        else f.distIdx = avg.z < 0 ? 4 : 5;
+    } else {
+        if (fabsf(avg.y) > fabsf(avg.z)) f.distIdx = avg.y < 0 ? 2 : 3;
+        else f.distIdx = avg.z < 0 ? 4 : 5;
+    }
+    for (int p = 0; p < 4; p++) {
+        float c[3] = {plane[p].x, plane[p].y, plane[p].z};
+        for (int a = 0; a < 3; a++) {
+            f.tpLo[p][a] = c[a] < 0.0f ? c[a] : 0.0f;
+            f.tpHi[p][a] = c[a] > 0.0f ? -c[a] : 0.0f;
+        }
+        f.w[p] = plane[p].w;
+    }
+    // projections onto the axes: lanes 0-3 max side, lanes 4-7 -min side
+    for (int a = 0; a < 3; a++) {
+        float lane[8];
+        for (int i = 0; i < 4; i++) {
+            float oc = (&origin[i].x)[a], dc = (&dir[i].x)[a];
+            float so0 = -oc, so1 = -(-oc);
+            float nd0 = -dc, nd1 = -(-dc);
+            float m0 = (0.0f > nd0) ? 0.0f : nd0; // _mm256_max_ps(zero, v)
+            float m1 = (0.0f > nd1) ? 0.0f : nd1;
+            lane[i] = so0 + FLT_MAX * m0;
+            lane[4 + i] = so1 + FLT_MAX * m1;
+        }
+        float y[8], z[8];
+        static const int p1[4] = {2, 3, 0, 1}, p2[4] = {1, 0, 3, 2};
+        for (int h = 0; h < 2; h++)
+            for (int i = 0; i < 4; i++) { float a0 = lane[4 * h + i], b0 = lane[4 * h + p1[i]]; y[4 * h + i] = a0 > b0 ? a0 : b0; }
+        for (int h = 0; h < 2; h++)
+            for (int i = 0; i < 4; i++) { float a0 = y[4 * h + i], b0 = y[4 * h + p2[i]]; z[4 * h + i] = a0 > b0 ? a0 : b0; }
+        for (int i = 0; i < 8; i++) f.proj[a][i] = -z[i];
+    }
+    // edge axes d_i x e_k and the frustum's interval on each (RC/traverse_avx.cpp:152-210)
+    const V3 axes[3] = {mk(1, 0, 0), mk(0, 1, 0), mk(0, 0, 1)};
+    for (int i = 0; i < 4; i++)
+        for (int k = 0; k < 3; k++) {
+            V3 e = cross(dir[i], axes[k]);
+            f.edge[i * 3 + k][0] = e.x; f.edge[i * 3 + k][1] = e.y; f.edge[i * 3 + k][2] = e.z;
+        }
+    for (int e = 0; e < 12; e++) {
+        float ex = f.edge[e][0], ey = f.edge[e][1], ez = f.edge[e][2];
+        float mn = FLT_MAX, mx = -FLT_MAX;
+        for (int p = 0; p < 4; p++) {
+            float d0 = fmaf(ex, origin[p].x, fmaf(ey, origin[p].y, ez * origin[p].z));
+            mn = mn < d0 ? mn : d0;
+            mx = mx > d0 ? mx : d0;
+            float d1 = fmaf(ex, dir[p].x, fmaf(ey, dir[p].y, ez * dir[p].z));
+            const float eps = .000001f;
+            float a = d1 + eps, b = d1 - eps;
+            float amin = a < 0.0f ? a : 0.0f;  // _mm256_min_ps(a, zero)
+            float bmax = b > 0.0f ? b : 0.0f;  // _mm256_max_ps(b, zero)
+            mn = amin * FLT_MAX + mn;
+            mx = bmax * FLT_MAX + mx;
+        }
+        f.minF[e] = mn; f.maxF[e] = mx;
+    }
+}
+
+// Frustum::testBVHNodeChildren (RC/traverse_avx.h:104-164)
+uint32_t testChildren(const Node& n, const TravFrustum& f) {
+    uint32_t result = 0;
+    for (int c = 0; c < 4; c++) {
+        bool pass = true;
+        for (int p = 0; p < 4; p++) {
+            float lo = fmaf(f.tpLo[p][0], n.b[0][c], fmaf(f.tpLo[p][1], n.b[2][c], f.tpLo[p][2] * n.b[4][c]));
+            float hi = fmaf(f.tpHi[p][0], n.b[1][c], fmaf(f.tpHi[p][1], n.b[3][c], f.tpHi[p][2] * n.b[5][c]));
+            float d = lo + hi;
+            if (!(d <= f.w[p])) pass = false;
+        }
+        if (pass) result |= 1u << c;
+    }
+    if (!result) return 0;
+    uint32_t m = 0;
+    for (int c = 0; c < 4; c++) {
+        bool ok = true;
+        for (int a = 0; a < 3; a++) {
+            if (!(n.b[2 * a][c] >= f.proj[a][c])) ok = false;
+            if (!(n.b[2 * a + 1][c] >= f.proj[a][4 + c])) ok = false;
+        }
+        if (ok) m |= 1u << c;
+    }
+    return result & m;
+}
+
+// Frustum::testBVHNodeChildrenRefine (RC/traverse_avx.h:166-217)
+uint32_t refineChildren(const Node& n, const TravFrustum& f, uint32_t prev) {
+    uint32_t result = prev;
+    for (int e = 0; e < 12; e++) {
+        float ex = f.edge[e][0], ey = f.edge[e][1], ez = f.edge[e][2];
+        bool px = ex > 0.0f, py = ey > 0.0f, pz = ez > 0.0f;
+        for (int c = 0; c < 4; c++) {
+            float pX = (px ? n.b[0][c] : -n.b[1][c]) + 0.0f;
+            float pY = (py ? n.b[2][c] : -n.b[3][c]) + 0.0f;
+            float pZ = (pz ? n.b[4][c] : -n.b[5][c]) + 0.0f;
+            float nX = (px ? -n.b[1][c] : n.b[0][c]) + 0.0f;
+            float nY = (py ? -n.b[3][c] : n.b[2][c]) + 0.0f;
+            float nZ = (pz ? -n.b[5][c] : n.b[4][c]) + 0.0f;
+            float maxBox = fmaf(ex, pX, fmaf(ey, pY, ez * pZ));
+            float minBox = fmaf(ex, nX, fmaf(ey, nY, ez * nZ));
+            if ((maxBox < f.minF[e]) || (f.maxF[e] < minBox)) result &= ~(1u << c);
+        }
+    }
+    return result;
+}
+
+struct StackEntry { float tMin; uint32_t mask; uint32_t node; };
+struct CullEntry { uint32_t tDeltaBits; float tMinTemp; uint32_t node; };
+
+inline bool comigt(float a, float b) { return daz(a) > daz(b); }
+inline bool comilt(float a, float b) { return daz(a) < daz(b); }
+
+// traverseBlocks + BlockFrame::sort (RC/traverse_avx.h:293-410)
+uint32_t traverseBlock(const Node* nodes, const TravFrustum& f, StackEntry* sorted) {
+    if (f.degenerate) return 0;
+    CullEntry cull[kBlockStackSize + 4];
+    uint32_t top = 0;
+    float tMin = 0.0f;
+    uint32_t node = 0;
+    for (;;) {
+        const Node& nd = nodes[node];
+        uint32_t mask = testChildren(nd, f);
+        mask = refineChildren(nd, f, mask);
+        if (mask) {
+            uint32_t leaf = mask & nd.leafMask;
+            if (leaf) {
+                mask &= ~leaf;
+                uint32_t i = top;
+                while (comigt(i > 0 ? bitsf(cull[i - 1].tDeltaBits) : -1.0f, 0.0f)) { cull[i] = cull[i - 1]; --i; }
+                ++top;
+                cull[i] = CullEntry{leaf, tMin, node};
+            }
+            if (mask) {
+                float tMinK[4], tDeltaK[4];
+                int maxIdx = f.distIdx & ~1;
+                for (int k = 0; k < 4; k++) {
+                    tMinK[k] = bitsf(fbits(nd.b[f.distIdx][k]) ^ 0x80000000u);
+                    tDeltaK[k] = nd.b[maxIdx][k] + nd.b[maxIdx + 1][k];
+                }
+                do {
+                    int k = __builtin_ctz(mask);
+                    float td = tDeltaK[k];
+                    uint32_t i = top;
+                    while (comigt(i > 0 ? bitsf(cull[i - 1].tDeltaBits) : -1.0f, td)) { cull[i] = cull[i - 1]; --i; }
+                    cull[i] = CullEntry{fbits(td), tMinK[k], childOf(nodes, node, k)};
+                    mask &= mask - 1;
+                    ++top;
+                } while (mask);
+            }
+        }
+        // POP
+        if (top >= kBlockStackSize - 4 || top == 0 || cull[top - 1].tDeltaBits <= 0xf) break;
+        --top;
+        node = cull[top].node;
+        tMin = cull[top].tMinTemp;
+    }
+    uint32_t stackSize = top;
+    for (uint32_t t = 0; t < stackSize; t++) {
+        StackEntry data{cull[t].tMinTemp, cull[t].tDeltaBits, cull[t].node};
+        uint32_t slot = t;
+        while (comilt(slot > 0 ? sorted[slot - 1].tMin : INFINITY, data.tMin)) { sorted[slot] = sorted[slot - 1]; slot--; }
+        sorted[slot] = data;
+        if (cull[t].tDeltaBits > 0xf) sorted[slot].mask = 0;
+    }
+    return stackSize;
+}
+
+// traverseTiles (RC/traverse_avx.h:412-527)
+uint32_t traverseTile(const Node* nodes, const TravFrustum& f, const StackEntry* blockStack, uint32_t stackSize,
+                      std::vector<uint32_t>& out, uint32_t& status) {
+    out.clear();
+    if (f.degenerate || stackSize == 0) return 0;
+    std::vector<StackEntry> stack(blockStack, blockStack + stackSize);
+    stack.resize(kTileStackMax);
+    uint32_t top = stackSize - 1;
+    uint32_t node = stack[top].node;
+    for (;;) {
+        const Node& nd = nodes[node];
+        uint32_t mask = testChildren(nd, f);
+        bool descend = false;
+        if (mask) {
+            uint32_t leaf = mask & nd.leafMask;
+            if (leaf) {
+                mask = refineChildren(nd, f, mask);
+                leaf = mask & nd.leafMask;
+                uint32_t emit = leaf;
+                while (emit) {
+                    int k = __builtin_ctz(emit);
+                    uint32_t t0 = nd.tri[k], t1 = nd.tri[k + 1];
+                    if (t1 <= t0) status |= 2;
+                    for (uint32_t t = t0; t < t1; t++) out.push_back(t);
+                    emit &= emit - 1;
+                }
+            }
+            mask &= ~nd.leafMask;
+            if (mask && !stack[top].mask) {
+                float tMinK[4];
+                for (int k = 0; k < 4; k++) tMinK[k] = bitsf(fbits(nd.b[f.distIdx][k]) ^ 0x80000000u);
+                int k = __builtin_ctz(mask);
+                if (!(mask & (mask - 1))) {
+                    node = childOf(nodes, node, k);
+                    continue; // TEST
+                }
+                bool first = true;
+                do {
+                    if (!first) ++top;
+                    first = false;
+                    k = __builtin_ctz(mask);
+                    if (top + 1 >= kTileStackMax) { status |= 4; return uint32_t(out.size()); }
+                    float tm = tMinK[k];
+                    uint32_t i = top;
+                    while (comilt(i > 0 ? stack[i - 1].tMin : INFINITY, tm)) { stack[i] = stack[i - 1]; --i; }
+                    stack[i] = StackEntry{tm, 0, childOf(nodes, node, k)};
+                    mask &= mask - 1;
+                } while (mask);
+                descend = true;
+            }
+        }
+        if (descend) { node = stack[top].node; continue; } // POP_LAST
+        if (top == 0) break;                                 // POP
+        --top;
+        node = stack[top].node;
+    }
+    return uint32_t(out.size());
+}
+
+// ------------------------------------------------------------------ intersect (RC/prim_tests.h, RC/intersect.cu)
+struct FrustumPlanes { V4 p[4]; };
+// FrustumPlanes::FrustumPlanes (RC/prim_tests.h:22-28)
+FrustumPlanes makePlanes(const Rays4& r) {
+    FrustumPlanes fp;
+    for (int n = 0; n < 4; n++) {
+        V3 d = cross(r.d[n], r.d[(n + 1) % 4]);
+        fp.p[n] = V4{d.x, d.y, d.z, dot(r.o[n], d)};
+    }
+    return fp;
+}
+// FrustumPlanes::test (RC/prim_tests.h:30-49)
+bool planesTest(const FrustumPlanes& fp, const Tri& t) {
+    for (int n = 0; n < 4; n++) {
+        V3 dir = mk(fp.p[n].x, fp.p[n].y, fp.p[n].z);
+        float dist = fp.p[n].w;
+        float d0 = dot(dir, t.v0);
+        float d1 = d0 + dot(dir, t.e0);
+        float d2 = d0 + dot(dir, t.e1);
+        if (d0 > dist && d1 > dist && d2 > dist) return false;
+    }
+    return true;
+}
+// TestRayTriangle<false> (RC/prim_tests.h:53-82)
+V4 testRayTriangle(V3 ro, V3 rd, const Tri& tri) {
+    V3 n = cross(tri.e0, tri.e1);
+    float denom = dot(-rd, n);
+    V3 v0r = ro - tri.v0;
+    float t = dot(v0r, n);
+    V3 e = cross(-rd, v0r);
+    float v = dot(tri.e1, e);
+    float w = -dot(tri.e0, e);
+    float ood = 1.0f / denom;
+    t *= ood; v *= ood; w *= ood;
+    float u = 1.0f - v - w;
+    return V4{u, v, w, t};
+}
+// TestTriangleFrustaUVW (RC/prim_tests.h:89-116); returns true unless all-out
+bool uvwNotAllOut(const Rays4& r, const Tri& tri) {
+    V4 uvw[4];
+    for (int n = 0; n < 4; n++) uvw[n] = testRayTriangle(r.o[n], r.d[n], tri);
+    float uMin = FLT_MAX, uMax = -FLT_MAX, vMin = FLT_MAX, vMax = -FLT_MAX, wMin = FLT_MAX, wMax = -FLT_MAX;
+    for (int n = 0; n < 4; n++) {
+        uMin = tmin(uMin, uvw[n].x); uMax = tmax(uMax, uvw[n].x);
+        vMin = tmin(vMin, uvw[n].y); vMax = tmax(vMax, uvw[n].y);
+        wMin = tmin(wMin, uvw[n].z); wMax = tmax(wMax, uvw[n].z);
+    }
+    if (uMax < 0 || uMin > 1 || vMax < 0 || vMin > 1 || wMax < 0 || wMin > 1) return false;
+    return true;
+}
+
+struct TriTile { float t; V3 e0, e1, v0r; };
+// IntersectTriangleTile<false>::setup (RC/prim_tests.h:148-163)
+bool tileSetup(const Tri& tri, V3 ro, TriTile& tt) {
+    tt.e0 = tri.e0; tt.e1 = tri.e1;
+    V3 normal = cross(tt.e0, tt.e1);
+    tt.v0r = ro - tri.v0;
+    tt.t = dot(tt.v0r, normal);
+    return !(tt.t < 0.0f);
+}
+
+struct TriThread { float dc, vc, wc; V2 dd, dv, dw; };
+// IntersectTriangleThread ctor + GetDifferentials (RC/prim_tests.h:118-134, 175-188)
+TriThread threadSetup(const TriTile& tt, V3 c, V3 du, V3 dv) {
+    TriThread r;
+    V3 normal = cross(tt.e0, tt.e1);
+    r.dc = dot(-c, normal);
+    V3 ec = cross(-c, tt.v0r);
+    r.vc = dot(tt.e1, ec);
+    r.wc = -dot(tt.e0, ec);
+    V3 n2 = cross(tt.e0, tt.e1);
+    r.dd = V2{dot(-du, n2), dot(-dv, n2)};
+    r.dv = V2{dot(tt.e1, cross(-du, tt.v0r)), dot(tt.e1, cross(-dv, tt.v0r))};
+    r.dw = V2{-dot(tt.e0, cross(-du, tt.v0r)), -dot(tt.e0, cross(-dv, tt.v0r))};
+    return r;
+}
+// IntersectTriangleThread::test (RC/prim_tests.h:192-231)
+inline bool threadTest(const TriThread& th, float tt_t, V2 a, float& depth, bool fma) {
+    float denom, depthDelta, v, w;
+    if (fma) {
+        denom = fmaf(th.dd.y, a.y, fmaf(th.dd.x, a.x, th.dc));
+        depthDelta = fmaf(depth, denom, -tt_t);
+        v = fmaf(th.dv.y, a.y, fmaf(th.dv.x, a.x, th.vc));
+        w = fmaf(th.dw.y, a.y, fmaf(th.dw.x, a.x, th.wc));
+    } else {
+        denom = th.dc + th.dd.x * a.x + th.dd.y * a.y;
+        depthDelta = depth * denom - tt_t;
+        v = th.vc + th.dv.x * a.x + th.dv.y * a.y;
+        w = th.wc + th.dw.x * a.x + th.dw.y * a.y;
+    }
+    float u = denom - v - w;
+    int32_t test = int32_t(fbits(depthDelta) | fbits(u) | fbits(v) | fbits(w));
+    if (test < 0) return false;
+    depth = tt_t * (1.0f / denom);
+    return true;
+}
+// IntersectTriangleThread::calcUVW (RC/prim_tests.h:233-245)
+inline V3 calcUVW(const TriThread& th, V2 a, bool fma) {
+    float denom, v, w;
+    if (fma) {
+        denom = fmaf(th.dd.y, a.y, fmaf(th.dd.x, a.x, th.dc));
+        v = fmaf(th.dv.y, a.y, fmaf(th.dv.x, a.x, th.vc));
+        w = fmaf(th.dw.y, a.y, fmaf(th.dw.x, a.x, th.wc));
+    } else {
+        denom = th.dc + th.dd.x * a.x + th.dd.y * a.y;
+        v = th.vc + th.dv.x * a.x + th.dv.y * a.y;
+        w = th.wc + th.dw.x * a.x + th.dw.y * a.y;
+    }
+    float u = denom - v - w;
+    float inv = 1.0f / denom;
+    return mk(u * inv, v * inv, w * inv);
+}
+
+// ------------------------------------------------------------------ shading (RC/shading.h, RC/shading_helpers.h)
+const int kTau[] = {1,  1,  1,  2,  3,  2,  5,  2,  3,  2,  3,  3,  5,  5,  3,  4,  7,  5,  5,  7,
+                    9,  8,  5,  5,  7,  7,  7,  8,  5,  8,  11, 12, 7,  10, 13, 8,  11, 8,  7,  14};
+
+struct Material { V3 emissive, diffuse, specular; float glossiness; uint64_t code; };
+
+struct LightEnv {
+    int nd = 0, np = 0, ns = 0;
+    hvvr_light_directional dir[1];
+    hvvr_light_point pt[4];
+    hvvr_light_spot spot[4];
+};
+
+inline V3 v3(hvvr_vec3 v) { return mk(v.x, v.y, v.z); }
+inline float pow5(float x) { float x2 = x * x; return x2 * x2 * x; }
+
+// GGX_SchlickFresnel_SchlickSmithGGX (RC/shading_helpers.h:89-112)
+V3 ggxSpec(V3 N, V3 L, V3 V, float roughness, V3 F0) {
+    float alpha = roughness * roughness;
+    V3 H = normalize(L + V);
+    float alpha2 = alpha * alpha;
+    float NdotH = sat(dot(N, H));
+    float nh2 = NdotH * NdotH;
+    float q = nh2 * (alpha2 - 1.0f) + 1.0f;
+    float D = alpha2 / (3.141592653589f * (q * q));
+    float LdotH = sat(dot(L, H));
+    V3 F = F0 + (mk(1, 1, 1) - F0) * pow5(1.0f - LdotH);
+    float NdotL = sat(dot(N, L));
+    float NdotV = sat(dot(N, V));
+    float k = alpha * 0.5f;
+    float vis = (1.0f / (NdotL * (1.0f - k) + k)) * (1.0f / (NdotV * (1.0f - k) + k));
+    return divs((F * D) * vis, 4.0f);
+}
+// PBR_BRDF1 (RC/shading_helpers.h:115-122)
+V3 pbr(V3 L, V3 N, V3 V, V3 base, float roughness, V3 F0, V3 lightColor) {
+    V3 spec = ggxSpec(N, L, V, roughness, F0);
+    float NdotL = sat(dot(N, L));
+    V3 diffuse = ((base * lightColor) * (mk(1, 1, 1) - spec)) * NdotL;
+    V3 glossy = lightColor * spec;
+    return diffuse + glossy;
+}
+// GGXShade (RC/shading.h:84-161); materials carry no textures (badTextureIndex)
+V3 ggxShade(const Material& m, V3 pos, V3 nrm, V3 camPos, const LightEnv& env) {
+    V3 normal = normalize(nrm);
+    uint32_t model = uint32_t(m.code & 0xffff);
+    if (model == 2) return m.emissive; // emissive
+    V3 base = m.diffuse;
+    V3 V = normalize(camPos - pos);
+    V3 F0 = m.specular;
+    float roughness = 1.0f - m.glossiness;
+    V3 radiance = m.emissive;
+    radiance = radiance + base * mk(.15f, .15f, .165f);
+    for (int i = 0; i < env.nd && i < 1; i++)
+        radiance = radiance + pbr(v3(env.dir[i].direction), normal, V, base, roughness, F0, v3(env.dir[i].power));
+    for (int i = 0; i < env.np && i < 4; i++) {
+        const hvvr_light_point& l = env.pt[i];
+        V3 delta = v3(l.position) - pos;
+        float r = length(delta);
+        V3 L = normalize(delta);
+        float fd = sat((l.falloff_end - r) * l.falloff_scale);
+        radiance = radiance + pbr(L, normal, V, base, roughness, F0, v3(l.color) * fd);
+    }
+    for (int i = 0; i < env.ns && i < 4; i++) {
+        const hvvr_light_spot& l = env.spot[i];
+        V3 delta = v3(l.position) - pos;
+        float r = length(delta);
+        V3 L = normalize(delta);
+        float fd = sat((l.falloff_end - r) * l.falloff_scale);
+        V3 lit = pbr(L, normal, V, base, roughness, F0, v3(l.color) * fd);
+        float cosA = dot(v3(l.direction), -L);
+        float fa = sat((cosA - l.cos_outer_angle) * l.cos_angle_scale);
+        radiance = radiance + lit * fa;
+    }
+    return mk(tmax(radiance.x, 0.0f), tmax(radiance.y, 0.0f), tmax(radiance.z, 0.0f));
+}
+// ACESFilm + linearToSRgb + ToColor4Unorm8SRgb (RC/shading_helpers.h:158-200; SH/util_graphics.h:26-28)
+inline float aces(float x) {
+    float r = (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+    return sat(r);
+}
+inline float toSrgb(float x) { return (x <= 0.0031308f) ? (x * 12.92f) : (powf(x, (1.0f / 2.4f)) * 1.055f - .055f); }
+inline uint32_t packColor(V3 c) {
+    uint32_t r = uint32_t(toSrgb(c.x) * 255.0f), g = uint32_t(toSrgb(c.y) * 255.0f), b = uint32_t(toSrgb(c.z) * 255.0f);
+    uint32_t a = uint32_t(1.0f * 255.0f);
+    return r | (g << 8) | (b << 16) | (a << 24);
+}
+
+struct MxcsrScope {
+    unsigned saved;
+    MxcsrScope() { saved = _mm_getcsr(); _mm_setcsr(saved | 0x8040); }
+    ~MxcsrScope() { _mm_setcsr(saved); }
+};
+
+} // namespace
+
+extern "C" void oracle_msaa_offsets(uint32_t n, float* out) {
+    // tapLocation / getSubsampleUnitOffset with JITTER_SAMPLES=0 (RC/gpu_samples.h:35-61)
+    int turns = kTau[n];
+    for (uint32_t i = 0; i < n; i++) {
+        float alpha = float(int(i) + 0.5f) * (1.0f / float(n));
+        float angle = alpha * (float(turns) * 6.28f) + 0.0f;
+        float radius = sqrtf(alpha);
+        out[2 * i + 0] = cosf(angle) * radius;
+        out[2 * i + 1] = sinf(angle) * radius;
+    }
+}
+
+extern "C" void oracle_layout(uint32_t sample_count, uint32_t* blocks, uint32_t* tiles, uint32_t* padded) {
+    uint32_t b = (sample_count + kBlockSize - 1) / kBlockSize;
+    if (blocks) *blocks = b;
+    if (tiles) *tiles = b * kTilesPerBlock;
+    if (padded) *padded = b * kBlockSize;
+}
+
+extern "C" void oracle_scene_counts(const oracle_frame_in* in, uint32_t* nodes, uint32_t* tris, uint32_t* verts) {
+    uint32_t n = in->model_count ? (in->model_count + 1) / 3 : 1, t = 0, v = 0;
+    for (uint32_t m = 0; m < in->model_count; m++) {
+        n += in->models[m].node_count; t += in->models[m].tri_count; v += in->models[m].vert_count;
+    }
+    if (nodes) *nodes = n;
+    if (tris) *tris = t;
+    if (verts) *verts = v;
+}
+
+extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
+    MxcsrScope mx;
+    if (!in || !out || in->sample_count == 0) return 1;
+    uint32_t N = in->msaa;
+    if (!(N == 1 || N == 2 || N == 4 || N == 8 || N == 16 || N == 32)) return 1;
+    bool useFma = in->fp_mode == HVVR_FP_FMA;
+    out->status = 0;
+
+    Scene scene;
+    buildScene(in, scene);
+    refitScene(in, scene);
+    out->status |= scene.status;
+    if (out->nodes) memcpy(out->nodes, scene.nodes.data(), scene.nodes.size() * sizeof(Node));
+    if (out->tris) memcpy(out->tris, scene.tris.data(), scene.tris.size() * sizeof(Tri));
+
+    SampleSetup ss;
+    setupSamples(in, ss);
+    if (out->remap) memcpy(out->remap, ss.remap.data(), ss.remap.size() * sizeof(int32_t));
+    if (out->beams) memcpy(out->beams, ss.beams.data(), ss.beams.size() * sizeof(Beam));
+
+    // per-frame transform (RC/render.cpp:282-365, RC/traversal.h:38-47); no cull planes on the plain path
+    M4 c2w = transformToMatrix(in->cam_xf);
+    M3 R = m3of(c2w);
+    auto xformRays = [&](const Rays4& r) {
+        Rays4 w;
+        for (int v = 0; v < 4; v++) {
+            V4 o = mul(c2w, V4{r.o[v].x, r.o[v].y, r.o[v].z, 1.0f});
+            w.o[v] = mk(o.x, o.y, o.z);
+            w.d[v] = mul(R, r.d[v]);
+        }
+        return w;
+    };
+    std::vector<Rays4> tileW(ss.tiles), blockW(ss.blocks);
+    for (uint32_t i = 0; i < ss.tiles; i++) tileW[i] = xformRays(ss.tileRays[i]);
+    for (uint32_t i = 0; i < ss.blocks; i++) blockW[i] = xformRays(ss.blockRays[i]);
+
+    const Node* nodes = scene.nodes.data();
+    std::vector<StackEntry> blockStacks(size_t(ss.blocks) * kBlockStackSize);
+    std::vector<uint32_t> blockSizes(ss.blocks);
+    for (uint32_t b = 0; b < ss.blocks; b++) {
+        TravFrustum f;
+        buildTravFrustum(blockW[b].o, blockW[b].d, f);
+        blockSizes[b] = traverseBlock(nodes, f, &blockStacks[size_t(b) * kBlockStackSize]);
+        if (out->block_sizes) out->block_sizes[b] = blockSizes[b];
+        if (out->block_entries) {
+            for (uint32_t i = 0; i < kBlockStackSize; i++) {
+                const StackEntry& e = blockStacks[size_t(b) * kBlockStackSize + i];
+                uint32_t* dst = out->block_entries + (size_t(b) * kBlockStackSize + i) * 3;
+                if (i < blockSizes[b]) { dst[0] = fbits(e.tMin); dst[1] = e.mask; dst[2] = e.node; }
+                else { dst[0] = dst[1] = dst[2] = 0; }
+            }
+        }
+    }
+
+    // MSAA offsets and the lighting environment (GPUSceneState::updateLighting, RC/gpu_scene_state.cu:47-81)
+    std::vector<float> off(2 * N);
+    oracle_msaa_offsets(N, off.data());
+    LightEnv env;
+    for (uint32_t i = 0; i < in->light_count; i++) {
+        const hvvr_light_union& l = in->lights[i];
+        if (l.type == HVVR_LIGHT_DIRECTIONAL && env.nd < 1) env.dir[env.nd++] = l.u.directional;
+        else if (l.type == HVVR_LIGHT_POINT && env.np < 4) env.pt[env.np++] = l.u.point;
+        else if (l.type == HVVR_LIGHT_SPOT && env.ns < 4) env.spot[env.ns++] = l.u.spot;
+    }
+    std::vector<Material> mats(scene.materials.size());
+    for (size_t i = 0; i < mats.size(); i++) {
+        const hvvr_material& m = scene.materials[i];
+        mats[i] = Material{mk(m.emissive.x, m.emissive.y, m.emissive.z), mk(m.diffuse.x, m.diffuse.y, m.diffuse.z),
+                           mk(m.specular.x, m.specular.y, m.specular.z), m.glossiness, m.texture_ids_and_shading_model};
+    }
+    V3 camPos = mk(c2w.m3.x, c2w.m3.y, c2w.m3.z);
+
+    // tiles: traversal, then intersect + shade (RC/intersect.cu:171-342, RC/resolve.cu:161-458)
+    std::vector<std::vector<uint32_t>> lists(ss.tiles);
+    std::vector<uint32_t> colors(ss.padded, 0xFF000000u);
+    std::atomic<uint32_t> next(0), status(0);
+    auto worker = [&]() {
+        std::vector<uint32_t> scratch;
+        MxcsrScope mxw;
+        for (;;) {
+            uint32_t tile = next.fetch_add(1);
+            if (tile >= ss.tiles) break;
+            uint32_t b = tile / kTilesPerBlock;
+            TravFrustum f;
+            buildTravFrustum(tileW[tile].o, tileW[tile].d, f);
+            uint32_t st = 0;
+            traverseTile(nodes, f, &blockStacks[size_t(b) * kBlockStackSize], blockSizes[b], lists[tile], st);
+            if (st) status.fetch_or(st);
+            const std::vector<uint32_t>& list = lists[tile];
+            uint32_t base = tile * kTileSize;
+            if (list.empty()) {
+                // ClearEmptyKernel (RC/resolve.cu:527-542)
+                for (uint32_t s = 0; s < kTileSize; s++) {
+                    for (uint32_t i = 0; i < N; i++) {
+                        size_t o = size_t(base + s) * N + i;
+                        if (out->hit_ids) out->hit_ids[o] = ~0u;
+                        if (out->depth) out->depth[o] = INFINITY;
+                        if (out->depth64) out->depth64[o] = NAN;
+                        if (out->gb_tri) out->gb_tri[o] = (i == 0) ? ~0u : 0u;
+                        if (out->gb_mask) out->gb_mask[o] = (i == 0) ? (N == 32 ? ~0u : ((1u << N) - 1)) : 0u;
+                    }
+                    if (out->gb_n) out->gb_n[base + s] = 1;
+                    colors[base + s] = 0xFF000000u;
+                }
+                continue;
+            }
+            FrustumPlanes fp = makePlanes(tileW[tile]);
+            // per-chunk culling and compaction preserves list order, so the surviving sequence is
+            // the list filtered by the three pre-tests
+            std::vector<uint32_t> surv;
+            std::vector<TriTile> survTT;
+            surv.reserve(list.size());
+            for (uint32_t idx : list) {
+                const Tri& tri = scene.tris[idx];
+                if (!planesTest(fp, tri)) continue;
+                TriTile tt;
+                if (!tileSetup(tri, camPos, tt)) continue;
+                if (!uvwNotAllOut(tileW[tile], tri)) continue;
+                surv.push_back(idx);
+                survTT.push_back(tt);
+            }
+            for (uint32_t s = 0; s < kTileSize; s++) {
+                uint32_t sid = base + s;
+                const Beam& bm = ss.beams[sid];
+                V3 c = mul(R, bm.c), du = mul(R, bm.du), dv = mul(R, bm.dv);
+                float tmaxv[32];
+                uint32_t hit[32];
+                for (uint32_t i = 0; i < N; i++) { tmaxv[i] = FLT_MAX; hit[i] = ~0u; }
+                for (size_t j = 0; j < surv.size(); j++) {
+                    TriThread th = threadSetup(survTT[j], c, du, dv);
+                    for (uint32_t i = 0; i < N; i++) {
+                        V2 a{off[2 * i], off[2 * i + 1]};
+                        if (threadTest(th, survTT[j].t, a, tmaxv[i], useFma)) hit[i] = surv[j];
+                    }
+                }
+                for (uint32_t i = 0; i < N; i++) {
+                    size_t o = size_t(sid) * N + i;
+                    if (out->hit_ids) out->hit_ids[o] = hit[i];
+                    if (out->depth) out->depth[o] = hit[i] == ~0u ? INFINITY : tmaxv[i];
+                    if (out->depth64) {
+                        if (hit[i] == ~0u) out->depth64[o] = NAN;
+                        else {
+                            const Tri& t = scene.tris[hit[i]];
+                            double D[3] = {double(c.x) + double(off[2 * i]) * du.x + double(off[2 * i + 1]) * dv.x,
+                                           double(c.y) + double(off[2 * i]) * du.y + double(off[2 * i + 1]) * dv.y,
+                                           double(c.z) + double(off[2 * i]) * du.z + double(off[2 * i + 1]) * dv.z};
+                            double e0[3] = {t.e0.x, t.e0.y, t.e0.z}, e1[3] = {t.e1.x, t.e1.y, t.e1.z};
+                            double n[3] = {e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2],
+                                           e0[0] * e1[1] - e0[1] * e1[0]};
+                            double w0[3] = {double(camPos.x) - t.v0.x, double(camPos.y) - t.v0.y, double(camPos.z) - t.v0.z};
+                            double num = w0[0] * n[0] + w0[1] * n[1] + w0[2] * n[2];
+                            double den = -(D[0] * n[0] + D[1] * n[1] + D[2] * n[2]);
+                            out->depth64[o] = num / den;
+                        }
+                    }
+                }
+                // G-buffer compression (EmitGBuffer, RC/intersect.cu:28-89): pairs sorted by tri, misses last
+                uint32_t keys[32];
+                for (uint32_t i = 0; i < N; i++) keys[i] = (hit[i] << 5) | i;
+                std::sort(keys, keys + N);
+                uint32_t gtri[32], gmask[32], gn = 0;
+                for (uint32_t i = 0; i < N; i++) {
+                    uint32_t t = uint32_t(int32_t(keys[i]) >> 5);
+                    uint32_t m = 1u << (keys[i] & 31);
+                    if (gn && gtri[gn - 1] == t) gmask[gn - 1] |= m;
+                    else { gtri[gn] = t; gmask[gn] = m; gn++; }
+                }
+                if (out->gb_n) out->gb_n[sid] = gn;
+                for (uint32_t i = 0; i < N; i++) {
+                    if (out->gb_tri) out->gb_tri[size_t(sid) * N + i] = i < gn ? gtri[i] : 0;
+                    if (out->gb_mask) out->gb_mask[size_t(sid) * N + i] = i < gn ? gmask[i] : 0;
+                }
+                // ShadeMSAA (RC/resolve.cu:161-284), centroid shading per unique triangle
+                float res[4] = {0, 0, 0, 0};
+                uint32_t all = N == 32 ? ~0u : ((1u << N) - 1), combined = 0;
+                for (uint32_t g = 0; g < gn; g++) {
+                    if (combined == all) break;
+                    uint32_t triIndex = gtri[g];
+                    if (triIndex == ~0u) break;
+                    uint32_t sm = gmask[g];
+                    combined |= sm;
+                    float inv = 1.0f / float(__builtin_popcount(sm));
+                    V2 ca{0.0f, 0.0f};
+                    for (uint32_t cm = sm; cm;) {
+                        int si = __builtin_ctz(cm);
+                        cm &= ~(1u << si);
+                        ca.x = ca.x + off[2 * si] * inv;
+                        ca.y = ca.y + off[2 * si + 1] * inv;
+                    }
+                    const Tri& tri = scene.tris[triIndex];
+                    TriTile tt;
+                    tileSetup(tri, camPos, tt);
+                    TriThread th = threadSetup(tt, c, du, dv);
+                    V3 bc = calcUVW(th, ca, useFma);
+                    const hvvr_tri_shade& ts = scene.triShade[triIndex];
+                    const hvvr_shading_vertex& a0 = scene.world[ts.indices[0]];
+                    const hvvr_shading_vertex& a1 = scene.world[ts.indices[1]];
+                    const hvvr_shading_vertex& a2 = scene.world[ts.indices[2]];
+                    V3 pos = (v3(a0.pos) * bc.x + v3(a1.pos) * bc.y) + v3(a2.pos) * bc.z;
+                    V3 n0 = mk(halfToFloat(a0.normal[0]), halfToFloat(a0.normal[1]), halfToFloat(a0.normal[2]));
+                    V3 n1 = mk(halfToFloat(a1.normal[0]), halfToFloat(a1.normal[1]), halfToFloat(a1.normal[2]));
+                    V3 n2 = mk(halfToFloat(a2.normal[0]), halfToFloat(a2.normal[1]), halfToFloat(a2.normal[2]));
+                    V3 nrm = (n0 * bc.x + n1 * bc.y) + n2 * bc.z;
+                    V3 col = ggxShade(mats[ts.material], pos, nrm, camPos, env);
+                    float pc = float(__builtin_popcount(sm));
+                    res[0] = res[0] + col.x * pc; res[1] = res[1] + col.y * pc; res[2] = res[2] + col.z * pc;
+                }
+                float sN = 1.0f / float(N);
+                V3 lin = mk(res[0] * sN, res[1] * sN, res[2] * sN);
+                colors[sid] = packColor(mk(aces(lin.x), aces(lin.y), aces(lin.z)));
+            }
+        }
+    };
+    uint32_t nt = in->threads ? in->threads : 1;
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nt; t++) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    out->status |= status.load();
+
+    uint64_t total = 0;
+    for (uint32_t t = 0; t < ss.tiles; t++) {
+        if (out->tile_counts) out->tile_counts[t] = uint32_t(lists[t].size());
+        if (out->tile_indices) {
+            for (uint32_t v : lists[t]) {
+                if (total < out->tile_capacity) out->tile_indices[total] = v;
+                total++;
+            }
+        } else {
+            total += lists[t].size();
+        }
+    }
+    out->tile_total = total;
+    if (out->tile_indices && total > out->tile_capacity) out->status |= 8;
+    if (out->colors) memcpy(out->colors, colors.data(), colors.size() * 4);
+    // RemapKernel (RC/remap.cu:35-77)
+    if (out->image) {
+        uint32_t split = in->split_color_samples;
+        for (uint32_t y = 0; y < in->height; y++)
+            for (uint32_t x = 0; x < in->width; x++) {
+                size_t p = size_t(y) * in->width + x;
+                if (split == 1) {
+                    int32_t o = ss.remap[p];
+                    if (o >= 0) out->image[p] = colors[o];
+                } else {
+                    uint32_t c[3] = {0, 0, 0};
+                    for (uint32_t ch = 0; ch < split; ch++) {
+                        int32_t o = ss.remap[p * split + ch];
+                        if (o >= 0) c[ch] = colors[o];
+                    }
+                    out->image[p] = split == 2 ? ((c[1] & 0xff) | (c[0] & 0xff00) | (c[1] & 0xff0000) | 0xff000000u)
+                                               : ((c[0] & 0xff) | (c[1] & 0xff00) | (c[2] & 0xff0000) | 0xff000000u);
+                }
+            }
+    }
+    return 0;
+}

@@ -1,0 +1,76 @@
+/*
+ * hvvr_oracle.h - TEST INFRASTRUCTURE ONLY.
+ *
+ * Scalar CPU restatement of the reference's primary-visibility-and-shading path,
+ * used as the checker for the CUDA path. Nothing in the product links, loads or
+ * calls this library; only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg do.
+ *
+ * Parity pin: tests compare this restatement against the reference's own sources
+ * compiled here (oracle/refshim -> oracle/_ref) on committed seeded fixtures.
+ */
+#ifndef HVVR_ORACLE_H
+#define HVVR_ORACLE_H
+
+#include "../include/hvvr_c.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    /* scene: one entry per model (Raycaster::buildScene merges them) */
+    uint32_t model_count;
+    const hvvr_mesh_data* models;
+    const hvvr_transform* model_xf;
+    const hvvr_light_union* lights;
+    uint32_t light_count;
+    /* camera */
+    hvvr_float_rect viewport;
+    hvvr_thin_lens lens;
+    hvvr_transform cam_xf;
+    const hvvr_sample* samples;
+    uint32_t sample_count;
+    uint32_t split_color_samples;
+    uint32_t width, height;
+    uint32_t msaa;
+    uint32_t fp_mode; /* HVVR_FP_FMA or HVVR_FP_STRICT */
+    uint32_t threads; /* worker threads for the tile loop (0 = 1) */
+} oracle_frame_in;
+
+typedef struct {
+    /* every pointer may be NULL to skip that output */
+    uint32_t* block_sizes;     /* [blocks] */
+    uint32_t* block_entries;   /* [blocks*64*3] {tMin bits, mask, node} */
+    uint32_t* tile_counts;     /* [tiles] */
+    uint32_t* tile_indices;    /* concatenated, capacity entries */
+    uint64_t tile_capacity;
+    uint64_t tile_total;       /* written */
+    uint32_t* hit_ids;         /* [padded*msaa] */
+    float* depth;              /* [padded*msaa] */
+    double* depth64;           /* [padded*msaa] FP64 ray-triangle depth of the same hit (NaN on miss) */
+    uint32_t* gb_n;            /* [padded] */
+    uint32_t* gb_tri;          /* [padded*msaa] */
+    uint32_t* gb_mask;         /* [padded*msaa] */
+    uint32_t* colors;          /* [padded] RGBA8 */
+    uint32_t* image;           /* [height*width] RGBA8 */
+    int32_t* remap;            /* [height*width*split] */
+    float* beams;              /* [padded*9] camera-space DirectionalBeam */
+    void* nodes;               /* [node_count*128 bytes] refit BVH */
+    float* tris;               /* [tri_count*9] PrecomputedTriangleIntersect */
+    uint32_t status;           /* nonzero if a capacity was exceeded */
+} oracle_frame_out;
+
+/* sizes for a given sample count: blocks = ceil(n/8192) */
+void oracle_layout(uint32_t sample_count, uint32_t* blocks, uint32_t* tiles, uint32_t* padded);
+/* merged scene sizes for the given models */
+void oracle_scene_counts(const oracle_frame_in* in, uint32_t* nodes, uint32_t* tris, uint32_t* verts);
+/* runs the whole frame; returns 0 on success */
+int oracle_render(const oracle_frame_in* in, oracle_frame_out* out);
+/* MSAA unit offsets for rate n (n*2 floats), the spiral pattern of the reference */
+void oracle_msaa_offsets(uint32_t n, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

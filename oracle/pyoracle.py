@@ -1,0 +1,172 @@
+"""Python bindings of the CPU oracle and of the reference build (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs import
+this module. ``Oracle`` wraps oracle/libhvvr_oracle.so (the scalar restatement);
+``Reference`` wraps oracle/_ref/libhvvr_ref.so (the reference's own sources compiled here),
+which exists only where the reference tree was available at build time.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from hvvr_b200 import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libhvvr_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhvvr_ref.so")
+
+
+class FrameIn(C.Structure):
+    _fields_ = [("model_count", C.c_uint32), ("models", C.POINTER(_abi.MeshData)),
+                ("model_xf", C.POINTER(_abi.Transform)), ("lights", C.POINTER(_abi.LightUnion)),
+                ("light_count", C.c_uint32), ("viewport", _abi.FloatRect), ("lens", _abi.ThinLens),
+                ("cam_xf", _abi.Transform), ("samples", C.c_void_p), ("sample_count", C.c_uint32),
+                ("split_color_samples", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("msaa", C.c_uint32), ("fp_mode", C.c_uint32), ("threads", C.c_uint32)]
+
+
+class FrameOut(C.Structure):
+    _fields_ = [("block_sizes", C.c_void_p), ("block_entries", C.c_void_p), ("tile_counts", C.c_void_p),
+                ("tile_indices", C.c_void_p), ("tile_capacity", C.c_uint64), ("tile_total", C.c_uint64),
+                ("hit_ids", C.c_void_p), ("depth", C.c_void_p), ("depth64", C.c_void_p), ("gb_n", C.c_void_p),
+                ("gb_tri", C.c_void_p), ("gb_mask", C.c_void_p), ("colors", C.c_void_p), ("image", C.c_void_p),
+                ("remap", C.c_void_p), ("beams", C.c_void_p), ("nodes", C.c_void_p), ("tris", C.c_void_p),
+                ("status", C.c_uint32)]
+
+
+def layout(sample_count):
+    blocks = (sample_count + 8191) // 8192
+    return blocks, blocks * 64, blocks * 8192
+
+
+class Frame:
+    """Outputs of one rendered frame, as numpy arrays."""
+
+
+def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi.HVVR_FP_FMA, lens=(0.0, 1.0),
+         threads=None, split=1, want=("lists", "hits", "colors", "image", "blocks", "gbuffer", "scene", "beams"),
+         model_xf=None, tile_capacity=None):
+    if scene.nodes is None:
+        raise ValueError("scene has no topology")
+    n = len(samples)
+    blocks, tiles, padded = layout(n)
+    md = _abi.MeshData(_abi.ptr(scene.verts), len(scene.verts), _abi.ptr(scene.tri_shade), len(scene.tri_shade),
+                       _abi.ptr(scene.nodes), len(scene.nodes), _abi.ptr(scene.materials), len(scene.materials))
+    mds = (_abi.MeshData * 1)(md)
+    xfs = (_abi.Transform * 1)(model_xf if model_xf is not None else _abi.transform())
+    lights = (_abi.LightUnion * len(scene.lights))(*scene.lights)
+    fin = FrameIn()
+    fin.model_count = 1
+    fin.models = mds
+    fin.model_xf = xfs
+    fin.lights = lights
+    fin.light_count = len(scene.lights)
+    fin.viewport = viewport
+    fin.lens = _abi.ThinLens(*lens)
+    fin.cam_xf = cam_xf
+    fin.samples = _abi.ptr(samples)
+    fin.sample_count = n
+    fin.split_color_samples = split
+    fin.width, fin.height = width, height
+    fin.msaa = msaa
+    fin.fp_mode = fp_mode
+    fin.threads = threads if threads is not None else (os.cpu_count() or 1)
+    f = Frame()
+    out = FrameOut()
+    keep = []
+
+    def alloc(name, shape, dtype, field):
+        a = np.zeros(shape, dtype=dtype)
+        setattr(f, name, a)
+        setattr(out, field, a.ctypes.data)
+        keep.append(a)
+
+    if "blocks" in want:
+        alloc("block_sizes", blocks, np.uint32, "block_sizes")
+        alloc("block_entries", (blocks, 64, 3), np.uint32, "block_entries")
+    if "lists" in want:
+        alloc("tile_counts", tiles, np.uint32, "tile_counts")
+        cap = tile_capacity if tile_capacity is not None else 64 << 20
+        alloc("tile_indices", cap, np.uint32, "tile_indices")
+        out.tile_capacity = cap
+    if "hits" in want:
+        alloc("hit_ids", (padded, msaa), np.uint32, "hit_ids")
+        alloc("depth", (padded, msaa), np.float32, "depth")
+        alloc("depth64", (padded, msaa), np.float64, "depth64")
+    if "gbuffer" in want:
+        alloc("gb_n", padded, np.uint32, "gb_n")
+        alloc("gb_tri", (padded, msaa), np.uint32, "gb_tri")
+        alloc("gb_mask", (padded, msaa), np.uint32, "gb_mask")
+    if "colors" in want:
+        alloc("colors", padded, np.uint32, "colors")
+    if "image" in want:
+        alloc("image", (height, width), np.uint32, "image")
+        alloc("remap", height * width * split, np.int32, "remap")
+    if "beams" in want:
+        alloc("beams", (padded, 9), np.float32, "beams")
+    if "scene" in want:
+        alloc("nodes", len(scene.nodes), _abi.NODE_DTYPE, "nodes")
+        alloc("tris", (len(scene.tri_shade), 9), np.float32, "tris")
+    rc = fn(C.byref(fin), C.byref(out))
+    if rc != 0:
+        raise RuntimeError("render failed: %d" % rc)
+    f.status = out.status
+    f.tile_total = out.tile_total
+    if "lists" in want:
+        f.tile_indices = f.tile_indices[: min(out.tile_total, len(f.tile_indices))]
+        f.tile_offsets = np.concatenate([[0], np.cumsum(f.tile_counts, dtype=np.uint64)])
+    f.blocks, f.tiles, f.padded = blocks, tiles, padded
+    return f
+
+
+class Oracle:
+    def __init__(self, path=ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError("oracle library not built: %s" % path)
+        self.lib = C.CDLL(path)
+        self.lib.oracle_render.argtypes = [C.POINTER(FrameIn), C.POINTER(FrameOut)]
+        self.lib.oracle_render.restype = C.c_int
+        self.lib.oracle_msaa_offsets.argtypes = [C.c_uint32, C.c_void_p]
+
+    def render(self, *a, **k):
+        return _run(self.lib.oracle_render, *a, **k)
+
+    def msaa_offsets(self, n):
+        o = np.zeros((n, 2), dtype=np.float32)
+        self.lib.oracle_msaa_offsets(n, o.ctypes.data)
+        return o
+
+
+class Reference:
+    """The reference's own sources compiled here (oracle/_ref)."""
+
+    def __init__(self, path=REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError("reference build not present: %s" % path)
+        self.lib = C.CDLL(path)
+        self.lib.ref_render.argtypes = [C.POINTER(FrameIn), C.POINTER(FrameOut)]
+        self.lib.ref_render.restype = C.c_int
+        self.lib.ref_generate_topology.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                                   C.c_uint32, C.POINTER(C.c_uint32)]
+        self.lib.ref_generate_topology.restype = C.c_int
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_SO)
+
+    def render(self, *a, **k):
+        return _run(self.lib.ref_render, *a, **k)
+
+    def generate_topology(self, scene):
+        """GenerateTopology on copies of the scene arrays; returns (verts, tri_shade, nodes)."""
+        verts = scene.verts.copy()
+        tris = scene.tri_shade.copy()
+        cap = len(tris) + 4
+        nodes = np.zeros(cap, dtype=_abi.TOPO_DTYPE)
+        cnt = C.c_uint32(0)
+        rc = self.lib.ref_generate_topology(verts.ctypes.data, len(verts), tris.ctypes.data, len(tris),
+                                            nodes.ctypes.data, cap, C.byref(cnt))
+        if rc != 0:
+            raise RuntimeError("GenerateTopology failed: %d" % rc)
+        return verts, tris, nodes[: cnt.value].copy()

@@ -1,0 +1,30 @@
+# Compiles the reference's own sources, unmodified and in place, plus the harness in this
+# directory into _ref/libhvvr_ref.so. Test infrastructure only: run from oracle/ by the
+# oracle Makefile when the reference tree is present. Output goes to _ref/ (git-ignored).
+REF_ROOT ?= /root/reference
+RC = $(REF_ROOT)/libraries/hvvr/raycaster
+SH = $(REF_ROOT)/libraries/hvvr/shared
+CUDA_INC ?= /usr/local/cuda/include
+CXX ?= g++
+# -ffp-contract=off: the reference's host code is built without contraction (MSVC /fp:precise)
+REF_FLAGS = -std=c++17 -O2 -fPIC -mavx2 -mfma -mf16c -mbmi -mbmi2 -ffp-contract=off -fpermissive -w -pthread \
+            -include refshim/compat/hvvr_gcc_compat.h -Irefshim/compat -I$(SH) -I$(RC) -I$(CUDA_INC)
+REF_SRCS = $(RC)/traverse_avx.cpp $(RC)/sample_hierarchy.cpp $(RC)/samples.cpp $(RC)/camera.cpp \
+           $(RC)/foveated.cpp $(SH)/bvh.cpp $(SH)/debug.cpp
+OBJS = $(patsubst %.cpp,_ref/obj/%.o,$(notdir $(REF_SRCS))) _ref/obj/ref_harness.o _ref/obj/ref_stubs.o
+
+_ref/libhvvr_ref.so: $(OBJS)
+	$(CXX) -shared -pthread -o $@ $(OBJS)
+
+_ref/obj/%.o: $(RC)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
+	@mkdir -p _ref/obj
+	$(CXX) $(REF_FLAGS) -c $< -o $@
+_ref/obj/%.o: $(SH)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
+	@mkdir -p _ref/obj
+	$(CXX) $(REF_FLAGS) -c $< -o $@
+_ref/obj/ref_harness.o: refshim/ref_harness.cpp hvvr_oracle.h ../include/hvvr_c.h refshim/compat/hvvr_gcc_compat.h
+	@mkdir -p _ref/obj
+	$(CXX) $(REF_FLAGS) -c $< -o $@
+_ref/obj/ref_stubs.o: refshim/ref_stubs.cpp refshim/compat/hvvr_gcc_compat.h
+	@mkdir -p _ref/obj
+	$(CXX) $(REF_FLAGS) -c $< -o $@

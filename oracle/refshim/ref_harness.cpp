@@ -1,0 +1,380 @@
+// ref_harness.cpp - TEST INFRASTRUCTURE ONLY.
+//
+// Drives the reference's own sources (compiled unmodified from the reference tree by
+// oracle/refshim/ref.mk) through the same C API as the oracle, so tests can pin the
+// oracle restatement against the reference's code:
+//   * SampleData (RC/camera.cpp:21-64) for sorting, 2D->3D frusta and beams;
+//   * frustumTransform (RC/traversal.h:38-47) and traverse::avx::Frustum (RC/traverse_avx.cpp);
+//   * traverseBlocks / BlockFrame::sort / traverseTiles (RC/traverse_avx.h) driven exactly
+//     like cullThread (RC/traversal.cpp:99-190);
+//   * the kernels' per-thread math compiled for the host: FrustumPlanes,
+//     IntersectTriangleTile<false>, TestTriangleFrustaUVW, IntersectTriangleThread
+//     (RC/prim_tests.h), getSubsampleUnitOffset (RC/gpu_samples.h), sortBitonic (RC/sort.h),
+//     interpolate / GGXShade / ACESFilm / ToColor4Unorm8SRgb (RC/shading*.h);
+//   * GenerateTopology (SH/bvh.cpp).
+// The kernel control structure (128-triangle chunks, order-preserving compaction, the
+// G-buffer grouping and the MSAA resolve loop of RC/intersect.cu and RC/resolve.cu) and the
+// GPU refit kernels cannot run on a CPU as written; they are restated here around the
+// reference functions, with -ffp-contract=off (the HVVR_FP_STRICT arithmetic).
+
+#define TRAVERSAL_IMP 1
+#include "traversal.h"
+
+#include "bvh.h"
+#include "bvh_node.h"
+#include "camera.h"
+#include "gpu_samples.h"
+#include "graphics_types.h"
+#include "light.h"
+#include "lighting_env.h"
+#include "material.h"
+#include "model.h"
+#include "prim_tests.h"
+#include "shading.h"
+#include "sort.h"
+
+#include "../hvvr_oracle.h"
+
+#include <atomic>
+#include <thread>
+
+uint3 threadIdx;
+uint3 blockIdx;
+
+namespace hvvr {
+// Link stubs for GPU-side classes referenced by camera.cpp's Camera methods. The harness
+// only constructs SampleData, so none of these run.
+class GPUCamera;
+class GPUContext;
+} // namespace hvvr
+
+using namespace hvvr;
+
+namespace {
+
+struct MxcsrScope {
+    unsigned saved;
+    MxcsrScope() { saved = _mm_getcsr(); _mm_setcsr(saved | 0x8040); }
+    ~MxcsrScope() { _mm_setcsr(saved); }
+};
+
+inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+inline float bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+template <uint32_t N> vector2 subOffset(int i) { return getSubsampleUnitOffset<N>(vector2(0.0f, 0.0f), i); }
+vector2 subsampleOffset(uint32_t n, int i) {
+    switch (n) {
+    case 1: return subOffset<1>(i);
+    case 2: return subOffset<2>(i);
+    case 4: return subOffset<4>(i);
+    case 8: return subOffset<8>(i);
+    case 16: return subOffset<16>(i);
+    default: return subOffset<32>(i);
+    }
+}
+
+} // namespace
+
+extern "C" int ref_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr_tri_shade* tri_shade,
+                                     uint32_t tri_count, hvvr_topology_node* nodes_out, uint32_t capacity,
+                                     uint32_t* node_count) {
+    MeshData mesh;
+    mesh.verts.assign((ShadingVertex*)verts, (ShadingVertex*)verts + vert_count);
+    mesh.triShade.assign((PrecomputedTriangleShade*)tri_shade, (PrecomputedTriangleShade*)tri_shade + tri_count);
+    if (!GenerateTopology(mesh)) return 1;
+    if (mesh.nodes.size() > capacity) return 2;
+    memcpy(verts, mesh.verts.data(), vert_count * sizeof(ShadingVertex));
+    memcpy(tri_shade, mesh.triShade.data(), tri_count * sizeof(PrecomputedTriangleShade));
+    memcpy(nodes_out, mesh.nodes.data(), mesh.nodes.size() * sizeof(TopologyNode));
+    *node_count = uint32_t(mesh.nodes.size());
+    return 0;
+}
+
+extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
+    MxcsrScope mx;
+    if (in->model_count != 1 || in->sample_count == 0) return 1; // harness covers single-model scenes
+    const uint32_t N = in->msaa;
+    out->status = 0;
+    const hvvr_mesh_data& md = in->models[0];
+
+    // scene build for one model (RC/scene_update.cpp:86-101 with offsets 0, no root fix-up)
+    DynamicArray<BVHNode> nodes(md.node_count);
+    memset(nodes.data(), 0, md.node_count * sizeof(BVHNode));
+    for (uint32_t n = 0; n < md.node_count; n++) {
+        const TopologyNode& tn = ((const TopologyNode*)md.nodes)[n];
+        BVHNode& node = nodes[n];
+        node.boxData.leafMask = tn.leafMask;
+        node.boxData.leaf.triIndex[0] = tn.getFirstTriangleIndex(0);
+        for (size_t k = 0; k < 4; k++) {
+            if (tn.isLeaf(k)) node.boxData.leaf.triIndex[1 + k] = tn.getBoundTriangleIndex(k);
+            else node.boxData.children.offset[k] = tn.getChildOffset(k);
+        }
+    }
+    // refit (restatement of RC/gpu_scene_state.cu:88-375 with the reference's types and operators)
+    matrix4x4 modelToWorld = matrix4x4(*(const transform*)&in->model_xf[0]);
+    std::vector<ShadingVertex> world(md.vert_count);
+    for (uint32_t i = 0; i < md.vert_count; i++) {
+        ShadingVertex vertex = ((const ShadingVertex*)md.verts)[i];
+        vector4 fp = modelToWorld * vector4(vertex.pos, 1.0);
+        vertex.pos = vector3(fp) * (1.0f / fp.w);
+        vertex.normal = vector4h(normalize(matrix3x3(modelToWorld) * vector3(vertex.normal)));
+        world[i] = vertex;
+    }
+    const PrecomputedTriangleShade* triShade = (const PrecomputedTriangleShade*)md.tri_shade;
+    std::vector<uint32_t> triToNodeChild(md.tri_count, 0);
+    for (int64_t n = int64_t(md.node_count) - 1; n >= 0; --n) {
+        for (int k = 3; k >= 0; k--) {
+            if (_bittest((const long*)&nodes[n].boxData.leafMask, k)) {
+                for (uint32_t t = nodes[n].boxData.leaf.triIndex[k]; t < nodes[n].boxData.leaf.triIndex[k + 1]; t++)
+                    triToNodeChild[t] = (uint32_t(n) << 2) | uint32_t(k);
+            }
+        }
+    }
+    std::vector<uint32_t> flip(size_t(md.node_count) * 24, FloatFlip(0xff800000));
+    std::vector<PrecomputedTriangleIntersect> tris(md.tri_count);
+    for (uint32_t i = 0; i < md.tri_count; i++) {
+        vector3 v0 = world[triShade[i].indices[0]].pos, v1 = world[triShade[i].indices[1]].pos,
+                v2 = world[triShade[i].indices[2]].pos;
+        tris[i].v0 = v0; tris[i].edge0 = v1 - v0; tris[i].edge1 = v2 - v0;
+        float mx3[3] = {max(v0.x, max(v1.x, v2.x)), max(v0.y, max(v1.y, v2.y)), max(v0.z, max(v1.z, v2.z))};
+        float nm3[3] = {max(-v0.x, max(-v1.x, -v2.x)), max(-v0.y, max(-v1.y, -v2.y)), max(-v0.z, max(-v1.z, -v2.z))};
+        uint32_t parent = triToNodeChild[i] >> 2, slot = triToNodeChild[i] & 3;
+        for (int a = 0; a < 3; a++) {
+            uint32_t& m = flip[size_t(parent) * 24 + 8 * a + slot];
+            uint32_t& g = flip[size_t(parent) * 24 + 8 * a + 4 + slot];
+            m = std::max(m, FloatFlipF(mx3[a]));
+            g = std::max(g, FloatFlipF(nm3[a]));
+        }
+    }
+    for (uint32_t n = 0; n < md.node_count; n++) {
+        float* b = nodes[n].xMax;
+        for (int j = 0; j < 24; j++) b[j] = IFloatFlipF(flip[size_t(n) * 24 + j]);
+    }
+    std::vector<uint32_t> depthOf(md.node_count, 0);
+    uint32_t maxDepth = 0;
+    for (uint32_t n = 0; n < md.node_count; n++)
+        for (int k = 3; k >= 0; k--)
+            if (!_bittest((const long*)&nodes[n].boxData.leafMask, k)) {
+                uint32_t c = n + nodes[n].boxData.children.offset[k];
+                depthOf[c] = depthOf[n] + 1;
+                maxDepth = std::max(maxDepth, depthOf[c]);
+            }
+    for (int64_t d = maxDepth; d >= 0; d--)
+        for (uint32_t n = 0; n < md.node_count; n++) {
+            if (depthOf[n] != d) continue;
+            for (int k = 0; k < 4; k++) {
+                if (_bittest((const long*)&nodes[n].boxData.leafMask, k)) continue;
+                const float* bp = nodes[n + nodes[n].boxData.children.offset[k]].xMax;
+                float* pb = nodes[n].xMax;
+                for (int j = 0; j < 6; j++)
+                    pb[j * 4 + k] = max(bp[j * 4 + 0], max(bp[j * 4 + 1], max(bp[j * 4 + 2], bp[j * 4 + 3])));
+            }
+        }
+    if (out->nodes) memcpy(out->nodes, nodes.data(), md.node_count * sizeof(BVHNode));
+    if (out->tris) memcpy(out->tris, tris.data(), md.tri_count * sizeof(PrecomputedTriangleIntersect));
+
+    // samples: the reference's SampleData with Camera::getSampleToCamera (RC/camera.cpp:167-171)
+    const FloatRect vp(vector2(in->viewport.lower.x, in->viewport.lower.y), vector2(in->viewport.upper.x, in->viewport.upper.y));
+    matrix3x3 sampleToCamera(vector3(vp.upper.x - vp.lower.x, 0, 0), vector3(0, vp.lower.y - vp.upper.y, 0),
+                             vector3(vp.lower.x, vp.upper.y, -1));
+    ThinLens lens{in->lens.radius, in->lens.focal_distance};
+    SampleData sd((const Sample*)in->samples, in->sample_count, in->split_color_samples,
+                  Sample2Dto3DMappingSettings(sampleToCamera, lens), in->width, in->height);
+    const BeamBatch& batch = sd.samples;
+    uint32_t blockCount = uint32_t(batch.blockFrusta3D.size());
+    uint32_t tileCount = uint32_t(batch.tileFrusta3D.size());
+    uint32_t padded = uint32_t(batch.directionalBeams.size());
+    if (out->remap) memcpy(out->remap, sd.imageLocationToSampleIndex.data(), sd.imageLocationToSampleIndex.size() * 4);
+    if (out->beams) memcpy(out->beams, batch.directionalBeams.data(), size_t(padded) * sizeof(DirectionalBeam));
+
+    // per-frame transform (transformHierarchyCameraToWorld without cull planes, RC/render.cpp:293-310)
+    matrix4x4 cameraToWorld = matrix4x4(*(const transform*)&in->cam_xf);
+    DynamicArray<Frustum> blocksW(blockCount), tilesW(tileCount);
+    std::vector<SimpleRayFrustum> simple(tileCount);
+    for (uint32_t b = 0; b < blockCount; b++) blocksW[b] = frustumTransform(batch.blockFrusta3D[b], cameraToWorld);
+    for (uint32_t t = 0; t < tileCount; t++) {
+        tilesW[t] = frustumTransform(batch.tileFrusta3D[t], cameraToWorld);
+        for (int n = 0; n < Frustum::pointCount; n++) {
+            simple[t].origins[n] = tilesW[t].pointOrigin[n];
+            simple[t].directions[n] = tilesW[t].pointDir[n];
+        }
+    }
+
+    // cullThread (RC/traversal.cpp:99-190), one block at a time
+    std::vector<std::vector<uint32_t>> lists(tileCount);
+    std::vector<uint32_t> scratch(1 << 20);
+    for (uint32_t b = 0; b < blockCount; b++) {
+        BlockFrame blockFrame;
+        uint32_t stackSize = traverseBlocks(blockFrame, nodes.data(), blocksW[b]);
+        if (out->block_sizes) out->block_sizes[b] = stackSize;
+        if (!stackSize) {
+            if (out->block_entries) memset(out->block_entries + size_t(b) * 64 * 3, 0, 64 * 3 * 4);
+            continue;
+        }
+        blockFrame.sort(stackSize);
+        if (out->block_entries) {
+            for (uint32_t i = 0; i < 64; i++) {
+                uint32_t* dst = out->block_entries + (size_t(b) * 64 + i) * 3;
+                if (i < stackSize) {
+                    dst[0] = fbits(blockFrame.sortedStack[i].tMin);
+                    dst[1] = blockFrame.sortedStack[i].mask;
+                    dst[2] = uint32_t(blockFrame.sortedStack[i].node - nodes.data());
+                } else {
+                    dst[0] = dst[1] = dst[2] = 0;
+                }
+            }
+        }
+        for (uint32_t ti = 0; ti < TILES_PER_BLOCK; ti++) {
+            uint32_t tile = b * TILES_PER_BLOCK + ti;
+            TileFrame tileFrame;
+            for (uint32_t slot = 0; slot != stackSize; ++slot)
+                store(&(tileFrame.stack + slot)->tMin, load_m128(&(blockFrame.sortedStack + slot)->tMin));
+            uint32_t count = traverseTiles(scratch.data(), uint32_t(scratch.size()), tileFrame, stackSize, tilesW[tile]);
+            lists[tile].assign(scratch.begin(), scratch.begin() + count);
+        }
+    }
+
+    // lighting environment (GPUSceneState::updateLighting, RC/gpu_scene_state.cu:47-81)
+    LightingEnvironment env;
+    memset(&env, 0, sizeof(env));
+    for (uint32_t i = 0; i < in->light_count; i++) {
+        const LightUnion& l = ((const LightUnion*)in->lights)[i];
+        if (l.type == LightType::directional && env.directionalLightCount < int(MAX_DIRECTIONAL_LIGHTS))
+            env.directionalLights[env.directionalLightCount++] = l.directional;
+        else if (l.type == LightType::point && env.pointLightCount < int(MAX_POINT_LIGHTS))
+            env.pointLights[env.pointLightCount++] = l.point;
+        else if (l.type == LightType::spot && env.spotLightCount < int(MAX_SPOT_LIGHTS))
+            env.spotLights[env.spotLightCount++] = l.spot;
+    }
+    const SimpleMaterial* materials = (const SimpleMaterial*)md.materials;
+    vector3 cameraPos = vector3(cameraToWorld.m3);
+    std::vector<vector2> alphaTab(N);
+    for (uint32_t i = 0; i < N; i++) alphaTab[i] = subsampleOffset(N, int(i));
+    uint32_t maskAll = N < 32 ? ((1u << N) - 1) : ~0u;
+    std::vector<uint32_t> colors(padded, 0xFF000000u);
+
+    std::atomic<uint32_t> next(0);
+    auto worker = [&]() {
+        MxcsrScope mxw;
+        for (;;) {
+            uint32_t tile = next.fetch_add(1);
+            if (tile >= tileCount) break;
+            const std::vector<uint32_t>& list = lists[tile];
+            uint32_t base = tile * TILE_SIZE;
+            if (list.empty()) {
+                for (uint32_t s = 0; s < TILE_SIZE; s++) {
+                    for (uint32_t i = 0; i < N; i++) {
+                        size_t o = size_t(base + s) * N + i;
+                        if (out->hit_ids) out->hit_ids[o] = ~0u;
+                        if (out->depth) out->depth[o] = INFINITY;
+                        if (out->gb_tri) out->gb_tri[o] = i == 0 ? ~0u : 0u;
+                        if (out->gb_mask) out->gb_mask[o] = i == 0 ? maskAll : 0u;
+                    }
+                    if (out->gb_n) out->gb_n[base + s] = 1;
+                }
+                continue;
+            }
+            // IntersectKernel / IntersectTile (RC/intersect.cu:171-342)
+            FrustumPlanes planes(simple[tile]);
+            std::vector<uint32_t> survIdx;
+            std::vector<IntersectTriangleTile<false>> survTile;
+            for (uint32_t idx : list) {
+                const PrecomputedTriangleIntersect& tri = tris[idx];
+                if (!planes.test(tri)) continue;
+                IntersectTriangleTile<false> tt;
+                if (tt.setup(tri, cameraPos) == intersect_all_out) continue;
+                if (TestTriangleFrustaUVW(simple[tile], tri) == intersect_all_out) continue;
+                survIdx.push_back(idx);
+                survTile.push_back(tt);
+            }
+            for (uint32_t s = 0; s < TILE_SIZE; s++) {
+                uint32_t sid = base + s;
+                DirectionalBeam sample = matrix3x3(cameraToWorld) * batch.directionalBeams[sid];
+                float tmaxv[32];
+                uint32_t hit[32];
+                for (uint32_t i = 0; i < N; i++) { tmaxv[i] = FLT_MAX; hit[i] = ~0u; }
+                for (size_t j = 0; j < survIdx.size(); j++) {
+                    IntersectTriangleThread th(survTile[j], sample.centerRay, sample.du, sample.dv);
+                    for (uint32_t i = 0; i < N; i++)
+                        if (th.test(survTile[j], alphaTab[i], tmaxv[i])) hit[i] = survIdx[j];
+                }
+                for (uint32_t i = 0; i < N; i++) {
+                    size_t o = size_t(sid) * N + i;
+                    if (out->hit_ids) out->hit_ids[o] = hit[i];
+                    if (out->depth) out->depth[o] = hit[i] == ~0u ? INFINITY : tmaxv[i];
+                }
+                // EmitGBuffer grouping (RC/intersect.cu:51-87) with the reference's sortBitonic
+                uint32_t keys[32];
+                for (uint32_t i = 0; i < N; i++) keys[i] = (hit[i] << 5) | i;
+                sortBitonic(keys, int(N));
+                uint32_t gtri[32], gmask[32], gn = 0;
+                gtri[0] = uint32_t(int32_t(keys[0]) >> 5);
+                gmask[0] = 1u << (keys[0] & 31);
+                gn = 1;
+                for (uint32_t i = 1; i < N; i++) {
+                    uint32_t t = uint32_t(int32_t(keys[i]) >> 5), m = 1u << (keys[i] & 31);
+                    if (gtri[gn - 1] == t) gmask[gn - 1] |= m;
+                    else { gtri[gn] = t; gmask[gn] = m; gn++; }
+                }
+                if (out->gb_n) out->gb_n[sid] = gn;
+                for (uint32_t i = 0; i < N; i++) {
+                    if (out->gb_tri) out->gb_tri[size_t(sid) * N + i] = i < gn ? gtri[i] : 0;
+                    if (out->gb_mask) out->gb_mask[size_t(sid) * N + i] = i < gn ? gmask[i] : 0;
+                }
+                // ShadeMSAA, non-DoF branch (RC/resolve.cu:161-284)
+                vector4 result(0.0f, 0.0f, 0.0f, 0.0f);
+                uint32_t combined = 0;
+                for (uint32_t g = 0; g < gn; g++) {
+                    if (combined == maskAll) break;
+                    uint32_t triIndex = gtri[g];
+                    if (triIndex == ~0u) break;
+                    uint32_t sampleMask = gmask[g];
+                    combined |= sampleMask;
+                    float sampleCountInv = 1.0f / __builtin_popcount(sampleMask);
+                    vector2 centroidAlpha(0.0f, 0.0f);
+                    for (uint32_t cm = sampleMask; cm != 0;) {
+                        int si = __builtin_ctz(cm);
+                        cm &= ~(1u << si);
+                        centroidAlpha += alphaTab[si] * sampleCountInv;
+                    }
+                    IntersectTriangleTile<false> tt;
+                    tt.setup(tris[triIndex], cameraPos);
+                    IntersectTriangleThread th(tt, sample.centerRay, sample.du, sample.dv);
+                    vector3 b;
+                    th.calcUVW(tt, centroidAlpha, b);
+                    InterpolatedVertex vI = interpolate(world.data(), triShade[triIndex], b);
+                    vector4 shaded = GGXShade(triShade[triIndex].material, vI, vector2(0.0f), vector2(0.0f), cameraPos,
+                                              materials, nullptr, env);
+                    result += shaded * float(__builtin_popcount(sampleMask));
+                }
+                result *= 1.0f / N;
+                result.w = 1.0f;
+                colors[sid] = ToColor4Unorm8SRgb(ACESFilm(result));
+            }
+        }
+    };
+    uint32_t nt = in->threads ? in->threads : 1;
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nt; t++) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+
+    uint64_t total = 0;
+    for (uint32_t t = 0; t < tileCount; t++) {
+        if (out->tile_counts) out->tile_counts[t] = uint32_t(lists[t].size());
+        for (uint32_t v : lists[t]) {
+            if (out->tile_indices && total < out->tile_capacity) out->tile_indices[total] = v;
+            total++;
+        }
+    }
+    out->tile_total = total;
+    if (out->colors) memcpy(out->colors, colors.data(), size_t(padded) * 4);
+    if (out->image) {
+        for (uint32_t y = 0; y < in->height; y++)
+            for (uint32_t x = 0; x < in->width; x++) {
+                int32_t o = sd.imageLocationToSampleIndex[size_t(y) * in->width + x];
+                if (o >= 0 && in->split_color_samples == 1) out->image[size_t(y) * in->width + x] = colors[o];
+            }
+    }
+    return 0;
+}
