@@ -1,0 +1,378 @@
+"""Benchmark: primary visibility + shading of a stereo VR frame on one B200 per rank.
+
+Workload (the configuration the headline metric is quoted on): a 995,072-triangle seeded
+procedural scene (256x256-quad heightfield + 72,000 boxes), two eyes of 1080x1200 with a
+64 mm IPD, per-pixel sample positions warped by barrel distortion
+r' = r (1 + 0.22 r^2 + 0.24 r^4), 8x MSAA, GGX shading with 1 directional + 4 point lights.
+
+One step = one stereo frame through the full path on the GPU: block cull, tile cull,
+intersect + G-buffer compression + shade + resolve, remap to the eye images.
+
+value  : Gsamples/s with everything resident in HBM (device images), device-timed with
+         CUDA events per frame; an L2 flush (a 256 MiB write) separates frames and is not timed.
+e2e    : the same metric through the C ABI with CPU_MEMORY render targets: the per-frame
+         camera transforms go in, both RGBA8 images come back to host memory inside the timing.
+Multi-GPU (torchrun): replicas - each rank renders its own stereo frame; no collective on
+the data path. value = frames of all ranks / max-over-ranks time.
+
+--impl reference runs the reference's own traversal + intersect/shade code, compiled from the
+reference sources into oracle/_ref (else the oracle port), on the host cores over a bounded
+crop of the same frame.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, MSAA, IPD = 1080, 1200, 8, 0.064
+CROP_ROWS = (540, 660)  # bounded CPU sample: a 120-row band across the middle of the left eye
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="hvvr_b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="small case for ncu: one eye of the stereo workload, 3 frames, 32M-entry index pool")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per intersect launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "intersect_shade_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def stereo_setup(hv, scenes, sc, target_cuda, torch):
+    rc = hv.Raycaster(tri_index_capacity=128 << 20)
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    smp = scenes.barrel_samples(W, H)
+    eyes = scenes.stereo_eyes(IPD)
+    cams, images = [], []
+    for xf in eyes:
+        cam = rc.create_camera(scenes.viewport_for(W, H))
+        if target_cuda:
+            img = torch.zeros((H, W), dtype=torch.int32, device="cuda")
+            cam.set_render_target(W, H, device_ptr=img.data_ptr())
+            images.append(img)
+        else:
+            cam.set_render_target(W, H)
+        cam.set_samples(smp)
+        cam.set_camera_to_world(xf)
+        cam.set_msaa(MSAA)
+        cams.append(cam)
+    return rc, cams, images, smp, eyes
+
+
+def algorithmic_bytes(hv, scenes, sc, torch):
+    """Compulsory HBM bytes of one intersect+shade launch (per eye, left eye), from one capture frame:
+    per sample 48 B beam + 4 B RGBA8 written; per list entry 4 B index + 48 B triangle; per unique
+    (sample, triangle) hit 16 B shade record + 3 x 32 B vertices + 64 B material + 48 B triangle."""
+    rc = hv.Raycaster()
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    cam = rc.create_camera(scenes.viewport_for(W, H))
+    cam.set_render_target(W, H)
+    cam.set_samples(scenes.barrel_samples(W, H))
+    cam.set_camera_to_world(scenes.stereo_eyes(IPD)[0])
+    cam.set_msaa(MSAA)
+    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+    rc.render()
+    blocks, tiles, padded, msaa = cam.layout()
+    list_total = cam.list_total()
+    n, tri, mask = cam.gbuffer()
+    valid_pairs = int(((tri != 0xFFFFFFFF) & (mask != 0)).sum())
+    rc.close()
+    b = padded * (48 + 4) + list_total * (4 + 48) + valid_pairs * (16 + 96 + 64 + 48)
+    return b, {"padded_samples": padded, "list_entries": list_total, "unique_hits": valid_pairs}
+
+
+def run_reference_arm(args, rank):
+    """The reference's own CPU path (oracle/_ref) on the host cores, bounded crop of the left eye."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    if rank != 0:
+        return
+    kind = "reference" if pyoracle.Reference.available() else "port"
+    impl = pyoracle.Reference() if kind == "reference" else pyoracle.Oracle()
+    sc = scenes.scene_c2()
+    hv.generate_topology(sc)
+    smp = scenes.barrel_samples(W, H)
+    crop = smp[(smp["pixel"][:, 1] >= CROP_ROWS[0]) & (smp["pixel"][:, 1] < CROP_ROWS[1])]
+    xf = scenes.stereo_eyes(IPD)[0]
+    cores = os.cpu_count() or 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        impl.render(sc, crop, xf, scenes.viewport_for(W, H), W, H, MSAA, fp_mode=hv.HVVR_FP_STRICT,
+                    threads=cores, want=("colors",))
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    ms = 1e3 * statistics.median(times)
+    value = len(crop) / (ms * 1e-3) / 1e9
+    line = {"metric": "vis+shade Gsamples/s", "impl": "reference", "value": value, "unit": "Gsamples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene and barrel-distorted sample set)",
+            "config": {"workload": "stereo 2x1080x1200 8xMSAA barrel-distorted, 995k-tri scene; crop rows %d-%d of the "
+                                   "left eye (%d samples) per step" % (CROP_ROWS[0], CROP_ROWS[1], len(crop)),
+                       "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": "Gsamples/s", "cores": cores, "kind": kind,
+                             "sample": "%d samples (rows %d-%d of one eye), full traversal+intersect+shade" %
+                                       (len(crop), CROP_ROWS[0], CROP_ROWS[1])},
+            "e2e": {"value": value, "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(sc):
+    """Oracle (scalar restatement) timed on this host over the bounded crop, all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    kind = "reference" if pyoracle.Reference.available() else "port"
+    impl = pyoracle.Reference() if kind == "reference" else pyoracle.Oracle()
+    smp = scenes.barrel_samples(W, H)
+    crop = smp[(smp["pixel"][:, 1] >= CROP_ROWS[0]) & (smp["pixel"][:, 1] < CROP_ROWS[1])]
+    cores = os.cpu_count() or 1
+    xf = scenes.stereo_eyes(IPD)[0]
+    t0 = time.perf_counter()
+    impl.render(sc, crop, xf, scenes.viewport_for(W, H), W, H, MSAA, fp_mode=hv.HVVR_FP_STRICT, threads=cores,
+                want=("colors",))
+    dt = time.perf_counter() - t0
+    return {"value": len(crop) / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": kind,
+            "sample": "%d samples (rows %d-%d of the left eye), traversal+intersect+shade, %.1f s" %
+                      (len(crop), CROP_ROWS[0], CROP_ROWS[1], dt)}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    if args.profile:
+        run_profile_case()
+        return
+    import numpy as np
+    import torch
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    sc = scenes.scene_c2()
+    hv.generate_topology(sc)
+    alg_bytes, alg_counts = algorithmic_bytes(hv, scenes, sc, torch)
+
+    rc, cams, images, smp, eyes = stereo_setup(hv, scenes, sc, True, torch)
+    samples_per_frame = 2 * len(smp)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = ctypes_stream(stream)
+    for _ in range(args.warmup):
+        rc.render(stream=sp)
+    torch.cuda.synchronize()
+    rc.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    isect_ms, stage_ms = [], []
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        flush.fill_(i & 0xff)
+        starts[i].record(stream)
+        rc.render(stream=sp)
+        ends[i].record(stream)
+        torch.cuda.synchronize()
+        for c in cams:
+            tm = c.timings()
+            isect_ms.append(float(tm[3]))
+            stage_ms.append([float(x) for x in tm])
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    rc.synchronize()
+    frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(frame_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * samples_per_frame * args.steps / (total_ms * 1e-3) / 1e9
+
+    # end to end through the C ABI: CPU_MEMORY targets, images copied to host every frame
+    rc.close()
+    rc2, cams2, _, _, _ = stereo_setup(hv, scenes, sc, False, torch)
+    for _ in range(max(2, args.warmup)):
+        for c, xf in zip(cams2, eyes):
+            c.set_camera_to_world(xf)
+        rc2.render()
+    e2e_steps = max(3, args.steps // 2)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for c, xf in zip(cams2, eyes):
+            c.set_camera_to_world(xf)
+        rc2.render()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * samples_per_frame * e2e_steps / e2e_s / 1e9
+    rc2.close()
+
+    peak, peak_kind = load_peaks()
+    isect_avg = statistics.mean(isect_ms)
+    achieved = alg_bytes / (isect_avg * 1e-3) / 1e9
+    tr = committed_traffic()
+    traffic = tr.get("dram_bytes_per_launch_full") if tr else None
+    line = {
+        "metric": "vis+shade Gsamples/s", "value": value, "unit": "Gsamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "p50_frame_ms": statistics.median(frame_ms), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural 995k-triangle scene, barrel-distorted sample set)",
+        "config": {"workload": "stereo 2x1080x1200 8xMSAA barrel-distorted samples, 995,072-triangle scene, "
+                               "one plain frame per step", "samples_per_frame": samples_per_frame,
+                   "parallelism": "replicas x%d" % world, "l2": "flushed between frames (256 MiB write, untimed)"},
+        "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 2 * 32,
+                "d2h_bytes_per_step": 2 * W * H * 4},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "intersectShadeKernel<8,FMA> (one eye)",
+                     "algorithmic_bytes": alg_bytes, "avg_launch_ms": isect_avg, "counts": alg_counts,
+                     "peak_source": peak_kind},
+        "stage_ms_per_eye": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
+                             [(1, "block_cull"), (2, "tile_cull"), (3, "intersect_shade"), (4, "remap"), (5, "total")]},
+        "gpu_launches": args.steps * 2 * 4,
+        "clocks": ck,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(sc)
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_profile_case():
+    """One eye of the benchmark frame, 3 frames, for ncu captures (a few GB on the device)."""
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    sc = scenes.scene_c2()
+    hv.generate_topology(sc)
+    with hv.Raycaster(tri_index_capacity=32 << 20) as rc:
+        rc.create_model(sc)
+        for l in sc.lights:
+            rc.create_light(l)
+        cam = rc.create_camera(scenes.viewport_for(W, H))
+        cam.set_render_target(W, H)
+        cam.set_samples(scenes.barrel_samples(W, H))
+        cam.set_camera_to_world(scenes.stereo_eyes(IPD)[0])
+        cam.set_msaa(MSAA)
+        for _ in range(3):
+            rc.render()
+        rc.synchronize()
+        print(json.dumps({"profile_case": "one eye 1080x1200 8xMSAA, 995k tris", "stage_ms": [float(x) for x in cam.timings()],
+                          "list_entries": cam.list_total()}))
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+if __name__ == "__main__":
+    main()

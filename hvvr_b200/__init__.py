@@ -1,0 +1,349 @@
+"""hvvr_b200 - B200-native primary-visibility-and-shading path with HVVR's interface.
+
+Python mirror of the reference's Raycaster / Camera / Model / Light API over the C ABI in
+include/hvvr_c.h (libhvvr_b200.so, built in-tree by ``make -C hvvr_b200/csrc``). There is
+no CPU fallback: every entry point runs the CUDA library, and importing this package when
+the library has not been built raises immediately.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import (HVVR_CAPTURE_HITS, HVVR_FP_FMA, HVVR_FP_STRICT, HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA,  # noqa: F401
+                   HVVR_OK)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libhvvr_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("hvvr_b200: %s is not built; run `make -C hvvr_b200/csrc` (or __graft_entry__.build())" % LIB_PATH)
+
+_lib = C.CDLL(LIB_PATH)
+_vp = C.c_void_p
+_u32 = C.c_uint32
+_p = C.POINTER
+
+
+def _sig(name, *args):
+    f = getattr(_lib, name)
+    f.argtypes = list(args)
+    f.restype = C.c_int
+    return f
+
+
+_lib.hvvr_last_error.restype = C.c_char_p
+_lib.hvvr_last_error.argtypes = []
+_lib.hvvr_spec_default.argtypes = [_p(_abi.Spec)]
+_lib.hvvr_spec_default.restype = None
+_sig("hvvr_version")
+_sig("hvvr_raycaster_create", _p(_abi.Spec), _p(_vp))
+_sig("hvvr_raycaster_destroy", _vp)
+_sig("hvvr_raycaster_set_scene_dirty", _vp)
+_sig("hvvr_raycaster_render", _vp, C.c_double, _vp)
+_sig("hvvr_raycaster_synchronize", _vp)
+_sig("hvvr_model_create", _vp, _p(_abi.MeshData), _p(_vp))
+_sig("hvvr_model_destroy", _vp, _vp)
+_sig("hvvr_model_set_transform", _vp, _p(_abi.Transform))
+_sig("hvvr_model_update_vertices", _vp, _vp, _u32)
+_sig("hvvr_light_create", _vp, _p(_abi.LightUnion), _p(_vp))
+_sig("hvvr_light_destroy", _vp, _vp)
+_sig("hvvr_camera_create", _vp, _p(_abi.FloatRect), C.c_float, _p(_vp))
+_sig("hvvr_camera_destroy", _vp, _vp)
+_sig("hvvr_camera_set_enabled", _vp, C.c_int)
+_sig("hvvr_camera_set_viewport", _vp, _p(_abi.FloatRect))
+_sig("hvvr_camera_set_lens", _vp, _p(_abi.ThinLens))
+_sig("hvvr_camera_set_aperture", _vp, C.c_float)
+_sig("hvvr_camera_set_focal_depth", _vp, C.c_float)
+_sig("hvvr_camera_set_eye_dir", _vp, _p(_abi.Vec3))
+_sig("hvvr_camera_set_spherical_warp", _vp, C.c_float, C.c_float)
+_sig("hvvr_camera_set_render_target", _vp, _p(_abi.ImageDesc))
+_sig("hvvr_camera_set_samples", _vp, _vp, _u32, _u32)
+_sig("hvvr_camera_set_camera_to_world", _vp, _p(_abi.Transform))
+_sig("hvvr_camera_set_msaa", _vp, _u32)
+_sig("hvvr_camera_get_sample_count", _vp, _p(_u32))
+_sig("hvvr_camera_set_capture", _vp, _u32)
+_sig("hvvr_camera_get_layout", _vp, _p(_u32), _p(_u32), _p(_u32), _p(_u32))
+_sig("hvvr_camera_read_tile_lists", _vp, _vp, _vp, C.c_uint64, _p(C.c_uint64))
+_sig("hvvr_camera_read_block_stacks", _vp, _vp, _vp)
+_sig("hvvr_camera_read_hits", _vp, _vp, _vp)
+_sig("hvvr_camera_read_gbuffer", _vp, _vp, _vp, _vp)
+_sig("hvvr_camera_read_sample_colors", _vp, _vp)
+_sig("hvvr_camera_read_sample_remap", _vp, _vp, C.c_uint64)
+_sig("hvvr_camera_read_beams", _vp, _vp)
+_sig("hvvr_camera_read_timings", _vp, _vp)
+_sig("hvvr_camera_read_list_total", _vp, _p(C.c_uint64))
+_sig("hvvr_scene_get_counts", _vp, _p(_u32), _p(_u32), _p(_u32))
+_sig("hvvr_scene_read_nodes", _vp, _vp)
+_sig("hvvr_scene_read_triangles", _vp, _vp)
+_sig("hvvr_generate_topology", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32))
+_sig("hvvr_grid_samples", _u32, _u32, _vp)
+
+EXPORTED = [
+    "hvvr_last_error", "hvvr_version", "hvvr_spec_default", "hvvr_raycaster_create", "hvvr_raycaster_destroy",
+    "hvvr_raycaster_set_scene_dirty", "hvvr_raycaster_render", "hvvr_raycaster_synchronize", "hvvr_model_create",
+    "hvvr_model_destroy", "hvvr_model_set_transform", "hvvr_model_update_vertices", "hvvr_light_create",
+    "hvvr_light_destroy", "hvvr_camera_create", "hvvr_camera_destroy", "hvvr_camera_set_enabled",
+    "hvvr_camera_set_viewport", "hvvr_camera_set_lens", "hvvr_camera_set_aperture", "hvvr_camera_set_focal_depth",
+    "hvvr_camera_set_eye_dir", "hvvr_camera_set_spherical_warp", "hvvr_camera_set_render_target",
+    "hvvr_camera_set_samples", "hvvr_camera_set_camera_to_world", "hvvr_camera_set_msaa",
+    "hvvr_camera_get_sample_count", "hvvr_camera_set_capture", "hvvr_camera_get_layout",
+    "hvvr_camera_read_tile_lists", "hvvr_camera_read_block_stacks", "hvvr_camera_read_hits",
+    "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
+    "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
+    "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
+]
+
+
+class HvvrError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("hvvr error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _check(rc):
+    if rc != HVVR_OK:
+        raise HvvrError(rc, _lib.hvvr_last_error().decode())
+
+
+def lib():
+    """The loaded ctypes library (for callers that bind the C ABI directly)."""
+    return _lib
+
+
+def generate_topology(scene):
+    """GenerateTopology: builds scene.nodes and reorders scene.verts / scene.tri_shade in place."""
+    nodes = np.zeros(len(scene.tri_shade) + 4, dtype=_abi.TOPO_DTYPE)
+    cnt = _u32(0)
+    _check(_lib.hvvr_generate_topology(scene.verts.ctypes.data, len(scene.verts), scene.tri_shade.ctypes.data,
+                                       len(scene.tri_shade), nodes.ctypes.data, len(nodes), C.byref(cnt)))
+    scene.nodes = nodes[: cnt.value].copy()
+    return scene
+
+
+def grid_samples(width, height):
+    s = np.zeros(width * height, dtype=_abi.SAMPLE_DTYPE)
+    _check(_lib.hvvr_grid_samples(width, height, s.ctypes.data))
+    return s
+
+
+class Model:
+    def __init__(self, rc, handle, scene):
+        self._rc, self.handle, self.scene = rc, handle, scene
+
+    def set_transform(self, xf):
+        _check(_lib.hvvr_model_set_transform(self.handle, C.byref(xf)))
+
+    def update_vertices(self, verts):
+        verts = np.ascontiguousarray(verts, dtype=_abi.VERTEX_DTYPE)
+        _check(_lib.hvvr_model_update_vertices(self.handle, verts.ctypes.data, len(verts)))
+
+
+class Camera:
+    def __init__(self, rc, handle):
+        self._rc, self.handle = rc, handle
+        self._target = None
+        self.width = self.height = 0
+
+    def set_render_target(self, width, height, device_ptr=None, stride=0):
+        """CPU_MEMORY target (a numpy image owned by the camera) or CUDA_MEMORY (device_ptr)."""
+        d = _abi.ImageDesc()
+        d.pixel_format = 0
+        d.width, d.height, d.stride = width, height, stride
+        if device_ptr is None:
+            self._target = np.zeros((height, stride or width), dtype=np.uint32)
+            d.memory_type = HVVR_MEMORY_CPU
+            d.data = self._target.ctypes.data
+        else:
+            self._target = None
+            d.memory_type = HVVR_MEMORY_CUDA
+            d.data = device_ptr
+        self.width, self.height = width, height
+        _check(_lib.hvvr_camera_set_render_target(self.handle, C.byref(d)))
+
+    @property
+    def image(self):
+        return self._target
+
+    def set_samples(self, samples, split=1):
+        samples = np.ascontiguousarray(samples, dtype=_abi.SAMPLE_DTYPE)
+        self._samples = samples
+        _check(_lib.hvvr_camera_set_samples(self.handle, samples.ctypes.data, len(samples), split))
+
+    def set_camera_to_world(self, xf):
+        _check(_lib.hvvr_camera_set_camera_to_world(self.handle, C.byref(xf)))
+
+    def set_viewport(self, vp):
+        _check(_lib.hvvr_camera_set_viewport(self.handle, C.byref(vp)))
+
+    def set_msaa(self, rate):
+        _check(_lib.hvvr_camera_set_msaa(self.handle, rate))
+
+    def set_enabled(self, enabled):
+        _check(_lib.hvvr_camera_set_enabled(self.handle, 1 if enabled else 0))
+
+    def set_capture(self, flags):
+        _check(_lib.hvvr_camera_set_capture(self.handle, flags))
+
+    def set_lens(self, radius, focal_distance):
+        _check(_lib.hvvr_camera_set_lens(self.handle, C.byref(_abi.ThinLens(radius, focal_distance))))
+
+    def sample_count(self):
+        n = _u32(0)
+        _check(_lib.hvvr_camera_get_sample_count(self.handle, C.byref(n)))
+        return n.value
+
+    def layout(self):
+        b, t, p, m = _u32(0), _u32(0), _u32(0), _u32(0)
+        _check(_lib.hvvr_camera_get_layout(self.handle, C.byref(b), C.byref(t), C.byref(p), C.byref(m)))
+        return b.value, t.value, p.value, m.value
+
+    def tile_lists(self):
+        blocks, tiles, padded, msaa = self.layout()
+        counts = np.zeros(tiles, dtype=np.uint32)
+        total = C.c_uint64(0)
+        _check(_lib.hvvr_camera_read_tile_lists(self.handle, counts.ctypes.data, None, 0, C.byref(total)))
+        idx = np.zeros(max(total.value, 1), dtype=np.uint32)
+        _check(_lib.hvvr_camera_read_tile_lists(self.handle, counts.ctypes.data, idx.ctypes.data, len(idx),
+                                                C.byref(total)))
+        return counts, idx[: total.value]
+
+    def block_stacks(self):
+        blocks, tiles, padded, msaa = self.layout()
+        sizes = np.zeros(blocks, dtype=np.uint32)
+        entries = np.zeros((blocks, 64, 3), dtype=np.uint32)
+        _check(_lib.hvvr_camera_read_block_stacks(self.handle, sizes.ctypes.data, entries.ctypes.data))
+        return sizes, entries
+
+    def hits(self):
+        blocks, tiles, padded, msaa = self.layout()
+        ids = np.zeros((padded, msaa), dtype=np.uint32)
+        depth = np.zeros((padded, msaa), dtype=np.float32)
+        _check(_lib.hvvr_camera_read_hits(self.handle, ids.ctypes.data, depth.ctypes.data))
+        return ids, depth
+
+    def gbuffer(self):
+        blocks, tiles, padded, msaa = self.layout()
+        n = np.zeros(padded, dtype=np.uint32)
+        tri = np.zeros((padded, msaa), dtype=np.uint32)
+        mask = np.zeros((padded, msaa), dtype=np.uint32)
+        _check(_lib.hvvr_camera_read_gbuffer(self.handle, n.ctypes.data, tri.ctypes.data, mask.ctypes.data))
+        return n, tri, mask
+
+    def sample_colors(self):
+        blocks, tiles, padded, msaa = self.layout()
+        c = np.zeros(padded, dtype=np.uint32)
+        _check(_lib.hvvr_camera_read_sample_colors(self.handle, c.ctypes.data))
+        return c
+
+    def beams(self):
+        blocks, tiles, padded, msaa = self.layout()
+        b = np.zeros((padded, 9), dtype=np.float32)
+        _check(_lib.hvvr_camera_read_beams(self.handle, b.ctypes.data))
+        return b
+
+    def sample_remap(self, split=1):
+        r = np.zeros(self.width * self.height * split, dtype=np.int32)
+        _check(_lib.hvvr_camera_read_sample_remap(self.handle, r.ctypes.data, len(r)))
+        return r
+
+    def timings(self):
+        t = np.zeros(6, dtype=np.float32)
+        _check(_lib.hvvr_camera_read_timings(self.handle, t.ctypes.data))
+        return t
+
+    def list_total(self):
+        total = C.c_uint64(0)
+        _check(_lib.hvvr_camera_read_list_total(self.handle, C.byref(total)))
+        return total.value
+
+
+class Raycaster:
+    """Raycaster(const RayCasterSpecification&) (libraries/hvvr/raycaster/raycaster.h:44)."""
+
+    def __init__(self, fp_mode=HVVR_FP_FMA, tri_index_capacity=0, device=0):
+        spec = _abi.Spec()
+        _lib.hvvr_spec_default(C.byref(spec))
+        spec.fp_mode = fp_mode
+        spec.tri_index_capacity = tri_index_capacity
+        spec.device = device
+        h = _vp()
+        _check(_lib.hvvr_raycaster_create(C.byref(spec), C.byref(h)))
+        self.handle = h
+        self.cameras, self.models, self.lights = [], [], []
+
+    def close(self):
+        if self.handle:
+            _check(_lib.hvvr_raycaster_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def create_model(self, scene):
+        md = _abi.MeshData(_abi.ptr(scene.verts), len(scene.verts), _abi.ptr(scene.tri_shade), len(scene.tri_shade),
+                           _abi.ptr(scene.nodes) if scene.nodes is not None else None,
+                           len(scene.nodes) if scene.nodes is not None else 0,
+                           _abi.ptr(scene.materials), len(scene.materials))
+        h = _vp()
+        _check(_lib.hvvr_model_create(self.handle, C.byref(md), C.byref(h)))
+        m = Model(self, h, scene)
+        self.models.append(m)
+        return m
+
+    def create_light(self, light):
+        h = _vp()
+        _check(_lib.hvvr_light_create(self.handle, C.byref(light), C.byref(h)))
+        self.lights.append(h)
+        return h
+
+    def create_camera(self, viewport, aperture=0.0):
+        h = _vp()
+        _check(_lib.hvvr_camera_create(self.handle, C.byref(viewport), C.c_float(aperture), C.byref(h)))
+        c = Camera(self, h)
+        self.cameras.append(c)
+        return c
+
+    def destroy_camera(self, cam):
+        _check(_lib.hvvr_camera_destroy(self.handle, cam.handle))
+        self.cameras.remove(cam)
+
+    def destroy_model(self, model):
+        _check(_lib.hvvr_model_destroy(self.handle, model.handle))
+        self.models.remove(model)
+
+    def set_scene_dirty(self):
+        _check(_lib.hvvr_raycaster_set_scene_dirty(self.handle))
+
+    def render(self, elapsed=0.0, stream=None):
+        _check(_lib.hvvr_raycaster_render(self.handle, C.c_double(elapsed), stream))
+
+    def synchronize(self):
+        _check(_lib.hvvr_raycaster_synchronize(self.handle))
+
+    def scene_counts(self):
+        n, t, v = _u32(0), _u32(0), _u32(0)
+        _check(_lib.hvvr_scene_get_counts(self.handle, C.byref(n), C.byref(t), C.byref(v)))
+        return n.value, t.value, v.value
+
+    def scene_nodes(self):
+        n, t, v = self.scene_counts()
+        a = np.zeros(n, dtype=_abi.NODE_DTYPE)
+        _check(_lib.hvvr_scene_read_nodes(self.handle, a.ctypes.data))
+        return a
+
+    def scene_triangles(self):
+        n, t, v = self.scene_counts()
+        a = np.zeros((t, 9), dtype=np.float32)
+        _check(_lib.hvvr_scene_read_triangles(self.handle, a.ctypes.data))
+        return a

@@ -1,0 +1,42 @@
+// host_setup.h - host-side setup shared by the driver: camera matrices, the sample
+// hierarchy and MSAA offsets. Computed once per sample-set change on the CPU, exactly as
+// the reference does, with no floating-point contraction (built with -ffp-contract=off)
+// and with MXCSR FTZ|DAZ set like the reference's worker threads.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/hvvr_c.h"
+#include "hvvr_internal.h"
+
+namespace hvb {
+
+// scoped MXCSR FTZ|DAZ (libraries/hvvr/raycaster/raycaster.cpp:21-27)
+struct FtzDazScope {
+    unsigned saved;
+    FtzDazScope();
+    ~FtzDazScope();
+};
+
+// matrix4x4(const transform&) (libraries/hvvr/shared/vector_math.h:1021-1037, 1158-1161)
+Mat4 transformToMatrix(const hvvr_transform& t);
+
+// getSubsampleUnitOffset<N> with JITTER_SAMPLES=0 (libraries/hvvr/raycaster/gpu_samples.h:35-61)
+void msaaOffsets(uint32_t n, float* out2n);
+
+struct SampleSetup {
+    uint32_t blocks = 0, tiles = 0, padded = 0, valid = 0;
+    std::vector<Rays4> tileRays, blockRays; // camera space
+    std::vector<float> beams;               // padded * 12 (centerRay, du, dv; 3 x float4, last lane 0)
+    std::vector<int32_t> remap;             // width*height*split
+};
+
+// SampleData::SampleData (libraries/hvvr/raycaster/camera.cpp:21-64) for the perspective
+// and spherical-section mappings (libraries/hvvr/raycaster/sample_hierarchy.cpp:27-152)
+void buildSampleSetup(const hvvr_sample* samples, uint32_t count, uint32_t split, const hvvr_float_rect& viewport,
+                      const hvvr_thin_lens& lens, float fovXDeg, float fovYDeg, uint32_t width, uint32_t height,
+                      SampleSetup& out);
+
+} // namespace hvb

@@ -1,0 +1,990 @@
+// raycaster.cpp - the C ABI (include/hvvr_c.h) and the host frame driver.
+//
+// Object model and frame order follow the reference's Raycaster (libraries/hvvr/raycaster/
+// raycaster.h, render.cpp:204-451, scene_update.cpp:22-174): models, lights and cameras are
+// owned by the raycaster; render() rebuilds and refits the scene when it is dirty, then per
+// enabled camera runs block cull -> tile cull -> intersect/shade/resolve -> remap. Unlike
+// the reference, traversal runs on the GPU, the refit BVH never returns to the host, and
+// the per-tile triangle lists never cross PCIe.
+#include <cuda_runtime.h>
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hvvr_c.h"
+#include "host_setup.h"
+#include "hvvr_internal.h"
+
+using namespace hvb;
+
+namespace {
+
+thread_local std::string gLastError;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    gLastError = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? HVVR_ERR_OOM : HVVR_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #expr, cudaGetErrorString(e_), __FILE__, __LINE__);                               \
+    } while (0)
+
+#define TRY(expr)                \
+    do {                         \
+        int r_ = (expr);         \
+        if (r_ != HVVR_OK) return r_; \
+    } while (0)
+
+// owning device allocation
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count) {
+        if (count == n && p) return HVVR_OK;
+        release();
+        if (count == 0) return HVVR_OK;
+        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(HVVR_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        n = count;
+        return HVVR_OK;
+    }
+    int upload(const void* src, size_t count, cudaStream_t st) {
+        TRY(alloc(count));
+        if (count) CUDA_TRY(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
+        return HVVR_OK;
+    }
+};
+
+} // namespace
+
+struct hvvr_model {
+    hvvr_raycaster* rc = nullptr;
+    std::vector<hvvr_shading_vertex> verts;
+    std::vector<hvvr_tri_shade> triShade;
+    std::vector<hvvr_topology_node> nodes;
+    std::vector<hvvr_material> materials;
+    hvvr_transform xf{};
+};
+
+struct hvvr_light {
+    hvvr_raycaster* rc = nullptr;
+    hvvr_light_union light{};
+};
+
+struct hvvr_camera {
+    hvvr_raycaster* rc = nullptr;
+    bool enabled = true;
+    hvvr_float_rect viewport{};
+    hvvr_thin_lens lens{0.0f, 1.0f};
+    hvvr_vec3 eyeDir{0.0f, 0.0f, -1.0f};
+    float fovX = 0.0f, fovY = 0.0f;
+    hvvr_image_desc target{};
+    std::vector<hvvr_sample> samples;
+    uint32_t split = 1;
+    hvvr_transform xf{};
+    uint32_t msaa = 16;
+    uint32_t capture = 0;
+    bool setupDirty = true;
+    bool rendered = false;
+    CameraDev dev;
+    SampleSetup setup;
+    // device storage behind dev
+    DevBuf<Rays4> tileRays, blockRays;
+    DevBuf<float4> beams;
+    DevBuf<int32_t> remap;
+    DevBuf<StackEntry> blockStacks;
+    DevBuf<uint32_t> blockSizes;
+    DevBuf<TileList> tileLists;
+    DevBuf<uint32_t> pool, chunkNext, counters, colors, hitIds, image;
+    DevBuf<float> depth;
+    uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
+    void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
+    cudaEvent_t ev[6] = {};
+    float lastMs[6] = {};
+};
+
+struct hvvr_raycaster {
+    hvvr_spec spec{};
+    cudaStream_t stream = nullptr;
+    std::vector<std::unique_ptr<hvvr_model>> models;
+    std::vector<std::unique_ptr<hvvr_light>> lights;
+    std::vector<std::unique_ptr<hvvr_camera>> cameras;
+    bool sceneDirty = true;
+    bool refitDirty = true;
+    bool msaaUploaded[33] = {};
+    SceneDev scene;
+    DevBuf<Node> nodes;
+    DevBuf<float4> tris, vertsIn, verts, materials;
+    DevBuf<uint4> triShade;
+    DevBuf<uint32_t> vertModel, parentSlot, internalCount, arrivals, refitStarts;
+    DevBuf<Mat4> modelToWorld;
+    std::vector<Node> hostNodes;
+    uint32_t refitStatus = 0;
+};
+
+namespace {
+
+const char* kEmpty = "";
+
+bool validRate(uint32_t r) { return r == 1 || r == 2 || r == 4 || r == 8 || r == 16 || r == 32; }
+
+// Raycaster::buildScene (libraries/hvvr/raycaster/scene_update.cpp:22-143), plus validation
+// that every leaf range lies inside the model and every child offset inside its node array.
+int buildScene(hvvr_raycaster* rc, std::vector<Node>& nodes, std::vector<uint4>& triShade,
+               std::vector<float4>& verts, std::vector<uint32_t>& vertModel, std::vector<float4>& materials) {
+    const uint32_t modelCount = uint32_t(rc->models.size());
+    nodes.clear();
+    triShade.clear();
+    verts.clear();
+    vertModel.clear();
+    materials.clear();
+    if (modelCount == 0) {
+        nodes.assign(1, Node{});
+        nodes[0].leafMask = 0xf;
+        return HVVR_OK;
+    }
+    const uint32_t rootNodeCount = (modelCount + 1) / 3;
+    size_t nc = rootNodeCount;
+    for (auto& m : rc->models) nc += m->nodes.size();
+    nodes.assign(nc, Node{});
+    std::vector<uint32_t> viewOffsets(modelCount);
+    uint32_t vOff = 0, tOff = 0, mOff = 0, nOff = rootNodeCount;
+    for (uint32_t mi = 0; mi < modelCount; mi++) {
+        const hvvr_model& m = *rc->models[mi];
+        const uint32_t tc = uint32_t(m.triShade.size()), vc = uint32_t(m.verts.size());
+        for (const hvvr_material& mat : m.materials) {
+            const float4* q = reinterpret_cast<const float4*>(&mat);
+            materials.insert(materials.end(), q, q + 4);
+        }
+        for (const hvvr_tri_shade& t : m.triShade) {
+            if (t.indices[0] >= vc || t.indices[1] >= vc || t.indices[2] >= vc)
+                return fail(HVVR_ERR_INVALID, "model %u: vertex index out of range", mi);
+            if (t.material >= m.materials.size()) return fail(HVVR_ERR_INVALID, "model %u: material out of range", mi);
+            triShade.push_back(make_uint4(t.indices[0] + vOff, t.indices[1] + vOff, t.indices[2] + vOff, t.material + mOff));
+        }
+        for (const hvvr_shading_vertex& v : m.verts) {
+            const float4* q = reinterpret_cast<const float4*>(&v);
+            verts.push_back(q[0]);
+            verts.push_back(q[1]);
+            vertModel.push_back(mi);
+        }
+        viewOffsets[mi] = nOff;
+        std::vector<uint32_t> cover(tc, 0);
+        for (size_t i = 0; i < m.nodes.size(); i++) {
+            const hvvr_topology_node& tn = m.nodes[i];
+            Node& n = nodes[nOff + i];
+            n.leafMask = tn.leaf_mask & 0xfu;
+            n.tri[0] = tOff + tn.data[0];
+            for (int k = 0; k < 4; k++) {
+                if (tn.leaf_mask & (1u << k)) {
+                    n.tri[1 + k] = tOff + tn.data[1 + k];
+                    const uint32_t a = tn.data[k], b = tn.data[1 + k];
+                    if (a > b || b > tc) return fail(HVVR_ERR_INVALID, "model %u node %zu: bad leaf range", mi, i);
+                    for (uint32_t t = a; t < b; t++) cover[t]++;
+                } else {
+                    n.tri[1 + k] = tn.data[1 + k];
+                    if (tn.data[1 + k] == 0 || i + tn.data[1 + k] >= m.nodes.size())
+                        return fail(HVVR_ERR_INVALID, "model %u node %zu: bad child offset", mi, i);
+                }
+            }
+        }
+        for (uint32_t t = 0; t < tc; t++)
+            if (cover[t] != 1)
+                return fail(HVVR_ERR_INVALID, "model %u: triangle %u covered by %u leaves (topology must partition)",
+                            mi, t, cover[t]);
+        vOff += vc;
+        tOff += tc;
+        mOff += uint32_t(m.materials.size());
+        nOff += uint32_t(m.nodes.size());
+    }
+    if (rootNodeCount > 0) {
+        std::vector<int64_t> children(rootNodeCount * 4);
+        size_t w = 0;
+        for (size_t i = children.size() - modelCount - (rootNodeCount - 1); i != 0; --i) children[w++] = -1;
+        for (uint32_t i = 1; i < rootNodeCount; i++) children[w++] = i;
+        for (uint32_t mi = 0; mi < modelCount; mi++) children[w++] = viewOffsets[mi];
+        for (uint32_t i = 0; i < rootNodeCount; i++) {
+            Node& n = nodes[i];
+            n.tri[0] = 0;
+            n.leafMask = 0;
+            for (int k = 0; k < 4; k++) {
+                const int64_t c = children[4 * i + k];
+                if (c < 0) {
+                    n.tri[1 + k] = 0;
+                    n.leafMask |= 1u << k;
+                    continue;
+                }
+                n.tri[1 + k] = uint32_t(c - i);
+            }
+        }
+    }
+    return HVVR_OK;
+}
+
+int uploadScene(hvvr_raycaster* rc, cudaStream_t st) {
+    std::vector<Node> nodes;
+    std::vector<uint4> triShade;
+    std::vector<float4> verts, materials;
+    std::vector<uint32_t> vertModel;
+    TRY(buildScene(rc, nodes, triShade, verts, vertModel, materials));
+    const uint32_t nodeCount = uint32_t(nodes.size());
+    // refit order: parent slot of every internal child, internal child counts, start nodes
+    std::vector<uint32_t> parentSlot(nodeCount, 0xffffffffu), internalCount(nodeCount, 0), depth(nodeCount, 0), starts;
+    uint32_t maxDepth = 0;
+    for (uint32_t n = 0; n < nodeCount; n++) {
+        for (int k = 0; k < 4; k++) {
+            if (nodes[n].leafMask & (1u << k)) continue;
+            const uint32_t c = n + nodes[n].tri[k + 1];
+            if (c >= nodeCount || c <= n) return fail(HVVR_ERR_INVALID, "node %u: child offset out of range", n);
+            parentSlot[c] = (n << 2) | uint32_t(k);
+            internalCount[n]++;
+            depth[c] = depth[n] + 1;
+            maxDepth = std::max(maxDepth, depth[c]);
+        }
+    }
+    for (uint32_t n = 0; n < nodeCount; n++)
+        if (internalCount[n] == 0) starts.push_back(n);
+    std::vector<Mat4> xf(std::max<size_t>(rc->models.size(), 1));
+    for (size_t i = 0; i < rc->models.size(); i++) xf[i] = transformToMatrix(rc->models[i]->xf);
+
+    TRY(rc->nodes.upload(nodes.data(), nodes.size(), st));
+    TRY(rc->triShade.upload(triShade.data(), triShade.size(), st));
+    TRY(rc->vertsIn.upload(verts.data(), verts.size(), st));
+    TRY(rc->verts.alloc(verts.size()));
+    TRY(rc->vertModel.upload(vertModel.data(), vertModel.size(), st));
+    TRY(rc->materials.upload(materials.data(), materials.size(), st));
+    TRY(rc->tris.alloc(triShade.size() * 3));
+    TRY(rc->modelToWorld.upload(xf.data(), xf.size(), st));
+    TRY(rc->parentSlot.upload(parentSlot.data(), parentSlot.size(), st));
+    TRY(rc->internalCount.upload(internalCount.data(), internalCount.size(), st));
+    TRY(rc->arrivals.alloc(size_t(nodeCount) + 1));
+    TRY(rc->refitStarts.upload(starts.data(), starts.size(), st));
+    SceneDev& s = rc->scene;
+    s.nodes = rc->nodes.p;
+    s.nodeCount = nodeCount;
+    s.tris = rc->tris.p;
+    s.triShade = rc->triShade.p;
+    s.triCount = uint32_t(triShade.size());
+    s.vertsIn = rc->vertsIn.p;
+    s.verts = rc->verts.p;
+    s.vertModel = rc->vertModel.p;
+    s.vertCount = uint32_t(vertModel.size());
+    s.modelToWorld = rc->modelToWorld.p;
+    s.modelCount = uint32_t(rc->models.size());
+    s.materials = rc->materials.p;
+    s.materialCount = uint32_t(materials.size() / 4);
+    s.parentSlot = rc->parentSlot.p;
+    s.internalCount = rc->internalCount.p;
+    s.arrivals = rc->arrivals.p;
+    s.refitStarts = rc->refitStarts.p;
+    s.refitStartCount = uint32_t(starts.size());
+    s.maxDepth = maxDepth;
+    rc->hostNodes = std::move(nodes);
+    // GPUSceneState::updateLighting (libraries/hvvr/raycaster/gpu_scene_state.cu:47-81)
+    LightEnvDev& env = s.env;
+    memset(&env, 0, sizeof(env));
+    for (auto& l : rc->lights) {
+        const hvvr_light_union& u = l->light;
+        if (u.type == HVVR_LIGHT_DIRECTIONAL && env.nd < 1) {
+            const hvvr_light_directional& d = u.u.directional;
+            float* o = env.dir[env.nd++];
+            o[0] = d.direction.x; o[1] = d.direction.y; o[2] = d.direction.z;
+            o[3] = d.power.x; o[4] = d.power.y; o[5] = d.power.z;
+        } else if (u.type == HVVR_LIGHT_POINT && env.np < 4) {
+            const hvvr_light_point& p = u.u.point;
+            float* o = env.pt[env.np++];
+            o[0] = p.position.x; o[1] = p.position.y; o[2] = p.position.z; o[3] = p.falloff_end;
+            o[4] = p.color.x; o[5] = p.color.y; o[6] = p.color.z; o[7] = p.falloff_scale;
+        } else if (u.type == HVVR_LIGHT_SPOT && env.ns < 4) {
+            const hvvr_light_spot& p = u.u.spot;
+            float* o = env.spot[env.ns++];
+            o[0] = p.position.x; o[1] = p.position.y; o[2] = p.position.z; o[3] = p.falloff_end;
+            o[4] = p.direction.x; o[5] = p.direction.y; o[6] = p.direction.z; o[7] = p.falloff_scale;
+            o[8] = p.color.x; o[9] = p.color.y; o[10] = p.color.z; o[11] = p.cos_outer_angle; o[12] = p.cos_angle_scale;
+        }
+    }
+    return HVVR_OK;
+}
+
+int uploadTransforms(hvvr_raycaster* rc, cudaStream_t st) {
+    std::vector<Mat4> xf(std::max<size_t>(rc->models.size(), 1));
+    for (size_t i = 0; i < rc->models.size(); i++) xf[i] = transformToMatrix(rc->models[i]->xf);
+    return rc->modelToWorld.upload(xf.data(), xf.size(), st);
+}
+
+int setupCamera(hvvr_camera* cam, cudaStream_t st) {
+    if (cam->samples.empty()) return fail(HVVR_ERR_STATE, "camera has no samples");
+    const uint32_t w = cam->target.width, h = cam->target.height;
+    buildSampleSetup(cam->samples.data(), uint32_t(cam->samples.size()), cam->split, cam->viewport, cam->lens,
+                     cam->fovX, cam->fovY, w, h, cam->setup);
+    const SampleSetup& ss = cam->setup;
+    TRY(cam->tileRays.upload(ss.tileRays.data(), ss.tileRays.size(), st));
+    TRY(cam->blockRays.upload(ss.blockRays.data(), ss.blockRays.size(), st));
+    TRY(cam->beams.upload(ss.beams.data(), ss.beams.size() / 4, st));
+    TRY(cam->remap.upload(ss.remap.data(), ss.remap.size(), st));
+    TRY(cam->blockStacks.alloc(size_t(ss.blocks) * kBlockStack));
+    TRY(cam->blockSizes.alloc(ss.blocks));
+    TRY(cam->tileLists.alloc(ss.tiles));
+    TRY(cam->colors.alloc(ss.padded));
+    TRY(cam->counters.alloc(4));
+    if (!cam->hostCounters) CUDA_TRY(cudaMallocHost((void**)&cam->hostCounters, 4 * sizeof(uint32_t)));
+    const uint64_t capEntries = cam->rc->spec.tri_index_capacity ? cam->rc->spec.tri_index_capacity : (128ull << 20);
+    const uint64_t chunks = (capEntries + kChunk - 1) / kChunk;
+    if (chunks > 0xfffffff0ull) return fail(HVVR_ERR_INVALID, "tri_index_capacity too large");
+    if (cam->chunkNext.n != chunks) {
+        TRY(cam->pool.alloc(size_t(chunks) * kChunk));
+        TRY(cam->chunkNext.alloc(size_t(chunks)));
+    }
+    const bool cpuTarget = cam->target.memory_type == HVVR_MEMORY_CPU;
+    if (cpuTarget && w && h) TRY(cam->image.alloc(size_t(w) * h));
+    CameraDev& d = cam->dev;
+    d.blocks = ss.blocks;
+    d.tiles = ss.tiles;
+    d.padded = ss.padded;
+    d.valid = ss.valid;
+    d.tileRays = cam->tileRays.p;
+    d.blockRays = cam->blockRays.p;
+    d.beams = cam->beams.p;
+    d.remap = cam->remap.p;
+    d.width = w;
+    d.height = h;
+    d.split = cam->split;
+    d.blockStacks = cam->blockStacks.p;
+    d.blockSizes = cam->blockSizes.p;
+    d.tileLists = cam->tileLists.p;
+    d.pool = cam->pool.p;
+    d.chunkNext = cam->chunkNext.p;
+    d.poolChunks = uint32_t(chunks);
+    d.counters = cam->counters.p;
+    d.colors = cam->colors.p;
+    if (cpuTarget) {
+        d.image = cam->image.p;
+        d.imageStride = w;
+    } else {
+        d.image = static_cast<uint32_t*>(cam->target.data);
+        d.imageStride = cam->target.stride ? cam->target.stride : w;
+    }
+    if (!cam->ev[0])
+        for (auto& e : cam->ev) CUDA_TRY(cudaEventCreate(&e));
+    cam->setupDirty = false;
+    return HVVR_OK;
+}
+
+int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t st) {
+    if (cam->setupDirty) TRY(setupCamera(cam, st));
+    CameraDev& d = cam->dev;
+    d.msaa = cam->msaa;
+    if (cam->capture & HVVR_CAPTURE_HITS) {
+        TRY(cam->hitIds.alloc(size_t(d.padded) * d.msaa));
+        TRY(cam->depth.alloc(size_t(d.padded) * d.msaa));
+        d.hitIds = cam->hitIds.p;
+        d.depth = cam->depth.p;
+    }
+    if (!rc->msaaUploaded[d.msaa]) {
+        float off[64];
+        msaaOffsets(d.msaa, off);
+        CUDA_TRY(uploadMsaaTable(d.msaa, off, st));
+        rc->msaaUploaded[d.msaa] = true;
+    }
+    FrameParams f;
+    f.cameraToWorld = transformToMatrix(cam->xf);
+    f.fpStrict = rc->spec.fp_mode == HVVR_FP_STRICT ? 1u : 0u;
+    f.capture = (cam->capture & HVVR_CAPTURE_HITS) ? 1u : 0u;
+    CUDA_TRY(cudaEventRecord(cam->ev[0], st));
+    CUDA_TRY(cudaMemsetAsync(d.counters, 0, 4 * sizeof(uint32_t), st));
+    CUDA_TRY(launchBlockCull(rc->scene, d, f, st));
+    CUDA_TRY(cudaEventRecord(cam->ev[1], st));
+    CUDA_TRY(launchTileCull(rc->scene, d, f, st));
+    CUDA_TRY(cudaEventRecord(cam->ev[2], st));
+    CUDA_TRY(launchIntersectShade(rc->scene, d, f, st));
+    CUDA_TRY(cudaEventRecord(cam->ev[3], st));
+    CUDA_TRY(launchRemap(d, st));
+    CUDA_TRY(cudaEventRecord(cam->ev[4], st));
+    CUDA_TRY(cudaMemcpyAsync(cam->hostCounters, d.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    if (cam->target.memory_type == HVVR_MEMORY_CPU && cam->target.data && d.width && d.height) {
+        const uint64_t stride = cam->target.stride ? cam->target.stride : d.width;
+        CUDA_TRY(cudaMemcpy2DAsync(cam->target.data, stride * 4, d.image, size_t(d.width) * 4, size_t(d.width) * 4,
+                                   d.height, cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaEventRecord(cam->ev[5], st));
+    cam->rendered = true;
+    return HVVR_OK;
+}
+
+// CPU_MEMORY render targets are page-locked while they are bound, so the per-frame image
+// copy runs at pinned-memory bandwidth; if registration fails the copy stays pageable.
+void unregisterTarget(hvvr_camera* cam) {
+    if (cam->registered) {
+        cudaHostUnregister(cam->registered);
+        cam->registered = nullptr;
+    }
+}
+
+int checkStatus(hvvr_raycaster* rc) {
+    for (auto& c : rc->cameras) {
+        if (!c->rendered || !c->hostCounters) continue;
+        const uint32_t s = c->hostCounters[1];
+        if (s & kStatusPoolOverflow)
+            return fail(HVVR_ERR_OVERFLOW, "triangle-index pool exhausted (%u chunks); raise tri_index_capacity",
+                        c->dev.poolChunks);
+        if (s & kStatusStackOverflow) return fail(HVVR_ERR_OVERFLOW, "tile traversal stack exhausted");
+        if (s & kStatusBadLeaf) return fail(HVVR_ERR_INVALID, "BVH leaf with an empty triangle range passed the cull");
+    }
+    return HVVR_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* hvvr_last_error(void) { return gLastError.empty() ? kEmpty : gLastError.c_str(); }
+int hvvr_version(void) { return 10000; }
+
+void hvvr_spec_default(hvvr_spec* spec) {
+    if (!spec) return;
+    memset(spec, 0, sizeof(*spec));
+    spec->mode = HVVR_MODE_DEFERRED_MSAA_RESOLVE;
+    spec->foveated_degree_tracking_error = 0.5f;
+    spec->foveated_max_fov_degrees = 110.0f;
+    spec->foveated_mar_slope = 0.022f;
+    spec->foveated_foveal_mar_degrees = 1.0f / 60.0f;
+    spec->fp_mode = HVVR_FP_FMA;
+}
+
+int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out) {
+    if (!out) return fail(HVVR_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    hvvr_spec s;
+    if (spec) s = *spec;
+    else hvvr_spec_default(&s);
+    if (s.output_to_3d_api) return fail(HVVR_ERR_INVALID, "output to a 3D API is not available: no graphics stack");
+    if (s.mode != HVVR_MODE_DEFERRED_MSAA_RESOLVE)
+        return fail(HVVR_ERR_INVALID, "only the deferred MSAA resolve mode is built");
+    if (s.fp_mode != HVVR_FP_FMA && s.fp_mode != HVVR_FP_STRICT) return fail(HVVR_ERR_INVALID, "bad fp_mode");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(HVVR_ERR_CUDA, "no CUDA device available");
+    if (s.device < 0 || s.device >= count) return fail(HVVR_ERR_INVALID, "device %d out of range", s.device);
+    CUDA_TRY(cudaSetDevice(s.device));
+    auto rc = std::make_unique<hvvr_raycaster>();
+    rc->spec = s;
+    CUDA_TRY(cudaStreamCreateWithFlags(&rc->stream, cudaStreamNonBlocking));
+    *out = rc.release();
+    return HVVR_OK;
+}
+
+int hvvr_raycaster_destroy(hvvr_raycaster* rc) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    cudaStreamSynchronize(rc->stream);
+    for (auto& c : rc->cameras) {
+        unregisterTarget(c.get());
+        if (c->hostCounters) cudaFreeHost(c->hostCounters);
+        for (auto& e : c->ev)
+            if (e) cudaEventDestroy(e);
+    }
+    cudaStreamDestroy(rc->stream);
+    delete rc;
+    return HVVR_OK;
+}
+
+int hvvr_raycaster_set_scene_dirty(hvvr_raycaster* rc) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    rc->sceneDirty = true;
+    return HVVR_OK;
+}
+
+int hvvr_raycaster_render(hvvr_raycaster* rc, double elapsed_time, void* stream) {
+    (void)elapsed_time;
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    CUDA_TRY(cudaSetDevice(rc->spec.device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : rc->stream;
+    if (rc->sceneDirty) {
+        TRY(uploadScene(rc, st));
+        rc->sceneDirty = false;
+        rc->refitDirty = true;
+    }
+    if (rc->scene.nodeCount == 0) return HVVR_OK;
+    if (rc->refitDirty) {
+        CUDA_TRY(launchRefit(rc->scene, st));
+        rc->refitDirty = false;
+    }
+    bool cpuTargets = false;
+    for (auto& c : rc->cameras) {
+        if (!c->enabled || c->samples.empty()) continue;
+        TRY(renderCamera(rc, c.get(), st));
+        if (c->target.memory_type == HVVR_MEMORY_CPU) cpuTargets = true;
+    }
+    if (cpuTargets) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        TRY(checkStatus(rc));
+    }
+    return HVVR_OK;
+}
+
+int hvvr_raycaster_synchronize(hvvr_raycaster* rc) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    CUDA_TRY(cudaSetDevice(rc->spec.device));
+    CUDA_TRY(cudaStreamSynchronize(rc->stream));
+    CUDA_TRY(cudaDeviceSynchronize());
+    return checkStatus(rc);
+}
+
+int hvvr_model_create(hvvr_raycaster* rc, const hvvr_mesh_data* mesh, hvvr_model** out) {
+    if (!rc || !mesh || !out) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (mesh->tri_count && (!mesh->verts || !mesh->tri_shade)) return fail(HVVR_ERR_INVALID, "missing arrays");
+    if (mesh->tri_count >= (1u << 27)) return fail(HVVR_ERR_INVALID, "at most 2^27-1 triangles (G-buffer key width)");
+    auto m = std::make_unique<hvvr_model>();
+    m->rc = rc;
+    m->verts.assign(mesh->verts, mesh->verts + mesh->vert_count);
+    m->triShade.assign(mesh->tri_shade, mesh->tri_shade + mesh->tri_count);
+    if (mesh->materials) m->materials.assign(mesh->materials, mesh->materials + mesh->material_count);
+    if (mesh->nodes && mesh->node_count) {
+        m->nodes.assign(mesh->nodes, mesh->nodes + mesh->node_count);
+    } else {
+        std::vector<hvvr_topology_node> nodes(size_t(mesh->tri_count) + 4);
+        uint32_t count = 0;
+        TRY(hvvr_generate_topology(m->verts.data(), uint32_t(m->verts.size()), m->triShade.data(),
+                                   uint32_t(m->triShade.size()), nodes.data(), uint32_t(nodes.size()), &count));
+        nodes.resize(count);
+        m->nodes = std::move(nodes);
+    }
+    m->xf.rotation = hvvr_vec4{0.0f, 0.0f, 0.0f, 1.0f};
+    m->xf.scale = 1.0f;
+    *out = m.get();
+    rc->models.push_back(std::move(m));
+    rc->sceneDirty = true;
+    return HVVR_OK;
+}
+
+int hvvr_model_destroy(hvvr_raycaster* rc, hvvr_model* model) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    for (auto it = rc->models.begin(); it != rc->models.end(); ++it) {
+        if (it->get() == model) {
+            rc->models.erase(it);
+            rc->sceneDirty = true;
+            return HVVR_OK;
+        }
+    }
+    return fail(HVVR_ERR_NOT_FOUND, "model not owned by this raycaster");
+}
+
+int hvvr_model_set_transform(hvvr_model* model, const hvvr_transform* xf) {
+    if (!model || !xf) return fail(HVVR_ERR_INVALID, "NULL argument");
+    model->xf = *xf;
+    hvvr_raycaster* rc = model->rc;
+    if (!rc->sceneDirty) {
+        int r = uploadTransforms(rc, rc->stream);
+        if (r != HVVR_OK) return r;
+        rc->refitDirty = true;
+    }
+    return HVVR_OK;
+}
+
+int hvvr_model_update_vertices(hvvr_model* model, const hvvr_shading_vertex* verts, uint32_t count) {
+    if (!model || !verts) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (count != model->verts.size()) return fail(HVVR_ERR_INVALID, "vertex count mismatch");
+    model->verts.assign(verts, verts + count);
+    hvvr_raycaster* rc = model->rc;
+    if (rc->sceneDirty) return HVVR_OK;
+    size_t off = 0;
+    for (auto& m : rc->models) {
+        if (m.get() == model) break;
+        off += m->verts.size();
+    }
+    CUDA_TRY(cudaMemcpyAsync(rc->vertsIn.p + 2 * off, verts, size_t(count) * sizeof(hvvr_shading_vertex),
+                             cudaMemcpyHostToDevice, rc->stream));
+    rc->refitDirty = true;
+    return HVVR_OK;
+}
+
+int hvvr_light_create(hvvr_raycaster* rc, const hvvr_light_union* light, hvvr_light** out) {
+    if (!rc || !light || !out) return fail(HVVR_ERR_INVALID, "NULL argument");
+    auto l = std::make_unique<hvvr_light>();
+    l->rc = rc;
+    l->light = *light;
+    *out = l.get();
+    rc->lights.push_back(std::move(l));
+    rc->sceneDirty = true;
+    return HVVR_OK;
+}
+
+int hvvr_light_destroy(hvvr_raycaster* rc, hvvr_light* light) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    for (auto it = rc->lights.begin(); it != rc->lights.end(); ++it) {
+        if (it->get() == light) {
+            rc->lights.erase(it);
+            rc->sceneDirty = true;
+            return HVVR_OK;
+        }
+    }
+    return fail(HVVR_ERR_NOT_FOUND, "light not owned by this raycaster");
+}
+
+int hvvr_camera_create(hvvr_raycaster* rc, const hvvr_float_rect* viewport, float aperture_radius, hvvr_camera** out) {
+    if (!rc || !viewport || !out) return fail(HVVR_ERR_INVALID, "NULL argument");
+    auto c = std::make_unique<hvvr_camera>();
+    c->rc = rc;
+    c->viewport = *viewport;
+    c->lens = hvvr_thin_lens{aperture_radius, 1.0f};
+    c->xf.rotation = hvvr_vec4{0.0f, 0.0f, 0.0f, 1.0f};
+    c->xf.scale = 1.0f;
+    *out = c.get();
+    rc->cameras.push_back(std::move(c));
+    return HVVR_OK;
+}
+
+int hvvr_camera_destroy(hvvr_raycaster* rc, hvvr_camera* cam) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    for (auto it = rc->cameras.begin(); it != rc->cameras.end(); ++it) {
+        if (it->get() == cam) {
+            cudaStreamSynchronize(rc->stream);
+            unregisterTarget(cam);
+            if (cam->hostCounters) cudaFreeHost(cam->hostCounters);
+            for (auto& e : cam->ev)
+                if (e) cudaEventDestroy(e);
+            rc->cameras.erase(it);
+            return HVVR_OK;
+        }
+    }
+    return fail(HVVR_ERR_NOT_FOUND, "camera not owned by this raycaster");
+}
+
+#define CAM_CHECK(c) \
+    if (!(c)) return fail(HVVR_ERR_INVALID, "NULL camera")
+
+int hvvr_camera_set_enabled(hvvr_camera* cam, int enabled) {
+    CAM_CHECK(cam);
+    cam->enabled = enabled != 0;
+    return HVVR_OK;
+}
+int hvvr_camera_set_viewport(hvvr_camera* cam, const hvvr_float_rect* viewport) {
+    CAM_CHECK(cam);
+    if (!viewport) return fail(HVVR_ERR_INVALID, "NULL viewport");
+    cam->viewport = *viewport;
+    cam->setupDirty = true;
+    return HVVR_OK;
+}
+int hvvr_camera_set_lens(hvvr_camera* cam, const hvvr_thin_lens* lens) {
+    CAM_CHECK(cam);
+    if (!lens) return fail(HVVR_ERR_INVALID, "NULL lens");
+    if (lens->radius != 0.0f) return fail(HVVR_ERR_INVALID, "thin-lens depth of field is not built (radius must be 0)");
+    cam->lens = *lens;
+    cam->setupDirty = true;
+    return HVVR_OK;
+}
+int hvvr_camera_set_aperture(hvvr_camera* cam, float radius) {
+    CAM_CHECK(cam);
+    hvvr_thin_lens l = cam->lens;
+    l.radius = radius;
+    return hvvr_camera_set_lens(cam, &l);
+}
+int hvvr_camera_set_focal_depth(hvvr_camera* cam, float depth) {
+    CAM_CHECK(cam);
+    cam->lens.focal_distance = depth;
+    cam->setupDirty = true;
+    return HVVR_OK;
+}
+int hvvr_camera_set_eye_dir(hvvr_camera* cam, const hvvr_vec3* eye_dir) {
+    CAM_CHECK(cam);
+    if (!eye_dir) return fail(HVVR_ERR_INVALID, "NULL eye_dir");
+    cam->eyeDir = *eye_dir;
+    return HVVR_OK;
+}
+int hvvr_camera_set_spherical_warp(hvvr_camera* cam, float fov_x_degrees, float fov_y_degrees) {
+    CAM_CHECK(cam);
+    cam->fovX = fov_x_degrees;
+    cam->fovY = fov_y_degrees;
+    cam->setupDirty = true;
+    return HVVR_OK;
+}
+int hvvr_camera_set_render_target(hvvr_camera* cam, const hvvr_image_desc* target) {
+    CAM_CHECK(cam);
+    if (!target) return fail(HVVR_ERR_INVALID, "NULL target");
+    if (target->memory_type != HVVR_MEMORY_CPU && target->memory_type != HVVR_MEMORY_CUDA)
+        return fail(HVVR_ERR_INVALID, "render target must be CPU or CUDA memory (no graphics API here)");
+    if (target->pixel_format != HVVR_PIXEL_RGBA8_SRGB) return fail(HVVR_ERR_INVALID, "pixel format must be RGBA8 sRGB");
+    if (target->stride && target->stride < target->width) return fail(HVVR_ERR_INVALID, "stride < width");
+    cudaStreamSynchronize(cam->rc->stream);
+    unregisterTarget(cam);
+    cam->target = *target;
+    if (target->memory_type == HVVR_MEMORY_CPU && target->data && target->width && target->height) {
+        const size_t bytes = size_t(target->stride ? target->stride : target->width) * target->height * 4;
+        if (cudaHostRegister(target->data, bytes, cudaHostRegisterDefault) == cudaSuccess) cam->registered = target->data;
+        else cudaGetLastError();
+    }
+    cam->setupDirty = true;
+    return HVVR_OK;
+}
+int hvvr_camera_set_samples(hvvr_camera* cam, const hvvr_sample* samples, uint32_t count, uint32_t split) {
+    CAM_CHECK(cam);
+    if (!samples || count == 0) return fail(HVVR_ERR_INVALID, "no samples");
+    if (split < 1 || split > 3) return fail(HVVR_ERR_INVALID, "splitColorSamples must be 1, 2 or 3");
+    cam->samples.assign(samples, samples + count);
+    cam->split = split;
+    cam->setupDirty = true;
+    return HVVR_OK;
+}
+int hvvr_camera_set_camera_to_world(hvvr_camera* cam, const hvvr_transform* xf) {
+    CAM_CHECK(cam);
+    if (!xf) return fail(HVVR_ERR_INVALID, "NULL transform");
+    cam->xf = *xf;
+    return HVVR_OK;
+}
+int hvvr_camera_set_msaa(hvvr_camera* cam, uint32_t rate) {
+    CAM_CHECK(cam);
+    if (!validRate(rate)) return fail(HVVR_ERR_INVALID, "MSAA rate must be 1, 2, 4, 8, 16 or 32");
+    cam->msaa = rate;
+    return HVVR_OK;
+}
+int hvvr_camera_get_sample_count(const hvvr_camera* cam, uint32_t* count) {
+    CAM_CHECK(cam);
+    if (!count) return fail(HVVR_ERR_INVALID, "NULL count");
+    *count = uint32_t(cam->samples.size());
+    return HVVR_OK;
+}
+int hvvr_camera_set_capture(hvvr_camera* cam, uint32_t flags) {
+    CAM_CHECK(cam);
+    cam->capture = flags;
+    if (!(flags & HVVR_CAPTURE_HITS)) {
+        cam->dev.hitIds = nullptr;
+        cam->dev.depth = nullptr;
+    }
+    return HVVR_OK;
+}
+int hvvr_camera_get_layout(const hvvr_camera* cam, uint32_t* block_count, uint32_t* tile_count,
+                           uint32_t* padded_sample_count, uint32_t* msaa_rate) {
+    CAM_CHECK(cam);
+    const uint32_t n = uint32_t(cam->samples.size());
+    const uint32_t blocks = (n + kBlockSize - 1) / kBlockSize;
+    if (block_count) *block_count = blocks;
+    if (tile_count) *tile_count = blocks * kTilesPerBlock;
+    if (padded_sample_count) *padded_sample_count = blocks * kBlockSize;
+    if (msaa_rate) *msaa_rate = cam->msaa;
+    return HVVR_OK;
+}
+
+static int requireRendered(const hvvr_camera* cam) {
+    if (!cam) return fail(HVVR_ERR_INVALID, "NULL camera");
+    if (!cam->rendered) return fail(HVVR_ERR_STATE, "camera has not rendered a frame");
+    cudaError_t e = cudaStreamSynchronize(cam->rc->stream);
+    if (e != cudaSuccess) return fail(HVVR_ERR_CUDA, "sync: %s", cudaGetErrorString(e));
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(HVVR_ERR_CUDA, "sync: %s", cudaGetErrorString(e));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_tile_lists(const hvvr_camera* cam, uint32_t* counts, uint32_t* indices, uint64_t capacity,
+                                uint64_t* total) {
+    TRY(requireRendered(cam));
+    const CameraDev& d = cam->dev;
+    std::vector<TileList> lists(d.tiles);
+    CUDA_TRY(cudaMemcpy(lists.data(), d.tileLists, sizeof(TileList) * d.tiles, cudaMemcpyDeviceToHost));
+    uint64_t sum = 0;
+    for (uint32_t t = 0; t < d.tiles; t++) {
+        if (counts) counts[t] = lists[t].count;
+        sum += lists[t].count;
+    }
+    if (total) *total = sum;
+    if (!indices) return HVVR_OK;
+    if (capacity < sum) return fail(HVVR_ERR_OVERFLOW, "capacity %llu < %llu entries", (unsigned long long)capacity,
+                                    (unsigned long long)sum);
+    uint32_t used = 0;
+    CUDA_TRY(cudaMemcpy(&used, d.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    used = std::min(used, d.poolChunks);
+    std::vector<uint32_t> pool(size_t(used) * kChunk), next(used);
+    if (used) {
+        CUDA_TRY(cudaMemcpy(pool.data(), d.pool, pool.size() * 4, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(next.data(), d.chunkNext, next.size() * 4, cudaMemcpyDeviceToHost));
+    }
+    uint64_t w = 0;
+    for (uint32_t t = 0; t < d.tiles; t++) {
+        uint32_t c = lists[t].first, left = lists[t].count;
+        while (left) {
+            if (c >= used) return fail(HVVR_ERR_STATE, "broken chunk chain in tile %u", t);
+            const uint32_t n = std::min<uint32_t>(left, kChunk);
+            memcpy(indices + w, &pool[size_t(c) * kChunk], n * 4);
+            w += n;
+            left -= n;
+            c = next[c];
+        }
+    }
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_block_stacks(const hvvr_camera* cam, uint32_t* sizes, uint32_t* entries) {
+    TRY(requireRendered(cam));
+    const CameraDev& d = cam->dev;
+    std::vector<uint32_t> sz(d.blocks);
+    CUDA_TRY(cudaMemcpy(sz.data(), d.blockSizes, 4 * size_t(d.blocks), cudaMemcpyDeviceToHost));
+    if (sizes) memcpy(sizes, sz.data(), 4 * size_t(d.blocks));
+    if (entries) {
+        std::vector<StackEntry> e(size_t(d.blocks) * kBlockStack);
+        CUDA_TRY(cudaMemcpy(e.data(), d.blockStacks, e.size() * sizeof(StackEntry), cudaMemcpyDeviceToHost));
+        for (uint32_t b = 0; b < d.blocks; b++)
+            for (uint32_t i = 0; i < kBlockStack; i++) {
+                uint32_t* dst = entries + (size_t(b) * kBlockStack + i) * 3;
+                if (i < sz[b]) {
+                    const StackEntry& s = e[size_t(b) * kBlockStack + i];
+                    memcpy(&dst[0], &s.tMin, 4);
+                    dst[1] = s.mask;
+                    dst[2] = s.node;
+                } else {
+                    dst[0] = dst[1] = dst[2] = 0;
+                }
+            }
+    }
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_hits(const hvvr_camera* cam, uint32_t* tri_ids, float* depth) {
+    TRY(requireRendered(cam));
+    const CameraDev& d = cam->dev;
+    if (!d.hitIds) return fail(HVVR_ERR_STATE, "hit capture was not enabled for the last frame");
+    const size_t n = size_t(d.padded) * d.msaa;
+    if (tri_ids) CUDA_TRY(cudaMemcpy(tri_ids, d.hitIds, n * 4, cudaMemcpyDeviceToHost));
+    if (depth) CUDA_TRY(cudaMemcpy(depth, d.depth, n * 4, cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_gbuffer(const hvvr_camera* cam, uint32_t* n, uint32_t* tri, uint32_t* mask) {
+    TRY(requireRendered(cam));
+    const CameraDev& d = cam->dev;
+    if (!d.hitIds) return fail(HVVR_ERR_STATE, "hit capture was not enabled for the last frame");
+    const uint32_t N = d.msaa;
+    std::vector<uint32_t> hits(size_t(d.padded) * N);
+    CUDA_TRY(cudaMemcpy(hits.data(), d.hitIds, hits.size() * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t s = 0; s < d.padded; s++) {
+        uint32_t keys[32];
+        for (uint32_t i = 0; i < N; i++) keys[i] = (hits[size_t(s) * N + i] << 5) | i;
+        std::sort(keys, keys + N);
+        uint32_t gn = 0, gt[32], gm[32];
+        for (uint32_t i = 0; i < N; i++) {
+            const uint32_t t = uint32_t(int32_t(keys[i]) >> 5), m = 1u << (keys[i] & 31);
+            if (gn && gt[gn - 1] == t) gm[gn - 1] |= m;
+            else { gt[gn] = t; gm[gn] = m; gn++; }
+        }
+        if (n) n[s] = gn;
+        for (uint32_t i = 0; i < N; i++) {
+            if (tri) tri[size_t(s) * N + i] = i < gn ? gt[i] : 0;
+            if (mask) mask[size_t(s) * N + i] = i < gn ? gm[i] : 0;
+        }
+    }
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_sample_colors(const hvvr_camera* cam, uint32_t* rgba) {
+    TRY(requireRendered(cam));
+    if (!rgba) return fail(HVVR_ERR_INVALID, "NULL output");
+    CUDA_TRY(cudaMemcpy(rgba, cam->dev.colors, size_t(cam->dev.padded) * 4, cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_sample_remap(const hvvr_camera* cam, int32_t* remap, uint64_t count) {
+    CAM_CHECK(cam);
+    if (cam->setupDirty) return fail(HVVR_ERR_STATE, "sample setup not built yet (render once first)");
+    if (!remap || count < cam->setup.remap.size()) return fail(HVVR_ERR_INVALID, "remap buffer too small");
+    memcpy(remap, cam->setup.remap.data(), cam->setup.remap.size() * 4);
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9) {
+    CAM_CHECK(cam);
+    if (cam->setupDirty) return fail(HVVR_ERR_STATE, "sample setup not built yet (render once first)");
+    if (!beams9) return fail(HVVR_ERR_INVALID, "NULL output");
+    for (size_t i = 0; i < cam->setup.padded; i++) memcpy(beams9 + 9 * i, &cam->setup.beams[12 * i], 9 * 4);
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_timings(const hvvr_camera* cam, float* ms6) {
+    TRY(requireRendered(cam));
+    if (!ms6) return fail(HVVR_ERR_INVALID, "NULL output");
+    ms6[0] = 0.0f;
+    for (int i = 1; i < 5; i++) CUDA_TRY(cudaEventElapsedTime(&ms6[i], cam->ev[i - 1], cam->ev[i]));
+    CUDA_TRY(cudaEventElapsedTime(&ms6[5], cam->ev[0], cam->ev[5]));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_list_total(const hvvr_camera* cam, uint64_t* total) {
+    return hvvr_camera_read_tile_lists(cam, nullptr, nullptr, 0, total);
+}
+
+int hvvr_scene_get_counts(const hvvr_raycaster* rc, uint32_t* node_count, uint32_t* tri_count, uint32_t* vert_count) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    if (node_count) *node_count = rc->scene.nodeCount;
+    if (tri_count) *tri_count = rc->scene.triCount;
+    if (vert_count) *vert_count = rc->scene.vertCount;
+    return HVVR_OK;
+}
+
+int hvvr_scene_read_nodes(hvvr_raycaster* rc, void* nodes128) {
+    if (!rc || !nodes128) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (rc->scene.nodeCount == 0) return fail(HVVR_ERR_STATE, "no scene uploaded");
+    CUDA_TRY(cudaStreamSynchronize(rc->stream));
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(nodes128, rc->scene.nodes, size_t(rc->scene.nodeCount) * sizeof(Node), cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
+int hvvr_scene_read_triangles(hvvr_raycaster* rc, float* tris9) {
+    if (!rc || !tris9) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (rc->scene.nodeCount == 0) return fail(HVVR_ERR_STATE, "no scene uploaded");
+    CUDA_TRY(cudaDeviceSynchronize());
+    std::vector<float4> t(size_t(rc->scene.triCount) * 3);
+    CUDA_TRY(cudaMemcpy(t.data(), rc->scene.tris, t.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < rc->scene.triCount; i++) memcpy(tris9 + 9 * i, &t[3 * i], 9 * 4);
+    return HVVR_OK;
+}
+
+int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out) {
+    if (!out || !width || !height) return fail(HVVR_ERR_INVALID, "bad arguments");
+    // getGridSamples (libraries/hvvr/raycaster/samples.cpp:21-42)
+    const float invW = 1.0f / width, invH = 1.0f / height;
+    for (uint32_t y = 0; y < height; y++)
+        for (uint32_t x = 0; x < width; x++) {
+            hvvr_sample& s = out[size_t(y) * width + x];
+            s.pixel_x = x;
+            s.pixel_y = y;
+            s.position.x = (float(x) + 0.5f) * invW;
+            s.position.y = (float(y) + 0.5f) * invH;
+            if (width > height) {
+                s.minor_axis = hvvr_vec2{invW, 0.0f};
+                s.major_axis_length = invH;
+            } else {
+                s.minor_axis = hvvr_vec2{0.0f, invH};
+                s.major_axis_length = invW;
+            }
+        }
+    return HVVR_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,552 @@
+// shade.cu - fused intersect + G-buffer compression + MSAA shade/resolve, and the remap.
+//
+// intersectShadeKernel<N, FMA> runs one 128-thread CTA per tile (thread = sample), like
+// the reference's IntersectKernel and ResolveKernel (libraries/hvvr/raycaster/intersect.cu:298-342,
+// libraries/hvvr/raycaster/resolve.cu:324-458), but as one launch: the per-subsample hit
+// IDs stay in registers, are grouped into (triangle, coverage mask) pairs exactly as
+// EmitGBuffer does (intersect.cu:28-89), and are shaded and resolved in the same thread
+// (ShadeMSAA, resolve.cu:161-284). The G-buffer therefore never goes to HBM.
+//
+// The tile's triangle list is consumed in its chunks of 128 entries. Each thread tests one
+// entry against the tile frustum planes, the ray-origin half space and the corner-ray
+// barycentric bounds (FrustumPlanes::test, IntersectTriangleTile<false>::setup,
+// TestTriangleFrustaUVW; libraries/hvvr/raycaster/prim_tests.h:18-164); survivors are compacted
+// into shared memory in list order with warp ballots, and every thread then tests its
+// sample's N subsamples against them in that order, so depth ties resolve as in the reference.
+#include "dev_common.cuh"
+
+namespace hvb {
+
+__constant__ float2 cMsaa[6][32]; // unit offsets for rates 1,2,4,8,16,32
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <uint32_t N> struct RateIndex;
+template <> struct RateIndex<1> { static constexpr int v = 0; };
+template <> struct RateIndex<2> { static constexpr int v = 1; };
+template <> struct RateIndex<4> { static constexpr int v = 2; };
+template <> struct RateIndex<8> { static constexpr int v = 3; };
+template <> struct RateIndex<16> { static constexpr int v = 4; };
+template <> struct RateIndex<32> { static constexpr int v = 5; };
+
+struct TriGeom {
+    F3 v0, e0, e1;
+};
+__device__ __forceinline__ TriGeom loadTri(const float4* __restrict__ tris, uint32_t i) {
+    const float4 a = __ldg(tris + 3 * size_t(i) + 0);
+    const float4 b = __ldg(tris + 3 * size_t(i) + 1);
+    const float4 c = __ldg(tris + 3 * size_t(i) + 2);
+    return TriGeom{f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x)};
+}
+
+// per-thread scaled barycentric setup (IntersectTriangleThread ctor + GetDifferentials,
+// prim_tests.h:118-134, 175-188)
+struct TriThread {
+    float dc, vc, wc, ddx, ddy, dvx, dvy, dwx, dwy;
+};
+__device__ __forceinline__ TriThread threadSetup(F3 e0, F3 e1, F3 v0r, F3 c, F3 du, F3 dv) {
+    TriThread r;
+    const F3 normal = cross3(e0, e1);
+    r.dc = dot3(-c, normal);
+    const F3 ec = cross3(-c, v0r);
+    r.vc = dot3(e1, ec);
+    r.wc = -dot3(e0, ec);
+    r.ddx = dot3(-du, normal);
+    r.ddy = dot3(-dv, normal);
+    const F3 cu = cross3(-du, v0r), cv = cross3(-dv, v0r);
+    r.dvx = dot3(e1, cu);
+    r.dvy = dot3(e1, cv);
+    r.dwx = -dot3(e0, cu);
+    r.dwy = -dot3(e0, cv);
+    return r;
+}
+
+// IntersectTriangleThread::test (prim_tests.h:192-231)
+template <bool FMA>
+__device__ __forceinline__ bool threadTest(const TriThread& th, float t, float ax, float ay, float& depth) {
+    float denom, depthDelta, v, w;
+    if (FMA) {
+        denom = fmaf(th.ddy, ay, fmaf(th.ddx, ax, th.dc));
+        depthDelta = fmaf(depth, denom, -t);
+        v = fmaf(th.dvy, ay, fmaf(th.dvx, ax, th.vc));
+        w = fmaf(th.dwy, ay, fmaf(th.dwx, ax, th.wc));
+    } else {
+        denom = th.dc + th.ddx * ax + th.ddy * ay;
+        depthDelta = depth * denom - t;
+        v = th.vc + th.dvx * ax + th.dvy * ay;
+        w = th.wc + th.dwx * ax + th.dwy * ay;
+    }
+    const float u = denom - v - w;
+    const int test = __float_as_int(depthDelta) | __float_as_int(u) | __float_as_int(v) | __float_as_int(w);
+    if (test < 0) return false;
+    depth = t * (1.0f / denom);
+    return true;
+}
+
+// IntersectTriangleThread::calcUVW (prim_tests.h:233-245)
+template <bool FMA>
+__device__ __forceinline__ F3 calcUVW(const TriThread& th, float ax, float ay) {
+    float denom, v, w;
+    if (FMA) {
+        denom = fmaf(th.ddy, ay, fmaf(th.ddx, ax, th.dc));
+        v = fmaf(th.dvy, ay, fmaf(th.dvx, ax, th.vc));
+        w = fmaf(th.dwy, ay, fmaf(th.dwx, ax, th.wc));
+    } else {
+        denom = th.dc + th.ddx * ax + th.ddy * ay;
+        v = th.vc + th.dvx * ax + th.dvy * ay;
+        w = th.wc + th.dwx * ax + th.dwy * ay;
+    }
+    const float u = denom - v - w;
+    const float inv = 1.0f / denom;
+    return f3(u * inv, v * inv, w * inv);
+}
+
+// TestRayTriangle<false> barycentrics (prim_tests.h:53-82)
+__device__ __forceinline__ void rayTriUVW(F3 ro, F3 rd, const TriGeom& tri, float& u, float& v, float& w) {
+    const F3 n = cross3(tri.e0, tri.e1);
+    const float denom = dot3(-rd, n);
+    const F3 v0r = ro - tri.v0;
+    const F3 e = cross3(-rd, v0r);
+    v = dot3(tri.e1, e);
+    w = -dot3(tri.e0, e);
+    const float ood = 1.0f / denom;
+    v = v * ood;
+    w = w * ood;
+    u = 1.0f - v - w;
+}
+
+struct Material {
+    F3 emissive, diffuse, specular;
+    float glossiness;
+    uint32_t model;
+};
+
+__device__ __forceinline__ float pow5(float x) {
+    const float x2 = x * x;
+    return x2 * x2 * x;
+}
+
+// GGX_SchlickFresnel_SchlickSmithGGX + PBR_BRDF1 (libraries/hvvr/raycaster/shading_helpers.h:89-122)
+__device__ F3 pbr(F3 L, F3 N, F3 V, F3 base, float roughness, F3 F0, F3 lightColor) {
+    const float alpha = roughness * roughness;
+    const F3 H = normalize3(L + V);
+    const float alpha2 = alpha * alpha;
+    const float NdotH = satf(dot3(N, H));
+    const float q = (NdotH * NdotH) * (alpha2 - 1.0f) + 1.0f;
+    const float D = alpha2 / (3.141592653589f * (q * q));
+    const float LdotH = satf(dot3(L, H));
+    const F3 F = F0 + (f3(1.0f, 1.0f, 1.0f) - F0) * pow5(1.0f - LdotH);
+    const float NdotL = satf(dot3(N, L));
+    const float NdotV = satf(dot3(N, V));
+    const float k = alpha * 0.5f;
+    const float vis = (1.0f / (NdotL * (1.0f - k) + k)) * (1.0f / (NdotV * (1.0f - k) + k));
+    const F3 spec = ((F * D) * vis) * (1.0f / 4.0f);
+    const float NdotL2 = satf(dot3(N, L));
+    const F3 diffuse = ((base * lightColor) * (f3(1.0f, 1.0f, 1.0f) - spec)) * NdotL2;
+    return diffuse + lightColor * spec;
+}
+
+// GGXShade for untextured materials (libraries/hvvr/raycaster/shading.h:84-161)
+__device__ F3 ggxShade(const Material& m, F3 pos, F3 nrm, F3 camPos, const LightEnvDev& env) {
+    const F3 normal = normalize3(nrm);
+    if (m.model == 2u) return m.emissive;
+    const F3 V = normalize3(camPos - pos);
+    const float roughness = 1.0f - m.glossiness;
+    F3 radiance = m.emissive + m.diffuse * f3(.15f, .15f, .165f);
+    if (env.nd > 0) {
+        radiance = radiance + pbr(f3(env.dir[0][0], env.dir[0][1], env.dir[0][2]), normal, V, m.diffuse, roughness,
+                                  m.specular, f3(env.dir[0][3], env.dir[0][4], env.dir[0][5]));
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (i >= env.np) break;
+        const float* l = env.pt[i];
+        const F3 delta = f3(l[0], l[1], l[2]) - pos;
+        const float r = sqrtf(dot3(delta, delta));
+        const F3 L = normalize3(delta);
+        const float fd = satf((l[3] - r) * l[7]);
+        radiance = radiance + pbr(L, normal, V, m.diffuse, roughness, m.specular, f3(l[4], l[5], l[6]) * fd);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (i >= env.ns) break;
+        const float* l = env.spot[i];
+        const F3 delta = f3(l[0], l[1], l[2]) - pos;
+        const float r = sqrtf(dot3(delta, delta));
+        const F3 L = normalize3(delta);
+        const float fd = satf((l[3] - r) * l[7]);
+        const F3 lit = pbr(L, normal, V, m.diffuse, roughness, m.specular, f3(l[8], l[9], l[10]) * fd);
+        const float cosA = dot3(f3(l[4], l[5], l[6]), -L);
+        const float fa = satf((cosA - l[11]) * l[12]);
+        radiance = radiance + lit * fa;
+    }
+    return f3(tmaxf(radiance.x, 0.0f), tmaxf(radiance.y, 0.0f), tmaxf(radiance.z, 0.0f));
+}
+
+// ACESFilm, linearToSRgb, ToColor4Unorm8SRgb (shading_helpers.h:158-200; libraries/hvvr/shared/util_graphics.h:26-28)
+__device__ __forceinline__ float aces(float x) { return satf((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f)); }
+__device__ __forceinline__ float toSrgb(float x) {
+    return (x <= 0.0031308f) ? (x * 12.92f) : (powf(x, (1.0f / 2.4f)) * 1.055f - .055f);
+}
+__device__ __forceinline__ uint32_t packColor(F3 c) {
+    const uint32_t r = uint32_t(toSrgb(c.x) * 255.0f);
+    const uint32_t g = uint32_t(toSrgb(c.y) * 255.0f);
+    const uint32_t b = uint32_t(toSrgb(c.z) * 255.0f);
+    return r | (g << 8) | (b << 16) | 0xFF000000u;
+}
+
+__device__ __forceinline__ F3 halfNormal(float4 a, float4 b) {
+    const uint32_t n01 = __float_as_uint(a.w), n23 = __float_as_uint(b.x);
+    return f3(__half2float(__ushort_as_half((unsigned short)(n01 & 0xffffu))),
+              __half2float(__ushort_as_half((unsigned short)(n01 >> 16))),
+              __half2float(__ushort_as_half((unsigned short)(n23 & 0xffffu))));
+}
+
+// ascending sort of N unique keys held in registers (odd-even transposition; N <= 32)
+template <uint32_t N>
+__device__ __forceinline__ void sortKeys(uint32_t (&k)[N]) {
+#pragma unroll
+    for (uint32_t r = 0; r < N; r++) {
+#pragma unroll
+        for (uint32_t i = (r & 1u); i + 1 < N; i += 2) {
+            const uint32_t a = k[i], b = k[i + 1];
+            k[i] = a < b ? a : b;
+            k[i + 1] = a < b ? b : a;
+        }
+    }
+}
+
+struct ShadeSmem {
+    float ro[4][3], rd[4][3]; // world corner rays
+    float pl[4][4];           // frustum planes
+    uint32_t idx[kChunk];
+    float tt[kChunk];
+    float e0[3][kChunk];
+    float e1[3][kChunk];
+    float vr[3][kChunk];
+    float nl[kChunk]; // |e0 x e1| as computed in float, for the depth skip
+    uint32_t warpCount[4];
+};
+
+template <uint32_t N, bool FMA>
+__global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
+    const float4* __restrict__ tris, const uint4* __restrict__ triShade, const float4* __restrict__ verts,
+    const float4* __restrict__ materials, const Rays4* __restrict__ tileRays, const float4* __restrict__ beams,
+    const TileList* __restrict__ lists, const uint32_t* __restrict__ pool, const uint32_t* __restrict__ chunkNext,
+    Mat4 M, LightEnvDev env, uint32_t* __restrict__ colors, uint32_t* __restrict__ hitOut,
+    float* __restrict__ depthOut) {
+    __shared__ ShadeSmem sm;
+    const uint32_t tile = blockIdx.x, tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t sid = tile * kTileSize + tid;
+    const TileList L = lists[tile];
+    if (L.count == 0) {
+        // ClearEmptyKernel (resolve.cu:527-542)
+        colors[sid] = 0xFF000000u;
+        if (hitOut) {
+#pragma unroll
+            for (uint32_t i = 0; i < N; i++) {
+                hitOut[size_t(sid) * N + i] = ~0u;
+                depthOut[size_t(sid) * N + i] = INFINITY;
+            }
+        }
+        return;
+    }
+    const int rate = RateIndex<N>::v;
+    // world-space tile rays (the SimpleRayFrustum of transformHierarchyCameraToWorld) and
+    // FrustumPlanes (prim_tests.h:22-28)
+    if (tid < 8) {
+        const Rays4& cr = tileRays[tile];
+        const uint32_t i = tid & 3u;
+        if (tid < 4) {
+            const F3 o = xformPoint(M, f3(cr.o[i][0], cr.o[i][1], cr.o[i][2]));
+            sm.ro[i][0] = o.x; sm.ro[i][1] = o.y; sm.ro[i][2] = o.z;
+        } else {
+            const F3 d = xformDir(M, f3(cr.d[i][0], cr.d[i][1], cr.d[i][2]));
+            sm.rd[i][0] = d.x; sm.rd[i][1] = d.y; sm.rd[i][2] = d.z;
+        }
+    }
+    __syncthreads();
+    if (tid < 4) {
+        const F3 d0 = f3(sm.rd[tid][0], sm.rd[tid][1], sm.rd[tid][2]);
+        const F3 d1 = f3(sm.rd[(tid + 1) & 3][0], sm.rd[(tid + 1) & 3][1], sm.rd[(tid + 1) & 3][2]);
+        const F3 n = cross3(d0, d1);
+        sm.pl[tid][0] = n.x; sm.pl[tid][1] = n.y; sm.pl[tid][2] = n.z;
+        sm.pl[tid][3] = dot3(f3(sm.ro[tid][0], sm.ro[tid][1], sm.ro[tid][2]), n);
+    }
+    const F3 camPos = f3(M.m[3][0], M.m[3][1], M.m[3][2]);
+    // this thread's beam, rotated to world space (GetDirectionalSample3D, gpu_samples.h:78-82)
+    const float4 b0 = __ldg(beams + 3 * size_t(sid) + 0);
+    const float4 b1 = __ldg(beams + 3 * size_t(sid) + 1);
+    const float4 b2 = __ldg(beams + 3 * size_t(sid) + 2);
+    const F3 c = xformDir(M, f3(b0.x, b0.y, b0.z));
+    const F3 du = xformDir(M, f3(b0.w, b1.x, b1.y));
+    const F3 dv = xformDir(M, f3(b1.z, b1.w, b2.x));
+    // Upper bound on |denom| / |e0 x e1| over this sample's subsamples: denom = -dir . n with
+    // dir = c + ax du + ay dv and |ax|,|ay| <= 1, so |denom| <= (|c| + |du| + |dv|) |n|.
+    const float dirLen = (sqrtf(dot3(c, c)) + sqrtf(dot3(du, du)) + sqrtf(dot3(dv, dv))) * 1.0001f;
+    float tmax[N];
+    uint32_t hit[N];
+#pragma unroll
+    for (uint32_t i = 0; i < N; i++) {
+        tmax[i] = FLT_MAX;
+        hit[i] = ~0u;
+    }
+    __syncthreads();
+
+    uint32_t chunk = L.first;
+    uint32_t remaining = L.count;
+    while (remaining > 0) {
+        const uint32_t n = remaining < kChunk ? remaining : kChunk;
+        const uint32_t nextChunk = chunkNext[chunk];
+        bool keep = false;
+        uint32_t idx = 0;
+        float t = 0.0f, nlen = 0.0f;
+        F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0);
+        if (tid < n) {
+            idx = pool[size_t(chunk) * kChunk + tid];
+            const TriGeom tri = loadTri(tris, idx);
+            // FrustumPlanes::test
+            bool in = true;
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const F3 dir = f3(sm.pl[p][0], sm.pl[p][1], sm.pl[p][2]);
+                const float dist = sm.pl[p][3];
+                const float d0 = dot3(dir, tri.v0);
+                const float d1 = d0 + dot3(dir, tri.e0);
+                const float d2 = d0 + dot3(dir, tri.e1);
+                if (d0 > dist && d1 > dist && d2 > dist) in = false;
+            }
+            if (in) {
+                // IntersectTriangleTile<false>::setup
+                const F3 normal = cross3(tri.e0, tri.e1);
+                v0r = camPos - tri.v0;
+                t = dot3(v0r, normal);
+                if (!(t < 0.0f)) {
+                    // TestTriangleFrustaUVW != intersect_all_out
+                    float uMin = FLT_MAX, uMax = -FLT_MAX, vMin = FLT_MAX, vMax = -FLT_MAX, wMin = FLT_MAX,
+                          wMax = -FLT_MAX;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        float u, v, w;
+                        rayTriUVW(f3(sm.ro[r][0], sm.ro[r][1], sm.ro[r][2]), f3(sm.rd[r][0], sm.rd[r][1], sm.rd[r][2]),
+                                  tri, u, v, w);
+                        uMin = tminf(uMin, u); uMax = tmaxf(uMax, u);
+                        vMin = tminf(vMin, v); vMax = tmaxf(vMax, v);
+                        wMin = tminf(wMin, w); wMax = tmaxf(wMax, w);
+                    }
+                    const bool allOut = uMax < 0 || uMin > 1 || vMax < 0 || vMin > 1 || wMax < 0 || wMin > 1;
+                    if (!allOut) {
+                        keep = true;
+                        e0 = tri.e0;
+                        e1 = tri.e1;
+                        nlen = sqrtf(dot3(normal, normal));
+                    }
+                }
+            }
+        }
+        const uint32_t bal = __ballot_sync(kFull, keep);
+        if (lane == 0) sm.warpCount[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t off = __popc(bal & ((1u << lane) - 1u));
+        uint32_t total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < 4; w++) {
+            const uint32_t cw = sm.warpCount[w];
+            off += (w < warp) ? cw : 0u;
+            total += cw;
+        }
+        if (keep) {
+            sm.idx[off] = idx;
+            sm.tt[off] = t;
+            sm.e0[0][off] = e0.x; sm.e0[1][off] = e0.y; sm.e0[2][off] = e0.z;
+            sm.e1[0][off] = e1.x; sm.e1[1][off] = e1.y; sm.e1[2][off] = e1.z;
+            sm.vr[0][off] = v0r.x; sm.vr[1][off] = v0r.y; sm.vr[2][off] = v0r.z;
+            sm.nl[off] = nlen;
+        }
+        __syncthreads();
+        // Depth skip. The test rejects a subsample when depth * denom < t (FMA mode, exactly;
+        // STRICT mode with the product rounded, covered by the 1e-4 margin in dirLen). With
+        // denom <= dirLen * |n| and depth <= laneT, t > laneT * dirLen * |n| rejects every
+        // subsample of the lane; a triangle is skipped only when that holds for all 32 lanes,
+        // so the hits are exactly those of the full loop. Misses keep laneT at FLT_MAX (no skip).
+        float laneT = 0.0f;
+#pragma unroll
+        for (uint32_t i = 0; i < N; i++) laneT = fmaxf(laneT, tmax[i]);
+        const float laneBound = laneT * dirLen;
+        for (uint32_t j = 0; j < total; j++) {
+            if (__all_sync(kFull, sm.tt[j] > laneBound * sm.nl[j])) continue;
+            const F3 je0 = f3(sm.e0[0][j], sm.e0[1][j], sm.e0[2][j]);
+            const F3 je1 = f3(sm.e1[0][j], sm.e1[1][j], sm.e1[2][j]);
+            const F3 jvr = f3(sm.vr[0][j], sm.vr[1][j], sm.vr[2][j]);
+            const float jt = sm.tt[j];
+            const uint32_t jidx = sm.idx[j];
+            const TriThread th = threadSetup(je0, je1, jvr, c, du, dv);
+#pragma unroll
+            for (uint32_t i = 0; i < N; i++) {
+                const float2 a = cMsaa[rate][i];
+                if (threadTest<FMA>(th, jt, a.x, a.y, tmax[i])) hit[i] = jidx;
+            }
+        }
+        __syncthreads();
+        remaining -= n;
+        chunk = nextChunk;
+    }
+
+    if (hitOut) {
+#pragma unroll
+        for (uint32_t i = 0; i < N; i++) {
+            hitOut[size_t(sid) * N + i] = hit[i];
+            depthOut[size_t(sid) * N + i] = hit[i] == ~0u ? INFINITY : tmax[i];
+        }
+    }
+
+    // G-buffer grouping (EmitGBuffer): (triangle, mask) pairs in ascending triangle order,
+    // misses (~0) last; then ShadeMSAA over the groups in that order.
+    uint32_t keys[N];
+#pragma unroll
+    for (uint32_t i = 0; i < N; i++) keys[i] = (hit[i] << 5) | i;
+    bool uniform = true;
+#pragma unroll
+    for (uint32_t i = 1; i < N; i++) uniform = uniform && (hit[i] == hit[0]);
+    if (!uniform) sortKeys<N>(keys);
+    float rx = 0.0f, ry = 0.0f, rz = 0.0f;
+    const uint32_t maskAll = N < 32 ? ((1u << N) - 1u) : ~0u;
+    uint32_t combined = 0;
+    uint32_t gi = 0;
+    while (gi < N) {
+        if (combined == maskAll) break;
+        const uint32_t triIndex = uint32_t(int32_t(keys[gi]) >> 5);
+        if (triIndex == ~0u) break;
+        uint32_t sampleMask = 0;
+        uint32_t gj = gi;
+        if (uniform) {
+            sampleMask = maskAll;
+            gj = N;
+        } else {
+            while (gj < N && uint32_t(int32_t(keys[gj]) >> 5) == triIndex) {
+                sampleMask |= 1u << (keys[gj] & 31u);
+                gj++;
+            }
+        }
+        gi = gj;
+        combined |= sampleMask;
+        const float pc = float(__popc(sampleMask));
+        const float inv = 1.0f / pc;
+        float cax = 0.0f, cay = 0.0f;
+        for (uint32_t cm = sampleMask; cm;) {
+            const int si = __ffs(cm) - 1;
+            cm &= ~(1u << si);
+            const float2 a = cMsaa[rate][si];
+            cax = cax + a.x * inv;
+            cay = cay + a.y * inv;
+        }
+        const TriGeom tri = loadTri(tris, triIndex);
+        const F3 v0r = camPos - tri.v0;
+        const TriThread th = threadSetup(tri.e0, tri.e1, v0r, c, du, dv);
+        const F3 bc = calcUVW<FMA>(th, cax, cay);
+        const uint4 ts = __ldg(triShade + triIndex);
+        const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
+        const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
+        const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
+        const F3 pos = (f3(a0.x, a0.y, a0.z) * bc.x + f3(p0.x, p0.y, p0.z) * bc.y) + f3(q0.x, q0.y, q0.z) * bc.z;
+        const F3 nrm = (halfNormal(a0, a1) * bc.x + halfNormal(p0, p1) * bc.y) + halfNormal(q0, q1) * bc.z;
+        const float4 m0 = __ldg(materials + 4 * size_t(ts.w) + 0);
+        const float4 m1 = __ldg(materials + 4 * size_t(ts.w) + 1);
+        const float4 m2 = __ldg(materials + 4 * size_t(ts.w) + 2);
+        const float4 m3 = __ldg(materials + 4 * size_t(ts.w) + 3);
+        Material mat;
+        mat.emissive = f3(m0.x, m0.y, m0.z);
+        mat.diffuse = f3(m1.x, m1.y, m1.z);
+        mat.specular = f3(m2.x, m2.y, m2.z);
+        mat.glossiness = m3.x;
+        mat.model = __float_as_uint(m3.z) & 0xffffu;
+        const F3 col = ggxShade(mat, pos, nrm, camPos, env);
+        rx = rx + col.x * pc;
+        ry = ry + col.y * pc;
+        rz = rz + col.z * pc;
+    }
+    const float sN = 1.0f / float(N);
+    colors[sid] = packColor(f3(aces(rx * sN), aces(ry * sN), aces(rz * sN)));
+}
+
+template <uint32_t N>
+cudaError_t launchRate(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
+    uint32_t* hitOut = f.capture ? c.hitIds : nullptr;
+    float* depthOut = f.capture ? c.depth : nullptr;
+    if (f.fpStrict)
+        intersectShadeKernel<N, false><<<c.tiles, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
+                                                                      c.tileRays, c.beams, c.tileLists, c.pool,
+                                                                      c.chunkNext, f.cameraToWorld, s.env, c.colors,
+                                                                      hitOut, depthOut);
+    else
+        intersectShadeKernel<N, true><<<c.tiles, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
+                                                                     c.tileRays, c.beams, c.tileLists, c.pool,
+                                                                     c.chunkNext, f.cameraToWorld, s.env, c.colors,
+                                                                     hitOut, depthOut);
+    return cudaGetLastError();
+}
+
+// RemapKernel (libraries/hvvr/raycaster/remap.cu:35-77) for split-colour 1, 2 (pentile) and 3
+__global__ void remapKernel(const uint32_t* __restrict__ src, const int32_t* __restrict__ remap,
+                            uint32_t* __restrict__ dst, uint32_t width, uint32_t height, uint64_t stride,
+                            uint32_t split) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= width || y >= height) return;
+    const size_t p = size_t(y) * width + x;
+    if (split == 1) {
+        const int32_t o = remap[p];
+        if (o >= 0) dst[size_t(y) * stride + x] = src[o];
+        return;
+    }
+    uint32_t cc[3] = {0, 0, 0};
+    for (uint32_t ch = 0; ch < split; ch++) {
+        const int32_t o = remap[p * split + ch];
+        if (o >= 0) cc[ch] = src[o];
+    }
+    dst[size_t(y) * stride + x] = split == 2
+                                      ? ((cc[1] & 0xffu) | (cc[0] & 0xff00u) | (cc[1] & 0xff0000u) | 0xff000000u)
+                                      : ((cc[0] & 0xffu) | (cc[1] & 0xff00u) | (cc[2] & 0xff0000u) | 0xff000000u);
+}
+
+} // namespace
+
+cudaError_t launchIntersectShade(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
+    if (c.tiles == 0) return cudaSuccess;
+    switch (c.msaa) {
+    case 1: return launchRate<1>(s, c, f, st);
+    case 2: return launchRate<2>(s, c, f, st);
+    case 4: return launchRate<4>(s, c, f, st);
+    case 8: return launchRate<8>(s, c, f, st);
+    case 16: return launchRate<16>(s, c, f, st);
+    case 32: return launchRate<32>(s, c, f, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchRemap(const CameraDev& c, cudaStream_t st) {
+    if (!c.image || c.width == 0 || c.height == 0) return cudaSuccess;
+    const dim3 block(16, 8);
+    const dim3 grid((c.width + 15) / 16, (c.height + 7) / 8);
+    remapKernel<<<grid, block, 0, st>>>(c.colors, c.remap, c.image, c.width, c.height, c.imageStride, c.split);
+    return cudaGetLastError();
+}
+
+cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st) {
+    int idx = -1;
+    switch (n) {
+    case 1: idx = 0; break;
+    case 2: idx = 1; break;
+    case 4: idx = 2; break;
+    case 8: idx = 3; break;
+    case 16: idx = 4; break;
+    case 32: idx = 5; break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaMemcpyToSymbolAsync(cMsaa, offsets, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
+                                   cudaMemcpyHostToDevice, st);
+}
+
+} // namespace hvb
