@@ -151,16 +151,18 @@ class Camera:
         d = _abi.ImageDesc()
         d.pixel_format = 0
         d.width, d.height, d.stride = width, height, stride
+        # the previous image stays alive until the library has released (unregistered) it
+        new = None
         if device_ptr is None:
-            self._target = np.zeros((height, stride or width), dtype=np.uint32)
+            new = np.zeros((height, stride or width), dtype=np.uint32)
             d.memory_type = HVVR_MEMORY_CPU
-            d.data = self._target.ctypes.data
+            d.data = new.ctypes.data
         else:
-            self._target = None
             d.memory_type = HVVR_MEMORY_CUDA
             d.data = device_ptr
-        self.width, self.height = width, height
         _check(_lib.hvvr_camera_set_render_target(self.handle, C.byref(d)))
+        self._target = new
+        self.width, self.height = width, height
 
     @property
     def image(self):
