@@ -79,6 +79,7 @@ _sig("hvvr_scene_read_nodes", _vp, _vp)
 _sig("hvvr_scene_read_triangles", _vp, _vp)
 _sig("hvvr_generate_topology", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32))
 _sig("hvvr_grid_samples", _u32, _u32, _vp)
+_sig("hvvr_tile_cull_static", _vp, _vp, _vp, C.c_uint64, _p(C.c_uint64), _vp)
 
 EXPORTED = [
     "hvvr_last_error", "hvvr_version", "hvvr_spec_default", "hvvr_raycaster_create", "hvvr_raycaster_destroy",
@@ -93,6 +94,7 @@ EXPORTED = [
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
     "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
+    "hvvr_tile_cull_static",
 ]
 
 

@@ -89,6 +89,13 @@ class Spec(C.Structure):
                 ("fp_mode", C.c_uint32), ("tri_index_capacity", C.c_uint64), ("device", C.c_int)]
 
 
+class TileCullArgs(C.Structure):
+    """hvvr_tile_cull_args: device inputs of hvvr_tile_cull_static."""
+    _fields_ = [("nodes", C.c_void_p), ("node_count", C.c_uint32), ("tile_rays", C.c_void_p),
+                ("tile_count", C.c_uint32), ("block_stacks", C.c_void_p), ("block_sizes", C.c_void_p),
+                ("camera_to_world", Transform)]
+
+
 # numpy layouts of the bulk arrays
 SAMPLE_DTYPE = np.dtype([("pixel", "<u4", 2), ("position", "<f4", 2), ("minor", "<f4", 2), ("major", "<f4")])
 VERTEX_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<u2", 4), ("uv", "<f4", 2), ("pad", "<u4")])

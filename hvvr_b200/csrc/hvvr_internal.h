@@ -125,6 +125,9 @@ struct FrameParams {
     uint32_t capture;
 };
 
+// records the message returned by hvvr_last_error() on this thread and returns code
+int setLastError(int code, const char* msg);
+
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
 cudaError_t launchBlockCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
 cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);

@@ -87,6 +87,11 @@ struct DevBuf {
 
 } // namespace
 
+int hvb::setLastError(int code, const char* msg) {
+    gLastError = msg ? msg : "";
+    return code;
+}
+
 struct hvvr_model {
     hvvr_raycaster* rc = nullptr;
     std::vector<hvvr_shading_vertex> verts;

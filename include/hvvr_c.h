@@ -244,6 +244,31 @@ int hvvr_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr
 /* getGridSamples(width, height) (libraries/hvvr/raycaster/samples.cpp:21-42) */
 int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
 
+/* ---------------------------------------------------------------- cull without device allocation
+ * No counterpart in the reference. For callers that may not call cudaMalloc: a render thread
+ * with a frame deadline (an allocation can synchronise the device), a plugin whose host
+ * application owns every device allocation, or code whose device memory all belongs to its own
+ * pool. The caller passes device inputs and outputs; the working memory for the per-tile lists
+ * is a fixed area compiled into the library (about 31 MiB, present on every GPU that loads the
+ * library until the process exits), so one call handles at most 65,536 tiles and 7,864,320
+ * list entries and rejects larger work with HVVR_ERR_INVALID / HVVR_ERR_OVERFLOW.
+ * Calls share that area: calls whose GPU work overlaps race and must be serialised by the caller.
+ * The first call on each device looks up the area's device address; make it before any stream
+ * capture begins. The call waits for its own work (stream sync) to report the status.
+ * Output: counts[tile_count] and, when total <= capacity, the lists concatenated in tile order
+ * in indices[] - the same lists as hvvr_camera_read_tile_lists for the same frame. */
+typedef struct {
+    const void* nodes;            /* device: node_count BVH nodes, 128-byte layout, refit bounds */
+    uint32_t node_count;
+    const void* tile_rays;        /* device: tile_count x {float origin[4][3]; float dir[4][3]}, camera space */
+    uint32_t tile_count;          /* positive multiple of 64; tile t belongs to block t/64 */
+    const void* block_stacks;     /* device: (tile_count/64) x 64 x {float tMin; uint32_t mask; uint32_t node} */
+    const uint32_t* block_sizes;  /* device: tile_count/64 sorted block-stack sizes */
+    hvvr_transform camera_to_world;
+} hvvr_tile_cull_args;
+int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* counts, uint32_t* indices, uint64_t capacity,
+                          uint64_t* total, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -908,6 +908,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     setupSamples(in, ss);
     if (out->remap) memcpy(out->remap, ss.remap.data(), ss.remap.size() * sizeof(int32_t));
     if (out->beams) memcpy(out->beams, ss.beams.data(), ss.beams.size() * sizeof(Beam));
+    if (out->tile_rays) memcpy(out->tile_rays, ss.tileRays.data(), ss.tileRays.size() * sizeof(Rays4));
 
     // per-frame transform (RC/render.cpp:282-365, RC/traversal.h:38-47); no cull planes on the plain path
     M4 c2w = transformToMatrix(in->cam_xf);

@@ -58,6 +58,7 @@ typedef struct {
     float* beams;              /* [padded*9] camera-space DirectionalBeam */
     void* nodes;               /* [node_count*128 bytes] refit BVH */
     float* tris;               /* [tri_count*9] PrecomputedTriangleIntersect */
+    float* tile_rays;          /* [tiles*24] camera-space corner rays {origin[4][3], dir[4][3]} */
     uint32_t status;           /* nonzero if a capacity was exceeded */
 } oracle_frame_out;
 

@@ -32,7 +32,7 @@ class FrameOut(C.Structure):
                 ("hit_ids", C.c_void_p), ("depth", C.c_void_p), ("depth64", C.c_void_p), ("gb_n", C.c_void_p),
                 ("gb_tri", C.c_void_p), ("gb_mask", C.c_void_p), ("colors", C.c_void_p), ("image", C.c_void_p),
                 ("remap", C.c_void_p), ("beams", C.c_void_p), ("nodes", C.c_void_p), ("tris", C.c_void_p),
-                ("status", C.c_uint32)]
+                ("tile_rays", C.c_void_p), ("status", C.c_uint32)]
 
 
 def layout(sample_count):
@@ -105,6 +105,8 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
         alloc("remap", height * width * split, np.int32, "remap")
     if "beams" in want:
         alloc("beams", (padded, 9), np.float32, "beams")
+    if "tile_rays" in want:
+        alloc("tile_rays", (tiles, 24), np.float32, "tile_rays")
     if "scene" in want:
         alloc("nodes", len(scene.nodes), _abi.NODE_DTYPE, "nodes")
         alloc("tris", (len(scene.tri_shade), 9), np.float32, "tris")
