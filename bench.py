@@ -113,6 +113,21 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def max_over_ranks(x, dist, device):
+    """Max of a float over all ranks (identity without a process group)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(samples_per_frame, frames, seconds, world):
+    """Whole-job Gsamples/s for replicas: every rank renders `frames` frames; seconds is the max over ranks."""
+    return world * samples_per_frame * frames / seconds / 1e9
+
+
 def stereo_setup(hv, scenes, sc, target_cuda, torch):
     rc = hv.Raycaster(tri_index_capacity=128 << 20)
     rc.create_model(sc)
@@ -280,13 +295,9 @@ def main():
     ck = clocks.stop()
     rc.synchronize()
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(frame_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(frame_ms), dist, "cuda")
     ms_per_step = total_ms / args.steps
-    value = world * samples_per_frame * args.steps / (total_ms * 1e-3) / 1e9
+    value = replica_throughput(samples_per_frame, args.steps, total_ms * 1e-3, world)
 
     # end to end through the C ABI: CPU_MEMORY targets, images copied to host every frame
     rc.close()
@@ -303,12 +314,8 @@ def main():
         for c, xf in zip(cams2, eyes):
             c.set_camera_to_world(xf)
         rc2.render()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * samples_per_frame * e2e_steps / e2e_s / 1e9
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e_value = replica_throughput(samples_per_frame, e2e_steps, e2e_s, world)
     rc2.close()
 
     peak, peak_kind = load_peaks()

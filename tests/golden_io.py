@@ -1,0 +1,28 @@
+"""Loads tests/golden/*.npz fixtures into scenes and camera parameters."""
+import ctypes as C
+import glob
+import os
+
+import numpy as np
+
+from hvvr_b200 import _abi, scenes
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+
+def load(name):
+    g = dict(np.load(os.path.join(GOLDEN_DIR, name + ".npz")))
+    lights = []
+    raw = g["lights"].tobytes()
+    for i in range(len(raw) // C.sizeof(_abi.LightUnion)):
+        lights.append(_abi.LightUnion.from_buffer_copy(raw[i * C.sizeof(_abi.LightUnion):(i + 1) * C.sizeof(_abi.LightUnion)]))
+    sc = scenes.Scene(g["topo_verts"].copy(), g["topo_tris"].copy(), g["materials"].copy(), lights)
+    sc.nodes = g["topo_nodes"].copy()
+    xf = _abi.Transform.from_buffer_copy(g["cam_xf"].tobytes())
+    vp = _abi.FloatRect.from_buffer_copy(g["viewport"].tobytes())
+    w, h, msaa = (int(v) for v in g["dims"])
+    return g, sc, g["samples"], xf, vp, w, h, msaa
