@@ -15,7 +15,7 @@ from ._abi import (HVVR_CAPTURE_HITS, HVVR_FP_FMA, HVVR_FP_STRICT, HVVR_MEMORY_C
                    HVVR_OK)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libhvvr_b200.so")
+LIB_PATH = os.environ.get("HVVR_B200_LIB") or os.path.join(_HERE, "_lib", "libhvvr_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("hvvr_b200: %s is not built; run `make -C hvvr_b200/csrc` (or __graft_entry__.build())" % LIB_PATH)

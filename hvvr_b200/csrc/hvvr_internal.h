@@ -111,7 +111,10 @@ struct CameraDev {
     uint32_t* pool = nullptr;          // [poolChunks * kChunk]
     uint32_t* chunkNext = nullptr;     // [poolChunks]
     uint32_t poolChunks = 0;
-    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2..3] spare
+    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2] tile queue head, [3] spare
+    uint32_t* tileCost = nullptr;      // [tiles] node visits of the last frame (scheduling only)
+    uint32_t* tileOrder = nullptr;     // [tiles] longest-first tile order built from tileCost
+    bool costValid = false;            // tileCost holds a previous frame's values
     uint32_t* colors = nullptr;        // [padded] RGBA8 per sorted sample
     uint32_t* hitIds = nullptr;        // [padded * msaa] when capturing
     float* depth = nullptr;            // [padded * msaa] when capturing

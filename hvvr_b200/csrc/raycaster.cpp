@@ -130,12 +130,16 @@ struct hvvr_camera {
     DevBuf<StackEntry> blockStacks;
     DevBuf<uint32_t> blockSizes;
     DevBuf<TileList> tileLists;
-    DevBuf<uint32_t> pool, chunkNext, counters, colors, hitIds, image;
+    DevBuf<uint32_t> pool, chunkNext, counters, colors, hitIds, image, tileCost, tileOrder;
     DevBuf<float> depth;
     uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
     void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
     cudaEvent_t ev[6] = {};
     float lastMs[6] = {};
+    // each camera renders on its own stream, forked from and joined back to the render stream,
+    // so the cameras of a frame (e.g. both eyes) overlap on the device
+    cudaStream_t stream = nullptr;
+    cudaEvent_t joinEv = nullptr;
 };
 
 struct hvvr_raycaster {
@@ -155,6 +159,7 @@ struct hvvr_raycaster {
     DevBuf<Mat4> modelToWorld;
     std::vector<Node> hostNodes;
     uint32_t refitStatus = 0;
+    cudaEvent_t forkEv = nullptr;
 };
 
 namespace {
@@ -362,6 +367,9 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     TRY(cam->tileLists.alloc(ss.tiles));
     TRY(cam->colors.alloc(ss.padded));
     TRY(cam->counters.alloc(4));
+    TRY(cam->tileCost.alloc(ss.tiles));
+    TRY(cam->tileOrder.alloc(ss.tiles));
+    cam->dev.costValid = false;
     if (!cam->hostCounters) CUDA_TRY(cudaMallocHost((void**)&cam->hostCounters, 4 * sizeof(uint32_t)));
     const uint64_t capEntries = cam->rc->spec.tri_index_capacity ? cam->rc->spec.tri_index_capacity : (128ull << 20);
     const uint64_t chunks = (capEntries + kChunk - 1) / kChunk;
@@ -391,6 +399,8 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     d.chunkNext = cam->chunkNext.p;
     d.poolChunks = uint32_t(chunks);
     d.counters = cam->counters.p;
+    d.tileCost = cam->tileCost.p;
+    d.tileOrder = cam->tileOrder.p;
     d.colors = cam->colors.p;
     if (cpuTarget) {
         d.image = cam->image.p;
@@ -401,12 +411,18 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     }
     if (!cam->ev[0])
         for (auto& e : cam->ev) CUDA_TRY(cudaEventCreate(&e));
+    if (!cam->stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&cam->stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&cam->joinEv, cudaEventDisableTiming));
+    }
     cam->setupDirty = false;
     return HVVR_OK;
 }
 
-int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t st) {
-    if (cam->setupDirty) TRY(setupCamera(cam, st));
+int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t parent) {
+    if (cam->setupDirty) TRY(setupCamera(cam, parent));
+    cudaStream_t st = cam->stream;
+    CUDA_TRY(cudaStreamWaitEvent(st, rc->forkEv, 0));
     CameraDev& d = cam->dev;
     d.msaa = cam->msaa;
     if (cam->capture & HVVR_CAPTURE_HITS) {
@@ -414,12 +430,6 @@ int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t st) {
         TRY(cam->depth.alloc(size_t(d.padded) * d.msaa));
         d.hitIds = cam->hitIds.p;
         d.depth = cam->depth.p;
-    }
-    if (!rc->msaaUploaded[d.msaa]) {
-        float off[64];
-        msaaOffsets(d.msaa, off);
-        CUDA_TRY(uploadMsaaTable(d.msaa, off, st));
-        rc->msaaUploaded[d.msaa] = true;
     }
     FrameParams f;
     f.cameraToWorld = transformToMatrix(cam->xf);
@@ -442,6 +452,9 @@ int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t st) {
                                    d.height, cudaMemcpyDeviceToHost, st));
     }
     CUDA_TRY(cudaEventRecord(cam->ev[5], st));
+    CUDA_TRY(cudaEventRecord(cam->joinEv, st));
+    CUDA_TRY(cudaStreamWaitEvent(parent, cam->joinEv, 0));
+    d.costValid = true; // the next frame schedules its tiles by this frame's visit counts
     cam->rendered = true;
     return HVVR_OK;
 }
@@ -511,12 +524,16 @@ int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out) {
 int hvvr_raycaster_destroy(hvvr_raycaster* rc) {
     if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
     cudaStreamSynchronize(rc->stream);
+    cudaDeviceSynchronize();
     for (auto& c : rc->cameras) {
         unregisterTarget(c.get());
         if (c->hostCounters) cudaFreeHost(c->hostCounters);
         for (auto& e : c->ev)
             if (e) cudaEventDestroy(e);
+        if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->joinEv) cudaEventDestroy(c->joinEv);
     }
+    if (rc->forkEv) cudaEventDestroy(rc->forkEv);
     cudaStreamDestroy(rc->stream);
     delete rc;
     return HVVR_OK;
@@ -543,6 +560,17 @@ int hvvr_raycaster_render(hvvr_raycaster* rc, double elapsed_time, void* stream)
         CUDA_TRY(launchRefit(rc->scene, st));
         rc->refitDirty = false;
     }
+    for (auto& c : rc->cameras) {
+        if (!c->enabled || c->samples.empty()) continue;
+        if (!rc->msaaUploaded[c->msaa]) {
+            float off[64];
+            msaaOffsets(c->msaa, off);
+            CUDA_TRY(uploadMsaaTable(c->msaa, off, st));
+            rc->msaaUploaded[c->msaa] = true;
+        }
+    }
+    if (!rc->forkEv) CUDA_TRY(cudaEventCreateWithFlags(&rc->forkEv, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(rc->forkEv, st));
     bool cpuTargets = false;
     for (auto& c : rc->cameras) {
         if (!c->enabled || c->samples.empty()) continue;
@@ -672,11 +700,13 @@ int hvvr_camera_destroy(hvvr_raycaster* rc, hvvr_camera* cam) {
     if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
     for (auto it = rc->cameras.begin(); it != rc->cameras.end(); ++it) {
         if (it->get() == cam) {
-            cudaStreamSynchronize(rc->stream);
+            cudaDeviceSynchronize();
             unregisterTarget(cam);
             if (cam->hostCounters) cudaFreeHost(cam->hostCounters);
             for (auto& e : cam->ev)
                 if (e) cudaEventDestroy(e);
+            if (cam->stream) cudaStreamDestroy(cam->stream);
+            if (cam->joinEv) cudaEventDestroy(cam->joinEv);
             rc->cameras.erase(it);
             return HVVR_OK;
         }
@@ -739,7 +769,7 @@ int hvvr_camera_set_render_target(hvvr_camera* cam, const hvvr_image_desc* targe
         return fail(HVVR_ERR_INVALID, "render target must be CPU or CUDA memory (no graphics API here)");
     if (target->pixel_format != HVVR_PIXEL_RGBA8_SRGB) return fail(HVVR_ERR_INVALID, "pixel format must be RGBA8 sRGB");
     if (target->stride && target->stride < target->width) return fail(HVVR_ERR_INVALID, "stride < width");
-    cudaStreamSynchronize(cam->rc->stream);
+    cudaDeviceSynchronize();
     unregisterTarget(cam);
     cam->target = *target;
     if (target->memory_type == HVVR_MEMORY_CPU && target->data && target->width && target->height) {

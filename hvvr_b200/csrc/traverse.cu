@@ -16,6 +16,8 @@
 // fold the per-lane results into the reference's 4-bit child masks, so the arithmetic per
 // test is exactly the reference's lane arithmetic (explicit fmaf where it uses
 // _mm256_fmadd_ps, IEEE single ops elsewhere) and the stacks evolve identically.
+#include <algorithm>
+
 #include "dev_common.cuh"
 
 namespace hvb {
@@ -33,9 +35,15 @@ struct SmemFrustum {
     int degenerate;
 };
 
+// Lane layout (child-major): lane l serves child c = l >> 3 and test slot j = l & 7. Slots
+// 0-3 are the four frustum planes, 4-6 the x/y/z projection overlaps, 7 always passes; so
+// child c passes testBVHNodeChildren when byte c of the ballot is 0xFF. For the refine, slot j
+// tests edge axis j and, for j < 4, also edge axis 8 + j; child c is rejected when byte c of
+// that ballot is nonzero.
 struct LaneTest {
-    float c0, c1, c2, c3, c4, c5, c6;  // plane lanes: lo xyz, hi xyz, w; projection lanes: max, -min
-    bool always;                       // projection lanes 28-31 (no axis)
+    float c0, c1, c2, c3, c4, c5, c6; // plane slots: lo xyz, hi xyz, w; projection slots: c0 = max side, c1 = -min side
+    int kind;                         // 0 plane, 1 projection, 2 always pass
+    int axis;                         // projection axis
     float e0x, e0y, e0z, mn0, mx0;
     float e1x, e1y, e1z, mn1, mx1;
     bool has1;
@@ -137,24 +145,26 @@ __device__ void buildFrustum(const Rays4& cr, const Mat4& M, SmemFrustum& f) {
 __device__ LaneTest loadLaneTest(const SmemFrustum& f) {
     LaneTest t;
     const uint32_t lane = laneId();
-    if (lane < 16) {
-        const int p = int(lane >> 2);
-        t.c0 = f.tpLo[p][0]; t.c1 = f.tpLo[p][1]; t.c2 = f.tpLo[p][2];
-        t.c3 = f.tpHi[p][0]; t.c4 = f.tpHi[p][1]; t.c5 = f.tpHi[p][2];
-        t.c6 = f.w[p];
-        t.always = false;
+    const int c = int(lane >> 3), j = int(lane & 7);
+    t.c0 = t.c1 = t.c2 = t.c3 = t.c4 = t.c5 = t.c6 = 0.0f;
+    t.axis = 0;
+    if (j < 4) {
+        t.kind = 0;
+        t.c0 = f.tpLo[j][0]; t.c1 = f.tpLo[j][1]; t.c2 = f.tpLo[j][2];
+        t.c3 = f.tpHi[j][0]; t.c4 = f.tpHi[j][1]; t.c5 = f.tpHi[j][2];
+        t.c6 = f.w[j];
+    } else if (j < 7) {
+        t.kind = 1;
+        t.axis = j - 4;
+        t.c0 = f.proj[j - 4][c];
+        t.c1 = f.proj[j - 4][4 + c];
     } else {
-        const int a = int(lane - 16) >> 2, c = int(lane & 3);
-        t.always = (a == 3);
-        t.c0 = a < 3 ? f.proj[a][c] : 0.0f;
-        t.c1 = a < 3 ? f.proj[a][4 + c] : 0.0f;
-        t.c2 = t.c3 = t.c4 = t.c5 = t.c6 = 0.0f;
+        t.kind = 2;
     }
-    const int e0 = int(lane >> 2);
-    t.e0x = f.edge[e0][0]; t.e0y = f.edge[e0][1]; t.e0z = f.edge[e0][2];
-    t.mn0 = f.minF[e0]; t.mx0 = f.maxF[e0];
-    t.has1 = lane < 16;
-    const int e1 = t.has1 ? 8 + int(lane >> 2) : e0;
+    t.e0x = f.edge[j][0]; t.e0y = f.edge[j][1]; t.e0z = f.edge[j][2];
+    t.mn0 = f.minF[j]; t.mx0 = f.maxF[j];
+    t.has1 = j < 4;
+    const int e1 = t.has1 ? 8 + j : j;
     t.e1x = f.edge[e1][0]; t.e1y = f.edge[e1][1]; t.e1z = f.edge[e1][2];
     t.mn1 = f.minF[e1]; t.mx1 = f.maxF[e1];
     return t;
@@ -165,7 +175,7 @@ struct ChildBox {
 };
 
 __device__ __forceinline__ ChildBox childBox(float v) {
-    const uint32_t c = laneId() & 3u;
+    const uint32_t c = laneId() >> 3;
     ChildBox b;
     b.xM = __shfl_sync(kFull, v, c);
     b.xN = __shfl_sync(kFull, v, 4 + c);
@@ -176,22 +186,26 @@ __device__ __forceinline__ ChildBox childBox(float v) {
     return b;
 }
 
+// bit c set where byte c of m is all ones / nonzero
+__device__ __forceinline__ uint32_t bytesAllOnes(uint32_t m) {
+    const uint32_t x = __vcmpeq4(m, 0xffffffffu);
+    return ((x >> 7) & 1u) | ((x >> 14) & 2u) | ((x >> 21) & 4u) | ((x >> 28) & 8u);
+}
+__device__ __forceinline__ uint32_t bytesNonZero(uint32_t m) {
+    const uint32_t x = __vcmpne4(m, 0u);
+    return ((x >> 7) & 1u) | ((x >> 14) & 2u) | ((x >> 21) & 4u) | ((x >> 28) & 8u);
+}
+
 // Frustum::testBVHNodeChildren (traverse_avx.h:104-164)
 __device__ __forceinline__ uint32_t testChildren(const ChildBox& b, const LaneTest& t) {
-    const uint32_t lane = laneId();
-    bool pass;
-    if (lane < 16) {
-        const float lo = fmaf(t.c0, b.xM, fmaf(t.c1, b.yM, t.c2 * b.zM));
-        const float hi = fmaf(t.c3, b.xN, fmaf(t.c4, b.yN, t.c5 * b.zN));
-        pass = (lo + hi) <= t.c6;
-    } else {
-        const int a = int(lane - 16) >> 2;
-        const float am = a == 0 ? b.xM : (a == 1 ? b.yM : b.zM);
-        const float an = a == 0 ? b.xN : (a == 1 ? b.yN : b.zN);
-        pass = t.always || (am >= t.c0 && an >= t.c1);
-    }
-    const uint32_t m = __ballot_sync(kFull, pass);
-    return (m & (m >> 4) & (m >> 8) & (m >> 12) & (m >> 16) & (m >> 20) & (m >> 24) & (m >> 28)) & 0xfu;
+    const float lo = fmaf(t.c0, b.xM, fmaf(t.c1, b.yM, t.c2 * b.zM));
+    const float hi = fmaf(t.c3, b.xN, fmaf(t.c4, b.yN, t.c5 * b.zN));
+    const bool planePass = (lo + hi) <= t.c6;
+    const float am = t.axis == 0 ? b.xM : (t.axis == 1 ? b.yM : b.zM);
+    const float an = t.axis == 0 ? b.xN : (t.axis == 1 ? b.yN : b.zN);
+    const bool projPass = (am >= t.c0) && (an >= t.c1);
+    const bool pass = t.kind == 0 ? planePass : (t.kind == 1 ? projPass : true);
+    return bytesAllOnes(__ballot_sync(kFull, pass));
 }
 
 __device__ __forceinline__ bool edgeReject(const ChildBox& b, float ex, float ey, float ez, float mn, float mx) {
@@ -206,10 +220,9 @@ __device__ __forceinline__ bool edgeReject(const ChildBox& b, float ex, float ey
 
 // Frustum::testBVHNodeChildrenRefine (traverse_avx.h:166-217): mask of rejected children
 __device__ __forceinline__ uint32_t refineReject(const ChildBox& b, const LaneTest& t) {
-    bool rej = edgeReject(b, t.e0x, t.e0y, t.e0z, t.mn0, t.mx0);
-    if (t.has1) rej = rej || edgeReject(b, t.e1x, t.e1y, t.e1z, t.mn1, t.mx1);
-    const uint32_t m = __ballot_sync(kFull, rej);
-    return (m | (m >> 4) | (m >> 8) | (m >> 12) | (m >> 16) | (m >> 20) | (m >> 24) | (m >> 28)) & 0xfu;
+    const bool rej0 = edgeReject(b, t.e0x, t.e0y, t.e0z, t.mn0, t.mx0);
+    const bool rej1 = edgeReject(b, t.e1x, t.e1y, t.e1z, t.mn1, t.mx1);
+    return bytesNonZero(__ballot_sync(kFull, rej0 || (t.has1 && rej1)));
 }
 
 // Number of consecutive stack entries, from position top-1 downwards, for which pred holds.
@@ -328,7 +341,7 @@ __global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(const Node* 
     if (lane == 0) sizes[blk] = stackSize;
 }
 
-constexpr int kTileWarps = 8;
+constexpr int kTileWarps = 4;
 
 struct TileSmem {
     SmemFrustum f;
@@ -368,45 +381,71 @@ struct Emitter {
         __syncwarp();
     }
 
-    __device__ void emitRange(uint32_t* buf, uint32_t t0, uint32_t t1) {
-        if (t1 <= t0) {
-            if (laneId() == 0) atomicOr(&counters[1], kStatusBadLeaf);
-            return;
+    // Appends the triangle ranges of the passing leaf slots of one node, in slot order. v holds
+    // word l of the node in lane l; leaf slot k covers [tri[k], tri[k+1]) = words 25+k, 26+k.
+    __device__ void emitLeaves(uint32_t* buf, float v, uint32_t leaf) {
+        uint32_t start[4], len[4], pre[4], n = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t t0 = __float_as_uint(__shfl_sync(kFull, v, 25 + k));
+            const uint32_t t1 = __float_as_uint(__shfl_sync(kFull, v, 26 + k));
+            const bool on = (leaf >> k) & 1u;
+            if (on && t1 <= t0 && laneId() == 0) atomicOr(&counters[1], kStatusBadLeaf);
+            start[k] = t0;
+            len[k] = (on && t1 > t0) ? t1 - t0 : 0u;
+            pre[k] = n;
+            n += len[k];
         }
-        uint32_t n = t1 - t0;
-        while (n && !dead) {
-            const uint32_t m = min(n, kChunk - bufCount);
-            for (uint32_t j = laneId(); j < m; j += 32) buf[bufCount + j] = t0 + j;
+        uint32_t done = 0;
+        while (done < n && !dead) {
+            const uint32_t m = min(n - done, kChunk - bufCount);
+            for (uint32_t j = laneId(); j < m; j += 32) {
+                const uint32_t p = done + j;
+                // the last non-empty slot whose range starts at or before p
+                uint32_t kk = 0;
+#pragma unroll
+                for (uint32_t q = 1; q < 4; q++)
+                    if (len[q] && p >= pre[q]) kk = q;
+                buf[bufCount + j] = start[kk] + (p - pre[kk]);
+            }
             bufCount += m;
-            t0 += m;
-            n -= m;
+            done += m;
             total += m;
             if (bufCount == kChunk) flush(buf);
         }
     }
+
 };
 
-__global__ void __launch_bounds__(kTileWarps * 32) tileCullKernel(const Node* __restrict__ nodes,
-                                                                  const Rays4* __restrict__ tileRays, uint32_t tiles,
-                                                                  Mat4 M, const StackEntry* __restrict__ blockStacks,
-                                                                  const uint32_t* __restrict__ blockSizes,
-                                                                  TileList* __restrict__ lists, uint32_t* pool,
-                                                                  uint32_t* chunkNext, uint32_t poolChunks,
-                                                                  uint32_t* counters) {
-    __shared__ TileSmem smem[kTileWarps];
-    const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-    const uint32_t tile = blockIdx.x * kTileWarps + warp;
-    if (tile >= tiles) return;
-    TileSmem& s = smem[warp];
+struct TileCullArgs {
+    const Node* nodes;
+    const Rays4* tileRays;
+    uint32_t tiles;
+    Mat4 M;
+    const StackEntry* blockStacks;
+    const uint32_t* blockSizes;
+    TileList* lists;
+    uint32_t* pool;
+    uint32_t* chunkNext;
+    uint32_t poolChunks;
+    uint32_t* counters;   // [0] chunk allocator, [1] status, [2] work-queue head
+    const uint32_t* order; // tile order for the queue (nullptr = natural order)
+    uint32_t* cost;       // node visits per tile, written for next frame's order (may be nullptr)
+};
+
+// traverseTiles for one tile; returns the number of node visits
+__device__ uint32_t cullTile(const TileCullArgs& a, uint32_t tile, TileSmem& s) {
+    const uint32_t lane = laneId();
+    const Node* __restrict__ nodes = a.nodes;
     const uint32_t blk = tile / kTilesPerBlock;
-    const uint32_t stackSize = blockSizes[blk];
-    buildFrustum(tileRays[tile], M, s.f);
+    const uint32_t stackSize = a.blockSizes[blk];
+    buildFrustum(a.tileRays[tile], a.M, s.f);
     if (stackSize == 0 || s.f.degenerate) {
-        if (lane == 0) lists[tile] = TileList{kNoChunk, 0};
-        return;
+        if (lane == 0) a.lists[tile] = TileList{kNoChunk, 0};
+        return 0;
     }
     for (uint32_t i = lane; i < stackSize; i += 32) {
-        const StackEntry e = blockStacks[size_t(blk) * kBlockStack + i];
+        const StackEntry e = a.blockStacks[size_t(blk) * kBlockStack + i];
         s.tMin[i] = e.tMin;
         s.mask[i] = e.mask;
         s.node[i] = e.node;
@@ -414,71 +453,184 @@ __global__ void __launch_bounds__(kTileWarps * 32) tileCullKernel(const Node* __
     __syncwarp();
     const LaneTest t = loadLaneTest(s.f);
     const int distIdx = s.f.distIdx;
-    Emitter em{pool, chunkNext, poolChunks, counters, kNoChunk, kNoChunk, 0, 0, 0, false};
+    Emitter em{a.pool, a.chunkNext, a.poolChunks, a.counters, kNoChunk, kNoChunk, 0, 0, 0, false};
     uint32_t top = stackSize - 1;
     uint32_t node = s.node[top];
+    uint32_t visits = 0;
+    const float* rows = reinterpret_cast<const float*>(nodes);
+    float v = rows[size_t(node) * 32 + lane];
     for (;;) {
-        const float v = reinterpret_cast<const float*>(nodes + node)[lane];
+        ++visits;
+        // The next visit is always one of this node's internal children or the stack entry
+        // below the current one (a pop, or a push whose children all sort below it), so their
+        // rows are loaded now and consumed at the end of the visit, hiding the load latency.
+        const uint32_t leafMask = __float_as_uint(__shfl_sync(kFull, v, 24));
+        uint32_t childNode[4];
+        float vc[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            childNode[k] = node + __float_as_uint(__shfl_sync(kFull, v, 26 + k));
+            vc[k] = ((leafMask >> k) & 1u) ? 0.0f : rows[size_t(childNode[k]) * 32 + lane];
+        }
+        const bool hasPop = top > 0;
+        const uint32_t popNode = hasPop ? s.node[top - 1] : 0u;
+        const float vp = hasPop ? rows[size_t(popNode) * 32 + lane] : 0.0f;
         const ChildBox cb = childBox(v);
         uint32_t mask = testChildren(cb, t);
         bool descend = false;
         if (mask) {
-            const uint32_t leafMask = __float_as_uint(__shfl_sync(kFull, v, 24));
             uint32_t leaf = mask & leafMask;
             if (leaf) {
                 mask &= ~refineReject(cb, t);
                 leaf = mask & leafMask;
-                while (leaf && !em.dead) {
-                    const int k = __ffs(leaf) - 1;
-                    const uint32_t t0 = __float_as_uint(__shfl_sync(kFull, v, 25 + k));
-                    const uint32_t t1 = __float_as_uint(__shfl_sync(kFull, v, 26 + k));
-                    em.emitRange(s.buf, t0, t1);
-                    leaf &= leaf - 1;
-                }
+                if (leaf) em.emitLeaves(s.buf, v, leaf);
                 if (em.dead) break;
             }
             mask &= ~leafMask;
             if (mask && s.mask[top] == 0u) {
                 int k = __ffs(mask) - 1;
                 if (!(mask & (mask - 1))) {
-                    node = node + __float_as_uint(__shfl_sync(kFull, v, 26 + k));
+                    node = childNode[k];
+                    v = vc[0];
+#pragma unroll
+                    for (int q = 1; q < 4; q++)
+                        if (q == k) v = vc[q];
                     continue;
                 }
-                bool first = true;
-                bool overflow = false;
-                while (mask) {
-                    if (!first) ++top;
-                    first = false;
-                    if (top + 1 >= kTileStack) { overflow = true; break; }
-                    k = __ffs(mask) - 1;
-                    const float tm = __uint_as_float(__float_as_uint(__shfl_sync(kFull, v, distIdx * 4 + k)) ^ 0x80000000u);
-                    const uint32_t child = node + __float_as_uint(__shfl_sync(kFull, v, 26 + k));
-                    const float tmz = dazf(tm);
-                    const uint32_t n = shiftCount(top, [&](uint32_t p) { return dazf(s.tMin[p]) < tmz; });
-                    shiftUp(s.tMin, s.mask, s.node, top, n);
-                    if (lane == 0) { s.tMin[top - n] = tm; s.mask[top - n] = 0u; s.node[top - n] = child; }
-                    __syncwarp();
-                    mask &= mask - 1;
-                }
-                if (overflow) {
-                    if (lane == 0) atomicOr(&counters[1], kStatusStackOverflow);
+                // Insert all m >= 2 children at once. Keys are never NaN (a child that passes the
+                // plane test has finite bounds), so the stack stays sorted, non-increasing from
+                // bottom to top under the DAZ comparison, and the reference's one-at-a-time
+                // insertion (shift entries with a smaller key up, place the child, newest above
+                // equal keys) is equivalent to: an old entry moves up by the number of children
+                // with a larger key; child i lands at
+                //   top - #{old < key_i} + #{children with a larger key}
+                //       + #{earlier children with an equal key}.
+                const uint32_t m = __popc(mask);
+                if (top + m >= kTileStack) {
+                    if (lane == 0) atomicOr(&a.counters[1], kStatusStackOverflow);
                     break;
                 }
+                float ck[4], ckz[4];
+                uint32_t cnode[4];
+                float maxKey = -INFINITY;
+                {
+                    uint32_t mm = mask;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int kk = mm ? __ffs(mm) - 1 : 0;
+                        ck[i] = __uint_as_float(__float_as_uint(__shfl_sync(kFull, v, distIdx * 4 + kk)) ^ 0x80000000u);
+                        ckz[i] = dazf(ck[i]);
+                        cnode[i] = childNode[kk];
+                        if (mm) maxKey = fmaxf(maxKey, ckz[i]);
+                        mm &= mm - 1;
+                    }
+                }
+                // old entries that move: those with a key below the largest child key (a top run)
+                const uint32_t region = shiftCount(top, [&](uint32_t p) { return dazf(s.tMin[p]) < maxKey; });
+                uint32_t less[4] = {0u, 0u, 0u, 0u};
+                for (uint32_t base = 0; base < region; base += 32) {
+                    const uint32_t j = base + lane;
+                    const bool act = j < region;
+                    const uint32_t p = act ? top - 1 - j : 0u;
+                    float e = 0.0f, ez = 0.0f;
+                    uint32_t em_ = 0, en = 0;
+                    if (act) { e = s.tMin[p]; em_ = s.mask[p]; en = s.node[p]; ez = dazf(e); }
+                    uint32_t d = 0;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const bool valid = uint32_t(i) < m;
+                        d += (act && valid && ckz[i] > ez) ? 1u : 0u;
+                        less[i] += __popc(__ballot_sync(kFull, act && valid && ez < ckz[i]));
+                    }
+                    __syncwarp();
+                    if (act && d) { s.tMin[p + d] = e; s.mask[p + d] = em_; s.node[p + d] = en; }
+                    __syncwarp();
+                }
+                if (lane < m) {
+                    uint32_t pos = top - less[0];
+                    float mine = ckz[0];
+                    float rawk = ck[0];
+                    uint32_t nd = cnode[0];
+#pragma unroll
+                    for (int i = 1; i < 4; i++)
+                        if (uint32_t(i) == lane) { pos = top - less[i]; mine = ckz[i]; rawk = ck[i]; nd = cnode[i]; }
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        if (uint32_t(i) >= m || uint32_t(i) == lane) continue;
+                        if (ckz[i] > mine || (ckz[i] == mine && uint32_t(i) < lane)) pos++;
+                    }
+                    s.tMin[pos] = rawk;
+                    s.mask[pos] = 0u;
+                    s.node[pos] = nd;
+                }
+                __syncwarp();
+                top += m - 1;
                 descend = true;
             }
         }
         if (descend) {
-            node = s.node[top];
+            const uint32_t next = s.node[top];
+            float nv = vp;
+            bool have = hasPop && (next == popNode);
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (!have && next == childNode[q] && !((leafMask >> q) & 1u)) { nv = vc[q]; have = true; }
+            node = next;
+            v = have ? nv : rows[size_t(node) * 32 + lane];
             continue;
         }
         if (top == 0) break;
         --top;
-        node = s.node[top];
+        node = popNode;
+        v = vp;
     }
     if (!em.dead && em.bufCount) em.flush(s.buf);
     if (lane == 0) {
-        if (em.prev != kNoChunk) chunkNext[em.prev] = kNoChunk;
-        lists[tile] = TileList{em.first, em.dead ? em.stored : em.total};
+        if (em.prev != kNoChunk) a.chunkNext[em.prev] = kNoChunk;
+        a.lists[tile] = TileList{em.first, em.dead ? em.stored : em.total};
+    }
+    return visits;
+}
+
+// Persistent warps pull tiles from a queue (longest-first when an order is given), so a
+// few long horizon tiles overlap with the rest instead of holding a CTA slot each.
+__global__ void __launch_bounds__(kTileWarps * 32) tileCullKernel(TileCullArgs a) {
+    __shared__ TileSmem smem[kTileWarps];
+    const uint32_t warp = threadIdx.x >> 5, lane = laneId();
+    TileSmem& s = smem[warp];
+    for (;;) {
+        uint32_t w = 0;
+        if (lane == 0) w = atomicAdd(&a.counters[2], 1u);
+        w = __shfl_sync(kFull, w, 0);
+        if (w >= a.tiles) return;
+        const uint32_t tile = a.order ? a.order[w] : w;
+        __syncwarp();
+        const uint32_t visits = cullTile(a, tile, s);
+        if (a.cost && lane == 0) a.cost[tile] = visits;
+        __syncwarp();
+    }
+}
+
+// Orders tiles by descending cost (log2 buckets of last frame's visit counts); one block.
+__global__ void __launch_bounds__(1024) tileOrderKernel(const uint32_t* __restrict__ cost, uint32_t tiles,
+                                                        uint32_t* __restrict__ order) {
+    __shared__ uint32_t hist[33];
+    __shared__ uint32_t start[33];
+    if (threadIdx.x < 33) hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) atomicAdd(&hist[32 - __clz(cost[t] + 1u)], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int b = 32; b >= 0; b--) {
+            start[b] = run;
+            run += hist[b];
+        }
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) {
+        const uint32_t pos = atomicAdd(&start[32 - __clz(cost[t] + 1u)], 1u);
+        order[pos] = t;
     }
 }
 
@@ -494,10 +646,23 @@ cudaError_t launchBlockCull(const SceneDev& s, const CameraDev& c, const FramePa
 
 cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
     if (c.tiles == 0) return cudaSuccess;
-    const uint32_t grid = (c.tiles + kTileWarps - 1) / kTileWarps;
-    tileCullKernel<<<grid, kTileWarps * 32, 0, st>>>(s.nodes, c.tileRays, c.tiles, f.cameraToWorld, c.blockStacks,
-                                                      c.blockSizes, c.tileLists, c.pool, c.chunkNext, c.poolChunks,
-                                                      c.counters);
+    static int ctasPerSm = 0, sms = 0;
+    if (!ctasPerSm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctasPerSm, tileCullKernel, kTileWarps * 32, 0);
+        if (ctasPerSm < 1) ctasPerSm = 1;
+        if (sms < 1) sms = 1;
+    }
+    if (c.tileOrder && c.tileCost && c.costValid) {
+        tileOrderKernel<<<1, 1024, 0, st>>>(c.tileCost, c.tiles, c.tileOrder);
+    }
+    TileCullArgs a{s.nodes, c.tileRays, c.tiles, f.cameraToWorld, c.blockStacks, c.blockSizes, c.tileLists, c.pool,
+                   c.chunkNext, c.poolChunks, c.counters, c.costValid ? c.tileOrder : nullptr, c.tileCost};
+    const uint32_t needed = (c.tiles + kTileWarps - 1) / kTileWarps;
+    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(sms * ctasPerSm));
+    tileCullKernel<<<grid, kTileWarps * 32, 0, st>>>(a);
     return cudaGetLastError();
 }
 
