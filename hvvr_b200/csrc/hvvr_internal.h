@@ -111,7 +111,7 @@ struct CameraDev {
     uint32_t* pool = nullptr;          // [poolChunks * kChunk]
     uint32_t* chunkNext = nullptr;     // [poolChunks]
     uint32_t poolChunks = 0;
-    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2] tile queue head, [3] spare
+    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2], [3] tile queue heads
     uint32_t* tileCost = nullptr;      // [tiles] node visits of the last frame (scheduling only)
     uint32_t* tileOrder = nullptr;     // [tiles] longest-first tile order built from tileCost
     bool costValid = false;            // tileCost holds a previous frame's values
@@ -133,8 +133,17 @@ int setLastError(int code, const char* msg);
 
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
 cudaError_t launchBlockCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
+// whole-camera tile cull (longest-first when c.costValid) on queue counters[2]
 cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
+// c.tileOrder <- tiles sorted by descending c.tileCost (log2 buckets)
+cudaError_t launchTileOrder(const CameraDev& c, cudaStream_t st);
+// tile cull / intersect of the tiles order[first, first + count) (order == nullptr: tiles 0..count-1);
+// concurrent tile-cull launches of one camera need distinct zeroed queue heads
+cudaError_t launchTileCullRange(const SceneDev& s, const CameraDev& c, const FrameParams& f, const uint32_t* order,
+                                uint32_t first, uint32_t count, uint32_t* queue, cudaStream_t st);
 cudaError_t launchIntersectShade(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
+cudaError_t launchIntersectShadeRange(const SceneDev& s, const CameraDev& c, const FrameParams& f,
+                                      const uint32_t* order, uint32_t first, uint32_t count, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
 cudaError_t launchRefit(const SceneDev& s, cudaStream_t st);
 cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);

@@ -140,6 +140,11 @@ struct hvvr_camera {
     // so the cameras of a frame (e.g. both eyes) overlap on the device
     cudaStream_t stream = nullptr;
     cudaEvent_t joinEv = nullptr;
+    // from the second frame on, the tiles that were slowest to traverse last frame are culled
+    // and shaded on a high-priority side stream, while the rest are culled and shaded on
+    // `stream`; the long traversals of the few heavy tiles then overlap with shading work
+    cudaStream_t heavyStream = nullptr;
+    cudaEvent_t orderEv = nullptr, heavyEv = nullptr;
 };
 
 struct hvvr_raycaster {
@@ -414,9 +419,27 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     if (!cam->stream) {
         CUDA_TRY(cudaStreamCreateWithFlags(&cam->stream, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&cam->joinEv, cudaEventDisableTiming));
+        int leastPriority = 0, greatestPriority = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+        CUDA_TRY(cudaStreamCreateWithPriority(&cam->heavyStream, cudaStreamNonBlocking, greatestPriority));
+        CUDA_TRY(cudaEventCreateWithFlags(&cam->orderEv, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&cam->heavyEv, cudaEventDisableTiming));
     }
     cam->setupDirty = false;
     return HVVR_OK;
+}
+
+// cameras with fewer tiles run one tile-cull launch
+constexpr uint32_t kSplitMinTiles = 32;
+// heavy share of the tiles (1/8 was fastest on the 1M-triangle stereo 2x1080x1200 frame;
+// 1/4 and 1/16 within 1%, no split 4.5% slower)
+constexpr uint32_t kHeavyDiv = 8;
+
+// Number of heavy tiles split off to the side stream (0: one tile-cull launch for the whole
+// camera). Needs last frame's per-tile visit counts.
+uint32_t heavyTiles(const CameraDev& d) {
+    if (!d.costValid || d.tiles < kSplitMinTiles) return 0;
+    return std::max<uint32_t>(1u, d.tiles / kHeavyDiv);
 }
 
 int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t parent) {
@@ -439,9 +462,24 @@ int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t parent) {
     CUDA_TRY(cudaMemsetAsync(d.counters, 0, 4 * sizeof(uint32_t), st));
     CUDA_TRY(launchBlockCull(rc->scene, d, f, st));
     CUDA_TRY(cudaEventRecord(cam->ev[1], st));
-    CUDA_TRY(launchTileCull(rc->scene, d, f, st));
-    CUDA_TRY(cudaEventRecord(cam->ev[2], st));
-    CUDA_TRY(launchIntersectShade(rc->scene, d, f, st));
+    const uint32_t heavy = heavyTiles(d);
+    if (heavy) {
+        // tileOrder[0, heavy) are last frame's slowest tiles; each set gets its own queue head
+        CUDA_TRY(launchTileOrder(d, st));
+        CUDA_TRY(cudaEventRecord(cam->orderEv, st));
+        CUDA_TRY(cudaStreamWaitEvent(cam->heavyStream, cam->orderEv, 0));
+        CUDA_TRY(launchTileCullRange(rc->scene, d, f, d.tileOrder, 0, heavy, &d.counters[2], cam->heavyStream));
+        CUDA_TRY(launchIntersectShadeRange(rc->scene, d, f, d.tileOrder, 0, heavy, cam->heavyStream));
+        CUDA_TRY(cudaEventRecord(cam->heavyEv, cam->heavyStream));
+        CUDA_TRY(launchTileCullRange(rc->scene, d, f, d.tileOrder, heavy, d.tiles - heavy, &d.counters[3], st));
+        CUDA_TRY(cudaEventRecord(cam->ev[2], st));
+        CUDA_TRY(launchIntersectShadeRange(rc->scene, d, f, d.tileOrder, heavy, d.tiles - heavy, st));
+        CUDA_TRY(cudaStreamWaitEvent(st, cam->heavyEv, 0));
+    } else {
+        CUDA_TRY(launchTileCull(rc->scene, d, f, st));
+        CUDA_TRY(cudaEventRecord(cam->ev[2], st));
+        CUDA_TRY(launchIntersectShade(rc->scene, d, f, st));
+    }
     CUDA_TRY(cudaEventRecord(cam->ev[3], st));
     CUDA_TRY(launchRemap(d, st));
     CUDA_TRY(cudaEventRecord(cam->ev[4], st));
@@ -466,6 +504,18 @@ void unregisterTarget(hvvr_camera* cam) {
         cudaHostUnregister(cam->registered);
         cam->registered = nullptr;
     }
+}
+
+// frees the camera's pinned memory, streams and events (the device must be idle)
+void releaseCamera(hvvr_camera* cam) {
+    unregisterTarget(cam);
+    if (cam->hostCounters) cudaFreeHost(cam->hostCounters);
+    for (auto& e : cam->ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {cam->joinEv, cam->orderEv, cam->heavyEv})
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t t : {cam->stream, cam->heavyStream})
+        if (t) cudaStreamDestroy(t);
 }
 
 int checkStatus(hvvr_raycaster* rc) {
@@ -525,14 +575,7 @@ int hvvr_raycaster_destroy(hvvr_raycaster* rc) {
     if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
     cudaStreamSynchronize(rc->stream);
     cudaDeviceSynchronize();
-    for (auto& c : rc->cameras) {
-        unregisterTarget(c.get());
-        if (c->hostCounters) cudaFreeHost(c->hostCounters);
-        for (auto& e : c->ev)
-            if (e) cudaEventDestroy(e);
-        if (c->stream) cudaStreamDestroy(c->stream);
-        if (c->joinEv) cudaEventDestroy(c->joinEv);
-    }
+    for (auto& c : rc->cameras) releaseCamera(c.get());
     if (rc->forkEv) cudaEventDestroy(rc->forkEv);
     cudaStreamDestroy(rc->stream);
     delete rc;
@@ -701,12 +744,7 @@ int hvvr_camera_destroy(hvvr_raycaster* rc, hvvr_camera* cam) {
     for (auto it = rc->cameras.begin(); it != rc->cameras.end(); ++it) {
         if (it->get() == cam) {
             cudaDeviceSynchronize();
-            unregisterTarget(cam);
-            if (cam->hostCounters) cudaFreeHost(cam->hostCounters);
-            for (auto& e : cam->ev)
-                if (e) cudaEventDestroy(e);
-            if (cam->stream) cudaStreamDestroy(cam->stream);
-            if (cam->joinEv) cudaEventDestroy(cam->joinEv);
+            releaseCamera(cam);
             rc->cameras.erase(it);
             return HVVR_OK;
         }

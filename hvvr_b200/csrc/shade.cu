@@ -236,9 +236,10 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
     const float4* __restrict__ materials, const Rays4* __restrict__ tileRays, const float4* __restrict__ beams,
     const TileList* __restrict__ lists, const uint32_t* __restrict__ pool, const uint32_t* __restrict__ chunkNext,
     Mat4 M, LightEnvDev env, uint32_t* __restrict__ colors, uint32_t* __restrict__ hitOut,
-    float* __restrict__ depthOut) {
+    float* __restrict__ depthOut, const uint32_t* __restrict__ order, uint32_t first) {
     __shared__ ShadeSmem sm;
-    const uint32_t tile = blockIdx.x, tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t tile = order ? order[first + blockIdx.x] : blockIdx.x;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sid = tile * kTileSize + tid;
     const TileList L = lists[tile];
     if (L.count == 0) {
@@ -472,19 +473,20 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
 }
 
 template <uint32_t N>
-cudaError_t launchRate(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
+cudaError_t launchRate(const SceneDev& s, const CameraDev& c, const FrameParams& f, const uint32_t* order,
+                       uint32_t first, uint32_t count, cudaStream_t st) {
     uint32_t* hitOut = f.capture ? c.hitIds : nullptr;
     float* depthOut = f.capture ? c.depth : nullptr;
     if (f.fpStrict)
-        intersectShadeKernel<N, false><<<c.tiles, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
-                                                                      c.tileRays, c.beams, c.tileLists, c.pool,
-                                                                      c.chunkNext, f.cameraToWorld, s.env, c.colors,
-                                                                      hitOut, depthOut);
+        intersectShadeKernel<N, false><<<count, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
+                                                                    c.tileRays, c.beams, c.tileLists, c.pool,
+                                                                    c.chunkNext, f.cameraToWorld, s.env, c.colors,
+                                                                    hitOut, depthOut, order, first);
     else
-        intersectShadeKernel<N, true><<<c.tiles, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
-                                                                     c.tileRays, c.beams, c.tileLists, c.pool,
-                                                                     c.chunkNext, f.cameraToWorld, s.env, c.colors,
-                                                                     hitOut, depthOut);
+        intersectShadeKernel<N, true><<<count, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
+                                                                   c.tileRays, c.beams, c.tileLists, c.pool,
+                                                                   c.chunkNext, f.cameraToWorld, s.env, c.colors,
+                                                                   hitOut, depthOut, order, first);
     return cudaGetLastError();
 }
 
@@ -513,17 +515,22 @@ __global__ void remapKernel(const uint32_t* __restrict__ src, const int32_t* __r
 
 } // namespace
 
-cudaError_t launchIntersectShade(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
-    if (c.tiles == 0) return cudaSuccess;
+cudaError_t launchIntersectShadeRange(const SceneDev& s, const CameraDev& c, const FrameParams& f,
+                                      const uint32_t* order, uint32_t first, uint32_t count, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
     switch (c.msaa) {
-    case 1: return launchRate<1>(s, c, f, st);
-    case 2: return launchRate<2>(s, c, f, st);
-    case 4: return launchRate<4>(s, c, f, st);
-    case 8: return launchRate<8>(s, c, f, st);
-    case 16: return launchRate<16>(s, c, f, st);
-    case 32: return launchRate<32>(s, c, f, st);
+    case 1: return launchRate<1>(s, c, f, order, first, count, st);
+    case 2: return launchRate<2>(s, c, f, order, first, count, st);
+    case 4: return launchRate<4>(s, c, f, order, first, count, st);
+    case 8: return launchRate<8>(s, c, f, order, first, count, st);
+    case 16: return launchRate<16>(s, c, f, order, first, count, st);
+    case 32: return launchRate<32>(s, c, f, order, first, count, st);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launchIntersectShade(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
+    return launchIntersectShadeRange(s, c, f, nullptr, 0, c.tiles, st);
 }
 
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st) {

@@ -428,8 +428,11 @@ struct TileCullArgs {
     uint32_t* pool;
     uint32_t* chunkNext;
     uint32_t poolChunks;
-    uint32_t* counters;   // [0] chunk allocator, [1] status, [2] work-queue head
+    uint32_t* counters;   // [0] chunk allocator, [1] status
     const uint32_t* order; // tile order for the queue (nullptr = natural order)
+    uint32_t first;       // this launch culls order[first, first + count)
+    uint32_t count;
+    uint32_t* queue;      // work-queue head of this launch, zero at launch
     uint32_t* cost;       // node visits per tile, written for next frame's order (may be nullptr)
 };
 
@@ -600,10 +603,10 @@ __global__ void __launch_bounds__(kTileWarps * 32) tileCullKernel(TileCullArgs a
     TileSmem& s = smem[warp];
     for (;;) {
         uint32_t w = 0;
-        if (lane == 0) w = atomicAdd(&a.counters[2], 1u);
+        if (lane == 0) w = atomicAdd(a.queue, 1u);
         w = __shfl_sync(kFull, w, 0);
-        if (w >= a.tiles) return;
-        const uint32_t tile = a.order ? a.order[w] : w;
+        if (w >= a.count) return;
+        const uint32_t tile = a.order ? a.order[a.first + w] : w;
         __syncwarp();
         const uint32_t visits = cullTile(a, tile, s);
         if (a.cost && lane == 0) a.cost[tile] = visits;
@@ -644,8 +647,15 @@ cudaError_t launchBlockCull(const SceneDev& s, const CameraDev& c, const FramePa
     return cudaGetLastError();
 }
 
-cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
+cudaError_t launchTileOrder(const CameraDev& c, cudaStream_t st) {
     if (c.tiles == 0) return cudaSuccess;
+    tileOrderKernel<<<1, 1024, 0, st>>>(c.tileCost, c.tiles, c.tileOrder);
+    return cudaGetLastError();
+}
+
+cudaError_t launchTileCullRange(const SceneDev& s, const CameraDev& c, const FrameParams& f, const uint32_t* order,
+                                uint32_t first, uint32_t count, uint32_t* queue, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
     static int ctasPerSm = 0, sms = 0;
     if (!ctasPerSm) {
         int dev = 0;
@@ -655,15 +665,22 @@ cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FramePar
         if (ctasPerSm < 1) ctasPerSm = 1;
         if (sms < 1) sms = 1;
     }
-    if (c.tileOrder && c.tileCost && c.costValid) {
-        tileOrderKernel<<<1, 1024, 0, st>>>(c.tileCost, c.tiles, c.tileOrder);
-    }
     TileCullArgs a{s.nodes, c.tileRays, c.tiles, f.cameraToWorld, c.blockStacks, c.blockSizes, c.tileLists, c.pool,
-                   c.chunkNext, c.poolChunks, c.counters, c.costValid ? c.tileOrder : nullptr, c.tileCost};
-    const uint32_t needed = (c.tiles + kTileWarps - 1) / kTileWarps;
+                   c.chunkNext, c.poolChunks, c.counters, order, first, count, queue, c.tileCost};
+    const uint32_t needed = (count + kTileWarps - 1) / kTileWarps;
     const uint32_t grid = std::min<uint32_t>(needed, uint32_t(sms * ctasPerSm));
     tileCullKernel<<<grid, kTileWarps * 32, 0, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
+    if (c.tiles == 0) return cudaSuccess;
+    const bool ordered = c.tileOrder && c.tileCost && c.costValid;
+    if (ordered) {
+        cudaError_t e = launchTileOrder(c, st);
+        if (e != cudaSuccess) return e;
+    }
+    return launchTileCullRange(s, c, f, ordered ? c.tileOrder : nullptr, 0, c.tiles, &c.counters[2], st);
 }
 
 } // namespace hvb

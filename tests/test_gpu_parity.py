@@ -72,3 +72,36 @@ def test_c1_barrel_msaa8_offaxis(oracle):
     fo = render_oracle(oracle, sc, smp, w, h, 8, cam_xf=xf)
     _compare(cam, rc, fo, 8)
     rc.close()
+
+
+def test_c1_frame_sequence_two_cameras(oracle):
+    """Frames after the first schedule tiles by the previous frame's traversal cost and cull
+    the slowest ones on a second stream; two cameras render concurrently. Every frame of a
+    moving camera pair must still match the oracle exactly."""
+    sc = scene("c1")
+    w, h = 320, 288
+    smp = scenes.barrel_samples(w, h)
+    rc = hv.Raycaster()
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    cams = []
+    for _ in range(2):
+        cam = rc.create_camera(scenes.viewport_for(w, h))
+        cam.set_render_target(w, h)
+        cam.set_samples(smp, 1)
+        cam.set_msaa(4)
+        cam.set_capture(hv.HVVR_CAPTURE_HITS)
+        cams.append(cam)
+    path = [((0.0, 2.0, 10.0), (0.0, 0.0, 0.0)), ((2.5, 1.0, 7.0), (-1.0, 0.5, 0.0)), ((-3.0, 3.0, 8.0), (1.0, 0.0, -2.0))]
+    for frame, (eye, target) in enumerate(path):
+        xfs = []
+        for k, cam in enumerate(cams):
+            xf = scenes.camera_transform(eye=(eye[0] + 0.3 * k, eye[1], eye[2]), target=target)
+            cam.set_camera_to_world(xf)
+            xfs.append(xf)
+        rc.render()
+        for cam, xf in zip(cams, xfs):
+            fo = render_oracle(oracle, sc, smp, w, h, 4, cam_xf=xf)
+            _compare(cam, rc, fo, 4)
+    rc.close()
