@@ -57,8 +57,8 @@ def load_peaks():
 
 
 def committed_traffic():
-    """DRAM bytes per intersect launch from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "intersect_shade_traffic.json")
+    """DRAM bytes per frame of each kernel, scaled from the committed ncu captures, if present."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
@@ -128,6 +128,9 @@ def replica_throughput(samples_per_frame, frames, seconds, world):
     return world * samples_per_frame * frames / seconds / 1e9
 
 
+import numpy as np  # noqa: E402
+
+
 def stereo_setup(hv, scenes, sc, target_cuda, torch):
     rc = hv.Raycaster(tri_index_capacity=128 << 20)
     rc.create_model(sc)
@@ -151,28 +154,37 @@ def stereo_setup(hv, scenes, sc, target_cuda, torch):
     return rc, cams, images, smp, eyes
 
 
-def algorithmic_bytes(hv, scenes, sc, torch):
-    """Compulsory HBM bytes of one intersect+shade launch (per eye, left eye), from one capture frame:
-    per sample 48 B beam + 4 B RGBA8 written; per list entry 4 B index + 48 B triangle; per unique
-    (sample, triangle) hit 16 B shade record + 3 x 32 B vertices + 64 B material + 48 B triangle."""
-    rc = hv.Raycaster()
-    rc.create_model(sc)
-    for l in sc.lights:
-        rc.create_light(l)
-    cam = rc.create_camera(scenes.viewport_for(W, H))
-    cam.set_render_target(W, H)
-    cam.set_samples(scenes.barrel_samples(W, H))
-    cam.set_camera_to_world(scenes.stereo_eyes(IPD)[0])
-    cam.set_msaa(MSAA)
-    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+def frame_counts(hv, scenes, sc):
+    """Counts of one captured stereo frame (both eyes) that define the algorithmic bytes."""
+    rc, cams, _, _, _ = stereo_setup(hv, scenes, sc, False, None)
+    for c in cams:
+        c.set_capture(hv.HVVR_CAPTURE_HITS)
     rc.render()
-    blocks, tiles, padded, msaa = cam.layout()
-    list_total = cam.list_total()
-    n, tri, mask = cam.gbuffer()
-    valid_pairs = int(((tri != 0xFFFFFFFF) & (mask != 0)).sum())
+    rc.render()
+    out = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0}
+    for cam in cams:
+        blocks, tiles, padded, msaa = cam.layout()
+        n, tri, mask = cam.gbuffer()
+        out["padded_samples"] += padded
+        out["tiles"] += tiles
+        out["list_entries"] += cam.list_total()
+        out["unique_hits"] += int(((tri != 0xFFFFFFFF) & (mask != 0)).sum())
+        out["node_visits"] += int(cam.tile_costs().astype(np.int64).sum())
     rc.close()
-    b = padded * (48 + 4) + list_total * (4 + 48) + valid_pairs * (16 + 96 + 64 + 48)
-    return b, {"padded_samples": padded, "list_entries": list_total, "unique_hits": valid_pairs}
+    return out
+
+
+def intersect_bytes(c):
+    """Compulsory HBM bytes of a frame's intersect+shade launches: per sample 48 B beam + 4 B RGBA8
+    written; per list entry 4 B index + 48 B triangle; per unique (sample, triangle) hit 16 B shade
+    record + 3 x 32 B vertices + 64 B material + 48 B triangle."""
+    return c["padded_samples"] * (48 + 4) + c["list_entries"] * (4 + 48) + c["unique_hits"] * (16 + 96 + 64 + 48)
+
+
+def cull_bytes(c):
+    """Compulsory HBM bytes of a frame's tile-cull launches: one 128 B BVH node per visit, 4 B per
+    list entry written, 96 B of corner rays per tile."""
+    return c["node_visits"] * 128 + c["list_entries"] * 4 + c["tiles"] * 96
 
 
 def run_reference_arm(args, rank):
@@ -261,7 +273,7 @@ def main():
 
     sc = scenes.scene_c2()
     hv.generate_topology(sc)
-    alg_bytes, alg_counts = algorithmic_bytes(hv, scenes, sc, torch)
+    counts = frame_counts(hv, scenes, sc)
 
     rc, cams, images, smp, eyes = stereo_setup(hv, scenes, sc, True, torch)
     samples_per_frame = 2 * len(smp)
@@ -275,7 +287,7 @@ def main():
     rc.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    isect_ms, stage_ms = [], []
+    kernel_ms, stage_ms = [], []
     clocks = Clocks(local)
     if dist:
         dist.barrier()
@@ -287,10 +299,8 @@ def main():
         rc.render(stream=sp)
         ends[i].record(stream)
         torch.cuda.synchronize()
-        for c in cams:
-            tm = c.timings()
-            isect_ms.append(float(tm[3]))
-            stage_ms.append([float(x) for x in tm])
+        kernel_ms.append([float(x) for x in rc.kernel_times()])
+        stage_ms.append([float(x) for x in cams[0].timings()])
     torch.cuda.synchronize()
     ck = clocks.stop()
     rc.synchronize()
@@ -319,10 +329,18 @@ def main():
     rc2.close()
 
     peak, peak_kind = load_peaks()
-    isect_avg = statistics.mean(isect_ms)
-    achieved = alg_bytes / (isect_avg * 1e-3) / 1e9
+    cull_ms = statistics.mean(k[0] for k in kernel_ms)
+    isect_ms = statistics.mean(k[1] for k in kernel_ms)
+    kernels = {
+        "tileCullKernel": {"algorithmic_bytes": cull_bytes(counts), "launch_ms_per_frame": cull_ms},
+        "intersectShadeKernel<8,FMA>": {"algorithmic_bytes": intersect_bytes(counts), "launch_ms_per_frame": isect_ms},
+    }
     tr = committed_traffic()
-    traffic = tr.get("dram_bytes_per_launch_full") if tr else None
+    for name, k in kernels.items():
+        k["achieved_gbs"] = k["algorithmic_bytes"] / (k["launch_ms_per_frame"] * 1e-3) / 1e9
+        k["frac"] = k["achieved_gbs"] / peak
+        k["traffic"] = (tr or {}).get(name)
+    dom = max(kernels, key=lambda n: kernels[n]["launch_ms_per_frame"])
     line = {
         "metric": "vis+shade Gsamples/s", "value": value, "unit": "Gsamples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -330,17 +348,20 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded procedural 995k-triangle scene, barrel-distorted sample set)",
         "config": {"workload": "stereo 2x1080x1200 8xMSAA barrel-distorted samples, 995,072-triangle scene, "
-                               "one plain frame per step", "samples_per_frame": samples_per_frame,
+                               "one frame (both eyes) per step", "samples_per_frame": samples_per_frame,
                    "parallelism": "replicas x%d" % world, "l2": "flushed between frames (256 MiB write, untimed)"},
         "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 2 * 32,
                 "d2h_bytes_per_step": 2 * W * H * 4},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "intersectShadeKernel<8,FMA> (one eye)",
-                     "algorithmic_bytes": alg_bytes, "avg_launch_ms": isect_avg, "counts": alg_counts,
-                     "peak_source": peak_kind},
-        "stage_ms_per_eye": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
-                             [(1, "block_cull"), (2, "tile_cull"), (3, "intersect_shade"), (4, "remap"), (5, "total")]},
-        "gpu_launches": args.steps * 2 * 4,
+        "roofline": {"bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": kernels[dom]["frac"], "traffic": kernels[dom]["traffic"], "kernel": dom,
+                     "per_frame": "launches of one stereo frame; bytes and times summed over them",
+                     "peak_source": peak_kind, "kernels": kernels, "counts": counts},
+        "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
+                               [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
+                                (4, "remap"), (5, "total")]},
+        # per frame: block cull, tile order, per eye set of tiles 2 tile-cull + 2 intersect launches
+        # (slowest tiles on their own stream), remap per eye
+        "gpu_launches": args.steps * 8,
         "clocks": ck,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -373,7 +394,7 @@ def run_profile_case():
             rc.render()
         rc.synchronize()
         print(json.dumps({"profile_case": "one eye 1080x1200 8xMSAA, 995k tris", "stage_ms": [float(x) for x in cam.timings()],
-                          "list_entries": cam.list_total()}))
+                          "kernel_ms": [float(x) for x in rc.kernel_times()], "list_entries": cam.list_total()}))
 
 
 def ctypes_stream(stream):

@@ -80,6 +80,19 @@ _sig("hvvr_scene_read_triangles", _vp, _vp)
 _sig("hvvr_generate_topology", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32))
 _sig("hvvr_grid_samples", _u32, _u32, _vp)
 _sig("hvvr_tile_cull_static", _vp, _vp, _vp, C.c_uint64, _p(C.c_uint64), _vp)
+_lib.hvvr_batch_config_default.argtypes = [_p(_abi.BatchConfig)]
+_lib.hvvr_batch_config_default.restype = None
+_sig("hvvr_batch_create", _p(_vp), _u32, _p(_abi.BatchConfig), _p(_vp))
+_sig("hvvr_batch_destroy", _vp)
+_sig("hvvr_batch_render", _vp, C.c_double, _vp)
+_sig("hvvr_batch_synchronize", _vp)
+_sig("hvvr_batch_get_config", _vp, _p(_abi.BatchConfig))
+_sig("hvvr_batch_set_config", _vp, _p(_abi.BatchConfig))
+_sig("hvvr_batch_autotune", _vp, _u32, _p(_abi.BatchConfig))
+_sig("hvvr_batch_read_timings", _vp, _vp)
+_sig("hvvr_batch_read_kernel_times", _vp, _vp)
+_sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
+_sig("hvvr_camera_read_tile_costs", _vp, _vp)
 
 EXPORTED = [
     "hvvr_last_error", "hvvr_version", "hvvr_spec_default", "hvvr_raycaster_create", "hvvr_raycaster_destroy",
@@ -94,7 +107,10 @@ EXPORTED = [
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
     "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
-    "hvvr_tile_cull_static",
+    "hvvr_tile_cull_static", "hvvr_batch_config_default", "hvvr_batch_create", "hvvr_batch_destroy",
+    "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
+    "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
+    "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs",
 ]
 
 
@@ -257,6 +273,13 @@ class Camera:
         _check(_lib.hvvr_camera_read_timings(self.handle, t.ctypes.data))
         return t
 
+    def tile_costs(self):
+        """BVH nodes visited per tile by the last frame's tile cull"""
+        n = self.layout()[1]
+        v = np.zeros(n, dtype=np.uint32)
+        _check(_lib.hvvr_camera_read_tile_costs(self.handle, v.ctypes.data))
+        return v
+
     def list_total(self):
         total = C.c_uint64(0)
         _check(_lib.hvvr_camera_read_list_total(self.handle, C.byref(total)))
@@ -276,9 +299,12 @@ class Raycaster:
         _check(_lib.hvvr_raycaster_create(C.byref(spec), C.byref(h)))
         self.handle = h
         self.cameras, self.models, self.lights = [], [], []
+        self.batches = []
 
     def close(self):
         if self.handle:
+            for b in list(self.batches):
+                b.close()
             _check(_lib.hvvr_raycaster_destroy(self.handle))
             self.handle = None
 
@@ -335,6 +361,12 @@ class Raycaster:
     def synchronize(self):
         _check(_lib.hvvr_raycaster_synchronize(self.handle))
 
+    def kernel_times(self):
+        """device ms of the last frame's launches: tile cull, intersect/shade, block cull, remap"""
+        t = np.zeros(4, dtype=np.float32)
+        _check(_lib.hvvr_raycaster_read_kernel_times(self.handle, t.ctypes.data))
+        return t
+
     def scene_counts(self):
         n, t, v = _u32(0), _u32(0), _u32(0)
         _check(_lib.hvvr_scene_get_counts(self.handle, C.byref(n), C.byref(t), C.byref(v)))
@@ -351,3 +383,75 @@ class Raycaster:
         a = np.zeros((t, 9), dtype=np.float32)
         _check(_lib.hvvr_scene_read_triangles(self.handle, a.ctypes.data))
         return a
+
+
+def batch_config(**kw):
+    """hvvr_batch_config with the library defaults, overridden by keyword."""
+    cfg = _abi.BatchConfig()
+    _lib.hvvr_batch_config_default(C.byref(cfg))
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+class Batch:
+    """The enabled cameras of several raycasters (one scene each, one device) rendered as one
+    frame: one launch per stage over all views, replayed from a CUDA graph once stable."""
+
+    def __init__(self, raycasters, config=None):
+        arr = (_vp * len(raycasters))(*[r.handle for r in raycasters])
+        h = _vp()
+        _check(_lib.hvvr_batch_create(arr, len(raycasters), C.byref(config) if config is not None else None,
+                                      C.byref(h)))
+        self.handle = h
+        self.raycasters = list(raycasters)
+        for r in self.raycasters:
+            r.batches.append(self)
+
+    def close(self):
+        if self.handle:
+            _check(_lib.hvvr_batch_destroy(self.handle))
+            self.handle = None
+            for r in self.raycasters:
+                if self in r.batches:
+                    r.batches.remove(self)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, elapsed=0.0, stream=None):
+        _check(_lib.hvvr_batch_render(self.handle, C.c_double(elapsed), stream))
+
+    def synchronize(self):
+        _check(_lib.hvvr_batch_synchronize(self.handle))
+
+    @property
+    def config(self):
+        cfg = _abi.BatchConfig()
+        _check(_lib.hvvr_batch_get_config(self.handle, C.byref(cfg)))
+        return cfg
+
+    @config.setter
+    def config(self, cfg):
+        _check(_lib.hvvr_batch_set_config(self.handle, C.byref(cfg)))
+
+    def autotune(self, frames=5):
+        cfg = _abi.BatchConfig()
+        _check(_lib.hvvr_batch_autotune(self.handle, frames, C.byref(cfg)))
+        return cfg
+
+    def kernel_times(self):
+        """device ms of the last frame's launches: tile cull, intersect/shade, block cull, remap"""
+        t = np.zeros(4, dtype=np.float32)
+        _check(_lib.hvvr_batch_read_kernel_times(self.handle, t.ctypes.data))
+        return t
+
+    def timings(self):
+        """device ms of the last frame: total, block cull, first tile cull, rest of cull +
+        intersect/shade, remap + copies (stages 0 for a graph replay)"""
+        t = np.zeros(5, dtype=np.float32)
+        _check(_lib.hvvr_batch_read_timings(self.handle, t.ctypes.data))
+        return t

@@ -96,6 +96,12 @@ class TileCullArgs(C.Structure):
                 ("camera_to_world", Transform)]
 
 
+class BatchConfig(C.Structure):
+    """hvvr_batch_config: knobs of a frame batch (set by hand or by hvvr_batch_autotune)."""
+    _fields_ = [("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32), ("tri_index_capacity", C.c_uint64),
+                ("use_graph", C.c_uint32), ("frame_ms", C.c_float)]
+
+
 # numpy layouts of the bulk arrays
 SAMPLE_DTYPE = np.dtype([("pixel", "<u4", 2), ("position", "<f4", 2), ("minor", "<f4", 2), ("major", "<f4")])
 VERTEX_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<u2", 4), ("uv", "<f4", 2), ("pad", "<u4")])

@@ -107,14 +107,8 @@ struct CameraDev {
     // per frame
     StackEntry* blockStacks = nullptr; // [blocks * kBlockStack]
     uint32_t* blockSizes = nullptr;    // [blocks]
-    TileList* tileLists = nullptr;     // [tiles]
-    uint32_t* pool = nullptr;          // [poolChunks * kChunk]
-    uint32_t* chunkNext = nullptr;     // [poolChunks]
-    uint32_t poolChunks = 0;
-    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2], [3] tile queue heads
+    TileList* tileLists = nullptr;     // [tiles], chunk indices into the rendering batch's pool
     uint32_t* tileCost = nullptr;      // [tiles] node visits of the last frame (scheduling only)
-    uint32_t* tileOrder = nullptr;     // [tiles] longest-first tile order built from tileCost
-    bool costValid = false;            // tileCost holds a previous frame's values
     uint32_t* colors = nullptr;        // [padded] RGBA8 per sorted sample
     uint32_t* hitIds = nullptr;        // [padded * msaa] when capturing
     float* depth = nullptr;            // [padded * msaa] when capturing
@@ -122,30 +116,65 @@ struct CameraDev {
     uint64_t imageStride = 0;
 };
 
-struct FrameParams {
-    Mat4 cameraToWorld;
-    uint32_t fpStrict;
-    uint32_t capture;
+// One view of a frame: a camera and the scene it renders. A frame is a table of views whose
+// blocks and tiles are numbered consecutively ("global" indices); every stage runs one launch
+// over all views, and a kernel finds its view through blockView[global block].
+struct ViewDev {
+    Mat4 M;                          // camera to world for this frame
+    LightEnvDev env;
+    const Node* nodes;
+    const float4* tris;
+    const uint4* triShade;
+    const float4* verts;
+    const float4* materials;
+    const Rays4* tileRays;
+    const Rays4* blockRays;
+    const float4* beams;
+    StackEntry* blockStacks;
+    uint32_t* blockSizes;
+    TileList* tileLists;
+    uint32_t* tileCost;
+    uint32_t* colors;
+    uint32_t* hitIds;                // nullptr unless capturing
+    float* depth;
+    uint32_t tileStart, blockStart;  // first global tile / block
+    uint32_t msaa, rateIdx;          // rate and its index in 1,2,4,8,16,32
 };
+
+// frame-wide device state shared by the launches of one batch
+struct FrameDev {
+    const ViewDev* views = nullptr;    // [viewCount]
+    const uint32_t* blockView = nullptr; // [blocks] view of each global block
+    uint32_t viewCount = 0, tiles = 0, blocks = 0;
+    uint32_t* pool = nullptr;          // [poolChunks * kChunk] triangle-list chunks
+    uint32_t* chunkNext = nullptr;     // [poolChunks]
+    uint32_t poolChunks = 0;
+    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2 + k] work-queue heads
+    uint32_t* order = nullptr;         // [tiles] tile order: grouped by rate, then longest first
+};
+
 
 // records the message returned by hvvr_last_error() on this thread and returns code
 int setLastError(int code, const char* msg);
 
+enum : uint32_t { kCounterWords = 16, kQueueBase = 2 };
+
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
-cudaError_t launchBlockCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
-// whole-camera tile cull (longest-first when c.costValid) on queue counters[2]
-cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
-// c.tileOrder <- tiles sorted by descending c.tileCost (log2 buckets)
-cudaError_t launchTileOrder(const CameraDev& c, cudaStream_t st);
-// tile cull / intersect of the tiles order[first, first + count) (order == nullptr: tiles 0..count-1);
-// concurrent tile-cull launches of one camera need distinct zeroed queue heads
-cudaError_t launchTileCullRange(const SceneDev& s, const CameraDev& c, const FrameParams& f, const uint32_t* order,
-                                uint32_t first, uint32_t count, uint32_t* queue, cudaStream_t st);
-cudaError_t launchIntersectShade(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st);
-cudaError_t launchIntersectShadeRange(const SceneDev& s, const CameraDev& c, const FrameParams& f,
-                                      const uint32_t* order, uint32_t first, uint32_t count, cudaStream_t st);
+cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st);
+// fr.order <- global tiles grouped by ascending rate index, longest first (log2 buckets of
+// last frame's visit counts) within a rate
+cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st);
+// tile cull / intersect-shade of the global tiles order[first, first + count) (order ==
+// nullptr: tiles first..first+count-1); concurrent tile-cull launches need distinct zeroed
+// queue heads. warps = tile-cull warps per CTA (2, 4 or 8).
+cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                           uint32_t* queue, uint32_t warps, cudaStream_t st);
+cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, const uint32_t* order,
+                                 uint32_t first, uint32_t count, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
 cudaError_t launchRefit(const SceneDev& s, cudaStream_t st);
 cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);
+// writes v to *dst with a one-thread kernel (no host memory involved; capturable)
+cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st);
 
 } // namespace hvb

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <memory>
 #include <string>
 #include <vector>
@@ -121,6 +122,8 @@ struct hvvr_camera {
     uint32_t capture = 0;
     bool setupDirty = true;
     bool rendered = false;
+    uint64_t setupGen = 0;            // process-unique id of the current sample setup and buffers
+    hvvr_batch* lastBatch = nullptr;  // batch whose pool holds this camera's last tile lists
     CameraDev dev;
     SampleSetup setup;
     // device storage behind dev
@@ -130,21 +133,48 @@ struct hvvr_camera {
     DevBuf<StackEntry> blockStacks;
     DevBuf<uint32_t> blockSizes;
     DevBuf<TileList> tileLists;
-    DevBuf<uint32_t> pool, chunkNext, counters, colors, hitIds, image, tileCost, tileOrder;
+    DevBuf<uint32_t> colors, hitIds, image, tileCost;
     DevBuf<float> depth;
-    uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
     void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
-    cudaEvent_t ev[6] = {};
-    float lastMs[6] = {};
-    // each camera renders on its own stream, forked from and joined back to the render stream,
-    // so the cameras of a frame (e.g. both eyes) overlap on the device
-    cudaStream_t stream = nullptr;
-    cudaEvent_t joinEv = nullptr;
-    // from the second frame on, the tiles that were slowest to traverse last frame are culled
-    // and shaded on a high-priority side stream, while the rest are culled and shaded on
-    // `stream`; the long traversals of the few heavy tiles then overlap with shading work
-    cudaStream_t heavyStream = nullptr;
-    cudaEvent_t orderEv = nullptr, heavyEv = nullptr;
+};
+
+// A frame batch: the enabled cameras of one or more raycasters (one scene each, same device)
+// rendered as one frame - one launch per stage over all views, the tile cull as one
+// persistent work queue, intersect/shade once per MSAA rate - optionally replayed from a
+// CUDA graph. Every raycaster renders its own cameras through an internal batch.
+struct hvvr_batch {
+    std::vector<hvvr_raycaster*> rcs;
+    bool internal = false;            // a raycaster's own batch
+    bool detached = false;            // one of its raycasters was destroyed
+    hvvr_batch_config cfg{};
+    // layout of the current frame
+    struct View {
+        hvvr_camera* cam;
+        uint32_t tileStart, blockStart;
+    };
+    std::vector<View> views;
+    std::vector<uint64_t> layoutKey;
+    uint32_t tiles = 0, blocks = 0;
+    uint32_t rateTiles[6] = {}, rateStart[6] = {};
+    bool fpStrict = false;
+    bool costValid = false;           // every view's tileCost holds a previous frame's counts
+    DevBuf<ViewDev> viewsDev;
+    DevBuf<uint32_t> blockView, order, pool, chunkNext, counters;
+    uint32_t poolChunks = 0;
+    ViewDev* hostViews[2] = {};       // pinned staging of the per-frame view table
+    size_t hostViewsCap = 0;
+    cudaEvent_t hostViewsEv[2] = {};
+    bool hostViewsUsed[2] = {};
+    int hostSlot = 0;
+    uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
+    bool counterValid = false;
+    cudaStream_t side[12] = {};       // per rate: [2r] heavy tiles (high priority), [2r+1] the rest
+    cudaEvent_t forkEv = nullptr, doneEv[12] = {}, ev[6] = {};
+    cudaEvent_t kev[12][3] = {};      // per side stream: before tile cull, after it, after intersect
+    bool kevUsed[12] = {};
+    bool stageTimes = false;          // ev[1..4] and kev were recorded by the last frame
+    cudaGraphExec_t graph = nullptr;
+    std::vector<uint64_t> graphKey;
 };
 
 struct hvvr_raycaster {
@@ -164,7 +194,8 @@ struct hvvr_raycaster {
     DevBuf<Mat4> modelToWorld;
     std::vector<Node> hostNodes;
     uint32_t refitStatus = 0;
-    cudaEvent_t forkEv = nullptr;
+    std::unique_ptr<hvvr_batch> own;      // renders this raycaster's cameras
+    std::vector<hvvr_batch*> batches;     // user batches that include this raycaster
 };
 
 namespace {
@@ -357,6 +388,8 @@ int uploadTransforms(hvvr_raycaster* rc, cudaStream_t st) {
     return rc->modelToWorld.upload(xf.data(), xf.size(), st);
 }
 
+std::atomic<uint64_t> gSetupGen{0};
+
 int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     if (cam->samples.empty()) return fail(HVVR_ERR_STATE, "camera has no samples");
     const uint32_t w = cam->target.width, h = cam->target.height;
@@ -371,18 +404,8 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     TRY(cam->blockSizes.alloc(ss.blocks));
     TRY(cam->tileLists.alloc(ss.tiles));
     TRY(cam->colors.alloc(ss.padded));
-    TRY(cam->counters.alloc(4));
     TRY(cam->tileCost.alloc(ss.tiles));
-    TRY(cam->tileOrder.alloc(ss.tiles));
-    cam->dev.costValid = false;
-    if (!cam->hostCounters) CUDA_TRY(cudaMallocHost((void**)&cam->hostCounters, 4 * sizeof(uint32_t)));
-    const uint64_t capEntries = cam->rc->spec.tri_index_capacity ? cam->rc->spec.tri_index_capacity : (128ull << 20);
-    const uint64_t chunks = (capEntries + kChunk - 1) / kChunk;
-    if (chunks > 0xfffffff0ull) return fail(HVVR_ERR_INVALID, "tri_index_capacity too large");
-    if (cam->chunkNext.n != chunks) {
-        TRY(cam->pool.alloc(size_t(chunks) * kChunk));
-        TRY(cam->chunkNext.alloc(size_t(chunks)));
-    }
+    CUDA_TRY(cudaMemsetAsync(cam->tileCost.p, 0, size_t(ss.tiles) * 4, st));
     const bool cpuTarget = cam->target.memory_type == HVVR_MEMORY_CPU;
     if (cpuTarget && w && h) TRY(cam->image.alloc(size_t(w) * h));
     CameraDev& d = cam->dev;
@@ -400,12 +423,7 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     d.blockStacks = cam->blockStacks.p;
     d.blockSizes = cam->blockSizes.p;
     d.tileLists = cam->tileLists.p;
-    d.pool = cam->pool.p;
-    d.chunkNext = cam->chunkNext.p;
-    d.poolChunks = uint32_t(chunks);
-    d.counters = cam->counters.p;
     d.tileCost = cam->tileCost.p;
-    d.tileOrder = cam->tileOrder.p;
     d.colors = cam->colors.p;
     if (cpuTarget) {
         d.image = cam->image.p;
@@ -414,86 +432,8 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
         d.image = static_cast<uint32_t*>(cam->target.data);
         d.imageStride = cam->target.stride ? cam->target.stride : w;
     }
-    if (!cam->ev[0])
-        for (auto& e : cam->ev) CUDA_TRY(cudaEventCreate(&e));
-    if (!cam->stream) {
-        CUDA_TRY(cudaStreamCreateWithFlags(&cam->stream, cudaStreamNonBlocking));
-        CUDA_TRY(cudaEventCreateWithFlags(&cam->joinEv, cudaEventDisableTiming));
-        int leastPriority = 0, greatestPriority = 0;
-        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
-        CUDA_TRY(cudaStreamCreateWithPriority(&cam->heavyStream, cudaStreamNonBlocking, greatestPriority));
-        CUDA_TRY(cudaEventCreateWithFlags(&cam->orderEv, cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&cam->heavyEv, cudaEventDisableTiming));
-    }
     cam->setupDirty = false;
-    return HVVR_OK;
-}
-
-// cameras with fewer tiles run one tile-cull launch
-constexpr uint32_t kSplitMinTiles = 32;
-// heavy share of the tiles (1/8 was fastest on the 1M-triangle stereo 2x1080x1200 frame;
-// 1/4 and 1/16 within 1%, no split 4.5% slower)
-constexpr uint32_t kHeavyDiv = 8;
-
-// Number of heavy tiles split off to the side stream (0: one tile-cull launch for the whole
-// camera). Needs last frame's per-tile visit counts.
-uint32_t heavyTiles(const CameraDev& d) {
-    if (!d.costValid || d.tiles < kSplitMinTiles) return 0;
-    return std::max<uint32_t>(1u, d.tiles / kHeavyDiv);
-}
-
-int renderCamera(hvvr_raycaster* rc, hvvr_camera* cam, cudaStream_t parent) {
-    if (cam->setupDirty) TRY(setupCamera(cam, parent));
-    cudaStream_t st = cam->stream;
-    CUDA_TRY(cudaStreamWaitEvent(st, rc->forkEv, 0));
-    CameraDev& d = cam->dev;
-    d.msaa = cam->msaa;
-    if (cam->capture & HVVR_CAPTURE_HITS) {
-        TRY(cam->hitIds.alloc(size_t(d.padded) * d.msaa));
-        TRY(cam->depth.alloc(size_t(d.padded) * d.msaa));
-        d.hitIds = cam->hitIds.p;
-        d.depth = cam->depth.p;
-    }
-    FrameParams f;
-    f.cameraToWorld = transformToMatrix(cam->xf);
-    f.fpStrict = rc->spec.fp_mode == HVVR_FP_STRICT ? 1u : 0u;
-    f.capture = (cam->capture & HVVR_CAPTURE_HITS) ? 1u : 0u;
-    CUDA_TRY(cudaEventRecord(cam->ev[0], st));
-    CUDA_TRY(cudaMemsetAsync(d.counters, 0, 4 * sizeof(uint32_t), st));
-    CUDA_TRY(launchBlockCull(rc->scene, d, f, st));
-    CUDA_TRY(cudaEventRecord(cam->ev[1], st));
-    const uint32_t heavy = heavyTiles(d);
-    if (heavy) {
-        // tileOrder[0, heavy) are last frame's slowest tiles; each set gets its own queue head
-        CUDA_TRY(launchTileOrder(d, st));
-        CUDA_TRY(cudaEventRecord(cam->orderEv, st));
-        CUDA_TRY(cudaStreamWaitEvent(cam->heavyStream, cam->orderEv, 0));
-        CUDA_TRY(launchTileCullRange(rc->scene, d, f, d.tileOrder, 0, heavy, &d.counters[2], cam->heavyStream));
-        CUDA_TRY(launchIntersectShadeRange(rc->scene, d, f, d.tileOrder, 0, heavy, cam->heavyStream));
-        CUDA_TRY(cudaEventRecord(cam->heavyEv, cam->heavyStream));
-        CUDA_TRY(launchTileCullRange(rc->scene, d, f, d.tileOrder, heavy, d.tiles - heavy, &d.counters[3], st));
-        CUDA_TRY(cudaEventRecord(cam->ev[2], st));
-        CUDA_TRY(launchIntersectShadeRange(rc->scene, d, f, d.tileOrder, heavy, d.tiles - heavy, st));
-        CUDA_TRY(cudaStreamWaitEvent(st, cam->heavyEv, 0));
-    } else {
-        CUDA_TRY(launchTileCull(rc->scene, d, f, st));
-        CUDA_TRY(cudaEventRecord(cam->ev[2], st));
-        CUDA_TRY(launchIntersectShade(rc->scene, d, f, st));
-    }
-    CUDA_TRY(cudaEventRecord(cam->ev[3], st));
-    CUDA_TRY(launchRemap(d, st));
-    CUDA_TRY(cudaEventRecord(cam->ev[4], st));
-    CUDA_TRY(cudaMemcpyAsync(cam->hostCounters, d.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    if (cam->target.memory_type == HVVR_MEMORY_CPU && cam->target.data && d.width && d.height) {
-        const uint64_t stride = cam->target.stride ? cam->target.stride : d.width;
-        CUDA_TRY(cudaMemcpy2DAsync(cam->target.data, stride * 4, d.image, size_t(d.width) * 4, size_t(d.width) * 4,
-                                   d.height, cudaMemcpyDeviceToHost, st));
-    }
-    CUDA_TRY(cudaEventRecord(cam->ev[5], st));
-    CUDA_TRY(cudaEventRecord(cam->joinEv, st));
-    CUDA_TRY(cudaStreamWaitEvent(parent, cam->joinEv, 0));
-    d.costValid = true; // the next frame schedules its tiles by this frame's visit counts
-    cam->rendered = true;
+    cam->setupGen = ++gSetupGen;
     return HVVR_OK;
 }
 
@@ -506,27 +446,347 @@ void unregisterTarget(hvvr_camera* cam) {
     }
 }
 
-// frees the camera's pinned memory, streams and events (the device must be idle)
-void releaseCamera(hvvr_camera* cam) {
-    unregisterTarget(cam);
-    if (cam->hostCounters) cudaFreeHost(cam->hostCounters);
-    for (auto& e : cam->ev)
-        if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : {cam->joinEv, cam->orderEv, cam->heavyEv})
-        if (e) cudaEventDestroy(e);
-    for (cudaStream_t t : {cam->stream, cam->heavyStream})
-        if (t) cudaStreamDestroy(t);
+void releaseCamera(hvvr_camera* cam) { unregisterTarget(cam); }
+
+uint32_t rateIndex(uint32_t rate) { return rate <= 1 ? 0u : uint32_t(31 - __builtin_clz(rate)); }
+
+constexpr uint64_t kDefaultCapacity = 128ull << 20; // MAX_TRI_INDICES_TO_INTERSECT
+// rate groups with fewer tiles are not split
+constexpr uint32_t kSplitMinTiles = 32;
+
+void batchConfigDefault(hvvr_batch_config* c) {
+    c->tile_cull_warps = 4;
+    // 1/8 was fastest on the 1M-triangle stereo 2x1080x1200 frame (1/4 and 1/16 within 1%,
+    // no split 4.5% slower)
+    c->heavy_divisor = 8;
+    c->tri_index_capacity = kDefaultCapacity;
+    c->use_graph = 1;
+    c->frame_ms = 0.0f;
 }
 
-int checkStatus(hvvr_raycaster* rc) {
-    for (auto& c : rc->cameras) {
-        if (!c->rendered || !c->hostCounters) continue;
-        const uint32_t s = c->hostCounters[1];
-        if (s & kStatusPoolOverflow)
-            return fail(HVVR_ERR_OVERFLOW, "triangle-index pool exhausted (%u chunks); raise tri_index_capacity",
-                        c->dev.poolChunks);
-        if (s & kStatusStackOverflow) return fail(HVVR_ERR_OVERFLOW, "tile traversal stack exhausted");
-        if (s & kStatusBadLeaf) return fail(HVVR_ERR_INVALID, "BVH leaf with an empty triangle range passed the cull");
+int checkConfig(const hvvr_batch_config& c) {
+    if (c.tile_cull_warps != 2 && c.tile_cull_warps != 4 && c.tile_cull_warps != 8)
+        return fail(HVVR_ERR_INVALID, "tile_cull_warps must be 2, 4 or 8");
+    const uint64_t chunks = (c.tri_index_capacity + kChunk - 1) / kChunk;
+    if (c.tri_index_capacity == 0 || chunks > 0xfffffff0ull) return fail(HVVR_ERR_INVALID, "bad tri_index_capacity");
+    return HVVR_OK;
+}
+
+void dropGraph(hvvr_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graphKey.clear();
+}
+
+int batchResources(hvvr_batch* b) {
+    if (!b->forkEv) {
+        int leastPriority = 0, greatestPriority = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+        for (int r = 0; r < 6; r++) {
+            CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r], cudaStreamNonBlocking, greatestPriority));
+            CUDA_TRY(cudaStreamCreateWithFlags(&b->side[2 * r + 1], cudaStreamNonBlocking));
+        }
+        CUDA_TRY(cudaEventCreateWithFlags(&b->forkEv, cudaEventDisableTiming));
+        for (auto& e : b->doneEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : b->hostViewsEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : b->ev) CUDA_TRY(cudaEventCreate(&e));
+        for (auto& k : b->kev)
+            for (auto& e : k) CUDA_TRY(cudaEventCreate(&e));
+        CUDA_TRY(cudaMallocHost((void**)&b->hostCounters, kCounterWords * sizeof(uint32_t)));
+        memset(b->hostCounters, 0, kCounterWords * sizeof(uint32_t));
+    }
+    const uint64_t chunks = (b->cfg.tri_index_capacity + kChunk - 1) / kChunk;
+    if (b->chunkNext.n != chunks) {
+        b->chunkNext.release();
+        b->pool.release();
+        TRY(b->pool.alloc(size_t(chunks) * kChunk));
+        TRY(b->chunkNext.alloc(size_t(chunks)));
+        b->poolChunks = uint32_t(chunks);
+        dropGraph(b);
+    }
+    TRY(b->counters.alloc(kCounterWords));
+    return HVVR_OK;
+}
+
+void releaseBatch(hvvr_batch* b) {
+    dropGraph(b);
+    for (auto& t : b->side)
+        if (t) cudaStreamDestroy(t), t = nullptr;
+    for (cudaEvent_t* e : {&b->forkEv})
+        if (*e) cudaEventDestroy(*e), *e = nullptr;
+    for (auto& e : b->doneEv)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto& e : b->hostViewsEv)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto& e : b->ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto& k : b->kev)
+        for (auto& e : k)
+            if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto& h : b->hostViews)
+        if (h) cudaFreeHost(h), h = nullptr;
+    if (b->hostCounters) cudaFreeHost(b->hostCounters), b->hostCounters = nullptr;
+}
+
+int checkStatus(const hvvr_batch* b) {
+    if (!b || !b->counterValid || !b->hostCounters) return HVVR_OK;
+    const uint32_t s = b->hostCounters[1];
+    if (s & kStatusPoolOverflow)
+        return fail(HVVR_ERR_OVERFLOW, "triangle-index pool exhausted (%u chunks); raise tri_index_capacity",
+                    b->poolChunks);
+    if (s & kStatusStackOverflow) return fail(HVVR_ERR_OVERFLOW, "tile traversal stack exhausted");
+    if (s & kStatusBadLeaf) return fail(HVVR_ERR_INVALID, "BVH leaf with an empty triangle range passed the cull");
+    return HVVR_OK;
+}
+
+uint32_t heavyTiles(const hvvr_batch* b, uint32_t n) {
+    if (!b->costValid || !b->cfg.heavy_divisor || n < kSplitMinTiles) return 0;
+    return std::max<uint32_t>(1u, n / b->cfg.heavy_divisor);
+}
+
+// Enqueues one frame on st (and the side streams, forked from and joined back to st).
+// timing: record the stage events (not inside a graph capture).
+int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing) {
+    if (timing) CUDA_TRY(cudaEventRecord(b->ev[0], st));
+    CUDA_TRY(cudaMemsetAsync(fr.counters, 0, kCounterWords * sizeof(uint32_t), st));
+    CUDA_TRY(launchBlockCull(fr, st));
+    if (timing) CUDA_TRY(cudaEventRecord(b->ev[1], st));
+    CUDA_TRY(launchTileOrder(fr, st));
+    CUDA_TRY(cudaEventRecord(b->forkEv, st));
+    bool first = true;
+    for (auto& u : b->kevUsed) u = false;
+    for (uint32_t r = 0; r < 6; r++) {
+        const uint32_t n = b->rateTiles[r];
+        if (!n) continue;
+        const uint32_t rs = b->rateStart[r], heavy = heavyTiles(b, n), msaa = 1u << r;
+        // part 0: last frame's slowest tiles on the high-priority stream; part 1: the rest
+        for (uint32_t part = heavy ? 0u : 1u; part < 2; part++) {
+            const uint32_t k = 2 * r + part;
+            const uint32_t p0 = part ? rs + heavy : rs, pn = part ? n - heavy : heavy;
+            cudaStream_t ps = b->side[k];
+            CUDA_TRY(cudaStreamWaitEvent(ps, b->forkEv, 0));
+            if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][0], ps));
+            CUDA_TRY(launchTileCull(fr, fr.order, p0, pn, fr.counters + kQueueBase + k, b->cfg.tile_cull_warps, ps));
+            if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][1], ps));
+            if (timing && part == 1 && first) CUDA_TRY(cudaEventRecord(b->ev[2], ps));
+            CUDA_TRY(launchIntersectShade(fr, msaa, b->fpStrict, fr.order, p0, pn, ps));
+            if (timing) {
+                CUDA_TRY(cudaEventRecord(b->kev[k][2], ps));
+                b->kevUsed[k] = true;
+            }
+            CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
+            CUDA_TRY(cudaStreamWaitEvent(st, b->doneEv[k], 0));
+        }
+        first = false;
+    }
+    if (timing) CUDA_TRY(cudaEventRecord(b->ev[3], st));
+    for (const auto& v : b->views) CUDA_TRY(launchRemap(v.cam->dev, st));
+    if (timing) CUDA_TRY(cudaEventRecord(b->ev[4], st));
+    CUDA_TRY(cudaMemcpyAsync(b->hostCounters, fr.counters, kCounterWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    for (const auto& v : b->views) {
+        const hvvr_camera* c = v.cam;
+        const CameraDev& d = c->dev;
+        if (c->target.memory_type == HVVR_MEMORY_CPU && c->target.data && d.width && d.height) {
+            const uint64_t stride = c->target.stride ? c->target.stride : d.width;
+            CUDA_TRY(cudaMemcpy2DAsync(c->target.data, stride * 4, d.image, size_t(d.width) * 4, size_t(d.width) * 4,
+                                       d.height, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    if (timing) CUDA_TRY(cudaEventRecord(b->ev[5], st));
+    return HVVR_OK;
+}
+
+// Scene update and refit of every raycaster, then one frame of all their enabled cameras.
+int renderBatch(hvvr_batch* b, cudaStream_t st) {
+    if (b->detached) return fail(HVVR_ERR_STATE, "a raycaster of this batch was destroyed");
+    if (b->rcs.empty()) return HVVR_OK;
+    const int device = b->rcs[0]->spec.device;
+    const bool strict = b->rcs[0]->spec.fp_mode == HVVR_FP_STRICT;
+    CUDA_TRY(cudaSetDevice(device));
+    for (hvvr_raycaster* rc : b->rcs) {
+        if (rc->spec.device != device) return fail(HVVR_ERR_INVALID, "batched raycasters must share one device");
+        if ((rc->spec.fp_mode == HVVR_FP_STRICT) != strict)
+            return fail(HVVR_ERR_INVALID, "batched raycasters must share one fp_mode");
+        if (rc->sceneDirty) {
+            TRY(uploadScene(rc, st));
+            rc->sceneDirty = false;
+            rc->refitDirty = true;
+        }
+        if (rc->scene.nodeCount && rc->refitDirty) {
+            CUDA_TRY(launchRefit(rc->scene, st));
+            rc->refitDirty = false;
+        }
+    }
+    std::vector<hvvr_camera*> cams;
+    bool cpuTargets = false, capturable = true;
+    for (hvvr_raycaster* rc : b->rcs) {
+        if (rc->scene.nodeCount == 0) continue;
+        for (auto& cp : rc->cameras) {
+            hvvr_camera* c = cp.get();
+            if (!c->enabled || c->samples.empty()) continue;
+            if (c->setupDirty) TRY(setupCamera(c, st));
+            if (!rc->msaaUploaded[c->msaa]) {
+                float off[64];
+                msaaOffsets(c->msaa, off);
+                CUDA_TRY(uploadMsaaTable(c->msaa, off, st));
+                rc->msaaUploaded[c->msaa] = true;
+            }
+            CameraDev& d = c->dev;
+            d.msaa = c->msaa;
+            if (c->capture & HVVR_CAPTURE_HITS) {
+                TRY(c->hitIds.alloc(size_t(d.padded) * d.msaa));
+                TRY(c->depth.alloc(size_t(d.padded) * d.msaa));
+                d.hitIds = c->hitIds.p;
+                d.depth = c->depth.p;
+            } else {
+                d.hitIds = nullptr;
+                d.depth = nullptr;
+            }
+            if (c->target.memory_type == HVVR_MEMORY_CPU && c->target.data) {
+                cpuTargets = true;
+                if (!c->registered) capturable = false; // pageable copies cannot be captured
+            }
+            cams.push_back(c);
+        }
+    }
+    if (cams.empty()) return HVVR_OK;
+    TRY(batchResources(b));
+
+    std::vector<uint64_t> key;
+    for (const hvvr_camera* c : cams) {
+        const uint64_t k[] = {uint64_t(uintptr_t(c)), c->setupGen, c->msaa, uint64_t(uintptr_t(c->dev.hitIds)),
+                              uint64_t(uintptr_t(c->target.data)), c->target.memory_type, c->target.stride,
+                              uint64_t(uintptr_t(c->registered))};
+        key.insert(key.end(), k, k + 8);
+    }
+    if (key != b->layoutKey) {
+        b->views.clear();
+        b->tiles = b->blocks = 0;
+        uint32_t rateTiles[6] = {};
+        std::vector<uint32_t> blockView;
+        for (const hvvr_camera* c : cams) rateTiles[rateIndex(c->msaa)] += c->dev.tiles;
+        for (uint32_t i = 0; i < cams.size(); i++) {
+            hvvr_camera* c = cams[i];
+            b->views.push_back(hvvr_batch::View{c, b->tiles, b->blocks});
+            blockView.insert(blockView.end(), c->dev.blocks, i);
+            b->tiles += c->dev.tiles;
+            b->blocks += c->dev.blocks;
+        }
+        uint32_t run = 0;
+        for (int r = 0; r < 6; r++) {
+            b->rateTiles[r] = rateTiles[r];
+            b->rateStart[r] = run;
+            run += rateTiles[r];
+        }
+        TRY(b->blockView.upload(blockView.data(), blockView.size(), st));
+        TRY(b->order.alloc(b->tiles));
+        TRY(b->viewsDev.alloc(b->views.size()));
+        if (b->hostViewsCap < b->views.size()) {
+            for (int k = 0; k < 2; k++) {
+                if (b->hostViewsUsed[k]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[k]));
+                if (b->hostViews[k]) cudaFreeHost(b->hostViews[k]);
+                b->hostViews[k] = nullptr;
+                b->hostViewsUsed[k] = false;
+            }
+            b->hostViewsCap = 0;
+            for (int k = 0; k < 2; k++)
+                CUDA_TRY(cudaMallocHost((void**)&b->hostViews[k], b->views.size() * sizeof(ViewDev)));
+            b->hostViewsCap = b->views.size();
+        }
+        b->layoutKey = key;
+        b->costValid = false;
+        dropGraph(b);
+    }
+    b->fpStrict = strict;
+
+    // this frame's view table (transforms, scene pointers), staged in pinned memory that the
+    // frame before last has finished reading
+    const int slot = b->hostSlot;
+    b->hostSlot ^= 1;
+    if (b->hostViewsUsed[slot]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[slot]));
+    ViewDev* hv = b->hostViews[slot];
+    for (size_t i = 0; i < b->views.size(); i++) {
+        const hvvr_camera* c = b->views[i].cam;
+        const SceneDev& sc = c->rc->scene;
+        const CameraDev& d = c->dev;
+        ViewDev v{};
+        v.M = transformToMatrix(c->xf);
+        v.env = sc.env;
+        v.nodes = sc.nodes;
+        v.tris = sc.tris;
+        v.triShade = sc.triShade;
+        v.verts = sc.verts;
+        v.materials = sc.materials;
+        v.tileRays = d.tileRays;
+        v.blockRays = d.blockRays;
+        v.beams = d.beams;
+        v.blockStacks = d.blockStacks;
+        v.blockSizes = d.blockSizes;
+        v.tileLists = d.tileLists;
+        v.tileCost = d.tileCost;
+        v.colors = d.colors;
+        v.hitIds = d.hitIds;
+        v.depth = d.depth;
+        v.tileStart = b->views[i].tileStart;
+        v.blockStart = b->views[i].blockStart;
+        v.msaa = c->msaa;
+        v.rateIdx = rateIndex(c->msaa);
+        hv[i] = v;
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->viewsDev.p, hv, b->views.size() * sizeof(ViewDev), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaEventRecord(b->hostViewsEv[slot], st));
+    b->hostViewsUsed[slot] = true;
+
+    FrameDev fr;
+    fr.views = b->viewsDev.p;
+    fr.blockView = b->blockView.p;
+    fr.viewCount = uint32_t(b->views.size());
+    fr.tiles = b->tiles;
+    fr.blocks = b->blocks;
+    fr.pool = b->pool.p;
+    fr.chunkNext = b->chunkNext.p;
+    fr.poolChunks = b->poolChunks;
+    fr.counters = b->counters.p;
+    fr.order = b->order.p;
+    if (b->cfg.use_graph && b->costValid && capturable) {
+        std::vector<uint64_t> gkey = b->layoutKey;
+        const uint64_t extra[] = {b->cfg.tile_cull_warps, b->cfg.heavy_divisor, b->poolChunks, strict ? 1u : 0u,
+                                  uint64_t(uintptr_t(st))};
+        gkey.insert(gkey.end(), extra, extra + 5);
+        if (!b->graph || gkey != b->graphKey) {
+            dropGraph(b);
+            CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            const int r = enqueueFrame(b, fr, st, false);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (r != HVVR_OK) {
+                if (g) cudaGraphDestroy(g);
+                return r;
+            }
+            CUDA_TRY(e);
+            const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) b->graph = nullptr;
+            CUDA_TRY(ie);
+            b->graphKey = gkey;
+        }
+        CUDA_TRY(cudaEventRecord(b->ev[0], st));
+        CUDA_TRY(cudaGraphLaunch(b->graph, st));
+        CUDA_TRY(cudaEventRecord(b->ev[5], st));
+        b->stageTimes = false;
+    } else {
+        TRY(enqueueFrame(b, fr, st, true));
+        b->stageTimes = true;
+    }
+    for (hvvr_camera* c : cams) {
+        c->lastBatch = b;
+        c->rendered = true;
+    }
+    b->costValid = true; // the next frame schedules its tiles by this frame's visit counts
+    b->counterValid = true;
+    if (cpuTargets) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        TRY(checkStatus(b));
     }
     return HVVR_OK;
 }
@@ -573,10 +833,15 @@ int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out) {
 
 int hvvr_raycaster_destroy(hvvr_raycaster* rc) {
     if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    cudaSetDevice(rc->spec.device);
     cudaStreamSynchronize(rc->stream);
     cudaDeviceSynchronize();
+    for (hvvr_batch* b : rc->batches) {
+        b->detached = true;
+        b->rcs.clear();
+    }
     for (auto& c : rc->cameras) releaseCamera(c.get());
-    if (rc->forkEv) cudaEventDestroy(rc->forkEv);
+    if (rc->own) releaseBatch(rc->own.get());
     cudaStreamDestroy(rc->stream);
     delete rc;
     return HVVR_OK;
@@ -591,40 +856,16 @@ int hvvr_raycaster_set_scene_dirty(hvvr_raycaster* rc) {
 int hvvr_raycaster_render(hvvr_raycaster* rc, double elapsed_time, void* stream) {
     (void)elapsed_time;
     if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
-    CUDA_TRY(cudaSetDevice(rc->spec.device));
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : rc->stream;
-    if (rc->sceneDirty) {
-        TRY(uploadScene(rc, st));
-        rc->sceneDirty = false;
-        rc->refitDirty = true;
+    if (!rc->own) {
+        rc->own = std::make_unique<hvvr_batch>();
+        hvvr_batch* b = rc->own.get();
+        b->rcs.push_back(rc);
+        b->internal = true;
+        batchConfigDefault(&b->cfg);
+        b->cfg.use_graph = 0; // per-stage timings stay available
+        if (rc->spec.tri_index_capacity) b->cfg.tri_index_capacity = rc->spec.tri_index_capacity;
     }
-    if (rc->scene.nodeCount == 0) return HVVR_OK;
-    if (rc->refitDirty) {
-        CUDA_TRY(launchRefit(rc->scene, st));
-        rc->refitDirty = false;
-    }
-    for (auto& c : rc->cameras) {
-        if (!c->enabled || c->samples.empty()) continue;
-        if (!rc->msaaUploaded[c->msaa]) {
-            float off[64];
-            msaaOffsets(c->msaa, off);
-            CUDA_TRY(uploadMsaaTable(c->msaa, off, st));
-            rc->msaaUploaded[c->msaa] = true;
-        }
-    }
-    if (!rc->forkEv) CUDA_TRY(cudaEventCreateWithFlags(&rc->forkEv, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventRecord(rc->forkEv, st));
-    bool cpuTargets = false;
-    for (auto& c : rc->cameras) {
-        if (!c->enabled || c->samples.empty()) continue;
-        TRY(renderCamera(rc, c.get(), st));
-        if (c->target.memory_type == HVVR_MEMORY_CPU) cpuTargets = true;
-    }
-    if (cpuTargets) {
-        CUDA_TRY(cudaStreamSynchronize(st));
-        TRY(checkStatus(rc));
-    }
-    return HVVR_OK;
+    return renderBatch(rc->own.get(), stream ? static_cast<cudaStream_t>(stream) : rc->stream);
 }
 
 int hvvr_raycaster_synchronize(hvvr_raycaster* rc) {
@@ -632,7 +873,167 @@ int hvvr_raycaster_synchronize(hvvr_raycaster* rc) {
     CUDA_TRY(cudaSetDevice(rc->spec.device));
     CUDA_TRY(cudaStreamSynchronize(rc->stream));
     CUDA_TRY(cudaDeviceSynchronize());
-    return checkStatus(rc);
+    return checkStatus(rc->own.get());
+}
+
+void hvvr_batch_config_default(hvvr_batch_config* cfg) {
+    if (cfg) batchConfigDefault(cfg);
+}
+
+int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,
+                      hvvr_batch** out) {
+    if (!out) return fail(HVVR_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!raycasters || count == 0) return fail(HVVR_ERR_INVALID, "no raycasters");
+    for (uint32_t i = 0; i < count; i++) {
+        if (!raycasters[i]) return fail(HVVR_ERR_INVALID, "NULL raycaster %u", i);
+        for (uint32_t k = 0; k < i; k++)
+            if (raycasters[k] == raycasters[i]) return fail(HVVR_ERR_INVALID, "raycaster %u listed twice", i);
+        if (raycasters[i]->spec.device != raycasters[0]->spec.device)
+            return fail(HVVR_ERR_INVALID, "batched raycasters must share one device");
+        if (raycasters[i]->spec.fp_mode != raycasters[0]->spec.fp_mode)
+            return fail(HVVR_ERR_INVALID, "batched raycasters must share one fp_mode");
+    }
+    auto b = std::make_unique<hvvr_batch>();
+    batchConfigDefault(&b->cfg);
+    if (cfg) {
+        b->cfg = *cfg;
+        TRY(checkConfig(b->cfg));
+    }
+    b->rcs.assign(raycasters, raycasters + count);
+    for (hvvr_raycaster* rc : b->rcs) rc->batches.push_back(b.get());
+    *out = b.release();
+    return HVVR_OK;
+}
+
+int hvvr_batch_destroy(hvvr_batch* b) {
+    if (!b || b->internal) return fail(HVVR_ERR_INVALID, "not a batch");
+    if (!b->rcs.empty()) cudaSetDevice(b->rcs[0]->spec.device);
+    cudaDeviceSynchronize();
+    for (hvvr_raycaster* rc : b->rcs) {
+        rc->batches.erase(std::remove(rc->batches.begin(), rc->batches.end(), b), rc->batches.end());
+        for (auto& c : rc->cameras)
+            if (c->lastBatch == b) c->lastBatch = nullptr;
+    }
+    releaseBatch(b);
+    delete b;
+    return HVVR_OK;
+}
+
+int hvvr_batch_render(hvvr_batch* b, double elapsed_time, void* stream) {
+    (void)elapsed_time;
+    if (!b || b->internal) return fail(HVVR_ERR_INVALID, "not a batch");
+    if (b->detached || b->rcs.empty()) return fail(HVVR_ERR_STATE, "a raycaster of this batch was destroyed");
+    return renderBatch(b, stream ? static_cast<cudaStream_t>(stream) : b->rcs[0]->stream);
+}
+
+int hvvr_batch_synchronize(hvvr_batch* b) {
+    if (!b || b->internal) return fail(HVVR_ERR_INVALID, "not a batch");
+    if (b->detached || b->rcs.empty()) return fail(HVVR_ERR_STATE, "a raycaster of this batch was destroyed");
+    CUDA_TRY(cudaSetDevice(b->rcs[0]->spec.device));
+    CUDA_TRY(cudaDeviceSynchronize());
+    return checkStatus(b);
+}
+
+int hvvr_batch_get_config(const hvvr_batch* b, hvvr_batch_config* cfg) {
+    if (!b || !cfg) return fail(HVVR_ERR_INVALID, "NULL argument");
+    *cfg = b->cfg;
+    return HVVR_OK;
+}
+
+int hvvr_batch_set_config(hvvr_batch* b, const hvvr_batch_config* cfg) {
+    if (!b || !cfg || b->internal) return fail(HVVR_ERR_INVALID, "NULL argument");
+    TRY(checkConfig(*cfg));
+    b->cfg = *cfg;
+    return HVVR_OK;
+}
+
+int hvvr_batch_read_timings(const hvvr_batch* b, float* ms5) {
+    if (!b || !ms5) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (!b->counterValid) return fail(HVVR_ERR_STATE, "the batch has not rendered a frame");
+    CUDA_TRY(cudaEventSynchronize(b->ev[5]));
+    CUDA_TRY(cudaEventElapsedTime(&ms5[0], b->ev[0], b->ev[5]));
+    for (int i = 1; i < 5; i++) {
+        ms5[i] = 0.0f;
+        if (b->stageTimes) CUDA_TRY(cudaEventElapsedTime(&ms5[i], b->ev[i == 4 ? 3 : i - 1], b->ev[i == 4 ? 5 : i]));
+    }
+    return HVVR_OK;
+}
+
+namespace {
+int kernelTimes(const hvvr_batch* b, float* ms4) {
+    if (!b || !b->counterValid) return fail(HVVR_ERR_STATE, "no frame rendered");
+    if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was a graph replay (no per-launch events)");
+    CUDA_TRY(cudaEventSynchronize(b->ev[5]));
+    float cull = 0.0f, isect = 0.0f, t = 0.0f;
+    for (int k = 0; k < 12; k++) {
+        if (!b->kevUsed[k]) continue;
+        CUDA_TRY(cudaEventElapsedTime(&t, b->kev[k][0], b->kev[k][1]));
+        cull += t;
+        CUDA_TRY(cudaEventElapsedTime(&t, b->kev[k][1], b->kev[k][2]));
+        isect += t;
+    }
+    ms4[0] = cull;
+    ms4[1] = isect;
+    CUDA_TRY(cudaEventElapsedTime(&ms4[2], b->ev[0], b->ev[1]));
+    CUDA_TRY(cudaEventElapsedTime(&ms4[3], b->ev[3], b->ev[4]));
+    return HVVR_OK;
+}
+} // namespace
+
+int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4) {
+    if (!rc || !ms4) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return kernelTimes(rc->own.get(), ms4);
+}
+
+int hvvr_batch_read_kernel_times(const hvvr_batch* b, float* ms4) {
+    if (!ms4) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return kernelTimes(b, ms4);
+}
+
+int hvvr_batch_autotune(hvvr_batch* b, uint32_t frames, hvvr_batch_config* out) {
+    if (!b || b->internal) return fail(HVVR_ERR_INVALID, "not a batch");
+    if (b->detached || b->rcs.empty()) return fail(HVVR_ERR_STATE, "a raycaster of this batch was destroyed");
+    if (frames == 0) frames = 5;
+    cudaStream_t st = b->rcs[0]->stream;
+    const hvvr_batch_config base = b->cfg;
+    hvvr_batch_config best = base;
+    float bestMs = INFINITY;
+    uint32_t maxChunks = 0;
+    for (uint32_t warps : {2u, 4u, 8u}) {
+        for (uint32_t div : {0u, 16u, 8u, 4u}) {
+            b->cfg = base;
+            b->cfg.tile_cull_warps = warps;
+            b->cfg.heavy_divisor = div;
+            std::vector<float> ms;
+            for (uint32_t f = 0; f <= frames; f++) {
+                int r = renderBatch(b, st);
+                if (r == HVVR_OK && cudaStreamSynchronize(st) != cudaSuccess) r = fail(HVVR_ERR_CUDA, "frame failed");
+                if (r == HVVR_OK) r = checkStatus(b);
+                if (r != HVVR_OK) {
+                    b->cfg = base;
+                    return r;
+                }
+                maxChunks = std::max(maxChunks, b->hostCounters[0]);
+                float t = 0.0f;
+                CUDA_TRY(cudaEventElapsedTime(&t, b->ev[0], b->ev[5]));
+                if (f > 0) ms.push_back(t);
+            }
+            std::sort(ms.begin(), ms.end());
+            const float med = ms[ms.size() / 2];
+            if (med < bestMs) {
+                bestMs = med;
+                best = b->cfg;
+            }
+        }
+    }
+    const uint64_t unit = 1ull << 20;
+    const uint64_t want = (uint64_t(maxChunks) * kChunk * 5 / 4 + unit - 1) / unit * unit;
+    best.tri_index_capacity = std::max<uint64_t>(want, unit);
+    best.frame_ms = bestMs;
+    b->cfg = best;
+    if (out) *out = best;
+    return HVVR_OK;
 }
 
 int hvvr_model_create(hvvr_raycaster* rc, const hvvr_mesh_data* mesh, hvvr_model** out) {
@@ -891,13 +1292,15 @@ int hvvr_camera_read_tile_lists(const hvvr_camera* cam, uint32_t* counts, uint32
     if (!indices) return HVVR_OK;
     if (capacity < sum) return fail(HVVR_ERR_OVERFLOW, "capacity %llu < %llu entries", (unsigned long long)capacity,
                                     (unsigned long long)sum);
+    const hvvr_batch* b = cam->lastBatch;
+    if (!b) return fail(HVVR_ERR_STATE, "the batch that rendered this camera's lists was destroyed");
     uint32_t used = 0;
-    CUDA_TRY(cudaMemcpy(&used, d.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    used = std::min(used, d.poolChunks);
+    CUDA_TRY(cudaMemcpy(&used, b->counters.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    used = std::min(used, b->poolChunks);
     std::vector<uint32_t> pool(size_t(used) * kChunk), next(used);
     if (used) {
-        CUDA_TRY(cudaMemcpy(pool.data(), d.pool, pool.size() * 4, cudaMemcpyDeviceToHost));
-        CUDA_TRY(cudaMemcpy(next.data(), d.chunkNext, next.size() * 4, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(pool.data(), b->pool.p, pool.size() * 4, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(next.data(), b->chunkNext.p, next.size() * 4, cudaMemcpyDeviceToHost));
     }
     uint64_t w = 0;
     for (uint32_t t = 0; t < d.tiles; t++) {
@@ -1001,9 +1404,21 @@ int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9) {
 int hvvr_camera_read_timings(const hvvr_camera* cam, float* ms6) {
     TRY(requireRendered(cam));
     if (!ms6) return fail(HVVR_ERR_INVALID, "NULL output");
+    const hvvr_batch* b = cam->lastBatch;
+    if (!b) return fail(HVVR_ERR_STATE, "the batch that rendered this camera was destroyed");
     ms6[0] = 0.0f;
-    for (int i = 1; i < 5; i++) CUDA_TRY(cudaEventElapsedTime(&ms6[i], cam->ev[i - 1], cam->ev[i]));
-    CUDA_TRY(cudaEventElapsedTime(&ms6[5], cam->ev[0], cam->ev[5]));
+    for (int i = 1; i < 5; i++) {
+        ms6[i] = 0.0f;
+        if (b->stageTimes) CUDA_TRY(cudaEventElapsedTime(&ms6[i], b->ev[i - 1], b->ev[i]));
+    }
+    CUDA_TRY(cudaEventElapsedTime(&ms6[5], b->ev[0], b->ev[5]));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_tile_costs(const hvvr_camera* cam, uint32_t* visits) {
+    TRY(requireRendered(cam));
+    if (!visits) return fail(HVVR_ERR_INVALID, "NULL output");
+    CUDA_TRY(cudaMemcpy(visits, cam->dev.tileCost, size_t(cam->dev.tiles) * 4, cudaMemcpyDeviceToHost));
     return HVVR_OK;
 }
 

@@ -31,6 +31,16 @@ template <> struct RateIndex<8> { static constexpr int v = 3; };
 template <> struct RateIndex<16> { static constexpr int v = 4; };
 template <> struct RateIndex<32> { static constexpr int v = 5; };
 
+// Loads a pointer field of the view table where it is used. The asm is volatile so the
+// compiler re-issues the (L1-resident) load instead of keeping ten 64-bit pointers live in
+// registers across the tile loop, which costs two CTAs per SM of occupancy.
+template <class T>
+__device__ __forceinline__ T* viewPtr(T* const& field) {
+    uint64_t v;
+    asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(&field));
+    return reinterpret_cast<T*>(v);
+}
+
 struct TriGeom {
     F3 v0, e0, e1;
 };
@@ -230,21 +240,26 @@ struct ShadeSmem {
     uint32_t warpCount[4];
 };
 
+// resident CTAs per SM the register allocation must allow (7 = 72 registers per thread)
+template <uint32_t N> struct MinCtas { static constexpr int v = N <= 8 ? 7 : (N == 16 ? 5 : 4); };
+
 template <uint32_t N, bool FMA>
-__global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
-    const float4* __restrict__ tris, const uint4* __restrict__ triShade, const float4* __restrict__ verts,
-    const float4* __restrict__ materials, const Rays4* __restrict__ tileRays, const float4* __restrict__ beams,
-    const TileList* __restrict__ lists, const uint32_t* __restrict__ pool, const uint32_t* __restrict__ chunkNext,
-    Mat4 M, LightEnvDev env, uint32_t* __restrict__ colors, uint32_t* __restrict__ hitOut,
-    float* __restrict__ depthOut, const uint32_t* __restrict__ order, uint32_t first) {
+__global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel(FrameDev fr, const uint32_t* __restrict__ order,
+                                                                  uint32_t first) {
     __shared__ ShadeSmem sm;
-    const uint32_t tile = order ? order[first + blockIdx.x] : blockIdx.x;
+    __shared__ LightEnvDev env;
+    __shared__ Mat4 M;
+    const uint32_t gt = order ? order[first + blockIdx.x] : first + blockIdx.x;
+    const ViewDev& V = fr.views[fr.viewCount == 1 ? 0u : __ldg(fr.blockView + gt / kTilesPerBlock)];
+    const uint32_t tile = gt - V.tileStart;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sid = tile * kTileSize + tid;
-    const TileList L = lists[tile];
+    const TileList L = V.tileLists[tile];
     if (L.count == 0) {
         // ClearEmptyKernel (resolve.cu:527-542)
-        colors[sid] = 0xFF000000u;
+        V.colors[sid] = 0xFF000000u;
+        uint32_t* __restrict__ hitOut = V.hitIds;
+        float* __restrict__ depthOut = V.depth;
         if (hitOut) {
 #pragma unroll
             for (uint32_t i = 0; i < N; i++) {
@@ -255,10 +270,14 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
         return;
     }
     const int rate = RateIndex<N>::v;
+    for (uint32_t i = tid; i < sizeof(LightEnvDev) / 4; i += kTileSize)
+        reinterpret_cast<uint32_t*>(&env)[i] = reinterpret_cast<const uint32_t*>(&V.env)[i];
+    if (tid < 16) reinterpret_cast<float*>(&M)[tid] = reinterpret_cast<const float*>(&V.M)[tid];
+    __syncthreads();
     // world-space tile rays (the SimpleRayFrustum of transformHierarchyCameraToWorld) and
     // FrustumPlanes (prim_tests.h:22-28)
     if (tid < 8) {
-        const Rays4& cr = tileRays[tile];
+        const Rays4& cr = V.tileRays[tile];
         const uint32_t i = tid & 3u;
         if (tid < 4) {
             const F3 o = xformPoint(M, f3(cr.o[i][0], cr.o[i][1], cr.o[i][2]));
@@ -278,6 +297,7 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
     }
     const F3 camPos = f3(M.m[3][0], M.m[3][1], M.m[3][2]);
     // this thread's beam, rotated to world space (GetDirectionalSample3D, gpu_samples.h:78-82)
+    const float4* __restrict__ beams = V.beams;
     const float4 b0 = __ldg(beams + 3 * size_t(sid) + 0);
     const float4 b1 = __ldg(beams + 3 * size_t(sid) + 1);
     const float4 b2 = __ldg(beams + 3 * size_t(sid) + 2);
@@ -300,14 +320,14 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
     uint32_t remaining = L.count;
     while (remaining > 0) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
-        const uint32_t nextChunk = chunkNext[chunk];
+        const uint32_t nextChunk = fr.chunkNext[chunk];
         bool keep = false;
         uint32_t idx = 0;
         float t = 0.0f, nlen = 0.0f;
         F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0);
         if (tid < n) {
-            idx = pool[size_t(chunk) * kChunk + tid];
-            const TriGeom tri = loadTri(tris, idx);
+            idx = fr.pool[size_t(chunk) * kChunk + tid];
+            const TriGeom tri = loadTri(viewPtr(V.tris), idx);
             // FrustumPlanes::test
             bool in = true;
 #pragma unroll
@@ -395,7 +415,8 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
         chunk = nextChunk;
     }
 
-    if (hitOut) {
+    if (uint32_t* hitOut = viewPtr(V.hitIds)) {
+        float* depthOut = viewPtr(V.depth);
 #pragma unroll
         for (uint32_t i = 0; i < N; i++) {
             hitOut[size_t(sid) * N + i] = hit[i];
@@ -443,11 +464,13 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
             cax = cax + a.x * inv;
             cay = cay + a.y * inv;
         }
-        const TriGeom tri = loadTri(tris, triIndex);
+        const TriGeom tri = loadTri(viewPtr(V.tris), triIndex);
         const F3 v0r = camPos - tri.v0;
         const TriThread th = threadSetup(tri.e0, tri.e1, v0r, c, du, dv);
         const F3 bc = calcUVW<FMA>(th, cax, cay);
-        const uint4 ts = __ldg(triShade + triIndex);
+        const uint4 ts = __ldg(viewPtr(V.triShade) + triIndex);
+        const float4* __restrict__ verts = viewPtr(V.verts);
+        const float4* __restrict__ materials = viewPtr(V.materials);
         const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
         const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
         const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
@@ -469,24 +492,14 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeKernel(
         rz = rz + col.z * pc;
     }
     const float sN = 1.0f / float(N);
-    colors[sid] = packColor(f3(aces(rx * sN), aces(ry * sN), aces(rz * sN)));
+    viewPtr(V.colors)[sid] = packColor(f3(aces(rx * sN), aces(ry * sN), aces(rz * sN)));
 }
 
 template <uint32_t N>
-cudaError_t launchRate(const SceneDev& s, const CameraDev& c, const FrameParams& f, const uint32_t* order,
-                       uint32_t first, uint32_t count, cudaStream_t st) {
-    uint32_t* hitOut = f.capture ? c.hitIds : nullptr;
-    float* depthOut = f.capture ? c.depth : nullptr;
-    if (f.fpStrict)
-        intersectShadeKernel<N, false><<<count, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
-                                                                    c.tileRays, c.beams, c.tileLists, c.pool,
-                                                                    c.chunkNext, f.cameraToWorld, s.env, c.colors,
-                                                                    hitOut, depthOut, order, first);
-    else
-        intersectShadeKernel<N, true><<<count, kTileSize, 0, st>>>(s.tris, s.triShade, s.verts, s.materials,
-                                                                   c.tileRays, c.beams, c.tileLists, c.pool,
-                                                                   c.chunkNext, f.cameraToWorld, s.env, c.colors,
-                                                                   hitOut, depthOut, order, first);
+cudaError_t launchRate(const FrameDev& fr, bool fpStrict, const uint32_t* order, uint32_t first, uint32_t count,
+                       cudaStream_t st) {
+    if (fpStrict) intersectShadeKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
+    else intersectShadeKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
     return cudaGetLastError();
 }
 
@@ -515,22 +528,18 @@ __global__ void remapKernel(const uint32_t* __restrict__ src, const int32_t* __r
 
 } // namespace
 
-cudaError_t launchIntersectShadeRange(const SceneDev& s, const CameraDev& c, const FrameParams& f,
-                                      const uint32_t* order, uint32_t first, uint32_t count, cudaStream_t st) {
+cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, const uint32_t* order,
+                                 uint32_t first, uint32_t count, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
-    switch (c.msaa) {
-    case 1: return launchRate<1>(s, c, f, order, first, count, st);
-    case 2: return launchRate<2>(s, c, f, order, first, count, st);
-    case 4: return launchRate<4>(s, c, f, order, first, count, st);
-    case 8: return launchRate<8>(s, c, f, order, first, count, st);
-    case 16: return launchRate<16>(s, c, f, order, first, count, st);
-    case 32: return launchRate<32>(s, c, f, order, first, count, st);
+    switch (msaa) {
+    case 1: return launchRate<1>(fr, fpStrict, order, first, count, st);
+    case 2: return launchRate<2>(fr, fpStrict, order, first, count, st);
+    case 4: return launchRate<4>(fr, fpStrict, order, first, count, st);
+    case 8: return launchRate<8>(fr, fpStrict, order, first, count, st);
+    case 16: return launchRate<16>(fr, fpStrict, order, first, count, st);
+    case 32: return launchRate<32>(fr, fpStrict, order, first, count, st);
     default: return cudaErrorInvalidValue;
     }
-}
-
-cudaError_t launchIntersectShade(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
-    return launchIntersectShadeRange(s, c, f, nullptr, 0, c.tiles, st);
 }
 
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st) {

@@ -21,7 +21,8 @@
 // is looked up with cudaGetSymbolAddress once per device, on the first call made with that
 // device current. Make that first call on each device before any stream capture starts.
 //
-// The cull itself is the unchanged tileCullKernel (traverse.cu) pointed at the scratch pool;
+// The cull itself is the tileCullKernel of the render path (traverse.cu), given a one-view
+// table written into the scratch by a one-thread kernel and pointed at the scratch pool;
 // a one-block scan and a per-tile gather then copy the chunked lists into the caller's
 // flat output in tile order. Nothing here calls cudaMalloc, cudaFree or an allocating library.
 #include <mutex>
@@ -39,9 +40,12 @@ constexpr uint32_t kMaxTiles = 65536;                  // 4,194,304 padded sampl
 constexpr uint32_t kMaxChunks = 61440;                 // kMaxChunks * kChunk entries
 constexpr uint64_t kMaxEntries = uint64_t(kMaxChunks) * kChunk; // 7,864,320 entries (30 MiB)
 // word layout of the scratch array
-constexpr size_t kOffCounters = 0;                     // [0] chunk allocator, [1] status, [2..3] total (u64)
-constexpr size_t kOffLists = 64;                       // TileList[kMaxTiles]
-constexpr size_t kOffNext = kOffLists + 2 * size_t(kMaxTiles);
+constexpr size_t kOffCounters = 0;                     // [0] chunk allocator, [1] status, [2..3] total (u64), [4] queue
+constexpr size_t kOffView = 64;                        // the one-view table of the cull (ViewDev)
+constexpr size_t kViewWords = (sizeof(ViewDev) + 255) / 256 * 64;
+constexpr size_t kOffLists = kOffView + kViewWords;    // TileList[kMaxTiles]
+constexpr size_t kOffCost = kOffLists + 2 * size_t(kMaxTiles); // per-tile visit counts (written, unused)
+constexpr size_t kOffNext = kOffCost + kMaxTiles;
 constexpr size_t kOffOffsets = kOffNext + kMaxChunks;  // exclusive prefix of counts, kMaxTiles + 1 words (u32 lo)
 constexpr size_t kOffPool = (kOffOffsets + kMaxTiles + 1 + 63) / 64 * 64;
 constexpr size_t kScratchWords = kOffPool + size_t(kMaxChunks) * kChunk;
@@ -151,29 +155,32 @@ extern "C" int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* 
         scratch = gScratchAddr[dev];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    SceneDev s;
-    s.nodes = static_cast<Node*>(const_cast<void*>(args->nodes));
-    s.nodeCount = args->node_count;
-    CameraDev c;
-    c.tiles = args->tile_count;
-    c.blocks = args->tile_count / kTilesPerBlock;
-    c.tileRays = const_cast<Rays4*>(static_cast<const Rays4*>(args->tile_rays));
-    c.blockStacks = const_cast<StackEntry*>(static_cast<const StackEntry*>(args->block_stacks));
-    c.blockSizes = const_cast<uint32_t*>(args->block_sizes);
-    c.tileLists = reinterpret_cast<TileList*>(scratch + kOffLists);
-    c.pool = scratch + kOffPool;
-    c.chunkNext = scratch + kOffNext;
-    c.poolChunks = kMaxChunks;
-    c.counters = scratch + kOffCounters;
-    FrameParams f;
-    f.cameraToWorld = transformToMatrix(args->camera_to_world);
-    f.fpStrict = 0;
-    f.capture = 0;
-    if ((e = cudaMemsetAsync(scratch + kOffCounters, 0, 4 * sizeof(uint32_t), st)) != cudaSuccess)
+    const uint32_t tiles = args->tile_count;
+    ViewDev v{};
+    v.M = transformToMatrix(args->camera_to_world);
+    v.nodes = static_cast<const Node*>(args->nodes);
+    v.tileRays = static_cast<const Rays4*>(args->tile_rays);
+    v.blockStacks = const_cast<StackEntry*>(static_cast<const StackEntry*>(args->block_stacks));
+    v.blockSizes = const_cast<uint32_t*>(args->block_sizes);
+    v.tileLists = reinterpret_cast<TileList*>(scratch + kOffLists);
+    v.tileCost = scratch + kOffCost;
+    FrameDev fr;
+    fr.views = reinterpret_cast<const ViewDev*>(scratch + kOffView);
+    fr.viewCount = 1;
+    fr.tiles = tiles;
+    fr.blocks = tiles / kTilesPerBlock;
+    fr.pool = scratch + kOffPool;
+    fr.chunkNext = scratch + kOffNext;
+    fr.poolChunks = kMaxChunks;
+    fr.counters = scratch + kOffCounters;
+    if ((e = cudaMemsetAsync(scratch + kOffCounters, 0, 8 * sizeof(uint32_t), st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "clearing the scratch counters failed", e);
-    if ((e = launchTileCull(s, c, f, st)) != cudaSuccess) return failStatic(HVVR_ERR_CUDA, "tile cull launch failed", e);
-    scanCounts<<<1, 1024, 0, st>>>(scratch, c.tiles);
-    gatherLists<<<(c.tiles + 7) / 8, 256, 0, st>>>(scratch, c.tiles, counts, indices, capacity);
+    if ((e = launchWriteView(v, reinterpret_cast<ViewDev*>(scratch + kOffView), st)) != cudaSuccess)
+        return failStatic(HVVR_ERR_CUDA, "view setup launch failed", e);
+    if ((e = launchTileCull(fr, nullptr, 0, tiles, scratch + kOffCounters + 4, 4, st)) != cudaSuccess)
+        return failStatic(HVVR_ERR_CUDA, "tile cull launch failed", e);
+    scanCounts<<<1, 1024, 0, st>>>(scratch, tiles);
+    gatherLists<<<(tiles + 7) / 8, 256, 0, st>>>(scratch, tiles, counts, indices, capacity);
     if ((e = cudaGetLastError()) != cudaSuccess) return failStatic(HVVR_ERR_CUDA, "gather launch failed", e);
     uint32_t status[4] = {0, 0, 0, 0};
     if ((e = cudaMemcpyAsync(status, scratch + kOffCounters, sizeof(status), cudaMemcpyDeviceToHost, st)) != cudaSuccess)

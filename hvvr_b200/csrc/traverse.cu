@@ -269,17 +269,25 @@ struct BlockSmem {
     uint32_t sNode[kBlockStack];
 };
 
-__global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(const Node* __restrict__ nodes,
-                                                                    const Rays4* __restrict__ blockRays,
-                                                                    uint32_t blocks, Mat4 M,
-                                                                    StackEntry* __restrict__ out,
-                                                                    uint32_t* __restrict__ sizes) {
+// the view of a global block (blocks of one view are consecutive)
+__device__ __forceinline__ const ViewDev& viewOfBlock(const ViewDev* __restrict__ views,
+                                                      const uint32_t* __restrict__ blockView, uint32_t viewCount,
+                                                      uint32_t blk) {
+    return views[viewCount == 1 ? 0u : __ldg(blockView + blk)];
+}
+
+__global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(FrameDev fr) {
     __shared__ BlockSmem smem[kBlockWarps];
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-    const uint32_t blk = blockIdx.x * kBlockWarps + warp;
-    if (blk >= blocks) return;
+    const uint32_t gblk = blockIdx.x * kBlockWarps + warp;
+    if (gblk >= fr.blocks) return;
+    const ViewDev& V = viewOfBlock(fr.views, fr.blockView, fr.viewCount, gblk);
+    const uint32_t blk = gblk - V.blockStart;
+    const Node* __restrict__ nodes = V.nodes;
+    StackEntry* __restrict__ out = V.blockStacks;
+    uint32_t* __restrict__ sizes = V.blockSizes;
     BlockSmem& s = smem[warp];
-    buildFrustum(blockRays[blk], M, s.f);
+    buildFrustum(V.blockRays[blk], V.M, s.f);
     if (s.f.degenerate) {
         if (lane == 0) sizes[blk] = 0;
         return;
@@ -341,7 +349,6 @@ __global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(const Node* 
     if (lane == 0) sizes[blk] = stackSize;
 }
 
-constexpr int kTileWarps = 4;
 
 struct TileSmem {
     SmemFrustum f;
@@ -418,37 +425,32 @@ struct Emitter {
 };
 
 struct TileCullArgs {
-    const Node* nodes;
-    const Rays4* tileRays;
-    uint32_t tiles;
-    Mat4 M;
-    const StackEntry* blockStacks;
-    const uint32_t* blockSizes;
-    TileList* lists;
+    const ViewDev* views;
+    const uint32_t* blockView;
+    uint32_t viewCount;
     uint32_t* pool;
     uint32_t* chunkNext;
     uint32_t poolChunks;
-    uint32_t* counters;   // [0] chunk allocator, [1] status
-    const uint32_t* order; // tile order for the queue (nullptr = natural order)
-    uint32_t first;       // this launch culls order[first, first + count)
+    uint32_t* counters;    // [0] chunk allocator, [1] status
+    const uint32_t* order; // global tile order for the queue (nullptr = natural order)
+    uint32_t first;        // this launch culls order[first, first + count)
     uint32_t count;
-    uint32_t* queue;      // work-queue head of this launch, zero at launch
-    uint32_t* cost;       // node visits per tile, written for next frame's order (may be nullptr)
+    uint32_t* queue;       // work-queue head of this launch, zero at launch
 };
 
-// traverseTiles for one tile; returns the number of node visits
-__device__ uint32_t cullTile(const TileCullArgs& a, uint32_t tile, TileSmem& s) {
+// traverseTiles for one tile of view V (tile = view-local index); returns the node visits
+__device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t tile, TileSmem& s) {
     const uint32_t lane = laneId();
-    const Node* __restrict__ nodes = a.nodes;
+    const Node* __restrict__ nodes = V.nodes;
     const uint32_t blk = tile / kTilesPerBlock;
-    const uint32_t stackSize = a.blockSizes[blk];
-    buildFrustum(a.tileRays[tile], a.M, s.f);
+    const uint32_t stackSize = V.blockSizes[blk];
+    buildFrustum(V.tileRays[tile], V.M, s.f);
     if (stackSize == 0 || s.f.degenerate) {
-        if (lane == 0) a.lists[tile] = TileList{kNoChunk, 0};
+        if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
         return 0;
     }
     for (uint32_t i = lane; i < stackSize; i += 32) {
-        const StackEntry e = a.blockStacks[size_t(blk) * kBlockStack + i];
+        const StackEntry e = V.blockStacks[size_t(blk) * kBlockStack + i];
         s.tMin[i] = e.tMin;
         s.mask[i] = e.mask;
         s.node[i] = e.node;
@@ -590,15 +592,16 @@ __device__ uint32_t cullTile(const TileCullArgs& a, uint32_t tile, TileSmem& s) 
     if (!em.dead && em.bufCount) em.flush(s.buf);
     if (lane == 0) {
         if (em.prev != kNoChunk) a.chunkNext[em.prev] = kNoChunk;
-        a.lists[tile] = TileList{em.first, em.dead ? em.stored : em.total};
+        V.tileLists[tile] = TileList{em.first, em.dead ? em.stored : em.total};
     }
     return visits;
 }
 
 // Persistent warps pull tiles from a queue (longest-first when an order is given), so a
 // few long horizon tiles overlap with the rest instead of holding a CTA slot each.
-__global__ void __launch_bounds__(kTileWarps * 32) tileCullKernel(TileCullArgs a) {
-    __shared__ TileSmem smem[kTileWarps];
+template <int W>
+__global__ void __launch_bounds__(W * 32) tileCullKernel(TileCullArgs a) {
+    __shared__ TileSmem smem[W];
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     TileSmem& s = smem[warp];
     for (;;) {
@@ -606,81 +609,93 @@ __global__ void __launch_bounds__(kTileWarps * 32) tileCullKernel(TileCullArgs a
         if (lane == 0) w = atomicAdd(a.queue, 1u);
         w = __shfl_sync(kFull, w, 0);
         if (w >= a.count) return;
-        const uint32_t tile = a.order ? a.order[a.first + w] : w;
+        const uint32_t gt = a.order ? a.order[a.first + w] : a.first + w;
+        const ViewDev& V = viewOfBlock(a.views, a.blockView, a.viewCount, gt / kTilesPerBlock);
+        const uint32_t tile = gt - V.tileStart;
         __syncwarp();
-        const uint32_t visits = cullTile(a, tile, s);
-        if (a.cost && lane == 0) a.cost[tile] = visits;
+        const uint32_t visits = cullTile(a, V, tile, s);
+        if (lane == 0) V.tileCost[tile] = visits;
         __syncwarp();
     }
 }
 
-// Orders tiles by descending cost (log2 buckets of last frame's visit counts); one block.
-__global__ void __launch_bounds__(1024) tileOrderKernel(const uint32_t* __restrict__ cost, uint32_t tiles,
-                                                        uint32_t* __restrict__ order) {
-    __shared__ uint32_t hist[33];
-    __shared__ uint32_t start[33];
-    if (threadIdx.x < 33) hist[threadIdx.x] = 0;
+// Orders the global tiles by (rate index ascending, cost descending), cost in log2 buckets
+// of last frame's visit counts. One block; positions within a bucket are in arrival order.
+constexpr uint32_t kOrderBuckets = 6 * 33;
+__global__ void __launch_bounds__(1024) tileOrderKernel(FrameDev fr) {
+    __shared__ uint32_t hist[kOrderBuckets];
+    __shared__ uint32_t start[kOrderBuckets];
+    for (uint32_t b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) hist[b] = 0;
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) atomicAdd(&hist[32 - __clz(cost[t] + 1u)], 1u);
+    auto bucket = [&](uint32_t t) {
+        const ViewDev& V = viewOfBlock(fr.views, fr.blockView, fr.viewCount, t / kTilesPerBlock);
+        const uint32_t c = V.tileCost[t - V.tileStart];
+        return V.rateIdx * 33u + uint32_t(__clz(c + 1u)); // clz falls as the cost grows
+    };
+    for (uint32_t t = threadIdx.x; t < fr.tiles; t += blockDim.x) atomicAdd(&hist[bucket(t)], 1u);
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t run = 0;
-        for (int b = 32; b >= 0; b--) {
+        for (uint32_t b = 0; b < kOrderBuckets; b++) {
             start[b] = run;
             run += hist[b];
         }
     }
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) {
-        const uint32_t pos = atomicAdd(&start[32 - __clz(cost[t] + 1u)], 1u);
-        order[pos] = t;
+    for (uint32_t t = threadIdx.x; t < fr.tiles; t += blockDim.x) fr.order[atomicAdd(&start[bucket(t)], 1u)] = t;
+}
+
+__global__ void writeViewKernel(ViewDev v, ViewDev* dst) { *dst = v; }
+
+template <int W>
+cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, cudaStream_t st) {
+    static int ctasPerSm[64] = {}, sms[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!ctasPerSm[dev]) {
+        cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tileCullKernel<W>, W * 32, 0);
+        if (sms[dev] < 1) sms[dev] = 1;
+        ctasPerSm[dev] = occ < 1 ? 1 : occ;
     }
+    const uint32_t needed = (count + W - 1) / W;
+    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(sms[dev] * ctasPerSm[dev]));
+    tileCullKernel<W><<<grid, W * 32, 0, st>>>(a);
+    return cudaGetLastError();
 }
 
 } // namespace
 
-cudaError_t launchBlockCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
-    if (c.blocks == 0) return cudaSuccess;
-    const uint32_t grid = (c.blocks + kBlockWarps - 1) / kBlockWarps;
-    blockCullKernel<<<grid, kBlockWarps * 32, 0, st>>>(s.nodes, c.blockRays, c.blocks, f.cameraToWorld, c.blockStacks,
-                                                        c.blockSizes);
+cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st) {
+    if (fr.blocks == 0) return cudaSuccess;
+    blockCullKernel<<<(fr.blocks + kBlockWarps - 1) / kBlockWarps, kBlockWarps * 32, 0, st>>>(fr);
     return cudaGetLastError();
 }
 
-cudaError_t launchTileOrder(const CameraDev& c, cudaStream_t st) {
-    if (c.tiles == 0) return cudaSuccess;
-    tileOrderKernel<<<1, 1024, 0, st>>>(c.tileCost, c.tiles, c.tileOrder);
+cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st) {
+    if (fr.tiles == 0) return cudaSuccess;
+    tileOrderKernel<<<1, 1024, 0, st>>>(fr);
     return cudaGetLastError();
 }
 
-cudaError_t launchTileCullRange(const SceneDev& s, const CameraDev& c, const FrameParams& f, const uint32_t* order,
-                                uint32_t first, uint32_t count, uint32_t* queue, cudaStream_t st) {
+cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                           uint32_t* queue, uint32_t warps, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
-    static int ctasPerSm = 0, sms = 0;
-    if (!ctasPerSm) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctasPerSm, tileCullKernel, kTileWarps * 32, 0);
-        if (ctasPerSm < 1) ctasPerSm = 1;
-        if (sms < 1) sms = 1;
+    const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
+                         order, first, count, queue};
+    switch (warps) {
+    case 2: return launchTileCullW<2>(a, count, st);
+    case 4: return launchTileCullW<4>(a, count, st);
+    case 8: return launchTileCullW<8>(a, count, st);
+    default: return cudaErrorInvalidValue;
     }
-    TileCullArgs a{s.nodes, c.tileRays, c.tiles, f.cameraToWorld, c.blockStacks, c.blockSizes, c.tileLists, c.pool,
-                   c.chunkNext, c.poolChunks, c.counters, order, first, count, queue, c.tileCost};
-    const uint32_t needed = (count + kTileWarps - 1) / kTileWarps;
-    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(sms * ctasPerSm));
-    tileCullKernel<<<grid, kTileWarps * 32, 0, st>>>(a);
-    return cudaGetLastError();
 }
 
-cudaError_t launchTileCull(const SceneDev& s, const CameraDev& c, const FrameParams& f, cudaStream_t st) {
-    if (c.tiles == 0) return cudaSuccess;
-    const bool ordered = c.tileOrder && c.tileCost && c.costValid;
-    if (ordered) {
-        cudaError_t e = launchTileOrder(c, st);
-        if (e != cudaSuccess) return e;
-    }
-    return launchTileCullRange(s, c, f, ordered ? c.tileOrder : nullptr, 0, c.tiles, &c.counters[2], st);
+cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st) {
+    writeViewKernel<<<1, 1, 0, st>>>(v, dst);
+    return cudaGetLastError();
 }
 
 } // namespace hvb

@@ -123,7 +123,7 @@ typedef struct {
     uint32_t output_to_3d_api; /* must be 0: no graphics API here */
     /* additions */
     uint32_t fp_mode;             /* HVVR_FP_FMA (reference kernel comments) or HVVR_FP_STRICT (no FMA in edge tests) */
-    uint64_t tri_index_capacity;  /* per-camera triangle-index pool, entries; 0 = default (128M as the reference) */
+    uint64_t tri_index_capacity;  /* triangle-index pool shared by the raycaster's cameras, entries; 0 = default (128M as the reference) */
     int device;                   /* CUDA device ordinal */
 } hvvr_spec;
 
@@ -131,6 +131,7 @@ typedef struct hvvr_raycaster hvvr_raycaster;
 typedef struct hvvr_camera hvvr_camera;
 typedef struct hvvr_model hvvr_model;
 typedef struct hvvr_light hvvr_light;
+typedef struct hvvr_batch hvvr_batch;
 
 /* ---------------------------------------------------------------- errors */
 /* Message of the last failing call on this thread (empty string if none). */
@@ -225,6 +226,9 @@ int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9);
 int hvvr_camera_read_timings(const hvvr_camera* cam, float* ms6);
 /* total triangle-index entries produced by the last frame's tile cull */
 int hvvr_camera_read_list_total(const hvvr_camera* cam, uint64_t* total);
+/* BVH nodes visited per tile by the last frame's tile cull [tile_count] (the schedule of the
+ * next frame is built from these) */
+int hvvr_camera_read_tile_costs(const hvvr_camera* cam, uint32_t* visits);
 
 /* ---------------------------------------------------------------- scene state read-back
  * The refit BVH (GPUSceneState::fetchUpdatedBVH, libraries/hvvr/raycaster/gpu_scene_state.cu:454-467):
@@ -243,6 +247,48 @@ int hvvr_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr
                            uint32_t* node_count);
 /* getGridSamples(width, height) (libraries/hvvr/raycaster/samples.cpp:21-42) */
 int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
+
+/* ---------------------------------------------------------------- batched frames
+ * No counterpart in the reference, whose render() walks the cameras of one scene one at a
+ * time. A batch renders the enabled cameras of several raycasters (one scene each, all on one
+ * device, all with the same fp_mode) as one frame: each stage is one launch over every view,
+ * the tile cull is one persistent work queue over all tiles (longest first after the first
+ * frame), and intersect/shade runs once per MSAA rate present. Per view the results are the
+ * same as rendering that camera alone (same lists, hit IDs and colours). After the first
+ * frame of a layout the frame is replayed from a CUDA graph (config.use_graph). Cameras keep
+ * their render targets and read-backs; a camera's tile lists live in the pool of the batch
+ * that rendered it last. Destroy batches before their raycasters; a batch whose raycaster
+ * was destroyed returns HVVR_ERR_STATE. */
+typedef struct {
+    uint32_t tile_cull_warps;     /* warps per CTA of the tile-cull work queue: 2, 4 or 8 */
+    uint32_t heavy_divisor;       /* 1/heavy_divisor of each rate's tiles (last frame's slowest) are
+                                     culled and shaded on their own stream; 0 = no split */
+    uint64_t tri_index_capacity;  /* triangle-list pool entries shared by all views */
+    uint32_t use_graph;           /* replay frames from a CUDA graph once the layout is stable */
+    float frame_ms;               /* autotune result: median device time of a frame */
+} hvvr_batch_config;
+void hvvr_batch_config_default(hvvr_batch_config* cfg);
+int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,
+                      hvvr_batch** out);
+int hvvr_batch_destroy(hvvr_batch* batch);
+/* scene update/refit of every raycaster, then one frame of all their enabled cameras on
+ * stream (NULL: the first raycaster's stream); CPU_MEMORY targets are complete on return */
+int hvvr_batch_render(hvvr_batch* batch, double elapsed_time, void* stream);
+int hvvr_batch_synchronize(hvvr_batch* batch);
+int hvvr_batch_get_config(const hvvr_batch* batch, hvvr_batch_config* cfg);
+int hvvr_batch_set_config(hvvr_batch* batch, const hvvr_batch_config* cfg);
+/* Autotuner: renders `frames` timed frames (after one warm-up) for each tile_cull_warps in
+ * {2,4,8} x heavy_divisor in {0,16,8,4}, keeps the fastest, then sizes the pool to 1.25x the
+ * largest list total seen (at least 1M entries). Writes the chosen config to *out. */
+int hvvr_batch_autotune(hvvr_batch* batch, uint32_t frames, hvvr_batch_config* out);
+/* device ms of the last frame: [0] total; [1] block cull, [2] first tile cull, [3] rest of
+ * cull + intersect/shade, [4] remap + copies - stages are 0 when the frame was a graph replay */
+int hvvr_batch_read_timings(const hvvr_batch* batch, float* ms5);
+/* device ms of the last frame's launches, summed over the launches of the frame (launches on
+ * different streams overlap, so the sum can exceed the frame time): [0] tile cull, [1]
+ * intersect/shade, [2] block cull, [3] remap. Not available after a graph replay. */
+int hvvr_batch_read_kernel_times(const hvvr_batch* batch, float* ms4);
+int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
 
 /* ---------------------------------------------------------------- cull without device allocation
  * No counterpart in the reference. For callers that may not call cudaMalloc: a render thread

@@ -1,0 +1,103 @@
+"""Batched frames: the cameras of several raycasters (different scenes, sizes and MSAA rates)
+rendered as one frame, over several frames so that the later ones replay a CUDA graph and
+cull the slowest tiles on their own streams. Every view must match the oracle exactly, as the
+same camera rendered on its own does (same lists, hit IDs, depth, G-buffer; colour <= 1 LSB).
+"""
+import numpy as np
+import pytest
+
+import hvvr_b200 as hv
+from hvvr_b200 import scenes
+
+from helpers import list_mismatch, render_oracle, scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_view(oracle, sc, cam, smp, w, h, msaa, xf):
+    fo = render_oracle(oracle, sc, smp, w, h, msaa, cam_xf=xf)
+    counts, idx = cam.tile_lists()
+    assert list_mismatch(counts, idx, fo.tile_counts, fo.tile_indices) == 0
+    ids, depth = cam.hits()
+    assert np.array_equal(ids, fo.hit_ids), "hit IDs differ at %d subsamples" % int((ids != fo.hit_ids).sum())
+    assert np.array_equal(depth.view(np.uint32), fo.depth.view(np.uint32)), "depth differs"
+    col = cam.sample_colors()
+    d = np.abs(col.view(np.uint8).astype(np.int32) - fo.colors.view(np.uint8).astype(np.int32))
+    assert d.max() <= 1
+    img = cam.image
+    di = np.abs(img.view(np.uint8).astype(np.int32) - fo.image.view(np.uint8).astype(np.int32))
+    assert di.max() <= 1
+
+
+def _make_rc(sc):
+    rc = hv.Raycaster()
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    return rc
+
+
+def _add_cam(rc, w, h, kind, msaa):
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h)
+    smp = scenes.grid_samples(w, h) if kind == "grid" else scenes.barrel_samples(w, h)
+    cam.set_samples(smp, 1)
+    cam.set_msaa(msaa)
+    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+    return cam, smp
+
+
+@pytest.mark.parametrize("use_graph", [1, 0])
+def test_batch_two_scenes_mixed_rates(oracle, use_graph):
+    sc_a, sc_b = scene("c1"), scene("small")
+    rc_a, rc_b = _make_rc(sc_a), _make_rc(sc_b)
+    views = []  # (raycaster scene, camera, samples, w, h, msaa)
+    for (rc, sc, w, h, kind, msaa) in [(rc_a, sc_a, 320, 288, "barrel", 4), (rc_a, sc_a, 256, 192, "grid", 1),
+                                       (rc_b, sc_b, 160, 176, "barrel", 8), (rc_b, sc_b, 200, 120, "grid", 4)]:
+        cam, smp = _add_cam(rc, w, h, kind, msaa)
+        views.append((sc, cam, smp, w, h, msaa))
+    batch = hv.Batch([rc_a, rc_b], hv.batch_config(use_graph=use_graph, tri_index_capacity=1 << 22))
+    path = [((0.0, 2.0, 10.0), (0.0, 0.0, 0.0)), ((2.5, 1.0, 7.0), (-1.0, 0.5, 0.0)),
+            ((-3.0, 3.0, 8.0), (1.0, 0.0, -2.0)), ((1.0, 1.5, 9.0), (0.0, 0.2, 0.0))]
+    for eye, target in path:
+        xfs = []
+        for k, (sc, cam, smp, w, h, msaa) in enumerate(views):
+            xf = scenes.camera_transform(eye=(eye[0] + 0.25 * k, eye[1], eye[2]), target=target)
+            cam.set_camera_to_world(xf)
+            xfs.append(xf)
+        batch.render()
+        t = batch.timings()
+        assert t[0] > 0
+        for (sc, cam, smp, w, h, msaa), xf in zip(views, xfs):
+            _check_view(oracle, sc, cam, smp, w, h, msaa, xf)
+    batch.close()
+    rc_a.close()
+    rc_b.close()
+
+
+def test_batch_matches_single_view_and_autotune():
+    """A camera in a batch gives the same bits as the camera rendered by its own raycaster,
+    before and after the autotuner has changed the batch configuration."""
+    sc = scene("small")
+    w, h = 160, 176
+    rc = _make_rc(sc)
+    cam, smp = _add_cam(rc, w, h, "barrel", 8)
+    other, _ = _add_cam(rc, 96, 64, "grid", 2)
+    xf = scenes.camera_transform(eye=(1.0, 2.5, 8.0), target=(0.0, 0.0, 0.0))
+    cam.set_camera_to_world(xf)
+    other.set_camera_to_world(xf)
+    rc.render()
+    ref_ids, ref_depth = cam.hits()
+    ref_img = cam.image.copy()
+    batch = hv.Batch([rc])
+    cfg = batch.autotune(frames=2)
+    assert cfg.tile_cull_warps in (2, 4, 8) and cfg.frame_ms > 0
+    assert cfg.tri_index_capacity >= 1 << 20
+    for _ in range(3):
+        batch.render()
+        ids, depth = cam.hits()
+        assert np.array_equal(ids, ref_ids)
+        assert np.array_equal(depth.view(np.uint32), ref_depth.view(np.uint32))
+        assert np.array_equal(cam.image, ref_img)
+    batch.close()
+    rc.close()
