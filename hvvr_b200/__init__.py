@@ -83,7 +83,9 @@ _sig("hvvr_tile_cull_static", _vp, _vp, _vp, C.c_uint64, _p(C.c_uint64), _vp)
 _lib.hvvr_batch_config_default.argtypes = [_p(_abi.BatchConfig)]
 _lib.hvvr_batch_config_default.restype = None
 _sig("hvvr_batch_create", _p(_vp), _u32, _p(_abi.BatchConfig), _p(_vp))
+_sig("hvvr_batch_create_views", _p(_vp), _u32, _p(_abi.BatchConfig), _p(_vp))
 _sig("hvvr_batch_destroy", _vp)
+_sig("hvvr_model_update_vertices_device", _vp, _u32, _u32, _vp, _vp)
 _sig("hvvr_batch_render", _vp, C.c_double, _vp)
 _sig("hvvr_batch_synchronize", _vp)
 _sig("hvvr_batch_get_config", _vp, _p(_abi.BatchConfig))
@@ -91,6 +93,7 @@ _sig("hvvr_batch_set_config", _vp, _p(_abi.BatchConfig))
 _sig("hvvr_batch_autotune", _vp, _u32, _p(_abi.BatchConfig))
 _sig("hvvr_batch_read_timings", _vp, _vp)
 _sig("hvvr_batch_read_kernel_times", _vp, _vp)
+_sig("hvvr_batch_read_stats", _vp, _vp)
 _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
 
@@ -107,10 +110,11 @@ EXPORTED = [
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
     "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
-    "hvvr_tile_cull_static", "hvvr_batch_config_default", "hvvr_batch_create", "hvvr_batch_destroy",
+    "hvvr_tile_cull_static", "hvvr_batch_config_default", "hvvr_batch_create", "hvvr_batch_create_views",
+    "hvvr_batch_destroy", "hvvr_model_update_vertices_device",
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
-    "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs",
+    "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
 ]
 
 
@@ -156,6 +160,10 @@ class Model:
     def update_vertices(self, verts):
         verts = np.ascontiguousarray(verts, dtype=_abi.VERTEX_DTYPE)
         _check(_lib.hvvr_model_update_vertices(self.handle, verts.ctypes.data, len(verts)))
+
+    def update_vertices_device(self, first, count, device_ptr, stream=None):
+        """copy count vertices (32 B each) from device memory over vertices [first, first+count)"""
+        _check(_lib.hvvr_model_update_vertices_device(self.handle, first, count, _vp(device_ptr), stream))
 
 
 class Camera:
@@ -398,11 +406,20 @@ class Batch:
     """The enabled cameras of several raycasters (one scene each, one device) rendered as one
     frame: one launch per stage over all views, replayed from a CUDA graph once stable."""
 
-    def __init__(self, raycasters, config=None):
-        arr = (_vp * len(raycasters))(*[r.handle for r in raycasters])
+    def __init__(self, raycasters=None, config=None, cameras=None):
+        """Every enabled camera of `raycasters`, or exactly `cameras` (of any raycasters)."""
         h = _vp()
-        _check(_lib.hvvr_batch_create(arr, len(raycasters), C.byref(config) if config is not None else None,
-                                      C.byref(h)))
+        cfg = C.byref(config) if config is not None else None
+        if cameras is not None:
+            arr = (_vp * len(cameras))(*[c.handle for c in cameras])
+            _check(_lib.hvvr_batch_create_views(arr, len(cameras), cfg, C.byref(h)))
+            raycasters = []
+            for c in cameras:
+                if c._rc not in raycasters:
+                    raycasters.append(c._rc)
+        else:
+            arr = (_vp * len(raycasters))(*[r.handle for r in raycasters])
+            _check(_lib.hvvr_batch_create(arr, len(raycasters), cfg, C.byref(h)))
         self.handle = h
         self.raycasters = list(raycasters)
         for r in self.raycasters:
@@ -448,6 +465,12 @@ class Batch:
         t = np.zeros(4, dtype=np.float32)
         _check(_lib.hvvr_batch_read_kernel_times(self.handle, t.ctypes.data))
         return t
+
+    def stats(self):
+        """last frame: list-pool entries taken, tiles re-culled with the large stack, status, views"""
+        t = np.zeros(4, dtype=np.uint64)
+        _check(_lib.hvvr_batch_read_stats(self.handle, t.ctypes.data))
+        return {"pool_entries": int(t[0]), "retried_tiles": int(t[1]), "status": int(t[2]), "views": int(t[3])}
 
     def timings(self):
         """device ms of the last frame: total, block cull, first tile cull, rest of cull +

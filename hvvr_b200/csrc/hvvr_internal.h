@@ -14,9 +14,10 @@ namespace hvb {
 enum : uint32_t { kTileSize = 128, kTilesPerBlock = 64, kBlockSize = kTileSize * kTilesPerBlock };
 // block cull stack capacity (BlockFrame::stackSize, libraries/hvvr/raycaster/traverse_avx.h:255)
 enum : uint32_t { kBlockStack = 64 };
-// per-warp tile traversal stack in shared memory; the reference's TileFrame holds 4096
-// entries, but a stack deeper than this needs a BVH deeper than ~60 levels. Overflow sets
-// kStatusStackOverflow and stops that tile instead of writing out of bounds.
+// per-warp tile traversal stack in shared memory. The reference's TileFrame holds 4096
+// entries; nearly every tile needs far fewer (at most 123 on the 1M-triangle stereo frame), so
+// the main pass uses kTileStack and a tile that would outgrow it is culled again by a retry
+// pass with 4096 entries. Outgrowing that sets kStatusStackOverflow and leaves the tile empty.
 enum : uint32_t { kTileStack = 256 };
 // triangle indices move between traversal and intersection in chunks of one intersect batch
 enum : uint32_t { kChunk = 128 };
@@ -149,15 +150,18 @@ struct FrameDev {
     uint32_t* pool = nullptr;          // [poolChunks * kChunk] triangle-list chunks
     uint32_t* chunkNext = nullptr;     // [poolChunks]
     uint32_t poolChunks = 0;
-    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2 + k] work-queue heads
+    uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2 + 3k ..] per-launch queues
     uint32_t* order = nullptr;         // [tiles] tile order: grouped by rate, then longest first
+    uint32_t* retry = nullptr;         // [tiles] tiles whose traversal stack overflowed, per range
 };
 
 
 // records the message returned by hvvr_last_error() on this thread and returns code
 int setLastError(int code, const char* msg);
 
-enum : uint32_t { kCounterWords = 16, kQueueBase = 2 };
+// counters: [0] chunk allocator, [1] status, then per tile-cull launch k (up to 12) three
+// words at kQueueBase + 3k: work-queue head, retry count, retry-queue head
+enum : uint32_t { kCounterWords = 40, kQueueBase = 2, kQueueWords = 3 };
 
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
 cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st);
@@ -165,10 +169,12 @@ cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st);
 // last frame's visit counts) within a rate
 cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st);
 // tile cull / intersect-shade of the global tiles order[first, first + count) (order ==
-// nullptr: tiles first..first+count-1); concurrent tile-cull launches need distinct zeroed
-// queue heads. warps = tile-cull warps per CTA (2, 4 or 8).
+// nullptr: tiles first..first+count-1). queues: kQueueWords zeroed words of this launch
+// (concurrent launches need their own). warps = tile-cull warps per CTA (2, 4 or 8). Tiles
+// whose traversal stack outgrows stackLimit (0 = kTileStack; at least 8) are
+// culled again by a second launch with a 4096-entry stack.
 cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
-                           uint32_t* queue, uint32_t warps, cudaStream_t st);
+                           uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st);
 cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, const uint32_t* order,
                                  uint32_t first, uint32_t count, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);

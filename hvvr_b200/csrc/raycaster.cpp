@@ -124,6 +124,7 @@ struct hvvr_camera {
     bool rendered = false;
     uint64_t setupGen = 0;            // process-unique id of the current sample setup and buffers
     hvvr_batch* lastBatch = nullptr;  // batch whose pool holds this camera's last tile lists
+    std::vector<hvvr_batch*> batches; // camera-list batches that name this camera
     CameraDev dev;
     SampleSetup setup;
     // device storage behind dev
@@ -144,6 +145,8 @@ struct hvvr_camera {
 // CUDA graph. Every raycaster renders its own cameras through an internal batch.
 struct hvvr_batch {
     std::vector<hvvr_raycaster*> rcs;
+    bool fixedViews = false;          // renders exactly `cams` (else every enabled camera of rcs)
+    std::vector<hvvr_camera*> cams;
     bool internal = false;            // a raycaster's own batch
     bool detached = false;            // one of its raycasters was destroyed
     hvvr_batch_config cfg{};
@@ -159,7 +162,7 @@ struct hvvr_batch {
     bool fpStrict = false;
     bool costValid = false;           // every view's tileCost holds a previous frame's counts
     DevBuf<ViewDev> viewsDev;
-    DevBuf<uint32_t> blockView, order, pool, chunkNext, counters;
+    DevBuf<uint32_t> blockView, order, retry, pool, chunkNext, counters;
     uint32_t poolChunks = 0;
     ViewDev* hostViews[2] = {};       // pinned staging of the per-frame view table
     size_t hostViewsCap = 0;
@@ -462,6 +465,7 @@ void batchConfigDefault(hvvr_batch_config* c) {
     c->tri_index_capacity = kDefaultCapacity;
     c->use_graph = 1;
     c->frame_ms = 0.0f;
+    c->tile_stack_entries = 0;
 }
 
 int checkConfig(const hvvr_batch_config& c) {
@@ -469,6 +473,8 @@ int checkConfig(const hvvr_batch_config& c) {
         return fail(HVVR_ERR_INVALID, "tile_cull_warps must be 2, 4 or 8");
     const uint64_t chunks = (c.tri_index_capacity + kChunk - 1) / kChunk;
     if (c.tri_index_capacity == 0 || chunks > 0xfffffff0ull) return fail(HVVR_ERR_INVALID, "bad tri_index_capacity");
+    if (c.tile_stack_entries && (c.tile_stack_entries < 8 || c.tile_stack_entries > kTileStack))
+        return fail(HVVR_ERR_INVALID, "tile_stack_entries must be 0 or in [8, 256]");
     return HVVR_OK;
 }
 
@@ -566,7 +572,8 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
             cudaStream_t ps = b->side[k];
             CUDA_TRY(cudaStreamWaitEvent(ps, b->forkEv, 0));
             if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][0], ps));
-            CUDA_TRY(launchTileCull(fr, fr.order, p0, pn, fr.counters + kQueueBase + k, b->cfg.tile_cull_warps, ps));
+            CUDA_TRY(launchTileCull(fr, fr.order, p0, pn, fr.counters + kQueueBase + kQueueWords * k,
+                                    b->cfg.tile_cull_warps, b->cfg.tile_stack_entries, ps));
             if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][1], ps));
             if (timing && part == 1 && first) CUDA_TRY(cudaEventRecord(b->ev[2], ps));
             CUDA_TRY(launchIntersectShade(fr, msaa, b->fpStrict, fr.order, p0, pn, ps));
@@ -617,13 +624,18 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
             rc->refitDirty = false;
         }
     }
-    std::vector<hvvr_camera*> cams;
+    std::vector<hvvr_camera*> candidates, cams;
+    if (b->fixedViews) {
+        candidates = b->cams;
+    } else {
+        for (hvvr_raycaster* rc : b->rcs)
+            for (auto& cp : rc->cameras) candidates.push_back(cp.get());
+    }
     bool cpuTargets = false, capturable = true;
-    for (hvvr_raycaster* rc : b->rcs) {
-        if (rc->scene.nodeCount == 0) continue;
-        for (auto& cp : rc->cameras) {
-            hvvr_camera* c = cp.get();
-            if (!c->enabled || c->samples.empty()) continue;
+    {
+        for (hvvr_camera* c : candidates) {
+            hvvr_raycaster* rc = c->rc;
+            if (rc->scene.nodeCount == 0 || !c->enabled || c->samples.empty()) continue;
             if (c->setupDirty) TRY(setupCamera(c, st));
             if (!rc->msaaUploaded[c->msaa]) {
                 float off[64];
@@ -680,6 +692,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
         }
         TRY(b->blockView.upload(blockView.data(), blockView.size(), st));
         TRY(b->order.alloc(b->tiles));
+        TRY(b->retry.alloc(b->tiles));
         TRY(b->viewsDev.alloc(b->views.size()));
         if (b->hostViewsCap < b->views.size()) {
             for (int k = 0; k < 2; k++) {
@@ -748,11 +761,12 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
     fr.poolChunks = b->poolChunks;
     fr.counters = b->counters.p;
     fr.order = b->order.p;
+    fr.retry = b->retry.p;
     if (b->cfg.use_graph && b->costValid && capturable) {
         std::vector<uint64_t> gkey = b->layoutKey;
         const uint64_t extra[] = {b->cfg.tile_cull_warps, b->cfg.heavy_divisor, b->poolChunks, strict ? 1u : 0u,
-                                  uint64_t(uintptr_t(st))};
-        gkey.insert(gkey.end(), extra, extra + 5);
+                                  uint64_t(uintptr_t(st)), b->cfg.tile_stack_entries};
+        gkey.insert(gkey.end(), extra, extra + 6);
         if (!b->graph || gkey != b->graphKey) {
             dropGraph(b);
             CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
@@ -837,8 +851,18 @@ int hvvr_raycaster_destroy(hvvr_raycaster* rc) {
     cudaStreamSynchronize(rc->stream);
     cudaDeviceSynchronize();
     for (hvvr_batch* b : rc->batches) {
+        // the batch stays a valid handle (destroy still works) but can no longer render
         b->detached = true;
+        for (hvvr_raycaster* other : b->rcs) {
+            if (other == rc) continue;
+            other->batches.erase(std::remove(other->batches.begin(), other->batches.end(), b), other->batches.end());
+            for (auto& c : other->cameras) {
+                if (c->lastBatch == b) c->lastBatch = nullptr;
+                c->batches.erase(std::remove(c->batches.begin(), c->batches.end(), b), c->batches.end());
+            }
+        }
         b->rcs.clear();
+        b->cams.clear();
     }
     for (auto& c : rc->cameras) releaseCamera(c.get());
     if (rc->own) releaseBatch(rc->own.get());
@@ -906,14 +930,47 @@ int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const h
     return HVVR_OK;
 }
 
+int hvvr_batch_create_views(hvvr_camera* const* cameras, uint32_t count, const hvvr_batch_config* cfg,
+                            hvvr_batch** out) {
+    if (!out) return fail(HVVR_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!cameras || count == 0) return fail(HVVR_ERR_INVALID, "no cameras");
+    auto b = std::make_unique<hvvr_batch>();
+    batchConfigDefault(&b->cfg);
+    if (cfg) {
+        b->cfg = *cfg;
+        TRY(checkConfig(b->cfg));
+    }
+    for (uint32_t i = 0; i < count; i++) {
+        hvvr_camera* c = cameras[i];
+        if (!c) return fail(HVVR_ERR_INVALID, "NULL camera %u", i);
+        if (std::find(b->cams.begin(), b->cams.end(), c) != b->cams.end())
+            return fail(HVVR_ERR_INVALID, "camera %u listed twice", i);
+        hvvr_raycaster* rc = c->rc;
+        if (rc->spec.device != cameras[0]->rc->spec.device)
+            return fail(HVVR_ERR_INVALID, "batched cameras must share one device");
+        if (rc->spec.fp_mode != cameras[0]->rc->spec.fp_mode)
+            return fail(HVVR_ERR_INVALID, "batched cameras must share one fp_mode");
+        b->cams.push_back(c);
+        if (std::find(b->rcs.begin(), b->rcs.end(), rc) == b->rcs.end()) b->rcs.push_back(rc);
+    }
+    b->fixedViews = true;
+    for (hvvr_raycaster* rc : b->rcs) rc->batches.push_back(b.get());
+    for (hvvr_camera* c : b->cams) c->batches.push_back(b.get());
+    *out = b.release();
+    return HVVR_OK;
+}
+
 int hvvr_batch_destroy(hvvr_batch* b) {
     if (!b || b->internal) return fail(HVVR_ERR_INVALID, "not a batch");
     if (!b->rcs.empty()) cudaSetDevice(b->rcs[0]->spec.device);
     cudaDeviceSynchronize();
     for (hvvr_raycaster* rc : b->rcs) {
         rc->batches.erase(std::remove(rc->batches.begin(), rc->batches.end(), b), rc->batches.end());
-        for (auto& c : rc->cameras)
+        for (auto& c : rc->cameras) {
             if (c->lastBatch == b) c->lastBatch = nullptr;
+            c->batches.erase(std::remove(c->batches.begin(), c->batches.end(), b), c->batches.end());
+        }
     }
     releaseBatch(b);
     delete b;
@@ -980,6 +1037,19 @@ int kernelTimes(const hvvr_batch* b, float* ms4) {
     return HVVR_OK;
 }
 } // namespace
+
+int hvvr_batch_read_stats(const hvvr_batch* b, uint64_t* out4) {
+    if (!b || !out4) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (!b->counterValid || !b->hostCounters) return fail(HVVR_ERR_STATE, "the batch has not rendered a frame");
+    CUDA_TRY(cudaEventSynchronize(b->ev[5]));
+    uint64_t retried = 0;
+    for (uint32_t k = 0; k < 12; k++) retried += b->hostCounters[kQueueBase + kQueueWords * k + 1];
+    out4[0] = uint64_t(std::min(b->hostCounters[0], b->poolChunks)) * kChunk;
+    out4[1] = retried;
+    out4[2] = b->hostCounters[1];
+    out4[3] = b->views.size();
+    return HVVR_OK;
+}
 
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4) {
     if (!rc || !ms4) return fail(HVVR_ERR_INVALID, "NULL argument");
@@ -1104,6 +1174,25 @@ int hvvr_model_update_vertices(hvvr_model* model, const hvvr_shading_vertex* ver
     return HVVR_OK;
 }
 
+int hvvr_model_update_vertices_device(hvvr_model* model, uint32_t first, uint32_t count, const void* device_verts,
+                                      void* stream) {
+    if (!model || (count && !device_verts)) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (uint64_t(first) + count > model->verts.size()) return fail(HVVR_ERR_INVALID, "vertex range out of bounds");
+    hvvr_raycaster* rc = model->rc;
+    if (rc->sceneDirty) return fail(HVVR_ERR_STATE, "the scene is not on the device yet (render once first)");
+    size_t off = 0;
+    for (auto& m : rc->models) {
+        if (m.get() == model) break;
+        off += m->verts.size();
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : rc->stream;
+    if (count)
+        CUDA_TRY(cudaMemcpyAsync(rc->vertsIn.p + 2 * (off + first), device_verts,
+                                 size_t(count) * sizeof(hvvr_shading_vertex), cudaMemcpyDeviceToDevice, st));
+    rc->refitDirty = true;
+    return HVVR_OK;
+}
+
 int hvvr_light_create(hvvr_raycaster* rc, const hvvr_light_union* light, hvvr_light** out) {
     if (!rc || !light || !out) return fail(HVVR_ERR_INVALID, "NULL argument");
     auto l = std::make_unique<hvvr_light>();
@@ -1145,6 +1234,7 @@ int hvvr_camera_destroy(hvvr_raycaster* rc, hvvr_camera* cam) {
     for (auto it = rc->cameras.begin(); it != rc->cameras.end(); ++it) {
         if (it->get() == cam) {
             cudaDeviceSynchronize();
+            for (hvvr_batch* b : cam->batches) b->cams.erase(std::remove(b->cams.begin(), b->cams.end(), cam), b->cams.end());
             releaseCamera(cam);
             rc->cameras.erase(it);
             return HVVR_OK;

@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
 
     uint32_t chunk = L.first;
     uint32_t remaining = L.count;
-    while (remaining > 0) {
+    while (remaining > 0 && chunk < fr.poolChunks) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
         const uint32_t nextChunk = fr.chunkNext[chunk];
         bool keep = false;

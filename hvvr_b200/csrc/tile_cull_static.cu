@@ -40,12 +40,14 @@ constexpr uint32_t kMaxTiles = 65536;                  // 4,194,304 padded sampl
 constexpr uint32_t kMaxChunks = 61440;                 // kMaxChunks * kChunk entries
 constexpr uint64_t kMaxEntries = uint64_t(kMaxChunks) * kChunk; // 7,864,320 entries (30 MiB)
 // word layout of the scratch array
-constexpr size_t kOffCounters = 0;                     // [0] chunk allocator, [1] status, [2..3] total (u64), [4] queue
+constexpr size_t kOffCounters = 0;                     // [0] chunk allocator, [1] status, [2..3] total (u64),
+                                                       // [4..6] work queue, retry count, retry queue
 constexpr size_t kOffView = 64;                        // the one-view table of the cull (ViewDev)
 constexpr size_t kViewWords = (sizeof(ViewDev) + 255) / 256 * 64;
 constexpr size_t kOffLists = kOffView + kViewWords;    // TileList[kMaxTiles]
 constexpr size_t kOffCost = kOffLists + 2 * size_t(kMaxTiles); // per-tile visit counts (written, unused)
-constexpr size_t kOffNext = kOffCost + kMaxTiles;
+constexpr size_t kOffRetry = kOffCost + kMaxTiles;    // tiles re-culled with the large stack
+constexpr size_t kOffNext = kOffRetry + kMaxTiles;
 constexpr size_t kOffOffsets = kOffNext + kMaxChunks;  // exclusive prefix of counts, kMaxTiles + 1 words (u32 lo)
 constexpr size_t kOffPool = (kOffOffsets + kMaxTiles + 1 + 63) / 64 * 64;
 constexpr size_t kScratchWords = kOffPool + size_t(kMaxChunks) * kChunk;
@@ -173,11 +175,12 @@ extern "C" int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* 
     fr.chunkNext = scratch + kOffNext;
     fr.poolChunks = kMaxChunks;
     fr.counters = scratch + kOffCounters;
+    fr.retry = scratch + kOffRetry;
     if ((e = cudaMemsetAsync(scratch + kOffCounters, 0, 8 * sizeof(uint32_t), st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "clearing the scratch counters failed", e);
     if ((e = launchWriteView(v, reinterpret_cast<ViewDev*>(scratch + kOffView), st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "view setup launch failed", e);
-    if ((e = launchTileCull(fr, nullptr, 0, tiles, scratch + kOffCounters + 4, 4, st)) != cudaSuccess)
+    if ((e = launchTileCull(fr, nullptr, 0, tiles, scratch + kOffCounters + 4, 4, 0, st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "tile cull launch failed", e);
     scanCounts<<<1, 1024, 0, st>>>(scratch, tiles);
     gatherLists<<<(tiles + 7) / 8, 256, 0, st>>>(scratch, tiles, counts, indices, capacity);

@@ -350,11 +350,13 @@ __global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(FrameDev fr)
 }
 
 
-struct TileSmem {
+// per-warp tile traversal state; S = sorted-stack capacity
+template <uint32_t S>
+struct TileSmemT {
     SmemFrustum f;
-    float tMin[kTileStack];
-    uint32_t mask[kTileStack];
-    uint32_t node[kTileStack];
+    float tMin[S];
+    uint32_t mask[S];
+    uint32_t node[S];
     alignas(16) uint32_t buf[kChunk];
 };
 
@@ -436,10 +438,18 @@ struct TileCullArgs {
     uint32_t first;        // this launch culls order[first, first + count)
     uint32_t count;
     uint32_t* queue;       // work-queue head of this launch, zero at launch
+    uint32_t* retry;       // tiles whose stack outgrew kTileStack, at retry[first + i]
+    uint32_t* retryCount;  // number of such tiles, zero at launch
+    uint32_t* retryQueue;  // work-queue head of the retry pass, zero at launch
+    uint32_t stackLimit;   // entries the main pass may use (<= kTileStack)
 };
 
-// traverseTiles for one tile of view V (tile = view-local index); returns the node visits
-__device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t tile, TileSmem& s) {
+// traverseTiles for one tile of view V (tile = view-local index); returns the node visits.
+// overflow: the sorted stack needed more than S entries; the tile's list is left empty.
+template <uint32_t S>
+__device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t tile, TileSmemT<S>& s,
+                             bool& overflow) {
+    overflow = false;
     const uint32_t lane = laneId();
     const Node* __restrict__ nodes = V.nodes;
     const uint32_t blk = tile / kTilesPerBlock;
@@ -511,8 +521,8 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                 //   top - #{old < key_i} + #{children with a larger key}
                 //       + #{earlier children with an equal key}.
                 const uint32_t m = __popc(mask);
-                if (top + m >= kTileStack) {
-                    if (lane == 0) atomicOr(&a.counters[1], kStatusStackOverflow);
+                if (top + m >= (S == kTileStack ? a.stackLimit : S)) {
+                    overflow = true;
                     break;
                 }
                 float ck[4], ckz[4];
@@ -589,6 +599,10 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
         node = popNode;
         v = vp;
     }
+    if (overflow) {
+        if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
+        return visits;
+    }
     if (!em.dead && em.bufCount) em.flush(s.buf);
     if (lane == 0) {
         if (em.prev != kNoChunk) a.chunkNext[em.prev] = kNoChunk;
@@ -601,9 +615,9 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
 // few long horizon tiles overlap with the rest instead of holding a CTA slot each.
 template <int W>
 __global__ void __launch_bounds__(W * 32) tileCullKernel(TileCullArgs a) {
-    __shared__ TileSmem smem[W];
+    __shared__ TileSmemT<kTileStack> smem[W];
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
-    TileSmem& s = smem[warp];
+    TileSmemT<kTileStack>& s = smem[warp];
     for (;;) {
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(a.queue, 1u);
@@ -613,8 +627,38 @@ __global__ void __launch_bounds__(W * 32) tileCullKernel(TileCullArgs a) {
         const ViewDev& V = viewOfBlock(a.views, a.blockView, a.viewCount, gt / kTilesPerBlock);
         const uint32_t tile = gt - V.tileStart;
         __syncwarp();
-        const uint32_t visits = cullTile(a, V, tile, s);
-        if (lane == 0) V.tileCost[tile] = visits;
+        bool overflow;
+        const uint32_t visits = cullTile(a, V, tile, s, overflow);
+        if (lane == 0) {
+            V.tileCost[tile] = visits;
+            if (overflow) a.retry[a.first + atomicAdd(a.retryCount, 1u)] = gt;
+        }
+        __syncwarp();
+    }
+}
+
+// The tiles whose sorted stack outgrew kTileStack, culled again from the start with the
+// reference's TileFrame capacity (4096 entries, 48 KiB of shared memory per warp).
+constexpr uint32_t kRetryStack = 4096;
+__global__ void __launch_bounds__(32) tileCullRetryKernel(TileCullArgs a) {
+    extern __shared__ __align__(16) unsigned char retrySmem[];
+    TileSmemT<kRetryStack>& s = *reinterpret_cast<TileSmemT<kRetryStack>*>(retrySmem);
+    const uint32_t lane = laneId();
+    for (;;) {
+        uint32_t w = 0;
+        if (lane == 0) w = atomicAdd(a.retryQueue, 1u);
+        w = __shfl_sync(kFull, w, 0);
+        if (w >= *reinterpret_cast<volatile uint32_t*>(a.retryCount)) return;
+        const uint32_t gt = a.retry[a.first + w];
+        const ViewDev& V = viewOfBlock(a.views, a.blockView, a.viewCount, gt / kTilesPerBlock);
+        const uint32_t tile = gt - V.tileStart;
+        __syncwarp();
+        bool overflow;
+        const uint32_t visits = cullTile(a, V, tile, s, overflow);
+        if (lane == 0) {
+            V.tileCost[tile] = visits;
+            if (overflow) atomicOr(&a.counters[1], kStatusStackOverflow);
+        }
         __syncwarp();
     }
 }
@@ -647,22 +691,50 @@ __global__ void __launch_bounds__(1024) tileOrderKernel(FrameDev fr) {
 
 __global__ void writeViewKernel(ViewDev v, ViewDev* dst) { *dst = v; }
 
-template <int W>
-cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, cudaStream_t st) {
-    static int ctasPerSm[64] = {}, sms[64] = {};
+struct DeviceLimits {
+    int sms = 0;
+    int ctasPerSm[9] = {};
+    bool retryReady = false;
+};
+
+DeviceLimits& limits() {
+    static DeviceLimits perDevice[64];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!ctasPerSm[dev]) {
-        cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    DeviceLimits& d = perDevice[dev < 0 || dev >= 64 ? 0 : dev];
+    if (!d.sms) {
+        cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+        if (d.sms < 1) d.sms = 1;
+    }
+    return d;
+}
+
+template <int W>
+cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, cudaStream_t st) {
+    DeviceLimits& d = limits();
+    if (!d.ctasPerSm[W]) {
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tileCullKernel<W>, W * 32, 0);
-        if (sms[dev] < 1) sms[dev] = 1;
-        ctasPerSm[dev] = occ < 1 ? 1 : occ;
+        d.ctasPerSm[W] = occ < 1 ? 1 : occ;
     }
     const uint32_t needed = (count + W - 1) / W;
-    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(sms[dev] * ctasPerSm[dev]));
+    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(d.sms * d.ctasPerSm[W]));
     tileCullKernel<W><<<grid, W * 32, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// the retry pass: one warp per CTA, one CTA per SM; it reads the retry count on the device and
+// exits at once when no tile overflowed
+cudaError_t launchTileCullRetry(const TileCullArgs& a, cudaStream_t st) {
+    DeviceLimits& d = limits();
+    const size_t smem = sizeof(TileSmemT<kRetryStack>);
+    if (!d.retryReady) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(tileCullRetryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        d.retryReady = true;
+    }
+    tileCullRetryKernel<<<d.sms, 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -681,16 +753,21 @@ cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st) {
 }
 
 cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
-                           uint32_t* queue, uint32_t warps, cudaStream_t st) {
+                           uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
+    if (stackLimit == 0 || stackLimit > kTileStack) stackLimit = kTileStack;
+    if (stackLimit < 8) return cudaErrorInvalidValue;
     const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
-                         order, first, count, queue};
+                         order, first, count, queues, fr.retry, queues + 1, queues + 2, stackLimit};
+    cudaError_t e;
     switch (warps) {
-    case 2: return launchTileCullW<2>(a, count, st);
-    case 4: return launchTileCullW<4>(a, count, st);
-    case 8: return launchTileCullW<8>(a, count, st);
+    case 2: e = launchTileCullW<2>(a, count, st); break;
+    case 4: e = launchTileCullW<4>(a, count, st); break;
+    case 8: e = launchTileCullW<8>(a, count, st); break;
     default: return cudaErrorInvalidValue;
     }
+    if (e != cudaSuccess) return e;
+    return launchTileCullRetry(a, st);
 }
 
 cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st) {

@@ -246,6 +246,66 @@ def barrel_samples(width, height, k1=0.22, k2=0.24):
     return s
 
 
+def foveated_samples(count, out_w=1440, out_h=1600, fov_deg=100.0, gaze_deg=(0.0, 0.0), e0_deg=5.0,
+                     jitter_seed=None):
+    """About `count` samples over a fov_deg (vertical) field whose density per unit angle falls
+    as 1 / (1 + (e / e0)^2) with the eccentricity e from the gaze direction.
+
+    Placement: a Vogel (golden-angle) spiral about the gaze point with radius from the inverse
+    of the radial CDF  N(E) ~ ln(1 + (E / e0)^2), clipped to the view rectangle; angles use
+    the small-angle image-plane approximation e ~ |p - gaze| * fov / height. With jitter_seed,
+    each sample moves by U[-0.5, 0.5] of its local spacing (per-frame temporal jitter).
+    Each sample's ellipse is isotropic with the local spacing; its pixel is the output pixel
+    under it. Use viewport_fov(out_w, out_h, fov_deg) for the matching camera viewport.
+    """
+    deg_per_px = fov_deg / out_h
+    gx = out_w * 0.5 + gaze_deg[0] / deg_per_px
+    gy = out_h * 0.5 + gaze_deg[1] / deg_per_px
+    # farthest corner from the gaze, in degrees
+    corners = np.array([[0, 0], [out_w, 0], [0, out_h], [out_w, out_h]], dtype=np.float64)
+    emax = np.sqrt(((corners - [gx, gy]) ** 2).sum(axis=1)).max() * deg_per_px
+    total_log = np.log1p((emax / e0_deg) ** 2)
+    n = int(count)
+    kept = None
+    for _ in range(8):  # grow the spiral until `count` samples fall inside the rectangle
+        i = np.arange(n, dtype=np.float64)
+        u = (i + 0.5) / n
+        e = e0_deg * np.sqrt(np.expm1(u * total_log))
+        theta = i * (math.pi * (3.0 - math.sqrt(5.0)))
+        r_px = e / deg_per_px
+        x = gx + r_px * np.cos(theta)
+        y = gy + r_px * np.sin(theta)
+        inside = (x >= 0) & (x < out_w) & (y >= 0) & (y < out_h)
+        kept = (x[inside], y[inside], e[inside], n)
+        if inside.sum() >= count:
+            break
+        n = int(n * count / max(1, inside.sum()) * 1.02) + 1
+    x, y, e, n = kept
+    x, y, e = x[:count], y[:count], e[:count]
+    # local density (samples per square degree) dN/dA = n / (pi e0^2 total_log) / (1 + (e/e0)^2)
+    dens = n / (math.pi * e0_deg ** 2 * total_log) / (1.0 + (e / e0_deg) ** 2)
+    spacing_px = 1.0 / np.sqrt(dens) / deg_per_px
+    if jitter_seed is not None:
+        rng = np.random.default_rng(jitter_seed)
+        x = np.clip(x + rng.uniform(-0.5, 0.5, len(x)) * spacing_px, 0.0, out_w - 1e-3)
+        y = np.clip(y + rng.uniform(-0.5, 0.5, len(y)) * spacing_px, 0.0, out_h - 1e-3)
+    out = np.zeros(len(x), dtype=_abi.SAMPLE_DTYPE)
+    out["pixel"][:, 0] = np.minimum(x.astype(np.int64), out_w - 1)
+    out["pixel"][:, 1] = np.minimum(y.astype(np.int64), out_h - 1)
+    out["position"][:, 0] = (x / out_w).astype(np.float32)
+    out["position"][:, 1] = (y / out_h).astype(np.float32)
+    out["minor"][:, 0] = (spacing_px / out_w).astype(np.float32)
+    out["major"] = (spacing_px / out_h).astype(np.float32)
+    return out
+
+
+def viewport_fov(width, height, fov_deg):
+    """Viewport with the given vertical field of view and the image's aspect ratio."""
+    t = math.tan(math.radians(fov_deg) * 0.5)
+    a = t * width / height
+    return _abi.FloatRect(_abi.Vec2(-a, -t), _abi.Vec2(a, t))
+
+
 # ---------------------------------------------------------------- cameras
 def look_at_quaternion(eye, target, up=(0.0, 1.0, 0.0)):
     """Rotation (x, y, z, w) whose -z axis looks from eye to target with +y up."""

@@ -162,6 +162,13 @@ int hvvr_model_set_transform(hvvr_model* model, const hvvr_transform* xf);
 /* Replace the model's vertex positions (animation) without rebuilding topology;
  * the next render refits the BVH in place on the device. count must equal the model's vertex count. */
 int hvvr_model_update_vertices(hvvr_model* model, const hvvr_shading_vertex* verts, uint32_t count);
+/* Device-side animation: copies count vertices from device memory over the model's vertices
+ * [first, first+count) on stream (NULL: the raycaster's stream); the next render refits the
+ * BVH on the device. The host copy of the mesh is not updated, so a later scene rebuild
+ * (adding/removing models or lights) restores the vertices last given on the host.
+ * No counterpart in the reference (its Model only has setTransform). */
+int hvvr_model_update_vertices_device(hvvr_model* model, uint32_t first, uint32_t count, const void* device_verts,
+                                      void* stream);
 
 /* ---------------------------------------------------------------- lights
  * createLight(const LightUnion&) / destroyLight (raycaster.h:55-56) */
@@ -266,10 +273,16 @@ typedef struct {
     uint64_t tri_index_capacity;  /* triangle-list pool entries shared by all views */
     uint32_t use_graph;           /* replay frames from a CUDA graph once the layout is stable */
     float frame_ms;               /* autotune result: median device time of a frame */
+    uint32_t tile_stack_entries;  /* traversal stack of the main tile-cull pass, 0 (= 256) or 8..256;
+                                     tiles that need more are culled again with 4096 entries */
 } hvvr_batch_config;
 void hvvr_batch_config_default(hvvr_batch_config* cfg);
 int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,
                       hvvr_batch** out);
+/* a batch of exactly these cameras (of any raycasters on one device); a destroyed camera
+ * leaves the batch */
+int hvvr_batch_create_views(hvvr_camera* const* cameras, uint32_t count, const hvvr_batch_config* cfg,
+                            hvvr_batch** out);
 int hvvr_batch_destroy(hvvr_batch* batch);
 /* scene update/refit of every raycaster, then one frame of all their enabled cameras on
  * stream (NULL: the first raycaster's stream); CPU_MEMORY targets are complete on return */
@@ -289,6 +302,9 @@ int hvvr_batch_read_timings(const hvvr_batch* batch, float* ms5);
  * intersect/shade, [2] block cull, [3] remap. Not available after a graph replay. */
 int hvvr_batch_read_kernel_times(const hvvr_batch* batch, float* ms4);
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
+/* counters of the last frame: [0] list-pool entries taken (whole chunks), [1] tiles culled
+ * again with the 4096-entry stack, [2] device status bits, [3] views */
+int hvvr_batch_read_stats(const hvvr_batch* batch, uint64_t* out4);
 
 /* ---------------------------------------------------------------- cull without device allocation
  * No counterpart in the reference. For callers that may not call cudaMalloc: a render thread

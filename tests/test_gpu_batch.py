@@ -101,3 +101,52 @@ def test_batch_matches_single_view_and_autotune():
         assert np.array_equal(cam.image, ref_img)
     batch.close()
     rc.close()
+
+
+def test_animated_refit_matches_oracle(oracle):
+    """Device-side vertex animation (10% of the vertices, one contiguous range) followed by the
+    GPU refit: refit BVH, lists and hits match the oracle run on the animated mesh, over frames."""
+    import copy
+    import torch
+    from hvvr_b200 import workloads
+    sc = scene("small")
+    w, h = 160, 176
+    rc = _make_rc(sc)
+    model = rc.models[0]
+    cam, smp = _add_cam(rc, w, h, "barrel", 4)
+    xf = scenes.camera_transform(eye=(0.5, 2.0, 9.0), target=(0.0, 0.0, 0.0))
+    cam.set_camera_to_world(xf)
+    rc.render()
+    anim = workloads.Animator(torch, model, sc)
+    for t in (0.3, 1.7, 2.9):
+        anim.step(t)
+        rc.render()
+        moved = copy.copy(sc)
+        moved.verts = anim.host_vertices(sc)
+        fo = render_oracle(oracle, moved, smp, w, h, 4, cam_xf=xf)
+        assert np.array_equal(rc.scene_nodes().view(np.uint8), fo.nodes.view(np.uint8)), "refit BVH differs"
+        counts, idx = cam.tile_lists()
+        assert list_mismatch(counts, idx, fo.tile_counts, fo.tile_indices) == 0
+        ids, depth = cam.hits()
+        assert np.array_equal(ids, fo.hit_ids)
+        assert np.array_equal(depth.view(np.uint32), fo.depth.view(np.uint32))
+    rc.close()
+
+
+def test_stack_retry_pass_matches_oracle(oracle):
+    """A 16-entry main-pass stack sends every tile whose sorted stack grows deeper to the retry
+    pass (4096 entries); the lists, hits and colours must not change."""
+    sc = scene("c1")
+    w, h = 320, 288
+    rc = _make_rc(sc)
+    cam, smp = _add_cam(rc, w, h, "barrel", 4)
+    xf = scenes.camera_transform(eye=(3.0, 1.2, 6.0), target=(-2.0, 0.3, -1.0))
+    cam.set_camera_to_world(xf)
+    batch = hv.Batch(cameras=[cam], config=hv.batch_config(tile_stack_entries=16, tri_index_capacity=1 << 22))
+    for _ in range(3):
+        batch.render()
+        st = batch.stats()
+        assert st["retried_tiles"] > 0 and st["status"] == 0
+        _check_view(oracle, sc, cam, smp, w, h, 4, xf)
+    batch.close()
+    rc.close()
