@@ -94,6 +94,15 @@ _sig("hvvr_batch_autotune", _vp, _u32, _p(_abi.BatchConfig))
 _sig("hvvr_batch_read_timings", _vp, _vp)
 _sig("hvvr_batch_read_kernel_times", _vp, _vp)
 _sig("hvvr_batch_read_stats", _vp, _vp)
+_lib.hvvr_server_config_default.argtypes = [_p(_abi.ServerConfig)]
+_lib.hvvr_server_config_default.restype = None
+_sig("hvvr_server_create", _p(_vp), _u32, _p(_abi.ServerConfig), _p(_vp))
+_sig("hvvr_server_destroy", _vp)
+_sig("hvvr_server_add_view", _vp, _u32, _p(_abi.FloatRect), _vp, _u32, _u32, _u32, _u32, _p(_u32))
+_sig("hvvr_server_submit", _vp, _p(_abi.Request), _p(C.c_uint64))
+_sig("hvvr_server_poll", _vp, _p(_abi.Completion), _u32, _p(_u32), C.c_double)
+_sig("hvvr_server_update_vertices", _vp, _vp, _u32, _u32, _vp)
+_sig("hvvr_server_get_stats", _vp, _p(_abi.ServerStats))
 _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
 
@@ -115,6 +124,8 @@ EXPORTED = [
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
+    "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
+    "hvvr_server_submit", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
 ]
 
 
@@ -478,3 +489,77 @@ class Batch:
         t = np.zeros(5, dtype=np.float32)
         _check(_lib.hvvr_batch_read_timings(self.handle, t.ctypes.data))
         return t
+
+
+def server_config(**kw):
+    """hvvr_server_config with the library defaults, overridden by keyword."""
+    cfg = _abi.ServerConfig()
+    _lib.hvvr_server_config_default(C.byref(cfg))
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+class Server:
+    """Render-request server over resident scenes (raycasters): admission against an HBM
+    budget, continuous batching into frame batches, completions with timestamps."""
+
+    def __init__(self, raycasters, config=None):
+        arr = (_vp * len(raycasters))(*[r.handle for r in raycasters])
+        h = _vp()
+        _check(_lib.hvvr_server_create(arr, len(raycasters), C.byref(config) if config is not None else None,
+                                       C.byref(h)))
+        self.handle = h
+        self.raycasters = list(raycasters)
+        self.views = []
+        for r in self.raycasters:
+            r.batches.append(self)  # closed before its raycasters
+
+    def close(self):
+        if self.handle:
+            _check(_lib.hvvr_server_destroy(self.handle))
+            self.handle = None
+            for r in self.raycasters:
+                if self in r.batches:
+                    r.batches.remove(self)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_view(self, scene_index, viewport, samples, width, height, split=1):
+        samples = np.ascontiguousarray(samples, dtype=_abi.SAMPLE_DTYPE)
+        vid = _u32(0)
+        _check(_lib.hvvr_server_add_view(self.handle, scene_index, C.byref(viewport), samples.ctypes.data,
+                                         len(samples), split, width, height, C.byref(vid)))
+        self.views.append((width, height, len(samples)))
+        return vid.value
+
+    def submit(self, view, msaa, camera_to_world, output=None, device_ptr=None, tag=0):
+        """output: a (height, width) uint32 numpy array (CPU), or device_ptr for CUDA memory"""
+        r = _abi.Request()
+        r.view, r.msaa, r.camera_to_world, r.tag = view, msaa, camera_to_world, tag
+        if device_ptr is not None:
+            r.memory_type, r.output = HVVR_MEMORY_CUDA, device_ptr
+        else:
+            assert output.flags["C_CONTIGUOUS"] and output.dtype == np.uint32
+            r.memory_type, r.output = HVVR_MEMORY_CPU, output.ctypes.data
+        rid = C.c_uint64(0)
+        _check(_lib.hvvr_server_submit(self.handle, C.byref(r), C.byref(rid)))
+        return rid.value
+
+    def poll(self, capacity=256, wait_ms=0.0):
+        out = (_abi.Completion * capacity)()
+        n = _u32(0)
+        _check(_lib.hvvr_server_poll(self.handle, out, capacity, C.byref(n), C.c_double(wait_ms)))
+        return [out[i] for i in range(n.value)]
+
+    def update_vertices(self, model, first, count, device_ptr):
+        _check(_lib.hvvr_server_update_vertices(self.handle, model.handle, first, count, _vp(device_ptr)))
+
+    def stats(self):
+        st = _abi.ServerStats()
+        _check(_lib.hvvr_server_get_stats(self.handle, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}

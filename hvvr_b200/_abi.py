@@ -102,6 +102,28 @@ class BatchConfig(C.Structure):
                 ("use_graph", C.c_uint32), ("frame_ms", C.c_float), ("tile_stack_entries", C.c_uint32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch_views", C.c_uint32),
+                ("slot_list_capacity", C.c_uint64), ("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("view", C.c_uint32), ("msaa", C.c_uint32), ("camera_to_world", Transform),
+                ("memory_type", C.c_uint32), ("output", C.c_void_p), ("tag", C.c_uint64)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("tag", C.c_uint64), ("status", C.c_int), ("batch_views", C.c_uint32),
+                ("submit_ms", C.c_double), ("dispatch_ms", C.c_double), ("done_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("queued", C.c_uint64), ("in_flight", C.c_uint64),
+                ("instances", C.c_uint64), ("hbm_used", C.c_uint64), ("hbm_peak", C.c_uint64),
+                ("mean_batch_views", C.c_double), ("evicted", C.c_uint64)]
+
+
 # numpy layouts of the bulk arrays
 SAMPLE_DTYPE = np.dtype([("pixel", "<u4", 2), ("position", "<f4", 2), ("minor", "<f4", 2), ("major", "<f4")])
 VERTEX_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<u2", 4), ("uv", "<f4", 2), ("pad", "<u4")])

@@ -1,0 +1,212 @@
+// host_objects.h - the library's host-side objects (raycaster, scene models, lights, cameras,
+// frame batches) and the frame driver entry points shared by raycaster.cpp and server.cpp.
+// Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <stdint.h>
+
+#include <atomic>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hvvr_c.h"
+#include "host_setup.h"
+#include "hvvr_internal.h"
+
+namespace hvb {
+
+// records a printf-style message for hvvr_last_error() on this thread and returns code
+int fail(int code, const char* fmt, ...);
+
+#define CUDA_TRY(expr)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? HVVR_ERR_OOM : HVVR_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #expr, cudaGetErrorString(e_), __FILE__, __LINE__);                               \
+    } while (0)
+
+#define TRY(expr)                \
+    do {                         \
+        int r_ = (expr);         \
+        if (r_ != HVVR_OK) return r_; \
+    } while (0)
+
+// owning device allocation
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count) {
+        if (count == n && p) return HVVR_OK;
+        release();
+        if (count == 0) return HVVR_OK;
+        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(HVVR_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        n = count;
+        return HVVR_OK;
+    }
+    // grows only (a smaller request keeps the buffer: no free, which would synchronise the device)
+    int ensure(size_t count) {
+        if (count <= n && (p || count == 0)) return HVVR_OK;
+        return alloc(count);
+    }
+    int upload(const void* src, size_t count, cudaStream_t st) {
+        TRY(alloc(count));
+        if (count) CUDA_TRY(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
+        return HVVR_OK;
+    }
+};
+
+} // namespace hvb
+
+// the object structs below are the C ABI's opaque types (global namespace)
+using namespace hvb;
+
+struct hvvr_model {
+    hvvr_raycaster* rc = nullptr;
+    std::vector<hvvr_shading_vertex> verts;
+    std::vector<hvvr_tri_shade> triShade;
+    std::vector<hvvr_topology_node> nodes;
+    std::vector<hvvr_material> materials;
+    hvvr_transform xf{};
+};
+
+struct hvvr_light {
+    hvvr_raycaster* rc = nullptr;
+    hvvr_light_union light{};
+};
+
+struct hvvr_camera {
+    hvvr_raycaster* rc = nullptr;
+    bool enabled = true;
+    hvvr_float_rect viewport{};
+    hvvr_thin_lens lens{0.0f, 1.0f};
+    hvvr_vec3 eyeDir{0.0f, 0.0f, -1.0f};
+    float fovX = 0.0f, fovY = 0.0f;
+    hvvr_image_desc target{};
+    std::vector<hvvr_sample> samples;
+    uint32_t split = 1;
+    hvvr_transform xf{};
+    uint32_t msaa = 16;
+    uint32_t capture = 0;
+    bool setupDirty = true;
+    bool rendered = false;
+    bool hidden = false;              // a server's camera: rendered only by batches that name it
+    uint64_t setupGen = 0;            // process-unique id of the current sample setup and buffers
+    uint64_t costFrames = 0;          // frames rendered since the setup (tileCost is valid when > 0)
+    hvvr_batch* lastBatch = nullptr;  // batch whose pool holds this camera's last tile lists
+    std::vector<hvvr_batch*> batches; // camera-list batches that name this camera
+    CameraDev dev;
+    SampleSetup setup;
+    // device storage behind dev
+    DevBuf<Rays4> tileRays, blockRays;
+    DevBuf<float4> beams;
+    DevBuf<int32_t> remap;
+    DevBuf<StackEntry> blockStacks;
+    DevBuf<uint32_t> blockSizes;
+    DevBuf<TileList> tileLists;
+    DevBuf<uint32_t> colors, hitIds, image, tileCost;
+    DevBuf<float> depth;
+    void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
+};
+
+// A frame batch: the enabled cameras of one or more raycasters (one scene each, same device)
+// rendered as one frame - one launch per stage over all views, the tile cull as one
+// persistent work queue, intersect/shade once per MSAA rate - optionally replayed from a
+// CUDA graph. Every raycaster renders its own cameras through an internal batch.
+struct hvvr_batch {
+    std::vector<hvvr_raycaster*> rcs;
+    bool fixedViews = false;          // renders exactly `cams` (else every enabled camera of rcs)
+    std::vector<hvvr_camera*> cams;
+    bool internal = false;            // a raycaster's own batch
+    bool detached = false;            // one of its raycasters was destroyed
+    hvvr_batch_config cfg{};
+    // layout of the current frame
+    struct View {
+        hvvr_camera* cam;
+        uint32_t tileStart, blockStart;
+    };
+    std::vector<View> views;
+    std::vector<uint64_t> layoutKey;
+    uint32_t tiles = 0, blocks = 0;
+    uint32_t rateTiles[6] = {}, rateStart[6] = {};
+    bool fpStrict = false;
+    bool costValid = false;           // every view's tileCost holds a previous frame's counts
+    DevBuf<ViewDev> viewsDev;
+    DevBuf<uint32_t> blockView, order, retry, pool, chunkNext, counters;
+    uint32_t poolChunks = 0;
+    ViewDev* hostViews[2] = {};       // pinned staging of the per-frame view table
+    size_t hostViewsCap = 0;
+    cudaEvent_t hostViewsEv[2] = {};
+    bool hostViewsUsed[2] = {};
+    int hostSlot = 0;
+    uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
+    bool counterValid = false;
+    cudaStream_t side[12] = {};       // per rate: [2r] heavy tiles (high priority), [2r+1] the rest
+    cudaEvent_t forkEv = nullptr, doneEv[12] = {}, ev[6] = {};
+    cudaEvent_t kev[12][3] = {};      // per side stream: before tile cull, after it, after intersect
+    bool kevUsed[12] = {};
+    bool stageTimes = false;          // ev[1..4] and kev were recorded by the last frame
+    cudaGraphExec_t graph = nullptr;
+    std::vector<uint64_t> graphKey;
+};
+
+struct hvvr_raycaster {
+    hvvr_spec spec{};
+    cudaStream_t stream = nullptr;
+    std::vector<std::unique_ptr<hvvr_model>> models;
+    std::vector<std::unique_ptr<hvvr_light>> lights;
+    std::vector<std::unique_ptr<hvvr_camera>> cameras;
+    bool sceneDirty = true;
+    bool refitDirty = true;
+    SceneDev scene;
+    DevBuf<Node> nodes;
+    DevBuf<float4> tris, vertsIn, verts, materials;
+    DevBuf<uint4> triShade;
+    DevBuf<uint32_t> vertModel, parentSlot, internalCount, arrivals, refitStarts;
+    DevBuf<Mat4> modelToWorld;
+    std::vector<Node> hostNodes;
+    uint32_t refitStatus = 0;
+    std::unique_ptr<hvvr_batch> own;      // renders this raycaster's cameras
+    std::vector<hvvr_batch*> batches;     // user batches that include this raycaster
+};
+
+namespace hvb {
+
+constexpr uint64_t kDefaultCapacity = 128ull << 20; // MAX_TRI_INDICES_TO_INTERSECT
+
+int uploadScene(hvvr_raycaster* rc, cudaStream_t st);
+int setupCamera(hvvr_camera* cam, cudaStream_t st);
+void releaseCamera(hvvr_camera* cam);
+void batchConfigDefault(hvvr_batch_config* c);
+int checkConfig(const hvvr_batch_config& c);
+void releaseBatch(hvvr_batch* b);
+int checkStatus(const hvvr_batch* b);
+uint32_t rateIndex(uint32_t rate);
+// scene update and refit of the batch's raycasters (unless skipScenes), then one frame of its views on st
+int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes = false);
+// uploads the MSAA offset table of `rate` to the current device once
+int ensureMsaaTable(uint32_t rate, cudaStream_t st);
+// a new camera of the same raycaster with cam's sample set and setup (device copies, no
+// re-clustering); cam must have been set up (rendered once)
+int cloneCamera(const hvvr_camera* cam, hvvr_camera** out);
+// device bytes a camera holds for its setup and per-frame buffers at the given MSAA rate
+size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa);
+
+} // namespace hvb

@@ -15,17 +15,16 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
 
-#include "../../include/hvvr_c.h"
-#include "host_setup.h"
-#include "hvvr_internal.h"
+#include "host_objects.h"
 
 using namespace hvb;
 
-namespace {
+namespace hvb {
 
 thread_local std::string gLastError;
 
@@ -39,169 +38,15 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define CUDA_TRY(expr)                                                                                    \
-    do {                                                                                                  \
-        cudaError_t e_ = (expr);                                                                          \
-        if (e_ != cudaSuccess)                                                                            \
-            return fail(e_ == cudaErrorMemoryAllocation ? HVVR_ERR_OOM : HVVR_ERR_CUDA, "%s: %s (%s:%d)", \
-                        #expr, cudaGetErrorString(e_), __FILE__, __LINE__);                               \
-    } while (0)
+} // namespace hvb
 
-#define TRY(expr)                \
-    do {                         \
-        int r_ = (expr);         \
-        if (r_ != HVVR_OK) return r_; \
-    } while (0)
-
-// owning device allocation
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    int alloc(size_t count) {
-        if (count == n && p) return HVVR_OK;
-        release();
-        if (count == 0) return HVVR_OK;
-        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return fail(HVVR_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
-        }
-        n = count;
-        return HVVR_OK;
-    }
-    int upload(const void* src, size_t count, cudaStream_t st) {
-        TRY(alloc(count));
-        if (count) CUDA_TRY(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
-        return HVVR_OK;
-    }
-};
-
-} // namespace
 
 int hvb::setLastError(int code, const char* msg) {
     gLastError = msg ? msg : "";
     return code;
 }
 
-struct hvvr_model {
-    hvvr_raycaster* rc = nullptr;
-    std::vector<hvvr_shading_vertex> verts;
-    std::vector<hvvr_tri_shade> triShade;
-    std::vector<hvvr_topology_node> nodes;
-    std::vector<hvvr_material> materials;
-    hvvr_transform xf{};
-};
-
-struct hvvr_light {
-    hvvr_raycaster* rc = nullptr;
-    hvvr_light_union light{};
-};
-
-struct hvvr_camera {
-    hvvr_raycaster* rc = nullptr;
-    bool enabled = true;
-    hvvr_float_rect viewport{};
-    hvvr_thin_lens lens{0.0f, 1.0f};
-    hvvr_vec3 eyeDir{0.0f, 0.0f, -1.0f};
-    float fovX = 0.0f, fovY = 0.0f;
-    hvvr_image_desc target{};
-    std::vector<hvvr_sample> samples;
-    uint32_t split = 1;
-    hvvr_transform xf{};
-    uint32_t msaa = 16;
-    uint32_t capture = 0;
-    bool setupDirty = true;
-    bool rendered = false;
-    uint64_t setupGen = 0;            // process-unique id of the current sample setup and buffers
-    hvvr_batch* lastBatch = nullptr;  // batch whose pool holds this camera's last tile lists
-    std::vector<hvvr_batch*> batches; // camera-list batches that name this camera
-    CameraDev dev;
-    SampleSetup setup;
-    // device storage behind dev
-    DevBuf<Rays4> tileRays, blockRays;
-    DevBuf<float4> beams;
-    DevBuf<int32_t> remap;
-    DevBuf<StackEntry> blockStacks;
-    DevBuf<uint32_t> blockSizes;
-    DevBuf<TileList> tileLists;
-    DevBuf<uint32_t> colors, hitIds, image, tileCost;
-    DevBuf<float> depth;
-    void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
-};
-
-// A frame batch: the enabled cameras of one or more raycasters (one scene each, same device)
-// rendered as one frame - one launch per stage over all views, the tile cull as one
-// persistent work queue, intersect/shade once per MSAA rate - optionally replayed from a
-// CUDA graph. Every raycaster renders its own cameras through an internal batch.
-struct hvvr_batch {
-    std::vector<hvvr_raycaster*> rcs;
-    bool fixedViews = false;          // renders exactly `cams` (else every enabled camera of rcs)
-    std::vector<hvvr_camera*> cams;
-    bool internal = false;            // a raycaster's own batch
-    bool detached = false;            // one of its raycasters was destroyed
-    hvvr_batch_config cfg{};
-    // layout of the current frame
-    struct View {
-        hvvr_camera* cam;
-        uint32_t tileStart, blockStart;
-    };
-    std::vector<View> views;
-    std::vector<uint64_t> layoutKey;
-    uint32_t tiles = 0, blocks = 0;
-    uint32_t rateTiles[6] = {}, rateStart[6] = {};
-    bool fpStrict = false;
-    bool costValid = false;           // every view's tileCost holds a previous frame's counts
-    DevBuf<ViewDev> viewsDev;
-    DevBuf<uint32_t> blockView, order, retry, pool, chunkNext, counters;
-    uint32_t poolChunks = 0;
-    ViewDev* hostViews[2] = {};       // pinned staging of the per-frame view table
-    size_t hostViewsCap = 0;
-    cudaEvent_t hostViewsEv[2] = {};
-    bool hostViewsUsed[2] = {};
-    int hostSlot = 0;
-    uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
-    bool counterValid = false;
-    cudaStream_t side[12] = {};       // per rate: [2r] heavy tiles (high priority), [2r+1] the rest
-    cudaEvent_t forkEv = nullptr, doneEv[12] = {}, ev[6] = {};
-    cudaEvent_t kev[12][3] = {};      // per side stream: before tile cull, after it, after intersect
-    bool kevUsed[12] = {};
-    bool stageTimes = false;          // ev[1..4] and kev were recorded by the last frame
-    cudaGraphExec_t graph = nullptr;
-    std::vector<uint64_t> graphKey;
-};
-
-struct hvvr_raycaster {
-    hvvr_spec spec{};
-    cudaStream_t stream = nullptr;
-    std::vector<std::unique_ptr<hvvr_model>> models;
-    std::vector<std::unique_ptr<hvvr_light>> lights;
-    std::vector<std::unique_ptr<hvvr_camera>> cameras;
-    bool sceneDirty = true;
-    bool refitDirty = true;
-    bool msaaUploaded[33] = {};
-    SceneDev scene;
-    DevBuf<Node> nodes;
-    DevBuf<float4> tris, vertsIn, verts, materials;
-    DevBuf<uint4> triShade;
-    DevBuf<uint32_t> vertModel, parentSlot, internalCount, arrivals, refitStarts;
-    DevBuf<Mat4> modelToWorld;
-    std::vector<Node> hostNodes;
-    uint32_t refitStatus = 0;
-    std::unique_ptr<hvvr_batch> own;      // renders this raycaster's cameras
-    std::vector<hvvr_batch*> batches;     // user batches that include this raycaster
-};
-
-namespace {
+namespace hvb {
 
 const char* kEmpty = "";
 
@@ -437,6 +282,7 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     }
     cam->setupDirty = false;
     cam->setupGen = ++gSetupGen;
+    cam->costFrames = 0;
     return HVVR_OK;
 }
 
@@ -453,7 +299,90 @@ void releaseCamera(hvvr_camera* cam) { unregisterTarget(cam); }
 
 uint32_t rateIndex(uint32_t rate) { return rate <= 1 ? 0u : uint32_t(31 - __builtin_clz(rate)); }
 
-constexpr uint64_t kDefaultCapacity = 128ull << 20; // MAX_TRI_INDICES_TO_INTERSECT
+// the offset tables live in one __constant__ array per device, written once per rate
+int ensureMsaaTable(uint32_t rate, cudaStream_t st) {
+    static std::mutex mu;
+    static bool uploaded[64][6] = {};
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(HVVR_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    bool& done = uploaded[dev][rateIndex(rate)];
+    if (done) return HVVR_OK;
+    float off[64];
+    msaaOffsets(rate, off);
+    CUDA_TRY(uploadMsaaTable(rate, off, st));
+    CUDA_TRY(cudaStreamSynchronize(st)); // visible before any other stream can use the rate
+    done = true;
+    return HVVR_OK;
+}
+
+size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa) {
+    const SampleSetup& ss = cam->setup;
+    size_t b = ss.tileRays.size() * sizeof(Rays4) + ss.blockRays.size() * sizeof(Rays4) + ss.beams.size() * 4 +
+               ss.remap.size() * 4;
+    b += size_t(ss.blocks) * kBlockStack * sizeof(StackEntry) + size_t(ss.blocks) * 4;
+    b += size_t(ss.tiles) * (sizeof(TileList) + 4) + size_t(ss.padded) * 4;
+    if (cam->target.memory_type == HVVR_MEMORY_CPU) b += size_t(cam->target.width) * cam->target.height * 4;
+    if (cam->capture & HVVR_CAPTURE_HITS) b += size_t(ss.padded) * msaa * 8;
+    return b;
+}
+
+int cloneCamera(const hvvr_camera* src, hvvr_camera** out) {
+    if (src->setupDirty) return fail(HVVR_ERR_STATE, "camera to clone has no setup yet");
+    auto c = std::make_unique<hvvr_camera>();
+    c->rc = src->rc;
+    c->viewport = src->viewport;
+    c->lens = src->lens;
+    c->eyeDir = src->eyeDir;
+    c->fovX = src->fovX;
+    c->fovY = src->fovY;
+    c->target = src->target;
+    c->target.data = nullptr;
+    c->samples = src->samples;
+    c->split = src->split;
+    c->xf = src->xf;
+    c->msaa = src->msaa;
+    c->setup = src->setup;
+    const SampleSetup& ss = c->setup;
+    const cudaStream_t st = src->rc->stream;
+    TRY(c->tileRays.alloc(ss.tileRays.size()));
+    TRY(c->blockRays.alloc(ss.blockRays.size()));
+    TRY(c->beams.alloc(ss.beams.size() / 4));
+    TRY(c->remap.alloc(ss.remap.size()));
+    CUDA_TRY(cudaMemcpyAsync(c->tileRays.p, src->tileRays.p, ss.tileRays.size() * sizeof(Rays4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->blockRays.p, src->blockRays.p, ss.blockRays.size() * sizeof(Rays4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->beams.p, src->beams.p, ss.beams.size() * 4, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->remap.p, src->remap.p, ss.remap.size() * 4, cudaMemcpyDeviceToDevice, st));
+    TRY(c->blockStacks.alloc(size_t(ss.blocks) * kBlockStack));
+    TRY(c->blockSizes.alloc(ss.blocks));
+    TRY(c->tileLists.alloc(ss.tiles));
+    TRY(c->colors.alloc(ss.padded));
+    TRY(c->tileCost.alloc(ss.tiles));
+    CUDA_TRY(cudaMemcpyAsync(c->tileCost.p, src->tileCost.p, size_t(ss.tiles) * 4, cudaMemcpyDeviceToDevice, st));
+    c->dev = src->dev;
+    CameraDev& d = c->dev;
+    d.tileRays = c->tileRays.p;
+    d.blockRays = c->blockRays.p;
+    d.beams = c->beams.p;
+    d.remap = c->remap.p;
+    d.blockStacks = c->blockStacks.p;
+    d.blockSizes = c->blockSizes.p;
+    d.tileLists = c->tileLists.p;
+    d.tileCost = c->tileCost.p;
+    d.colors = c->colors.p;
+    d.hitIds = nullptr;
+    d.depth = nullptr;
+    d.image = nullptr;
+    c->costFrames = src->costFrames;
+    c->setupDirty = false;
+    c->setupGen = ++gSetupGen;
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *out = c.get();
+    src->rc->cameras.push_back(std::move(c));
+    return HVVR_OK;
+}
+
 // rate groups with fewer tiles are not split
 constexpr uint32_t kSplitMinTiles = 32;
 
@@ -604,7 +533,7 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
 }
 
 // Scene update and refit of every raycaster, then one frame of all their enabled cameras.
-int renderBatch(hvvr_batch* b, cudaStream_t st) {
+int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     if (b->detached) return fail(HVVR_ERR_STATE, "a raycaster of this batch was destroyed");
     if (b->rcs.empty()) return HVVR_OK;
     const int device = b->rcs[0]->spec.device;
@@ -614,6 +543,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
         if (rc->spec.device != device) return fail(HVVR_ERR_INVALID, "batched raycasters must share one device");
         if ((rc->spec.fp_mode == HVVR_FP_STRICT) != strict)
             return fail(HVVR_ERR_INVALID, "batched raycasters must share one fp_mode");
+        if (skipScenes) continue;
         if (rc->sceneDirty) {
             TRY(uploadScene(rc, st));
             rc->sceneDirty = false;
@@ -629,7 +559,8 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
         candidates = b->cams;
     } else {
         for (hvvr_raycaster* rc : b->rcs)
-            for (auto& cp : rc->cameras) candidates.push_back(cp.get());
+            for (auto& cp : rc->cameras)
+                if (!cp->hidden) candidates.push_back(cp.get());
     }
     bool cpuTargets = false, capturable = true;
     {
@@ -637,12 +568,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
             hvvr_raycaster* rc = c->rc;
             if (rc->scene.nodeCount == 0 || !c->enabled || c->samples.empty()) continue;
             if (c->setupDirty) TRY(setupCamera(c, st));
-            if (!rc->msaaUploaded[c->msaa]) {
-                float off[64];
-                msaaOffsets(c->msaa, off);
-                CUDA_TRY(uploadMsaaTable(c->msaa, off, st));
-                rc->msaaUploaded[c->msaa] = true;
-            }
+            TRY(ensureMsaaTable(c->msaa, st));
             CameraDev& d = c->dev;
             d.msaa = c->msaa;
             if (c->capture & HVVR_CAPTURE_HITS) {
@@ -690,10 +616,11 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
             b->rateStart[r] = run;
             run += rateTiles[r];
         }
-        TRY(b->blockView.upload(blockView.data(), blockView.size(), st));
-        TRY(b->order.alloc(b->tiles));
-        TRY(b->retry.alloc(b->tiles));
-        TRY(b->viewsDev.alloc(b->views.size()));
+        TRY(b->blockView.ensure(blockView.size()));
+        CUDA_TRY(cudaMemcpyAsync(b->blockView.p, blockView.data(), blockView.size() * 4, cudaMemcpyHostToDevice, st));
+        TRY(b->order.ensure(b->tiles));
+        TRY(b->retry.ensure(b->tiles));
+        TRY(b->viewsDev.ensure(b->views.size()));
         if (b->hostViewsCap < b->views.size()) {
             for (int k = 0; k < 2; k++) {
                 if (b->hostViewsUsed[k]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[k]));
@@ -707,7 +634,8 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
             b->hostViewsCap = b->views.size();
         }
         b->layoutKey = key;
-        b->costValid = false;
+        // scheduling by last frame's cost needs a previous frame of every camera in the layout
+        b->costValid = std::all_of(cams.begin(), cams.end(), [](const hvvr_camera* c) { return c->costFrames > 0; });
         dropGraph(b);
     }
     b->fpStrict = strict;
@@ -795,6 +723,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
     for (hvvr_camera* c : cams) {
         c->lastBatch = b;
         c->rendered = true;
+        c->costFrames++;
     }
     b->costValid = true; // the next frame schedules its tiles by this frame's visit counts
     b->counterValid = true;
@@ -805,7 +734,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st) {
     return HVVR_OK;
 }
 
-} // namespace
+} // namespace hvb
 
 extern "C" {
 

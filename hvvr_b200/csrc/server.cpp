@@ -1,0 +1,550 @@
+// server.cpp - hvvr_server: a render-request loop with admission control and continuous
+// batching over resident scenes (no counterpart in the reference, whose Raycaster renders
+// its cameras once per render() call).
+//
+// Requests name a view template (a sample set and viewport over one resident scene, clustered
+// once when the template is added), an MSAA rate, a camera pose and an output image. One
+// worker thread owns all GPU work of the server:
+//   * admission - a request needs a camera instance of its template: a free one from the
+//     template's pool, or a new clone (device copies of the template's setup) if the device
+//     memory of all instances plus the slots' triangle-list pools stays within the HBM budget.
+//     Requests that cannot be admitted wait; later requests that fit may go first.
+//   * batching - up to max_batch_views admitted requests form one frame batch (one launch per
+//     stage over all views, traversal as one longest-first work queue) on a free slot. Up to
+//     `slots` batches are in flight on their own streams, so requests that arrive while a batch
+//     runs are rendered by the next one, overlapping on the device.
+//     When the budget is short, idle instances of other templates are freed first.
+//   * completion - a slot whose end event has fired returns its instances to the pools and its
+//     requests to the completion queue (CPU outputs are copied out of pinned staging first).
+//   * animation - vertex updates are staged on the device when submitted and applied between
+//     batches: the worker waits until no batch is in flight, copies them into the scenes,
+//     refits on the device and makes every slot stream wait for the refit.
+// A request's image does not depend on the other requests of its batch: each view is a
+// separate camera with its own buffers and the kernels are per tile, so the result is the
+// same alone and in any mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include <string.h>
+
+#include "host_objects.h"
+
+using namespace hvb;
+
+namespace {
+
+struct Template {
+    hvvr_raycaster* rc = nullptr;
+    hvvr_camera* proto = nullptr;
+    uint32_t width = 0, height = 0;
+    uint32_t samples = 0;
+    size_t instBytes = 0;
+    std::vector<struct Instance*> freeList;
+};
+
+struct Instance {
+    hvvr_camera* cam = nullptr;
+    uint32_t tmpl = 0;
+    DevBuf<uint32_t> image;         // device image the remap writes (CPU outputs and as scratch)
+    uint32_t* staging = nullptr;    // pinned copy of image for CPU outputs
+    size_t bytes = 0;
+};
+
+struct Request {
+    uint64_t id = 0;
+    hvvr_request r{};
+    double submitMs = 0, dispatchMs = 0, doneMs = 0;
+    int status = HVVR_OK;
+    Instance* inst = nullptr;
+    uint32_t batchViews = 0;
+};
+
+struct Update {
+    hvvr_raycaster* rc = nullptr;
+    size_t vertOffset = 0;   // in vertices, into the scene's concatenated vertex array
+    uint32_t count = 0;
+    DevBuf<float4> verts;    // 2 float4 per vertex
+};
+
+struct Slot {
+    std::unique_ptr<hvvr_batch> batch;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<Request*> reqs;
+    bool busy = false;
+};
+
+} // namespace
+
+struct hvvr_server {
+    hvvr_server_config cfg{};
+    std::vector<hvvr_raycaster*> scenes;
+    std::vector<Template> templates;
+    std::vector<std::unique_ptr<Instance>> instances;
+    std::vector<Slot> slots;
+    cudaStream_t updateStream = nullptr;
+    cudaEvent_t updateEv = nullptr;
+    size_t poolBytes = 0, memUsed = 0, memPeak = 0;
+
+    std::mutex mu;                       // guards everything below
+    std::condition_variable workCv, doneCv;
+    std::deque<Request*> pending;
+    std::vector<std::unique_ptr<Update>> updates;
+    std::deque<hvvr_completion> completions;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> live;
+    uint64_t nextId = 1;
+    hvvr_server_stats stats{};
+    uint64_t viewsDispatched = 0;
+    bool stop = false;
+    std::string workerError;
+
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    std::thread worker;
+
+    double nowMs() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+// returns instance for template t or nullptr when the budget does not allow a new one
+Instance* takeInstance(hvvr_server* s, uint32_t t) {
+    Template& tp = s->templates[t];
+    if (!tp.freeList.empty()) {
+        Instance* i = tp.freeList.back();
+        tp.freeList.pop_back();
+        return i;
+    }
+    if (s->memUsed + tp.instBytes > s->cfg.hbm_budget_bytes) {
+        // evict idle instances of other templates, largest first, until this one fits
+        std::vector<Instance*> idle;
+        for (uint32_t k = 0; k < s->templates.size(); k++)
+            if (k != t)
+                for (Instance* i : s->templates[k].freeList) idle.push_back(i);
+        std::sort(idle.begin(), idle.end(), [](const Instance* a, const Instance* b) { return a->bytes > b->bytes; });
+        size_t freeable = 0;
+        for (Instance* i : idle) freeable += i->bytes;
+        if (s->memUsed - freeable + tp.instBytes > s->cfg.hbm_budget_bytes) return nullptr;
+        for (Instance* i : idle) {
+            if (s->memUsed + tp.instBytes <= s->cfg.hbm_budget_bytes) break;
+            auto& fl = s->templates[i->tmpl].freeList;
+            fl.erase(std::remove(fl.begin(), fl.end(), i), fl.end());
+            if (i->staging) cudaFreeHost(i->staging);
+            hvvr_camera_destroy(i->cam->rc, i->cam);
+            s->memUsed -= i->bytes;
+            s->stats.evicted++;
+            s->instances.erase(std::remove_if(s->instances.begin(), s->instances.end(),
+                                              [&](const std::unique_ptr<Instance>& p) { return p.get() == i; }),
+                               s->instances.end());
+        }
+    }
+    auto inst = std::make_unique<Instance>();
+    hvvr_camera* cam = nullptr;
+    if (cloneCamera(tp.proto, &cam) != HVVR_OK) return nullptr;
+    cam->hidden = true;
+    inst->cam = cam;
+    inst->tmpl = t;
+    if (inst->image.alloc(size_t(tp.width) * tp.height) != HVVR_OK ||
+        cudaMallocHost((void**)&inst->staging, size_t(tp.width) * tp.height * 4) != cudaSuccess) {
+        cudaGetLastError();
+        inst->staging = nullptr;
+        hvvr_camera_destroy(cam->rc, cam);
+        return nullptr;
+    }
+    inst->bytes = tp.instBytes;
+    s->memUsed += inst->bytes;
+    s->memPeak = std::max(s->memPeak, s->memUsed);
+    Instance* raw = inst.get();
+    s->instances.push_back(std::move(inst));
+    return raw;
+}
+
+void complete(hvvr_server* s, Request* r, int status) {
+    r->status = status;
+    r->doneMs = s->nowMs();
+    hvvr_completion c{};
+    c.id = r->id;
+    c.tag = r->r.tag;
+    c.status = status;
+    c.submit_ms = r->submitMs;
+    c.dispatch_ms = r->dispatchMs;
+    c.done_ms = r->doneMs;
+    c.batch_views = r->batchViews;
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->completions.push_back(c);
+    if (status == HVVR_OK) s->stats.completed++;
+    else s->stats.failed++;
+    s->stats.in_flight--;
+    s->live.erase(r->id);
+    s->doneCv.notify_all();
+}
+
+void finishSlot(hvvr_server* s, Slot& sl) {
+    const int st = checkStatus(sl.batch.get());
+    for (Request* r : sl.reqs) {
+        Instance* in = r->inst;
+        const Template& tp = s->templates[in->tmpl];
+        if (st == HVVR_OK && r->r.memory_type == HVVR_MEMORY_CPU)
+            memcpy(r->r.output, in->staging, size_t(tp.width) * tp.height * 4);
+        s->templates[in->tmpl].freeList.push_back(in);
+        complete(s, r, st);
+    }
+    sl.reqs.clear();
+    sl.busy = false;
+}
+
+// applies staged vertex updates (no batch in flight) and refits the touched scenes
+int applyUpdates(hvvr_server* s, std::vector<std::unique_ptr<Update>>& ups) {
+    std::vector<hvvr_raycaster*> touched;
+    for (auto& u : ups) {
+        CUDA_TRY(cudaMemcpyAsync(u->rc->vertsIn.p + 2 * u->vertOffset, u->verts.p, size_t(u->count) * 32,
+                                 cudaMemcpyDeviceToDevice, s->updateStream));
+        if (std::find(touched.begin(), touched.end(), u->rc) == touched.end()) touched.push_back(u->rc);
+    }
+    for (hvvr_raycaster* rc : touched) {
+        CUDA_TRY(launchRefit(rc->scene, s->updateStream));
+        rc->refitDirty = false;
+    }
+    CUDA_TRY(cudaEventRecord(s->updateEv, s->updateStream));
+    for (Slot& sl : s->slots) CUDA_TRY(cudaStreamWaitEvent(sl.stream, s->updateEv, 0));
+    CUDA_TRY(cudaStreamSynchronize(s->updateStream)); // staging buffers are released after this
+    return HVVR_OK;
+}
+
+// forms and launches one batch on slot sl from the pending requests; false if none admitted
+bool dispatch(hvvr_server* s, Slot& sl) {
+    std::vector<Request*> take;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        for (auto it = s->pending.begin(); it != s->pending.end() && take.size() < s->cfg.max_batch_views;) {
+            Request* r = *it;
+            Instance* in = takeInstance(s, r->r.view);
+            if (!in) {
+                ++it;
+                continue;
+            }
+            r->inst = in;
+            take.push_back(r);
+            it = s->pending.erase(it);
+        }
+        s->stats.queued = s->pending.size();
+    }
+    if (take.empty()) return false;
+    hvvr_batch* b = sl.batch.get();
+    b->cams.clear();
+    const double now = s->nowMs();
+    for (Request* r : take) {
+        Instance* in = r->inst;
+        hvvr_camera* c = in->cam;
+        const Template& tp = s->templates[in->tmpl];
+        c->xf = r->r.camera_to_world;
+        c->msaa = r->r.msaa;
+        uint32_t* img = r->r.memory_type == HVVR_MEMORY_CUDA ? static_cast<uint32_t*>(r->r.output) : in->image.p;
+        c->target.memory_type = HVVR_MEMORY_CUDA;
+        c->target.data = img;
+        c->target.width = tp.width;
+        c->target.height = tp.height;
+        c->target.stride = tp.width;
+        c->dev.image = img;
+        c->dev.imageStride = tp.width;
+        b->cams.push_back(c);
+        r->dispatchMs = now;
+        r->batchViews = uint32_t(take.size());
+    }
+    int rc = renderBatch(b, sl.stream, true);
+    if (rc == HVVR_OK) {
+        for (Request* r : take) {
+            if (r->r.memory_type != HVVR_MEMORY_CPU) continue;
+            const Template& tp = s->templates[r->inst->tmpl];
+            if (cudaMemcpyAsync(r->inst->staging, r->inst->image.p, size_t(tp.width) * tp.height * 4,
+                                cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess)
+                rc = fail(HVVR_ERR_CUDA, "output copy failed");
+        }
+    }
+    if (rc == HVVR_OK && cudaEventRecord(sl.done, sl.stream) != cudaSuccess) rc = fail(HVVR_ERR_CUDA, "event record failed");
+    if (rc != HVVR_OK) {
+        cudaStreamSynchronize(sl.stream);
+        for (Request* r : take) {
+            s->templates[r->inst->tmpl].freeList.push_back(r->inst);
+            complete(s, r, rc);
+        }
+        return true;
+    }
+    sl.reqs = take;
+    sl.busy = true;
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stats.batches++;
+    s->viewsDispatched += take.size();
+    return true;
+}
+
+void workerLoop(hvvr_server* s) {
+    cudaSetDevice(s->scenes[0]->spec.device);
+    std::vector<std::unique_ptr<Update>> ups;
+    for (;;) {
+        bool progress = false;
+        for (Slot& sl : s->slots) {
+            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) {
+                finishSlot(s, sl);
+                progress = true;
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            if (s->stop) break;
+            for (auto& u : s->updates) ups.push_back(std::move(u));
+            s->updates.clear();
+        }
+        bool anyBusy = false;
+        for (Slot& sl : s->slots) anyBusy = anyBusy || sl.busy;
+        if (!ups.empty()) {
+            if (!anyBusy) {
+                if (applyUpdates(s, ups) != HVVR_OK) {
+                    std::lock_guard<std::mutex> lock(s->mu);
+                    s->workerError = hvvr_last_error();
+                }
+                ups.clear();
+                progress = true;
+            }
+        } else {
+            for (Slot& sl : s->slots) {
+                if (sl.busy) continue;
+                if (dispatch(s, sl)) progress = true;
+                else break;
+            }
+        }
+        if (!progress) {
+            std::unique_lock<std::mutex> lock(s->mu);
+            s->workCv.wait_for(lock, std::chrono::microseconds(50));
+        }
+    }
+    for (Slot& sl : s->slots)
+        if (sl.busy) {
+            cudaEventSynchronize(sl.done);
+            finishSlot(s, sl);
+        }
+}
+
+} // namespace
+
+extern "C" {
+
+void hvvr_server_config_default(hvvr_server_config* cfg) {
+    if (!cfg) return;
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->hbm_budget_bytes = 120ull << 30;
+    cfg->slots = 2;
+    cfg->max_batch_views = 64;
+    cfg->slot_list_capacity = 256ull << 20;
+    cfg->tile_cull_warps = 4;
+    cfg->heavy_divisor = 8;
+}
+
+int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr_server_config* cfg,
+                       hvvr_server** out) {
+    if (!out) return fail(HVVR_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scenes || count == 0) return fail(HVVR_ERR_INVALID, "no scenes");
+    auto s = std::make_unique<hvvr_server>();
+    hvvr_server_config_default(&s->cfg);
+    if (cfg) s->cfg = *cfg;
+    if (s->cfg.slots < 1 || s->cfg.slots > 8) return fail(HVVR_ERR_INVALID, "slots must be 1..8");
+    if (s->cfg.max_batch_views < 1) return fail(HVVR_ERR_INVALID, "max_batch_views must be >= 1");
+    for (uint32_t i = 0; i < count; i++) {
+        hvvr_raycaster* rc = scenes[i];
+        if (!rc) return fail(HVVR_ERR_INVALID, "NULL scene %u", i);
+        if (rc->spec.device != scenes[0]->spec.device || rc->spec.fp_mode != scenes[0]->spec.fp_mode)
+            return fail(HVVR_ERR_INVALID, "served scenes must share one device and fp_mode");
+        s->scenes.push_back(rc);
+    }
+    CUDA_TRY(cudaSetDevice(scenes[0]->spec.device));
+    // scenes resident and refit before the first request
+    for (hvvr_raycaster* rc : s->scenes) {
+        if (rc->sceneDirty) {
+            TRY(uploadScene(rc, rc->stream));
+            rc->sceneDirty = false;
+            rc->refitDirty = true;
+        }
+        if (rc->scene.nodeCount && rc->refitDirty) {
+            CUDA_TRY(launchRefit(rc->scene, rc->stream));
+            rc->refitDirty = false;
+        }
+        CUDA_TRY(cudaStreamSynchronize(rc->stream));
+    }
+    for (uint32_t rate : {1u, 2u, 4u, 8u, 16u, 32u}) TRY(ensureMsaaTable(rate, s->scenes[0]->stream));
+    hvvr_batch_config bc;
+    batchConfigDefault(&bc);
+    bc.use_graph = 0; // every batch has its own mix of views
+    bc.tile_cull_warps = s->cfg.tile_cull_warps;
+    bc.heavy_divisor = s->cfg.heavy_divisor;
+    bc.tri_index_capacity = s->cfg.slot_list_capacity;
+    TRY(checkConfig(bc));
+    s->slots.resize(s->cfg.slots);
+    for (Slot& sl : s->slots) {
+        sl.batch = std::make_unique<hvvr_batch>();
+        sl.batch->cfg = bc;
+        sl.batch->fixedViews = true;
+        sl.batch->internal = true;
+        sl.batch->rcs = s->scenes;
+        CUDA_TRY(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->updateStream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&s->updateEv, cudaEventDisableTiming));
+    s->poolBytes = size_t(s->cfg.slots) * size_t(bc.tri_index_capacity) * 4 * (kChunk + 1) / kChunk;
+    if (s->poolBytes > s->cfg.hbm_budget_bytes)
+        return fail(HVVR_ERR_INVALID, "the slots' triangle-list pools alone exceed the HBM budget");
+    s->memUsed = s->poolBytes;
+    s->memPeak = s->memUsed;
+    hvvr_server* raw = s.release();
+    raw->worker = std::thread(workerLoop, raw);
+    *out = raw;
+    return HVVR_OK;
+}
+
+int hvvr_server_destroy(hvvr_server* s) {
+    if (!s) return fail(HVVR_ERR_INVALID, "NULL server");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+        s->workCv.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->scenes[0]->spec.device);
+    cudaDeviceSynchronize();
+    for (Slot& sl : s->slots) {
+        if (sl.batch) releaseBatch(sl.batch.get());
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+        if (sl.done) cudaEventDestroy(sl.done);
+    }
+    // instance and prototype cameras go back to their raycasters and are destroyed there
+    for (auto& in : s->instances) {
+        if (in->staging) cudaFreeHost(in->staging);
+        hvvr_camera_destroy(in->cam->rc, in->cam);
+    }
+    for (Template& t : s->templates) hvvr_camera_destroy(t.rc, t.proto);
+    if (s->updateStream) cudaStreamDestroy(s->updateStream);
+    if (s->updateEv) cudaEventDestroy(s->updateEv);
+    delete s;
+    return HVVR_OK;
+}
+
+int hvvr_server_add_view(hvvr_server* s, uint32_t scene, const hvvr_float_rect* viewport, const hvvr_sample* samples,
+                         uint32_t count, uint32_t split, uint32_t width, uint32_t height, uint32_t* view_id) {
+    if (!s || !viewport || !samples || !view_id) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (scene >= s->scenes.size()) return fail(HVVR_ERR_INVALID, "scene %u out of range", scene);
+    if (!width || !height) return fail(HVVR_ERR_INVALID, "empty output image");
+    hvvr_raycaster* rc = s->scenes[scene];
+    hvvr_camera* cam = nullptr;
+    // the worker thread may be cloning cameras of this raycaster: serialise with it
+    std::lock_guard<std::mutex> lock(s->mu);
+    TRY(hvvr_camera_create(rc, viewport, 0.0f, &cam));
+    cam->hidden = true;
+    hvvr_image_desc d{};
+    d.pixel_format = HVVR_PIXEL_RGBA8_SRGB;
+    d.memory_type = HVVR_MEMORY_CUDA;
+    d.width = width;
+    d.height = height;
+    cam->target = d;
+    int r = hvvr_camera_set_samples(cam, samples, count, split);
+    if (r == HVVR_OK) r = setupCamera(cam, rc->stream);
+    if (r == HVVR_OK && cudaStreamSynchronize(rc->stream) != cudaSuccess) r = fail(HVVR_ERR_CUDA, "setup failed");
+    if (r != HVVR_OK) {
+        hvvr_camera_destroy(rc, cam);
+        return r;
+    }
+    Template t;
+    t.rc = rc;
+    t.proto = cam;
+    t.width = width;
+    t.height = height;
+    t.samples = count;
+    t.instBytes = cameraBytes(cam, 1) + size_t(width) * height * 4;
+    s->templates.push_back(t);
+    *view_id = uint32_t(s->templates.size() - 1);
+    return HVVR_OK;
+}
+
+int hvvr_server_submit(hvvr_server* s, const hvvr_request* req, uint64_t* id) {
+    if (!s || !req) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (req->memory_type != HVVR_MEMORY_CPU && req->memory_type != HVVR_MEMORY_CUDA)
+        return fail(HVVR_ERR_INVALID, "output must be CPU or CUDA memory");
+    if (!req->output) return fail(HVVR_ERR_INVALID, "NULL output");
+    if (req->msaa != 1 && req->msaa != 2 && req->msaa != 4 && req->msaa != 8 && req->msaa != 16 && req->msaa != 32)
+        return fail(HVVR_ERR_INVALID, "MSAA rate must be 1, 2, 4, 8, 16 or 32");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (req->view >= s->templates.size()) return fail(HVVR_ERR_INVALID, "unknown view %u", req->view);
+    if (s->templates[req->view].instBytes + s->poolBytes > s->cfg.hbm_budget_bytes)
+        return fail(HVVR_ERR_OOM, "one view of this template exceeds the HBM budget");
+    auto r = std::make_unique<Request>();
+    r->id = s->nextId++;
+    r->r = *req;
+    r->submitMs = s->nowMs();
+    if (id) *id = r->id;
+    s->pending.push_back(r.get());
+    s->live[r->id] = std::move(r);
+    s->stats.submitted++;
+    s->stats.in_flight++;
+    s->stats.queued = s->pending.size();
+    s->workCv.notify_all();
+    return HVVR_OK;
+}
+
+int hvvr_server_poll(hvvr_server* s, hvvr_completion* out, uint32_t capacity, uint32_t* count, double wait_ms) {
+    if (!s || !count || (capacity && !out)) return fail(HVVR_ERR_INVALID, "NULL argument");
+    std::unique_lock<std::mutex> lock(s->mu);
+    if (s->completions.empty() && wait_ms > 0)
+        s->doneCv.wait_for(lock, std::chrono::duration<double, std::milli>(wait_ms),
+                           [&] { return !s->completions.empty(); });
+    uint32_t n = 0;
+    while (n < capacity && !s->completions.empty()) {
+        out[n++] = s->completions.front();
+        s->completions.pop_front();
+    }
+    *count = n;
+    if (!s->workerError.empty()) return fail(HVVR_ERR_CUDA, "server worker: %s", s->workerError.c_str());
+    return HVVR_OK;
+}
+
+int hvvr_server_update_vertices(hvvr_server* s, hvvr_model* model, uint32_t first, uint32_t count,
+                                const void* device_verts) {
+    if (!s || !model || (count && !device_verts)) return fail(HVVR_ERR_INVALID, "NULL argument");
+    hvvr_raycaster* rc = model->rc;
+    if (std::find(s->scenes.begin(), s->scenes.end(), rc) == s->scenes.end())
+        return fail(HVVR_ERR_INVALID, "model is not in a served scene");
+    if (uint64_t(first) + count > model->verts.size()) return fail(HVVR_ERR_INVALID, "vertex range out of bounds");
+    auto u = std::make_unique<Update>();
+    u->rc = rc;
+    size_t off = 0;
+    for (auto& m : rc->models) {
+        if (m.get() == model) break;
+        off += m->verts.size();
+    }
+    u->vertOffset = off + first;
+    u->count = count;
+    TRY(u->verts.alloc(size_t(count) * 2));
+    CUDA_TRY(cudaMemcpy(u->verts.p, device_verts, size_t(count) * 32, cudaMemcpyDeviceToDevice));
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->updates.push_back(std::move(u));
+    s->workCv.notify_all();
+    return HVVR_OK;
+}
+
+int hvvr_server_get_stats(hvvr_server* s, hvvr_server_stats* out) {
+    if (!s || !out) return fail(HVVR_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    *out = s->stats;
+    out->instances = s->instances.size();
+    out->hbm_used = s->memUsed;
+    out->hbm_peak = s->memPeak;
+    out->mean_batch_views = s->stats.batches ? double(s->viewsDispatched) / double(s->stats.batches) : 0.0;
+    return HVVR_OK;
+}
+
+} // extern "C"

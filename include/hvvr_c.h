@@ -306,6 +306,65 @@ int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
  * again with the 4096-entry stack, [2] device status bits, [3] views */
 int hvvr_batch_read_stats(const hvvr_batch* batch, uint64_t* out4);
 
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference. A server owns one worker thread that renders requests as
+ * they arrive over resident scenes (raycasters whose scene is uploaded and refit once, then
+ * animated in place). Each request names a view template (sample set + viewport over one
+ * scene, clustered once by hvvr_server_add_view), an MSAA rate, a pose and an output image.
+ * Admission: a request runs on a camera instance of its template; instances are reused, and a
+ * new one is made only while the device memory of all instances plus the slots' triangle-list
+ * pools stays within hbm_budget_bytes (idle instances of other templates are freed to make
+ * room) - otherwise the request waits. Continuous batching: up to
+ * max_batch_views admitted requests form one frame batch on a free slot; `slots` batches are
+ * in flight at once on their own streams, so requests that arrive while a batch runs are
+ * batched into the next one and overlap with it on the device. A request's image is the same
+ * alone and in any mix. While a server exists its raycasters must not be rendered, edited or
+ * destroyed by other calls; destroy the server first. */
+typedef struct hvvr_server hvvr_server;
+typedef struct {
+    uint64_t hbm_budget_bytes;    /* view buffers + list pools + framebuffers; default 120 GiB */
+    uint32_t slots;               /* batches in flight (1..8, default 2) */
+    uint32_t max_batch_views;     /* views per batch (default 64) */
+    uint64_t slot_list_capacity;  /* triangle-list pool entries per slot (default 256M) */
+    uint32_t tile_cull_warps;     /* as hvvr_batch_config (default 4) */
+    uint32_t heavy_divisor;       /* as hvvr_batch_config (default 8) */
+} hvvr_server_config;
+typedef struct {
+    uint32_t view;                /* from hvvr_server_add_view */
+    uint32_t msaa;                /* 1,2,4,8,16,32 */
+    hvvr_transform camera_to_world;
+    uint32_t memory_type;         /* HVVR_MEMORY_CPU or HVVR_MEMORY_CUDA */
+    void* output;                 /* width x height RGBA8 (sRGB) pixels, row stride = width */
+    uint64_t tag;                 /* returned with the completion */
+} hvvr_request;
+typedef struct {
+    uint64_t id, tag;
+    int status;                   /* HVVR_OK, or the error of the batch that rendered it */
+    uint32_t batch_views;         /* views in that batch */
+    double submit_ms, dispatch_ms, done_ms; /* server clock (ms since creation); done = output ready */
+} hvvr_completion;
+typedef struct {
+    uint64_t submitted, completed, failed, batches, queued, in_flight;
+    uint64_t instances, hbm_used, hbm_peak;
+    double mean_batch_views;
+    uint64_t evicted;             /* idle instances freed to admit other templates */
+} hvvr_server_stats;
+void hvvr_server_config_default(hvvr_server_config* cfg);
+int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr_server_config* cfg,
+                       hvvr_server** out);
+int hvvr_server_destroy(hvvr_server* server);
+int hvvr_server_add_view(hvvr_server* server, uint32_t scene, const hvvr_float_rect* viewport,
+                         const hvvr_sample* samples, uint32_t count, uint32_t split_color_samples, uint32_t width,
+                         uint32_t height, uint32_t* view_id);
+int hvvr_server_submit(hvvr_server* server, const hvvr_request* request, uint64_t* id);
+/* moves up to capacity completions out; waits up to wait_ms for the first one */
+int hvvr_server_poll(hvvr_server* server, hvvr_completion* out, uint32_t capacity, uint32_t* count, double wait_ms);
+/* copies count device vertices (32 B each) now; they replace the model's vertices [first, first+count)
+ * between batches, followed by a device refit of the scene */
+int hvvr_server_update_vertices(hvvr_server* server, hvvr_model* model, uint32_t first, uint32_t count,
+                                const void* device_verts);
+int hvvr_server_get_stats(hvvr_server* server, hvvr_server_stats* out);
+
 /* ---------------------------------------------------------------- cull without device allocation
  * No counterpart in the reference. For callers that may not call cudaMalloc: a render thread
  * with a frame deadline (an allocation can synchronise the device), a plugin whose host
