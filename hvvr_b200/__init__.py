@@ -100,6 +100,7 @@ _sig("hvvr_server_create", _p(_vp), _u32, _p(_abi.ServerConfig), _p(_vp))
 _sig("hvvr_server_destroy", _vp)
 _sig("hvvr_server_add_view", _vp, _u32, _p(_abi.FloatRect), _vp, _u32, _u32, _u32, _u32, _p(_u32))
 _sig("hvvr_server_submit", _vp, _p(_abi.Request), _p(C.c_uint64))
+_sig("hvvr_server_prewarm", _vp, _u32, _u32)
 _sig("hvvr_server_poll", _vp, _p(_abi.Completion), _u32, _p(_u32), C.c_double)
 _sig("hvvr_server_update_vertices", _vp, _vp, _u32, _u32, _vp)
 _sig("hvvr_server_get_stats", _vp, _p(_abi.ServerStats))
@@ -125,7 +126,7 @@ EXPORTED = [
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
-    "hvvr_server_submit", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
+    "hvvr_server_submit", "hvvr_server_prewarm", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
 ]
 
 
@@ -536,6 +537,9 @@ class Server:
                                          len(samples), split, width, height, C.byref(vid)))
         self.views.append((width, height, len(samples)))
         return vid.value
+
+    def prewarm(self, view, count):
+        _check(_lib.hvvr_server_prewarm(self.handle, view, count))
 
     def submit(self, view, msaa, camera_to_world, output=None, device_ptr=None, tag=0):
         """output: a (height, width) uint32 numpy array (CPU), or device_ptr for CUDA memory"""

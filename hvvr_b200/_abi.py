@@ -104,7 +104,8 @@ class BatchConfig(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch_views", C.c_uint32),
-                ("slot_list_capacity", C.c_uint64), ("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32)]
+                ("slot_list_capacity", C.c_uint64), ("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32),
+                ("min_batch_views", C.c_uint32), ("max_wait_ms", C.c_float)]
 
 
 class Request(C.Structure):
@@ -121,7 +122,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("batches", C.c_uint64), ("queued", C.c_uint64), ("in_flight", C.c_uint64),
                 ("instances", C.c_uint64), ("hbm_used", C.c_uint64), ("hbm_peak", C.c_uint64),
-                ("mean_batch_views", C.c_double), ("evicted", C.c_uint64)]
+                ("mean_batch_views", C.c_double), ("evicted", C.c_uint64), ("batch_gpu_ms", C.c_double),
+                ("dispatch_host_ms", C.c_double)]
 
 
 # numpy layouts of the bulk arrays

@@ -201,6 +201,8 @@ int checkStatus(const hvvr_batch* b);
 uint32_t rateIndex(uint32_t rate);
 // scene update and refit of the batch's raycasters (unless skipScenes), then one frame of its views on st
 int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes = false);
+// grows the batch's frame buffers to hold a frame of this many tiles, blocks and views
+int reserveBatch(hvvr_batch* b, size_t tiles, size_t blocks, size_t views);
 // uploads the MSAA offset table of `rate` to the current device once
 int ensureMsaaTable(uint32_t rate, cudaStream_t st);
 // a new camera of the same raycaster with cam's sample set and setup (device copies, no

@@ -532,6 +532,25 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
     return HVVR_OK;
 }
 
+int reserveBatch(hvvr_batch* b, size_t tiles, size_t blocks, size_t views) {
+    TRY(b->blockView.ensure(blocks));
+    TRY(b->order.ensure(tiles));
+    TRY(b->retry.ensure(tiles));
+    TRY(b->viewsDev.ensure(views));
+    if (b->hostViewsCap < views) {
+        for (int k = 0; k < 2; k++) {
+            if (b->hostViewsUsed[k]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[k]));
+            if (b->hostViews[k]) cudaFreeHost(b->hostViews[k]);
+            b->hostViews[k] = nullptr;
+            b->hostViewsUsed[k] = false;
+        }
+        b->hostViewsCap = 0;
+        for (int k = 0; k < 2; k++) CUDA_TRY(cudaMallocHost((void**)&b->hostViews[k], views * sizeof(ViewDev)));
+        b->hostViewsCap = views;
+    }
+    return HVVR_OK;
+}
+
 // Scene update and refit of every raycaster, then one frame of all their enabled cameras.
 int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     if (b->detached) return fail(HVVR_ERR_STATE, "a raycaster of this batch was destroyed");
@@ -616,23 +635,8 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
             b->rateStart[r] = run;
             run += rateTiles[r];
         }
-        TRY(b->blockView.ensure(blockView.size()));
+        TRY(reserveBatch(b, b->tiles, b->blocks, b->views.size()));
         CUDA_TRY(cudaMemcpyAsync(b->blockView.p, blockView.data(), blockView.size() * 4, cudaMemcpyHostToDevice, st));
-        TRY(b->order.ensure(b->tiles));
-        TRY(b->retry.ensure(b->tiles));
-        TRY(b->viewsDev.ensure(b->views.size()));
-        if (b->hostViewsCap < b->views.size()) {
-            for (int k = 0; k < 2; k++) {
-                if (b->hostViewsUsed[k]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[k]));
-                if (b->hostViews[k]) cudaFreeHost(b->hostViews[k]);
-                b->hostViews[k] = nullptr;
-                b->hostViewsUsed[k] = false;
-            }
-            b->hostViewsCap = 0;
-            for (int k = 0; k < 2; k++)
-                CUDA_TRY(cudaMallocHost((void**)&b->hostViews[k], b->views.size() * sizeof(ViewDev)));
-            b->hostViewsCap = b->views.size();
-        }
         b->layoutKey = key;
         // scheduling by last frame's cost needs a previous frame of every camera in the layout
         b->costValid = std::all_of(cams.begin(), cams.end(), [](const hvvr_camera* c) { return c->costFrames > 0; });

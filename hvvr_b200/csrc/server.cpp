@@ -12,7 +12,9 @@
 //   * batching - up to max_batch_views admitted requests form one frame batch (one launch per
 //     stage over all views, traversal as one longest-first work queue) on a free slot. Up to
 //     `slots` batches are in flight on their own streams, so requests that arrive while a batch
-//     runs are rendered by the next one, overlapping on the device.
+//     runs are rendered by the next one, overlapping on the device. An idle GPU takes any
+//     request at once; with a batch in flight the next one waits for min_batch_views requests
+//     or for its oldest request to have waited max_wait_ms.
 //     When the budget is short, idle instances of other templates are freed first.
 //   * completion - a slot whose end event has fired returns its instances to the pools and its
 //     requests to the completion queue (CPU outputs are copied out of pinned staging first).
@@ -50,8 +52,8 @@ struct Template {
 struct Instance {
     hvvr_camera* cam = nullptr;
     uint32_t tmpl = 0;
-    DevBuf<uint32_t> image;         // device image the remap writes (CPU outputs and as scratch)
-    uint32_t* staging = nullptr;    // pinned copy of image for CPU outputs
+    DevBuf<uint32_t> image;         // device image the remap writes for CPU outputs
+    uint32_t* staging = nullptr;    // pinned copy of image for CPU outputs (made on first use)
     size_t bytes = 0;
 };
 
@@ -90,6 +92,7 @@ struct hvvr_server {
     cudaStream_t updateStream = nullptr;
     cudaEvent_t updateEv = nullptr;
     size_t poolBytes = 0, memUsed = 0, memPeak = 0;
+    size_t reservedFor = 0;             // template count the slots' frame buffers are sized for
 
     std::mutex mu;                       // guards everything below
     std::condition_variable workCv, doneCv;
@@ -113,47 +116,44 @@ struct hvvr_server {
 
 namespace {
 
-// returns instance for template t or nullptr when the budget does not allow a new one
-Instance* takeInstance(hvvr_server* s, uint32_t t) {
+// frees idle instances of templates other than t, largest first, until `need` more bytes fit
+bool evictFor(hvvr_server* s, uint32_t t, size_t need) {
+    if (s->memUsed + need <= s->cfg.hbm_budget_bytes) return true;
+    std::vector<Instance*> idle;
+    for (uint32_t k = 0; k < s->templates.size(); k++)
+        if (k != t)
+            for (Instance* i : s->templates[k].freeList) idle.push_back(i);
+    std::sort(idle.begin(), idle.end(), [](const Instance* a, const Instance* b) { return a->bytes > b->bytes; });
+    size_t freeable = 0;
+    for (Instance* i : idle) freeable += i->bytes;
+    if (s->memUsed - freeable + need > s->cfg.hbm_budget_bytes) return false;
+    for (Instance* i : idle) {
+        if (s->memUsed + need <= s->cfg.hbm_budget_bytes) break;
+        auto& fl = s->templates[i->tmpl].freeList;
+        fl.erase(std::remove(fl.begin(), fl.end(), i), fl.end());
+        if (i->staging) cudaFreeHost(i->staging);
+        hvvr_camera_destroy(i->cam->rc, i->cam);
+        s->memUsed -= i->bytes;
+        s->stats.evicted++;
+        s->instances.erase(std::remove_if(s->instances.begin(), s->instances.end(),
+                                          [&](const std::unique_ptr<Instance>& p) { return p.get() == i; }),
+                           s->instances.end());
+    }
+    return true;
+}
+
+// a new instance of template t (device copies of the template's setup), or nullptr when the
+// budget does not allow one even after evicting idle instances of other templates
+Instance* makeInstance(hvvr_server* s, uint32_t t) {
     Template& tp = s->templates[t];
-    if (!tp.freeList.empty()) {
-        Instance* i = tp.freeList.back();
-        tp.freeList.pop_back();
-        return i;
-    }
-    if (s->memUsed + tp.instBytes > s->cfg.hbm_budget_bytes) {
-        // evict idle instances of other templates, largest first, until this one fits
-        std::vector<Instance*> idle;
-        for (uint32_t k = 0; k < s->templates.size(); k++)
-            if (k != t)
-                for (Instance* i : s->templates[k].freeList) idle.push_back(i);
-        std::sort(idle.begin(), idle.end(), [](const Instance* a, const Instance* b) { return a->bytes > b->bytes; });
-        size_t freeable = 0;
-        for (Instance* i : idle) freeable += i->bytes;
-        if (s->memUsed - freeable + tp.instBytes > s->cfg.hbm_budget_bytes) return nullptr;
-        for (Instance* i : idle) {
-            if (s->memUsed + tp.instBytes <= s->cfg.hbm_budget_bytes) break;
-            auto& fl = s->templates[i->tmpl].freeList;
-            fl.erase(std::remove(fl.begin(), fl.end(), i), fl.end());
-            if (i->staging) cudaFreeHost(i->staging);
-            hvvr_camera_destroy(i->cam->rc, i->cam);
-            s->memUsed -= i->bytes;
-            s->stats.evicted++;
-            s->instances.erase(std::remove_if(s->instances.begin(), s->instances.end(),
-                                              [&](const std::unique_ptr<Instance>& p) { return p.get() == i; }),
-                               s->instances.end());
-        }
-    }
+    if (!evictFor(s, t, tp.instBytes)) return nullptr;
     auto inst = std::make_unique<Instance>();
     hvvr_camera* cam = nullptr;
     if (cloneCamera(tp.proto, &cam) != HVVR_OK) return nullptr;
     cam->hidden = true;
     inst->cam = cam;
     inst->tmpl = t;
-    if (inst->image.alloc(size_t(tp.width) * tp.height) != HVVR_OK ||
-        cudaMallocHost((void**)&inst->staging, size_t(tp.width) * tp.height * 4) != cudaSuccess) {
-        cudaGetLastError();
-        inst->staging = nullptr;
+    if (inst->image.alloc(size_t(tp.width) * tp.height) != HVVR_OK) {
         hvvr_camera_destroy(cam->rc, cam);
         return nullptr;
     }
@@ -163,6 +163,17 @@ Instance* takeInstance(hvvr_server* s, uint32_t t) {
     Instance* raw = inst.get();
     s->instances.push_back(std::move(inst));
     return raw;
+}
+
+// an idle instance of template t, else a new one; nullptr when the budget is exhausted
+Instance* takeInstance(hvvr_server* s, uint32_t t) {
+    Template& tp = s->templates[t];
+    if (!tp.freeList.empty()) {
+        Instance* i = tp.freeList.back();
+        tp.freeList.pop_back();
+        return i;
+    }
+    return makeInstance(s, t);
 }
 
 void complete(hvvr_server* s, Request* r, int status) {
@@ -187,6 +198,11 @@ void complete(hvvr_server* s, Request* r, int status) {
 
 void finishSlot(hvvr_server* s, Slot& sl) {
     const int st = checkStatus(sl.batch.get());
+    float gpuMs = 0.0f;
+    if (cudaEventElapsedTime(&gpuMs, sl.batch->ev[0], sl.batch->ev[5]) == cudaSuccess) {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stats.batch_gpu_ms += gpuMs;
+    }
     for (Request* r : sl.reqs) {
         Instance* in = r->inst;
         const Template& tp = s->templates[in->tmpl];
@@ -236,13 +252,34 @@ bool dispatch(hvvr_server* s, Slot& sl) {
         s->stats.queued = s->pending.size();
     }
     if (take.empty()) return false;
+    const double hostStart = s->nowMs();
     hvvr_batch* b = sl.batch.get();
+    // frame buffers sized once for the largest batch the templates allow, so that no batch
+    // reallocates (a free synchronises the device behind the other slots)
+    if (s->reservedFor != s->templates.size()) {
+        size_t maxTiles = 0;
+        for (const Template& t : s->templates) maxTiles = std::max<size_t>(maxTiles, t.proto->dev.tiles);
+        const size_t tiles = maxTiles * s->cfg.max_batch_views;
+        for (Slot& o : s->slots)
+            if (!o.busy || &o == &sl) {
+                if (reserveBatch(o.batch.get(), tiles, tiles / kTilesPerBlock, s->cfg.max_batch_views) != HVVR_OK)
+                    break;
+            }
+        bool all = true;
+        for (Slot& o : s->slots) all = all && o.batch->order.n >= tiles;
+        if (all) s->reservedFor = s->templates.size();
+    }
     b->cams.clear();
     const double now = s->nowMs();
     for (Request* r : take) {
         Instance* in = r->inst;
         hvvr_camera* c = in->cam;
         const Template& tp = s->templates[in->tmpl];
+        if (r->r.memory_type == HVVR_MEMORY_CPU && !in->staging &&
+            cudaMallocHost((void**)&in->staging, size_t(tp.width) * tp.height * 4) != cudaSuccess) {
+            cudaGetLastError();
+            in->staging = nullptr;
+        }
         c->xf = r->r.camera_to_world;
         c->msaa = r->r.msaa;
         uint32_t* img = r->r.memory_type == HVVR_MEMORY_CUDA ? static_cast<uint32_t*>(r->r.output) : in->image.p;
@@ -262,6 +299,10 @@ bool dispatch(hvvr_server* s, Slot& sl) {
         for (Request* r : take) {
             if (r->r.memory_type != HVVR_MEMORY_CPU) continue;
             const Template& tp = s->templates[r->inst->tmpl];
+            if (!r->inst->staging) {
+                rc = fail(HVVR_ERR_OOM, "pinned staging allocation failed");
+                break;
+            }
             if (cudaMemcpyAsync(r->inst->staging, r->inst->image.p, size_t(tp.width) * tp.height * 4,
                                 cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess)
                 rc = fail(HVVR_ERR_CUDA, "output copy failed");
@@ -279,6 +320,7 @@ bool dispatch(hvvr_server* s, Slot& sl) {
     sl.reqs = take;
     sl.busy = true;
     std::lock_guard<std::mutex> lock(s->mu);
+    s->stats.dispatch_host_ms += s->nowMs() - hostStart;
     s->stats.batches++;
     s->viewsDispatched += take.size();
     return true;
@@ -315,6 +357,16 @@ void workerLoop(hvvr_server* s) {
         } else {
             for (Slot& sl : s->slots) {
                 if (sl.busy) continue;
+                // an idle GPU takes any request; with a batch in flight, gather a fuller batch
+                // unless the oldest request has waited max_wait_ms
+                bool busyNow = false;
+                for (const Slot& o : s->slots) busyNow = busyNow || o.busy;
+                if (busyNow) {
+                    std::lock_guard<std::mutex> lock(s->mu);
+                    if (s->pending.empty()) break;
+                    const double waited = s->nowMs() - s->pending.front()->submitMs;
+                    if (s->pending.size() < s->cfg.min_batch_views && waited < s->cfg.max_wait_ms) break;
+                }
                 if (dispatch(s, sl)) progress = true;
                 else break;
             }
@@ -344,6 +396,8 @@ void hvvr_server_config_default(hvvr_server_config* cfg) {
     cfg->slot_list_capacity = 256ull << 20;
     cfg->tile_cull_warps = 4;
     cfg->heavy_divisor = 8;
+    cfg->min_batch_views = 8;
+    cfg->max_wait_ms = 2.0f;
 }
 
 int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr_server_config* cfg,
@@ -468,6 +522,21 @@ int hvvr_server_add_view(hvvr_server* s, uint32_t scene, const hvvr_float_rect* 
     t.instBytes = cameraBytes(cam, 1) + size_t(width) * height * 4;
     s->templates.push_back(t);
     *view_id = uint32_t(s->templates.size() - 1);
+    return HVVR_OK;
+}
+
+int hvvr_server_prewarm(hvvr_server* s, uint32_t view, uint32_t count) {
+    if (!s) return fail(HVVR_ERR_INVALID, "NULL server");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (view >= s->templates.size()) return fail(HVVR_ERR_INVALID, "unknown view %u", view);
+    Template& tp = s->templates[view];
+    while (tp.freeList.size() < count) {
+        if (s->memUsed + tp.instBytes > s->cfg.hbm_budget_bytes)
+            return fail(HVVR_ERR_OOM, "HBM budget reached after %zu instances", tp.freeList.size());
+        Instance* in = makeInstance(s, view);
+        if (!in) return fail(HVVR_ERR_OOM, "could not make an instance");
+        tp.freeList.push_back(in);
+    }
     return HVVR_OK;
 }
 

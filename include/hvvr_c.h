@@ -328,6 +328,9 @@ typedef struct {
     uint64_t slot_list_capacity;  /* triangle-list pool entries per slot (default 256M) */
     uint32_t tile_cull_warps;     /* as hvvr_batch_config (default 4) */
     uint32_t heavy_divisor;       /* as hvvr_batch_config (default 8) */
+    uint32_t min_batch_views;     /* with a batch in flight, wait for this many requests (default 8) ... */
+    float max_wait_ms;            /* ... or until the oldest has waited this long (default 2 ms);
+                                     an idle GPU takes any request at once */
 } hvvr_server_config;
 typedef struct {
     uint32_t view;                /* from hvvr_server_add_view */
@@ -348,6 +351,8 @@ typedef struct {
     uint64_t instances, hbm_used, hbm_peak;
     double mean_batch_views;
     uint64_t evicted;             /* idle instances freed to admit other templates */
+    double batch_gpu_ms;          /* sum over batches of their device time (first launch to last copy) */
+    double dispatch_host_ms;      /* sum over batches of the worker's host time to form and enqueue them */
 } hvvr_server_stats;
 void hvvr_server_config_default(hvvr_server_config* cfg);
 int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr_server_config* cfg,
@@ -356,6 +361,9 @@ int hvvr_server_destroy(hvvr_server* server);
 int hvvr_server_add_view(hvvr_server* server, uint32_t scene, const hvvr_float_rect* viewport,
                          const hvvr_sample* samples, uint32_t count, uint32_t split_color_samples, uint32_t width,
                          uint32_t height, uint32_t* view_id);
+/* makes idle camera instances of a view up to `count` ahead of the traffic (allocation stalls
+ * the device, so a warm server admits without allocating) */
+int hvvr_server_prewarm(hvvr_server* server, uint32_t view, uint32_t count);
 int hvvr_server_submit(hvvr_server* server, const hvvr_request* request, uint64_t* id);
 /* moves up to capacity completions out; waits up to wait_ms for the first one */
 int hvvr_server_poll(hvvr_server* server, hvvr_completion* out, uint32_t capacity, uint32_t* count, double wait_ms);
