@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <random>
 #include <thread>
 #include <vector>
 
@@ -765,6 +766,101 @@ inline V3 calcUVW(const TriThread& th, V2 a, bool fma) {
     return mk(u * inv, v * inv, w * inv);
 }
 
+// ------------------------------------------------------------------ depth of field
+// IntersectTriangleTile<true>, IntersectTriangleThreadDoF (RC/prim_tests.h:247-392), TileData<true>
+// (RC/tile_data.h:33-60), GetSampleUVsDoF (RC/gpu_samples.h:84-103), initLookupTables
+// (RC/gpu_camera.cu:59-88). fma selects the contraction the kernel comments mark (HVVR_FP_FMA).
+inline V3 fma3(float s, V3 a, V3 c) { return mk(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y), fmaf(s, a.z, c.z)); }
+
+struct DofTile { V3 lensU, lensV; V2 focalToLensScale; };
+// TileData<true>::load. The kernels call it with the world-space beam of GetDirectionalSample3D and
+// rotate it again (cameraToWorldRotation * sample.du); kept. rsqrtf is taken as 1/sqrtf.
+DofTile dofTileData(const M3& R, const Beam& bmCam, const hvvr_thin_lens& lens) {
+    V3 focalU = mul(R, mul(R, bmCam.du)), focalV = mul(R, mul(R, bmCam.dv));
+    float uInv = 1.0f / sqrtf(dot(focalU, focalU)), vInv = 1.0f / sqrtf(dot(focalV, focalV));
+    float uMag = 1.0f / uInv, vMag = 1.0f / vInv;
+    DofTile d;
+    d.lensU = focalU * (lens.radius * uInv);
+    d.lensV = focalV * (lens.radius * vInv);
+    float sc = lens.focal_distance / lens.radius;
+    d.focalToLensScale = V2{sc * uMag, sc * vMag};
+    return d;
+}
+
+struct DofTri { V3 e0, e1, v0l; float tC, tU, tV; V2 dd; };
+enum { kAllOut = 0, kPartial = 1, kAllIn = 2 };
+// IntersectTriangleTile<true>::setup
+int dofSetup(const Tri& tri, V3 lensCenter, V3 lensU, V3 lensV, DofTri& d) {
+    d.e0 = tri.e0; d.e1 = tri.e1;
+    V3 normal = cross(d.e0, d.e1);
+    d.v0l = lensCenter - tri.v0;
+    d.tC = dot(d.v0l, normal);
+    d.tU = dot(lensU, normal);
+    d.tV = dot(lensV, normal);
+    float tExtent = fabsf(d.tU) + fabsf(d.tV);
+    float tMax = d.tC + tExtent;
+    if (tMax < 0.0f) return kAllOut;
+    d.dd = V2{dot(-lensU, normal), dot(-lensV, normal)};
+    float tMin = d.tC - tExtent;
+    if (tMin < 0.0f) return kPartial;
+    return kAllIn;
+}
+// IntersectTriangleThreadDoF ctor
+inline float dofDenomCenter(const DofTri& d, V3 lc2fc) { return dot(-lc2fc, cross(d.e0, d.e1)); }
+
+// GetSampleUVsDoF: lens position from the table, direction offset from the MSAA pattern
+inline void dofSampleUVs(const V2* table, uint32_t n, uint32_t lensTile, uint32_t s, uint32_t i, V2 aa, V2 fls,
+                         bool fma, V2& lensUV, V2& dirUV) {
+    lensUV = table[size_t(lensTile) * kTileSize * n + size_t(i) * kTileSize + s];
+    if (fma) dirUV = V2{fmaf(aa.x, fls.x, -lensUV.x), fmaf(aa.y, fls.y, -lensUV.y)};
+    else dirUV = V2{aa.x * fls.x - lensUV.x, aa.y * fls.y - lensUV.y};
+}
+
+// the scaled barycentrics of IntersectTriangleThreadDoF::test / calcUVW
+inline void dofBary(const DofTri& d, float denomCenter, V3 lc2fc, V3 lensU, V3 lensV, V2 lensUV, V2 dirUV,
+                    bool fma, float& denom, float& v, float& w) {
+    V3 o, rd, e;
+    if (fma) {
+        denom = fmaf(d.dd.y, dirUV.y, fmaf(d.dd.x, dirUV.x, denomCenter));
+        o = fma3(lensUV.y, lensV, fma3(lensUV.x, lensU, d.v0l));
+        rd = fma3(dirUV.y, lensV, fma3(dirUV.x, lensU, lc2fc));
+        V3 a = -rd;
+        e = mk(fmaf(a.y, o.z, -(a.z * o.y)), fmaf(a.z, o.x, -(a.x * o.z)), fmaf(a.x, o.y, -(a.y * o.x)));
+        v = fmaf(d.e1.z, e.z, fmaf(d.e1.y, e.y, d.e1.x * e.x));
+        w = -fmaf(d.e0.z, e.z, fmaf(d.e0.y, e.y, d.e0.x * e.x));
+    } else {
+        denom = denomCenter + d.dd.x * dirUV.x + d.dd.y * dirUV.y;
+        o = d.v0l + lensU * lensUV.x + lensV * lensUV.y;
+        rd = lc2fc + lensU * dirUV.x + lensV * dirUV.y;
+        e = cross(-rd, o);
+        v = dot(d.e1, e);
+        w = -dot(d.e0, e);
+    }
+}
+
+// IntersectTriangleThreadDoF::test
+inline bool dofTest(const DofTri& d, float denomCenter, V3 lc2fc, V3 lensU, V3 lensV, V2 lensUV, V2 dirUV,
+                    float& depth, bool fma) {
+    float t = fma ? fmaf(d.tV, lensUV.y, fmaf(d.tU, lensUV.x, d.tC)) : d.tC + d.tU * lensUV.x + d.tV * lensUV.y;
+    float denom, v, w;
+    dofBary(d, denomCenter, lc2fc, lensU, lensV, lensUV, dirUV, fma, denom, v, w);
+    float depthDelta = fma ? fmaf(depth, denom, -t) : depth * denom - t;
+    float u = denom - v - w;
+    int32_t test = int32_t(fbits(t) | fbits(depthDelta) | fbits(u) | fbits(v) | fbits(w));
+    if (test < 0) return false;
+    depth = t * (1.0f / denom);
+    return true;
+}
+
+// IntersectTriangleThreadDoF::calcUVW
+inline V3 dofUVW(const DofTri& d, float denomCenter, V3 lc2fc, V3 lensU, V3 lensV, V2 lensUV, V2 dirUV, bool fma) {
+    float denom, v, w;
+    dofBary(d, denomCenter, lc2fc, lensU, lensV, lensUV, dirUV, fma, denom, v, w);
+    float u = denom - v - w;
+    float inv = 1.0f / denom;
+    return mk(u * inv, v * inv, w * inv);
+}
+
 // ------------------------------------------------------------------ shading (RC/shading.h, RC/shading_helpers.h)
 const int kTau[] = {1,  1,  1,  2,  3,  2,  5,  2,  3,  2,  3,  3,  5,  5,  3,  4,  7,  5,  5,  7,
                     9,  8,  5,  5,  7,  7,  7,  8,  5,  8,  11, 12, 7,  10, 13, 8,  11, 8,  7,  14};
@@ -872,6 +968,29 @@ extern "C" void oracle_msaa_offsets(uint32_t n, float* out) {
     }
 }
 
+// GPUCamera::initLookupTables (RC/gpu_camera.cu:59-88): DOF_LENS_POS_LOOKUP_TABLE_TILES (4) tiles of
+// per-sample random rotations of the spiral, subsample i taking spiral position (7 i + 7) mod n,
+// laid out [tile][subsample][sample]; std::mt19937 default seed, uniform_real_distribution<float>.
+extern "C" void oracle_lens_table(uint32_t n, float* out) {
+    std::uniform_real_distribution<float> dist(0.0f, 1.0f);
+    std::mt19937 gen;
+    const float tauF = 6.283185307180f; // Tau (SH/constants_math.h:16)
+    int turns = kTau[n];
+    for (uint32_t tile = 0; tile < 4; tile++)
+        for (uint32_t s = 0; s < kTileSize; s++) {
+            float rotation = dist(gen) * tauF;
+            for (uint32_t i = 0; i < n; i++) {
+                int k = int((i * 7 + 7) % n);
+                float alpha = float(k + 0.5f) * (1.0f / float(n));
+                float angle = alpha * (float(turns) * 6.28f) + rotation;
+                float radius = sqrtf(alpha);
+                size_t o = (size_t(tile) * kTileSize * n + size_t(i) * kTileSize + s) * 2;
+                out[o + 0] = cosf(angle) * radius;
+                out[o + 1] = sinf(angle) * radius;
+            }
+        }
+}
+
 extern "C" void oracle_layout(uint32_t sample_count, uint32_t* blocks, uint32_t* tiles, uint32_t* padded) {
     uint32_t b = (sample_count + kBlockSize - 1) / kBlockSize;
     if (blocks) *blocks = b;
@@ -962,12 +1081,20 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     }
     V3 camPos = mk(c2w.m3.x, c2w.m3.y, c2w.m3.z);
 
-    // tiles: traversal, then intersect + shade (RC/intersect.cu:171-342, RC/resolve.cu:161-458)
+    // tiles: traversal of every tile first (the reference's lists are complete before its
+    // intersect launch), then intersect + shade (RC/intersect.cu:171-342, RC/resolve.cu:161-458)
     std::vector<std::vector<uint32_t>> lists(ss.tiles);
     std::vector<uint32_t> colors(ss.padded, 0xFF000000u);
     std::atomic<uint32_t> next(0), status(0);
-    auto worker = [&]() {
-        std::vector<uint32_t> scratch;
+    uint32_t nt = in->threads ? in->threads : 1;
+    auto runPool = [&](auto&& fn) {
+        next = 0;
+        std::vector<std::thread> pool;
+        for (uint32_t t = 1; t < nt; t++) pool.emplace_back(fn);
+        fn();
+        for (auto& th : pool) th.join();
+    };
+    runPool([&]() {
         MxcsrScope mxw;
         for (;;) {
             uint32_t tile = next.fetch_add(1);
@@ -978,6 +1105,31 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
             uint32_t st = 0;
             traverseTile(nodes, f, &blockStacks[size_t(b) * kBlockStackSize], blockSizes[b], lists[tile], st);
             if (st) status.fetch_or(st);
+        }
+    });
+
+    // depth of field (lens radius > 0): the lens-position table is indexed by the intersect/resolve
+    // CTA index, which is the tile's rank among the occupied tiles (tileIndexRemapOccupied,
+    // RC/traversal.cpp:213-330); the per-tile lens values come from the tile's middle sample
+    const bool dof = in->lens.radius > 0.0f;
+    std::vector<V2> lensTab;
+    std::vector<uint32_t> occRank(ss.tiles, 0);
+    V3 look = mul(R, mk(0.0f, 0.0f, -1.0f));
+    if (dof) {
+        lensTab.resize(size_t(kTileSize) * 4 * N);
+        oracle_lens_table(N, &lensTab[0].x);
+        uint32_t r = 0;
+        for (uint32_t t = 0; t < ss.tiles; t++) {
+            occRank[t] = r;
+            if (!lists[t].empty()) r++;
+        }
+    }
+
+    runPool([&]() {
+        MxcsrScope mxw;
+        for (;;) {
+            uint32_t tile = next.fetch_add(1);
+            if (tile >= ss.tiles) break;
             const std::vector<uint32_t>& list = lists[tile];
             uint32_t base = tile * kTileSize;
             if (list.empty()) {
@@ -997,32 +1149,63 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                 continue;
             }
             FrustumPlanes fp = makePlanes(tileW[tile]);
+            DofTile dt{};
+            const uint32_t lensTile = occRank[tile] % 4;
+            if (dof) dt = dofTileData(R, ss.beams[base + kTileSize / 2], in->lens);
             // per-chunk culling and compaction preserves list order, so the surviving sequence is
             // the list filtered by the three pre-tests
             std::vector<uint32_t> surv;
             std::vector<TriTile> survTT;
+            std::vector<DofTri> survDT;
             surv.reserve(list.size());
             for (uint32_t idx : list) {
                 const Tri& tri = scene.tris[idx];
                 if (!planesTest(fp, tri)) continue;
-                TriTile tt;
-                if (!tileSetup(tri, camPos, tt)) continue;
-                if (!uvwNotAllOut(tileW[tile], tri)) continue;
-                surv.push_back(idx);
-                survTT.push_back(tt);
+                if (dof) {
+                    DofTri d;
+                    int r = dofSetup(tri, camPos, dt.lensU, dt.lensV, d);
+                    if (r == kAllOut) continue;
+                    // the corner-ray test only when every lens position sees the front of the plane
+                    if (r == kAllIn && !uvwNotAllOut(tileW[tile], tri)) continue;
+                    surv.push_back(idx);
+                    survDT.push_back(d);
+                } else {
+                    TriTile tt;
+                    if (!tileSetup(tri, camPos, tt)) continue;
+                    if (!uvwNotAllOut(tileW[tile], tri)) continue;
+                    surv.push_back(idx);
+                    survTT.push_back(tt);
+                }
             }
             for (uint32_t s = 0; s < kTileSize; s++) {
                 uint32_t sid = base + s;
                 const Beam& bm = ss.beams[sid];
                 V3 c = mul(R, bm.c), du = mul(R, bm.du), dv = mul(R, bm.dv);
+                V3 lc2fc{};
+                if (dof) {
+                    V3 centerDir = normalize(c);
+                    float zed = dot(look, centerDir);
+                    lc2fc = centerDir * (in->lens.focal_distance / zed);
+                }
                 float tmaxv[32];
                 uint32_t hit[32];
                 for (uint32_t i = 0; i < N; i++) { tmaxv[i] = FLT_MAX; hit[i] = ~0u; }
                 for (size_t j = 0; j < surv.size(); j++) {
-                    TriThread th = threadSetup(survTT[j], c, du, dv);
-                    for (uint32_t i = 0; i < N; i++) {
-                        V2 a{off[2 * i], off[2 * i + 1]};
-                        if (threadTest(th, survTT[j].t, a, tmaxv[i], useFma)) hit[i] = surv[j];
+                    if (dof) {
+                        float dc = dofDenomCenter(survDT[j], lc2fc);
+                        for (uint32_t i = 0; i < N; i++) {
+                            V2 lensUV, dirUV;
+                            dofSampleUVs(lensTab.data(), N, lensTile, s, i, V2{off[2 * i], off[2 * i + 1]},
+                                         dt.focalToLensScale, useFma, lensUV, dirUV);
+                            if (dofTest(survDT[j], dc, lc2fc, dt.lensU, dt.lensV, lensUV, dirUV, tmaxv[i], useFma))
+                                hit[i] = surv[j];
+                        }
+                    } else {
+                        TriThread th = threadSetup(survTT[j], c, du, dv);
+                        for (uint32_t i = 0; i < N; i++) {
+                            V2 a{off[2 * i], off[2 * i + 1]};
+                            if (threadTest(th, survTT[j].t, a, tmaxv[i], useFma)) hit[i] = surv[j];
+                        }
                     }
                 }
                 for (uint32_t i = 0; i < N; i++) {
@@ -1030,7 +1213,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                     if (out->hit_ids) out->hit_ids[o] = hit[i];
                     if (out->depth) out->depth[o] = hit[i] == ~0u ? INFINITY : tmaxv[i];
                     if (out->depth64) {
-                        if (hit[i] == ~0u) out->depth64[o] = NAN;
+                        if (hit[i] == ~0u || dof) out->depth64[o] = NAN;
                         else {
                             const Tri& t = scene.tris[hit[i]];
                             double D[3] = {double(c.x) + double(off[2 * i]) * du.x + double(off[2 * i + 1]) * dv.x,
@@ -1072,18 +1255,32 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                     uint32_t sm = gmask[g];
                     combined |= sm;
                     float inv = 1.0f / float(__builtin_popcount(sm));
-                    V2 ca{0.0f, 0.0f};
+                    V2 ca{0.0f, 0.0f}, cl{0.0f, 0.0f}, cd{0.0f, 0.0f};
                     for (uint32_t cm = sm; cm;) {
                         int si = __builtin_ctz(cm);
                         cm &= ~(1u << si);
                         ca.x = ca.x + off[2 * si] * inv;
                         ca.y = ca.y + off[2 * si + 1] * inv;
+                        if (dof) {
+                            V2 lensUV, dirUV;
+                            dofSampleUVs(lensTab.data(), N, lensTile, s, uint32_t(si), V2{off[2 * si], off[2 * si + 1]},
+                                         dt.focalToLensScale, useFma, lensUV, dirUV);
+                            cl.x = cl.x + lensUV.x * inv; cl.y = cl.y + lensUV.y * inv;
+                            cd.x = cd.x + dirUV.x * inv; cd.y = cd.y + dirUV.y * inv;
+                        }
                     }
                     const Tri& tri = scene.tris[triIndex];
-                    TriTile tt;
-                    tileSetup(tri, camPos, tt);
-                    TriThread th = threadSetup(tt, c, du, dv);
-                    V3 bc = calcUVW(th, ca, useFma);
+                    V3 bc;
+                    if (dof) {
+                        DofTri d;
+                        dofSetup(tri, camPos, dt.lensU, dt.lensV, d);
+                        bc = dofUVW(d, dofDenomCenter(d, lc2fc), lc2fc, dt.lensU, dt.lensV, cl, cd, useFma);
+                    } else {
+                        TriTile tt;
+                        tileSetup(tri, camPos, tt);
+                        TriThread th = threadSetup(tt, c, du, dv);
+                        bc = calcUVW(th, ca, useFma);
+                    }
                     const hvvr_tri_shade& ts = scene.triShade[triIndex];
                     const hvvr_shading_vertex& a0 = scene.world[ts.indices[0]];
                     const hvvr_shading_vertex& a1 = scene.world[ts.indices[1]];
@@ -1102,12 +1299,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                 colors[sid] = packColor(mk(aces(lin.x), aces(lin.y), aces(lin.z)));
             }
         }
-    };
-    uint32_t nt = in->threads ? in->threads : 1;
-    std::vector<std::thread> pool;
-    for (uint32_t t = 1; t < nt; t++) pool.emplace_back(worker);
-    worker();
-    for (auto& th : pool) th.join();
+    });
     out->status |= status.load();
 
     uint64_t total = 0;

@@ -70,6 +70,8 @@ void oracle_scene_counts(const oracle_frame_in* in, uint32_t* nodes, uint32_t* t
 int oracle_render(const oracle_frame_in* in, oracle_frame_out* out);
 /* MSAA unit offsets for rate n (n*2 floats), the spiral pattern of the reference */
 void oracle_msaa_offsets(uint32_t n, float* out);
+/* depth-of-field lens positions for rate n: [4 tiles][n subsamples][128 samples] x 2 floats */
+void oracle_lens_table(uint32_t n, float* out);
 
 #ifdef __cplusplus
 }

@@ -56,8 +56,8 @@ static inline void* _aligned_malloc(size_t size, size_t alignment) {
 static inline void _aligned_free(void* p) { free(p); }
 
 // CUDA builtins referenced by host-parsed device code (never executed on these paths)
-extern uint3 threadIdx;
-extern uint3 blockIdx;
+extern thread_local uint3 threadIdx;
+extern thread_local uint3 blockIdx;
 
 // Host definitions of the CUDA device intrinsics that the kernels' math headers call.
 #include <texture_types.h>

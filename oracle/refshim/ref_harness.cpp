@@ -32,14 +32,17 @@
 #include "prim_tests.h"
 #include "shading.h"
 #include "sort.h"
+#include "tile_data.h"
 
 #include "../hvvr_oracle.h"
 
 #include <atomic>
+#include <functional>
+#include <random>
 #include <thread>
 
-uint3 threadIdx;
-uint3 blockIdx;
+thread_local uint3 threadIdx;
+thread_local uint3 blockIdx;
 
 namespace hvvr {
 // Link stubs for GPU-side classes referenced by camera.cpp's Camera methods. The harness
@@ -62,6 +65,28 @@ inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
 inline float bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
 
 template <uint32_t N> vector2 subOffset(int i) { return getSubsampleUnitOffset<N>(vector2(0.0f, 0.0f), i); }
+template <uint32_t N> vector2 lensOffset(int i, float rot) { return getSubsampleUnitOffset<N>(vector2(0.0f, 0.0f), i, rot); }
+vector2 lensOffsetN(uint32_t n, int i, float rot) {
+    switch (n) {
+    case 1: return lensOffset<1>(i, rot);
+    case 2: return lensOffset<2>(i, rot);
+    case 4: return lensOffset<4>(i, rot);
+    case 8: return lensOffset<8>(i, rot);
+    case 16: return lensOffset<16>(i, rot);
+    default: return lensOffset<32>(i, rot);
+    }
+}
+// GetSampleUVsDoF for a run-time rate (it reads blockIdx.x and threadIdx.x like the kernels)
+void sampleUVsDoF(uint32_t n, const vector2* tab, vector2 fls, int i, vector2& lensUV, vector2& dirUV) {
+    switch (n) {
+    case 1: GetSampleUVsDoF<1, TILE_SIZE>(tab, vector2(0.0f, 0.0f), fls, i, lensUV, dirUV); break;
+    case 2: GetSampleUVsDoF<2, TILE_SIZE>(tab, vector2(0.0f, 0.0f), fls, i, lensUV, dirUV); break;
+    case 4: GetSampleUVsDoF<4, TILE_SIZE>(tab, vector2(0.0f, 0.0f), fls, i, lensUV, dirUV); break;
+    case 8: GetSampleUVsDoF<8, TILE_SIZE>(tab, vector2(0.0f, 0.0f), fls, i, lensUV, dirUV); break;
+    case 16: GetSampleUVsDoF<16, TILE_SIZE>(tab, vector2(0.0f, 0.0f), fls, i, lensUV, dirUV); break;
+    default: GetSampleUVsDoF<32, TILE_SIZE>(tab, vector2(0.0f, 0.0f), fls, i, lensUV, dirUV); break;
+    }
+}
 vector2 subsampleOffset(uint32_t n, int i) {
     switch (n) {
     case 1: return subOffset<1>(i);
@@ -253,6 +278,34 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
     uint32_t maskAll = N < 32 ? ((1u << N) - 1) : ~0u;
     std::vector<uint32_t> colors(padded, 0xFF000000u);
 
+    // depth of field: the lens table of GPUCamera::initLookupTables (RC/gpu_camera.cu:59-88) and the
+    // occupied-tile index the intersect/resolve kernels run under (tileIndexRemapOccupied)
+    const bool dof = in->lens.radius > 0.0f;
+    std::vector<vector2> lensTab;
+    std::vector<uint32_t> occRank(tileCount, 0);
+    alignas(CameraBeams) unsigned char cbStorage[sizeof(CameraBeams)];
+    memset(cbStorage, 0, sizeof(cbStorage));
+    CameraBeams& cameraBeams = *reinterpret_cast<CameraBeams*>(cbStorage); // TileData<true>::load reads .lens only
+    cameraBeams.lens = lens;
+    if (dof) {
+        std::uniform_real_distribution<float> uniformRandomDist(0.0f, 1.0f);
+        std::mt19937 generator;
+        auto r = std::bind(uniformRandomDist, std::ref(generator));
+        lensTab.resize(size_t(TILE_SIZE) * DOF_LENS_POS_LOOKUP_TABLE_TILES * N);
+        for (int tile = 0; tile < DOF_LENS_POS_LOOKUP_TABLE_TILES; tile++)
+            for (int sample = 0; sample < int(TILE_SIZE); sample++) {
+                float rotation = r() * Tau;
+                for (int subsample = 0; subsample < int(N); subsample++)
+                    lensTab[tile * TILE_SIZE * N + subsample * TILE_SIZE + sample] =
+                        lensOffsetN(N, (subsample * 7 + 7) % int(N), rotation);
+            }
+        uint32_t rank = 0;
+        for (uint32_t t = 0; t < tileCount; t++) {
+            occRank[t] = rank;
+            if (!lists[t].empty()) rank++;
+        }
+    }
+
     std::atomic<uint32_t> next(0);
     auto worker = [&]() {
         MxcsrScope mxw;
@@ -261,6 +314,7 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             if (tile >= tileCount) break;
             const std::vector<uint32_t>& list = lists[tile];
             uint32_t base = tile * TILE_SIZE;
+            blockIdx.x = occRank[tile];
             if (list.empty()) {
                 for (uint32_t s = 0; s < TILE_SIZE; s++) {
                     for (uint32_t i = 0; i < N; i++) {
@@ -278,9 +332,23 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             FrustumPlanes planes(simple[tile]);
             std::vector<uint32_t> survIdx;
             std::vector<IntersectTriangleTile<false>> survTile;
+            std::vector<IntersectTriangleTile<true>> survTileDoF;
+            // TileData<true>::load by thread BlockSize/2 on its world-space beam (RC/intersect.cu:182-186)
+            TileData<true> tileDoF;
+            if (dof) tileDoF.load(cameraBeams, cameraToWorld,
+                                  matrix3x3(cameraToWorld) * batch.directionalBeams[base + TILE_SIZE / 2]);
             for (uint32_t idx : list) {
                 const PrecomputedTriangleIntersect& tri = tris[idx];
                 if (!planes.test(tri)) continue;
+                if (dof) {
+                    IntersectTriangleTile<true> tt;
+                    IntersectResult r0 = tt.setup(tri, cameraPos, tileDoF.lensU, tileDoF.lensV);
+                    if (r0 == intersect_all_out) continue;
+                    if (r0 != intersect_partial && TestTriangleFrustaUVW(simple[tile], tri) == intersect_all_out) continue;
+                    survIdx.push_back(idx);
+                    survTileDoF.push_back(tt);
+                    continue;
+                }
                 IntersectTriangleTile<false> tt;
                 if (tt.setup(tri, cameraPos) == intersect_all_out) continue;
                 if (TestTriangleFrustaUVW(simple[tile], tri) == intersect_all_out) continue;
@@ -290,10 +358,26 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             for (uint32_t s = 0; s < TILE_SIZE; s++) {
                 uint32_t sid = base + s;
                 DirectionalBeam sample = matrix3x3(cameraToWorld) * batch.directionalBeams[sid];
+                threadIdx.x = s;
+                // IntersectSamples (RC/intersect.cu:117-168)
+                vector3 centerDir = normalize(sample.centerRay);
+                float zed = dot(matrix3x3(cameraToWorld) * vector3(0, 0, -1.0f), centerDir);
+                vector3 lensCenterToFocalCenter = (lens.focalDistance / zed) * centerDir;
                 float tmaxv[32];
                 uint32_t hit[32];
                 for (uint32_t i = 0; i < N; i++) { tmaxv[i] = FLT_MAX; hit[i] = ~0u; }
                 for (size_t j = 0; j < survIdx.size(); j++) {
+                    if (dof) {
+                        IntersectTriangleThreadDoF th(survTileDoF[j], lensCenterToFocalCenter);
+                        for (uint32_t i = 0; i < N; i++) {
+                            vector2 lensUV, dirUV;
+                            sampleUVsDoF(N, lensTab.data(), tileDoF.focalToLensScale, int(i), lensUV, dirUV);
+                            if (th.test(survTileDoF[j], lensCenterToFocalCenter, tileDoF.lensU, tileDoF.lensV, lensUV,
+                                        dirUV, tmaxv[i]))
+                                hit[i] = survIdx[j];
+                        }
+                        continue;
+                    }
                     IntersectTriangleThread th(survTile[j], sample.centerRay, sample.du, sample.dv);
                     for (uint32_t i = 0; i < N; i++)
                         if (th.test(survTile[j], alphaTab[i], tmaxv[i])) hit[i] = survIdx[j];
@@ -332,16 +416,31 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                     combined |= sampleMask;
                     float sampleCountInv = 1.0f / __builtin_popcount(sampleMask);
                     vector2 centroidAlpha(0.0f, 0.0f);
+                    vector2 centroidLensUV(0.0f, 0.0f), centroidDirUV(0.0f, 0.0f);
                     for (uint32_t cm = sampleMask; cm != 0;) {
                         int si = __builtin_ctz(cm);
                         cm &= ~(1u << si);
                         centroidAlpha += alphaTab[si] * sampleCountInv;
+                        if (dof) {
+                            vector2 lensUV, dirUV;
+                            sampleUVsDoF(N, lensTab.data(), tileDoF.focalToLensScale, si, lensUV, dirUV);
+                            centroidLensUV += lensUV * sampleCountInv;
+                            centroidDirUV += dirUV * sampleCountInv;
+                        }
                     }
-                    IntersectTriangleTile<false> tt;
-                    tt.setup(tris[triIndex], cameraPos);
-                    IntersectTriangleThread th(tt, sample.centerRay, sample.du, sample.dv);
                     vector3 b;
-                    th.calcUVW(tt, centroidAlpha, b);
+                    if (dof) {
+                        IntersectTriangleTile<true> tt;
+                        tt.setup(tris[triIndex], cameraPos, tileDoF.lensU, tileDoF.lensV);
+                        IntersectTriangleThreadDoF th(tt, lensCenterToFocalCenter);
+                        th.calcUVW(tt, lensCenterToFocalCenter, tileDoF.lensU, tileDoF.lensV, centroidLensUV,
+                                   centroidDirUV, b);
+                    } else {
+                        IntersectTriangleTile<false> tt;
+                        tt.setup(tris[triIndex], cameraPos);
+                        IntersectTriangleThread th(tt, sample.centerRay, sample.du, sample.dv);
+                        th.calcUVW(tt, centroidAlpha, b);
+                    }
                     InterpolatedVertex vI = interpolate(world.data(), triShade[triIndex], b);
                     vector4 shaded = GGXShade(triShade[triIndex].material, vI, vector2(0.0f), vector2(0.0f), cameraPos,
                                               materials, nullptr, env);

@@ -23,15 +23,17 @@ from hvvr_b200 import _abi, scenes  # noqa: E402
 import pyoracle  # noqa: E402
 
 CASES = {
-    # name: (grid quads, boxes, seed, sample kind, width, height, msaa, eye, target)
+    # name: (grid quads, boxes, seed, sample kind, width, height, msaa, eye, target[, thin lens (radius, focal distance)])
     "grid_msaa1": (8, 40, 3, "grid", 64, 48, 1, (0.0, 2.0, 10.0), (0.0, 0.0, 0.0)),
     "barrel_msaa4": (10, 60, 4, "barrel", 48, 56, 4, (2.0, 1.5, 7.0), (-1.0, 0.2, 0.0)),
     "grid_msaa8_low": (6, 30, 5, "grid", 40, 40, 8, (0.5, 0.6, 9.0), (0.0, 0.3, 0.0)),
+    "barrel_msaa4_dof": (10, 60, 6, "barrel", 56, 48, 4, (1.0, 1.8, 8.0), (0.0, 0.0, -1.0), (0.08, 7.5)),
 }
 
 
 def make(name, ref):
-    quads, boxes, seed, kind, w, h, msaa, eye, target = CASES[name]
+    quads, boxes, seed, kind, w, h, msaa, eye, target = CASES[name][:9]
+    lens = CASES[name][9] if len(CASES[name]) > 9 else (0.0, 1.0)
     sc = scenes.make_scene(quads, boxes, seed)
     in_verts, in_tris = sc.verts.copy(), sc.tri_shade.copy()
     verts, tris, nodes = ref.generate_topology(sc)
@@ -39,7 +41,8 @@ def make(name, ref):
     smp = scenes.grid_samples(w, h) if kind == "grid" else scenes.barrel_samples(w, h)
     xf = scenes.camera_transform(eye, target)
     vp = scenes.viewport_for(w, h)
-    f = ref.render(sc, smp, xf, vp, w, h, msaa, fp_mode=_abi.HVVR_FP_STRICT, threads=4, tile_capacity=1 << 20)
+    f = ref.render(sc, smp, xf, vp, w, h, msaa, fp_mode=_abi.HVVR_FP_STRICT, threads=4, tile_capacity=1 << 20,
+                   lens=lens)
     assert f.status == 0
     lights = np.frombuffer(b"".join(bytes(l) for l in sc.lights), dtype=np.uint8)
     xf_arr = np.frombuffer(bytes(xf), dtype=np.uint8)
@@ -48,6 +51,7 @@ def make(name, ref):
         os.path.join(ROOT, "tests", "golden", name + ".npz"),
         in_verts=in_verts, in_tris=in_tris, materials=sc.materials, lights=lights, samples=smp,
         cam_xf=xf_arr, viewport=vp_arr, dims=np.array([w, h, msaa], dtype=np.uint32),
+        lens=np.array(lens, dtype=np.float32),
         topo_verts=verts, topo_tris=tris, topo_nodes=nodes,
         nodes=f.nodes, tris_bits=f.tris.view(np.uint32), beams_bits=f.beams.view(np.uint32), remap=f.remap,
         block_sizes=f.block_sizes, block_entries=f.block_entries, tile_counts=f.tile_counts,
@@ -58,6 +62,7 @@ def make(name, ref):
 
 
 if __name__ == "__main__":
+    # optional case names on the command line regenerate only those fixtures
     ref = pyoracle.Reference()
-    for n in CASES:
+    for n in (sys.argv[1:] or CASES):
         make(n, ref)

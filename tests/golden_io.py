@@ -26,3 +26,8 @@ def load(name):
     vp = _abi.FloatRect.from_buffer_copy(g["viewport"].tobytes())
     w, h, msaa = (int(v) for v in g["dims"])
     return g, sc, g["samples"], xf, vp, w, h, msaa
+
+
+def lens(g):
+    """(radius, focal distance) of the fixture's thin lens ((0, 1): pinhole)."""
+    return tuple(float(v) for v in g["lens"]) if "lens" in g else (0.0, 1.0)

@@ -7,19 +7,21 @@ the valid samples: the reference leaves the padding samples that fill the last b
 uninitialised (BeamBatch2D stops writing at the last valid sample), while this build defines
 them as zero samples. HVVR_FP_FMA mode moves the FMA-marked
 edge-test terms, so hit IDs may differ only at exact triangle edges; the count is enumerated.
+The `_dof` fixture renders through a thin lens (radius 0.08, focal distance 7.5): the
+reference's IntersectTriangleThreadDoF path with its lens-position table.
 """
 import numpy as np
 import pytest
 
 from hvvr_b200 import _abi, scenes
 
-from golden_io import load, names
+from golden_io import lens, load, names
 
 
 @pytest.mark.parametrize("name", names())
 def test_oracle_matches_reference_golden(oracle, name):
     g, sc, smp, xf, vp, w, h, msaa = load(name)
-    f = oracle.render(sc, smp, xf, vp, w, h, msaa, fp_mode=_abi.HVVR_FP_STRICT, threads=2)
+    f = oracle.render(sc, smp, xf, vp, w, h, msaa, fp_mode=_abi.HVVR_FP_STRICT, threads=2, lens=lens(g))
     assert f.status == 0
     assert np.array_equal(f.nodes, g["nodes"])
     assert np.array_equal(f.tris.view(np.uint32), g["tris_bits"])
@@ -41,7 +43,7 @@ def test_oracle_matches_reference_golden(oracle, name):
 @pytest.mark.parametrize("name", names())
 def test_oracle_fma_mode_edge_mismatches(oracle, name):
     g, sc, smp, xf, vp, w, h, msaa = load(name)
-    f = oracle.render(sc, smp, xf, vp, w, h, msaa, fp_mode=_abi.HVVR_FP_FMA, threads=2)
+    f = oracle.render(sc, smp, xf, vp, w, h, msaa, fp_mode=_abi.HVVR_FP_FMA, threads=2, lens=lens(g))
     assert np.array_equal(f.tile_indices, g["tile_indices"])  # traversal does not depend on the mode
     n = len(smp)
     ids, gids = f.hit_ids[:n], g["hit_ids"][:n]
