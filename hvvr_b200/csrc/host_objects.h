@@ -121,8 +121,10 @@ struct hvvr_camera {
     DevBuf<StackEntry> blockStacks;
     DevBuf<uint32_t> blockSizes;
     DevBuf<TileList> tileLists;
-    DevBuf<uint32_t> colors, hitIds, image, tileCost;
+    DevBuf<uint32_t> colors, hitIds, image, tileCost, occRank;
     DevBuf<float> depth;
+    DevBuf<float2> lensPos;           // thin-lens table of rate lensRate
+    uint32_t lensRate = 0;
     void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
 };
 
@@ -145,7 +147,8 @@ struct hvvr_batch {
     std::vector<View> views;
     std::vector<uint64_t> layoutKey;
     uint32_t tiles = 0, blocks = 0;
-    uint32_t rateTiles[6] = {}, rateStart[6] = {};
+    uint32_t rateTiles[kRateClasses] = {}, rateStart[kRateClasses] = {};
+    bool anyLens = false;             // a thin-lens view is in the layout
     bool fpStrict = false;
     bool costValid = false;           // every view's tileCost holds a previous frame's counts
     DevBuf<ViewDev> viewsDev;
@@ -158,10 +161,11 @@ struct hvvr_batch {
     int hostSlot = 0;
     uint32_t* hostCounters = nullptr; // pinned copy of counters after each frame
     bool counterValid = false;
-    cudaStream_t side[12] = {};       // per rate: [2r] heavy tiles (high priority), [2r+1] the rest
-    cudaEvent_t forkEv = nullptr, doneEv[12] = {}, ev[6] = {};
-    cudaEvent_t kev[12][3] = {};      // per side stream: before tile cull, after it, after intersect
-    bool kevUsed[12] = {};
+    cudaStream_t side[2 * kRateClasses] = {}; // per rate class: [2r] heavy tiles (high priority), [2r+1] the rest
+    cudaEvent_t forkEv = nullptr, rankEv = nullptr, doneEv[2 * kRateClasses] = {}, cullEv[2 * kRateClasses] = {};
+    cudaEvent_t ev[6] = {};
+    cudaEvent_t kev[2 * kRateClasses][3] = {}; // per side stream: before tile cull, after it, after intersect
+    bool kevUsed[2 * kRateClasses] = {};
     bool stageTimes = false;          // ev[1..4] and kev were recorded by the last frame
     cudaGraphExec_t graph = nullptr;
     std::vector<uint64_t> graphKey;

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <random>
 
 namespace hvb {
 
@@ -162,6 +163,30 @@ void msaaOffsets(uint32_t n, float* out) {
         out[2 * i + 0] = cosf(angle) * radius;
         out[2 * i + 1] = sinf(angle) * radius;
     }
+}
+
+// GPUCamera::initLookupTables (libraries/hvvr/raycaster/gpu_camera.cu:59-88): for each of the 4
+// table tiles and 128 samples one random rotation (std::mt19937, default seed, drawn through
+// uniform_real_distribution<float> and scaled by Tau), and subsample i of that sample takes the
+// rotated spiral position (7 i + 7) mod n. Layout [tile][subsample][sample], 2 floats each.
+void lensTable(uint32_t n, float* out) {
+    std::uniform_real_distribution<float> dist(0.0f, 1.0f);
+    std::mt19937 gen;
+    const float tauF = 6.283185307180f; // Tau (libraries/hvvr/shared/constants_math.h:16)
+    const int turns = kTau[n];
+    for (uint32_t tile = 0; tile < 4; tile++)
+        for (uint32_t s = 0; s < kTileSize; s++) {
+            const float rotation = dist(gen) * tauF;
+            for (uint32_t i = 0; i < n; i++) {
+                const int k = int((i * 7 + 7) % n);
+                const float alpha = float(k + 0.5f) * (1.0f / float(n));
+                const float angle = alpha * (float(turns) * 6.28f) + rotation;
+                const float radius = sqrtf(alpha);
+                const size_t o = (size_t(tile) * kTileSize * n + size_t(i) * kTileSize + s) * 2;
+                out[o + 0] = cosf(angle) * radius;
+                out[o + 1] = sinf(angle) * radius;
+            }
+        }
 }
 
 void buildSampleSetup(const hvvr_sample* samples, uint32_t count, uint32_t split, const hvvr_float_rect& vp,

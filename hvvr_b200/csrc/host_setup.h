@@ -25,6 +25,8 @@ Mat4 transformToMatrix(const hvvr_transform& t);
 
 // getSubsampleUnitOffset<N> with JITTER_SAMPLES=0 (libraries/hvvr/raycaster/gpu_samples.h:35-61)
 void msaaOffsets(uint32_t n, float* out2n);
+// depth-of-field lens positions for rate n: [4 tiles][n subsamples][128 samples] x 2 floats
+void lensTable(uint32_t n, float* out);
 
 struct SampleSetup {
     uint32_t blocks = 0, tiles = 0, padded = 0, valid = 0;

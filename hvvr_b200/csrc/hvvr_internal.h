@@ -139,7 +139,11 @@ struct ViewDev {
     uint32_t* hitIds;                // nullptr unless capturing
     float* depth;
     uint32_t tileStart, blockStart;  // first global tile / block
-    uint32_t msaa, rateIdx;          // rate and its index in 1,2,4,8,16,32
+    uint32_t msaa, rateIdx;          // rate; its class: log2(msaa), + 6 for a thin-lens view
+    // thin lens (depth of field) when lensRadius > 0
+    float lensRadius, focalDistance;
+    const float2* lensPos;           // [4 tiles][msaa][128] lens positions (the reference's lookup table)
+    uint32_t* occRank;               // [tiles] rank of each tile among the view's non-empty tiles
 };
 
 // frame-wide device state shared by the launches of one batch
@@ -159,9 +163,11 @@ struct FrameDev {
 // records the message returned by hvvr_last_error() on this thread and returns code
 int setLastError(int code, const char* msg);
 
-// counters: [0] chunk allocator, [1] status, then per tile-cull launch k (up to 12) three
-// words at kQueueBase + 3k: work-queue head, retry count, retry-queue head
-enum : uint32_t { kCounterWords = 40, kQueueBase = 2, kQueueWords = 3 };
+// rate classes: log2(msaa) for pinhole views, 6 + log2(msaa) for thin-lens views
+enum : uint32_t { kRateClasses = 12 };
+// counters: [0] chunk allocator, [1] status, then per tile-cull launch k (2 per rate class)
+// three words at kQueueBase + 3k: work-queue head, retry count, retry-queue head
+enum : uint32_t { kQueueBase = 2, kQueueWords = 3, kCounterWords = kQueueBase + kQueueWords * 2 * kRateClasses };
 
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
 cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st);
@@ -175,8 +181,10 @@ cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st);
 // culled again by a second launch with a 4096-entry stack.
 cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
                            uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st);
-cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, const uint32_t* order,
+cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, bool dof, const uint32_t* order,
                                  uint32_t first, uint32_t count, cudaStream_t st);
+// occRank of every thin-lens view (one block per view; pinhole views are skipped)
+cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
 cudaError_t launchRefit(const SceneDev& s, cudaStream_t st);
 cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <mutex>
 #include <memory>
@@ -299,6 +300,10 @@ void releaseCamera(hvvr_camera* cam) { unregisterTarget(cam); }
 
 uint32_t rateIndex(uint32_t rate) { return rate <= 1 ? 0u : uint32_t(31 - __builtin_clz(rate)); }
 
+bool hasLens(const hvvr_camera* c) { return c->lens.radius > 0.0f; }
+// launches are grouped by rate class: log2(msaa), + 6 for a thin-lens view (a separate kernel)
+uint32_t rateClass(const hvvr_camera* c) { return rateIndex(c->msaa) + (hasLens(c) ? 6u : 0u); }
+
 // the offset tables live in one __constant__ array per device, written once per rate
 int ensureMsaaTable(uint32_t rate, cudaStream_t st) {
     static std::mutex mu;
@@ -417,10 +422,12 @@ int batchResources(hvvr_batch* b) {
     if (!b->forkEv) {
         int leastPriority = 0, greatestPriority = 0;
         CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
-        for (int r = 0; r < 6; r++) {
+        for (uint32_t r = 0; r < kRateClasses; r++) {
             CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r], cudaStreamNonBlocking, greatestPriority));
             CUDA_TRY(cudaStreamCreateWithFlags(&b->side[2 * r + 1], cudaStreamNonBlocking));
         }
+        CUDA_TRY(cudaEventCreateWithFlags(&b->rankEv, cudaEventDisableTiming));
+        for (auto& e : b->cullEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&b->forkEv, cudaEventDisableTiming));
         for (auto& e : b->doneEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto& e : b->hostViewsEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -451,6 +458,9 @@ void releaseBatch(hvvr_batch* b) {
         if (*e) cudaEventDestroy(*e), *e = nullptr;
     for (auto& e : b->doneEv)
         if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto& e : b->cullEv)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    if (b->rankEv) cudaEventDestroy(b->rankEv), b->rankEv = nullptr;
     for (auto& e : b->hostViewsEv)
         if (e) cudaEventDestroy(e), e = nullptr;
     for (auto& e : b->ev)
@@ -490,10 +500,14 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
     CUDA_TRY(cudaEventRecord(b->forkEv, st));
     bool first = true;
     for (auto& u : b->kevUsed) u = false;
-    for (uint32_t r = 0; r < 6; r++) {
+    // Pinhole classes: tile cull then intersect on the same stream, per part. Thin-lens
+    // classes (one part each) need the occupied-tile ranks of the whole view, so all their
+    // culls finish before one rank launch, and their intersects follow it.
+    for (uint32_t r = 0; r < kRateClasses; r++) {
         const uint32_t n = b->rateTiles[r];
         if (!n) continue;
-        const uint32_t rs = b->rateStart[r], heavy = heavyTiles(b, n), msaa = 1u << r;
+        const bool lens = r >= 6;
+        const uint32_t rs = b->rateStart[r], heavy = lens ? 0u : heavyTiles(b, n), msaa = 1u << (r % 6);
         // part 0: last frame's slowest tiles on the high-priority stream; part 1: the rest
         for (uint32_t part = heavy ? 0u : 1u; part < 2; part++) {
             const uint32_t k = 2 * r + part;
@@ -505,7 +519,11 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
                                     b->cfg.tile_cull_warps, b->cfg.tile_stack_entries, ps));
             if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][1], ps));
             if (timing && part == 1 && first) CUDA_TRY(cudaEventRecord(b->ev[2], ps));
-            CUDA_TRY(launchIntersectShade(fr, msaa, b->fpStrict, fr.order, p0, pn, ps));
+            if (lens) {
+                CUDA_TRY(cudaEventRecord(b->cullEv[k], ps));
+                continue;
+            }
+            CUDA_TRY(launchIntersectShade(fr, msaa, b->fpStrict, false, fr.order, p0, pn, ps));
             if (timing) {
                 CUDA_TRY(cudaEventRecord(b->kev[k][2], ps));
                 b->kevUsed[k] = true;
@@ -514,6 +532,26 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
             CUDA_TRY(cudaStreamWaitEvent(st, b->doneEv[k], 0));
         }
         first = false;
+    }
+    if (b->anyLens) {
+        for (uint32_t r = 6; r < kRateClasses; r++)
+            if (b->rateTiles[r]) CUDA_TRY(cudaStreamWaitEvent(st, b->cullEv[2 * r + 1], 0));
+        CUDA_TRY(launchOccupiedRank(fr, st));
+        CUDA_TRY(cudaEventRecord(b->rankEv, st));
+        for (uint32_t r = 6; r < kRateClasses; r++) {
+            const uint32_t n = b->rateTiles[r];
+            if (!n) continue;
+            const uint32_t k = 2 * r + 1;
+            cudaStream_t ps = b->side[k];
+            CUDA_TRY(cudaStreamWaitEvent(ps, b->rankEv, 0));
+            CUDA_TRY(launchIntersectShade(fr, 1u << (r % 6), b->fpStrict, true, fr.order, b->rateStart[r], n, ps));
+            if (timing) {
+                CUDA_TRY(cudaEventRecord(b->kev[k][2], ps));
+                b->kevUsed[k] = true;
+            }
+            CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
+            CUDA_TRY(cudaStreamWaitEvent(st, b->doneEv[k], 0));
+        }
     }
     if (timing) CUDA_TRY(cudaEventRecord(b->ev[3], st));
     for (const auto& v : b->views) CUDA_TRY(launchRemap(v.cam->dev, st));
@@ -599,6 +637,16 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
                 d.hitIds = nullptr;
                 d.depth = nullptr;
             }
+            if (hasLens(c)) {
+                if (c->lensRate != c->msaa || !c->lensPos.p) {
+                    std::vector<float> tab(size_t(kTileSize) * 4 * c->msaa * 2);
+                    lensTable(c->msaa, tab.data());
+                    TRY(c->lensPos.upload(tab.data(), tab.size() / 2, st));
+                    CUDA_TRY(cudaStreamSynchronize(st)); // the host table goes out of scope
+                    c->lensRate = c->msaa;
+                }
+                TRY(c->occRank.alloc(d.tiles));
+            }
             if (c->target.memory_type == HVVR_MEMORY_CPU && c->target.data) {
                 cpuTargets = true;
                 if (!c->registered) capturable = false; // pageable copies cannot be captured
@@ -613,15 +661,20 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     for (const hvvr_camera* c : cams) {
         const uint64_t k[] = {uint64_t(uintptr_t(c)), c->setupGen, c->msaa, uint64_t(uintptr_t(c->dev.hitIds)),
                               uint64_t(uintptr_t(c->target.data)), c->target.memory_type, c->target.stride,
-                              uint64_t(uintptr_t(c->registered))};
-        key.insert(key.end(), k, k + 8);
+                              uint64_t(uintptr_t(c->registered)), uint64_t(hasLens(c)),
+                              uint64_t(uintptr_t(c->lensPos.p)), uint64_t(uintptr_t(c->occRank.p))};
+        key.insert(key.end(), k, k + 11);
     }
     if (key != b->layoutKey) {
         b->views.clear();
         b->tiles = b->blocks = 0;
-        uint32_t rateTiles[6] = {};
+        uint32_t rateTiles[kRateClasses] = {};
         std::vector<uint32_t> blockView;
-        for (const hvvr_camera* c : cams) rateTiles[rateIndex(c->msaa)] += c->dev.tiles;
+        b->anyLens = false;
+        for (const hvvr_camera* c : cams) {
+            rateTiles[rateClass(c)] += c->dev.tiles;
+            b->anyLens = b->anyLens || hasLens(c);
+        }
         for (uint32_t i = 0; i < cams.size(); i++) {
             hvvr_camera* c = cams[i];
             b->views.push_back(hvvr_batch::View{c, b->tiles, b->blocks});
@@ -630,7 +683,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
             b->blocks += c->dev.blocks;
         }
         uint32_t run = 0;
-        for (int r = 0; r < 6; r++) {
+        for (uint32_t r = 0; r < kRateClasses; r++) {
             b->rateTiles[r] = rateTiles[r];
             b->rateStart[r] = run;
             run += rateTiles[r];
@@ -675,7 +728,11 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
         v.tileStart = b->views[i].tileStart;
         v.blockStart = b->views[i].blockStart;
         v.msaa = c->msaa;
-        v.rateIdx = rateIndex(c->msaa);
+        v.rateIdx = rateClass(c);
+        v.lensRadius = hasLens(c) ? c->lens.radius : 0.0f;
+        v.focalDistance = c->lens.focal_distance;
+        v.lensPos = hasLens(c) ? c->lensPos.p : nullptr;
+        v.occRank = hasLens(c) ? c->occRank.p : nullptr;
         hv[i] = v;
     }
     CUDA_TRY(cudaMemcpyAsync(b->viewsDev.p, hv, b->views.size() * sizeof(ViewDev), cudaMemcpyHostToDevice, st));
@@ -956,7 +1013,7 @@ int kernelTimes(const hvvr_batch* b, float* ms4) {
     if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was a graph replay (no per-launch events)");
     CUDA_TRY(cudaEventSynchronize(b->ev[5]));
     float cull = 0.0f, isect = 0.0f, t = 0.0f;
-    for (int k = 0; k < 12; k++) {
+    for (uint32_t k = 0; k < 2 * kRateClasses; k++) {
         if (!b->kevUsed[k]) continue;
         CUDA_TRY(cudaEventElapsedTime(&t, b->kev[k][0], b->kev[k][1]));
         cull += t;
@@ -976,7 +1033,7 @@ int hvvr_batch_read_stats(const hvvr_batch* b, uint64_t* out4) {
     if (!b->counterValid || !b->hostCounters) return fail(HVVR_ERR_STATE, "the batch has not rendered a frame");
     CUDA_TRY(cudaEventSynchronize(b->ev[5]));
     uint64_t retried = 0;
-    for (uint32_t k = 0; k < 12; k++) retried += b->hostCounters[kQueueBase + kQueueWords * k + 1];
+    for (uint32_t k = 0; k < 2 * kRateClasses; k++) retried += b->hostCounters[kQueueBase + kQueueWords * k + 1];
     out4[0] = uint64_t(std::min(b->hostCounters[0], b->poolChunks)) * kChunk;
     out4[1] = retried;
     out4[2] = b->hostCounters[1];
@@ -1194,7 +1251,9 @@ int hvvr_camera_set_viewport(hvvr_camera* cam, const hvvr_float_rect* viewport) 
 int hvvr_camera_set_lens(hvvr_camera* cam, const hvvr_thin_lens* lens) {
     CAM_CHECK(cam);
     if (!lens) return fail(HVVR_ERR_INVALID, "NULL lens");
-    if (lens->radius != 0.0f) return fail(HVVR_ERR_INVALID, "thin-lens depth of field is not built (radius must be 0)");
+    if (!(lens->radius >= 0.0f) || !std::isfinite(lens->radius) || !(lens->focal_distance > 0.0f) ||
+        !std::isfinite(lens->focal_distance))
+        return fail(HVVR_ERR_INVALID, "lens radius must be >= 0 and the focal distance > 0");
     cam->lens = *lens;
     cam->setupDirty = true;
     return HVVR_OK;
@@ -1207,9 +1266,9 @@ int hvvr_camera_set_aperture(hvvr_camera* cam, float radius) {
 }
 int hvvr_camera_set_focal_depth(hvvr_camera* cam, float depth) {
     CAM_CHECK(cam);
-    cam->lens.focal_distance = depth;
-    cam->setupDirty = true;
-    return HVVR_OK;
+    hvvr_thin_lens l = cam->lens;
+    l.focal_distance = depth;
+    return hvvr_camera_set_lens(cam, &l);
 }
 int hvvr_camera_set_eye_dir(hvvr_camera* cam, const hvvr_vec3* eye_dir) {
     CAM_CHECK(cam);

@@ -228,6 +228,44 @@ __device__ __forceinline__ void sortKeys(uint32_t (&k)[N]) {
     }
 }
 
+// interpolate (shading.h:18-36) the hit's vertices at barycentrics bc and GGXShade it
+__device__ F3 shadeHit(const ViewDev& V, uint32_t triIndex, F3 bc, F3 camPos, const LightEnvDev& env) {
+    const uint4 ts = __ldg(viewPtr(V.triShade) + triIndex);
+    const float4* __restrict__ verts = viewPtr(V.verts);
+    const float4* __restrict__ materials = viewPtr(V.materials);
+    const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
+    const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
+    const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
+    const F3 pos = (f3(a0.x, a0.y, a0.z) * bc.x + f3(p0.x, p0.y, p0.z) * bc.y) + f3(q0.x, q0.y, q0.z) * bc.z;
+    const F3 nrm = (halfNormal(a0, a1) * bc.x + halfNormal(p0, p1) * bc.y) + halfNormal(q0, q1) * bc.z;
+    const float4 m0 = __ldg(materials + 4 * size_t(ts.w) + 0);
+    const float4 m1 = __ldg(materials + 4 * size_t(ts.w) + 1);
+    const float4 m2 = __ldg(materials + 4 * size_t(ts.w) + 2);
+    const float4 m3 = __ldg(materials + 4 * size_t(ts.w) + 3);
+    Material mat;
+    mat.emissive = f3(m0.x, m0.y, m0.z);
+    mat.diffuse = f3(m1.x, m1.y, m1.z);
+    mat.specular = f3(m2.x, m2.y, m2.z);
+    mat.glossiness = m3.x;
+    mat.model = __float_as_uint(m3.z) & 0xffffu;
+    return ggxShade(mat, pos, nrm, camPos, env);
+}
+
+// TestTriangleFrustaUVW (prim_tests.h:89-116) over the tile's four world-space corner rays:
+// true when every barycentric coordinate is out of [0, 1] on the same side for all four
+__device__ __forceinline__ bool uvwAllOut(const float (&ro)[4][3], const float (&rd)[4][3], const TriGeom& tri) {
+    float uMin = FLT_MAX, uMax = -FLT_MAX, vMin = FLT_MAX, vMax = -FLT_MAX, wMin = FLT_MAX, wMax = -FLT_MAX;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        float u, v, w;
+        rayTriUVW(f3(ro[r][0], ro[r][1], ro[r][2]), f3(rd[r][0], rd[r][1], rd[r][2]), tri, u, v, w);
+        uMin = tminf(uMin, u); uMax = tmaxf(uMax, u);
+        vMin = tminf(vMin, v); vMax = tmaxf(vMax, v);
+        wMin = tminf(wMin, w); wMax = tmaxf(wMax, w);
+    }
+    return uMax < 0 || uMin > 1 || vMax < 0 || vMin > 1 || wMax < 0 || wMin > 1;
+}
+
 struct ShadeSmem {
     float ro[4][3], rd[4][3]; // world corner rays
     float pl[4][4];           // frustum planes
@@ -346,19 +384,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
                 t = dot3(v0r, normal);
                 if (!(t < 0.0f)) {
                     // TestTriangleFrustaUVW != intersect_all_out
-                    float uMin = FLT_MAX, uMax = -FLT_MAX, vMin = FLT_MAX, vMax = -FLT_MAX, wMin = FLT_MAX,
-                          wMax = -FLT_MAX;
-#pragma unroll
-                    for (int r = 0; r < 4; r++) {
-                        float u, v, w;
-                        rayTriUVW(f3(sm.ro[r][0], sm.ro[r][1], sm.ro[r][2]), f3(sm.rd[r][0], sm.rd[r][1], sm.rd[r][2]),
-                                  tri, u, v, w);
-                        uMin = tminf(uMin, u); uMax = tmaxf(uMax, u);
-                        vMin = tminf(vMin, v); vMax = tmaxf(vMax, v);
-                        wMin = tminf(wMin, w); wMax = tmaxf(wMax, w);
-                    }
-                    const bool allOut = uMax < 0 || uMin > 1 || vMax < 0 || vMin > 1 || wMax < 0 || wMin > 1;
-                    if (!allOut) {
+                    if (!uvwAllOut(sm.ro, sm.rd, tri)) {
                         keep = true;
                         e0 = tri.e0;
                         e1 = tri.e1;
@@ -468,25 +494,293 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         const F3 v0r = camPos - tri.v0;
         const TriThread th = threadSetup(tri.e0, tri.e1, v0r, c, du, dv);
         const F3 bc = calcUVW<FMA>(th, cax, cay);
-        const uint4 ts = __ldg(viewPtr(V.triShade) + triIndex);
-        const float4* __restrict__ verts = viewPtr(V.verts);
-        const float4* __restrict__ materials = viewPtr(V.materials);
-        const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
-        const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
-        const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
-        const F3 pos = (f3(a0.x, a0.y, a0.z) * bc.x + f3(p0.x, p0.y, p0.z) * bc.y) + f3(q0.x, q0.y, q0.z) * bc.z;
-        const F3 nrm = (halfNormal(a0, a1) * bc.x + halfNormal(p0, p1) * bc.y) + halfNormal(q0, q1) * bc.z;
-        const float4 m0 = __ldg(materials + 4 * size_t(ts.w) + 0);
-        const float4 m1 = __ldg(materials + 4 * size_t(ts.w) + 1);
-        const float4 m2 = __ldg(materials + 4 * size_t(ts.w) + 2);
-        const float4 m3 = __ldg(materials + 4 * size_t(ts.w) + 3);
-        Material mat;
-        mat.emissive = f3(m0.x, m0.y, m0.z);
-        mat.diffuse = f3(m1.x, m1.y, m1.z);
-        mat.specular = f3(m2.x, m2.y, m2.z);
-        mat.glossiness = m3.x;
-        mat.model = __float_as_uint(m3.z) & 0xffffu;
-        const F3 col = ggxShade(mat, pos, nrm, camPos, env);
+        const F3 col = shadeHit(V, triIndex, bc, camPos, env);
+        rx = rx + col.x * pc;
+        ry = ry + col.y * pc;
+        rz = rz + col.z * pc;
+    }
+    const float sN = 1.0f / float(N);
+    viewPtr(V.colors)[sid] = packColor(f3(aces(rx * sN), aces(ry * sN), aces(rz * sN)));
+}
+
+// ------------------------------------------------------------------ thin lens (depth of field)
+// IntersectTriangleTile<true>, IntersectTriangleThreadDoF (prim_tests.h:247-392), TileData<true>
+// (tile_data.h:33-60), GetSampleUVsDoF (gpu_samples.h:84-103), and the DoF branches of
+// IntersectSamples / ShadeMSAA (intersect.cu:117-168, resolve.cu:161-284). FMA selects the
+// contraction the kernel comments mark (per-subsample t, denom, depth, ray origin/direction,
+// cross and dot products).
+__device__ __forceinline__ F3 fma3(float s, F3 a, F3 c) { return f3(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y), fmaf(s, a.z, c.z)); }
+
+template <bool FMA>
+__device__ __forceinline__ void dofBary(F3 e0, F3 e1, F3 v0l, float ddx, float ddy, float dc, F3 lc2fc, F3 lu, F3 lv,
+                                        float2 luv, float2 duv, float& denom, float& v, float& w) {
+    if (FMA) {
+        denom = fmaf(ddy, duv.y, fmaf(ddx, duv.x, dc));
+        const F3 o = fma3(luv.y, lv, fma3(luv.x, lu, v0l));
+        const F3 a = -fma3(duv.y, lv, fma3(duv.x, lu, lc2fc));
+        const F3 e = f3(fmaf(a.y, o.z, -(a.z * o.y)), fmaf(a.z, o.x, -(a.x * o.z)), fmaf(a.x, o.y, -(a.y * o.x)));
+        v = fmaf(e1.z, e.z, fmaf(e1.y, e.y, e1.x * e.x));
+        w = -fmaf(e0.z, e.z, fmaf(e0.y, e.y, e0.x * e.x));
+    } else {
+        denom = dc + ddx * duv.x + ddy * duv.y;
+        const F3 o = (v0l + lu * luv.x) + lv * luv.y;
+        const F3 rd = (lc2fc + lu * duv.x) + lv * duv.y;
+        const F3 e = cross3(-rd, o);
+        v = dot3(e1, e);
+        w = -dot3(e0, e);
+    }
+}
+
+// dirUV = aaOffset * focalToLensScale - lensUV
+template <bool FMA>
+__device__ __forceinline__ float2 dofDirUV(float2 aa, float fx, float fy, float2 luv) {
+    return FMA ? make_float2(fmaf(aa.x, fx, -luv.x), fmaf(aa.y, fy, -luv.y))
+               : make_float2(aa.x * fx - luv.x, aa.y * fy - luv.y);
+}
+
+struct DofSmem {
+    float ro[4][3], rd[4][3]; // world corner rays
+    float pl[4][4];           // frustum planes
+    float lensU[3], lensV[3], fls[2];
+    uint32_t idx[kChunk];
+    float tc[kChunk], tu[kChunk], tv[kChunk], ddx[kChunk], ddy[kChunk];
+    float e0[3][kChunk];
+    float e1[3][kChunk];
+    float vl[3][kChunk];
+    uint32_t warpCount[4];
+};
+
+template <uint32_t N, bool FMA>
+__global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr, const uint32_t* __restrict__ order,
+                                                                     uint32_t first) {
+    __shared__ DofSmem sm;
+    __shared__ LightEnvDev env;
+    __shared__ Mat4 M;
+    const uint32_t gt = order ? order[first + blockIdx.x] : first + blockIdx.x;
+    const ViewDev& V = fr.views[fr.viewCount == 1 ? 0u : __ldg(fr.blockView + gt / kTilesPerBlock)];
+    const uint32_t tile = gt - V.tileStart;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t sid = tile * kTileSize + tid;
+    const TileList L = V.tileLists[tile];
+    if (L.count == 0) {
+        V.colors[sid] = 0xFF000000u;
+        if (uint32_t* hitOut = V.hitIds) {
+#pragma unroll
+            for (uint32_t i = 0; i < N; i++) {
+                hitOut[size_t(sid) * N + i] = ~0u;
+                V.depth[size_t(sid) * N + i] = INFINITY;
+            }
+        }
+        return;
+    }
+    const int rate = RateIndex<N>::v;
+    for (uint32_t i = tid; i < sizeof(LightEnvDev) / 4; i += kTileSize)
+        reinterpret_cast<uint32_t*>(&env)[i] = reinterpret_cast<const uint32_t*>(&V.env)[i];
+    if (tid < 16) reinterpret_cast<float*>(&M)[tid] = reinterpret_cast<const float*>(&V.M)[tid];
+    __syncthreads();
+    const float4* __restrict__ beams = V.beams;
+    const float4 b0 = __ldg(beams + 3 * size_t(sid) + 0);
+    const float4 b1 = __ldg(beams + 3 * size_t(sid) + 1);
+    const float4 b2 = __ldg(beams + 3 * size_t(sid) + 2);
+    const F3 c = xformDir(M, f3(b0.x, b0.y, b0.z));
+    if (tid < 8) {
+        const Rays4& cr = V.tileRays[tile];
+        const uint32_t i = tid & 3u;
+        if (tid < 4) {
+            const F3 o = xformPoint(M, f3(cr.o[i][0], cr.o[i][1], cr.o[i][2]));
+            sm.ro[i][0] = o.x; sm.ro[i][1] = o.y; sm.ro[i][2] = o.z;
+        } else {
+            const F3 d = xformDir(M, f3(cr.d[i][0], cr.d[i][1], cr.d[i][2]));
+            sm.rd[i][0] = d.x; sm.rd[i][1] = d.y; sm.rd[i][2] = d.z;
+        }
+    }
+    if (tid == kTileSize / 2) {
+        // TileData<true>::load on this sample's world-space beam; the reference rotates the
+        // already rotated du/dv a second time (cameraToWorldRotation * sample.du); kept
+        const F3 fu = xformDir(M, xformDir(M, f3(b0.w, b1.x, b1.y)));
+        const F3 fv = xformDir(M, xformDir(M, f3(b1.z, b1.w, b2.x)));
+        const float uInv = 1.0f / sqrtf(dot3(fu, fu)), vInv = 1.0f / sqrtf(dot3(fv, fv));
+        const float uMag = 1.0f / uInv, vMag = 1.0f / vInv;
+        const F3 lu = fu * (V.lensRadius * uInv), lv = fv * (V.lensRadius * vInv);
+        sm.lensU[0] = lu.x; sm.lensU[1] = lu.y; sm.lensU[2] = lu.z;
+        sm.lensV[0] = lv.x; sm.lensV[1] = lv.y; sm.lensV[2] = lv.z;
+        const float sc = V.focalDistance / V.lensRadius;
+        sm.fls[0] = sc * uMag;
+        sm.fls[1] = sc * vMag;
+    }
+    __syncthreads();
+    if (tid < 4) {
+        const F3 d0 = f3(sm.rd[tid][0], sm.rd[tid][1], sm.rd[tid][2]);
+        const F3 d1 = f3(sm.rd[(tid + 1) & 3][0], sm.rd[(tid + 1) & 3][1], sm.rd[(tid + 1) & 3][2]);
+        const F3 n = cross3(d0, d1);
+        sm.pl[tid][0] = n.x; sm.pl[tid][1] = n.y; sm.pl[tid][2] = n.z;
+        sm.pl[tid][3] = dot3(f3(sm.ro[tid][0], sm.ro[tid][1], sm.ro[tid][2]), n);
+    }
+    const F3 camPos = f3(M.m[3][0], M.m[3][1], M.m[3][2]);
+    // IntersectSamples: lens centre to the focal point of this sample's centre ray
+    const F3 centerDir = normalize3(c);
+    const float zed = dot3(xformDir(M, f3(0.0f, 0.0f, -1.0f)), centerDir);
+    const F3 lc2fc = centerDir * (V.focalDistance / zed);
+    // GetSampleUVsDoF: table tile = the reference's occupied-tile CTA index mod 4
+    const float2* __restrict__ lensPos = V.lensPos + (V.occRank[tile] & 3u) * kTileSize * N + tid;
+    float tmax[N];
+    uint32_t hit[N];
+#pragma unroll
+    for (uint32_t i = 0; i < N; i++) {
+        tmax[i] = FLT_MAX;
+        hit[i] = ~0u;
+    }
+    __syncthreads();
+    const F3 lu = f3(sm.lensU[0], sm.lensU[1], sm.lensU[2]), lv = f3(sm.lensV[0], sm.lensV[1], sm.lensV[2]);
+    const float flsx = sm.fls[0], flsy = sm.fls[1];
+
+    uint32_t chunk = L.first;
+    uint32_t remaining = L.count;
+    while (remaining > 0 && chunk < fr.poolChunks) {
+        const uint32_t n = remaining < kChunk ? remaining : kChunk;
+        const uint32_t nextChunk = fr.chunkNext[chunk];
+        bool keep = false;
+        uint32_t idx = 0;
+        TriGeom tri{};
+        F3 v0l = f3(0, 0, 0);
+        float tc = 0.0f, tu = 0.0f, tv = 0.0f, ddx = 0.0f, ddy = 0.0f;
+        if (tid < n) {
+            idx = fr.pool[size_t(chunk) * kChunk + tid];
+            tri = loadTri(viewPtr(V.tris), idx);
+            bool in = true;
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const F3 dir = f3(sm.pl[p][0], sm.pl[p][1], sm.pl[p][2]);
+                const float dist = sm.pl[p][3];
+                const float d0 = dot3(dir, tri.v0);
+                const float d1 = d0 + dot3(dir, tri.e0);
+                const float d2 = d0 + dot3(dir, tri.e1);
+                if (d0 > dist && d1 > dist && d2 > dist) in = false;
+            }
+            if (in) {
+                // IntersectTriangleTile<true>::setup
+                const F3 normal = cross3(tri.e0, tri.e1);
+                v0l = camPos - tri.v0;
+                tc = dot3(v0l, normal);
+                tu = dot3(lu, normal);
+                tv = dot3(lv, normal);
+                const float tExtent = fabsf(tu) + fabsf(tv);
+                if (!(tc + tExtent < 0.0f)) {
+                    ddx = dot3(-lu, normal);
+                    ddy = dot3(-lv, normal);
+                    // the corner-ray test only when every lens position sees the front of the plane
+                    keep = (tc - tExtent < 0.0f) || !uvwAllOut(sm.ro, sm.rd, tri);
+                }
+            }
+        }
+        const uint32_t bal = __ballot_sync(kFull, keep);
+        if (lane == 0) sm.warpCount[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t off = __popc(bal & ((1u << lane) - 1u));
+        uint32_t total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < 4; w++) {
+            const uint32_t cw = sm.warpCount[w];
+            off += (w < warp) ? cw : 0u;
+            total += cw;
+        }
+        if (keep) {
+            sm.idx[off] = idx;
+            sm.tc[off] = tc; sm.tu[off] = tu; sm.tv[off] = tv; sm.ddx[off] = ddx; sm.ddy[off] = ddy;
+            sm.e0[0][off] = tri.e0.x; sm.e0[1][off] = tri.e0.y; sm.e0[2][off] = tri.e0.z;
+            sm.e1[0][off] = tri.e1.x; sm.e1[1][off] = tri.e1.y; sm.e1[2][off] = tri.e1.z;
+            sm.vl[0][off] = v0l.x; sm.vl[1][off] = v0l.y; sm.vl[2][off] = v0l.z;
+        }
+        __syncthreads();
+        for (uint32_t j = 0; j < total; j++) {
+            const F3 je0 = f3(sm.e0[0][j], sm.e0[1][j], sm.e0[2][j]);
+            const F3 je1 = f3(sm.e1[0][j], sm.e1[1][j], sm.e1[2][j]);
+            const F3 jvl = f3(sm.vl[0][j], sm.vl[1][j], sm.vl[2][j]);
+            const float jtc = sm.tc[j], jtu = sm.tu[j], jtv = sm.tv[j], jdx = sm.ddx[j], jdy = sm.ddy[j];
+            const uint32_t jidx = sm.idx[j];
+            // IntersectTriangleThreadDoF ctor
+            const float dc = dot3(-lc2fc, cross3(je0, je1));
+#pragma unroll
+            for (uint32_t i = 0; i < N; i++) {
+                const float2 luv = __ldg(lensPos + i * kTileSize);
+                const float2 duv = dofDirUV<FMA>(cMsaa[rate][i], flsx, flsy, luv);
+                const float t = FMA ? fmaf(jtv, luv.y, fmaf(jtu, luv.x, jtc)) : jtc + jtu * luv.x + jtv * luv.y;
+                float denom, v, w;
+                dofBary<FMA>(je0, je1, jvl, jdx, jdy, dc, lc2fc, lu, lv, luv, duv, denom, v, w);
+                const float depthDelta = FMA ? fmaf(tmax[i], denom, -t) : tmax[i] * denom - t;
+                const float u = denom - v - w;
+                const int test = __float_as_int(t) | __float_as_int(depthDelta) | __float_as_int(u) |
+                                 __float_as_int(v) | __float_as_int(w);
+                // NaN fails (a padding sample's zero beam normalises to NaN; the sign-bit test alone
+                // would depend on which NaN the hardware produces)
+                if (test >= 0 && u == u && depthDelta == depthDelta) {
+                    tmax[i] = t * (1.0f / denom);
+                    hit[i] = jidx;
+                }
+            }
+        }
+        __syncthreads();
+        remaining -= n;
+        chunk = nextChunk;
+    }
+
+    if (uint32_t* hitOut = viewPtr(V.hitIds)) {
+        float* depthOut = viewPtr(V.depth);
+#pragma unroll
+        for (uint32_t i = 0; i < N; i++) {
+            hitOut[size_t(sid) * N + i] = hit[i];
+            depthOut[size_t(sid) * N + i] = hit[i] == ~0u ? INFINITY : tmax[i];
+        }
+    }
+
+    // EmitGBuffer grouping, then ShadeMSAA's DoF branch: centroid lens and direction UVs
+    uint32_t keys[N];
+#pragma unroll
+    for (uint32_t i = 0; i < N; i++) keys[i] = (hit[i] << 5) | i;
+    bool uniform = true;
+#pragma unroll
+    for (uint32_t i = 1; i < N; i++) uniform = uniform && (hit[i] == hit[0]);
+    if (!uniform) sortKeys<N>(keys);
+    float rx = 0.0f, ry = 0.0f, rz = 0.0f;
+    const uint32_t maskAll = N < 32 ? ((1u << N) - 1u) : ~0u;
+    uint32_t combined = 0;
+    uint32_t gi = 0;
+    while (gi < N) {
+        if (combined == maskAll) break;
+        const uint32_t triIndex = uint32_t(int32_t(keys[gi]) >> 5);
+        if (triIndex == ~0u) break;
+        uint32_t sampleMask = 0;
+        uint32_t gj = gi;
+        if (uniform) {
+            sampleMask = maskAll;
+            gj = N;
+        } else {
+            while (gj < N && uint32_t(int32_t(keys[gj]) >> 5) == triIndex) {
+                sampleMask |= 1u << (keys[gj] & 31u);
+                gj++;
+            }
+        }
+        gi = gj;
+        combined |= sampleMask;
+        const float pc = float(__popc(sampleMask));
+        const float inv = 1.0f / pc;
+        float clx = 0.0f, cly = 0.0f, cdx = 0.0f, cdy = 0.0f;
+        for (uint32_t cm = sampleMask; cm;) {
+            const int si = __ffs(cm) - 1;
+            cm &= ~(1u << si);
+            const float2 luv = __ldg(lensPos + uint32_t(si) * kTileSize);
+            const float2 duv = dofDirUV<FMA>(cMsaa[rate][si], flsx, flsy, luv);
+            clx = clx + luv.x * inv; cly = cly + luv.y * inv;
+            cdx = cdx + duv.x * inv; cdy = cdy + duv.y * inv;
+        }
+        const TriGeom tri = loadTri(viewPtr(V.tris), triIndex);
+        const F3 normal = cross3(tri.e0, tri.e1);
+        float denom, v, w;
+        dofBary<FMA>(tri.e0, tri.e1, camPos - tri.v0, dot3(-lu, normal), dot3(-lv, normal), dot3(-lc2fc, normal), lc2fc,
+                     lu, lv, make_float2(clx, cly), make_float2(cdx, cdy), denom, v, w);
+        const float u = denom - v - w;
+        const float dinv = 1.0f / denom;
+        const F3 col = shadeHit(V, triIndex, f3(u * dinv, v * dinv, w * dinv), camPos, env);
         rx = rx + col.x * pc;
         ry = ry + col.y * pc;
         rz = rz + col.z * pc;
@@ -496,10 +790,15 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
 }
 
 template <uint32_t N>
-cudaError_t launchRate(const FrameDev& fr, bool fpStrict, const uint32_t* order, uint32_t first, uint32_t count,
-                       cudaStream_t st) {
-    if (fpStrict) intersectShadeKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
-    else intersectShadeKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
+cudaError_t launchRate(const FrameDev& fr, bool fpStrict, bool dof, const uint32_t* order, uint32_t first,
+                       uint32_t count, cudaStream_t st) {
+    if (dof) {
+        if (fpStrict) intersectShadeDofKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
+        else intersectShadeDofKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
+    } else {
+        if (fpStrict) intersectShadeKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
+        else intersectShadeKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
+    }
     return cudaGetLastError();
 }
 
@@ -528,16 +827,16 @@ __global__ void remapKernel(const uint32_t* __restrict__ src, const int32_t* __r
 
 } // namespace
 
-cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, const uint32_t* order,
+cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, bool dof, const uint32_t* order,
                                  uint32_t first, uint32_t count, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     switch (msaa) {
-    case 1: return launchRate<1>(fr, fpStrict, order, first, count, st);
-    case 2: return launchRate<2>(fr, fpStrict, order, first, count, st);
-    case 4: return launchRate<4>(fr, fpStrict, order, first, count, st);
-    case 8: return launchRate<8>(fr, fpStrict, order, first, count, st);
-    case 16: return launchRate<16>(fr, fpStrict, order, first, count, st);
-    case 32: return launchRate<32>(fr, fpStrict, order, first, count, st);
+    case 1: return launchRate<1>(fr, fpStrict, dof, order, first, count, st);
+    case 2: return launchRate<2>(fr, fpStrict, dof, order, first, count, st);
+    case 4: return launchRate<4>(fr, fpStrict, dof, order, first, count, st);
+    case 8: return launchRate<8>(fr, fpStrict, dof, order, first, count, st);
+    case 16: return launchRate<16>(fr, fpStrict, dof, order, first, count, st);
+    case 32: return launchRate<32>(fr, fpStrict, dof, order, first, count, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -663,9 +663,9 @@ __global__ void __launch_bounds__(32) tileCullRetryKernel(TileCullArgs a) {
     }
 }
 
-// Orders the global tiles by (rate index ascending, cost descending), cost in log2 buckets
+// Orders the global tiles by (rate class ascending, cost descending), cost in log2 buckets
 // of last frame's visit counts. One block; positions within a bucket are in arrival order.
-constexpr uint32_t kOrderBuckets = 6 * 33;
+constexpr uint32_t kOrderBuckets = kRateClasses * 33;
 __global__ void __launch_bounds__(1024) tileOrderKernel(FrameDev fr) {
     __shared__ uint32_t hist[kOrderBuckets];
     __shared__ uint32_t start[kOrderBuckets];
@@ -690,6 +690,37 @@ __global__ void __launch_bounds__(1024) tileOrderKernel(FrameDev fr) {
 }
 
 __global__ void writeViewKernel(ViewDev v, ViewDev* dst) { *dst = v; }
+
+// The reference runs its intersect and resolve kernels over the compacted list of occupied tiles
+// (tileIndexRemapOccupied, libraries/hvvr/raycaster/traversal.cpp:213-330) and indexes the lens
+// table by that CTA index; this is each tile's rank among the view's non-empty tiles.
+__global__ void __launch_bounds__(1024) occupiedRankKernel(FrameDev fr) {
+    const ViewDev& V = fr.views[blockIdx.x];
+    if (!(V.lensRadius > 0.0f)) return;
+    __shared__ uint32_t warpSums[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const uint32_t lane = laneId(), warp = threadIdx.x >> 5;
+    const uint32_t tiles = (blockIdx.x + 1 < fr.viewCount ? fr.views[blockIdx.x + 1].tileStart : fr.tiles) - V.tileStart;
+    for (uint32_t base = 0; base < tiles; base += 1024) {
+        const uint32_t t = base + threadIdx.x;
+        const uint32_t occ = (t < tiles && V.tileLists[t].count > 0) ? 1u : 0u;
+        const uint32_t bal = __ballot_sync(kFull, occ);
+        if (lane == 0) warpSums[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = carry;
+        for (uint32_t w = 0; w < warp; w++) before += warpSums[w];
+        if (t < tiles) V.occRank[t] = before + __popc(bal & ((1u << lane) - 1u));
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t sum = 0;
+            for (uint32_t w = 0; w < 32; w++) sum += warpSums[w];
+            carry += sum;
+        }
+        __syncthreads();
+    }
+}
 
 struct DeviceLimits {
     int sms = 0;
@@ -768,6 +799,12 @@ cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t f
     }
     if (e != cudaSuccess) return e;
     return launchTileCullRetry(a, st);
+}
+
+cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st) {
+    if (fr.viewCount == 0) return cudaSuccess;
+    occupiedRankKernel<<<fr.viewCount, 1024, 0, st>>>(fr);
+    return cudaGetLastError();
 }
 
 cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st) {

@@ -848,6 +848,9 @@ inline bool dofTest(const DofTri& d, float denomCenter, V3 lc2fc, V3 lensU, V3 l
     float u = denom - v - w;
     int32_t test = int32_t(fbits(t) | fbits(depthDelta) | fbits(u) | fbits(v) | fbits(w));
     if (test < 0) return false;
+    // a NaN (the zero beam of a padding sample normalises to NaN) fails: the sign-bit test alone
+    // depends on which NaN the platform produces (x86's default NaN is negative)
+    if (u != u || depthDelta != depthDelta) return false;
     depth = t * (1.0f / denom);
     return true;
 }

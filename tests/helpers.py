@@ -24,7 +24,7 @@ def scene(name):
 
 
 def render_gpu(sc, samples, width, height, msaa, cam_xf=None, fp_mode=hv.HVVR_FP_FMA, capture=True, split=1,
-               viewport=None):
+               viewport=None, lens=None):
     rc = hv.Raycaster(fp_mode=fp_mode)
     rc.create_model(sc)
     for l in sc.lights:
@@ -34,6 +34,8 @@ def render_gpu(sc, samples, width, height, msaa, cam_xf=None, fp_mode=hv.HVVR_FP
     cam.set_samples(samples, split)
     cam.set_camera_to_world(cam_xf or scenes.camera_transform())
     cam.set_msaa(msaa)
+    if lens is not None:
+        cam.set_lens(*lens)
     if capture:
         cam.set_capture(hv.HVVR_CAPTURE_HITS)
     rc.render()
@@ -41,9 +43,9 @@ def render_gpu(sc, samples, width, height, msaa, cam_xf=None, fp_mode=hv.HVVR_FP
 
 
 def render_oracle(oracle, sc, samples, width, height, msaa, cam_xf=None, fp_mode=hv.HVVR_FP_FMA, split=1,
-                  viewport=None):
+                  viewport=None, lens=None):
     return oracle.render(sc, samples, cam_xf or scenes.camera_transform(), viewport or scenes.viewport_for(width, height),
-                         width, height, msaa, fp_mode=fp_mode, split=split)
+                         width, height, msaa, fp_mode=fp_mode, split=split, lens=lens or (0.0, 1.0))
 
 
 def list_mismatch(counts_a, idx_a, counts_b, idx_b):

@@ -150,3 +150,39 @@ def test_stack_retry_pass_matches_oracle(oracle):
         _check_view(oracle, sc, cam, smp, w, h, 4, xf)
     batch.close()
     rc.close()
+
+
+def test_batch_mixes_thin_lens_and_pinhole_views(oracle):
+    """Thin-lens and pinhole views of the same rate in one batch run as separate kernels
+    (rate classes); both match the oracle, over frames (graph replay)."""
+    sc_a, sc_b = scene("c1"), scene("small")
+    rc_a, rc_b = _make_rc(sc_a), _make_rc(sc_b)
+    views = []
+    for (rc, sc, w, h, kind, msaa, lens) in [(rc_a, sc_a, 192, 160, "barrel", 4, (0.06, 9.0)),
+                                             (rc_a, sc_a, 128, 96, "grid", 4, None),
+                                             (rc_b, sc_b, 160, 176, "barrel", 8, (0.1, 6.0)),
+                                             (rc_b, sc_b, 96, 96, "grid", 1, (0.03, 10.0))]:
+        cam, smp = _add_cam(rc, w, h, kind, msaa)
+        if lens:
+            cam.set_lens(*lens)
+        views.append((sc, cam, smp, w, h, msaa, lens))
+    batch = hv.Batch([rc_a, rc_b], hv.batch_config(tri_index_capacity=1 << 22))
+    for eye in ((0.0, 2.0, 10.0), (2.0, 1.5, 8.0), (-1.0, 2.5, 9.0)):
+        xfs = []
+        for k, (sc, cam, smp, w, h, msaa, lens) in enumerate(views):
+            xf = scenes.camera_transform(eye=(eye[0] + 0.2 * k, eye[1], eye[2]), target=(0.0, 0.0, 0.0))
+            cam.set_camera_to_world(xf)
+            xfs.append(xf)
+        batch.render()
+        for (sc, cam, smp, w, h, msaa, lens), xf in zip(views, xfs):
+            fo = render_oracle(oracle, sc, smp, w, h, msaa, cam_xf=xf, lens=lens)
+            counts, idx = cam.tile_lists()
+            assert list_mismatch(counts, idx, fo.tile_counts, fo.tile_indices) == 0
+            ids, depth = cam.hits()
+            assert np.array_equal(ids, fo.hit_ids)
+            assert np.array_equal(depth.view(np.uint32), fo.depth.view(np.uint32))
+            d = np.abs(cam.image.view(np.uint8).astype(np.int32) - fo.image.view(np.uint8).astype(np.int32))
+            assert d.max() <= 1
+    batch.close()
+    rc_a.close()
+    rc_b.close()

@@ -105,3 +105,24 @@ def test_c1_frame_sequence_two_cameras(oracle):
             fo = render_oracle(oracle, sc, smp, w, h, 4, cam_xf=xf)
             _compare(cam, rc, fo, 4)
     rc.close()
+
+
+@pytest.mark.parametrize("msaa,fp_mode", [(1, hv.HVVR_FP_FMA), (4, hv.HVVR_FP_FMA), (8, hv.HVVR_FP_STRICT),
+                                          (16, hv.HVVR_FP_FMA)])
+def test_thin_lens_depth_of_field(oracle, msaa, fp_mode):
+    """Thin-lens depth of field (the reference's IntersectTriangleThreadDoF path with its
+    lens-position table indexed by the occupied-tile rank), two frames so the second one
+    culls its slowest tiles first."""
+    sc = scene("small")
+    w, h = 160, 176
+    smp = scenes.barrel_samples(w, h)
+    xf = scenes.camera_transform(eye=(1.0, 2.2, 8.5), target=(0.0, 0.0, -1.0))
+    lens = (0.08, 7.5)
+    rc, cam = render_gpu(sc, smp, w, h, msaa, cam_xf=xf, fp_mode=fp_mode, lens=lens)
+    fo = render_oracle(oracle, sc, smp, w, h, msaa, cam_xf=xf, fp_mode=fp_mode, lens=lens)
+    _compare(cam, rc, fo, msaa)
+    rc.render()
+    _compare(cam, rc, fo, msaa)
+    pin = render_oracle(oracle, sc, smp, w, h, msaa, cam_xf=xf, fp_mode=fp_mode)
+    assert (fo.hit_ids != pin.hit_ids).any(), "the lens did not change the hits"
+    rc.close()
