@@ -79,6 +79,8 @@ _sig("hvvr_scene_read_nodes", _vp, _vp)
 _sig("hvvr_scene_read_triangles", _vp, _vp)
 _sig("hvvr_generate_topology", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32))
 _sig("hvvr_grid_samples", _u32, _u32, _vp)
+_sig("hvvr_polar_foveated_layout", _vp, _p(_u32), _p(_u32), _p(_u32), _p(_u32))
+_sig("hvvr_polar_foveated_samples", _vp, _vp, _vp, _vp, _vp)
 _sig("hvvr_tile_cull_static", _vp, _vp, _vp, C.c_uint64, _p(C.c_uint64), _vp)
 _lib.hvvr_batch_config_default.argtypes = [_p(_abi.BatchConfig)]
 _lib.hvvr_batch_config_default.restype = None
@@ -120,6 +122,7 @@ EXPORTED = [
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
     "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
+    "hvvr_polar_foveated_layout", "hvvr_polar_foveated_samples",
     "hvvr_tile_cull_static", "hvvr_batch_config_default", "hvvr_batch_create", "hvvr_batch_create_views",
     "hvvr_batch_destroy", "hvvr_model_update_vertices_device",
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
@@ -154,6 +157,34 @@ def generate_topology(scene):
                                        len(scene.tri_shade), nodes.ctypes.data, len(nodes), C.byref(cnt)))
     scene.nodes = nodes[: cnt.value].copy()
     return scene
+
+
+def foveated_spec(degree_tracking_error=0.5, max_fov_degrees=110.0, mar_slope=0.022, foveal_mar_degrees=1.0 / 60.0,
+                  **kw):
+    """hvvr_spec with the foveated sample-pattern parameters (RayCasterSpecification::FoveatedSamplePattern)."""
+    spec = _abi.Spec()
+    _lib.hvvr_spec_default(C.byref(spec))
+    spec.foveated_degree_tracking_error = degree_tracking_error
+    spec.foveated_max_fov_degrees = max_fov_degrees
+    spec.foveated_mar_slope = mar_slope
+    spec.foveated_foveal_mar_degrees = foveal_mar_degrees
+    for k, v in kw.items():
+        setattr(spec, k, v)
+    return spec
+
+
+def polar_foveated_samples(spec=None):
+    """The polar foveated sample set the library builds for spec (see hvvr_polar_foveated_samples)."""
+    spr, rings, valid, padded = _u32(0), _u32(0), _u32(0), _u32(0)
+    sp = C.byref(spec) if spec is not None else None
+    _check(_lib.hvvr_polar_foveated_layout(sp, C.byref(spr), C.byref(rings), C.byref(valid), C.byref(padded)))
+    out = {"samples_per_ring": spr.value, "ring_count": rings.value, "valid": valid.value, "padded": padded.value,
+           "beams": np.zeros((valid.value, 9), np.float32), "remap": np.zeros((padded.value, 2), np.uint32),
+           "tile_rays": np.zeros((padded.value // 128, 24), np.float32),
+           "block_rays": np.zeros((padded.value // 8192, 24), np.float32)}
+    _check(_lib.hvvr_polar_foveated_samples(sp, out["beams"].ctypes.data, out["remap"].ctypes.data,
+                                            out["tile_rays"].ctypes.data, out["block_rays"].ctypes.data))
+    return out
 
 
 def grid_samples(width, height):

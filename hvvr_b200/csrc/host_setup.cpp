@@ -53,28 +53,7 @@ struct Sorted {
 // naiveXYCluster (libraries/hvvr/raycaster/sample_clustering.h:17-49): y-then-x sort, then
 // x-then-y within rows of blocks, y-then-x within blocks, x-then-y within runs of 8 tiles
 void clusterXY(std::vector<Sorted>& v, size_t k) {
-    const size_t yStrata = (size_t)sqrt((double)k);
-    const size_t xStrata = (k + yStrata - 1) / yStrata;
-    const size_t blockYStrata = (size_t)sqrt((double)kTilesPerBlock);
-    const size_t blockXStrata = (kTilesPerBlock + blockYStrata - 1) / blockYStrata;
-    auto byYX = [](const Sorted& a, const Sorted& b) {
-        return (a.s.position.y < b.s.position.y) || (a.s.position.y == b.s.position.y && a.s.position.x < b.s.position.x);
-    };
-    auto byXY = [](const Sorted& a, const Sorted& b) {
-        return (a.s.position.x < b.s.position.x) || (a.s.position.x == b.s.position.x && a.s.position.y < b.s.position.y);
-    };
-    const size_t n = v.size();
-    std::sort(v.begin(), v.end(), byYX);
-    for (size_t row = 0; row < yStrata; ++row) {
-        const size_t lo = row * kBlockSize * xStrata, hi = std::min((row + 1) * kBlockSize * xStrata, n);
-        if (lo < hi) std::sort(v.begin() + lo, v.begin() + hi, byXY);
-    }
-    for (size_t b = 0; b < k; ++b) {
-        const size_t lo = b * kBlockSize, hi = std::min((b + 1) * kBlockSize, n);
-        if (lo < hi) std::sort(v.begin() + lo, v.begin() + hi, byYX);
-    }
-    const size_t run = kTileSize * blockXStrata;
-    for (size_t lo = 0; lo < n; lo += run) std::sort(v.begin() + lo, v.begin() + std::min(lo + run, n), byXY);
+    naiveCluster(v, k, [](const Sorted& a) { return a.s.position.x; }, [](const Sorted& a) { return a.s.position.y; });
 }
 
 // sphericalUVToDirection (libraries/hvvr/raycaster/sample_hierarchy.cpp:27-35)

@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "foveated.h"
 #include "host_objects.h"
 
 using namespace hvb;
@@ -1532,6 +1533,36 @@ int hvvr_scene_read_triangles(hvvr_raycaster* rc, float* tris9) {
     std::vector<float4> t(size_t(rc->scene.triCount) * 3);
     CUDA_TRY(cudaMemcpy(t.data(), rc->scene.tris, t.size() * sizeof(float4), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < rc->scene.triCount; i++) memcpy(tris9 + 9 * i, &t[3 * i], 9 * 4);
+    return HVVR_OK;
+}
+
+int hvvr_polar_foveated_layout(const hvvr_spec* spec, uint32_t* samples_per_ring, uint32_t* ring_count,
+                               uint32_t* valid, uint32_t* padded) {
+    hvvr_spec d;
+    hvvr_spec_default(&d);
+    const hvvr_spec& s = spec ? *spec : d;
+    PolarSetup ps;
+    buildPolarFoveatedSetup(s.foveated_degree_tracking_error, s.foveated_max_fov_degrees, s.foveated_mar_slope,
+                            s.foveated_foveal_mar_degrees, ps);
+    if (samples_per_ring) *samples_per_ring = ps.samplesPerRing;
+    if (ring_count) *ring_count = ps.ringCount;
+    if (valid) *valid = ps.valid;
+    if (padded) *padded = ps.padded;
+    return HVVR_OK;
+}
+
+int hvvr_polar_foveated_samples(const hvvr_spec* spec, float* beams9, uint32_t* remap2, float* tile_rays24,
+                                float* block_rays24) {
+    hvvr_spec d;
+    hvvr_spec_default(&d);
+    const hvvr_spec& s = spec ? *spec : d;
+    PolarSetup ps;
+    buildPolarFoveatedSetup(s.foveated_degree_tracking_error, s.foveated_max_fov_degrees, s.foveated_mar_slope,
+                            s.foveated_foveal_mar_degrees, ps);
+    if (beams9) memcpy(beams9, ps.beams.data(), ps.beams.size() * sizeof(PolarBeam));
+    if (remap2) memcpy(remap2, ps.remap.data(), ps.remap.size() * 4);
+    if (tile_rays24) memcpy(tile_rays24, ps.tileRays.data(), ps.tileRays.size() * sizeof(Rays4));
+    if (block_rays24) memcpy(block_rays24, ps.blockRays.data(), ps.blockRays.size() * sizeof(Rays4));
     return HVVR_OK;
 }
 

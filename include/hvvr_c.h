@@ -254,6 +254,17 @@ int hvvr_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr
                            uint32_t* node_count);
 /* getGridSamples(width, height) (libraries/hvvr/raycaster/samples.cpp:21-42) */
 int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
+/* The polar foveated sample set of spec's foveated parameters (spec NULL: defaults), as the
+ * reference's polarSpaceFoveatedSetup builds it: getEyeSpacePolarFoveatedSamples
+ * (libraries/hvvr/raycaster/samples.cpp:44-142), generateRemapForFoveatedSamples
+ * (libraries/hvvr/raycaster/foveated.cpp:19-45) and ComputeEyeSpaceFrusta (frusta.cu:26-118).
+ * Host only. Layout first; then beams9[valid*9] eye-space {centerRay, du, dv} in clustered
+ * order, remap2[padded*2] polar texel (azimuth, ring) per sample (~0 for padding), and the
+ * eye-space tile/block frusta as {origin[4][3], dir[4][3]} (origin at infinity: no samples). */
+int hvvr_polar_foveated_layout(const hvvr_spec* spec, uint32_t* samples_per_ring, uint32_t* ring_count,
+                               uint32_t* valid, uint32_t* padded);
+int hvvr_polar_foveated_samples(const hvvr_spec* spec, float* beams9, uint32_t* remap2, float* tile_rays24,
+                                float* block_rays24);
 
 /* ---------------------------------------------------------------- batched frames
  * No counterpart in the reference, whose render() walks the cameras of one scene one at a

@@ -160,6 +160,26 @@ class Reference:
     def render(self, *a, **k):
         return _run(self.lib.ref_render, *a, **k)
 
+    def polar_foveated(self, degree_tracking_error=0.5, max_fov_degrees=110.0, mar_slope=0.022,
+                       foveal_mar_degrees=1.0 / 60.0):
+        """The reference's polar foveated sample set: dict of samples_per_ring, ring_count, valid,
+        padded, beams [valid, 9], remap [valid, 2], tile_rays / block_rays [n, 24]."""
+        f = self.lib.ref_polar_foveated
+        f.argtypes = [C.c_float] * 4 + [C.c_void_p] * 5
+        f.restype = C.c_int
+        args = [C.c_float(degree_tracking_error), C.c_float(max_fov_degrees), C.c_float(mar_slope),
+                C.c_float(foveal_mar_degrees)]
+        counts = np.zeros(4, dtype=np.uint32)
+        f(*args, counts.ctypes.data, None, None, None, None)
+        spr, rings, valid, padded = (int(v) for v in counts)
+        out = {"samples_per_ring": spr, "ring_count": rings, "valid": valid, "padded": padded,
+               "beams": np.zeros((valid, 9), np.float32), "remap": np.zeros((valid, 2), np.uint32),
+               "tile_rays": np.zeros((padded // 128, 24), np.float32),
+               "block_rays": np.zeros((padded // 8192, 24), np.float32)}
+        f(*args, counts.ctypes.data, out["beams"].ctypes.data, out["remap"].ctypes.data,
+          out["tile_rays"].ctypes.data, out["block_rays"].ctypes.data)
+        return out
+
     def generate_topology(self, scene):
         """GenerateTopology on copies of the scene arrays; returns (verts, tri_shade, nodes)."""
         verts = scene.verts.copy()

@@ -68,4 +68,9 @@ static inline int __popc(unsigned x) { return __builtin_popcount(x); }
 static inline int __clz(int x) { return x ? __builtin_clz((unsigned)x) : 32; }
 static inline int __ffs(int x) { return __builtin_ffs(x); }
 static inline float rsqrtf(float x) { return 1.0f / sqrtf(x); }
+// warp intrinsics parsed in host compiles of .cu files (the harness never runs these paths)
+static inline unsigned __activemask() { return 0xffffffffu; }
+static inline unsigned __ballot_sync(unsigned, int p) { return p ? 1u : 0u; }
+template <class T> static inline T __shfl_sync(unsigned, T v, int, int = 32) { return v; }
+template <class T> static inline T __shfl_xor_sync(unsigned, T v, int, int = 32) { return v; }
 template <class T> static inline T tex2DGrad(cudaTextureObject_t, float, float, float2, float2) { return T(); }

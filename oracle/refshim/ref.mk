@@ -11,10 +11,12 @@ REF_FLAGS = -std=c++17 -O2 -fPIC -mavx2 -mfma -mf16c -mbmi -mbmi2 -ffp-contract=
             -include refshim/compat/hvvr_gcc_compat.h -Irefshim/compat -I$(SH) -I$(RC) -I$(CUDA_INC)
 REF_SRCS = $(RC)/traverse_avx.cpp $(RC)/sample_hierarchy.cpp $(RC)/samples.cpp $(RC)/camera.cpp \
            $(RC)/foveated.cpp $(SH)/bvh.cpp $(SH)/debug.cpp
-OBJS = $(patsubst %.cpp,_ref/obj/%.o,$(notdir $(REF_SRCS))) _ref/obj/ref_harness.o _ref/obj/ref_stubs.o
+OBJS = $(patsubst %.cpp,_ref/obj/%.o,$(notdir $(REF_SRCS))) _ref/obj/frusta.o _ref/obj/ref_harness.o _ref/obj/ref_stubs.o
 
+# -Bsymbolic: the host stand-ins for the CUDA runtime calls (ref_stubs.cpp) must bind inside this
+# library even when a real libcudart is already loaded into the process
 _ref/libhvvr_ref.so: $(OBJS)
-	$(CXX) -shared -pthread -o $@ $(OBJS)
+	$(CXX) -shared -pthread -Wl,-Bsymbolic -o $@ $(OBJS)
 
 _ref/obj/%.o: $(RC)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
 	@mkdir -p _ref/obj
@@ -22,6 +24,10 @@ _ref/obj/%.o: $(RC)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
 _ref/obj/%.o: $(SH)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
 	@mkdir -p _ref/obj
 	$(CXX) $(REF_FLAGS) -c $< -o $@
+# frusta.cu holds host code only on the path used (ComputeEyeSpaceFrusta); compiled as C++
+_ref/obj/frusta.o: $(RC)/frusta.cu refshim/compat/hvvr_gcc_compat.h
+	@mkdir -p _ref/obj
+	$(CXX) $(REF_FLAGS) -x c++ -c $< -o $@
 _ref/obj/ref_harness.o: refshim/ref_harness.cpp hvvr_oracle.h ../include/hvvr_c.h refshim/compat/hvvr_gcc_compat.h
 	@mkdir -p _ref/obj
 	$(CXX) $(REF_FLAGS) -c $< -o $@

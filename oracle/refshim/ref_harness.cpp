@@ -33,6 +33,8 @@
 #include "shading.h"
 #include "sort.h"
 #include "tile_data.h"
+#include "foveated.h"
+#include "gpu_buffer.h"
 
 #include "../hvvr_oracle.h"
 
@@ -474,6 +476,49 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                 int32_t o = sd.imageLocationToSampleIndex[size_t(y) * in->width + x];
                 if (o >= 0 && in->split_color_samples == 1) out->image[size_t(y) * in->width + x] = colors[o];
             }
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ foveated sample set
+// polarSpaceFoveatedSetup's sample-set part (libraries/hvvr/raycaster/foveated.cpp:47-110):
+// the reference's generateEyeSpacePolarFoveatedSampleData and ComputeEyeSpaceFrusta, run here
+// on the host (GPUBuffer over host memory, see ref_stubs.cpp). Counts first (null outputs).
+namespace hvvr {
+void ComputeEyeSpaceFrusta(const GPUBuffer<DirectionalBeam>& dirSamples, GPUBuffer<SimpleRayFrustum>& tileFrusta,
+                           GPUBuffer<SimpleRayFrustum>& blockFrusta);
+}
+extern "C" int ref_polar_foveated(float degreeTrackingError, float maxFOVDegrees, float marSlope,
+                                  float fovealMARDegrees, uint32_t* counts4, float* beams9, uint32_t* remap2,
+                                  float* tileRays24, float* blockRays24) {
+    MxcsrScope mx;
+    FoveatedSampleData fsd;
+    std::vector<vector2ui> polarRemapToPixel;
+    EccentricityMap emap;
+    size_t samplesPerRing = 0;
+    RayCasterSpecification::FoveatedSamplePattern pattern;
+    pattern.degreeTrackingError = degreeTrackingError;
+    pattern.maxFOVDegrees = maxFOVDegrees;
+    pattern.marSlope = marSlope;
+    pattern.fovealMARDegrees = fovealMARDegrees;
+    generateEyeSpacePolarFoveatedSampleData(fsd, polarRemapToPixel, emap, samplesPerRing, pattern);
+    const DynamicArray<DirectionalBeam>& beams = fsd.samples.directionalBeams;
+    const uint32_t valid = uint32_t(beams.size());
+    const uint32_t blocks = uint32_t(fsd.blockCount);
+    if (counts4) {
+        counts4[0] = uint32_t(samplesPerRing);
+        counts4[1] = uint32_t(valid / samplesPerRing);
+        counts4[2] = valid;
+        counts4[3] = blocks * BLOCK_SIZE;
+    }
+    if (beams9) memcpy(beams9, beams.data(), size_t(valid) * sizeof(DirectionalBeam));
+    if (remap2) memcpy(remap2, polarRemapToPixel.data(), size_t(valid) * sizeof(vector2ui));
+    if (tileRays24 || blockRays24) {
+        GPUBuffer<DirectionalBeam> d(beams.data(), beams.data() + valid);
+        GPUBuffer<SimpleRayFrustum> t(size_t(blocks) * TILES_PER_BLOCK), b(blocks);
+        ComputeEyeSpaceFrusta(d, t, b);
+        if (tileRays24) t.readback((SimpleRayFrustum*)tileRays24);
+        if (blockRays24) b.readback((SimpleRayFrustum*)blockRays24);
     }
     return 0;
 }

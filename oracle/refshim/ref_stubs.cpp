@@ -18,3 +18,22 @@ void GPUCamera::registerPolarFoveatedSamples(const std::vector<vector2ui>&, floa
                                              uint32_t) { hvvr_ref_stub_hits++; }
 void GPUCamera::updateEyeSpaceFoveatedSamples(BeamBatch&) { hvvr_ref_stub_hits++; }
 } // namespace hvvr
+
+// Host-memory stand-ins for the four CUDA runtime calls that GPUBuffer (gpu_buffer.h) makes in
+// the host code of frusta.cu (ComputeEyeSpaceFrusta moves its samples and frusta through
+// GPUBuffers). The harness has no GPU; "device" memory is host memory here.
+extern "C" {
+cudaError_t cudaMalloc(void** p, size_t bytes) {
+    *p = malloc(bytes ? bytes : 1);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaFree(void* p) {
+    free(p);
+    return cudaSuccess;
+}
+cudaError_t cudaMemcpy(void* dst, const void* src, size_t bytes, enum cudaMemcpyKind) {
+    if (bytes) memmove(dst, src, bytes);
+    return cudaSuccess;
+}
+const char* cudaGetErrorString(cudaError_t) { return "host stand-in"; }
+}

@@ -61,8 +61,31 @@ def make(name, ref):
           "hit subsamples", int((f.hit_ids != 0xFFFFFFFF).sum()))
 
 
+POLAR_CASES = {
+    # name: (degree tracking error, max FOV degrees, MAR slope, foveal MAR degrees)
+    "polar_setup_small": (1.0, 12.0, 0.03, 0.06),
+}
+
+
+def make_polar(name, ref):
+    """The reference's polar foveated sample set (getEyeSpacePolarFoveatedSamples,
+    generateRemapForFoveatedSamples, ComputeEyeSpaceFrusta) for one parameter set."""
+    dte, fov, slope, mar = POLAR_CASES[name]
+    r = ref.polar_foveated(dte, fov, slope, mar)
+    np.savez_compressed(
+        os.path.join(ROOT, "tests", "golden", name + ".npz"),
+        params=np.array([dte, fov, slope, mar], dtype=np.float32),
+        counts=np.array([r["samples_per_ring"], r["ring_count"], r["valid"], r["padded"]], dtype=np.uint32),
+        beams_bits=r["beams"].view(np.uint32), remap=r["remap"], tile_rays_bits=r["tile_rays"].view(np.uint32),
+        block_rays_bits=r["block_rays"].view(np.uint32))
+    print(name, "samples", r["valid"], "rings", r["ring_count"], "per ring", r["samples_per_ring"])
+
+
 if __name__ == "__main__":
     # optional case names on the command line regenerate only those fixtures
     ref = pyoracle.Reference()
-    for n in (sys.argv[1:] or CASES):
-        make(n, ref)
+    for n in (sys.argv[1:] or list(CASES) + list(POLAR_CASES)):
+        if n in POLAR_CASES:
+            make_polar(n, ref)
+        else:
+            make(n, ref)

@@ -11,7 +11,9 @@ GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    """The render fixtures (the polar_* fixtures hold sample sets only)."""
+    return sorted(n for n in (os.path.splitext(os.path.basename(p))[0]
+                              for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))) if not n.startswith("polar_"))
 
 
 def load(name):
