@@ -108,6 +108,7 @@ _sig("hvvr_server_update_vertices", _vp, _vp, _u32, _u32, _vp)
 _sig("hvvr_server_get_stats", _vp, _p(_abi.ServerStats))
 _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
+_sig("hvvr_camera_read_foveated_frame", _vp, _vp, _vp, _vp)
 
 EXPORTED = [
     "hvvr_last_error", "hvvr_version", "hvvr_spec_default", "hvvr_raycaster_create", "hvvr_raycaster_destroy",
@@ -128,6 +129,7 @@ EXPORTED = [
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
+    "hvvr_camera_read_foveated_frame",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
     "hvvr_server_submit", "hvvr_server_prewarm", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
 ]
@@ -257,6 +259,10 @@ class Camera:
     def set_capture(self, flags):
         _check(_lib.hvvr_camera_set_capture(self.handle, flags))
 
+    def set_eye_dir(self, d):
+        """gaze direction in camera space (Camera::setEyeDir); used by the foveated polar mode"""
+        _check(_lib.hvvr_camera_set_eye_dir(self.handle, C.byref(_abi.Vec3(*[float(x) for x in d]))))
+
     def set_lens(self, radius, focal_distance):
         _check(_lib.hvvr_camera_set_lens(self.handle, C.byref(_abi.ThinLens(radius, focal_distance))))
 
@@ -324,6 +330,14 @@ class Camera:
         _check(_lib.hvvr_camera_read_timings(self.handle, t.ctypes.data))
         return t
 
+    def foveated_frame(self):
+        """foveated polar mode: (eye_to_world [16], cull planes [4, 4], view depth [padded])"""
+        m = np.zeros(16, np.float32)
+        p = np.zeros((4, 4), np.float32)
+        d = np.zeros(self.layout()[2], np.float32)
+        _check(_lib.hvvr_camera_read_foveated_frame(self.handle, m.ctypes.data, p.ctypes.data, d.ctypes.data))
+        return m, p, d
+
     def tile_costs(self):
         """BVH nodes visited per tile by the last frame's tile cull"""
         n = self.layout()[1]
@@ -340,12 +354,14 @@ class Camera:
 class Raycaster:
     """Raycaster(const RayCasterSpecification&) (libraries/hvvr/raycaster/raycaster.h:44)."""
 
-    def __init__(self, fp_mode=HVVR_FP_FMA, tri_index_capacity=0, device=0):
-        spec = _abi.Spec()
-        _lib.hvvr_spec_default(C.byref(spec))
-        spec.fp_mode = fp_mode
-        spec.tri_index_capacity = tri_index_capacity
-        spec.device = device
+    def __init__(self, fp_mode=HVVR_FP_FMA, tri_index_capacity=0, device=0, spec=None):
+        """spec: a full hvvr_spec (e.g. foveated_spec(...)); otherwise the defaults with these fields"""
+        if spec is None:
+            spec = _abi.Spec()
+            _lib.hvvr_spec_default(C.byref(spec))
+            spec.fp_mode = fp_mode
+            spec.tri_index_capacity = tri_index_capacity
+            spec.device = device
         h = _vp()
         _check(_lib.hvvr_raycaster_create(C.byref(spec), C.byref(h)))
         self.handle = h

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/hvvr_c.h"
+#include "foveated.h"
 #include "host_setup.h"
 #include "hvvr_internal.h"
 
@@ -125,6 +126,14 @@ struct hvvr_camera {
     DevBuf<float> depth;
     DevBuf<float2> lensPos;           // thin-lens table of rate lensRate
     uint32_t lensRate = 0;
+    // foveated polar mode: the polar sample set replaces the camera's own samples for traversal
+    // and shading; the camera's samples give the screen bounds and the output image
+    bool foveated = false;
+    hvvr_float_rect sampleBounds{};
+    DevBuf<uint2> polarRemap;         // [padded] polar texel of each sample
+    DevBuf<float> tmax;               // [padded] view depth of subsample 0
+    float eyeToWorld[16] = {};        // the last frame's batch-to-world matrix and cull planes
+    float cullPlanes[4][4] = {};
     void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
 };
 
@@ -188,6 +197,7 @@ struct hvvr_raycaster {
     std::vector<Node> hostNodes;
     uint32_t refitStatus = 0;
     std::unique_ptr<hvvr_batch> own;      // renders this raycaster's cameras
+    std::unique_ptr<PolarSetup> polar;    // foveated polar mode: the sample set of spec's pattern
     std::vector<hvvr_batch*> batches;     // user batches that include this raycaster
 };
 

@@ -144,6 +144,11 @@ struct ViewDev {
     float lensRadius, focalDistance;
     const float2* lensPos;           // [4 tiles][msaa][128] lens positions (the reference's lookup table)
     uint32_t* occRank;               // [tiles] rank of each tile among the view's non-empty tiles
+    // foveated views: world-space cull planes {normal, dist} for the tile frusta, and the
+    // per-sample view depth of subsample 0 (the reference's TMaxBuffer)
+    float cull[4][4];
+    uint32_t hasCull;
+    float* tmaxOut;
 };
 
 // frame-wide device state shared by the launches of one batch

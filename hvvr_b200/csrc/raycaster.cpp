@@ -240,8 +240,11 @@ int uploadTransforms(hvvr_raycaster* rc, cudaStream_t st) {
 
 std::atomic<uint64_t> gSetupGen{0};
 
+int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st);
+
 int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     if (cam->samples.empty()) return fail(HVVR_ERR_STATE, "camera has no samples");
+    if (cam->rc->spec.mode == HVVR_MODE_FOVEATED_POLAR) return setupFoveatedCamera(cam, st);
     const uint32_t w = cam->target.width, h = cam->target.height;
     buildSampleSetup(cam->samples.data(), uint32_t(cam->samples.size()), cam->split, cam->viewport, cam->lens,
                      cam->fovX, cam->fovY, w, h, cam->setup);
@@ -282,6 +285,73 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
         d.image = static_cast<uint32_t*>(cam->target.data);
         d.imageStride = cam->target.stride ? cam->target.stride : w;
     }
+    cam->setupDirty = false;
+    cam->setupGen = ++gSetupGen;
+    cam->costFrames = 0;
+    return HVVR_OK;
+}
+
+// A camera of a foveated-polar raycaster (renderFoveatedPolarSpaceCudaReconstruct,
+// libraries/hvvr/raycaster/render.cpp:454-492): traversal and shading run on the raycaster's
+// polar sample set in eye space; the camera's own samples only bound the screen (sampleBounds,
+// libraries/hvvr/raycaster/camera.cpp:36-42) for the tile cull planes.
+int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st) {
+    hvvr_raycaster* rc = cam->rc;
+    if (!rc->polar) {
+        rc->polar = std::make_unique<PolarSetup>();
+        buildPolarFoveatedSetup(rc->spec.foveated_degree_tracking_error, rc->spec.foveated_max_fov_degrees,
+                                rc->spec.foveated_mar_slope, rc->spec.foveated_foveal_mar_degrees, *rc->polar);
+    }
+    const PolarSetup& ps = *rc->polar;
+    hvvr_float_rect b{{1.0f, 1.0f}, {0.0f, 0.0f}};
+    for (const hvvr_sample& smp : cam->samples) {
+        b.lower.x = std::min(b.lower.x, smp.position.x);
+        b.lower.y = std::min(b.lower.y, smp.position.y);
+        b.upper.x = std::max(b.upper.x, smp.position.x);
+        b.upper.y = std::max(b.upper.y, smp.position.y);
+    }
+    cam->sampleBounds = b;
+    std::vector<float4> beams(size_t(ps.padded) * 3, make_float4(0, 0, 0, 0));
+    for (size_t i = 0; i < ps.beams.size(); i++) {
+        const PolarBeam& pb = ps.beams[i];
+        beams[3 * i + 0] = make_float4(pb.c[0], pb.c[1], pb.c[2], pb.du[0]);
+        beams[3 * i + 1] = make_float4(pb.du[1], pb.du[2], pb.dv[0], pb.dv[1]);
+        beams[3 * i + 2] = make_float4(pb.dv[2], 0.0f, 0.0f, 0.0f);
+    }
+    TRY(cam->tileRays.upload(ps.tileRays.data(), ps.tileRays.size(), st));
+    TRY(cam->blockRays.upload(ps.blockRays.data(), ps.blockRays.size(), st));
+    TRY(cam->beams.upload(beams.data(), beams.size(), st));
+    TRY(cam->polarRemap.upload(ps.remap.data(), ps.padded, st));
+    CUDA_TRY(cudaStreamSynchronize(st)); // host staging goes out of scope
+    TRY(cam->blockStacks.alloc(size_t(ps.blocks) * kBlockStack));
+    TRY(cam->blockSizes.alloc(ps.blocks));
+    TRY(cam->tileLists.alloc(ps.tiles));
+    TRY(cam->colors.alloc(ps.padded));
+    TRY(cam->tmax.alloc(ps.padded));
+    TRY(cam->tileCost.alloc(ps.tiles));
+    CUDA_TRY(cudaMemsetAsync(cam->tileCost.p, 0, size_t(ps.tiles) * 4, st));
+    CameraDev& d = cam->dev;
+    d = CameraDev{};
+    d.blocks = ps.blocks;
+    d.tiles = ps.tiles;
+    d.padded = ps.padded;
+    d.valid = ps.valid;
+    d.tileRays = cam->tileRays.p;
+    d.blockRays = cam->blockRays.p;
+    d.beams = cam->beams.p;
+    d.blockStacks = cam->blockStacks.p;
+    d.blockSizes = cam->blockSizes.p;
+    d.tileLists = cam->tileLists.p;
+    d.tileCost = cam->tileCost.p;
+    d.colors = cam->colors.p;
+    d.width = cam->target.width;
+    d.height = cam->target.height;
+    cam->setup = SampleSetup{};
+    cam->setup.blocks = ps.blocks;
+    cam->setup.tiles = ps.tiles;
+    cam->setup.padded = ps.padded;
+    cam->setup.valid = ps.valid;
+    cam->foveated = true;
     cam->setupDirty = false;
     cam->setupGen = ++gSetupGen;
     cam->costFrames = 0;
@@ -561,7 +631,7 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
     for (const auto& v : b->views) {
         const hvvr_camera* c = v.cam;
         const CameraDev& d = c->dev;
-        if (c->target.memory_type == HVVR_MEMORY_CPU && c->target.data && d.width && d.height) {
+        if (c->target.memory_type == HVVR_MEMORY_CPU && c->target.data && d.image && d.width && d.height) {
             const uint64_t stride = c->target.stride ? c->target.stride : d.width;
             CUDA_TRY(cudaMemcpy2DAsync(c->target.data, stride * 4, d.image, size_t(d.width) * 4, size_t(d.width) * 4,
                                        d.height, cudaMemcpyDeviceToHost, st));
@@ -734,6 +804,16 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
         v.focalDistance = c->lens.focal_distance;
         v.lensPos = hasLens(c) ? c->lensPos.p : nullptr;
         v.occRank = hasLens(c) ? c->occRank.p : nullptr;
+        if (c->foveated) {
+            hvvr_camera* cm = b->views[i].cam;
+            float c2w[16];
+            memcpy(c2w, &v.M, sizeof(c2w));
+            foveatedFrame(c2w, c->eyeDir, c->sampleBounds, c->viewport, cm->eyeToWorld, cm->cullPlanes);
+            memcpy(&v.M, cm->eyeToWorld, sizeof(v.M));
+            memcpy(v.cull, cm->cullPlanes, sizeof(v.cull));
+            v.hasCull = 1;
+            v.tmaxOut = c->tmax.p;
+        }
         hv[i] = v;
     }
     CUDA_TRY(cudaMemcpyAsync(b->viewsDev.p, hv, b->views.size() * sizeof(ViewDev), cudaMemcpyHostToDevice, st));
@@ -821,8 +901,8 @@ int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out) {
     if (spec) s = *spec;
     else hvvr_spec_default(&s);
     if (s.output_to_3d_api) return fail(HVVR_ERR_INVALID, "output to a 3D API is not available: no graphics stack");
-    if (s.mode != HVVR_MODE_DEFERRED_MSAA_RESOLVE)
-        return fail(HVVR_ERR_INVALID, "only the deferred MSAA resolve mode is built");
+    if (s.mode != HVVR_MODE_DEFERRED_MSAA_RESOLVE && s.mode != HVVR_MODE_FOVEATED_POLAR)
+        return fail(HVVR_ERR_INVALID, "unknown mode");
     if (s.fp_mode != HVVR_FP_FMA && s.fp_mode != HVVR_FP_STRICT) return fail(HVVR_ERR_INVALID, "bad fp_mode");
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -1341,7 +1421,17 @@ int hvvr_camera_set_capture(hvvr_camera* cam, uint32_t flags) {
 int hvvr_camera_get_layout(const hvvr_camera* cam, uint32_t* block_count, uint32_t* tile_count,
                            uint32_t* padded_sample_count, uint32_t* msaa_rate) {
     CAM_CHECK(cam);
-    const uint32_t n = uint32_t(cam->samples.size());
+    uint32_t n = uint32_t(cam->samples.size());
+    hvvr_raycaster* rc = cam->rc;
+    if (rc->spec.mode == HVVR_MODE_FOVEATED_POLAR) {
+        // the raycaster's polar sample set replaces the camera's samples
+        if (!rc->polar) {
+            rc->polar = std::make_unique<PolarSetup>();
+            buildPolarFoveatedSetup(rc->spec.foveated_degree_tracking_error, rc->spec.foveated_max_fov_degrees,
+                                    rc->spec.foveated_mar_slope, rc->spec.foveated_foveal_mar_degrees, *rc->polar);
+        }
+        n = rc->polar->valid;
+    }
     const uint32_t blocks = (n + kBlockSize - 1) / kBlockSize;
     if (block_count) *block_count = blocks;
     if (tile_count) *tile_count = blocks * kTilesPerBlock;
@@ -1480,6 +1570,12 @@ int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9) {
     CAM_CHECK(cam);
     if (cam->setupDirty) return fail(HVVR_ERR_STATE, "sample setup not built yet (render once first)");
     if (!beams9) return fail(HVVR_ERR_INVALID, "NULL output");
+    if (cam->foveated) {
+        const PolarSetup& ps = *cam->rc->polar;
+        memset(beams9, 0, size_t(ps.padded) * 9 * 4);
+        memcpy(beams9, ps.beams.data(), ps.beams.size() * sizeof(PolarBeam));
+        return HVVR_OK;
+    }
     for (size_t i = 0; i < cam->setup.padded; i++) memcpy(beams9 + 9 * i, &cam->setup.beams[12 * i], 9 * 4);
     return HVVR_OK;
 }
@@ -1502,6 +1598,16 @@ int hvvr_camera_read_tile_costs(const hvvr_camera* cam, uint32_t* visits) {
     TRY(requireRendered(cam));
     if (!visits) return fail(HVVR_ERR_INVALID, "NULL output");
     CUDA_TRY(cudaMemcpy(visits, cam->dev.tileCost, size_t(cam->dev.tiles) * 4, cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_foveated_frame(const hvvr_camera* cam, float* eye_to_world16, float* cull_planes16,
+                                    float* view_depth) {
+    TRY(requireRendered(cam));
+    if (!cam->foveated) return fail(HVVR_ERR_STATE, "not a foveated camera");
+    if (eye_to_world16) memcpy(eye_to_world16, cam->eyeToWorld, 16 * 4);
+    if (cull_planes16) memcpy(cull_planes16, cam->cullPlanes, 16 * 4);
+    if (view_depth) CUDA_TRY(cudaMemcpy(view_depth, cam->tmax.p, size_t(cam->dev.padded) * 4, cudaMemcpyDeviceToHost));
     return HVVR_OK;
 }
 

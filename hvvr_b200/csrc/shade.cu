@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
     if (L.count == 0) {
         // ClearEmptyKernel (resolve.cu:527-542)
         V.colors[sid] = 0xFF000000u;
+        if (V.tmaxOut) V.tmaxOut[sid] = INFINITY;
         uint32_t* __restrict__ hitOut = V.hitIds;
         float* __restrict__ depthOut = V.depth;
         if (hitOut) {
@@ -448,6 +449,21 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
             hitOut[size_t(sid) * N + i] = hit[i];
             depthOut[size_t(sid) * N + i] = hit[i] == ~0u ? INFINITY : tmax[i];
         }
+    }
+    // ResolveKernel's TMaxBuffer (resolve.cu:386-457): depth along the view axis of subsample 0's
+    // triangle at subsample 0's position
+    if (float* tmaxOut = viewPtr(V.tmaxOut)) {
+        float tv = INFINITY;
+        if (hit[0] != ~0u) {
+            const TriGeom tri = loadTri(viewPtr(V.tris), hit[0]);
+            const TriThread th = threadSetup(tri.e0, tri.e1, camPos - tri.v0, c, du, dv);
+            const float2 a0 = cMsaa[rate][0];
+            const F3 uvw = calcUVW<FMA>(th, a0.x, a0.y);
+            const F3 p = (tri.v0 * uvw.x + (tri.v0 + tri.e0) * uvw.y) + (tri.v0 + tri.e1) * uvw.z;
+            const F3 look = f3(-M.m[2][0], -M.m[2][1], -M.m[2][2]);
+            tv = dot3(p - camPos, look);
+        }
+        tmaxOut[sid] = tv;
     }
 
     // G-buffer grouping (EmitGBuffer): (triangle, mask) pairs in ascending triangle order,
@@ -842,7 +858,7 @@ cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStric
 }
 
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st) {
-    if (!c.image || c.width == 0 || c.height == 0) return cudaSuccess;
+    if (!c.image || !c.remap || c.width == 0 || c.height == 0) return cudaSuccess;
     const dim3 block(16, 8);
     const dim3 grid((c.width + 15) / 16, (c.height + 7) / 8);
     remapKernel<<<grid, block, 0, st>>>(c.colors, c.remap, c.image, c.width, c.height, c.imageStride, c.split);

@@ -142,6 +142,32 @@ __device__ void buildFrustum(const Rays4& cr, const Mat4& M, SmemFrustum& f) {
     __syncwarp();
 }
 
+// blockTransformAndCullTask's cull of a tile frustum (libraries/hvvr/raycaster/render.cpp:270-279,
+// 314-338): culled when all four corner rays, at their origin and 10000 units out, lie beyond
+// one of the planes. Evaluated by every lane on the same world-space rays.
+__device__ bool tileCulled(const Rays4& cr, const Mat4& M, const float (&pl)[4][4]) {
+    F3 o[4], d[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        o[i] = xformPoint(M, f3(cr.o[i][0], cr.o[i][1], cr.o[i][2]));
+        d[i] = xformDir(M, f3(cr.d[i][0], cr.d[i][1], cr.d[i][2]));
+    }
+    bool culled = false;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+        const F3 n = f3(pl[p][0], pl[p][1], pl[p][2]);
+        const float dist = pl[p][3];
+        bool allout = true;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            allout = allout && dot3(n, o[i]) > dist;
+            allout = allout && dot3(n, o[i] + d[i] * 10000.0f) > dist;
+        }
+        culled = culled || allout;
+    }
+    return culled;
+}
+
 __device__ LaneTest loadLaneTest(const SmemFrustum& f) {
     LaneTest t;
     const uint32_t lane = laneId();
@@ -455,6 +481,10 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
     const uint32_t blk = tile / kTilesPerBlock;
     const uint32_t stackSize = V.blockSizes[blk];
     buildFrustum(V.tileRays[tile], V.M, s.f);
+    if (V.hasCull && tileCulled(V.tileRays[tile], V.M, V.cull)) {
+        if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
+        return 0;
+    }
     if (stackSize == 0 || s.f.degenerate) {
         if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
         return 0;

@@ -233,6 +233,11 @@ int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9);
 int hvvr_camera_read_timings(const hvvr_camera* cam, float* ms6);
 /* total triangle-index entries produced by the last frame's tile cull */
 int hvvr_camera_read_list_total(const hvvr_camera* cam, uint64_t* total);
+/* Foveated polar mode (spec.mode = HVVR_MODE_FOVEATED_POLAR): the last frame's eye-to-world
+ * matrix (column-major), the four world-space tile cull planes {normal, dist}, and the view
+ * depth of subsample 0 per polar sample [padded] (the reference's TMaxBuffer). */
+int hvvr_camera_read_foveated_frame(const hvvr_camera* cam, float* eye_to_world16, float* cull_planes16,
+                                    float* view_depth);
 /* BVH nodes visited per tile by the last frame's tile cull [tile_count] (the schedule of the
  * next frame is built from these) */
 int hvvr_camera_read_tile_costs(const hvvr_camera* cam, uint32_t* visits);

@@ -1011,9 +1011,44 @@ extern "C" void oracle_scene_counts(const oracle_frame_in* in, uint32_t* nodes, 
     if (verts) *verts = v;
 }
 
+namespace {
+int renderCore(const oracle_frame_in* in, const SampleSetup& ss, const M4& c2w, const float* cullPlanes,
+               oracle_frame_out* out);
+}
+
 extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     MxcsrScope mx;
     if (!in || !out || in->sample_count == 0) return 1;
+    SampleSetup ss;
+    setupSamples(in, ss);
+    if (out->remap) memcpy(out->remap, ss.remap.data(), ss.remap.size() * sizeof(int32_t));
+    if (out->beams) memcpy(out->beams, ss.beams.data(), ss.beams.size() * sizeof(Beam));
+    if (out->tile_rays) memcpy(out->tile_rays, ss.tileRays.data(), ss.tileRays.size() * sizeof(Rays4));
+    return renderCore(in, ss, transformToMatrix(in->cam_xf), nullptr, out);
+}
+
+extern "C" int oracle_render_beams(const oracle_frame_in* in, const oracle_beams_in* bi, oracle_frame_out* out) {
+    MxcsrScope mx;
+    if (!in || !bi || !out || bi->blocks == 0) return 1;
+    SampleSetup ss;
+    ss.blocks = bi->blocks;
+    ss.tiles = bi->blocks * kTilesPerBlock;
+    ss.padded = bi->blocks * kBlockSize;
+    ss.valid = ss.padded;
+    ss.beams.resize(ss.padded);
+    memcpy(ss.beams.data(), bi->beams, ss.beams.size() * sizeof(Beam));
+    ss.tileRays.resize(ss.tiles);
+    memcpy(ss.tileRays.data(), bi->tile_rays, ss.tileRays.size() * sizeof(Rays4));
+    ss.blockRays.resize(ss.blocks);
+    memcpy(ss.blockRays.data(), bi->block_rays, ss.blockRays.size() * sizeof(Rays4));
+    M4 m;
+    memcpy(&m, bi->batch_to_world, sizeof(M4));
+    return renderCore(in, ss, m, bi->cull_planes, out);
+}
+
+namespace {
+int renderCore(const oracle_frame_in* in, const SampleSetup& ss, const M4& c2w, const float* cullPlanes,
+               oracle_frame_out* out) {
     uint32_t N = in->msaa;
     if (!(N == 1 || N == 2 || N == 4 || N == 8 || N == 16 || N == 32)) return 1;
     bool useFma = in->fp_mode == HVVR_FP_FMA;
@@ -1026,14 +1061,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     if (out->nodes) memcpy(out->nodes, scene.nodes.data(), scene.nodes.size() * sizeof(Node));
     if (out->tris) memcpy(out->tris, scene.tris.data(), scene.tris.size() * sizeof(Tri));
 
-    SampleSetup ss;
-    setupSamples(in, ss);
-    if (out->remap) memcpy(out->remap, ss.remap.data(), ss.remap.size() * sizeof(int32_t));
-    if (out->beams) memcpy(out->beams, ss.beams.data(), ss.beams.size() * sizeof(Beam));
-    if (out->tile_rays) memcpy(out->tile_rays, ss.tileRays.data(), ss.tileRays.size() * sizeof(Rays4));
-
-    // per-frame transform (RC/render.cpp:282-365, RC/traversal.h:38-47); no cull planes on the plain path
-    M4 c2w = transformToMatrix(in->cam_xf);
+    // per-frame transform (RC/render.cpp:282-365, RC/traversal.h:38-47)
     M3 R = m3of(c2w);
     auto xformRays = [&](const Rays4& r) {
         Rays4 w;
@@ -1047,6 +1075,28 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     std::vector<Rays4> tileW(ss.tiles), blockW(ss.blocks);
     for (uint32_t i = 0; i < ss.tiles; i++) tileW[i] = xformRays(ss.tileRays[i]);
     for (uint32_t i = 0; i < ss.blocks; i++) blockW[i] = xformRays(ss.blockRays[i]);
+    // blockTransformAndCullTask: a tile frustum entirely beyond one of the cull planes becomes
+    // degenerate (origin at infinity); planeCullsFrustum (RC/render.cpp:270-279)
+    if (cullPlanes) {
+        for (uint32_t t = 0; t < ss.tiles; t++) {
+            bool culled = false;
+            for (int p = 0; p < 4; p++) {
+                V3 n = mk(cullPlanes[4 * p], cullPlanes[4 * p + 1], cullPlanes[4 * p + 2]);
+                float dist = cullPlanes[4 * p + 3];
+                bool allout = true;
+                for (int i = 0; i < 4; i++) {
+                    allout = allout && dot(n, tileW[t].o[i]) > dist;
+                    allout = allout && dot(n, tileW[t].o[i] + tileW[t].d[i] * 10000.0f) > dist;
+                }
+                culled = culled || allout;
+            }
+            if (culled)
+                for (int i = 0; i < 4; i++) {
+                    tileW[t].o[i] = mk(INFINITY, INFINITY, INFINITY);
+                    tileW[t].d[i] = mk(0.0f, 0.0f, 0.0f);
+                }
+        }
+    }
 
     const Node* nodes = scene.nodes.data();
     std::vector<StackEntry> blockStacks(size_t(ss.blocks) * kBlockStackSize);
@@ -1083,6 +1133,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                            mk(m.specular.x, m.specular.y, m.specular.z), m.glossiness, m.texture_ids_and_shading_model};
     }
     V3 camPos = mk(c2w.m3.x, c2w.m3.y, c2w.m3.z);
+    V3 lookVec = -mk(c2w.m2.x, c2w.m2.y, c2w.m2.z); // cameraLookVector = -vector3(cameraToWorld.m2)
 
     // tiles: traversal of every tile first (the reference's lists are complete before its
     // intersect launch), then intersect + shade (RC/intersect.cu:171-342, RC/resolve.cu:161-458)
@@ -1147,6 +1198,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                         if (out->gb_mask) out->gb_mask[o] = (i == 0) ? (N == 32 ? ~0u : ((1u << N) - 1)) : 0u;
                     }
                     if (out->gb_n) out->gb_n[base + s] = 1;
+                    if (out->tmax) out->tmax[base + s] = INFINITY;
                     colors[base + s] = 0xFF000000u;
                 }
                 continue;
@@ -1231,6 +1283,19 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
                             out->depth64[o] = num / den;
                         }
                     }
+                }
+                // TMaxBuffer (RC/resolve.cu:386-457): view depth of subsample 0's triangle at subsample 0
+                if (out->tmax) {
+                    float tv = INFINITY;
+                    if (hit[0] != ~0u && !dof) {
+                        const Tri& tri = scene.tris[hit[0]];
+                        TriTile tt;
+                        tileSetup(tri, camPos, tt);
+                        V3 uvw = calcUVW(threadSetup(tt, c, du, dv), V2{off[0], off[1]}, useFma);
+                        V3 p = (tri.v0 * uvw.x + (tri.v0 + tri.e0) * uvw.y) + (tri.v0 + tri.e1) * uvw.z;
+                        tv = dot(p - camPos, lookVec);
+                    }
+                    out->tmax[sid] = tv;
                 }
                 // G-buffer compression (EmitGBuffer, RC/intersect.cu:28-89): pairs sorted by tri, misses last
                 uint32_t keys[32];
@@ -1321,7 +1386,7 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     if (out->tile_indices && total > out->tile_capacity) out->status |= 8;
     if (out->colors) memcpy(out->colors, colors.data(), colors.size() * 4);
     // RemapKernel (RC/remap.cu:35-77)
-    if (out->image) {
+    if (out->image && !ss.remap.empty()) {
         uint32_t split = in->split_color_samples;
         for (uint32_t y = 0; y < in->height; y++)
             for (uint32_t x = 0; x < in->width; x++) {
@@ -1342,3 +1407,4 @@ extern "C" int oracle_render(const oracle_frame_in* in, oracle_frame_out* out) {
     }
     return 0;
 }
+} // namespace

@@ -60,7 +60,21 @@ typedef struct {
     float* tris;               /* [tri_count*9] PrecomputedTriangleIntersect */
     float* tile_rays;          /* [tiles*24] camera-space corner rays {origin[4][3], dir[4][3]} */
     uint32_t status;           /* nonzero if a capacity was exceeded */
+    float* tmax;               /* [padded] view depth of subsample 0's hit (TMaxBuffer), +inf on a miss */
 } oracle_frame_out;
+
+/* The foveated path's frame: given batch-space (eye-space) beams and tile/block frusta, the
+ * batch-to-world matrix (column-major 16 floats) and optional world-space cull planes
+ * {normal, dist} x 4 (tiles whose frustum lies beyond one plane are culled). Scene, msaa,
+ * fp_mode, lens and threads come from in; its samples, viewport and image are not used. */
+typedef struct {
+    const float* beams;        /* [padded*9] */
+    const float* tile_rays;    /* [tiles*24] */
+    const float* block_rays;   /* [blocks*24] */
+    uint32_t blocks;
+    const float* batch_to_world; /* 16 floats */
+    const float* cull_planes;  /* 16 floats or NULL */
+} oracle_beams_in;
 
 /* sizes for a given sample count: blocks = ceil(n/8192) */
 void oracle_layout(uint32_t sample_count, uint32_t* blocks, uint32_t* tiles, uint32_t* padded);
@@ -68,6 +82,7 @@ void oracle_layout(uint32_t sample_count, uint32_t* blocks, uint32_t* tiles, uin
 void oracle_scene_counts(const oracle_frame_in* in, uint32_t* nodes, uint32_t* tris, uint32_t* verts);
 /* runs the whole frame; returns 0 on success */
 int oracle_render(const oracle_frame_in* in, oracle_frame_out* out);
+int oracle_render_beams(const oracle_frame_in* in, const oracle_beams_in* beams, oracle_frame_out* out);
 /* MSAA unit offsets for rate n (n*2 floats), the spiral pattern of the reference */
 void oracle_msaa_offsets(uint32_t n, float* out);
 /* depth-of-field lens positions for rate n: [4 tiles][n subsamples][128 samples] x 2 floats */

@@ -32,7 +32,12 @@ class FrameOut(C.Structure):
                 ("hit_ids", C.c_void_p), ("depth", C.c_void_p), ("depth64", C.c_void_p), ("gb_n", C.c_void_p),
                 ("gb_tri", C.c_void_p), ("gb_mask", C.c_void_p), ("colors", C.c_void_p), ("image", C.c_void_p),
                 ("remap", C.c_void_p), ("beams", C.c_void_p), ("nodes", C.c_void_p), ("tris", C.c_void_p),
-                ("tile_rays", C.c_void_p), ("status", C.c_uint32)]
+                ("tile_rays", C.c_void_p), ("status", C.c_uint32), ("tmax", C.c_void_p)]
+
+
+class BeamsIn(C.Structure):
+    _fields_ = [("beams", C.c_void_p), ("tile_rays", C.c_void_p), ("block_rays", C.c_void_p), ("blocks", C.c_uint32),
+                ("batch_to_world", C.c_void_p), ("cull_planes", C.c_void_p)]
 
 
 def layout(sample_count):
@@ -46,10 +51,10 @@ class Frame:
 
 def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi.HVVR_FP_FMA, lens=(0.0, 1.0),
          threads=None, split=1, want=("lists", "hits", "colors", "image", "blocks", "gbuffer", "scene", "beams"),
-         model_xf=None, tile_capacity=None):
+         model_xf=None, tile_capacity=None, beams_in=None):
     if scene.nodes is None:
         raise ValueError("scene has no topology")
-    n = len(samples)
+    n = len(samples) if beams_in is None else len(beams_in["beams"])
     blocks, tiles, padded = layout(n)
     md = _abi.MeshData(_abi.ptr(scene.verts), len(scene.verts), _abi.ptr(scene.tri_shade), len(scene.tri_shade),
                        _abi.ptr(scene.nodes), len(scene.nodes), _abi.ptr(scene.materials), len(scene.materials))
@@ -65,7 +70,7 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
     fin.viewport = viewport
     fin.lens = _abi.ThinLens(*lens)
     fin.cam_xf = cam_xf
-    fin.samples = _abi.ptr(samples)
+    fin.samples = _abi.ptr(samples) if samples is not None else None
     fin.sample_count = n
     fin.split_color_samples = split
     fin.width, fin.height = width, height
@@ -110,7 +115,21 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
     if "scene" in want:
         alloc("nodes", len(scene.nodes), _abi.NODE_DTYPE, "nodes")
         alloc("tris", (len(scene.tri_shade), 9), np.float32, "tris")
-    rc = fn(C.byref(fin), C.byref(out))
+    if "tmax" in want:
+        alloc("tmax", padded, np.float32, "tmax")
+    if beams_in is None:
+        rc = fn(C.byref(fin), C.byref(out))
+    else:
+        arrs = {k: np.ascontiguousarray(beams_in[k], dtype=np.float32)
+                for k in ("beams", "tile_rays", "block_rays", "batch_to_world")}
+        planes = beams_in.get("cull_planes")
+        if planes is not None:
+            arrs["cull_planes"] = np.ascontiguousarray(planes, dtype=np.float32)
+        keep.extend(arrs.values())
+        bi = BeamsIn(arrs["beams"].ctypes.data, arrs["tile_rays"].ctypes.data, arrs["block_rays"].ctypes.data, blocks,
+                     arrs["batch_to_world"].ctypes.data,
+                     arrs["cull_planes"].ctypes.data if planes is not None else None)
+        rc = fn(C.byref(fin), C.byref(bi), C.byref(out))
     if rc != 0:
         raise RuntimeError("render failed: %d" % rc)
     f.status = out.status
@@ -133,6 +152,16 @@ class Oracle:
 
     def render(self, *a, **k):
         return _run(self.lib.oracle_render, *a, **k)
+
+    def render_beams(self, scene, beams_in, msaa, fp_mode=_abi.HVVR_FP_FMA, threads=None,
+                     want=("lists", "hits", "colors", "scene", "tmax")):
+        """The foveated frame on given batch-space beams [padded, 9], tile/block frusta, the
+        batch-to-world matrix (16 floats, column-major) and optional world cull planes (16 floats)."""
+        f = self.lib.oracle_render_beams
+        f.argtypes = [C.POINTER(FrameIn), C.POINTER(BeamsIn), C.POINTER(FrameOut)]
+        f.restype = C.c_int
+        return _run(f, scene, None, _abi.transform(), _abi.FloatRect(), 0, 0, msaa, fp_mode=fp_mode, threads=threads,
+                    want=want, beams_in=beams_in)
 
     def msaa_offsets(self, n):
         o = np.zeros((n, 2), dtype=np.float32)

@@ -1,0 +1,60 @@
+"""Foveated polar mode: the raycaster's polar sample set (pinned against the reference by
+test_foveated_setup.py) rendered in eye space with the per-frame eye transform and tile cull
+planes. Lists, hit IDs and depth must equal the oracle run on the same beams, frusta, matrix
+and planes; colours within 1 LSB; the per-sample view depth (TMaxBuffer) bit-exact."""
+import numpy as np
+import pytest
+
+import hvvr_b200 as hv
+from hvvr_b200 import _abi, scenes
+
+from helpers import list_mismatch, scene
+
+pytestmark = pytest.mark.gpu
+
+PATTERN = (1.0, 35.0, 0.03, 0.06)  # degree tracking error, max FOV, MAR slope, foveal MAR
+
+
+def _foveated_rc(sc, fp_mode=hv.HVVR_FP_FMA):
+    spec = hv.foveated_spec(*PATTERN, mode=_abi.HVVR_MODE_FOVEATED_POLAR, fp_mode=fp_mode)
+    rc = hv.Raycaster(spec=spec)
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    return rc
+
+
+@pytest.mark.parametrize("msaa,fp_mode", [(4, hv.HVVR_FP_FMA), (8, hv.HVVR_FP_STRICT), (1, hv.HVVR_FP_FMA)])
+def test_foveated_eye_space_render_matches_oracle(oracle, msaa, fp_mode):
+    sc = scene("c1")
+    rc = _foveated_rc(sc, fp_mode)
+    w, h = 320, 288
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h)
+    cam.set_samples(scenes.grid_samples(w, h))
+    cam.set_msaa(msaa)
+    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+    polar = hv.polar_foveated_samples(hv.foveated_spec(*PATTERN))
+    beams = np.zeros((polar["padded"], 9), np.float32)
+    beams[: polar["valid"]] = polar["beams"]
+    for eye, target, gaze in [((0.0, 2.0, 10.0), (0.0, 0.0, 0.0), (0.0, 0.0, -1.0)),
+                              ((2.0, 1.5, 8.0), (-1.0, 0.3, 0.0), (0.2, -0.1, -0.97))]:
+        cam.set_camera_to_world(scenes.camera_transform(eye=eye, target=target))
+        cam.set_eye_dir(gaze)
+        rc.render()
+        m, planes, depth = cam.foveated_frame()
+        assert np.isfinite(planes).all()
+        fo = oracle.render_beams(sc, {"beams": beams, "tile_rays": polar["tile_rays"],
+                                      "block_rays": polar["block_rays"], "batch_to_world": m, "cull_planes": planes},
+                                 msaa, fp_mode=fp_mode)
+        counts, idx = cam.tile_lists()
+        assert list_mismatch(counts, idx, fo.tile_counts, fo.tile_indices) == 0
+        assert (counts == 0).sum() > 0, "expected some tiles culled by the screen bounds"
+        ids, d = cam.hits()
+        assert np.array_equal(ids, fo.hit_ids)
+        assert np.array_equal(d.view(np.uint32), fo.depth.view(np.uint32))
+        assert np.array_equal(depth.view(np.uint32), fo.tmax.view(np.uint32))
+        col = cam.sample_colors()
+        dc = np.abs(col.view(np.uint8).astype(np.int32) - fo.colors.view(np.uint8).astype(np.int32))
+        assert dc.max() <= 1
+    rc.close()
