@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--views", type=int, default=64)
     ap.add_argument("--profile", action="store_true",
-                    help="small case for ncu: one eye of the stereo workload, 3 frames, 32M-entry index pool")
+                    help="case for ncu: the stereo frame, 3 frames, 32M-entry index pool")
     return ap.parse_args()
 
 
@@ -682,7 +682,8 @@ def run_served(args):
 
 
 def run_profile_case():
-    """One eye of the benchmark frame, 3 frames, for ncu captures (a few GB on the device)."""
+    """The benchmark's stereo frame (both eyes, one batch), 3 frames, 32M-entry list pool: the
+    case the ncu launch list and captures run on (a few GB on the device)."""
     import hvvr_b200 as hv
     from hvvr_b200 import scenes
     sc = scenes.scene_c2()
@@ -691,16 +692,21 @@ def run_profile_case():
         rc.create_model(sc)
         for l in sc.lights:
             rc.create_light(l)
-        cam = rc.create_camera(scenes.viewport_for(W, H))
-        cam.set_render_target(W, H)
-        cam.set_samples(scenes.barrel_samples(W, H))
-        cam.set_camera_to_world(scenes.stereo_eyes(IPD)[0])
-        cam.set_msaa(MSAA)
+        cams = []
+        for xf in scenes.stereo_eyes(IPD):
+            cam = rc.create_camera(scenes.viewport_for(W, H))
+            cam.set_render_target(W, H)
+            cam.set_samples(scenes.barrel_samples(W, H))
+            cam.set_camera_to_world(xf)
+            cam.set_msaa(MSAA)
+            cams.append(cam)
         for _ in range(3):
             rc.render()
         rc.synchronize()
-        print(json.dumps({"profile_case": "one eye 1080x1200 8xMSAA, 995k tris", "stage_ms": [float(x) for x in cam.timings()],
-                          "kernel_ms": [float(x) for x in rc.kernel_times()], "list_entries": cam.list_total()}))
+        print(json.dumps({"profile_case": "stereo 2x1080x1200 8xMSAA, 995k tris, frame 3",
+                          "stage_ms": [float(x) for x in cams[0].timings()],
+                          "kernel_ms": [float(x) for x in rc.kernel_times()],
+                          "list_entries": sum(c.list_total() for c in cams)}))
 
 
 def ctypes_stream(stream):
