@@ -109,6 +109,9 @@ _sig("hvvr_server_get_stats", _vp, _p(_abi.ServerStats))
 _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
 _sig("hvvr_camera_read_foveated_frame", _vp, _vp, _vp, _vp)
+_sig("hvvr_camera_read_foveated_resolve", _vp, _vp, _vp, _vp, _vp)
+_sig("hvvr_foveated_frame_matrices", _p(_abi.Transform), _p(_abi.Vec3), _p(_abi.FloatRect), _p(_abi.FloatRect),
+     _vp, _vp, _vp, _vp, _vp, _vp)
 
 EXPORTED = [
     "hvvr_last_error", "hvvr_version", "hvvr_spec_default", "hvvr_raycaster_create", "hvvr_raycaster_destroy",
@@ -129,7 +132,7 @@ EXPORTED = [
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
-    "hvvr_camera_read_foveated_frame",
+    "hvvr_camera_read_foveated_frame", "hvvr_camera_read_foveated_resolve", "hvvr_foveated_frame_matrices",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
     "hvvr_server_submit", "hvvr_server_prewarm", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
 ]
@@ -189,6 +192,26 @@ def polar_foveated_samples(spec=None):
     return out
 
 
+def foveated_frame_matrices(xf, eye_dir, sample_bounds, viewport, history=None):
+    """A foveated camera's per-frame matrices on the host (hvvr_foveated_frame_matrices).
+    history: (world_to_eye_prev [16], eye_prev_to_sample_prev [9]) or None for a new camera;
+    returns a dict with eye_to_world, cull_planes, sample_to_eye, eye_to_sample_prev and the
+    next frame's history."""
+    if history is None:
+        w2ep, ep2sp = np.zeros(16, np.float32), np.eye(3, dtype=np.float32).reshape(9)
+    else:
+        w2ep, ep2sp = (np.array(h, np.float32).reshape(n).copy() for h, n in zip(history, (16, 9)))
+    out = {"eye_to_world": np.zeros(16, np.float32), "cull_planes": np.zeros((4, 4), np.float32),
+           "sample_to_eye": np.zeros(9, np.float32), "eye_to_sample_prev": np.zeros(16, np.float32)}
+    ed = _abi.Vec3(*eye_dir)
+    _check(_lib.hvvr_foveated_frame_matrices(C.byref(xf), C.byref(ed), C.byref(sample_bounds), C.byref(viewport),
+                                             w2ep.ctypes.data, ep2sp.ctypes.data, out["eye_to_world"].ctypes.data,
+                                             out["cull_planes"].ctypes.data, out["sample_to_eye"].ctypes.data,
+                                             out["eye_to_sample_prev"].ctypes.data))
+    out["history"] = (w2ep, ep2sp)
+    return out
+
+
 def grid_samples(width, height):
     s = np.zeros(width * height, dtype=_abi.SAMPLE_DTYPE)
     _check(_lib.hvvr_grid_samples(width, height, s.ctypes.data))
@@ -222,6 +245,7 @@ class Camera:
         d = _abi.ImageDesc()
         d.pixel_format = 0
         d.width, d.height, d.stride = width, height, stride
+        self._size = (width, height)
         # the previous image stays alive until the library has released (unregistered) it
         new = None
         if device_ptr is None:
@@ -337,6 +361,16 @@ class Camera:
         d = np.zeros(self.layout()[2], np.float32)
         _check(_lib.hvvr_camera_read_foveated_frame(self.handle, m.ctypes.data, p.ctypes.data, d.ctypes.data))
         return m, p, d
+
+    def foveated_resolve(self):
+        """foveated polar mode: the last frame's resolve - (sample_to_eye [9], eye_to_sample_prev
+        [16], the temporally filtered image it wrote [h, w], the previous result it read [h, w])"""
+        w, h = self._size
+        s2e, e2p = np.zeros(9, np.float32), np.zeros(16, np.float32)
+        res, hist = np.zeros((h, w), np.uint32), np.zeros((h, w), np.uint32)
+        _check(_lib.hvvr_camera_read_foveated_resolve(self.handle, s2e.ctypes.data, e2p.ctypes.data,
+                                                      res.ctypes.data, hist.ctypes.data))
+        return s2e, e2p, res, hist
 
     def tile_costs(self):
         """BVH nodes visited per tile by the last frame's tile cull"""

@@ -7,7 +7,7 @@
 //   getEyeSpacePolarFoveatedSamples      libraries/hvvr/raycaster/samples.cpp:44-142
 //   generateRemapForFoveatedSamples      libraries/hvvr/raycaster/foveated.cpp:19-45
 //   ComputeEyeSpaceFrusta                libraries/hvvr/raycaster/frusta.cu:26-118 (host code)
-//   renderFoveatedPolarSpaceCudaReconstruct / cullRectToCullPlanes
+//   renderFoveatedPolarSpaceCudaReconstruct / cullRectToCullPlanes and the resolve matrices
 //                                        libraries/hvvr/raycaster/render.cpp:396-492
 // with the vector algebra of libraries/hvvr/shared/vector_math.h (quaternion rotation, 3x3 and
 // 4x4 inverses, Plane transform of graphics_types.h:195-200).
@@ -328,6 +328,49 @@ void foveatedFrame(const float cameraToWorld[16], const hvvr_vec3& eyeDir, const
         planes[i][1] = N.y;
         planes[i][2] = N.z;
         planes[i][3] = dot(v3(O.x, O.y, O.z), N);
+    }
+}
+
+void foveatedResolveFrame(const float eyeToWorld[16], const hvvr_vec3& eyeDir, const hvvr_float_rect& viewport,
+                          float worldToEyePrev[16], float eyePrevToSamplePrev[9], float sampleToEye[9],
+                          float eyeToSamplePrev[16]) {
+    FtzDazScope ftz;
+    auto col4 = [&](const float* m, int c) { return V4{m[4 * c + 0], m[4 * c + 1], m[4 * c + 2], m[4 * c + 3]}; };
+    auto col3 = [&](const float* m, int c) { return v3(m[3 * c + 0], m[3 * c + 1], m[3 * c + 2]); };
+    const M4 e2w{col4(eyeToWorld, 0), col4(eyeToWorld, 1), col4(eyeToWorld, 2), col4(eyeToWorld, 3)};
+    const M4 w2ep{col4(worldToEyePrev, 0), col4(worldToEyePrev, 1), col4(worldToEyePrev, 2), col4(worldToEyePrev, 3)};
+    const M3 ep2sp{col3(eyePrevToSamplePrev, 0), col3(eyePrevToSamplePrev, 1), col3(eyePrevToSamplePrev, 2)};
+    // sampleToEye = invert(eyeToCamera) * getSampleToCamera()
+    const M3 e2c = rotationFromZAxis(-v3(eyeDir.x, eyeDir.y, eyeDir.z));
+    const M3 s2c{v3(viewport.upper.x - viewport.lower.x, 0, 0), v3(0, viewport.lower.y - viewport.upper.y, 0),
+                 v3(viewport.lower.x, viewport.upper.y, -1)};
+    const M3 s2e = mul(invert3(e2c), s2c);
+    // eyeToSamplePrevious = matrix4x4(eyePreviousToSamplePrevious) * (worldToEyePrevious * eyeToWorld)
+    const M4 e2ep = mul(w2ep, e2w);
+    const M4 ep2sp4{V4{ep2sp.m0.x, ep2sp.m0.y, ep2sp.m0.z, 0.0f}, V4{ep2sp.m1.x, ep2sp.m1.y, ep2sp.m1.z, 0.0f},
+                    V4{ep2sp.m2.x, ep2sp.m2.y, ep2sp.m2.z, 0.0f}, V4{0.0f, 0.0f, 0.0f, 1.0f}};
+    const M4 e2sp = mul(ep2sp4, e2ep);
+    const V3* c3 = &s2e.m0;
+    for (int c = 0; c < 3; c++) {
+        sampleToEye[3 * c + 0] = c3[c].x; sampleToEye[3 * c + 1] = c3[c].y; sampleToEye[3 * c + 2] = c3[c].z;
+    }
+    const V4* c4 = &e2sp.m0;
+    for (int c = 0; c < 4; c++) {
+        eyeToSamplePrev[4 * c + 0] = c4[c].x; eyeToSamplePrev[4 * c + 1] = c4[c].y;
+        eyeToSamplePrev[4 * c + 2] = c4[c].z; eyeToSamplePrev[4 * c + 3] = c4[c].w;
+    }
+    // the camera's history for the next frame
+    const M4 w2e = invert4(e2w);
+    const V4* h4 = &w2e.m0;
+    for (int c = 0; c < 4; c++) {
+        worldToEyePrev[4 * c + 0] = h4[c].x; worldToEyePrev[4 * c + 1] = h4[c].y;
+        worldToEyePrev[4 * c + 2] = h4[c].z; worldToEyePrev[4 * c + 3] = h4[c].w;
+    }
+    const M3 e2s = invert3(s2e);
+    const V3* h3 = &e2s.m0;
+    for (int c = 0; c < 3; c++) {
+        eyePrevToSamplePrev[3 * c + 0] = h3[c].x; eyePrevToSamplePrev[3 * c + 1] = h3[c].y;
+        eyePrevToSamplePrev[3 * c + 2] = h3[c].z;
     }
 }
 

@@ -33,4 +33,14 @@ void buildPolarFoveatedSetup(float degreeTrackingError, float maxFOVDegrees, flo
 void foveatedFrame(const float cameraToWorld[16], const hvvr_vec3& eyeDir, const hvvr_float_rect& sampleBounds,
                    const hvvr_float_rect& viewport, float eyeToWorld[16], float planes[4][4]);
 
+// the foveated resolve's matrices for a frame (render.cpp:478-486): sampleToEye =
+// invert(eyeToCamera) * sampleToCamera and eyeToSamplePrevious = matrix4x4(eyePrevToSamplePrev)
+// * (worldToEyePrev * eyeToWorld); then the history (worldToEyePrev, eyePrevToSamplePrev)
+// becomes (invert(eyeToWorld), invert(sampleToEye)). A new camera's history is (zero,
+// identity): the zero matrix sends every reprojection to NaN, so the first frame reads no
+// history. Matrices column-major.
+void foveatedResolveFrame(const float eyeToWorld[16], const hvvr_vec3& eyeDir, const hvvr_float_rect& viewport,
+                          float worldToEyePrev[16], float eyePrevToSamplePrev[9], float sampleToEye[9],
+                          float eyeToSamplePrev[16]);
+
 } // namespace hvb

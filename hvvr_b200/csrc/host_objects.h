@@ -134,6 +134,17 @@ struct hvvr_camera {
     DevBuf<float> tmax;               // [padded] view depth of subsample 0
     float eyeToWorld[16] = {};        // the last frame's batch-to-world matrix and cull planes
     float cullPlanes[4][4] = {};
+    // foveated resolve: polar textures, screen planes (fovResult[fovCur] is written by the next
+    // frame, the other one holds the previous frame's result), the temporal history matrices
+    // and the last frame's resolve matrices
+    DevBuf<uint32_t> polarColor, fovResult[2], fovFiltered;
+    DevBuf<float> polarDepth, fovEcc;
+    DevBuf<ushort4> moments;
+    FoveaDev fovStatic{};             // buffers, sizes and mapping constants (no per-frame fields)
+    uint32_t fovCur = 0;
+    float worldToEyePrev[16] = {};
+    float eyePrevToSamplePrev[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    float lastSampleToEye[9] = {}, lastEyeToSamplePrev[16] = {};
     void* registered = nullptr;       // CPU render target page-locked by cudaHostRegister
 };
 
@@ -222,6 +233,8 @@ int ensureMsaaTable(uint32_t rate, cudaStream_t st);
 // a new camera of the same raycaster with cam's sample set and setup (device copies, no
 // re-clustering); cam must have been set up (rendered once)
 int cloneCamera(const hvvr_camera* cam, hvvr_camera** out);
+// forget a foveated camera's temporal history: its next frame reads no previous result
+void resetFoveatedHistory(hvvr_camera* cam);
 // device bytes a camera holds for its setup and per-frame buffers at the given MSAA rate
 size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa);
 

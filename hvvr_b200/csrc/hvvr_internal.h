@@ -117,6 +117,32 @@ struct CameraDev {
     uint64_t imageStride = 0;
 };
 
+// The foveated resolve of one view (polar sample texture -> screen image, with temporal
+// reprojection and eccentricity-dependent contrast enhancement). Buffers in HBM:
+//   polar textures [rings][samplesPerRing]: colour (RGBA8 sRGB), view depth, moments
+//   (first and second, RGBA16 unorm each, interleaved: ushort4 pairs)
+//   screen planes [height][width]: this frame's temporally filtered image and the previous
+//   frame's (RGBA8 sRGB), the vertical filter pass (RGBA8 sRGB), the eccentricity and the five
+//   filter weights pow(1 - |R| / 5.1, sqrt(eccentricity)), R = 1..5, of each pixel
+struct FoveaDev {
+    const uint2* remap;        // [valid] polar texel (azimuth index, ring) of each sample
+    uint32_t* polarColor;      // [rings * spr]
+    float* polarDepth;         // [rings * spr]
+    ushort4* moments;          // [rings * spr * 2]
+    uint32_t* result;          // [h * w] written this frame
+    const uint32_t* history;   // [h * w] the previous frame's result
+    uint32_t* filtered;        // [h * w]
+    float* ecc;                // [6][h * w]: eccentricity, then weights R = 1..5
+    uint32_t* image;           // nullptr: the view has no foveated resolve
+    uint32_t imageStride, width, height;
+    uint32_t spr, rings, valid;
+    // EccentricityMap {m, w_0, S, invLogA, invW_0, invM} and the texture-coordinate mapping
+    float eccM, eccW0, eccS, eccInvLogA, eccInvW0, eccInvM;
+    float texMapSize, invTexMapSize, invMaxEcc;
+    float sampleToEye[9];      // column-major 3x3
+    float eyeToSamplePrev[16]; // column-major 4x4: eye space -> previous frame's sample space
+};
+
 // One view of a frame: a camera and the scene it renders. A frame is a table of views whose
 // blocks and tiles are numbered consecutively ("global" indices); every stage runs one launch
 // over all views, and a kernel finds its view through blockView[global block].
@@ -149,6 +175,7 @@ struct ViewDev {
     float cull[4][4];
     uint32_t hasCull;
     float* tmaxOut;
+    FoveaDev fov;                    // foveated resolve (fov.image == nullptr: none)
 };
 
 // frame-wide device state shared by the launches of one batch
@@ -193,6 +220,12 @@ cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
 cudaError_t launchRefit(const SceneDev& s, cudaStream_t st);
 cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);
+// the foveated resolve of view `view` of the frame (fov: the host copy of its FoveaDev, for
+// the launch shapes): scatter to the polar textures, moments, polar -> screen with temporal
+// reprojection, two eccentricity filter passes and contrast enhancement into fov.image
+cudaError_t launchFoveatedResolve(const FrameDev& fr, uint32_t view, const FoveaDev& fov, cudaStream_t st);
+// sRGB byte -> linear decode table and the 255 linear -> sRGB byte encode thresholds
+cudaError_t uploadColorTables(const float* decode256, const float* thresholds256, cudaStream_t st);
 // writes v to *dst with a one-thread kernel (no host memory involved; capturable)
 cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st);
 

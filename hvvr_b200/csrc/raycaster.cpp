@@ -291,6 +291,31 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     return HVVR_OK;
 }
 
+void resetFoveatedHistory(hvvr_camera* cam) {
+    // a new camera's state (libraries/hvvr/raycaster/camera.h:121-122: _worldToEyePrevious
+    // zero, _eyePreviousToSamplePrevious identity)
+    memset(cam->worldToEyePrev, 0, sizeof(cam->worldToEyePrev));
+    const float id[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    memcpy(cam->eyePrevToSamplePrev, id, sizeof(id));
+}
+
+// the resolve's sRGB tables, once per device
+int ensureColorTables(cudaStream_t st) {
+    static std::mutex mu;
+    static bool uploaded[64] = {};
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(HVVR_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (uploaded[dev]) return HVVR_OK;
+    float dec[256], thr[256];
+    colorTables(dec, thr);
+    CUDA_TRY(uploadColorTables(dec, thr, st));
+    CUDA_TRY(cudaStreamSynchronize(st)); // the host tables go out of scope
+    uploaded[dev] = true;
+    return HVVR_OK;
+}
+
 // A camera of a foveated-polar raycaster (renderFoveatedPolarSpaceCudaReconstruct,
 // libraries/hvvr/raycaster/render.cpp:454-492): traversal and shading run on the raycaster's
 // polar sample set in eye space; the camera's own samples only bound the screen (sampleBounds,
@@ -330,6 +355,52 @@ int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st) {
     TRY(cam->tmax.alloc(ps.padded));
     TRY(cam->tileCost.alloc(ps.tiles));
     CUDA_TRY(cudaMemsetAsync(cam->tileCost.p, 0, size_t(ps.tiles) * 4, st));
+    // the resolve (GPUCamera::registerPolarFoveatedSamples and the image-sized textures,
+    // libraries/hvvr/raycaster/gpu_camera.cu:174-183, 194-230; getEccentricityMap,
+    // gpu_foveated.cu:80-85)
+    const uint32_t w = cam->target.width, h = cam->target.height;
+    const bool cpuTarget = cam->target.memory_type == HVVR_MEMORY_CPU;
+    FoveaDev& fv = cam->fovStatic;
+    fv = FoveaDev{};
+    if (w && h) {
+        TRY(ensureColorTables(st));
+        const size_t texels = size_t(ps.samplesPerRing) * ps.ringCount, npix = size_t(w) * h;
+        TRY(cam->polarColor.alloc(texels));
+        TRY(cam->polarDepth.alloc(texels));
+        TRY(cam->moments.alloc(2 * texels));
+        for (int k = 0; k < 2; k++) {
+            TRY(cam->fovResult[k].alloc(npix));
+            CUDA_TRY(cudaMemsetAsync(cam->fovResult[k].p, 0, npix * 4, st));
+        }
+        TRY(cam->fovFiltered.alloc(npix));
+        TRY(cam->fovEcc.alloc(6 * npix));
+        CUDA_TRY(cudaMemsetAsync(cam->polarColor.p, 0, texels * 4, st));
+        CUDA_TRY(cudaMemsetAsync(cam->polarDepth.p, 0, texels * 4, st));
+        if (cpuTarget) TRY(cam->image.alloc(npix));
+        fv.remap = cam->polarRemap.p;
+        fv.polarColor = cam->polarColor.p;
+        fv.polarDepth = cam->polarDepth.p;
+        fv.moments = cam->moments.p;
+        fv.filtered = cam->fovFiltered.p;
+        fv.ecc = cam->fovEcc.p;
+        fv.image = cpuTarget ? cam->image.p : static_cast<uint32_t*>(cam->target.data);
+        fv.imageStride = cpuTarget ? w : (cam->target.stride ? uint32_t(cam->target.stride) : w);
+        fv.width = w;
+        fv.height = h;
+        fv.spr = ps.samplesPerRing;
+        fv.rings = ps.ringCount;
+        fv.valid = ps.valid;
+        fv.eccM = ps.eccM;
+        fv.eccW0 = ps.eccW0;
+        fv.eccS = ps.eccS;
+        fv.eccInvLogA = ps.eccInvLogA;
+        fv.eccInvW0 = ps.eccInvW0;
+        fv.eccInvM = ps.eccInvM;
+        fv.texMapSize = float(ps.ringCount);
+        fv.invTexMapSize = 1.0f / float(ps.ringCount);
+        fv.invMaxEcc = 1.0f / ps.maxEccentricity;
+    }
+    resetFoveatedHistory(cam);
     CameraDev& d = cam->dev;
     d = CameraDev{};
     d.blocks = ps.blocks;
@@ -344,8 +415,10 @@ int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st) {
     d.tileLists = cam->tileLists.p;
     d.tileCost = cam->tileCost.p;
     d.colors = cam->colors.p;
-    d.width = cam->target.width;
-    d.height = cam->target.height;
+    d.width = w;
+    d.height = h;
+    d.image = fv.image;
+    d.imageStride = fv.imageStride;
     cam->setup = SampleSetup{};
     cam->setup.blocks = ps.blocks;
     cam->setup.tiles = ps.tiles;
@@ -625,7 +698,11 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
         }
     }
     if (timing) CUDA_TRY(cudaEventRecord(b->ev[3], st));
-    for (const auto& v : b->views) CUDA_TRY(launchRemap(v.cam->dev, st));
+    for (uint32_t i = 0; i < b->views.size(); i++) {
+        const hvvr_camera* c = b->views[i].cam;
+        if (c->foveated) CUDA_TRY(launchFoveatedResolve(fr, i, c->fovStatic, st));
+        else CUDA_TRY(launchRemap(c->dev, st));
+    }
     if (timing) CUDA_TRY(cudaEventRecord(b->ev[4], st));
     CUDA_TRY(cudaMemcpyAsync(b->hostCounters, fr.counters, kCounterWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     for (const auto& v : b->views) {
@@ -813,6 +890,18 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
             memcpy(v.cull, cm->cullPlanes, sizeof(v.cull));
             v.hasCull = 1;
             v.tmaxOut = c->tmax.p;
+            if (cm->fovStatic.image) {
+                // resolve into fovResult[fovCur] against the other buffer (the previous frame's
+                // result), then swap (GPUCamera::foveatedPolarToScreenSpace's std::swap)
+                v.fov = cm->fovStatic;
+                foveatedResolveFrame(cm->eyeToWorld, c->eyeDir, c->viewport, cm->worldToEyePrev,
+                                     cm->eyePrevToSamplePrev, v.fov.sampleToEye, v.fov.eyeToSamplePrev);
+                memcpy(cm->lastSampleToEye, v.fov.sampleToEye, sizeof(cm->lastSampleToEye));
+                memcpy(cm->lastEyeToSamplePrev, v.fov.eyeToSamplePrev, sizeof(cm->lastEyeToSamplePrev));
+                v.fov.result = cm->fovResult[cm->fovCur].p;
+                v.fov.history = cm->fovResult[cm->fovCur ^ 1u].p;
+                cm->fovCur ^= 1u;
+            }
         }
         hv[i] = v;
     }
@@ -1608,6 +1697,35 @@ int hvvr_camera_read_foveated_frame(const hvvr_camera* cam, float* eye_to_world1
     if (eye_to_world16) memcpy(eye_to_world16, cam->eyeToWorld, 16 * 4);
     if (cull_planes16) memcpy(cull_planes16, cam->cullPlanes, 16 * 4);
     if (view_depth) CUDA_TRY(cudaMemcpy(view_depth, cam->tmax.p, size_t(cam->dev.padded) * 4, cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
+int hvvr_camera_read_foveated_resolve(const hvvr_camera* cam, float* sample_to_eye9, float* eye_to_sample_prev16,
+                                      uint32_t* result, uint32_t* history) {
+    TRY(requireRendered(cam));
+    if (!cam->foveated || !cam->fovStatic.image) return fail(HVVR_ERR_STATE, "not a foveated camera with a render target");
+    if (sample_to_eye9) memcpy(sample_to_eye9, cam->lastSampleToEye, 9 * 4);
+    if (eye_to_sample_prev16) memcpy(eye_to_sample_prev16, cam->lastEyeToSamplePrev, 16 * 4);
+    const size_t npix = size_t(cam->fovStatic.width) * cam->fovStatic.height;
+    // the last frame wrote fovResult[fovCur ^ 1] and read fovResult[fovCur]
+    if (result) CUDA_TRY(cudaMemcpy(result, cam->fovResult[cam->fovCur ^ 1u].p, npix * 4, cudaMemcpyDeviceToHost));
+    if (history) CUDA_TRY(cudaMemcpy(history, cam->fovResult[cam->fovCur].p, npix * 4, cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
+int hvvr_foveated_frame_matrices(const hvvr_transform* camera_to_world, const hvvr_vec3* eye_dir,
+                                 const hvvr_float_rect* sample_bounds, const hvvr_float_rect* viewport,
+                                 float* world_to_eye_prev16, float* eye_prev_to_sample_prev9, float* eye_to_world16,
+                                 float* cull_planes16, float* sample_to_eye9, float* eye_to_sample_prev16) {
+    if (!camera_to_world || !eye_dir || !sample_bounds || !viewport || !world_to_eye_prev16 ||
+        !eye_prev_to_sample_prev9 || !eye_to_world16 || !cull_planes16 || !sample_to_eye9 || !eye_to_sample_prev16)
+        return fail(HVVR_ERR_INVALID, "null argument");
+    const Mat4 c2w = transformToMatrix(*camera_to_world);
+    float planes[4][4];
+    foveatedFrame(&c2w.m[0][0], *eye_dir, *sample_bounds, *viewport, eye_to_world16, planes);
+    memcpy(cull_planes16, planes, sizeof(planes));
+    foveatedResolveFrame(eye_to_world16, *eye_dir, *viewport, world_to_eye_prev16, eye_prev_to_sample_prev9,
+                         sample_to_eye9, eye_to_sample_prev16);
     return HVVR_OK;
 }
 

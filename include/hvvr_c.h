@@ -238,6 +238,24 @@ int hvvr_camera_read_list_total(const hvvr_camera* cam, uint64_t* total);
  * depth of subsample 0 per polar sample [padded] (the reference's TMaxBuffer). */
 int hvvr_camera_read_foveated_frame(const hvvr_camera* cam, float* eye_to_world16, float* cull_planes16,
                                     float* view_depth);
+/* Foveated polar mode: the last frame's resolve (Raycaster::renderFoveatedPolarSpaceCudaReconstruct,
+ * libraries/hvvr/raycaster/render.cpp:476-486, and GPUCamera::foveatedPolarToScreenSpace,
+ * gpu_foveated.cu:335-375) - its sample-to-eye matrix [9] and eye-to-previous-sample-space
+ * matrix [16] (column-major), the temporally filtered image it wrote (RGBA8 sRGB,
+ * [height * width], the next frame's history) and the previous result it read
+ * ([height * width]). Any pointer may be null. The final image goes to the render target. */
+int hvvr_camera_read_foveated_resolve(const hvvr_camera* cam, float* sample_to_eye9, float* eye_to_sample_prev16,
+                                      uint32_t* result, uint32_t* history);
+/* The per-frame matrices of a foveated camera, on the host (no device work; render.cpp:
+ * 463-486): from the camera-to-world transform, gaze, sample bounds and viewport, the
+ * eye-to-world matrix [16], the four tile cull planes [16], sample-to-eye [9] and
+ * eye-to-previous-sample-space [16]; the history pair (world_to_eye_prev16,
+ * eye_prev_to_sample_prev9) is read and then replaced by this frame's. A camera starts from
+ * (zero, identity). Column-major. */
+int hvvr_foveated_frame_matrices(const hvvr_transform* camera_to_world, const hvvr_vec3* eye_dir,
+                                 const hvvr_float_rect* sample_bounds, const hvvr_float_rect* viewport,
+                                 float* world_to_eye_prev16, float* eye_prev_to_sample_prev9, float* eye_to_world16,
+                                 float* cull_planes16, float* sample_to_eye9, float* eye_to_sample_prev16);
 /* BVH nodes visited per tile by the last frame's tile cull [tile_count] (the schedule of the
  * next frame is built from these) */
 int hvvr_camera_read_tile_costs(const hvvr_camera* cam, uint32_t* visits);

@@ -1408,3 +1408,344 @@ int renderCore(const oracle_frame_in* in, const SampleSetup& ss, const M4& c2w, 
     return 0;
 }
 } // namespace
+
+// ------------------------------------------------------------------ foveated resolve
+// Restatement, texel by texel and pixel by pixel, of the reference's foveated resolve in the
+// pass order of GPUCamera::foveatedPolarToScreenSpace (RC/gpu_foveated.cu:335-375):
+//   RemapPolarFoveatedKernel            RC/remap.cu:127-141
+//   ComputeMoments                      RC/gpu_foveated.cu:124-139, 159-172
+//   FoveatedPolarToScreenSpaceKernel    RC/gpu_foveated.cu:36-122, 141-157, 174-249
+//   SeparableFilterUsingEccentricity    RC/gpu_foveated.cu:251-294, steps {0,1} then {1,0}
+//   FinishConstrastEnhancement          RC/gpu_foveated.cu:296-333
+// with the colour conversions of shared/util_graphics.h:16-33 and RC/shading_helpers.h:
+// 178-224, the eccentricity map of RC/foveated.h:32-113 and the texture setup of
+// RC/gpu_camera.cu:174-230. The reference reads CUDA texture objects; a fetch here is the
+// texture unit's documented behaviour: normalized coordinates, wrap (u - floor(u)) or clamp
+// addressing, linear filtering between floor(x) and floor(x) + 1 at x = u * n - 0.5 with the
+// fraction held to 1/256, point sampling at floor(u * n), sRGB texels decoded by sRgbToLinear
+// (alpha linear) and unorm16 texels as v / 65535. acos, atan2, log, cos, sin and pow are
+// taken in double and rounded to float (the reference's single-precision device functions
+// are within a few ulp of that).
+namespace {
+
+struct C4 {
+    float x, y, z, w;
+};
+inline C4 c4(float x, float y, float z, float w) { return C4{x, y, z, w}; }
+inline C4 operator+(C4 a, C4 b) { return c4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+inline C4 operator-(C4 a, C4 b) { return c4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+inline C4 operator*(C4 a, C4 b) { return c4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+inline C4 operator*(C4 a, float s) { return c4(a.x * s, a.y * s, a.z * s, a.w * s); }
+// device min/max: a NaN operand yields the other one
+inline float dmin(float a, float b) { return fminf(a, b); }
+inline float dmax(float a, float b) { return fmaxf(a, b); }
+inline float clampF(float x, float lo, float hi) { return dmin(hi, dmax(lo, x)); }
+inline C4 clampC(C4 a, C4 lo, C4 hi) {
+    return c4(clampF(a.x, lo.x, hi.x), clampF(a.y, lo.y, hi.y), clampF(a.z, lo.z, hi.z), clampF(a.w, lo.w, hi.w));
+}
+inline C4 clampC(C4 a, float lo, float hi) { return clampC(a, c4(lo, lo, lo, lo), c4(hi, hi, hi, hi)); }
+
+inline float acosD(float x) { return float(acos(double(x))); }
+inline float atan2D(float y, float x) { return float(atan2(double(y), double(x))); }
+inline float logD(float x) { return float(log(double(x))); }
+inline float cosD(float x) { return float(cos(double(x))); }
+inline float sinD(float x) { return float(sin(double(x))); }
+inline float powD(float x, float y) { return float(pow(double(x), double(y))); }
+
+// sRgbToLinear / linearToSRgb (shared/util_graphics.h:16-33)
+inline float sRgbToLinear(float x) {
+    return (x <= 0.04045f) ? x * (1.0f / 12.92f) : powD((x + .055f) * (1.0f / 1.055f), 2.4f);
+}
+inline float linearToSRgb(float x) {
+    return (x <= 0.0031308f) ? (x * 12.92f) : (powD(x, (1.0f / 2.4f)) * 1.055f - .055f);
+}
+// uint32_t(float) / uint64_t(float) as the device converts (truncate, saturate, NaN -> 0)
+inline uint32_t toU32(float v) {
+    if (!(v > 0.0f)) return 0;
+    return v >= 4294967296.0f ? 0xffffffffu : uint32_t(v);
+}
+inline uint64_t toU64(float v) {
+    if (!(v > 0.0f)) return 0;
+    return v >= 18446744073709551616.0f ? ~0ull : uint64_t(v);
+}
+// ToColor4Unorm8SRgb(vector4), ToColor4Unorm16, FromColor4Unorm8SRgb (RC/shading_helpers.h)
+inline uint32_t toColor4Unorm8SRgb(C4 c) {
+    const uint32_t r = toU32(linearToSRgb(c.x) * 255.0f), g = toU32(linearToSRgb(c.y) * 255.0f);
+    const uint32_t b = toU32(linearToSRgb(c.z) * 255.0f), a = toU32(c.w * 255.0f);
+    return (r) | (g << 8) | (b << 16) | (a << 24);
+}
+inline uint64_t toColor4Unorm16(C4 c) {
+    const float C = 65535.0f;
+    const uint64_t r = toU64(c.x * C), g = toU64(c.y * C), b = toU64(c.z * C), a = toU64(c.w * C);
+    return (r) | (g << 16) | (b << 32) | (a << 48);
+}
+inline C4 fromColor4Unorm8SRgb(uint32_t c) {
+    const float r = (c & 0xFF) / 255.0f, g = ((c >> 8) & 0xFF) / 255.0f, b = ((c >> 16) & 0xFF) / 255.0f;
+    const float a = ((c >> 24) & 0xFF) / 255.0f;
+    return c4(sRgbToLinear(r), sRgbToLinear(g), sRgbToLinear(b), a);
+}
+
+// a texture: RGBA8 sRGB (uint32 texels), RGBA16 unorm (uint64 texels) or R32F
+enum TexFormat { kSrgb8, kUnorm16, kR32f };
+struct Tex {
+    const void* data;
+    int w, h;
+    bool wrapX, wrapY;
+    TexFormat fmt;
+};
+inline int address(int i, int n, bool wrap) {
+    if (wrap) return ((i % n) + n) % n;
+    return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+inline C4 texel(const Tex& t, int x, int y) {
+    const size_t o = size_t(address(y, t.h, t.wrapY)) * t.w + address(x, t.w, t.wrapX);
+    if (t.fmt == kSrgb8) return fromColor4Unorm8SRgb(static_cast<const uint32_t*>(t.data)[o]);
+    if (t.fmt == kUnorm16) {
+        const uint64_t v = static_cast<const uint64_t*>(t.data)[o];
+        return c4(float(v & 0xffff) / 65535.0f, float((v >> 16) & 0xffff) / 65535.0f,
+                  float((v >> 32) & 0xffff) / 65535.0f, float((v >> 48) & 0xffff) / 65535.0f);
+    }
+    const float f = static_cast<const float*>(t.data)[o];
+    return c4(f, 0.0f, 0.0f, 0.0f);
+}
+// one axis of a linear fetch: base texel and the 1/256-quantised fraction (in 256ths)
+inline void linearTap(float u, int n, bool wrap, int& i0, int& a8) {
+    if (wrap) u = u - floorf(u);
+    float x = u * float(n) - 0.5f;
+    x = dmax(dmin(x, float(n)), -1.0f);
+    const float fl = floorf(x);
+    i0 = int(fl);
+    a8 = int(nearbyintf((x - fl) * 256.0f));
+}
+// tex2D with linear filtering at normalized (u, v)
+inline C4 tex2DLinear(const Tex& t, float u, float v) {
+    int x0, y0, ax, ay;
+    linearTap(u, t.w, t.wrapX, x0, ax);
+    linearTap(v, t.h, t.wrapY, y0, ay);
+    const float wx1 = float(ax) * (1.0f / 256.0f), wx0 = float(256 - ax) * (1.0f / 256.0f);
+    const float wy1 = float(ay) * (1.0f / 256.0f), wy0 = float(256 - ay) * (1.0f / 256.0f);
+    return ((texel(t, x0, y0) * (wx0 * wy0) + texel(t, x0 + 1, y0) * (wx1 * wy0)) + texel(t, x0, y0 + 1) * (wx0 * wy1)) +
+           texel(t, x0 + 1, y0 + 1) * (wx1 * wy1);
+}
+// tex2D with point filtering at normalized (u, v)
+inline float tex2DPoint(const Tex& t, float u, float v) {
+    auto idx = [](float c, int n, bool wrap) {
+        if (wrap) c = c - floorf(c);
+        return int(floorf(dmax(dmin(c * float(n), float(n)), -1.0f)));
+    };
+    return texel(t, idx(u, t.w, t.wrapX), idx(v, t.h, t.wrapY)).x;
+}
+
+constexpr float kPiF = 3.141592653589f;  // shared/constants_math.h:15
+
+struct EccMapping {
+    // EccentricityMap (RC/foveated.h:46-55) and EccentricityToTexCoordMapping (RC/gpu_foveated.cu:73-85)
+    float m, w0, S, invLogA, invW0, invM, texMapSize, invTexMapSize, invMaxEccentricity;
+    float applyInverse(float E) const {
+        const float i0 = E * invW0;
+        const float sDivW = S * invW0;
+        const float x = logD((m * (i0 - sDivW)) + 1.0f) * invLogA;
+        const float i1 = x + sDivW;
+        return (E < S) ? i0 : i1;
+    }
+};
+
+// getNormalizedCoord + sampleSpaceToEyeSpaceMatrix * point + eyeSpaceDirectionToAngularEyeCoord
+inline void eyeCoord(const float* S, uint32_t i, uint32_t j, uint32_t w, uint32_t h, float& theta, float& ecc) {
+    const float nx = (float(i) + 0.5f) / float(w), ny = (float(j) + 0.5f) / float(h);
+    const float dx = S[0] * nx + S[3] * ny + S[6] * 1.0f;
+    const float dy = S[1] * nx + S[4] * ny + S[7] * 1.0f;
+    const float dz = S[2] * nx + S[5] * ny + S[8] * 1.0f;
+    const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
+    const float ex = dx * inv, ey = dy * inv, ez = dz * inv;
+    ecc = acosD(-ez);
+    theta = -atan2D(ey, ex);
+}
+
+// bicubicFast (RC/gpu_foveated.cu:36-71)
+C4 bicubicFast(const Tex& tex, float cx, float cy) {
+    const float W = float(tex.w), H = float(tex.h);
+    const float pcx = cx * W, pcy = cy * H;
+    const float ctx = floorf(pcx - 0.5f) + 0.5f, cty = floorf(pcy - 0.5f) + 0.5f;
+    const float iDx = 1.0f / W, iDy = 1.0f / H;
+    float s0[2], s1[2], t0[2], t1[2];
+    const float fv[2] = {pcx - ctx, pcy - cty}, cv[2] = {ctx, cty}, iv[2] = {iDx, iDy};
+    for (int k = 0; k < 2; k++) {
+        const float f = fv[k], f2 = f * f, f3 = f2 * f;
+        const float omf2 = (1.0f - f) * (1.0f - f);
+        const float omf3 = omf2 * (1.0f - f);
+        const float sixth = (1.0f / 6.0f);
+        const float w0 = omf3 * sixth;
+        const float w1 = ((4.0f / 6.0f) * 1.0f + f3 * 0.5f) - f2;
+        const float w3 = f3 * sixth;
+        const float w2 = ((1.0f - w0) - w1) - w3;
+        s0[k] = w0 + w1;
+        s1[k] = w2 + w3;
+        const float f0 = w1 / (w0 + w1), f1 = w3 / (w2 + w3);
+        t0[k] = ((cv[k] - 1.0f) + f0) * iv[k];
+        t1[k] = ((cv[k] + 1.0f) + f1) * iv[k];
+    }
+    return tex2DLinear(tex, t0[0], t0[1]) * s0[0] * s0[1] + tex2DLinear(tex, t1[0], t0[1]) * s1[0] * s0[1] +
+           tex2DLinear(tex, t0[0], t1[1]) * s0[0] * s1[1] + tex2DLinear(tex, t1[0], t1[1]) * s1[0] * s1[1];
+}
+
+template <class Fn>
+void forRows(uint32_t rows, uint32_t threads, Fn fn) {
+    std::atomic<uint32_t> next(0);
+    auto work = [&]() {
+        MxcsrScope mx;
+        for (uint32_t r; (r = next.fetch_add(1)) < rows;) fn(r);
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < (threads ? threads : 1); t++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+}
+
+} // namespace
+
+extern "C" int oracle_foveated_resolve(const oracle_fov_in* in, oracle_fov_out* out) {
+    MxcsrScope mx;
+    const uint32_t W = in->samples_per_ring, H = in->ring_count, w = in->width, h = in->height;
+    if (!W || !H || !w || !h || !out->result || !out->image) return 1;
+    const float radPerDeg = kPiF / 180.0f;
+    EccMapping em;
+    em.m = in->mar_slope;
+    em.w0 = in->foveal_mar_degrees * radPerDeg;
+    em.S = in->degree_tracking_error * radPerDeg;
+    em.invLogA = float(1.0 / log(1.0 + double(em.m)));
+    em.invW0 = float(1.0 / em.w0);
+    em.invM = float(1.0 / em.m);
+    em.texMapSize = float(H);
+    em.invTexMapSize = 1.0f / float(H);
+    em.invMaxEccentricity = 1.0f / (in->max_fov_degrees * radPerDeg);
+    // RemapPolarFoveatedKernel
+    std::vector<uint32_t> raw(size_t(W) * H, 0u);
+    std::vector<float> depth(size_t(W) * H, 0.0f);
+    for (uint32_t s = 0; s < in->valid; s++) {
+        const size_t o = size_t(in->remap[2 * s + 1]) * W + in->remap[2 * s];
+        raw[o] = toColor4Unorm8SRgb(fromColor4Unorm8SRgb(in->colors[s]));
+        depth[o] = in->tmax[s];
+    }
+    const Tex rawTex{raw.data(), int(W), int(H), true, false, kSrgb8};
+    const Tex depthTex{depth.data(), int(W), int(H), true, false, kR32f};
+    // ComputeMoments
+    std::vector<uint64_t> m1(size_t(W) * H), m2(size_t(W) * H);
+    forRows(H, in->threads, [&](uint32_t j) {
+        const float idx = 1.0f / float(W), idy = 1.0f / float(H);
+        const float offsets[3] = {-1.0f, 0.0f, 1.0f};
+        for (uint32_t i = 0; i < W; i++) {
+            const float cx = idx * float(i), cy = idy * float(j);
+            C4 a = c4(0, 0, 0, 0), b = c4(0, 0, 0, 0);
+            for (int x = 0; x < 3; ++x)
+                for (int y = 0; y < 3; ++y) {
+                    const C4 c = tex2DLinear(rawTex, cx + (offsets[x] * idx), cy + (offsets[y] * idy));
+                    a = a + c;
+                    b = b + c * c;
+                }
+            const float weight = 1.0f / 9.0f;
+            m1[size_t(j) * W + i] = toColor4Unorm16(a * weight);
+            m2[size_t(j) * W + i] = toColor4Unorm16(b * weight);
+        }
+    });
+    const Tex m1Tex{m1.data(), int(W), int(H), true, false, kUnorm16};
+    const Tex m2Tex{m2.data(), int(W), int(H), true, false, kUnorm16};
+    const Tex prevTex{in->history, int(w), int(h), false, false, kSrgb8};
+    // FoveatedPolarToScreenSpaceKernel (RGBA8_SRGB): the result texture
+    uint32_t* result = out->result;
+    forRows(h, in->threads, [&](uint32_t j) {
+        for (uint32_t i = 0; i < w; i++) {
+            float theta, ecc;
+            eyeCoord(in->sample_to_eye, i, j, w, h, theta, ecc);
+            const float cx = (theta + kPiF) / (2.0f * kPiF);
+            const float cy = (em.applyInverse(ecc) + 0.5f) * em.invTexMapSize;
+            const C4 newValue = bicubicFast(rawTex, cx, cy);
+            C4 surfaceResult = newValue;
+            const float tValue = tex2DPoint(depthTex, cx, cy);
+            if (tValue < INFINITY) {
+                // angularEyeCoordToDirection(theta, eccentricity) * tValue
+                const float z = -cosD(ecc);
+                const float xyLength = sqrtf(1.0f - z * z);
+                const float px = (cosD(-theta) * xyLength) * tValue, py = (sinD(-theta) * xyLength) * tValue;
+                const float pz = z * tValue;
+                const float* M = in->eye_to_sample_prev;
+                const float qx = M[0] * px + M[4] * py + M[8] * pz + M[12] * 1.0f;
+                const float qy = M[1] * px + M[5] * py + M[9] * pz + M[13] * 1.0f;
+                const float qz = M[2] * px + M[6] * py + M[10] * pz + M[14] * 1.0f;
+                const float ox = qx * (1.0f / qz), oy = qy * (1.0f / qz);
+                float alpha = 0.05f;
+                C4 oldValue = newValue;
+                if (ox > 0 && oy > 0 && ox < 1 && oy < 1 && tValue > 0) oldValue = tex2DLinear(prevTex, ox, oy);
+                // clampToNeighborhood (stddevMultiplier 1)
+                const C4 a = tex2DLinear(m1Tex, cx, cy), b = tex2DLinear(m2Tex, cx, cy);
+                const C4 var = b - (a * a);
+                const C4 sd = c4(sqrtf(var.x), sqrtf(var.y), sqrtf(var.z), sqrtf(var.w));
+                const float scaleFactor = 1.0f;
+                C4 clampedOld = clampC(oldValue, a - (sd * scaleFactor), a + (sd * scaleFactor));
+                float normalizedE = ecc * em.invMaxEccentricity;
+                const float mn = 0.2f, mxv = 0.35f;
+                const float t = clampF((normalizedE - mn) / (mxv - mn), 0.f, 1.f);
+                alpha = 0.5f + (alpha - 0.5f) * t;
+                normalizedE = sqrtf(sqrtf(sqrtf(sqrtf(normalizedE))));
+                clampedOld.x = clampedOld.x + (oldValue.x - clampedOld.x) * normalizedE;
+                clampedOld.y = clampedOld.y + (oldValue.y - clampedOld.y) * normalizedE;
+                clampedOld.z = clampedOld.z + (oldValue.z - clampedOld.z) * normalizedE;
+                clampedOld.w = clampedOld.w + (oldValue.w - clampedOld.w) * normalizedE;
+                surfaceResult = newValue * alpha + clampedOld * (1.0f - alpha);
+            }
+            result[size_t(j) * w + i] = toColor4Unorm8SRgb(surfaceResult);
+        }
+    });
+    // SeparableFilterUsingEccentricity: step {0, 1} into horizontallyFiltered, then {1, 0}
+    auto separable = [&](const uint32_t* input, uint32_t* output, int sx, int sy) {
+        const Tex inTex{input, int(w), int(h), false, false, kSrgb8};
+        forRows(h, in->threads, [&](uint32_t j) {
+            for (uint32_t i = 0; i < w; i++) {
+                float theta, ecc;
+                eyeCoord(in->sample_to_eye, i, j, w, h, theta, ecc);
+                const int filterRadius = 5;
+                C4 valueSum = c4(0.0f, 0.0f, 0.0f, 0.0f);
+                float weightSum = 0.0f;
+                for (int R = -filterRadius; R <= filterRadius; ++R) {
+                    const int tx = std::min(std::max(int(i) + R * sx, 0), int(w) - 1);
+                    const int ty = std::min(std::max(int(j) + R * sy, 0), int(h) - 1);
+                    const float normDist = fabsf(float(R)) / float(filterRadius + 0.1);
+                    const float weight = powD(1.0f - normDist, sqrtf(ecc));
+                    // texelFetch: a linear fetch at the texel centre
+                    valueSum = valueSum + tex2DLinear(inTex, (float(tx) + 0.5f) / float(w),
+                                                      (float(ty) + 0.5f) / float(h)) * weight;
+                    weightSum += weight;
+                }
+                output[size_t(j) * w + i] = toColor4Unorm8SRgb(valueSum * (1.0f / weightSum));
+            }
+        });
+    };
+    std::vector<uint32_t> hFiltered(size_t(w) * h), fFiltered(size_t(w) * h);
+    separable(result, hFiltered.data(), 0, 1);
+    separable(hFiltered.data(), fFiltered.data(), 1, 0);
+    if (out->filtered) memcpy(out->filtered, hFiltered.data(), hFiltered.size() * 4);
+    // FinishConstrastEnhancement (f_e = 1)
+    const Tex unfTex{result, int(w), int(h), false, false, kSrgb8};
+    const Tex filTex{fFiltered.data(), int(w), int(h), false, false, kSrgb8};
+    forRows(h, in->threads, [&](uint32_t j) {
+        for (uint32_t i = 0; i < w; i++) {
+            float theta, ecc;
+            eyeCoord(in->sample_to_eye, i, j, w, h, theta, ecc);
+            float sigma = 8.0f;
+            const float t = ecc * em.invMaxEccentricity;
+            sigma *= dmax(0.001f, clampF(t * t, 0.f, 1.f));
+            const float u = (float(i) + 0.5f) / float(w), v = (float(j) + 0.5f) / float(h);
+            const C4 pix = tex2DLinear(unfTex, u, v), pmean = tex2DLinear(filTex, u, v);
+            const float cScale = 1.f + sigma * 1.0f;
+            const C4 scaled = pmean + (pix - pmean) * cScale;
+            out->image[size_t(j) * w + i] = toColor4Unorm8SRgb(clampC(scaled, 0.0f, 1.0f));
+        }
+    });
+    if (out->polar_color) memcpy(out->polar_color, raw.data(), raw.size() * 4);
+    if (out->moments)
+        for (size_t k = 0; k < m1.size(); k++) {
+            memcpy(out->moments + 8 * k, &m1[k], 8);
+            memcpy(out->moments + 8 * k + 4, &m2[k], 8);
+        }
+    return 0;
+}

@@ -88,6 +88,30 @@ void oracle_msaa_offsets(uint32_t n, float* out);
 /* depth-of-field lens positions for rate n: [4 tiles][n subsamples][128 samples] x 2 floats */
 void oracle_lens_table(uint32_t n, float* out);
 
+/* Foveated resolve of one frame: the polar sample colours and view depths to the screen image
+ * (RemapPolarFoveated, ComputeMoments, FoveatedPolarToScreenSpace, two eccentricity filter
+ * passes and FinishConstrastEnhancement). */
+typedef struct {
+    float degree_tracking_error, max_fov_degrees, mar_slope, foveal_mar_degrees; /* sample pattern */
+    uint32_t samples_per_ring, ring_count, valid;
+    const uint32_t* colors;        /* [valid] RGBA8 per sample (clustered order) */
+    const float* tmax;             /* [valid] view depth of subsample 0 */
+    const uint32_t* remap;         /* [valid * 2] polar texel (azimuth index, ring) */
+    uint32_t width, height;
+    float sample_to_eye[9];        /* column-major */
+    float eye_to_sample_prev[16];  /* column-major */
+    const uint32_t* history;       /* [height * width] the previous frame's result (RGBA8 sRGB) */
+    uint32_t threads;
+} oracle_fov_in;
+typedef struct {
+    uint32_t* polar_color;         /* [ring_count * samples_per_ring] or null */
+    uint16_t* moments;             /* [ring_count * samples_per_ring * 8] (m1 rgba, m2 rgba) or null */
+    uint32_t* result;              /* [height * width] this frame's result (the next frame's history) */
+    uint32_t* filtered;            /* [height * width] the first filter pass, or null */
+    uint32_t* image;               /* [height * width] */
+} oracle_fov_out;
+int oracle_foveated_resolve(const oracle_fov_in* in, oracle_fov_out* out);
+
 #ifdef __cplusplus
 }
 #endif

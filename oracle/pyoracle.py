@@ -35,6 +35,19 @@ class FrameOut(C.Structure):
                 ("tile_rays", C.c_void_p), ("status", C.c_uint32), ("tmax", C.c_void_p)]
 
 
+class FovIn(C.Structure):
+    _fields_ = [("degree_tracking_error", C.c_float), ("max_fov_degrees", C.c_float), ("mar_slope", C.c_float),
+                ("foveal_mar_degrees", C.c_float), ("samples_per_ring", C.c_uint32), ("ring_count", C.c_uint32),
+                ("valid", C.c_uint32), ("colors", C.c_void_p), ("tmax", C.c_void_p), ("remap", C.c_void_p),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("sample_to_eye", C.c_float * 9),
+                ("eye_to_sample_prev", C.c_float * 16), ("history", C.c_void_p), ("threads", C.c_uint32)]
+
+
+class FovOut(C.Structure):
+    _fields_ = [("polar_color", C.c_void_p), ("moments", C.c_void_p), ("result", C.c_void_p),
+                ("filtered", C.c_void_p), ("image", C.c_void_p)]
+
+
 class BeamsIn(C.Structure):
     _fields_ = [("beams", C.c_void_p), ("tile_rays", C.c_void_p), ("block_rays", C.c_void_p), ("blocks", C.c_uint32),
                 ("batch_to_world", C.c_void_p), ("cull_planes", C.c_void_p)]
@@ -163,6 +176,34 @@ class Oracle:
         return _run(f, scene, None, _abi.transform(), _abi.FloatRect(), 0, 0, msaa, fp_mode=fp_mode, threads=threads,
                     want=want, beams_in=beams_in)
 
+    def foveated_resolve(self, pattern, polar, colors, tmax, width, height, sample_to_eye, eye_to_sample_prev,
+                         history, threads=None):
+        """One frame of the foveated resolve. pattern: (degree tracking error, max FOV, MAR slope,
+        foveal MAR); polar: the sample set dict (samples_per_ring, ring_count, valid, remap);
+        colors / tmax: per sample [>= valid]; history: the previous result [height, width].
+        Returns a dict of polar_color, moments [rings, spr, 2, 4], result, filtered, image."""
+        f = self.lib.oracle_foveated_resolve
+        f.argtypes = [C.POINTER(FovIn), C.POINTER(FovOut)]
+        f.restype = C.c_int
+        spr, rings, valid = polar["samples_per_ring"], polar["ring_count"], polar["valid"]
+        colors = np.ascontiguousarray(colors[:valid], np.uint32)
+        tmax = np.ascontiguousarray(tmax[:valid], np.float32)
+        remap = np.ascontiguousarray(polar["remap"][:valid], np.uint32)
+        history = np.ascontiguousarray(history, np.uint32)
+        fi = FovIn(*(float(v) for v in pattern), spr, rings, valid, colors.ctypes.data, tmax.ctypes.data,
+                   remap.ctypes.data, width, height)
+        fi.sample_to_eye[:] = [float(v) for v in np.asarray(sample_to_eye, np.float32).ravel()]
+        fi.eye_to_sample_prev[:] = [float(v) for v in np.asarray(eye_to_sample_prev, np.float32).ravel()]
+        fi.history = history.ctypes.data
+        fi.threads = threads or min(32, os.cpu_count() or 1)
+        out = {"polar_color": np.zeros((rings, spr), np.uint32), "moments": np.zeros((rings, spr, 2, 4), np.uint16),
+               "result": np.zeros((height, width), np.uint32), "filtered": np.zeros((height, width), np.uint32),
+               "image": np.zeros((height, width), np.uint32)}
+        fo = FovOut(*(out[k].ctypes.data for k in ("polar_color", "moments", "result", "filtered", "image")))
+        if f(C.byref(fi), C.byref(fo)) != 0:
+            raise RuntimeError("oracle_foveated_resolve failed")
+        return out
+
     def msaa_offsets(self, n):
         o = np.zeros((n, 2), dtype=np.float32)
         self.lib.oracle_msaa_offsets(n, o.ctypes.data)
@@ -207,6 +248,27 @@ class Reference:
                "block_rays": np.zeros((padded // 8192, 24), np.float32)}
         f(*args, counts.ctypes.data, out["beams"].ctypes.data, out["remap"].ctypes.data,
           out["tile_rays"].ctypes.data, out["block_rays"].ctypes.data)
+        return out
+
+    def foveated_frame_matrices(self, xf, eye_dir, sample_bounds, viewport, history=None):
+        """The reference's per-frame foveated matrices (same dict as hvvr_b200.foveated_frame_matrices)."""
+        f = self.lib.ref_foveated_frame_matrices
+        f.argtypes = [C.POINTER(_abi.Transform)] + [C.c_void_p] * 9
+        f.restype = C.c_int
+        if history is None:
+            w2ep, ep2sp = np.zeros(16, np.float32), np.eye(3, dtype=np.float32).reshape(9)
+        else:
+            w2ep, ep2sp = (np.array(h, np.float32).reshape(n).copy() for h, n in zip(history, (16, 9)))
+        ed = np.array(eye_dir, np.float32)
+        sb = np.array([sample_bounds.lower.x, sample_bounds.lower.y, sample_bounds.upper.x, sample_bounds.upper.y],
+                      np.float32)
+        vp = np.array([viewport.lower.x, viewport.lower.y, viewport.upper.x, viewport.upper.y], np.float32)
+        out = {"eye_to_world": np.zeros(16, np.float32), "cull_planes": np.zeros((4, 4), np.float32),
+               "sample_to_eye": np.zeros(9, np.float32), "eye_to_sample_prev": np.zeros(16, np.float32)}
+        f(C.byref(xf), ed.ctypes.data, sb.ctypes.data, vp.ctypes.data, w2ep.ctypes.data, ep2sp.ctypes.data,
+          out["eye_to_world"].ctypes.data, out["cull_planes"].ctypes.data, out["sample_to_eye"].ctypes.data,
+          out["eye_to_sample_prev"].ctypes.data)
+        out["history"] = (w2ep, ep2sp)
         return out
 
     def generate_topology(self, scene):

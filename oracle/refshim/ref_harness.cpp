@@ -522,3 +522,59 @@ extern "C" int ref_polar_foveated(float degreeTrackingError, float maxFOVDegrees
     }
     return 0;
 }
+
+// ------------------------------------------------------------------ foveated frame matrices
+// The per-frame matrices of Raycaster::renderFoveatedPolarSpaceCudaReconstruct
+// (RC/render.cpp:454-487) with the reference's own vector algebra: eyeToWorld, the cull planes
+// of cullRectToCullPlanes (RC/render.cpp:397-416, a file-static function, so its ten lines are
+// restated here on the reference's types), sampleToEye, and eyeToSamplePrevious as
+// GPUCamera::foveatedPolarToScreenSpace forms it (RC/gpu_foveated.cu:341); then the history
+// update. Column-major in and out.
+static_assert(sizeof(matrix4x4) == 64 && sizeof(matrix3x3) == 36, "column-major float matrices");
+extern "C" int ref_foveated_frame_matrices(const hvvr_transform* cameraToWorldXf, const float* eyeDir3,
+                                           const float* sampleBounds4, const float* viewport4,
+                                           float* worldToEyePrev16, float* eyePrevToSamplePrev9, float* eyeToWorld16,
+                                           float* cullPlanes16, float* sampleToEye9, float* eyeToSamplePrev16) {
+    MxcsrScope mx;
+    const FloatRect vp(vector2(viewport4[0], viewport4[1]), vector2(viewport4[2], viewport4[3]));
+    const FloatRect sb(vector2(sampleBounds4[0], sampleBounds4[1]), vector2(sampleBounds4[2], sampleBounds4[3]));
+    matrix3x3 sampleToCamera(vector3(vp.upper.x - vp.lower.x, 0, 0), vector3(0, vp.lower.y - vp.upper.y, 0),
+                             vector3(vp.lower.x, vp.upper.y, -1));
+    const vector3 eyeDirection(eyeDir3[0], eyeDir3[1], eyeDir3[2]);
+    matrix3x3 eyeToCamera = matrix3x3::rotationFromZAxis(-eyeDirection);
+    matrix4x4 cameraToWorld = matrix4x4(*(const transform*)cameraToWorldXf);
+    matrix4x4 eyeToWorld = cameraToWorld * matrix4x4(eyeToCamera);
+    {
+        const matrix3x3 cameraToEye = invert(eyeToCamera);
+        auto U = sb.upper;
+        auto L = sb.lower;
+        vector2 sampleDirs[4] = {{U.x, U.y}, {L.x, U.y}, {L.x, L.y}, {U.x, L.y}};
+        for (int i = 0; i < 4; ++i) {
+            vector3 dir0 = sampleToCamera * vector3(sampleDirs[i], 1.0f);
+            vector3 dir1 = sampleToCamera * vector3(sampleDirs[(i + 1) % 4], 1.0f);
+            Plane eyeSpacePlane;
+            eyeSpacePlane.normal = cameraToEye * normalize(cross(dir1, dir0));
+            eyeSpacePlane.dist = -0.01f;
+            Plane p = eyeToWorld * eyeSpacePlane;
+            cullPlanes16[4 * i + 0] = p.normal.x;
+            cullPlanes16[4 * i + 1] = p.normal.y;
+            cullPlanes16[4 * i + 2] = p.normal.z;
+            cullPlanes16[4 * i + 3] = p.dist;
+        }
+    }
+    matrix4x4 worldToEyePrevious;
+    matrix3x3 eyePreviousToSamplePrevious;
+    memcpy(&worldToEyePrevious, worldToEyePrev16, 64);
+    memcpy(&eyePreviousToSamplePrevious, eyePrevToSamplePrev9, 36);
+    matrix3x3 sampleToEye = invert(eyeToCamera) * sampleToCamera;
+    matrix4x4 eyeToEyePrevious = worldToEyePrevious * eyeToWorld;
+    matrix4x4 eyeToSamplePrevious = matrix4x4(eyePreviousToSamplePrevious) * eyeToEyePrevious;
+    memcpy(eyeToWorld16, &eyeToWorld, 64);
+    memcpy(sampleToEye9, &sampleToEye, 36);
+    memcpy(eyeToSamplePrev16, &eyeToSamplePrevious, 64);
+    worldToEyePrevious = invert(eyeToWorld);
+    eyePreviousToSamplePrevious = invert(sampleToEye);
+    memcpy(worldToEyePrev16, &worldToEyePrevious, 64);
+    memcpy(eyePrevToSamplePrev9, &eyePreviousToSamplePrevious, 36);
+    return 0;
+}
