@@ -110,6 +110,7 @@ _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
 _sig("hvvr_camera_read_foveated_frame", _vp, _vp, _vp, _vp)
 _sig("hvvr_camera_read_foveated_resolve", _vp, _vp, _vp, _vp, _vp)
+_sig("hvvr_camera_read_polar_textures", _vp, _vp, _vp, _vp)
 _sig("hvvr_foveated_frame_matrices", _p(_abi.Transform), _p(_abi.Vec3), _p(_abi.FloatRect), _p(_abi.FloatRect),
      _vp, _vp, _vp, _vp, _vp, _vp)
 
@@ -133,6 +134,7 @@ EXPORTED = [
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
     "hvvr_camera_read_foveated_frame", "hvvr_camera_read_foveated_resolve", "hvvr_foveated_frame_matrices",
+    "hvvr_camera_read_polar_textures",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
     "hvvr_server_submit", "hvvr_server_prewarm", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
 ]
@@ -371,6 +373,15 @@ class Camera:
         _check(_lib.hvvr_camera_read_foveated_resolve(self.handle, s2e.ctypes.data, e2p.ctypes.data,
                                                       res.ctypes.data, hist.ctypes.data))
         return s2e, e2p, res, hist
+
+    def polar_textures(self, samples_per_ring, ring_count):
+        """foveated polar mode: the last frame's polar colour [rings, spr], view depth [rings, spr]
+        and moments [rings, spr, 2, 4] (uint16)"""
+        col = np.zeros((ring_count, samples_per_ring), np.uint32)
+        dep = np.zeros((ring_count, samples_per_ring), np.float32)
+        mom = np.zeros((ring_count, samples_per_ring, 2, 4), np.uint16)
+        _check(_lib.hvvr_camera_read_polar_textures(self.handle, col.ctypes.data, dep.ctypes.data, mom.ctypes.data))
+        return col, dep, mom
 
     def tile_costs(self):
         """BVH nodes visited per tile by the last frame's tile cull"""

@@ -55,6 +55,10 @@ __device__ __forceinline__ float dlog(float x) { return float(log(double(x))); }
 __device__ __forceinline__ float dcos(float x) { return float(cos(double(x))); }
 __device__ __forceinline__ float dsin(float x) { return float(sin(double(x))); }
 __device__ __forceinline__ float dpow(float x, float y) { return float(pow(double(x), double(y))); }
+// IEEE round-to-nearest division. Every division in this file goes through it: nvcc compiles a
+// plain '/' by a compile-time constant to a multiply that can differ in the last bit, even under
+// -prec-div=true (divisions of two constants are folded at compile time and stay as written).
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 // clamp(x, lo, hi) = min(hi, max(lo, x)) with the device min/max (NaN bounds pass x through)
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(hi, fmaxf(lo, x)); }
 
@@ -73,10 +77,11 @@ __device__ __forceinline__ uint32_t encodeSrgb(const ColorTables& t, float4 c) {
 }
 // FromColor4Unorm8SRgb / an sRGB texel as the texture unit returns it
 __device__ __forceinline__ float4 decodeSrgb(const ColorTables& t, uint32_t c) {
-    return make_float4(t.dec[c & 255u], t.dec[(c >> 8) & 255u], t.dec[(c >> 16) & 255u], float(c >> 24) / 255.0f);
+    return make_float4(t.dec[c & 255u], t.dec[(c >> 8) & 255u], t.dec[(c >> 16) & 255u], fdiv(float(c >> 24), 255.0f));
 }
 __device__ __forceinline__ float4 decodeUnorm16(ushort4 v) {
-    return make_float4(float(v.x) / 65535.0f, float(v.y) / 65535.0f, float(v.z) / 65535.0f, float(v.w) / 65535.0f);
+    return make_float4(fdiv(float(v.x), 65535.0f), fdiv(float(v.y), 65535.0f), fdiv(float(v.z), 65535.0f),
+                       fdiv(float(v.w), 65535.0f));
 }
 // ToColor4Unorm16 (shading_helpers.h:201-208): truncating * 65535
 __device__ __forceinline__ ushort4 encodeUnorm16(float4 c) {
@@ -138,7 +143,7 @@ __device__ __forceinline__ float4 sampleSrgb(const ColorTables& t, const uint32_
 // sampleSpaceToEyeSpace * (x, y, 1), normalized; then (theta, eccentricity)
 // (getNormalizedCoord, eyeSpaceDirectionToAngularEyeCoord: gpu_foveated.cu:92-107)
 __device__ __forceinline__ void pixelEyeCoord(const FoveaDev& f, uint32_t i, uint32_t j, float& theta, float& ecc) {
-    const float nx = (float(i) + 0.5f) / float(f.width), ny = (float(j) + 0.5f) / float(f.height);
+    const float nx = fdiv(float(i) + 0.5f, float(f.width)), ny = fdiv(float(j) + 0.5f, float(f.height));
     const float* S = f.sampleToEye;
     const F3 d = f3(S[0] * nx + S[3] * ny + S[6] * 1.0f, S[1] * nx + S[4] * ny + S[7] * 1.0f,
                     S[2] * nx + S[5] * ny + S[8] * 1.0f);
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(256) momentsKernel(const ViewDev* views, uint3
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     const int w = int(f.spr), h = int(f.rings);
     if (i >= f.spr || j >= f.rings) return;
-    const float idx = 1.0f / float(w), idy = 1.0f / float(h);
+    const float idx = fdiv(1.0f, float(w)), idy = fdiv(1.0f, float(h));
     const float cx = idx * float(i), cy = idy * float(j);
     const float offs[3] = {-1.0f, 0.0f, 1.0f};
     float4 m1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), m2 = m1;
@@ -204,7 +209,7 @@ __device__ float4 bicubicFast(const ColorTables& t, const FoveaDev& f, float cx,
     const int w = int(f.spr), h = int(f.rings);
     const float px = cx * float(w), py = cy * float(h);
     const float ctrx = floorf(px - 0.5f) + 0.5f, ctry = floorf(py - 0.5f) + 0.5f;
-    const float idx = 1.0f / float(w), idy = 1.0f / float(h);
+    const float idx = fdiv(1.0f, float(w)), idy = fdiv(1.0f, float(h));
     float s0[2], s1[2], t0[2], t1[2];
     const float fr[2] = {px - ctrx, py - ctry}, ctr[2] = {ctrx, ctry}, id[2] = {idx, idy};
 #pragma unroll
@@ -219,7 +224,7 @@ __device__ float4 bicubicFast(const ColorTables& t, const FoveaDev& f, float cx,
         const float w2 = ((1.0f - w0) - w1) - w3;
         s0[k] = w0 + w1;
         s1[k] = w2 + w3;
-        const float f0 = w1 / (w0 + w1), f1 = w3 / (w2 + w3);
+        const float f0 = fdiv(w1, w0 + w1), f1 = fdiv(w3, w2 + w3);
         t0[k] = ((ctr[k] - 1.0f) + f0) * id[k];
         t1[k] = ((ctr[k] + 1.0f) + f1) * id[k];
     }
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(256) polarToScreenKernel(const ViewDev* views,
     float theta, ecc;
     pixelEyeCoord(f, i, j, theta, ecc);
     // angularEyeCoordToPolarTextureCoord
-    const float cx = (theta + kPi) / (2.0f * kPi);
+    const float cx = fdiv(theta + kPi, 2.0f * kPi);
     const float cy = (eccApplyInverse(f, ecc) + 0.5f) * f.invTexMapSize;
     const float4 newValue = bicubicFast(t, f, cx, cy);
     float4 result = newValue;
@@ -257,7 +262,7 @@ __global__ void __launch_bounds__(256) polarToScreenKernel(const ViewDev* views,
         const float qx = M[0] * p.x + M[4] * p.y + M[8] * p.z + M[12] * 1.0f;
         const float qy = M[1] * p.x + M[5] * p.y + M[9] * p.z + M[13] * 1.0f;
         const float qz = M[2] * p.x + M[6] * p.y + M[10] * p.z + M[14] * 1.0f;
-        const float iz = 1.0f / qz;
+        const float iz = fdiv(1.0f, qz);
         const float ox = qx * iz, oy = qy * iz;
         float alpha = 0.05f;  // TemporalFilterSettings::alpha
         float4 oldValue = newValue;
@@ -281,7 +286,7 @@ __global__ void __launch_bounds__(256) polarToScreenKernel(const ViewDev* views,
         co.w = clampf(oldValue.w, m1.w - sd.w * sm, m1.w + sd.w * sm);
         float nE = ecc * f.invMaxEcc;
         const float mn = 0.2f, mx = 0.35f;
-        const float tt = clampf((nE - mn) / (mx - mn), 0.0f, 1.0f);
+        const float tt = clampf(fdiv(nE - mn, mx - mn), 0.0f, 1.0f);
         alpha = 0.5f + (alpha - 0.5f) * tt;
         nE = sqrtf(sqrtf(sqrtf(sqrtf(nE))));
         co.x = co.x + (oldValue.x - co.x) * nE;
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(256) polarToScreenKernel(const ViewDev* views,
     f.ecc[o] = ecc;
     const float se = sqrtf(ecc);
 #pragma unroll
-    for (int r = 1; r <= 5; r++) f.ecc[r * npix + o] = dpow(1.0f - fabsf(float(r)) / kFilterDen, se);
+    for (int r = 1; r <= 5; r++) f.ecc[r * npix + o] = dpow(1.0f - fdiv(fabsf(float(r)), kFilterDen), se);
 }
 
 // SeparableFilterUsingEccentricity over in (radius 5, clamped taps) at pixel (i, j)
@@ -318,7 +323,7 @@ __device__ __forceinline__ float4 eccFilter(const ColorTables& t, const FoveaDev
         vs = add4(vs, mul4(decodeSrgb(t, in[size_t(y) * f.width + x]), w));
         ws += w;
     }
-    return mul4(vs, 1.0f / ws);
+    return mul4(vs, fdiv(1.0f, ws));
 }
 
 __global__ void __launch_bounds__(256) filterVerticalKernel(const ViewDev* views, uint32_t view) {

@@ -1713,6 +1713,16 @@ int hvvr_camera_read_foveated_resolve(const hvvr_camera* cam, float* sample_to_e
     return HVVR_OK;
 }
 
+int hvvr_camera_read_polar_textures(const hvvr_camera* cam, uint32_t* color, float* depth, uint16_t* moments) {
+    TRY(requireRendered(cam));
+    if (!cam->foveated || !cam->fovStatic.image) return fail(HVVR_ERR_STATE, "not a foveated camera with a render target");
+    const size_t texels = size_t(cam->fovStatic.spr) * cam->fovStatic.rings;
+    if (color) CUDA_TRY(cudaMemcpy(color, cam->polarColor.p, texels * 4, cudaMemcpyDeviceToHost));
+    if (depth) CUDA_TRY(cudaMemcpy(depth, cam->polarDepth.p, texels * 4, cudaMemcpyDeviceToHost));
+    if (moments) CUDA_TRY(cudaMemcpy(moments, cam->moments.p, texels * 16, cudaMemcpyDeviceToHost));
+    return HVVR_OK;
+}
+
 int hvvr_foveated_frame_matrices(const hvvr_transform* camera_to_world, const hvvr_vec3* eye_dir,
                                  const hvvr_float_rect* sample_bounds, const hvvr_float_rect* viewport,
                                  float* world_to_eye_prev16, float* eye_prev_to_sample_prev9, float* eye_to_world16,

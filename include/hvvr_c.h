@@ -246,6 +246,11 @@ int hvvr_camera_read_foveated_frame(const hvvr_camera* cam, float* eye_to_world1
  * ([height * width]). Any pointer may be null. The final image goes to the render target. */
 int hvvr_camera_read_foveated_resolve(const hvvr_camera* cam, float* sample_to_eye9, float* eye_to_sample_prev16,
                                       uint32_t* result, uint32_t* history);
+/* Foveated polar mode: the last frame's polar textures [ring_count][samples_per_ring] - colour
+ * (RGBA8 sRGB, RemapPolarFoveatedKernel, remap.cu:127-141), view depth, and the moments
+ * (8 x uint16 per texel: first then second moment, RGBA16 unorm; ComputeMoments,
+ * gpu_foveated.cu:159-172). Any pointer may be null. */
+int hvvr_camera_read_polar_textures(const hvvr_camera* cam, uint32_t* color, float* depth, uint16_t* moments);
 /* The per-frame matrices of a foveated camera, on the host (no device work; render.cpp:
  * 463-486): from the camera-to-world transform, gaze, sample bounds and viewport, the
  * eye-to-world matrix [16], the four tile cull planes [16], sample-to-eye [9] and
