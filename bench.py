@@ -21,6 +21,7 @@ crop of the same frame.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -42,9 +43,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="hvvr_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="stereo", choices=["stereo", "batched", "served"],
+    ap.add_argument("--workload", default="stereo", choices=["stereo", "batched", "served", "foveated"],
                     help="stereo: the headline 2x1080x1200 frame; batched: 64 views over 4 scenes, batched vs plain; "
-                         "served: Poisson request arrivals against the render server")
+                         "served: Poisson request arrivals against the render server; foveated: polar foveated "
+                         "stereo, 16xMSAA, resolved to 1440x1600 per eye, gaze in a 10-degree saccade")
     ap.add_argument("--rates", default="100,250,500,1000,2000,5000,10000,20000", help="served: arrival rates, req/s")
     ap.add_argument("--seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--views", type=int, default=64)
@@ -271,6 +273,9 @@ def main():
         return
     if args.workload == "served":
         run_served(args)
+        return
+    if args.workload == "foveated":
+        run_foveated(args)
         return
     import numpy as np
     import torch
@@ -679,6 +684,197 @@ def run_served(args):
     print(json.dumps(line), flush=True)
     for rc in rcs:
         rc.close()
+
+
+# polar foveated stereo: the reference's polar sample set with its foveal MAR (1/60 degree) and a
+# slope of 1/300 (MAR(e) = w0 (1 + e / 5 deg) past 0.5 degrees of tracking error, density
+# ~ 1 / (1 + e / 5 deg)^2) out to 50 degrees of eccentricity: 1,173,612 samples per eye
+FOV_PATTERN = (0.5, 50.0, 1.0 / 300.0, 1.0 / 60.0)
+FOV_W, FOV_H, FOV_MSAA, FOV_FIELD = 1440, 1600, 16, 100.0
+
+
+def saccade(frame):
+    """Gaze of frame k of the 8-frame saccade: 10 degrees of azimuth, left to right."""
+    a = math.radians(-5.0 + 10.0 * (frame % 8) / 7.0)
+    return (math.sin(a), 0.0, -math.cos(a))
+
+
+def foveated_setup(hv, scenes, sc, target_cuda, torch):
+    from hvvr_b200 import _abi
+    spec = hv.foveated_spec(*FOV_PATTERN, mode=_abi.HVVR_MODE_FOVEATED_POLAR)
+    rc = hv.Raycaster(spec=spec, tri_index_capacity=256 << 20)
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    smp = scenes.grid_samples(FOV_W, FOV_H)
+    cams, images = [], []
+    for xf in scenes.stereo_eyes(IPD):
+        cam = rc.create_camera(scenes.viewport_fov(FOV_W, FOV_H, FOV_FIELD))
+        if target_cuda:
+            img = torch.zeros((FOV_H, FOV_W), dtype=torch.int32, device="cuda")
+            cam.set_render_target(FOV_W, FOV_H, device_ptr=img.data_ptr())
+            images.append(img)
+        else:
+            cam.set_render_target(FOV_W, FOV_H)
+        cam.set_samples(smp)
+        cam.set_camera_to_world(xf)
+        cam.set_msaa(FOV_MSAA)
+        cam.set_eye_dir(saccade(0))
+        cams.append(cam)
+    return rc, cams, images
+
+
+def resolve_bytes(polar, pixels):
+    """Compulsory HBM bytes of a frame's foveated resolve launches, per eye summed: per polar
+    sample 4 B colour + 4 B depth + 8 B remap read and 8 B written to the polar textures; per
+    polar texel the moments pass reads 4 B and writes 16 B, the polar -> screen pass reads 24 B;
+    per pixel the polar -> screen pass reads 4 B of history and writes 4 B of result and 24 B of
+    eccentricity and filter weights, the vertical pass reads 24 B and writes 4 B, the horizontal
+    pass reads 32 B and writes 4 B of image."""
+    texels = polar["samples_per_ring"] * polar["ring_count"]
+    return polar["valid"] * 24 + texels * (4 + 16 + 24) + pixels * (4 + 4 + 24 + 24 + 4 + 32 + 4)
+
+
+def run_foveated(args):
+    """Polar foveated stereo on the 995k-triangle scene: both eyes in one batch, 16xMSAA, eye-space
+    traversal with the per-frame gaze, the foveated resolve (temporal reprojection, eccentricity
+    filters, contrast enhancement) to 1440x1600 per eye; the gaze cycles through an 8-frame
+    10-degree saccade. One step = one stereo frame."""
+    import numpy as np
+    import torch
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    sc = scenes.scene_c2()
+    hv.generate_topology(sc)
+    polar = hv.polar_foveated_samples(hv.foveated_spec(*FOV_PATTERN))
+    # counts of one frame (both eyes) for the algorithmic bytes
+    rc, cams, _ = foveated_setup(hv, scenes, sc, False, torch)
+    for c in cams:
+        c.set_capture(hv.HVVR_CAPTURE_HITS)
+    rc.render()
+    rc.render()
+    counts = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0}
+    for cam in cams:
+        blocks, tiles, padded, msaa = cam.layout()
+        n, tri, mask = cam.gbuffer()
+        counts["padded_samples"] += padded
+        counts["tiles"] += tiles
+        counts["list_entries"] += cam.list_total()
+        counts["unique_hits"] += int(((tri != 0xFFFFFFFF) & (mask != 0)).sum())
+        counts["node_visits"] += int(cam.tile_costs().astype(np.int64).sum())
+    rc.close()
+
+    rc, cams, images = foveated_setup(hv, scenes, sc, True, torch)
+    samples_per_frame = 2 * polar["valid"]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = ctypes_stream(stream)
+    frame = 0
+    for _ in range(args.warmup):
+        for c in cams:
+            c.set_eye_dir(saccade(frame))
+        rc.render(stream=sp)
+        frame += 1
+    torch.cuda.synchronize()
+    rc.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms, stage_ms = [], []
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        flush.fill_(i & 0xff)
+        for c in cams:
+            c.set_eye_dir(saccade(frame))
+        frame += 1
+        starts[i].record(stream)
+        rc.render(stream=sp)
+        ends[i].record(stream)
+        torch.cuda.synchronize()
+        kernel_ms.append([float(x) for x in rc.kernel_times()])
+        stage_ms.append([float(x) for x in cams[0].timings()])
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    rc.synchronize()
+    frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = max_over_ranks(sum(frame_ms), dist, "cuda")
+    value = replica_throughput(samples_per_frame, args.steps, total_ms * 1e-3, world)
+    rc.close()
+
+    # end to end through the C ABI: CPU_MEMORY targets, both resolved images copied to host
+    rc2, cams2, _ = foveated_setup(hv, scenes, sc, False, torch)
+    for k in range(max(3, args.warmup)):
+        for c in cams2:
+            c.set_eye_dir(saccade(k))
+        rc2.render()
+    e2e_steps = max(3, args.steps // 2)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        for c in cams2:
+            c.set_eye_dir(saccade(k))
+        rc2.render()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e_value = replica_throughput(samples_per_frame, e2e_steps, e2e_s, world)
+    rc2.close()
+
+    peak, peak_kind = load_peaks()
+    resolve_ms = statistics.mean(s[4] for s in stage_ms)
+    kernels = {
+        "tileCullKernel": {"algorithmic_bytes": cull_bytes(counts),
+                           "launch_ms_per_frame": statistics.mean(k[0] for k in kernel_ms)},
+        "intersectShadeKernel<16,FMA>": {"algorithmic_bytes": intersect_bytes(counts),
+                                         "launch_ms_per_frame": statistics.mean(k[1] for k in kernel_ms)},
+        "foveated resolve (5 kernels per eye)": {"algorithmic_bytes": 2 * resolve_bytes(polar, FOV_W * FOV_H),
+                                                 "launch_ms_per_frame": resolve_ms},
+    }
+    for name, k in kernels.items():
+        k["achieved_gbs"] = k["algorithmic_bytes"] / (k["launch_ms_per_frame"] * 1e-3) / 1e9
+        k["frac"] = k["achieved_gbs"] / peak
+        k["traffic"] = None
+    dom = max(kernels, key=lambda n: kernels[n]["launch_ms_per_frame"])
+    line = {
+        "metric": "vis+shade+resolve Gsamples/s", "value": value, "unit": "Gsamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "p50_frame_ms": statistics.median(frame_ms), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural 995k-triangle scene, polar foveated sample set)",
+        "config": {"workload": "polar foveated stereo, %d samples per eye (pattern %s), 16xMSAA, resolved to "
+                               "1440x1600 per eye over a 100-degree field, gaze in an 8-frame 10-degree saccade, "
+                               "995,072-triangle scene; one frame (both eyes) per step" % (polar["valid"], FOV_PATTERN),
+                   "samples_per_frame": samples_per_frame, "parallelism": "replicas x%d" % world,
+                   "l2": "flushed between frames (256 MiB write, untimed)"},
+        "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 2 * 12,
+                "d2h_bytes_per_step": 2 * FOV_W * FOV_H * 4},
+        "roofline": {"bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": kernels[dom]["frac"], "traffic": None, "kernel": dom,
+                     "per_frame": "launches of one stereo frame; bytes and times summed over them",
+                     "peak_source": peak_kind, "kernels": kernels, "counts": counts},
+        "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
+                               [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
+                                (4, "resolve"), (5, "total")]},
+        # per frame: block cull, tile order, tile cull + intersect (2 parts), 5 resolve kernels per eye
+        "gpu_launches": args.steps * 16,
+        "clocks": ck,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
 
 
 def run_profile_case():
