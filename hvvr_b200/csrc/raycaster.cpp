@@ -467,6 +467,17 @@ int ensureMsaaTable(uint32_t rate, cudaStream_t st) {
 }
 
 size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa) {
+    if (cam->foveated) {
+        const CameraDev& d = cam->dev;
+        const FoveaDev& f = cam->fovStatic;
+        size_t b = size_t(d.tiles) * (sizeof(Rays4) + sizeof(TileList) + 4) +
+                   size_t(d.blocks) * (sizeof(Rays4) + kBlockStack * sizeof(StackEntry) + 4) +
+                   size_t(d.padded) * (48 + 8 + 4 + 4);
+        b += size_t(f.spr) * f.rings * (4 + 4 + 16) + size_t(f.width) * f.height * (4 * 3 + 24);
+        if (cam->target.memory_type == HVVR_MEMORY_CPU) b += size_t(f.width) * f.height * 4;
+        if (cam->capture & HVVR_CAPTURE_HITS) b += size_t(d.padded) * msaa * 8;
+        return b;
+    }
     const SampleSetup& ss = cam->setup;
     size_t b = ss.tileRays.size() * sizeof(Rays4) + ss.blockRays.size() * sizeof(Rays4) + ss.beams.size() * 4 +
                ss.remap.size() * 4;
@@ -479,6 +490,28 @@ size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa) {
 
 int cloneCamera(const hvvr_camera* src, hvvr_camera** out) {
     if (src->setupDirty) return fail(HVVR_ERR_STATE, "camera to clone has no setup yet");
+    if (src->foveated) {
+        // a polar-mode camera's samples are the raycaster's polar set: set the clone up from it
+        auto c = std::make_unique<hvvr_camera>();
+        c->rc = src->rc;
+        c->viewport = src->viewport;
+        c->lens = src->lens;
+        c->eyeDir = src->eyeDir;
+        c->target = src->target;
+        c->target.data = nullptr;
+        c->samples = src->samples;
+        c->split = src->split;
+        c->xf = src->xf;
+        c->msaa = src->msaa;
+        const cudaStream_t st = src->rc->stream;
+        TRY(setupFoveatedCamera(c.get(), st));
+        CUDA_TRY(cudaMemcpyAsync(c->tileCost.p, src->tileCost.p, size_t(c->dev.tiles) * 4, cudaMemcpyDeviceToDevice, st));
+        c->costFrames = src->costFrames;
+        CUDA_TRY(cudaStreamSynchronize(st));
+        *out = c.get();
+        src->rc->cameras.push_back(std::move(c));
+        return HVVR_OK;
+    }
     auto c = std::make_unique<hvvr_camera>();
     c->rc = src->rc;
     c->viewport = src->viewport;

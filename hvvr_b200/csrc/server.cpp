@@ -290,6 +290,13 @@ bool dispatch(hvvr_server* s, Slot& sl) {
         c->target.stride = tp.width;
         c->dev.image = img;
         c->dev.imageStride = tp.width;
+        if (c->foveated) {
+            // the resolve writes this request's image, and a request is one frame: no history
+            // from whichever request this instance served before
+            c->fovStatic.image = img;
+            c->fovStatic.imageStride = tp.width;
+            resetFoveatedHistory(c);
+        }
         b->cams.push_back(c);
         r->dispatchMs = now;
         r->batchViews = uint32_t(take.size());

@@ -149,3 +149,53 @@ def test_served_animation_matches_oracle(oracle):
         assert d.max() <= 1
     srv.close()
     rc.close()
+
+
+def test_polar_foveated_requests_same_alone_in_mix_and_direct():
+    """Polar foveated templates: every request is one first frame (no temporal history), so its
+    resolved image must be the same alone, in a mix, and rendered directly by a camera of the
+    same raycaster."""
+    from hvvr_b200 import _abi
+    sc = scene("small")
+    spec = hv.foveated_spec(1.0, 35.0, 0.03, 0.06, mode=_abi.HVVR_MODE_FOVEATED_POLAR)
+    rc = hv.Raycaster(spec=spec)
+    rc.create_model(sc)
+    for l in sc.lights:
+        rc.create_light(l)
+    srv = hv.Server([rc], hv.server_config(slots=2, max_batch_views=4, slot_list_capacity=1 << 22))
+    sizes = [(160, 144), (128, 112)]
+    vids = []
+    for w, h in sizes:
+        vids.append(srv.add_view(0, scenes.viewport_for(w, h), scenes.grid_samples(w, h), w, h))
+    rng = np.random.default_rng(11)
+    reqs = []
+    for k in range(8):
+        t = k % 2
+        ang = rng.uniform(-0.5, 0.5)
+        xf = scenes.camera_transform(eye=(8.0 * np.sin(ang), 2.5, 8.0 * np.cos(ang)), target=(0.0, 0.0, 0.0))
+        reqs.append((t, int([4, 8][k % 2]), xf))
+    mix = []
+    for t, msaa, xf in reqs:
+        w, h = sizes[t]
+        out = np.zeros((h, w), np.uint32)
+        mix.append((srv.submit(vids[t], msaa, xf, output=out), out))
+    done = _drain(srv, len(mix))
+    assert all(c.status == 0 for c in done.values())
+    for k, (t, msaa, xf) in enumerate(reqs):
+        w, h = sizes[t]
+        out = np.zeros((h, w), np.uint32)
+        rid = srv.submit(vids[t], msaa, xf, output=out)
+        assert _drain(srv, 1)[rid].status == 0
+        assert np.array_equal(out, mix[k][1]), "request %d differs alone and in the mix" % k
+        assert (out & 0xFFFFFF).any()
+        if k < 2:
+            cam = rc.create_camera(scenes.viewport_for(w, h))
+            cam.set_render_target(w, h)
+            cam.set_samples(scenes.grid_samples(w, h))
+            cam.set_msaa(msaa)
+            cam.set_camera_to_world(xf)
+            rc.render()
+            assert np.array_equal(cam.image, out), "request %d differs from a direct render" % k
+            cam.set_enabled(False)
+    srv.close()
+    rc.close()
