@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--views", type=int, default=64)
     ap.add_argument("--profile", action="store_true",
-                    help="case for ncu: the stereo frame, 3 frames, 32M-entry index pool")
+                    help="case for ncu: the stereo frame (or with --workload foveated the foveated frame), 3 frames")
     return ap.parse_args()
 
 
@@ -266,7 +266,10 @@ def main():
         run_reference_arm(args, rank)
         return
     if args.profile:
-        run_profile_case()
+        if args.workload == "foveated":
+            run_profile_case_foveated()
+        else:
+            run_profile_case()
         return
     if args.workload == "batched":
         run_batched(args)
@@ -903,6 +906,27 @@ def run_profile_case():
                           "stage_ms": [float(x) for x in cams[0].timings()],
                           "kernel_ms": [float(x) for x in rc.kernel_times()],
                           "list_entries": sum(c.list_total() for c in cams)}))
+
+
+def run_profile_case_foveated():
+    """The foveated benchmark frame (both eyes, resolve to 1440x1600 each), 3 frames of the
+    saccade, 64M-entry list pool: the case the foveated launch list and captures run on."""
+    import torch
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    sc = scenes.scene_c2()
+    hv.generate_topology(sc)
+    rc, cams, _ = foveated_setup(hv, scenes, sc, False, torch)
+    for k in range(3):
+        for c in cams:
+            c.set_eye_dir(saccade(k))
+        rc.render()
+    rc.synchronize()
+    print(json.dumps({"profile_case": "polar foveated stereo 16xMSAA, resolve 2x1440x1600, 995k tris, frame 3",
+                      "stage_ms": [float(x) for x in cams[0].timings()],
+                      "kernel_ms": [float(x) for x in rc.kernel_times()],
+                      "list_entries": sum(c.list_total() for c in cams)}))
+    rc.close()
 
 
 def ctypes_stream(stream):

@@ -107,6 +107,8 @@ _sig("hvvr_server_poll", _vp, _p(_abi.Completion), _u32, _p(_u32), C.c_double)
 _sig("hvvr_server_update_vertices", _vp, _vp, _u32, _u32, _vp)
 _sig("hvvr_server_get_stats", _vp, _p(_abi.ServerStats))
 _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
+_sig("hvvr_raycaster_read_part_times", _vp, _vp)
+_sig("hvvr_batch_read_part_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
 _sig("hvvr_camera_read_foveated_frame", _vp, _vp, _vp, _vp)
 _sig("hvvr_camera_read_foveated_resolve", _vp, _vp, _vp, _vp, _vp)
@@ -133,6 +135,7 @@ EXPORTED = [
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
+    "hvvr_raycaster_read_part_times", "hvvr_batch_read_part_times",
     "hvvr_camera_read_foveated_frame", "hvvr_camera_read_foveated_resolve", "hvvr_foveated_frame_matrices",
     "hvvr_camera_read_polar_textures",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
@@ -479,6 +482,14 @@ class Raycaster:
         _check(_lib.hvvr_raycaster_read_kernel_times(self.handle, t.ctypes.data))
         return t
 
+    def part_times(self):
+        """the last frame's timeline per launch part [24, 3]: tile cull start, tile cull end,
+        intersect end (ms from the frame start, -1 where the part did not run); part 2r holds
+        rate class r's slowest tiles, 2r+1 the rest"""
+        t = np.zeros((24, 3), dtype=np.float32)
+        _check(_lib.hvvr_raycaster_read_part_times(self.handle, t.ctypes.data))
+        return t
+
     def scene_counts(self):
         n, t, v = _u32(0), _u32(0), _u32(0)
         _check(_lib.hvvr_scene_get_counts(self.handle, C.byref(n), C.byref(t), C.byref(v)))
@@ -568,6 +579,12 @@ class Batch:
         """device ms of the last frame's launches: tile cull, intersect/shade, block cull, remap"""
         t = np.zeros(4, dtype=np.float32)
         _check(_lib.hvvr_batch_read_kernel_times(self.handle, t.ctypes.data))
+        return t
+
+    def part_times(self):
+        """the last frame's timeline per launch part [24, 3] (see Raycaster.part_times)"""
+        t = np.zeros((24, 3), dtype=np.float32)
+        _check(_lib.hvvr_batch_read_part_times(self.handle, t.ctypes.data))
         return t
 
     def stats(self):

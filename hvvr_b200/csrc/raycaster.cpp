@@ -1231,6 +1231,18 @@ int kernelTimes(const hvvr_batch* b, float* ms4) {
 }
 } // namespace
 
+static int partTimes(const hvvr_batch* b, float* ms72) {
+    if (!b || !b->counterValid) return fail(HVVR_ERR_STATE, "no frame rendered");
+    if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was a graph replay (no per-launch events)");
+    CUDA_TRY(cudaEventSynchronize(b->ev[5]));
+    for (uint32_t k = 0; k < 2 * kRateClasses; k++) {
+        float* o = ms72 + 3 * k;
+        o[0] = o[1] = o[2] = -1.0f;
+        if (!b->kevUsed[k]) continue;
+        for (int i = 0; i < 3; i++) CUDA_TRY(cudaEventElapsedTime(&o[i], b->ev[0], b->kev[k][i]));
+    }
+    return HVVR_OK;
+}
 int hvvr_batch_read_stats(const hvvr_batch* b, uint64_t* out4) {
     if (!b || !out4) return fail(HVVR_ERR_INVALID, "NULL argument");
     if (!b->counterValid || !b->hostCounters) return fail(HVVR_ERR_STATE, "the batch has not rendered a frame");
@@ -1247,6 +1259,16 @@ int hvvr_batch_read_stats(const hvvr_batch* b, uint64_t* out4) {
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4) {
     if (!rc || !ms4) return fail(HVVR_ERR_INVALID, "NULL argument");
     return kernelTimes(rc->own.get(), ms4);
+}
+
+int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72) {
+    if (!rc || !ms72) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return partTimes(rc->own.get(), ms72);
+}
+
+int hvvr_batch_read_part_times(const hvvr_batch* b, float* ms72) {
+    if (!ms72) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return partTimes(b, ms72);
 }
 
 int hvvr_batch_read_kernel_times(const hvvr_batch* b, float* ms4) {

@@ -341,6 +341,13 @@ int hvvr_batch_read_timings(const hvvr_batch* batch, float* ms5);
  * intersect/shade, [2] block cull, [3] remap. Not available after a graph replay. */
 int hvvr_batch_read_kernel_times(const hvvr_batch* batch, float* ms4);
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
+/* The last frame's launch timeline per part: rate class r (log2 MSAA, + 6 for thin-lens views)
+ * runs as part 2r (its slowest tiles by the previous frame's cost, on a high-priority stream)
+ * and part 2r+1 (the rest). ms72[3 * part + i] = tile cull start, tile cull end, intersect/shade
+ * end, in ms from the frame start; -1 for parts that did not run. Not available after a graph
+ * replay. */
+int hvvr_batch_read_part_times(const hvvr_batch* batch, float* ms72);
+int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72);
 /* counters of the last frame: [0] list-pool entries taken (whole chunks), [1] tiles culled
  * again with the 4096-entry stack, [2] device status bits, [3] views */
 int hvvr_batch_read_stats(const hvvr_batch* batch, uint64_t* out4);
