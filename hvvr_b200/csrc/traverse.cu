@@ -377,6 +377,9 @@ __global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(FrameDev fr)
 
 
 // per-warp tile traversal state; S = sorted-stack capacity
+// passing leaf slots buffered per warp as triangle ranges before they are expanded into the list
+constexpr uint32_t kRanges = 128;
+
 template <uint32_t S>
 struct TileSmemT {
     SmemFrustum f;
@@ -384,6 +387,7 @@ struct TileSmemT {
     uint32_t mask[S];
     uint32_t node[S];
     alignas(16) uint32_t buf[kChunk];
+    uint32_t rStart[kRanges], rLen[kRanges];
 };
 
 struct Emitter {
@@ -416,40 +420,73 @@ struct Emitter {
         __syncwarp();
     }
 
-    // Appends the triangle ranges of the passing leaf slots of one node, in slot order. v holds
-    // word l of the node in lane l; leaf slot k covers [tri[k], tri[k+1]) = words 25+k, 26+k.
-    __device__ void emitLeaves(uint32_t* buf, float v, uint32_t leaf) {
-        uint32_t start[4], len[4], pre[4], n = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t t0 = __float_as_uint(__shfl_sync(kFull, v, 25 + k));
-            const uint32_t t1 = __float_as_uint(__shfl_sync(kFull, v, 26 + k));
-            const bool on = (leaf >> k) & 1u;
-            if (on && t1 <= t0 && laneId() == 0) atomicOr(&counters[1], kStatusBadLeaf);
-            start[k] = t0;
-            len[k] = (on && t1 > t0) ? t1 - t0 : 0u;
-            pre[k] = n;
-            n += len[k];
+    uint32_t rc; // ranges buffered in rStart/rLen
+
+    // Records the triangle ranges of the passing leaf slots of one node, in slot order (leaf
+    // slot k covers [tri[k], tri[k+1]) = words 25+k, 26+k of the node; v holds word l of the
+    // node in lane l). The entries are written out later by expand(), in the same order.
+    template <uint32_t S>
+    __device__ void addLeaves(TileSmemT<S>& s, float v, uint32_t leaf) {
+        const uint32_t lane = laneId(), k = lane & 3u;
+        const uint32_t t0 = __float_as_uint(__shfl_sync(kFull, v, 25 + k));
+        const uint32_t t1 = __float_as_uint(__shfl_sync(kFull, v, 26 + k));
+        const bool on = lane < 4 && ((leaf >> k) & 1u);
+        if (on && t1 <= t0) atomicOr(&counters[1], kStatusBadLeaf);
+        const bool emit = on && t1 > t0;
+        const uint32_t b = __ballot_sync(kFull, emit);
+        if (rc + 4 > kRanges) expand(s);
+        if (emit) {
+            const uint32_t pos = rc + __popc(b & ((1u << lane) - 1u));
+            s.rStart[pos] = t0;
+            s.rLen[pos] = t1 - t0;
         }
-        uint32_t done = 0;
-        while (done < n && !dead) {
-            const uint32_t m = min(n - done, kChunk - bufCount);
-            for (uint32_t j = laneId(); j < m; j += 32) {
-                const uint32_t p = done + j;
-                // the last non-empty slot whose range starts at or before p
-                uint32_t kk = 0;
-#pragma unroll
-                for (uint32_t q = 1; q < 4; q++)
-                    if (len[q] && p >= pre[q]) kk = q;
-                buf[bufCount + j] = start[kk] + (p - pre[kk]);
-            }
-            bufCount += m;
-            done += m;
-            total += m;
-            if (bufCount == kChunk) flush(buf);
-        }
+        rc += __popc(b);
+        __syncwarp();
     }
 
+    // Expands the buffered ranges into list entries (through buf, flushed to the pool per
+    // chunk), 32 ranges at a time: lane r holds range r's start and the exclusive prefix of
+    // the lengths, and each entry finds its range by a binary search over the lanes.
+    template <uint32_t S>
+    __device__ void expand(TileSmemT<S>& s) {
+        const uint32_t lane = laneId();
+        for (uint32_t r0 = 0; r0 < rc && !dead; r0 += 32) {
+            const uint32_t r = r0 + lane;
+            const uint32_t len = r < rc ? s.rLen[r] : 0u;
+            const uint32_t start = r < rc ? s.rStart[r] : 0u;
+            uint32_t inc = len;
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, inc, o);
+                if (lane >= o) inc += y;
+            }
+            const uint32_t n = __shfl_sync(kFull, inc, 31);
+            const uint32_t excl = inc - len; // lanes past the last range hold n
+            uint32_t done = 0;
+            while (done < n && !dead) {
+                const uint32_t m = min(n - done, kChunk - bufCount);
+                for (uint32_t base = 0; base < m; base += 32) {
+                    const uint32_t j = base + lane;
+                    const uint32_t p = done + j;
+                    uint32_t lo = 0;
+#pragma unroll
+                    for (uint32_t step = 16; step; step >>= 1) {
+                        const uint32_t e = __shfl_sync(kFull, excl, lo + step);
+                        if (e <= p) lo += step;
+                    }
+                    const uint32_t st = __shfl_sync(kFull, start, lo);
+                    const uint32_t pre = __shfl_sync(kFull, excl, lo);
+                    if (j < m) s.buf[bufCount + j] = st + (p - pre);
+                }
+                bufCount += m;
+                done += m;
+                total += m;
+                if (bufCount == kChunk) flush(s.buf);
+            }
+        }
+        rc = 0;
+        __syncwarp();
+    }
 };
 
 struct TileCullArgs {
@@ -498,7 +535,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
     __syncwarp();
     const LaneTest t = loadLaneTest(s.f);
     const int distIdx = s.f.distIdx;
-    Emitter em{a.pool, a.chunkNext, a.poolChunks, a.counters, kNoChunk, kNoChunk, 0, 0, 0, false};
+    Emitter em{a.pool, a.chunkNext, a.poolChunks, a.counters, kNoChunk, kNoChunk, 0, 0, 0, false, 0};
     uint32_t top = stackSize - 1;
     uint32_t node = s.node[top];
     uint32_t visits = 0;
@@ -528,7 +565,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
             if (leaf) {
                 mask &= ~refineReject(cb, t);
                 leaf = mask & leafMask;
-                if (leaf) em.emitLeaves(s.buf, v, leaf);
+                if (leaf) em.addLeaves(s, v, leaf);
                 if (em.dead) break;
             }
             mask &= ~leafMask;
@@ -633,6 +670,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
         if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
         return visits;
     }
+    if (!em.dead && em.rc) em.expand(s);
     if (!em.dead && em.bufCount) em.flush(s.buf);
     if (lane == 0) {
         if (em.prev != kNoChunk) a.chunkNext[em.prev] = kNoChunk;
