@@ -56,9 +56,8 @@ __device__ __forceinline__ TriGeom loadTri(const float4* __restrict__ tris, uint
 struct TriThread {
     float dc, vc, wc, ddx, ddy, dvx, dvy, dwx, dwy;
 };
-__device__ __forceinline__ TriThread threadSetup(F3 e0, F3 e1, F3 v0r, F3 c, F3 du, F3 dv) {
+__device__ __forceinline__ TriThread threadSetupN(F3 normal, F3 e0, F3 e1, F3 v0r, F3 c, F3 du, F3 dv) {
     TriThread r;
-    const F3 normal = cross3(e0, e1);
     r.dc = dot3(-c, normal);
     const F3 ec = cross3(-c, v0r);
     r.vc = dot3(e1, ec);
@@ -71,6 +70,11 @@ __device__ __forceinline__ TriThread threadSetup(F3 e0, F3 e1, F3 v0r, F3 c, F3 
     r.dwx = -dot3(e0, cu);
     r.dwy = -dot3(e0, cv);
     return r;
+}
+// the same with normal = e0 x e1 computed here (the per-triangle part, which the tile loop
+// computes once per triangle instead of once per thread)
+__device__ __forceinline__ TriThread threadSetup(F3 e0, F3 e1, F3 v0r, F3 c, F3 du, F3 dv) {
+    return threadSetupN(cross3(e0, e1), e0, e1, v0r, c, du, dv);
 }
 
 // IntersectTriangleThread::test (prim_tests.h:192-231)
@@ -269,12 +273,10 @@ __device__ __forceinline__ bool uvwAllOut(const float (&ro)[4][3], const float (
 struct ShadeSmem {
     float ro[4][3], rd[4][3]; // world corner rays
     float pl[4][4];           // frustum planes
-    uint32_t idx[kChunk];
-    float tt[kChunk];
-    float e0[3][kChunk];
-    float e1[3][kChunk];
-    float vr[3][kChunk];
-    float nl[kChunk]; // |e0 x e1| as computed in float, for the depth skip
+    // the chunk's surviving triangles, one 16-byte record each (read by all threads at once):
+    // {e0, t}, {e1, |e0 x e1|} (the norm as computed in float, for the depth skip),
+    // {camPos - v0, index}, {e0 x e1, 0}
+    float4 te0[kChunk], te1[kChunk], tvr[kChunk], tn[kChunk];
     uint32_t warpCount[4];
 };
 
@@ -363,7 +365,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         bool keep = false;
         uint32_t idx = 0;
         float t = 0.0f, nlen = 0.0f;
-        F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0);
+        F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0), nrm = f3(0, 0, 0);
         if (tid < n) {
             idx = fr.pool[size_t(chunk) * kChunk + tid];
             const TriGeom tri = loadTri(viewPtr(V.tris), idx);
@@ -389,6 +391,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
                         keep = true;
                         e0 = tri.e0;
                         e1 = tri.e1;
+                        nrm = normal;
                         nlen = sqrtf(dot3(normal, normal));
                     }
                 }
@@ -406,12 +409,10 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
             total += cw;
         }
         if (keep) {
-            sm.idx[off] = idx;
-            sm.tt[off] = t;
-            sm.e0[0][off] = e0.x; sm.e0[1][off] = e0.y; sm.e0[2][off] = e0.z;
-            sm.e1[0][off] = e1.x; sm.e1[1][off] = e1.y; sm.e1[2][off] = e1.z;
-            sm.vr[0][off] = v0r.x; sm.vr[1][off] = v0r.y; sm.vr[2][off] = v0r.z;
-            sm.nl[off] = nlen;
+            sm.te0[off] = make_float4(e0.x, e0.y, e0.z, t);
+            sm.te1[off] = make_float4(e1.x, e1.y, e1.z, nlen);
+            sm.tvr[off] = make_float4(v0r.x, v0r.y, v0r.z, __uint_as_float(idx));
+            sm.tn[off] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
         }
         __syncthreads();
         // Depth skip. The test rejects a subsample when depth * denom < t (FMA mode, exactly;
@@ -424,13 +425,15 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         for (uint32_t i = 0; i < N; i++) laneT = fmaxf(laneT, tmax[i]);
         const float laneBound = laneT * dirLen;
         for (uint32_t j = 0; j < total; j++) {
-            if (__all_sync(kFull, sm.tt[j] > laneBound * sm.nl[j])) continue;
-            const F3 je0 = f3(sm.e0[0][j], sm.e0[1][j], sm.e0[2][j]);
-            const F3 je1 = f3(sm.e1[0][j], sm.e1[1][j], sm.e1[2][j]);
-            const F3 jvr = f3(sm.vr[0][j], sm.vr[1][j], sm.vr[2][j]);
-            const float jt = sm.tt[j];
-            const uint32_t jidx = sm.idx[j];
-            const TriThread th = threadSetup(je0, je1, jvr, c, du, dv);
+            const float4 a0 = sm.te0[j], a1 = sm.te1[j];
+            if (__all_sync(kFull, a0.w > laneBound * a1.w)) continue;
+            const float4 a2 = sm.tvr[j], a3 = sm.tn[j];
+            const F3 je0 = f3(a0.x, a0.y, a0.z);
+            const F3 je1 = f3(a1.x, a1.y, a1.z);
+            const F3 jvr = f3(a2.x, a2.y, a2.z);
+            const float jt = a0.w;
+            const uint32_t jidx = __float_as_uint(a2.w);
+            const TriThread th = threadSetupN(f3(a3.x, a3.y, a3.z), je0, je1, jvr, c, du, dv);
 #pragma unroll
             for (uint32_t i = 0; i < N; i++) {
                 const float2 a = cMsaa[rate][i];

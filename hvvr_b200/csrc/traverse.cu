@@ -234,11 +234,13 @@ __device__ __forceinline__ uint32_t testChildren(const ChildBox& b, const LaneTe
     return bytesAllOnes(__ballot_sync(kFull, pass));
 }
 
+// The reference adds +0.0f to each selected bound (turning -0 into +0); that only changes the
+// sign of a zero product or sum, which no comparison below can see, so it is left out.
 __device__ __forceinline__ bool edgeReject(const ChildBox& b, float ex, float ey, float ez, float mn, float mx) {
     const bool px = ex > 0.0f, py = ey > 0.0f, pz = ez > 0.0f;
-    const float pX = (px ? b.xM : -b.xN) + 0.0f, nX = (px ? -b.xN : b.xM) + 0.0f;
-    const float pY = (py ? b.yM : -b.yN) + 0.0f, nY = (py ? -b.yN : b.yM) + 0.0f;
-    const float pZ = (pz ? b.zM : -b.zN) + 0.0f, nZ = (pz ? -b.zN : b.zM) + 0.0f;
+    const float pX = px ? b.xM : -b.xN, nX = px ? -b.xN : b.xM;
+    const float pY = py ? b.yM : -b.yN, nY = py ? -b.yN : b.yM;
+    const float pZ = pz ? b.zM : -b.zN, nZ = pz ? -b.zN : b.zM;
     const float maxBox = fmaf(ex, pX, fmaf(ey, pY, ez * pZ));
     const float minBox = fmaf(ex, nX, fmaf(ey, nY, ez * nZ));
     return (maxBox < mn) || (mx < minBox);
