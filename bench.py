@@ -169,7 +169,8 @@ def frame_counts(hv, scenes, sc):
         c.set_capture(hv.HVVR_CAPTURE_HITS)
     rc.render()
     rc.render()
-    out = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0}
+    out = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0,
+           "tested_entries": int(rc.counters()[4])}
     for cam in cams:
         blocks, tiles, padded, msaa = cam.layout()
         n, tri, mask = cam.gbuffer()
@@ -187,6 +188,23 @@ def intersect_bytes(c):
     written; per list entry 4 B index + 48 B triangle; per unique (sample, triangle) hit 16 B shade
     record + 3 x 32 B vertices + 64 B material + 48 B triangle."""
     return c["padded_samples"] * (48 + 4) + c["list_entries"] * (4 + 48) + c["unique_hits"] * (16 + 96 + 64 + 48)
+
+
+def intersect_flops(c, msaa):
+    """FP32 operations of a frame's intersect tests: every list entry that passes the per-tile tests
+    is tested against the 128 samples of its tile, 72 flops of per-(sample, triangle) setup
+    (IntersectTriangleThread + GetDifferentials) and 16 per subsample (7 FMA + 2 adds)."""
+    return c["tested_entries"] * 128 * (72 + 16 * msaa)
+
+
+def fp32_line(c, msaa, launch_ms, sm_mhz):
+    """achieved FP32 rate of the intersect launches against the FP32 peak at the sampled SM clock
+    (148 SMs x 128 FP32 lanes x 2 flops per FMA: a nominal figure; no FP32 peak is measured)"""
+    flops = intersect_flops(c, msaa)
+    peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = flops / (launch_ms * 1e-3) / 1e12
+    return {"flops_per_frame": flops, "achieved_tflops": achieved, "peak_tflops": peak, "frac": achieved / peak,
+            "peak_source": "nominal at %.0f MHz" % sm_mhz}
 
 
 def cull_bytes(c):
@@ -376,6 +394,7 @@ def main():
                      "frac": kernels[dom]["frac"], "traffic": kernels[dom]["traffic"], "kernel": dom,
                      "per_frame": "launches of one stereo frame; bytes and times summed over them",
                      "peak_source": peak_kind, "kernels": kernels, "counts": counts},
+        "fp32": fp32_line(counts, MSAA, isect_ms, ck.get("sm_mhz") or 1965.0),
         "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
                                [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
                                 (4, "remap"), (5, "total")]},
@@ -765,7 +784,8 @@ def run_foveated(args):
         c.set_capture(hv.HVVR_CAPTURE_HITS)
     rc.render()
     rc.render()
-    counts = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0}
+    counts = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0,
+              "tested_entries": int(rc.counters()[4])}
     for cam in cams:
         blocks, tiles, padded, msaa = cam.layout()
         n, tri, mask = cam.gbuffer()
@@ -867,6 +887,8 @@ def run_foveated(args):
                      "frac": kernels[dom]["frac"], "traffic": None, "kernel": dom,
                      "per_frame": "launches of one stereo frame; bytes and times summed over them",
                      "peak_source": peak_kind, "kernels": kernels, "counts": counts},
+        "fp32": fp32_line(counts, FOV_MSAA, kernels["intersectShadeKernel<16,FMA>"]["launch_ms_per_frame"],
+                          ck.get("sm_mhz") or 1965.0),
         "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
                                [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
                                 (4, "resolve"), (5, "total")]},

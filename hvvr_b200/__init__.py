@@ -96,6 +96,8 @@ _sig("hvvr_batch_autotune", _vp, _u32, _p(_abi.BatchConfig))
 _sig("hvvr_batch_read_timings", _vp, _vp)
 _sig("hvvr_batch_read_kernel_times", _vp, _vp)
 _sig("hvvr_batch_read_stats", _vp, _vp)
+_sig("hvvr_batch_read_counters", _vp, _vp, _u32)
+_sig("hvvr_raycaster_read_counters", _vp, _vp, _u32)
 _lib.hvvr_server_config_default.argtypes = [_p(_abi.ServerConfig)]
 _lib.hvvr_server_config_default.restype = None
 _sig("hvvr_server_create", _p(_vp), _u32, _p(_abi.ServerConfig), _p(_vp))
@@ -135,7 +137,8 @@ EXPORTED = [
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
-    "hvvr_raycaster_read_part_times", "hvvr_batch_read_part_times",
+    "hvvr_raycaster_read_part_times", "hvvr_batch_read_part_times", "hvvr_batch_read_counters",
+    "hvvr_raycaster_read_counters",
     "hvvr_camera_read_foveated_frame", "hvvr_camera_read_foveated_resolve", "hvvr_foveated_frame_matrices",
     "hvvr_camera_read_polar_textures",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
@@ -480,6 +483,13 @@ class Raycaster:
         """device ms of the last frame's launches: tile cull, intersect/shade, block cull, remap"""
         t = np.zeros(4, dtype=np.float32)
         _check(_lib.hvvr_raycaster_read_kernel_times(self.handle, t.ctypes.data))
+        return t
+
+    def counters(self):
+        """the last frame's counters: list pool entries, retried tiles, status, views, list entries
+        that passed the intersect's per-tile tests"""
+        t = np.zeros(5, dtype=np.uint64)
+        _check(_lib.hvvr_raycaster_read_counters(self.handle, t.ctypes.data, 5))
         return t
 
     def part_times(self):

@@ -199,7 +199,13 @@ int setLastError(int code, const char* msg);
 enum : uint32_t { kRateClasses = 12 };
 // counters: [0] chunk allocator, [1] status, then per tile-cull launch k (2 per rate class)
 // three words at kQueueBase + 3k: work-queue head, retry count, retry-queue head
-enum : uint32_t { kQueueBase = 2, kQueueWords = 3, kCounterWords = kQueueBase + kQueueWords * 2 * kRateClasses };
+// then one word counting the list entries that survive the intersect's per-tile tests
+enum : uint32_t {
+    kQueueBase = 2,
+    kQueueWords = 3,
+    kSurvivorWord = kQueueBase + kQueueWords * 2 * kRateClasses,
+    kCounterWords = kSurvivorWord + 1
+};
 
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
 cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st);

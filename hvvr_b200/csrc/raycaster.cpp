@@ -1231,6 +1231,18 @@ int kernelTimes(const hvvr_batch* b, float* ms4) {
 }
 } // namespace
 
+static int frameCounters(const hvvr_batch* b, uint64_t* out, uint32_t count) {
+    if (!b || !out) return fail(HVVR_ERR_INVALID, "NULL argument");
+    if (!b->counterValid || !b->hostCounters) return fail(HVVR_ERR_STATE, "the batch has not rendered a frame");
+    CUDA_TRY(cudaEventSynchronize(b->ev[5]));
+    uint64_t retried = 0;
+    for (uint32_t k = 0; k < 2 * kRateClasses; k++) retried += b->hostCounters[kQueueBase + kQueueWords * k + 1];
+    const uint64_t v[5] = {uint64_t(std::min(b->hostCounters[0], b->poolChunks)) * kChunk, retried, b->hostCounters[1],
+                           b->views.size(), b->hostCounters[kSurvivorWord]};
+    for (uint32_t i = 0; i < count; i++) out[i] = i < 5 ? v[i] : 0u;
+    return HVVR_OK;
+}
+
 static int partTimes(const hvvr_batch* b, float* ms72) {
     if (!b || !b->counterValid) return fail(HVVR_ERR_STATE, "no frame rendered");
     if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was a graph replay (no per-launch events)");
@@ -1259,6 +1271,15 @@ int hvvr_batch_read_stats(const hvvr_batch* b, uint64_t* out4) {
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4) {
     if (!rc || !ms4) return fail(HVVR_ERR_INVALID, "NULL argument");
     return kernelTimes(rc->own.get(), ms4);
+}
+
+int hvvr_batch_read_counters(const hvvr_batch* b, uint64_t* out, uint32_t count) {
+    return frameCounters(b, out, count);
+}
+
+int hvvr_raycaster_read_counters(const hvvr_raycaster* rc, uint64_t* out, uint32_t count) {
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return frameCounters(rc->own.get(), out, count);
 }
 
 int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72) {

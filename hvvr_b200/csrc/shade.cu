@@ -281,7 +281,7 @@ struct ShadeSmem {
 };
 
 // resident CTAs per SM the register allocation must allow (7 = 72 registers per thread)
-template <uint32_t N> struct MinCtas { static constexpr int v = N <= 8 ? 7 : (N == 16 ? 5 : 4); };
+template <uint32_t N> struct MinCtas { static constexpr int v = N <= 8 ? 7 : 4; }; // N = 16: 107 registers, no spill
 
 template <uint32_t N, bool FMA>
 __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel(FrameDev fr, const uint32_t* __restrict__ order,
@@ -359,6 +359,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
 
     uint32_t chunk = L.first;
     uint32_t remaining = L.count;
+    uint32_t survivors = 0;
     while (remaining > 0 && chunk < fr.poolChunks) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
         const uint32_t nextChunk = fr.chunkNext[chunk];
@@ -420,6 +421,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         // denom <= dirLen * |n| and depth <= laneT, t > laneT * dirLen * |n| rejects every
         // subsample of the lane; a triangle is skipped only when that holds for all 32 lanes,
         // so the hits are exactly those of the full loop. Misses keep laneT at FLT_MAX (no skip).
+        survivors += total;
         float laneT = 0.0f;
 #pragma unroll
         for (uint32_t i = 0; i < N; i++) laneT = fmaxf(laneT, tmax[i]);
@@ -445,6 +447,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         chunk = nextChunk;
     }
 
+    if (tid == 0 && survivors) atomicAdd(&fr.counters[kSurvivorWord], survivors);
     if (uint32_t* hitOut = viewPtr(V.hitIds)) {
         float* depthOut = viewPtr(V.depth);
 #pragma unroll
@@ -655,6 +658,7 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr
 
     uint32_t chunk = L.first;
     uint32_t remaining = L.count;
+    uint32_t survivors = 0;
     while (remaining > 0 && chunk < fr.poolChunks) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
         const uint32_t nextChunk = fr.chunkNext[chunk];
@@ -710,6 +714,7 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr
             sm.e1[0][off] = tri.e1.x; sm.e1[1][off] = tri.e1.y; sm.e1[2][off] = tri.e1.z;
             sm.vl[0][off] = v0l.x; sm.vl[1][off] = v0l.y; sm.vl[2][off] = v0l.z;
         }
+        survivors += total;
         __syncthreads();
         for (uint32_t j = 0; j < total; j++) {
             const F3 je0 = f3(sm.e0[0][j], sm.e0[1][j], sm.e0[2][j]);
@@ -742,6 +747,7 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr
         remaining -= n;
         chunk = nextChunk;
     }
+    if (tid == 0 && survivors) atomicAdd(&fr.counters[kSurvivorWord], survivors);
 
     if (uint32_t* hitOut = viewPtr(V.hitIds)) {
         float* depthOut = viewPtr(V.depth);

@@ -351,6 +351,12 @@ int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72);
 /* counters of the last frame: [0] list-pool entries taken (whole chunks), [1] tiles culled
  * again with the 4096-entry stack, [2] device status bits, [3] views */
 int hvvr_batch_read_stats(const hvvr_batch* batch, uint64_t* out4);
+/* The last frame's counters, out[0..count): [0] triangle-list pool entries used (whole chunks),
+ * [1] tiles culled again with the 4096-entry stack, [2] status bits, [3] views, [4] list entries
+ * that passed the intersect's per-tile tests (frustum planes, ray-origin side, corner-ray
+ * barycentrics) and were tested against every sample of the tile; later indices read 0. */
+int hvvr_batch_read_counters(const hvvr_batch* batch, uint64_t* out, uint32_t count);
+int hvvr_raycaster_read_counters(const hvvr_raycaster* rc, uint64_t* out, uint32_t count);
 
 /* ---------------------------------------------------------------- serving
  * No counterpart in the reference. A server owns one worker thread that renders requests as
