@@ -325,7 +325,6 @@ def main():
     rc.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kernel_ms, stage_ms = [], []
     clocks = Clocks(local)
     if dist:
         dist.barrier()
@@ -337,11 +336,10 @@ def main():
         rc.render(stream=sp)
         ends[i].record(stream)
         torch.cuda.synchronize()
-        kernel_ms.append([float(x) for x in rc.kernel_times()])
-        stage_ms.append([float(x) for x in cams[0].timings()])
     torch.cuda.synchronize()
     ck = clocks.stop()
     rc.synchronize()
+    kernel_ms, stage_ms = launch_times(rc, cams[0], lambda k: rc.render(stream=sp), flush)
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = max_over_ranks(sum(frame_ms), dist, "cuda")
     ms_per_step = total_ms / args.steps
@@ -398,9 +396,9 @@ def main():
         "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
                                [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
                                 (4, "remap"), (5, "total")]},
-        # per frame: block cull, tile order, per eye set of tiles 2 tile-cull + 2 intersect launches
-        # (slowest tiles on their own stream), remap per eye
-        "gpu_launches": args.steps * 8,
+        # per frame (ncu launch list): block cull, tile order, tile cull + retry pass + intersect for
+        # the slowest tiles and for the rest, remap per eye
+        "gpu_launches": args.steps * 10,
         "clocks": ck,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -812,7 +810,6 @@ def run_foveated(args):
     rc.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kernel_ms, stage_ms = [], []
     clocks = Clocks(local)
     if dist:
         dist.barrier()
@@ -827,11 +824,15 @@ def run_foveated(args):
         rc.render(stream=sp)
         ends[i].record(stream)
         torch.cuda.synchronize()
-        kernel_ms.append([float(x) for x in rc.kernel_times()])
-        stage_ms.append([float(x) for x in cams[0].timings()])
     torch.cuda.synchronize()
     ck = clocks.stop()
     rc.synchronize()
+
+    def fov_frame(k):
+        for c in cams:
+            c.set_eye_dir(saccade(frame + k))
+        rc.render(stream=sp)
+    kernel_ms, stage_ms = launch_times(rc, cams[0], fov_frame, flush)
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = max_over_ranks(sum(frame_ms), dist, "cuda")
     value = replica_throughput(samples_per_frame, args.steps, total_ms * 1e-3, world)
@@ -892,8 +893,9 @@ def run_foveated(args):
         "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
                                [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
                                 (4, "resolve"), (5, "total")]},
-        # per frame: block cull, tile order, tile cull + intersect (2 parts), 5 resolve kernels per eye
-        "gpu_launches": args.steps * 16,
+        # per frame (ncu launch list): block cull, tile order, tile cull + retry pass + intersect
+        # (2 parts), 5 resolve kernels per eye
+        "gpu_launches": args.steps * 18,
         "clocks": ck,
     }
     if rank == 0:
@@ -910,6 +912,7 @@ def run_profile_case():
     sc = scenes.scene_c2()
     hv.generate_topology(sc)
     with hv.Raycaster(tri_index_capacity=32 << 20) as rc:
+        rc.set_batch_config(timing=1)
         rc.create_model(sc)
         for l in sc.lights:
             rc.create_light(l)
@@ -939,6 +942,7 @@ def run_profile_case_foveated():
     sc = scenes.scene_c2()
     hv.generate_topology(sc)
     rc, cams, _ = foveated_setup(hv, scenes, sc, False, torch)
+    rc.set_batch_config(timing=1)
     for k in range(3):
         for c in cams:
             c.set_eye_dir(saccade(k))
@@ -949,6 +953,24 @@ def run_profile_case_foveated():
                       "kernel_ms": [float(x) for x in rc.kernel_times()],
                       "list_entries": sum(c.list_total() for c in cams)}))
     rc.close()
+
+
+def launch_times(rc, cam, render, flush, frames=5):
+    """Per-launch device times of the workload's frames: the timed frames run without per-launch
+    events (they cost device time), so these come from `frames` more frames of the same workload
+    rendered right after them with config.timing = 1 (L2 flushed before each, as in the timed
+    loop). Returns ([cull, intersect, block cull, remap/resolve] ms, camera stage ms) per frame."""
+    import torch
+    rc.set_batch_config(timing=1)
+    kernel_ms, stage_ms = [], []
+    for k in range(frames):
+        flush.fill_(k & 0xff)
+        render(k)
+        torch.cuda.synchronize()
+        kernel_ms.append([float(x) for x in rc.kernel_times()])
+        stage_ms.append([float(x) for x in cam.timings()])
+    rc.set_batch_config(timing=0)
+    return kernel_ms, stage_ms
 
 
 def ctypes_stream(stream):

@@ -109,6 +109,8 @@ _sig("hvvr_server_poll", _vp, _p(_abi.Completion), _u32, _p(_u32), C.c_double)
 _sig("hvvr_server_update_vertices", _vp, _vp, _u32, _u32, _vp)
 _sig("hvvr_server_get_stats", _vp, _p(_abi.ServerStats))
 _sig("hvvr_raycaster_read_kernel_times", _vp, _vp)
+_sig("hvvr_raycaster_get_batch_config", _vp, _p(_abi.BatchConfig))
+_sig("hvvr_raycaster_set_batch_config", _vp, _p(_abi.BatchConfig))
 _sig("hvvr_raycaster_read_part_times", _vp, _vp)
 _sig("hvvr_batch_read_part_times", _vp, _vp)
 _sig("hvvr_camera_read_tile_costs", _vp, _vp)
@@ -138,7 +140,7 @@ EXPORTED = [
     "hvvr_batch_autotune", "hvvr_batch_read_timings", "hvvr_batch_read_kernel_times",
     "hvvr_raycaster_read_kernel_times", "hvvr_camera_read_tile_costs", "hvvr_batch_read_stats",
     "hvvr_raycaster_read_part_times", "hvvr_batch_read_part_times", "hvvr_batch_read_counters",
-    "hvvr_raycaster_read_counters",
+    "hvvr_raycaster_read_counters", "hvvr_raycaster_get_batch_config", "hvvr_raycaster_set_batch_config",
     "hvvr_camera_read_foveated_frame", "hvvr_camera_read_foveated_resolve", "hvvr_foveated_frame_matrices",
     "hvvr_camera_read_polar_textures",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
@@ -485,6 +487,20 @@ class Raycaster:
         _check(_lib.hvvr_raycaster_read_kernel_times(self.handle, t.ctypes.data))
         return t
 
+    def batch_config(self):
+        """the configuration of the batch behind render()"""
+        cfg = _abi.BatchConfig()
+        _check(_lib.hvvr_raycaster_get_batch_config(self.handle, C.byref(cfg)))
+        return cfg
+
+    def set_batch_config(self, cfg=None, **kw):
+        """set the configuration of the batch behind render(): cfg, or the current one with the
+        keyword fields changed (e.g. timing=1 for per-stage, kernel and part times)"""
+        cfg = cfg if cfg is not None else self.batch_config()
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        _check(_lib.hvvr_raycaster_set_batch_config(self.handle, C.byref(cfg)))
+
     def counters(self):
         """the last frame's counters: list pool entries, retried tiles, status, views, list entries
         that passed the intersect's per-tile tests"""
@@ -605,7 +621,7 @@ class Batch:
 
     def timings(self):
         """device ms of the last frame: total, block cull, first tile cull, rest of cull +
-        intersect/shade, remap + copies (stages 0 for a graph replay)"""
+        intersect/shade, remap + copies (stages 0 unless config.timing is 1)"""
         t = np.zeros(5, dtype=np.float32)
         _check(_lib.hvvr_batch_read_timings(self.handle, t.ctypes.data))
         return t

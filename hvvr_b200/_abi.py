@@ -99,7 +99,8 @@ class TileCullArgs(C.Structure):
 class BatchConfig(C.Structure):
     """hvvr_batch_config: knobs of a frame batch (set by hand or by hvvr_batch_autotune)."""
     _fields_ = [("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32), ("tri_index_capacity", C.c_uint64),
-                ("use_graph", C.c_uint32), ("frame_ms", C.c_float), ("tile_stack_entries", C.c_uint32)]
+                ("use_graph", C.c_uint32), ("frame_ms", C.c_float), ("tile_stack_entries", C.c_uint32),
+                ("timing", C.c_uint32)]
 
 
 class ServerConfig(C.Structure):

@@ -577,6 +577,7 @@ void batchConfigDefault(hvvr_batch_config* c) {
     c->use_graph = 1;
     c->frame_ms = 0.0f;
     c->tile_stack_entries = 0;
+    c->timing = 0;
 }
 
 int checkConfig(const hvvr_batch_config& c) {
@@ -586,6 +587,7 @@ int checkConfig(const hvvr_batch_config& c) {
     if (c.tri_index_capacity == 0 || chunks > 0xfffffff0ull) return fail(HVVR_ERR_INVALID, "bad tri_index_capacity");
     if (c.tile_stack_entries && (c.tile_stack_entries < 8 || c.tile_stack_entries > kTileStack))
         return fail(HVVR_ERR_INVALID, "tile_stack_entries must be 0 or in [8, 256]");
+    if (c.timing > 1) return fail(HVVR_ERR_INVALID, "timing must be 0 or 1");
     return HVVR_OK;
 }
 
@@ -666,13 +668,20 @@ uint32_t heavyTiles(const hvvr_batch* b, uint32_t n) {
     return std::max<uint32_t>(1u, n / b->cfg.heavy_divisor);
 }
 
-// Enqueues one frame on st (and the side streams, forked from and joined back to st).
-// timing: record the stage events (not inside a graph capture).
-int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing) {
-    if (timing) CUDA_TRY(cudaEventRecord(b->ev[0], st));
+// a stage-timing event: inside a stream capture it must be recorded as an external event so
+// that the graph records it on every replay (a plain record only orders the capture)
+cudaError_t recordStage(cudaEvent_t ev, cudaStream_t s, bool capturing) {
+    return capturing ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal) : cudaEventRecord(ev, s);
+}
+
+// Enqueues one frame on st (and the side streams, forked from and joined back to st), recording
+// the stage and per-part events (as graph nodes when capturing).
+int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool capturing) {
+    const bool stages = b->cfg.timing != 0;
+    CUDA_TRY(recordStage(b->ev[0], st, capturing));
     CUDA_TRY(cudaMemsetAsync(fr.counters, 0, kCounterWords * sizeof(uint32_t), st));
     CUDA_TRY(launchBlockCull(fr, st));
-    if (timing) CUDA_TRY(cudaEventRecord(b->ev[1], st));
+    if (stages) CUDA_TRY(recordStage(b->ev[1], st, capturing));
     CUDA_TRY(launchTileOrder(fr, st));
     CUDA_TRY(cudaEventRecord(b->forkEv, st));
     bool first = true;
@@ -691,20 +700,18 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
             const uint32_t p0 = part ? rs + heavy : rs, pn = part ? n - heavy : heavy;
             cudaStream_t ps = b->side[k];
             CUDA_TRY(cudaStreamWaitEvent(ps, b->forkEv, 0));
-            if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][0], ps));
+            if (stages) CUDA_TRY(recordStage(b->kev[k][0], ps, capturing));
             CUDA_TRY(launchTileCull(fr, fr.order, p0, pn, fr.counters + kQueueBase + kQueueWords * k,
                                     b->cfg.tile_cull_warps, b->cfg.tile_stack_entries, ps));
-            if (timing) CUDA_TRY(cudaEventRecord(b->kev[k][1], ps));
-            if (timing && part == 1 && first) CUDA_TRY(cudaEventRecord(b->ev[2], ps));
+            if (stages) CUDA_TRY(recordStage(b->kev[k][1], ps, capturing));
+            if (stages && part == 1 && first) CUDA_TRY(recordStage(b->ev[2], ps, capturing));
             if (lens) {
                 CUDA_TRY(cudaEventRecord(b->cullEv[k], ps));
                 continue;
             }
             CUDA_TRY(launchIntersectShade(fr, msaa, b->fpStrict, false, fr.order, p0, pn, ps));
-            if (timing) {
-                CUDA_TRY(cudaEventRecord(b->kev[k][2], ps));
-                b->kevUsed[k] = true;
-            }
+            if (stages) CUDA_TRY(recordStage(b->kev[k][2], ps, capturing));
+            b->kevUsed[k] = true;
             CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
             CUDA_TRY(cudaStreamWaitEvent(st, b->doneEv[k], 0));
         }
@@ -722,21 +729,19 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
             cudaStream_t ps = b->side[k];
             CUDA_TRY(cudaStreamWaitEvent(ps, b->rankEv, 0));
             CUDA_TRY(launchIntersectShade(fr, 1u << (r % 6), b->fpStrict, true, fr.order, b->rateStart[r], n, ps));
-            if (timing) {
-                CUDA_TRY(cudaEventRecord(b->kev[k][2], ps));
-                b->kevUsed[k] = true;
-            }
+            if (stages) CUDA_TRY(recordStage(b->kev[k][2], ps, capturing));
+            b->kevUsed[k] = true;
             CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
             CUDA_TRY(cudaStreamWaitEvent(st, b->doneEv[k], 0));
         }
     }
-    if (timing) CUDA_TRY(cudaEventRecord(b->ev[3], st));
+    if (stages) CUDA_TRY(recordStage(b->ev[3], st, capturing));
     for (uint32_t i = 0; i < b->views.size(); i++) {
         const hvvr_camera* c = b->views[i].cam;
         if (c->foveated) CUDA_TRY(launchFoveatedResolve(fr, i, c->fovStatic, st));
         else CUDA_TRY(launchRemap(c->dev, st));
     }
-    if (timing) CUDA_TRY(cudaEventRecord(b->ev[4], st));
+    if (stages) CUDA_TRY(recordStage(b->ev[4], st, capturing));
     CUDA_TRY(cudaMemcpyAsync(b->hostCounters, fr.counters, kCounterWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     for (const auto& v : b->views) {
         const hvvr_camera* c = v.cam;
@@ -747,7 +752,7 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool timing
                                        d.height, cudaMemcpyDeviceToHost, st));
         }
     }
-    if (timing) CUDA_TRY(cudaEventRecord(b->ev[5], st));
+    CUDA_TRY(recordStage(b->ev[5], st, capturing));
     return HVVR_OK;
 }
 
@@ -957,12 +962,12 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     if (b->cfg.use_graph && b->costValid && capturable) {
         std::vector<uint64_t> gkey = b->layoutKey;
         const uint64_t extra[] = {b->cfg.tile_cull_warps, b->cfg.heavy_divisor, b->poolChunks, strict ? 1u : 0u,
-                                  uint64_t(uintptr_t(st)), b->cfg.tile_stack_entries};
-        gkey.insert(gkey.end(), extra, extra + 6);
+                                  uint64_t(uintptr_t(st)), b->cfg.tile_stack_entries, b->cfg.timing};
+        gkey.insert(gkey.end(), extra, extra + 7);
         if (!b->graph || gkey != b->graphKey) {
             dropGraph(b);
             CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-            const int r = enqueueFrame(b, fr, st, false);
+            const int r = enqueueFrame(b, fr, st, true);
             cudaGraph_t g = nullptr;
             const cudaError_t e = cudaStreamEndCapture(st, &g);
             if (r != HVVR_OK) {
@@ -976,14 +981,11 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
             CUDA_TRY(ie);
             b->graphKey = gkey;
         }
-        CUDA_TRY(cudaEventRecord(b->ev[0], st));
         CUDA_TRY(cudaGraphLaunch(b->graph, st));
-        CUDA_TRY(cudaEventRecord(b->ev[5], st));
-        b->stageTimes = false;
     } else {
-        TRY(enqueueFrame(b, fr, st, true));
-        b->stageTimes = true;
+        TRY(enqueueFrame(b, fr, st, false));
     }
+    b->stageTimes = b->cfg.timing != 0;
     for (hvvr_camera* c : cams) {
         c->lastBatch = b;
         c->rendered = true;
@@ -1070,19 +1072,36 @@ int hvvr_raycaster_set_scene_dirty(hvvr_raycaster* rc) {
     return HVVR_OK;
 }
 
-int hvvr_raycaster_render(hvvr_raycaster* rc, double elapsed_time, void* stream) {
-    (void)elapsed_time;
-    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+// the raycaster's own batch (made on first use)
+hvvr_batch* ownBatch(hvvr_raycaster* rc) {
     if (!rc->own) {
         rc->own = std::make_unique<hvvr_batch>();
         hvvr_batch* b = rc->own.get();
         b->rcs.push_back(rc);
         b->internal = true;
         batchConfigDefault(&b->cfg);
-        b->cfg.use_graph = 0; // per-stage timings stay available
         if (rc->spec.tri_index_capacity) b->cfg.tri_index_capacity = rc->spec.tri_index_capacity;
     }
-    return renderBatch(rc->own.get(), stream ? static_cast<cudaStream_t>(stream) : rc->stream);
+    return rc->own.get();
+}
+
+int hvvr_raycaster_render(hvvr_raycaster* rc, double elapsed_time, void* stream) {
+    (void)elapsed_time;
+    if (!rc) return fail(HVVR_ERR_INVALID, "NULL raycaster");
+    return renderBatch(ownBatch(rc), stream ? static_cast<cudaStream_t>(stream) : rc->stream);
+}
+
+int hvvr_raycaster_get_batch_config(hvvr_raycaster* rc, hvvr_batch_config* cfg) {
+    if (!rc || !cfg) return fail(HVVR_ERR_INVALID, "NULL argument");
+    *cfg = ownBatch(rc)->cfg;
+    return HVVR_OK;
+}
+
+int hvvr_raycaster_set_batch_config(hvvr_raycaster* rc, const hvvr_batch_config* cfg) {
+    if (!rc || !cfg) return fail(HVVR_ERR_INVALID, "NULL argument");
+    TRY(checkConfig(*cfg));
+    ownBatch(rc)->cfg = *cfg; // the pool follows tri_index_capacity on the next frame
+    return HVVR_OK;
 }
 
 int hvvr_raycaster_synchronize(hvvr_raycaster* rc) {
@@ -1213,7 +1232,7 @@ int hvvr_batch_read_timings(const hvvr_batch* b, float* ms5) {
 namespace {
 int kernelTimes(const hvvr_batch* b, float* ms4) {
     if (!b || !b->counterValid) return fail(HVVR_ERR_STATE, "no frame rendered");
-    if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was a graph replay (no per-launch events)");
+    if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was rendered without per-launch events (config.timing = 0)");
     CUDA_TRY(cudaEventSynchronize(b->ev[5]));
     float cull = 0.0f, isect = 0.0f, t = 0.0f;
     for (uint32_t k = 0; k < 2 * kRateClasses; k++) {
@@ -1245,7 +1264,7 @@ static int frameCounters(const hvvr_batch* b, uint64_t* out, uint32_t count) {
 
 static int partTimes(const hvvr_batch* b, float* ms72) {
     if (!b || !b->counterValid) return fail(HVVR_ERR_STATE, "no frame rendered");
-    if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was a graph replay (no per-launch events)");
+    if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was rendered without per-launch events (config.timing = 0)");
     CUDA_TRY(cudaEventSynchronize(b->ev[5]));
     for (uint32_t k = 0; k < 2 * kRateClasses; k++) {
         float* o = ms72 + 3 * k;

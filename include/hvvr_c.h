@@ -314,6 +314,9 @@ typedef struct {
     float frame_ms;               /* autotune result: median device time of a frame */
     uint32_t tile_stack_entries;  /* traversal stack of the main tile-cull pass, 0 (= 256) or 8..256;
                                      tiles that need more are culled again with 4096 entries */
+    uint32_t timing;              /* 1: record per-stage and per-launch events (the stage, kernel and
+                                     part read-backs); they cost device time (about 0.4 ms of a 6 ms
+                                     stereo frame). 0 (default): the frame's start and end only */
 } hvvr_batch_config;
 void hvvr_batch_config_default(hvvr_batch_config* cfg);
 int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,
@@ -334,18 +337,21 @@ int hvvr_batch_set_config(hvvr_batch* batch, const hvvr_batch_config* cfg);
  * largest list total seen (at least 1M entries). Writes the chosen config to *out. */
 int hvvr_batch_autotune(hvvr_batch* batch, uint32_t frames, hvvr_batch_config* out);
 /* device ms of the last frame: [0] total; [1] block cull, [2] first tile cull, [3] rest of
- * cull + intersect/shade, [4] remap + copies - stages are 0 when the frame was a graph replay */
+ * cull + intersect/shade, [4] remap + copies - stages are 0 unless config.timing is 1 */
 int hvvr_batch_read_timings(const hvvr_batch* batch, float* ms5);
 /* device ms of the last frame's launches, summed over the launches of the frame (launches on
  * different streams overlap, so the sum can exceed the frame time): [0] tile cull, [1]
- * intersect/shade, [2] block cull, [3] remap. Not available after a graph replay. */
+ * intersect/shade, [2] block cull, [3] remap. Needs config.timing = 1 for that frame. */
 int hvvr_batch_read_kernel_times(const hvvr_batch* batch, float* ms4);
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
+/* the configuration of the batch behind hvvr_raycaster_render (default: hvvr_batch_config_default
+ * with the spec's tri_index_capacity) */
+int hvvr_raycaster_get_batch_config(hvvr_raycaster* rc, hvvr_batch_config* cfg);
+int hvvr_raycaster_set_batch_config(hvvr_raycaster* rc, const hvvr_batch_config* cfg);
 /* The last frame's launch timeline per part: rate class r (log2 MSAA, + 6 for thin-lens views)
  * runs as part 2r (its slowest tiles by the previous frame's cost, on a high-priority stream)
  * and part 2r+1 (the rest). ms72[3 * part + i] = tile cull start, tile cull end, intersect/shade
- * end, in ms from the frame start; -1 for parts that did not run. Not available after a graph
- * replay. */
+ * end, in ms from the frame start; -1 for parts that did not run. Needs config.timing = 1. */
 int hvvr_batch_read_part_times(const hvvr_batch* batch, float* ms72);
 int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72);
 /* counters of the last frame: [0] list-pool entries taken (whole chunks), [1] tiles culled
