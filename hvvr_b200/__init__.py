@@ -79,6 +79,16 @@ _sig("hvvr_scene_read_nodes", _vp, _vp)
 _sig("hvvr_scene_read_triangles", _vp, _vp)
 _sig("hvvr_generate_topology", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32))
 _sig("hvvr_grid_samples", _u32, _u32, _vp)
+_sig("hvvr_scene_file_load", C.c_char_p, _p(_vp))
+_sig("hvvr_scene_file_counts", _vp, _p(_u32), _p(_u32), _p(_u32))
+_sig("hvvr_scene_file_mesh", _vp, _u32, _p(_abi.MeshData), _p(_abi.Transform))
+_sig("hvvr_scene_file_light", _vp, _u32, _p(_abi.LightUnion))
+_sig("hvvr_scene_file_texture", _vp, _u32, _p(_u32), _p(_u32), _p(_u32), _p(_u32), _p(_vp), _p(C.c_uint64))
+_lib.hvvr_scene_file_close.argtypes = [_vp]
+_lib.hvvr_scene_file_close.restype = None
+_sig("hvvr_scene_file_save", C.c_char_p, _vp, _vp, _u32, _vp, _u32)
+_sig("hvvr_samples_load", C.c_char_p, _vp, _u32, _p(_u32))
+_sig("hvvr_samples_save", C.c_char_p, _vp, _u32)
 _sig("hvvr_polar_foveated_layout", _vp, _p(_u32), _p(_u32), _p(_u32), _p(_u32))
 _sig("hvvr_polar_foveated_samples", _vp, _vp, _vp, _vp, _vp)
 _sig("hvvr_tile_cull_static", _vp, _vp, _vp, C.c_uint64, _p(C.c_uint64), _vp)
@@ -133,7 +143,9 @@ EXPORTED = [
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
     "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
-    "hvvr_polar_foveated_layout", "hvvr_polar_foveated_samples",
+    "hvvr_polar_foveated_layout", "hvvr_polar_foveated_samples", "hvvr_scene_file_load", "hvvr_scene_file_counts",
+    "hvvr_scene_file_mesh", "hvvr_scene_file_light", "hvvr_scene_file_texture", "hvvr_scene_file_close",
+    "hvvr_scene_file_save", "hvvr_samples_load", "hvvr_samples_save",
     "hvvr_tile_cull_static", "hvvr_batch_config_default", "hvvr_batch_create", "hvvr_batch_create_views",
     "hvvr_batch_destroy", "hvvr_model_update_vertices_device",
     "hvvr_batch_render", "hvvr_batch_synchronize", "hvvr_batch_get_config", "hvvr_batch_set_config",
@@ -220,6 +232,80 @@ def foveated_frame_matrices(xf, eye_dir, sample_bounds, viewport, history=None):
                                              out["eye_to_sample_prev"].ctypes.data))
     out["history"] = (w2ep, ep2sp)
     return out
+
+
+def load_scene_file(path):
+    """A scene file in the reference's binary format (model_import::loadBin): dict with "meshes"
+    (a scenes.Scene per mesh, its topology in .nodes and model transform in .transform), "lights"
+    (LightUnion list) and "textures" (dicts of format, width, height, stride, texels)."""
+    from . import scenes
+    h = _vp()
+    _check(_lib.hvvr_scene_file_load(os.fsencode(path), C.byref(h)))
+    try:
+        nt, nl, nm = _u32(0), _u32(0), _u32(0)
+        _check(_lib.hvvr_scene_file_counts(h, C.byref(nt), C.byref(nl), C.byref(nm)))
+        lights = []
+        for i in range(nl.value):
+            l = _abi.LightUnion()
+            _check(_lib.hvvr_scene_file_light(h, i, C.byref(l)))
+            lights.append(l)
+        meshes = []
+        for i in range(nm.value):
+            md, xf = _abi.MeshData(), _abi.Transform()
+            _check(_lib.hvvr_scene_file_mesh(h, i, C.byref(md), C.byref(xf)))
+
+            def arr(ptr, n, dt):
+                if not n:
+                    return np.zeros(0, dt)
+                return np.frombuffer(C.string_at(ptr, n * dt.itemsize), dt).copy()
+            sc = scenes.Scene(arr(md.verts, md.vert_count, _abi.VERTEX_DTYPE),
+                              arr(md.tri_shade, md.tri_count, _abi.TRISHADE_DTYPE),
+                              arr(md.materials, md.material_count, _abi.MATERIAL_DTYPE), lights)
+            sc.nodes = arr(md.nodes, md.node_count, _abi.TOPO_DTYPE) if md.node_count else None
+            sc.transform = xf
+            meshes.append(sc)
+        textures = []
+        for i in range(nt.value):
+            fmt, w, hh, st, ptr, nb = _u32(0), _u32(0), _u32(0), _u32(0), _vp(), C.c_uint64(0)
+            _check(_lib.hvvr_scene_file_texture(h, i, C.byref(fmt), C.byref(w), C.byref(hh), C.byref(st), C.byref(ptr),
+                                                C.byref(nb)))
+            textures.append({"format": fmt.value, "width": w.value, "height": hh.value, "stride": st.value,
+                             "texels": np.frombuffer(C.string_at(ptr, nb.value), np.uint8).copy()})
+        return {"meshes": meshes, "lights": lights, "textures": textures}
+    finally:
+        _lib.hvvr_scene_file_close(h)
+
+
+def save_scene_file(path, meshes, lights=()):
+    """Writes scenes.Scene meshes (topology from .nodes when set, transform from .transform or
+    identity) and lights in the reference's binary scene format."""
+    mds = (_abi.MeshData * max(1, len(meshes)))()
+    xfs = (_abi.Transform * max(1, len(meshes)))()
+    keep = []
+    for i, sc in enumerate(meshes):
+        nodes = sc.nodes if sc.nodes is not None else np.zeros(0, _abi.TOPO_DTYPE)
+        arrays = [np.ascontiguousarray(a) for a in (sc.verts, sc.tri_shade, nodes, sc.materials)]
+        keep.append(arrays)
+        mds[i] = _abi.MeshData(_abi.ptr(arrays[0]), len(arrays[0]), _abi.ptr(arrays[1]), len(arrays[1]),
+                               _abi.ptr(arrays[2]) if len(arrays[2]) else None, len(arrays[2]),
+                               _abi.ptr(arrays[3]), len(arrays[3]))
+        xfs[i] = getattr(sc, "transform", None) or _abi.transform()
+    ls = (_abi.LightUnion * max(1, len(lights)))(*lights)
+    _check(_lib.hvvr_scene_file_save(os.fsencode(path), mds, xfs, len(meshes), ls, len(lights)))
+
+
+def load_samples(path):
+    """A sample file in the reference's format (loadSamples): SAMPLE_DTYPE array."""
+    n = _u32(0)
+    _check(_lib.hvvr_samples_load(os.fsencode(path), None, 0, C.byref(n)))
+    out = np.zeros(n.value, dtype=_abi.SAMPLE_DTYPE)
+    _check(_lib.hvvr_samples_load(os.fsencode(path), out.ctypes.data, n.value, C.byref(n)))
+    return out
+
+
+def save_samples(path, samples):
+    samples = np.ascontiguousarray(samples, dtype=_abi.SAMPLE_DTYPE)
+    _check(_lib.hvvr_samples_save(os.fsencode(path), samples.ctypes.data, len(samples)))
 
 
 def grid_samples(width, height):

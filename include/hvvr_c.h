@@ -26,7 +26,7 @@ extern "C" {
 enum {
     HVVR_OK = 0,
     HVVR_ERR_INVALID = 1,   /* bad argument or unsupported configuration */
-    HVVR_ERR_NOT_FOUND = 2, /* destroy of an object this raycaster does not own */
+    HVVR_ERR_NOT_FOUND = 2, /* destroy of an object this raycaster does not own; a file that cannot be opened */
     HVVR_ERR_CUDA = 3,      /* a CUDA runtime call failed */
     HVVR_ERR_OOM = 4,       /* device allocation failed */
     HVVR_ERR_OVERFLOW = 5,  /* a per-frame capacity (triangle-index pool, traversal stack) was exceeded */
@@ -282,6 +282,33 @@ int hvvr_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr
                            uint32_t* node_count);
 /* getGridSamples(width, height) (libraries/hvvr/raycaster/samples.cpp:21-42) */
 int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
+
+/* ---------------------------------------------------------------- scene and sample files
+ * The reference's binary scene files (model_import::loadBin / saveBin,
+ * libraries/hvvr/samples_shared/model_import_bin.cpp:15-168): header {version 1, texture,
+ * light and mesh counts}; per texture {TextureFormat, width, height, stride} and its texels
+ * (getTextureSize, libraries/hvvr/raycaster/texture.h:56-76); the lights; per mesh {transform,
+ * vertex, triangle, node and material counts} and those arrays, each record byte-compatible
+ * with the types above. A loaded file owns its arrays until hvvr_scene_file_close; a short or
+ * malformed file is HVVR_ERR_INVALID. Textures are read and handed back as bytes (this library
+ * shades untextured materials). */
+typedef struct hvvr_scene_file hvvr_scene_file;
+int hvvr_scene_file_load(const char* path, hvvr_scene_file** out);
+int hvvr_scene_file_counts(const hvvr_scene_file* file, uint32_t* textures, uint32_t* lights, uint32_t* meshes);
+/* mesh i as borrowed arrays (valid until close) and its model transform */
+int hvvr_scene_file_mesh(const hvvr_scene_file* file, uint32_t i, hvvr_mesh_data* mesh, hvvr_transform* xf);
+int hvvr_scene_file_light(const hvvr_scene_file* file, uint32_t i, hvvr_light_union* light);
+/* texture i: the reference's TextureFormat value, size, stride in elements and texel bytes */
+int hvvr_scene_file_texture(const hvvr_scene_file* file, uint32_t i, uint32_t* format, uint32_t* width,
+                            uint32_t* height, uint32_t* stride, const void** texels, uint64_t* bytes);
+void hvvr_scene_file_close(hvvr_scene_file* file);
+/* writes meshes (with their transforms) and lights, no textures, in the same format */
+int hvvr_scene_file_save(const char* path, const hvvr_mesh_data* meshes, const hvvr_transform* transforms,
+                         uint32_t mesh_count, const hvvr_light_union* lights, uint32_t light_count);
+/* sample files (loadSamples / saveSamples, libraries/hvvr/raycaster/samples.cpp:161-187):
+ * {magic 0x0CD1, version 0, reserved, count} then the samples. samples == NULL: count only. */
+int hvvr_samples_load(const char* path, hvvr_sample* samples, uint32_t capacity, uint32_t* count);
+int hvvr_samples_save(const char* path, const hvvr_sample* samples, uint32_t count);
 /* The polar foveated sample set of spec's foveated parameters (spec NULL: defaults), as the
  * reference's polarSpaceFoveatedSetup builds it: getEyeSpacePolarFoveatedSamples
  * (libraries/hvvr/raycaster/samples.cpp:44-142), generateRemapForFoveatedSamples

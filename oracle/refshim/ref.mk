@@ -4,13 +4,14 @@
 REF_ROOT ?= /root/reference
 RC = $(REF_ROOT)/libraries/hvvr/raycaster
 SH = $(REF_ROOT)/libraries/hvvr/shared
+SS = $(REF_ROOT)/libraries/hvvr/samples_shared
 CUDA_INC ?= /usr/local/cuda/include
 CXX ?= g++
 # -ffp-contract=off: the reference's host code is built without contraction (MSVC /fp:precise)
 REF_FLAGS = -std=c++17 -O2 -fPIC -mavx2 -mfma -mf16c -mbmi -mbmi2 -ffp-contract=off -fpermissive -w -pthread \
-            -include refshim/compat/hvvr_gcc_compat.h -Irefshim/compat -I$(SH) -I$(RC) -I$(CUDA_INC)
+            -include refshim/compat/hvvr_gcc_compat.h -Irefshim/compat -I$(SH) -I$(RC) -I$(SS) -I$(CUDA_INC)
 REF_SRCS = $(RC)/traverse_avx.cpp $(RC)/sample_hierarchy.cpp $(RC)/samples.cpp $(RC)/camera.cpp \
-           $(RC)/foveated.cpp $(SH)/bvh.cpp $(SH)/debug.cpp
+           $(RC)/foveated.cpp $(SH)/bvh.cpp $(SH)/debug.cpp $(SS)/model_import_bin.cpp
 OBJS = $(patsubst %.cpp,_ref/obj/%.o,$(notdir $(REF_SRCS))) _ref/obj/frusta.o _ref/obj/ref_harness.o _ref/obj/ref_stubs.o
 
 # -Bsymbolic: the host stand-ins for the CUDA runtime calls (ref_stubs.cpp) must bind inside this
@@ -22,6 +23,9 @@ _ref/obj/%.o: $(RC)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
 	@mkdir -p _ref/obj
 	$(CXX) $(REF_FLAGS) -c $< -o $@
 _ref/obj/%.o: $(SH)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
+	@mkdir -p _ref/obj
+	$(CXX) $(REF_FLAGS) -c $< -o $@
+_ref/obj/%.o: $(SS)/%.cpp refshim/compat/hvvr_gcc_compat.h refshim/compat/avx.h
 	@mkdir -p _ref/obj
 	$(CXX) $(REF_FLAGS) -c $< -o $@
 # frusta.cu holds host code only on the path used (ComputeEyeSpaceFrusta); compiled as C++

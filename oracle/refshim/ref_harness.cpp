@@ -578,3 +578,90 @@ extern "C" int ref_foveated_frame_matrices(const hvvr_transform* cameraToWorldXf
     memcpy(eyePrevToSamplePrev9, &eyePreviousToSamplePrevious, 36);
     return 0;
 }
+
+// ------------------------------------------------------------------ scene and sample files
+// The reference's own model_import::saveBin / loadBin (SS/model_import_bin.cpp) and
+// saveSamples / loadSamples (RC/samples.cpp:161-187), for checking the library's file formats
+// byte for byte in both directions.
+#include "model_import.h"
+namespace hvvr {
+void saveSamples(const std::vector<hvvr::Sample>& samples, const std::string& filename);
+}
+static_assert(sizeof(hvvr::ShadingVertex) == 32 && sizeof(hvvr::PrecomputedTriangleShade) == 16 &&
+                  sizeof(hvvr::SimpleMaterial) == 64 && sizeof(hvvr::LightUnion) == 56 &&
+                  sizeof(hvvr::transform) == 32 && sizeof(hvvr::TopologyNode) == 32,
+              "record layouts");
+
+// saveBin of the given meshes and lights, plus one r8g8b8a8_unorm texture when texels != NULL
+extern "C" int ref_bin_save(const char* path, const hvvr_mesh_data* meshes, const hvvr_transform* xfs,
+                            uint32_t meshCount, const hvvr_light_union* lights, uint32_t lightCount,
+                            const uint8_t* texels, uint32_t texWidth, uint32_t texHeight) {
+    model_import::Model model;
+    if (texels) {
+        hvvr::TextureData td = {};
+        td.format = hvvr::TextureFormat::r8g8b8a8_unorm;
+        td.width = texWidth;
+        td.height = texHeight;
+        td.strideElements = texWidth;
+        uint8_t* data = new uint8_t[size_t(texWidth) * texHeight * 4];
+        memcpy(data, texels, size_t(texWidth) * texHeight * 4);
+        td.data = data;
+        model.textures.emplace_back(model_import::Texture(td));
+    }
+    for (uint32_t i = 0; i < lightCount; i++) model.lights.push_back(*reinterpret_cast<const hvvr::LightUnion*>(&lights[i]));
+    for (uint32_t i = 0; i < meshCount; i++) {
+        const hvvr_mesh_data& md = meshes[i];
+        model_import::Mesh mesh;
+        mesh.transform = *reinterpret_cast<const hvvr::transform*>(&xfs[i]);
+        const auto* v = reinterpret_cast<const hvvr::ShadingVertex*>(md.verts);
+        const auto* t = reinterpret_cast<const hvvr::PrecomputedTriangleShade*>(md.tri_shade);
+        const auto* n = reinterpret_cast<const hvvr::TopologyNode*>(md.nodes);
+        const auto* m = reinterpret_cast<const hvvr::SimpleMaterial*>(md.materials);
+        mesh.data.verts.assign(v, v + md.vert_count);
+        mesh.data.triShade.assign(t, t + md.tri_count);
+        if (md.node_count) mesh.data.nodes.assign(n, n + md.node_count);
+        mesh.data.materials.assign(m, m + md.material_count);
+        model.meshes.emplace_back(std::move(mesh));
+    }
+    return model_import::saveBin(path, model) ? 0 : 1;
+}
+
+// loadBin: counts[4] = {textures, lights, meshes, total bytes of the mesh arrays}; with out != NULL
+// the lights then every mesh's transform and arrays are packed into out in file order
+extern "C" int ref_bin_load(const char* path, uint64_t* counts, uint8_t* out) {
+    model_import::Model model;
+    if (!model_import::loadBin(path, model)) return 1;
+    uint64_t bytes = model.lights.size() * sizeof(hvvr::LightUnion);
+    for (const auto& m : model.meshes)
+        bytes += sizeof(hvvr::transform) + m.data.verts.size() * 32 + m.data.triShade.size() * 16 +
+                 m.data.nodes.size() * 32 + m.data.materials.size() * 64;
+    counts[0] = model.textures.size();
+    counts[1] = model.lights.size();
+    counts[2] = model.meshes.size();
+    counts[3] = bytes;
+    if (!out) return 0;
+    auto put = [&](const void* p, size_t n) { memcpy(out, p, n); out += n; };
+    put(model.lights.data(), model.lights.size() * sizeof(hvvr::LightUnion));
+    for (const auto& m : model.meshes) {
+        put(&m.transform, sizeof(hvvr::transform));
+        put(m.data.verts.data(), m.data.verts.size() * 32);
+        put(m.data.triShade.data(), m.data.triShade.size() * 16);
+        put(m.data.nodes.data(), m.data.nodes.size() * 32);
+        put(m.data.materials.data(), m.data.materials.size() * 64);
+    }
+    return 0;
+}
+
+extern "C" int ref_samples_save(const char* path, const hvvr_sample* samples, uint32_t count) {
+    const auto* s = reinterpret_cast<const hvvr::Sample*>(samples);
+    hvvr::saveSamples(std::vector<hvvr::Sample>(s, s + count), path);
+    return 0;
+}
+
+extern "C" int ref_samples_load(const char* path, hvvr_sample* out, uint32_t capacity, uint32_t* count) {
+    hvvr::DynamicArray<hvvr::Sample> samples;
+    hvvr::loadSamples(samples, path);
+    *count = uint32_t(samples.size());
+    if (out && capacity >= samples.size()) memcpy(out, samples.data(), samples.size() * sizeof(hvvr::Sample));
+    return 0;
+}
