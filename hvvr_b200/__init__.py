@@ -12,7 +12,9 @@ import numpy as np
 
 from . import _abi
 from ._abi import (HVVR_CAPTURE_HITS, HVVR_FP_FMA, HVVR_FP_STRICT, HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA,  # noqa: F401
-                   HVVR_OK)
+                   HVVR_OK, HVVR_TEXTURE_R32_FLOAT, HVVR_TEXTURE_RGBA8_UNORM, HVVR_TEXTURE_RGBA8_UNORM_SRGB,
+                   HVVR_TEXTURE_RGBA16_FLOAT, HVVR_TEXTURE_RGBA16_UNORM, HVVR_TEXTURE_RGBA32_FLOAT,
+                   HVVR_TEXTURE_R11G11B10_FLOAT)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("HVVR_B200_LIB") or os.path.join(_HERE, "_lib", "libhvvr_b200.so")
@@ -49,6 +51,11 @@ _sig("hvvr_model_set_transform", _vp, _p(_abi.Transform))
 _sig("hvvr_model_update_vertices", _vp, _vp, _u32)
 _sig("hvvr_light_create", _vp, _p(_abi.LightUnion), _p(_vp))
 _sig("hvvr_light_destroy", _vp, _vp)
+_sig("hvvr_texture_create", _vp, _p(_abi.TextureData), _p(_vp))
+_sig("hvvr_texture_destroy", _vp, _vp)
+_sig("hvvr_texture_get_id", _vp, _p(_u32))
+_sig("hvvr_texture_read_level", _vp, _u32, _vp, C.c_uint64, _p(_u32), _p(_u32))
+_sig("hvvr_texture_sample", _vp, _u32, _vp, _vp)
 _sig("hvvr_camera_create", _vp, _p(_abi.FloatRect), C.c_float, _p(_vp))
 _sig("hvvr_camera_destroy", _vp, _vp)
 _sig("hvvr_camera_set_enabled", _vp, C.c_int)
@@ -134,7 +141,8 @@ EXPORTED = [
     "hvvr_last_error", "hvvr_version", "hvvr_spec_default", "hvvr_raycaster_create", "hvvr_raycaster_destroy",
     "hvvr_raycaster_set_scene_dirty", "hvvr_raycaster_render", "hvvr_raycaster_synchronize", "hvvr_model_create",
     "hvvr_model_destroy", "hvvr_model_set_transform", "hvvr_model_update_vertices", "hvvr_light_create",
-    "hvvr_light_destroy", "hvvr_camera_create", "hvvr_camera_destroy", "hvvr_camera_set_enabled",
+    "hvvr_light_destroy", "hvvr_texture_create", "hvvr_texture_destroy", "hvvr_texture_get_id",
+    "hvvr_texture_read_level", "hvvr_texture_sample", "hvvr_camera_create", "hvvr_camera_destroy", "hvvr_camera_set_enabled",
     "hvvr_camera_set_viewport", "hvvr_camera_set_lens", "hvvr_camera_set_aperture", "hvvr_camera_set_focal_depth",
     "hvvr_camera_set_eye_dir", "hvvr_camera_set_spherical_warp", "hvvr_camera_set_render_target",
     "hvvr_camera_set_samples", "hvvr_camera_set_camera_to_world", "hvvr_camera_set_msaa",
@@ -330,6 +338,38 @@ class Model:
         _check(_lib.hvvr_model_update_vertices_device(self.handle, first, count, _vp(device_ptr), stream))
 
 
+_TEXEL_DTYPE = {HVVR_TEXTURE_RGBA8_UNORM_SRGB: (np.uint8, 4), HVVR_TEXTURE_RGBA8_UNORM: (np.uint8, 4),
+                HVVR_TEXTURE_RGBA16_UNORM: (np.uint16, 4), HVVR_TEXTURE_RGBA32_FLOAT: (np.float32, 4),
+                HVVR_TEXTURE_RGBA16_FLOAT: (np.float16, 4), HVVR_TEXTURE_R32_FLOAT: (np.float32, 1)}
+
+
+class Texture:
+    """A material texture (Raycaster::createTexture); materials name it by .id."""
+
+    def __init__(self, rc, handle, fmt, width, height):
+        self.rc, self.handle, self.format, self.width, self.height = rc, handle, fmt, width, height
+        i = _u32(0)
+        _check(_lib.hvvr_texture_get_id(handle, C.byref(i)))
+        self.id = i.value
+
+    def read_level(self, level):
+        """Mip level `level` as [h, w, channels] of the format's texel type."""
+        w, h = _u32(0), _u32(0)
+        _check(_lib.hvvr_texture_read_level(self.handle, level, None, 0, C.byref(w), C.byref(h)))
+        dt, ch = _TEXEL_DTYPE[self.format]
+        out = np.zeros((h.value, w.value, ch), dt)
+        _check(_lib.hvvr_texture_read_level(self.handle, level, out.ctypes.data_as(_vp), out.nbytes, C.byref(w),
+                                            C.byref(h)))
+        return out
+
+    def sample(self, q):
+        """ReadTexture at queries q [n, 6] = (u, v, ddx.x, ddx.y, ddy.x, ddy.y): [n, 4] float32."""
+        q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1, 6)
+        out = np.zeros((len(q), 4), np.float32)
+        _check(_lib.hvvr_texture_sample(self.handle, len(q), q.ctypes.data_as(_vp), out.ctypes.data_as(_vp)))
+        return out
+
+
 class Camera:
     def __init__(self, rc, handle):
         self._rc, self.handle = rc, handle
@@ -504,7 +544,7 @@ class Raycaster:
         h = _vp()
         _check(_lib.hvvr_raycaster_create(C.byref(spec), C.byref(h)))
         self.handle = h
-        self.cameras, self.models, self.lights = [], [], []
+        self.cameras, self.models, self.lights, self.textures = [], [], [], []
         self.batches = []
 
     def close(self):
@@ -542,6 +582,24 @@ class Raycaster:
         _check(_lib.hvvr_light_create(self.handle, C.byref(light), C.byref(h)))
         self.lights.append(h)
         return h
+
+    def create_texture(self, texels, fmt=HVVR_TEXTURE_RGBA8_UNORM_SRGB, width=None, height=None, stride=None):
+        """createTexture(TextureData): texels as [h, w, channels] of the format's texel type, or raw
+        bytes with width, height and stride (in texels) given."""
+        a = np.ascontiguousarray(texels)
+        if width is None:
+            height, width = a.shape[0], a.shape[1]
+        stride = stride if stride is not None else width
+        td = _abi.TextureData(a.ctypes.data, fmt, width, height, stride)
+        h = _vp()
+        _check(_lib.hvvr_texture_create(self.handle, C.byref(td), C.byref(h)))
+        t = Texture(self, h, fmt, width, height)
+        self.textures.append(t)
+        return t
+
+    def destroy_texture(self, tex):
+        _check(_lib.hvvr_texture_destroy(self.handle, tex.handle))
+        self.textures.remove(tex)
 
     def create_camera(self, viewport, aperture=0.0):
         h = _vp()

@@ -76,6 +76,17 @@ class MeshData(C.Structure):
                 ("materials", C.c_void_p), ("material_count", C.c_uint32)]
 
 
+# TextureFormat (libraries/hvvr/raycaster/texture.h:16-27) and its texel sizes (getTextureSize)
+(HVVR_TEXTURE_NONE, HVVR_TEXTURE_RGBA8_UNORM_SRGB, HVVR_TEXTURE_RGBA8_UNORM, HVVR_TEXTURE_RGBA16_UNORM,
+ HVVR_TEXTURE_RGBA32_FLOAT, HVVR_TEXTURE_RGBA16_FLOAT, HVVR_TEXTURE_R11G11B10_FLOAT, HVVR_TEXTURE_R32_FLOAT) = range(8)
+TEXTURE_ELEMENT_SIZE = {1: 4, 2: 4, 3: 8, 4: 16, 5: 8, 6: 4, 7: 4}
+
+
+class TextureData(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("format", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("stride_elements", C.c_uint32)]
+
+
 class ImageDesc(C.Structure):
     _fields_ = [("pixel_format", C.c_uint32), ("memory_type", C.c_uint32), ("data", C.c_void_p),
                 ("width", C.c_uint32), ("height", C.c_uint32), ("stride", C.c_uint64)]

@@ -57,4 +57,10 @@ __device__ __forceinline__ float dazf(float f) {
 
 __device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
 
+// ReadTexture (libraries/hvvr/raycaster/shading.h:45-47): one gradient read through a texture
+// object made as the reference makes its material textures (texture.cu:234-265)
+__device__ __forceinline__ float4 readTexture(cudaTextureObject_t t, float u, float v, float2 ddx, float2 ddy) {
+    return tex2DGrad<float4>(t, u, v, ddx, ddy);
+}
+
 } // namespace hvb

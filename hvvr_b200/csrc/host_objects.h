@@ -93,6 +93,16 @@ struct hvvr_light {
     hvvr_light_union light{};
 };
 
+// A material texture: a mipmapped CUDA array and the texture object the shading reads
+struct hvvr_texture {
+    hvvr_raycaster* rc = nullptr;
+    uint32_t id = 0;
+    uint32_t format = 0, width = 0, height = 0, levels = 0, elementSize = 0;
+    cudaMipmappedArray_t array = nullptr;
+    cudaTextureObject_t object = 0;
+    ~hvvr_texture();
+};
+
 struct hvvr_camera {
     hvvr_raycaster* rc = nullptr;
     bool enabled = true;
@@ -197,6 +207,9 @@ struct hvvr_raycaster {
     std::vector<std::unique_ptr<hvvr_model>> models;
     std::vector<std::unique_ptr<hvvr_light>> lights;
     std::vector<std::unique_ptr<hvvr_camera>> cameras;
+    std::vector<std::unique_ptr<hvvr_texture>> textures;
+    uint32_t nextTextureId = 0;           // texture ids are not reused
+    DevBuf<unsigned long long> texTable;  // [nextTextureId] texture object by id, 0 for none
     bool sceneDirty = true;
     bool refitDirty = true;
     SceneDev scene;
@@ -235,6 +248,8 @@ int ensureMsaaTable(uint32_t rate, cudaStream_t st);
 int cloneCamera(const hvvr_camera* cam, hvvr_camera** out);
 // forget a foveated camera's temporal history: its next frame reads no previous result
 void resetFoveatedHistory(hvvr_camera* cam);
+// the raycaster's texture objects by id, uploaded for the scene
+int uploadTextureTable(hvvr_raycaster* rc, cudaStream_t st);
 // device bytes a camera holds for its setup and per-frame buffers at the given MSAA rate
 size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa);
 

@@ -86,6 +86,8 @@ struct SceneDev {
     uint32_t modelCount = 0;
     float4* materials = nullptr;     // SimpleMaterial, 4 x float4 each
     uint32_t materialCount = 0;
+    const unsigned long long* textures = nullptr; // texture object of each texture id (0: none)
+    uint32_t textureCount = 0;
     // bottom-up refit support (computed on the host once per topology)
     uint32_t* parentSlot = nullptr;  // (parent << 2) | slot, or ~0 for roots
     uint32_t* internalCount = nullptr; // number of internal children per node
@@ -154,6 +156,8 @@ struct ViewDev {
     const uint4* triShade;
     const float4* verts;
     const float4* materials;
+    const unsigned long long* textures; // texture objects by id (0: none); textureCount entries
+    uint32_t textureCount;
     const Rays4* tileRays;
     const Rays4* blockRays;
     const float4* beams;

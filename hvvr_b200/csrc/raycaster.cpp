@@ -901,6 +901,8 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
         v.triShade = sc.triShade;
         v.verts = sc.verts;
         v.materials = sc.materials;
+        v.textures = sc.textures;
+        v.textureCount = sc.textureCount;
         v.tileRays = d.tileRays;
         v.blockRays = d.blockRays;
         v.beams = d.beams;

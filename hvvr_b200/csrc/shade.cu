@@ -131,10 +131,13 @@ __device__ __forceinline__ void rayTriUVW(F3 ro, F3 rd, const TriGeom& tri, floa
     u = 1.0f - v - w;
 }
 
+// SimpleMaterial (material.h:15-49): textureIDsAndShadingModel holds the shading model in bits
+// 0-15 and the glossiness, specular and diffuse/emissive texture ids in bits 16-31, 32-47, 48-63
+constexpr uint32_t kNoTexture = 0xffffu;
 struct Material {
     F3 emissive, diffuse, specular;
     float glossiness;
-    uint32_t model;
+    uint32_t model, texGloss, texSpecular, texDiffuse;
 };
 
 __device__ __forceinline__ float pow5(float x) {
@@ -162,16 +165,14 @@ __device__ F3 pbr(F3 L, F3 N, F3 V, F3 base, float roughness, F3 F0, F3 lightCol
     return diffuse + lightColor * spec;
 }
 
-// GGXShade for untextured materials (libraries/hvvr/raycaster/shading.h:84-161)
-__device__ F3 ggxShade(const Material& m, F3 pos, F3 nrm, F3 camPos, const LightEnvDev& env) {
-    const F3 normal = normalize3(nrm);
-    if (m.model == 2u) return m.emissive;
-    const F3 V = normalize3(camPos - pos);
-    const float roughness = 1.0f - m.glossiness;
-    F3 radiance = m.emissive + m.diffuse * f3(.15f, .15f, .165f);
+// the phong branch of GGXShade (libraries/hvvr/raycaster/shading.h:127-160) once the base colour,
+// F0 and roughness are known (material constants or texture reads): emissive, ambient and the
+// lights, clamped at zero
+__device__ F3 ggxLit(F3 emissive, F3 base, F3 F0, float roughness, F3 pos, F3 normal, F3 V, const LightEnvDev& env) {
+    F3 radiance = emissive + base * f3(.15f, .15f, .165f);
     if (env.nd > 0) {
-        radiance = radiance + pbr(f3(env.dir[0][0], env.dir[0][1], env.dir[0][2]), normal, V, m.diffuse, roughness,
-                                  m.specular, f3(env.dir[0][3], env.dir[0][4], env.dir[0][5]));
+        radiance = radiance + pbr(f3(env.dir[0][0], env.dir[0][1], env.dir[0][2]), normal, V, base, roughness, F0,
+                                  f3(env.dir[0][3], env.dir[0][4], env.dir[0][5]));
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -181,7 +182,7 @@ __device__ F3 ggxShade(const Material& m, F3 pos, F3 nrm, F3 camPos, const Light
         const float r = sqrtf(dot3(delta, delta));
         const F3 L = normalize3(delta);
         const float fd = satf((l[3] - r) * l[7]);
-        radiance = radiance + pbr(L, normal, V, m.diffuse, roughness, m.specular, f3(l[4], l[5], l[6]) * fd);
+        radiance = radiance + pbr(L, normal, V, base, roughness, F0, f3(l[4], l[5], l[6]) * fd);
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -191,12 +192,38 @@ __device__ F3 ggxShade(const Material& m, F3 pos, F3 nrm, F3 camPos, const Light
         const float r = sqrtf(dot3(delta, delta));
         const F3 L = normalize3(delta);
         const float fd = satf((l[3] - r) * l[7]);
-        const F3 lit = pbr(L, normal, V, m.diffuse, roughness, m.specular, f3(l[8], l[9], l[10]) * fd);
+        const F3 lit = pbr(L, normal, V, base, roughness, F0, f3(l[8], l[9], l[10]) * fd);
         const float cosA = dot3(f3(l[4], l[5], l[6]), -L);
         const float fa = satf((cosA - l[11]) * l[12]);
         radiance = radiance + lit * fa;
     }
     return f3(tmaxf(radiance.x, 0.0f), tmaxf(radiance.y, 0.0f), tmaxf(radiance.z, 0.0f));
+}
+
+// GGXShade for a material without textures (shading.h:84-161)
+__device__ F3 ggxShade(const Material& m, F3 pos, F3 nrm, F3 camPos, const LightEnvDev& env) {
+    const F3 normal = normalize3(nrm);
+    if (m.model == 2u) return m.emissive;
+    const F3 V = normalize3(camPos - pos);
+    const float roughness = 1.0f - m.glossiness;
+    return ggxLit(m.emissive, m.diffuse, m.specular, roughness, pos, normal, V, env);
+}
+
+// true when GGXShade reads a texture for m: the emissive id for the emissive model, else any of
+// the diffuse, specular and glossiness ids
+__device__ __forceinline__ bool readsTextures(const Material& m) {
+    return m.model == 2u ? m.texDiffuse != kNoTexture : (m.texDiffuse & m.texSpecular & m.texGloss) != kNoTexture;
+}
+
+// ReadTexture for material texture `id` (shading.h:45-47); false (the material's constant stays)
+// for no texture, and for an id that names no live texture of the scene
+__device__ __forceinline__ bool materialTexture(const ViewDev& V, uint32_t id, float2 uv, float2 dx, float2 dy,
+                                                float4& out) {
+    if (id == kNoTexture || id >= V.textureCount) return false;
+    const unsigned long long t = __ldg(viewPtr(V.textures) + id);
+    if (!t) return false;
+    out = readTexture(t, uv.x, uv.y, dx, dy);
+    return true;
 }
 
 // ACESFilm, linearToSRgb, ToColor4Unorm8SRgb (shading_helpers.h:158-200; libraries/hvvr/shared/util_graphics.h:26-28)
@@ -232,26 +259,83 @@ __device__ __forceinline__ void sortKeys(uint32_t (&k)[N]) {
     }
 }
 
-// interpolate (shading.h:18-36) the hit's vertices at barycentrics bc and GGXShade it
-__device__ F3 shadeHit(const ViewDev& V, uint32_t triIndex, F3 bc, F3 camPos, const LightEnvDev& env) {
-    const uint4 ts = __ldg(viewPtr(V.triShade) + triIndex);
-    const float4* __restrict__ verts = viewPtr(V.verts);
+__device__ __forceinline__ Material loadMaterial(const ViewDev& V, uint32_t index) {
     const float4* __restrict__ materials = viewPtr(V.materials);
-    const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
-    const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
-    const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
-    const F3 pos = (f3(a0.x, a0.y, a0.z) * bc.x + f3(p0.x, p0.y, p0.z) * bc.y) + f3(q0.x, q0.y, q0.z) * bc.z;
-    const F3 nrm = (halfNormal(a0, a1) * bc.x + halfNormal(p0, p1) * bc.y) + halfNormal(q0, q1) * bc.z;
-    const float4 m0 = __ldg(materials + 4 * size_t(ts.w) + 0);
-    const float4 m1 = __ldg(materials + 4 * size_t(ts.w) + 1);
-    const float4 m2 = __ldg(materials + 4 * size_t(ts.w) + 2);
-    const float4 m3 = __ldg(materials + 4 * size_t(ts.w) + 3);
+    const float4 m0 = __ldg(materials + 4 * size_t(index) + 0);
+    const float4 m1 = __ldg(materials + 4 * size_t(index) + 1);
+    const float4 m2 = __ldg(materials + 4 * size_t(index) + 2);
+    const float4 m3 = __ldg(materials + 4 * size_t(index) + 3);
     Material mat;
     mat.emissive = f3(m0.x, m0.y, m0.z);
     mat.diffuse = f3(m1.x, m1.y, m1.z);
     mat.specular = f3(m2.x, m2.y, m2.z);
     mat.glossiness = m3.x;
-    mat.model = __float_as_uint(m3.z) & 0xffffu;
+    const uint32_t code0 = __float_as_uint(m3.z), code1 = __float_as_uint(m3.w);
+    mat.model = code0 & 0xffffu;
+    mat.texGloss = code0 >> 16;
+    mat.texSpecular = code1 & 0xffffu;
+    mat.texDiffuse = code1 >> 16;
+    return mat;
+}
+
+// interpolate (shading.h:18-36) of a vertex attribute pair
+__device__ __forceinline__ float2 interp2(float2 t0, float2 t1, float2 t2, F3 b) {
+    return make_float2((t0.x * b.x + t1.x * b.y) + t2.x * b.z, (t0.y * b.x + t1.y * b.y) + t2.y * b.z);
+}
+
+// GGXShade (shading.h:84-161) of a hit whose material reads textures. The texture coordinates and
+// their screen derivatives come from the hit's barycentrics at the shading point (bc) and one
+// sample step along x (bx) and y (by): dUVdX = uv(bx) - uv(bc), dUVdY = uv(by) - uv(bc)
+// (ShadeMSAA, resolve.cu:230-270). Kept out of line so the untextured path's registers do not
+// grow.
+__device__ __noinline__ F3 shadeTextured(const ViewDev& V, uint32_t triIndex, F3 bc, F3 bx, F3 by, F3 camPos,
+                                         const LightEnvDev& env) {
+    const uint4 ts = __ldg(viewPtr(V.triShade) + triIndex);
+    const Material m = loadMaterial(V, ts.w);
+    const float4* __restrict__ verts = viewPtr(V.verts);
+    const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
+    const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
+    const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
+    const F3 pos = (f3(a0.x, a0.y, a0.z) * bc.x + f3(p0.x, p0.y, p0.z) * bc.y) + f3(q0.x, q0.y, q0.z) * bc.z;
+    const F3 nrm = (halfNormal(a0, a1) * bc.x + halfNormal(p0, p1) * bc.y) + halfNormal(q0, q1) * bc.z;
+    const float2 t0 = make_float2(a1.y, a1.z), t1 = make_float2(p1.y, p1.z), t2 = make_float2(q1.y, q1.z);
+    const float2 uv = interp2(t0, t1, t2, bc);
+    const float2 uvx = interp2(t0, t1, t2, bx), uvy = interp2(t0, t1, t2, by);
+    const float2 dx = make_float2(uvx.x - uv.x, uvx.y - uv.y), dy = make_float2(uvy.x - uv.x, uvy.y - uv.y);
+    const F3 normal = normalize3(nrm);
+    float4 tex;
+    if (m.model == 2u) return materialTexture(V, m.texDiffuse, uv, dx, dy, tex) ? f3(tex.x, tex.y, tex.z) : m.emissive;
+    F3 base = m.diffuse;
+    if (materialTexture(V, m.texDiffuse, uv, dx, dy, tex)) base = f3(tex.x, tex.y, tex.z);
+    const F3 Vd = normalize3(camPos - pos);
+    F3 F0 = m.specular;
+    if (materialTexture(V, m.texSpecular, uv, dx, dy, tex)) F0 = f3(tex.x, tex.y, tex.z);
+    float roughness = 1.0f - m.glossiness;
+    if (materialTexture(V, m.texGloss, uv, dx, dy, tex)) roughness = 1.0f - tex.x;
+    return ggxLit(m.emissive, base, F0, roughness, pos, normal, Vd, env);
+}
+
+// interpolate (shading.h:18-36) the hit's vertices at barycentrics bc and GGXShade it.
+// deriv(bx, by) gives the barycentrics one sample step along x and y; it runs only when the
+// material reads textures.
+template <class Deriv>
+__device__ __forceinline__ F3 shadeHit(const ViewDev& V, uint32_t triIndex, F3 bc, F3 camPos, const LightEnvDev& env,
+                                       Deriv deriv) {
+    const uint4 ts = __ldg(viewPtr(V.triShade) + triIndex);
+    const Material mat = loadMaterial(V, ts.w);
+    // with no texture in the scene every read falls back to the constants, which is the
+    // untextured path
+    if (V.textureCount && readsTextures(mat)) {
+        F3 bx, by;
+        deriv(bx, by);
+        return shadeTextured(V, triIndex, bc, bx, by, camPos, env);
+    }
+    const float4* __restrict__ verts = viewPtr(V.verts);
+    const float4 a0 = __ldg(verts + 2 * size_t(ts.x)), a1 = __ldg(verts + 2 * size_t(ts.x) + 1);
+    const float4 p0 = __ldg(verts + 2 * size_t(ts.y)), p1 = __ldg(verts + 2 * size_t(ts.y) + 1);
+    const float4 q0 = __ldg(verts + 2 * size_t(ts.z)), q1 = __ldg(verts + 2 * size_t(ts.z) + 1);
+    const F3 pos = (f3(a0.x, a0.y, a0.z) * bc.x + f3(p0.x, p0.y, p0.z) * bc.y) + f3(q0.x, q0.y, q0.z) * bc.z;
+    const F3 nrm = (halfNormal(a0, a1) * bc.x + halfNormal(p0, p1) * bc.y) + halfNormal(q0, q1) * bc.z;
     return ggxShade(mat, pos, nrm, camPos, env);
 }
 
@@ -516,7 +600,10 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         const F3 v0r = camPos - tri.v0;
         const TriThread th = threadSetup(tri.e0, tri.e1, v0r, c, du, dv);
         const F3 bc = calcUVW<FMA>(th, cax, cay);
-        const F3 col = shadeHit(V, triIndex, bc, camPos, env);
+        const F3 col = shadeHit(V, triIndex, bc, camPos, env, [&](F3& bx, F3& by) {
+            bx = calcUVW<FMA>(th, cax + 1.0f, cay + 0.0f);
+            by = calcUVW<FMA>(th, cax + 0.0f, cay + 1.0f);
+        });
         rx = rx + col.x * pc;
         ry = ry + col.y * pc;
         rz = rz + col.z * pc;
@@ -800,12 +887,21 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr
         }
         const TriGeom tri = loadTri(viewPtr(V.tris), triIndex);
         const F3 normal = cross3(tri.e0, tri.e1);
-        float denom, v, w;
-        dofBary<FMA>(tri.e0, tri.e1, camPos - tri.v0, dot3(-lu, normal), dot3(-lv, normal), dot3(-lc2fc, normal), lc2fc,
-                     lu, lv, make_float2(clx, cly), make_float2(cdx, cdy), denom, v, w);
-        const float u = denom - v - w;
-        const float dinv = 1.0f / denom;
-        const F3 col = shadeHit(V, triIndex, f3(u * dinv, v * dinv, w * dinv), camPos, env);
+        const F3 v0l = camPos - tri.v0;
+        const float tdx = dot3(-lu, normal), tdy = dot3(-lv, normal), tdc = dot3(-lc2fc, normal);
+        // IntersectTriangleThreadDoF::calcUVW at the centroid lens position and direction duv
+        auto baryAt = [&](float2 duv) {
+            float denom, v, w;
+            dofBary<FMA>(tri.e0, tri.e1, v0l, tdx, tdy, tdc, lc2fc, lu, lv, make_float2(clx, cly), duv, denom, v, w);
+            const float u = denom - v - w;
+            const float dinv = 1.0f / denom;
+            return f3(u * dinv, v * dinv, w * dinv);
+        };
+        // the derivatives step the centroid direction by (1, 0) and (0, 1) (ShadeMSAA's DoF branch)
+        const F3 col = shadeHit(V, triIndex, baryAt(make_float2(cdx, cdy)), camPos, env, [&](F3& bx, F3& by) {
+            bx = baryAt(make_float2(cdx + 1.0f, cdy + 0.0f));
+            by = baryAt(make_float2(cdx + 0.0f, cdy + 1.0f));
+        });
         rx = rx + col.x * pc;
         ry = ry + col.y * pc;
         rz = rz + col.z * pc;

@@ -8,7 +8,7 @@ sizes and value distributions of the benchmark configurations stand in for them:
 * ``box_count`` boxes (12 triangles each) with centres uniform over the region resting on
   the terrain, edge lengths log-uniform in [0.05, 1.0] and a random yaw;
 * one material per triangle: albedo U[0,1]^3, GGX roughness U[0.1, 0.9] (glossiness
-  1 - roughness), F0 = 0.04, phong shading model, no textures;
+  1 - roughness), F0 = 0.04, phong shading model, no textures (``with_textures`` adds them);
 * one directional light plus four point lights.
 
 Triangles are wound so their geometric normal e0 x e1 faces outward / up, since the
@@ -163,6 +163,60 @@ def make_scene(grid_quads, box_count, seed=1):
 
     lights = make_lights(rng)
     return Scene(verts, tri_shade, materials, lights, heightfield=params)
+
+
+EMISSIVE = 2
+
+
+def shading_code(model=PHONG, diffuse=BAD_TEXTURE, specular=BAD_TEXTURE, glossiness=BAD_TEXTURE):
+    """SimpleMaterial::buildShadingCode (material.h:32-38): model in bits 0-15, then the glossiness,
+    specular and diffuse/emissive texture ids."""
+    return int(model) | (int(glossiness) << 16) | (int(specular) << 32) | (int(diffuse) << 48)
+
+
+def texture_rgba8(width, height, seed=1, cells=8):
+    """Seeded RGBA8 texels (rows of `width`): a checkerboard of random cell colours with
+    per-texel noise, as a uint8 array [height, width, 4]."""
+    rng = np.random.default_rng(seed)
+    cw, ch = max(1, width // cells), max(1, height // cells)
+    pal = rng.integers(0, 256, (cells + 1, cells + 1, 4))
+    y, x = np.mgrid[0:height, 0:width]
+    base = pal[np.minimum(y // ch, cells), np.minimum(x // cw, cells)]
+    tex = np.clip(base + rng.integers(-24, 25, (height, width, 4)), 0, 255).astype(np.uint8)
+    return tex
+
+
+def with_textures(sc, texture_count, seed=1):
+    """The scene with per-material texture use drawn from a seeded mix: untextured; a diffuse
+    texture; diffuse, specular and glossiness textures; glossiness only; the emissive model with
+    and without an emissive texture. Texture ids are below texture_count."""
+    rng = np.random.default_rng(seed)
+    m = sc.materials.copy()
+    n = len(m)
+    kind = rng.integers(0, 6, n)
+    ids = rng.integers(0, texture_count, (n, 3))
+    codes = np.empty(n, np.uint64)
+    for i in range(n):
+        k = kind[i]
+        if k == 0:
+            c = shading_code()
+        elif k == 1:
+            c = shading_code(diffuse=ids[i, 0])
+        elif k == 2:
+            c = shading_code(diffuse=ids[i, 0], specular=ids[i, 1], glossiness=ids[i, 2])
+        elif k == 3:
+            c = shading_code(glossiness=ids[i, 2])
+        elif k == 4:
+            c = shading_code(EMISSIVE, diffuse=ids[i, 0])
+        else:
+            c = shading_code(EMISSIVE)
+        codes[i] = c
+    m["code"] = codes
+    em = rng.uniform(0.0, 0.6, (n, 3)).astype(np.float32)
+    m["emissive"][:, :3] = np.where((kind >= 4)[:, None], em, 0.0)
+    out = Scene(sc.verts, sc.tri_shade, m, sc.lights, heightfield=sc.heightfield)
+    out.nodes = sc.nodes
+    return out
 
 
 def make_lights(rng):

@@ -99,6 +99,26 @@ typedef struct {
     const hvvr_material* materials; uint32_t material_count;
 } hvvr_mesh_data;
 
+/* TextureFormat and TextureData (libraries/hvvr/raycaster/texture.h:16-34): the reference's
+ * format values; data points at height rows of stride_elements texels of the format's size
+ * (4, 4, 8, 16, 8, 4, 4 bytes). 24 bytes on LP64, byte-compatible with TextureData. */
+enum {
+    HVVR_TEXTURE_NONE = 0,
+    HVVR_TEXTURE_RGBA8_UNORM_SRGB = 1,
+    HVVR_TEXTURE_RGBA8_UNORM = 2,
+    HVVR_TEXTURE_RGBA16_UNORM = 3,
+    HVVR_TEXTURE_RGBA32_FLOAT = 4,
+    HVVR_TEXTURE_RGBA16_FLOAT = 5,
+    HVVR_TEXTURE_R11G11B10_FLOAT = 6,
+    HVVR_TEXTURE_R32_FLOAT = 7
+};
+typedef struct {
+    const uint8_t* data;
+    uint32_t format;
+    uint32_t width, height;
+    uint32_t stride_elements;
+} hvvr_texture_data;
+
 /* ImageResourceDescriptor (libraries/hvvr/shared/graphics_types.h:56-80).
  * Only CPU_MEMORY and CUDA_MEMORY exist here (no graphics API on the target). */
 enum { HVVR_PIXEL_RGBA8_SRGB = 0 };
@@ -132,6 +152,7 @@ typedef struct hvvr_camera hvvr_camera;
 typedef struct hvvr_model hvvr_model;
 typedef struct hvvr_light hvvr_light;
 typedef struct hvvr_batch hvvr_batch;
+typedef struct hvvr_texture hvvr_texture;
 
 /* ---------------------------------------------------------------- errors */
 /* Message of the last failing call on this thread (empty string if none). */
@@ -174,6 +195,30 @@ int hvvr_model_update_vertices_device(hvvr_model* model, uint32_t first, uint32_
  * createLight(const LightUnion&) / destroyLight (raycaster.h:55-56) */
 int hvvr_light_create(hvvr_raycaster* rc, const hvvr_light_union* light, hvvr_light** out);
 int hvvr_light_destroy(hvvr_raycaster* rc, hvvr_light* light);
+
+/* ---------------------------------------------------------------- textures
+ * createTexture(const TextureData&) / destroyTexture (raycaster.h:51-52; libraries/hvvr/raycaster/
+ * scene.cpp:28-40; texture.cu:201-272). A mipmapped CUDA array with the reference's texture object
+ * (normalized coordinates, wrap/wrap addressing, linear and linear-mip filtering, anisotropy 8,
+ * sRGB decode for HVVR_TEXTURE_RGBA8_UNORM_SRGB); mip levels of the 8-bit formats come from the
+ * reference's generator (texture.cu:78-186), other formats use its four taps stored in their own
+ * format. HVVR_TEXTURE_R11G11B10_FLOAT has no CUDA array format and is HVVR_ERR_INVALID.
+ * Materials name textures by id (SimpleMaterial::textureIDsAndShadingModel, 0xffff = none): ids
+ * count up from 0 per raycaster in creation order and are not reused after a destroy (the
+ * reference's ids count over one process-wide atlas). Shading reads an id that names no live
+ * texture as no texture. Returns after the texture is complete on the device; data is not
+ * retained. Destroy waits for the device to finish the work in flight. */
+int hvvr_texture_create(hvvr_raycaster* rc, const hvvr_texture_data* data, hvvr_texture** out);
+int hvvr_texture_destroy(hvvr_raycaster* rc, hvvr_texture* texture);
+/* Texture::getID (texture.h:44-46) */
+int hvvr_texture_get_id(const hvvr_texture* texture, uint32_t* id);
+/* parity read-back: mip level `level` (0 = the texels given) as rows of width * element-size
+ * bytes; with data NULL only the level's size is returned */
+int hvvr_texture_read_level(const hvvr_texture* texture, uint32_t level, void* data, uint64_t capacity,
+                            uint32_t* width, uint32_t* height);
+/* parity read-back: ReadTexture (libraries/hvvr/raycaster/shading.h:45-47), the tex2DGrad read the
+ * shading makes, at count queries q[i] = {u, v, ddx.x, ddx.y, ddy.x, ddy.y}; rgba is [count][4] */
+int hvvr_texture_sample(const hvvr_texture* texture, uint32_t count, const float* q, float* rgba);
 
 /* ---------------------------------------------------------------- cameras
  * createCamera(const FloatRect&, float) / destroyCamera (raycaster.h:49-50) and the
@@ -290,8 +335,9 @@ int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
  * (getTextureSize, libraries/hvvr/raycaster/texture.h:56-76); the lights; per mesh {transform,
  * vertex, triangle, node and material counts} and those arrays, each record byte-compatible
  * with the types above. A loaded file owns its arrays until hvvr_scene_file_close; a short or
- * malformed file is HVVR_ERR_INVALID. Textures are read and handed back as bytes (this library
- * shades untextured materials). */
+ * malformed file is HVVR_ERR_INVALID. Textures are handed back as bytes, in file order, for
+ * hvvr_texture_create (model_import::createObjects creates them first, so their ids are the
+ * file's texture indices). */
 typedef struct hvvr_scene_file hvvr_scene_file;
 int hvvr_scene_file_load(const char* path, hvvr_scene_file** out);
 int hvvr_scene_file_counts(const hvvr_scene_file* file, uint32_t* textures, uint32_t* lights, uint32_t* meshes);

@@ -18,7 +18,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <random>
 #include <thread>
 #include <vector>
@@ -905,15 +908,44 @@ V3 pbr(V3 L, V3 N, V3 V, V3 base, float roughness, V3 F0, V3 lightColor) {
     V3 glossy = lightColor * spec;
     return diffuse + glossy;
 }
-// GGXShade (RC/shading.h:84-161); materials carry no textures (badTextureIndex)
-V3 ggxShade(const Material& m, V3 pos, V3 nrm, V3 camPos, const LightEnv& env) {
+// the texture reads of one shading point: uv, its screen derivatives and the sampler
+struct TexRead {
+    V2 uv, dx, dy;
+    const oracle_frame_in* in;
+    // ReadTexture (RC/shading.h:45-47) for material texture slot `id`; false (the constant
+    // stays) for badTextureIndex and for an id with no live texture
+    bool read(uint32_t id, float* rgba) const {
+        if (id == 0xffffu || id >= in->texture_count || !in->texture_sample) return false;
+        const float q[6] = {uv.x, uv.y, dx.x, dx.y, dy.x, dy.y};
+        in->texture_sample(in->texture_ctx, id, q, rgba);
+        return true;
+    }
+};
+// true when GGXShade reads a texture for m (the emissive texture for the emissive model, else
+// any of diffuse, specular, glossiness; SimpleMaterial bit layout, RC/material.h:22-49)
+bool readsTextures(const Material& m) {
+    uint32_t model = uint32_t(m.code & 0xffff);
+    uint32_t gl = uint32_t(m.code >> 16) & 0xffff, sp = uint32_t(m.code >> 32) & 0xffff, di = uint32_t(m.code >> 48);
+    return model == 2 ? di != 0xffff : (di != 0xffff || sp != 0xffff || gl != 0xffff);
+}
+// GGXShade (RC/shading.h:84-161); tex NULL: no texture reads (the constants stay)
+V3 ggxShade(const Material& m, V3 pos, V3 nrm, V3 camPos, const LightEnv& env, const TexRead* tex) {
     V3 normal = normalize(nrm);
     uint32_t model = uint32_t(m.code & 0xffff);
-    if (model == 2) return m.emissive; // emissive
+    const uint32_t texGloss = uint32_t(m.code >> 16) & 0xffff, texSpec = uint32_t(m.code >> 32) & 0xffff,
+                   texDiffuse = uint32_t(m.code >> 48) & 0xffff;
+    float t[4];
+    if (model == 2) { // emissive
+        if (tex && tex->read(texDiffuse, t)) return mk(t[0], t[1], t[2]);
+        return m.emissive;
+    }
     V3 base = m.diffuse;
+    if (tex && tex->read(texDiffuse, t)) base = mk(t[0], t[1], t[2]);
     V3 V = normalize(camPos - pos);
     V3 F0 = m.specular;
+    if (tex && tex->read(texSpec, t)) F0 = mk(t[0], t[1], t[2]);
     float roughness = 1.0f - m.glossiness;
+    if (tex && tex->read(texGloss, t)) roughness = 1.0f - t[0];
     V3 radiance = m.emissive;
     radiance = radiance + base * mk(.15f, .15f, .165f);
     for (int i = 0; i < env.nd && i < 1; i++)
@@ -1338,18 +1370,31 @@ int renderCore(const oracle_frame_in* in, const SampleSetup& ss, const M4& c2w, 
                         }
                     }
                     const Tri& tri = scene.tris[triIndex];
-                    V3 bc;
+                    const hvvr_tri_shade& ts = scene.triShade[triIndex];
+                    const bool textured = in->texture_count && readsTextures(mats[ts.material]);
+                    // bx, by: barycentrics one sample step along x and y, for the texture
+                    // derivatives (centroid alpha + (1,0) / (0,1); the DoF branch steps the
+                    // centroid direction the same way, RC/resolve.cu:232-262)
+                    V3 bc, bx{}, by{};
                     if (dof) {
                         DofTri d;
                         dofSetup(tri, camPos, dt.lensU, dt.lensV, d);
-                        bc = dofUVW(d, dofDenomCenter(d, lc2fc), lc2fc, dt.lensU, dt.lensV, cl, cd, useFma);
+                        const float dcen = dofDenomCenter(d, lc2fc);
+                        bc = dofUVW(d, dcen, lc2fc, dt.lensU, dt.lensV, cl, cd, useFma);
+                        if (textured) {
+                            bx = dofUVW(d, dcen, lc2fc, dt.lensU, dt.lensV, cl, V2{cd.x + 1.0f, cd.y + 0.0f}, useFma);
+                            by = dofUVW(d, dcen, lc2fc, dt.lensU, dt.lensV, cl, V2{cd.x + 0.0f, cd.y + 1.0f}, useFma);
+                        }
                     } else {
                         TriTile tt;
                         tileSetup(tri, camPos, tt);
                         TriThread th = threadSetup(tt, c, du, dv);
                         bc = calcUVW(th, ca, useFma);
+                        if (textured) {
+                            bx = calcUVW(th, V2{ca.x + 1.0f, ca.y + 0.0f}, useFma);
+                            by = calcUVW(th, V2{ca.x + 0.0f, ca.y + 1.0f}, useFma);
+                        }
                     }
-                    const hvvr_tri_shade& ts = scene.triShade[triIndex];
                     const hvvr_shading_vertex& a0 = scene.world[ts.indices[0]];
                     const hvvr_shading_vertex& a1 = scene.world[ts.indices[1]];
                     const hvvr_shading_vertex& a2 = scene.world[ts.indices[2]];
@@ -1358,7 +1403,17 @@ int renderCore(const oracle_frame_in* in, const SampleSetup& ss, const M4& c2w, 
                     V3 n1 = mk(halfToFloat(a1.normal[0]), halfToFloat(a1.normal[1]), halfToFloat(a1.normal[2]));
                     V3 n2 = mk(halfToFloat(a2.normal[0]), halfToFloat(a2.normal[1]), halfToFloat(a2.normal[2]));
                     V3 nrm = (n0 * bc.x + n1 * bc.y) + n2 * bc.z;
-                    V3 col = ggxShade(mats[ts.material], pos, nrm, camPos, env);
+                    TexRead tr;
+                    if (textured) {
+                        // interpolate (RC/shading.h:18-36) of uv at bc, bx, by; dUVdX/dUVdY as differences
+                        auto uvAt = [&](V3 b) {
+                            return V2{(a0.uv.x * b.x + a1.uv.x * b.y) + a2.uv.x * b.z,
+                                      (a0.uv.y * b.x + a1.uv.y * b.y) + a2.uv.y * b.z};
+                        };
+                        const V2 uv = uvAt(bc), ux = uvAt(bx), uy = uvAt(by);
+                        tr = TexRead{uv, V2{ux.x - uv.x, ux.y - uv.y}, V2{uy.x - uv.x, uy.y - uv.y}, in};
+                    }
+                    V3 col = ggxShade(mats[ts.material], pos, nrm, camPos, env, textured ? &tr : nullptr);
                     float pc = float(__builtin_popcount(sm));
                     res[0] = res[0] + col.x * pc; res[1] = res[1] + col.y * pc; res[2] = res[2] + col.z * pc;
                 }
@@ -1749,3 +1804,83 @@ extern "C" int oracle_foveated_resolve(const oracle_fov_in* in, oracle_fov_out* 
         }
     return 0;
 }
+
+// ---------------------------------------------------------------- texture samplers
+// Test samplers behind oracle_frame_in.texture_sample; see hvvr_oracle.h.
+namespace {
+typedef std::array<uint32_t, 7> TexKey; // id and the query's six float bit patterns
+std::mutex gTexMutex;
+std::map<TexKey, std::array<float, 4>> gTexTable;
+bool gTexRecord = false;
+std::atomic<uint32_t> gTexMissing{0};
+TexKey texKey(uint32_t id, const float* q) {
+    TexKey k;
+    k[0] = id;
+    memcpy(&k[1], q, 6 * sizeof(float));
+    return k;
+}
+} // namespace
+
+extern "C" {
+
+void oracle_texture_hash(void*, uint32_t id, const float* q, float* rgba) {
+    uint64_t h = 0x9E3779B97F4A7C15ull ^ id;
+    for (int i = 0; i < 6; i++) {
+        uint32_t b;
+        memcpy(&b, &q[i], 4);
+        h = (h ^ b) * 0x100000001B3ull;
+        h ^= h >> 29;
+    }
+    for (int c = 0; c < 4; c++) {
+        h = h * 6364136223846793005ull + 1442695040888963407ull;
+        rgba[c] = float((h >> 40) & 0xffffffu) / 16777216.0f;
+    }
+}
+
+void oracle_texture_table(void*, uint32_t id, const float* q, float* rgba) {
+    const TexKey k = texKey(id, q);
+    std::lock_guard<std::mutex> lock(gTexMutex);
+    if (gTexRecord) {
+        gTexTable.emplace(k, std::array<float, 4>{0.0f, 0.0f, 0.0f, 0.0f});
+        for (int c = 0; c < 4; c++) rgba[c] = 0.0f;
+        return;
+    }
+    auto it = gTexTable.find(k);
+    if (it == gTexTable.end()) {
+        gTexMissing++;
+        for (int c = 0; c < 4; c++) rgba[c] = NAN;
+        return;
+    }
+    for (int c = 0; c < 4; c++) rgba[c] = it->second[c];
+}
+
+void oracle_texture_table_reset(int record) {
+    std::lock_guard<std::mutex> lock(gTexMutex);
+    gTexTable.clear();
+    gTexRecord = record != 0;
+    gTexMissing = 0;
+}
+
+uint32_t oracle_texture_table_queries(uint32_t* ids, float* q, uint32_t capacity) {
+    std::lock_guard<std::mutex> lock(gTexMutex);
+    uint32_t n = 0;
+    for (const auto& e : gTexTable) {
+        if (n < capacity) {
+            if (ids) ids[n] = e.first[0];
+            if (q) memcpy(q + 6 * size_t(n), &e.first[1], 6 * sizeof(float));
+        }
+        n++;
+    }
+    return n;
+}
+
+void oracle_texture_table_set(uint32_t n, const uint32_t* ids, const float* q, const float* rgba) {
+    std::lock_guard<std::mutex> lock(gTexMutex);
+    gTexRecord = false;
+    for (uint32_t i = 0; i < n; i++)
+        gTexTable[texKey(ids[i], q + 6 * size_t(i))] = {rgba[4 * i], rgba[4 * i + 1], rgba[4 * i + 2], rgba[4 * i + 3]};
+}
+
+uint32_t oracle_texture_table_missing(void) { return gTexMissing.load(); }
+
+} // extern "C"

@@ -36,7 +36,27 @@ typedef struct {
     uint32_t msaa;
     uint32_t fp_mode; /* HVVR_FP_FMA or HVVR_FP_STRICT */
     uint32_t threads; /* worker threads for the tile loop (0 = 1) */
+    /* material textures: ids below texture_count are live; each texture read (ReadTexture,
+     * RC/shading.h:45-47) calls texture_sample(ctx, id, {u, v, ddx.x, ddx.y, ddy.x, ddy.y}, rgba)
+     * from any worker thread. texture_count 0: no texture is read. */
+    uint32_t texture_count;
+    void (*texture_sample)(void* ctx, uint32_t id, const float* q, float* rgba);
+    void* texture_ctx;
 } oracle_frame_in;
+
+/* Texture samplers for oracle_frame_in.texture_sample (and the reference harness's texture hook).
+ * oracle_texture_hash: a value that depends on every bit of the id and the query, so any
+ * difference in a texture coordinate or derivative shows in the colour.
+ * oracle_texture_table: a table of sampled values keyed by the exact bits of (id, query); in
+ * record mode it collects the queries (and reads zeros), in lookup mode it returns the values
+ * set for them and counts the queries it does not hold (which read NaN). */
+void oracle_texture_hash(void* ctx, uint32_t id, const float* q, float* rgba);
+void oracle_texture_table(void* ctx, uint32_t id, const float* q, float* rgba);
+void oracle_texture_table_reset(int record);
+/* the recorded queries in a fixed order: ids [n], q [n][6]; returns n (at most capacity written) */
+uint32_t oracle_texture_table_queries(uint32_t* ids, float* q, uint32_t capacity);
+void oracle_texture_table_set(uint32_t n, const uint32_t* ids, const float* q, const float* rgba);
+uint32_t oracle_texture_table_missing(void);
 
 typedef struct {
     /* every pointer may be NULL to skip that output */

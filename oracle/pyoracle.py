@@ -15,6 +15,7 @@ from hvvr_b200 import _abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libhvvr_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhvvr_ref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libhvvr_ref_gpu.so")
 
 
 class FrameIn(C.Structure):
@@ -23,7 +24,8 @@ class FrameIn(C.Structure):
                 ("light_count", C.c_uint32), ("viewport", _abi.FloatRect), ("lens", _abi.ThinLens),
                 ("cam_xf", _abi.Transform), ("samples", C.c_void_p), ("sample_count", C.c_uint32),
                 ("split_color_samples", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
-                ("msaa", C.c_uint32), ("fp_mode", C.c_uint32), ("threads", C.c_uint32)]
+                ("msaa", C.c_uint32), ("fp_mode", C.c_uint32), ("threads", C.c_uint32),
+                ("texture_count", C.c_uint32), ("texture_sample", C.c_void_p), ("texture_ctx", C.c_void_p)]
 
 
 class FrameOut(C.Structure):
@@ -64,7 +66,7 @@ class Frame:
 
 def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi.HVVR_FP_FMA, lens=(0.0, 1.0),
          threads=None, split=1, want=("lists", "hits", "colors", "image", "blocks", "gbuffer", "scene", "beams"),
-         model_xf=None, tile_capacity=None, beams_in=None):
+         model_xf=None, tile_capacity=None, beams_in=None, textures=0, sampler=None):
     if scene.nodes is None:
         raise ValueError("scene has no topology")
     n = len(samples) if beams_in is None else len(beams_in["beams"])
@@ -90,6 +92,10 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
     fin.msaa = msaa
     fin.fp_mode = fp_mode
     fin.threads = threads if threads is not None else (os.cpu_count() or 1)
+    # material textures: ids below `textures` are live and read through `sampler` (the address
+    # of a C sampler such as Oracle.hash_sampler / Oracle.table_sampler)
+    fin.texture_count = textures
+    fin.texture_sample = sampler
     f = Frame()
     out = FrameOut()
     keep = []
@@ -165,6 +171,39 @@ class Oracle:
 
     def render(self, *a, **k):
         return _run(self.lib.oracle_render, *a, **k)
+
+    # texture samplers (addresses for render(..., sampler=)) and the table sampler's state
+    @property
+    def hash_sampler(self):
+        return C.cast(self.lib.oracle_texture_hash, C.c_void_p).value
+
+    @property
+    def table_sampler(self):
+        return C.cast(self.lib.oracle_texture_table, C.c_void_p).value
+
+    def table_record(self):
+        self.lib.oracle_texture_table_reset(1)
+
+    def table_queries(self):
+        """The recorded texture queries: ids [n] uint32 and q [n, 6] float32 (u, v, ddx, ddy)."""
+        f = self.lib.oracle_texture_table_queries
+        f.restype = C.c_uint32
+        n = f(None, None, 0)
+        ids = np.zeros(n, np.uint32)
+        q = np.zeros((n, 6), np.float32)
+        f(ids.ctypes.data_as(C.c_void_p), q.ctypes.data_as(C.c_void_p), n)
+        return ids, q
+
+    def table_set(self, ids, q, rgba):
+        ids = np.ascontiguousarray(ids, np.uint32)
+        q = np.ascontiguousarray(q, np.float32)
+        rgba = np.ascontiguousarray(rgba, np.float32)
+        self.lib.oracle_texture_table_set(C.c_uint32(len(ids)), ids.ctypes.data_as(C.c_void_p),
+                                          q.ctypes.data_as(C.c_void_p), rgba.ctypes.data_as(C.c_void_p))
+
+    def table_missing(self):
+        self.lib.oracle_texture_table_missing.restype = C.c_uint32
+        return int(self.lib.oracle_texture_table_missing())
 
     def render_beams(self, scene, beams_in, msaa, fp_mode=_abi.HVVR_FP_FMA, threads=None,
                      want=("lists", "hits", "colors", "scene", "tmax")):
@@ -283,3 +322,54 @@ class Reference:
         if rc != 0:
             raise RuntimeError("GenerateTopology failed: %d" % rc)
         return verts, tris, nodes[: cnt.value].copy()
+
+
+class ReferenceGpu:
+    """The reference's own texture creation (CreateTexture with its mip generator) and texture
+    reads (ReadTexture) built for the GPU (oracle/_ref/libhvvr_ref_gpu.so); needs a GPU."""
+
+    def __init__(self, path=REF_GPU_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError("reference GPU library not built: %s" % path)
+        self.lib = C.CDLL(path)
+        self.lib.ref_gpu_texture_create.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+        self.lib.ref_gpu_texture_create.restype = C.c_int
+        self.lib.ref_gpu_texture_read_level.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
+                                                        C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        self.lib.ref_gpu_texture_read_level.restype = C.c_int
+        self.lib.ref_gpu_texture_sample.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.ref_gpu_texture_sample.restype = C.c_int
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_GPU_SO)
+
+    def create_texture(self, texels, fmt):
+        """RGBA8 texels [h, w, 4] (the reference's mip generator writes 8-bit texels); returns the
+        reference's atlas id"""
+        a = np.ascontiguousarray(texels, np.uint8)
+        h, w = a.shape[0], a.shape[1]
+        return self.lib.ref_gpu_texture_create(a.ctypes.data_as(C.c_void_p), fmt, w, h, w)
+
+    def read_level(self, tex_id, level):
+        w, h = C.c_uint32(0), C.c_uint32(0)
+        rc = self.lib.ref_gpu_texture_read_level(tex_id, level, None, 0, C.byref(w), C.byref(h))
+        if rc != 0:
+            raise RuntimeError("read_level: %d" % rc)
+        out = np.zeros((h.value, w.value, 4), np.uint8)
+        rc = self.lib.ref_gpu_texture_read_level(tex_id, level, out.ctypes.data_as(C.c_void_p), out.nbytes,
+                                                 C.byref(w), C.byref(h))
+        if rc != 0:
+            raise RuntimeError("read_level: %d" % rc)
+        return out
+
+    def sample(self, ids, q):
+        """ReadTexture through the reference's atlas: ids [n], q [n, 6] -> [n, 4] float32"""
+        ids = np.ascontiguousarray(ids, np.uint32)
+        q = np.ascontiguousarray(q, np.float32).reshape(-1, 6)
+        out = np.zeros((len(q), 4), np.float32)
+        rc = self.lib.ref_gpu_texture_sample(len(q), ids.ctypes.data_as(C.c_void_p), q.ctypes.data_as(C.c_void_p),
+                                             out.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("sample: %d" % rc)
+        return out

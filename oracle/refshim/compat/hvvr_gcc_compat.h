@@ -73,4 +73,19 @@ static inline unsigned __activemask() { return 0xffffffffu; }
 static inline unsigned __ballot_sync(unsigned, int p) { return p ? 1u : 0u; }
 template <class T> static inline T __shfl_sync(unsigned, T v, int, int = 32) { return v; }
 template <class T> static inline T __shfl_xor_sync(unsigned, T v, int, int = 32) { return v; }
-template <class T> static inline T tex2DGrad(cudaTextureObject_t, float, float, float2, float2) { return T(); }
+// texture reads of host-compiled shading code (ReadTexture) go to a hook the harness sets:
+// hook(ctx, texture object value, {u, v, ddx.x, ddx.y, ddy.x, ddy.y}, rgba)
+typedef void (*hv_texture_hook_fn)(void* ctx, uint32_t id, const float* q, float* rgba);
+extern hv_texture_hook_fn hv_texture_hook;
+extern void* hv_texture_hook_ctx;
+template <class T> static inline T tex2DGrad(cudaTextureObject_t t, float u, float v, float2 dx, float2 dy) {
+    const float q[6] = {u, v, dx.x, dx.y, dy.x, dy.y};
+    float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (hv_texture_hook) hv_texture_hook(hv_texture_hook_ctx, uint32_t(t), q, o);
+    T r;
+    r.x = o[0];
+    r.y = o[1];
+    r.z = o[2];
+    r.w = o[3];
+    return r;
+}

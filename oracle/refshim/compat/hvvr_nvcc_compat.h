@@ -1,0 +1,35 @@
+// Forced-include shim that lets the reference's texture sources (MSVC-targeted .cu files) compile
+// with nvcc on Linux for the GPU-side texture pin (oracle/_ref/libhvvr_ref_gpu.so). Test
+// infrastructure only; never part of the product.
+#pragma once
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#if !defined(__CUDA_ARCH__)
+#include <immintrin.h>
+#include <x86intrin.h>
+#endif
+// BMI1 lowest-bit clear (the reference's util.h), spelled out for compilers without -mbmi
+static inline uint32_t hv_blsr32(uint32_t a) { return a & (a - 1u); }
+static inline uint64_t hv_blsr64(uint64_t a) { return a & (a - 1u); }
+#define _blsr_u32 hv_blsr32
+#define _blsr_u64 hv_blsr64
+
+#ifndef __forceinline
+#define __forceinline inline __attribute__((always_inline))
+#endif
+static inline unsigned char _bittest(const long* base, long offset) {
+    return (unsigned char)((((const uint32_t*)base)[offset >> 5] >> (offset & 31)) & 1u);
+}
+static inline unsigned char _BitScanForward(unsigned long* index, unsigned long mask) {
+    if (!mask) return 0;
+    *index = (unsigned long)__builtin_ctzl(mask);
+    return 1;
+}
+static inline void* _aligned_malloc(size_t size, size_t alignment) {
+    if (alignment < sizeof(void*)) alignment = sizeof(void*);
+    void* p = nullptr;
+    if (posix_memalign(&p, alignment, size ? size : alignment)) return nullptr;
+    return p;
+}
+static inline void _aligned_free(void* p) { free(p); }

@@ -14,6 +14,23 @@ REF_SRCS = $(RC)/traverse_avx.cpp $(RC)/sample_hierarchy.cpp $(RC)/samples.cpp $
            $(RC)/foveated.cpp $(SH)/bvh.cpp $(SH)/debug.cpp $(SS)/model_import_bin.cpp
 OBJS = $(patsubst %.cpp,_ref/obj/%.o,$(notdir $(REF_SRCS))) _ref/obj/frusta.o _ref/obj/ref_harness.o _ref/obj/ref_stubs.o
 
+NVCC ?= nvcc
+# the reference's texture creation and sampling built for the GPU (its project compiles CUDA with
+# fast math), with the harness in ref_gpu_harness.cu
+REF_GPU_FLAGS = -gencode arch=compute_100a,code=sm_100a -use_fast_math -std=c++17 -Xcompiler -fPIC,-mf16c -w \
+                -include refshim/compat/hvvr_nvcc_compat.h -I$(SH) -I$(RC)
+
+all: _ref/libhvvr_ref.so _ref/libhvvr_ref_gpu.so
+
+_ref/libhvvr_ref_gpu.so: _ref/obj/texture.cu.o _ref/obj/ref_gpu_harness.cu.o
+	$(NVCC) -shared -gencode arch=compute_100a,code=sm_100a -o $@ $^
+_ref/obj/texture.cu.o: $(RC)/texture.cu refshim/compat/hvvr_nvcc_compat.h
+	@mkdir -p _ref/obj
+	$(NVCC) $(REF_GPU_FLAGS) -c $< -o $@
+_ref/obj/ref_gpu_harness.cu.o: refshim/ref_gpu_harness.cu refshim/compat/hvvr_nvcc_compat.h
+	@mkdir -p _ref/obj
+	$(NVCC) $(REF_GPU_FLAGS) -c $< -o $@
+
 # -Bsymbolic: the host stand-ins for the CUDA runtime calls (ref_stubs.cpp) must bind inside this
 # library even when a real libcudart is already loaded into the process
 _ref/libhvvr_ref.so: $(OBJS)

@@ -45,6 +45,8 @@
 
 thread_local uint3 threadIdx;
 thread_local uint3 blockIdx;
+hv_texture_hook_fn hv_texture_hook = nullptr;
+void* hv_texture_hook_ctx = nullptr;
 
 namespace hvvr {
 // Link stubs for GPU-side classes referenced by camera.cpp's Camera methods. The harness
@@ -274,6 +276,12 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             env.spotLights[env.spotLightCount++] = l.spot;
     }
     const SimpleMaterial* materials = (const SimpleMaterial*)md.materials;
+    // material textures: the texture object of id i is i, and ReadTexture's tex2DGrad goes to the
+    // frame's texture sampler
+    hv_texture_hook = in->texture_count ? in->texture_sample : nullptr;
+    hv_texture_hook_ctx = in->texture_ctx;
+    std::vector<cudaTextureObject_t> textureObjects(SimpleMaterial::maxTextureCount);
+    for (uint32_t i = 0; i < SimpleMaterial::maxTextureCount; i++) textureObjects[i] = cudaTextureObject_t(i);
     vector3 cameraPos = vector3(cameraToWorld.m3);
     std::vector<vector2> alphaTab(N);
     for (uint32_t i = 0; i < N; i++) alphaTab[i] = subsampleOffset(N, int(i));
@@ -430,22 +438,37 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                             centroidDirUV += dirUV * sampleCountInv;
                         }
                     }
-                    vector3 b;
+                    vector3 b, bOffX, bOffY;
                     if (dof) {
                         IntersectTriangleTile<true> tt;
                         tt.setup(tris[triIndex], cameraPos, tileDoF.lensU, tileDoF.lensV);
                         IntersectTriangleThreadDoF th(tt, lensCenterToFocalCenter);
                         th.calcUVW(tt, lensCenterToFocalCenter, tileDoF.lensU, tileDoF.lensV, centroidLensUV,
                                    centroidDirUV, b);
+                        vector2 derivScale = vector2(1.0f, 1.0f);
+                        vector2 dirUV_dX = centroidDirUV + vector2(derivScale.x, 0.0f);
+                        th.calcUVW(tt, lensCenterToFocalCenter, tileDoF.lensU, tileDoF.lensV, centroidLensUV, dirUV_dX,
+                                   bOffX);
+                        vector2 dirUV_dY = centroidDirUV + vector2(0.0f, derivScale.y);
+                        th.calcUVW(tt, lensCenterToFocalCenter, tileDoF.lensU, tileDoF.lensV, centroidLensUV, dirUV_dY,
+                                   bOffY);
                     } else {
                         IntersectTriangleTile<false> tt;
                         tt.setup(tris[triIndex], cameraPos);
                         IntersectTriangleThread th(tt, sample.centerRay, sample.du, sample.dv);
                         th.calcUVW(tt, centroidAlpha, b);
+                        vector2 alpha_dX = centroidAlpha + vector2(1.0f, 0.0f);
+                        th.calcUVW(tt, alpha_dX, bOffX);
+                        vector2 alpha_dY = centroidAlpha + vector2(0.0f, 1.0f);
+                        th.calcUVW(tt, alpha_dY, bOffY);
                     }
                     InterpolatedVertex vI = interpolate(world.data(), triShade[triIndex], b);
-                    vector4 shaded = GGXShade(triShade[triIndex].material, vI, vector2(0.0f), vector2(0.0f), cameraPos,
-                                              materials, nullptr, env);
+                    InterpolatedVertex vInterpX = interpolate(world.data(), triShade[triIndex], bOffX);
+                    InterpolatedVertex vInterpY = interpolate(world.data(), triShade[triIndex], bOffY);
+                    vector2 dUVdX = vInterpX.uv - vI.uv;
+                    vector2 dUVdY = vInterpY.uv - vI.uv;
+                    vector4 shaded = GGXShade(triShade[triIndex].material, vI, dUVdX, dUVdY, cameraPos, materials,
+                                              textureObjects.data(), env);
                     result += shaded * float(__builtin_popcount(sampleMask));
                 }
                 result *= 1.0f / N;
