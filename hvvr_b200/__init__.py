@@ -93,7 +93,7 @@ _sig("hvvr_scene_file_light", _vp, _u32, _p(_abi.LightUnion))
 _sig("hvvr_scene_file_texture", _vp, _u32, _p(_u32), _p(_u32), _p(_u32), _p(_u32), _p(_vp), _p(C.c_uint64))
 _lib.hvvr_scene_file_close.argtypes = [_vp]
 _lib.hvvr_scene_file_close.restype = None
-_sig("hvvr_scene_file_save", C.c_char_p, _vp, _vp, _u32, _vp, _u32)
+_sig("hvvr_scene_file_save", C.c_char_p, _vp, _u32, _vp, _vp, _u32, _vp, _u32)
 _sig("hvvr_samples_load", C.c_char_p, _vp, _u32, _p(_u32))
 _sig("hvvr_samples_save", C.c_char_p, _vp, _u32)
 _sig("hvvr_polar_foveated_layout", _vp, _p(_u32), _p(_u32), _p(_u32), _p(_u32))
@@ -284,9 +284,31 @@ def load_scene_file(path):
         _lib.hvvr_scene_file_close(h)
 
 
-def save_scene_file(path, meshes, lights=()):
-    """Writes scenes.Scene meshes (topology from .nodes when set, transform from .transform or
-    identity) and lights in the reference's binary scene format."""
+def create_objects(rc, loaded):
+    """model_import::createObjects (libraries/hvvr/samples_shared/model_import.cpp:41-63): the
+    textures of a load_scene_file result first (so their ids are the file's texture indices), then
+    its lights, then one model per mesh with the mesh's transform. Returns (textures, lights, models)."""
+    texs = [rc.create_texture(t["texels"], t["format"], t["width"], t["height"], t["stride"])
+            for t in loaded["textures"]]
+    lights = [rc.create_light(l) for l in loaded["lights"]]
+    models = []
+    for sc in loaded["meshes"]:
+        m = rc.create_model(sc)
+        m.set_transform(sc.transform)
+        models.append(m)
+    return texs, lights, models
+
+
+def save_scene_file(path, meshes, lights=(), textures=()):
+    """Writes textures (dicts as load_scene_file returns them), lights and scenes.Scene meshes
+    (topology from .nodes when set, transform from .transform or identity) in the reference's
+    binary scene format."""
+    tds = (_abi.TextureData * max(1, len(textures)))()
+    tkeep = []
+    for i, t in enumerate(textures):
+        b = np.ascontiguousarray(t["texels"]).view(np.uint8)
+        tkeep.append(b)
+        tds[i] = _abi.TextureData(b.ctypes.data, t["format"], t["width"], t["height"], t.get("stride", t["width"]))
     mds = (_abi.MeshData * max(1, len(meshes)))()
     xfs = (_abi.Transform * max(1, len(meshes)))()
     keep = []
@@ -299,7 +321,7 @@ def save_scene_file(path, meshes, lights=()):
                                _abi.ptr(arrays[3]), len(arrays[3]))
         xfs[i] = getattr(sc, "transform", None) or _abi.transform()
     ls = (_abi.LightUnion * max(1, len(lights)))(*lights)
-    _check(_lib.hvvr_scene_file_save(os.fsencode(path), mds, xfs, len(meshes), ls, len(lights)))
+    _check(_lib.hvvr_scene_file_save(os.fsencode(path), tds, len(textures), mds, xfs, len(meshes), ls, len(lights)))
 
 
 def load_samples(path):

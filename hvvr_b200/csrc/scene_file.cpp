@@ -180,15 +180,28 @@ int hvvr_scene_file_texture(const hvvr_scene_file* f, uint32_t i, uint32_t* form
 
 void hvvr_scene_file_close(hvvr_scene_file* f) { delete f; }
 
-int hvvr_scene_file_save(const char* path, const hvvr_mesh_data* meshes, const hvvr_transform* transforms,
-                         uint32_t mesh_count, const hvvr_light_union* lights, uint32_t light_count) {
-    if (!path || (mesh_count && (!meshes || !transforms)) || (light_count && !lights))
+int hvvr_scene_file_save(const char* path, const hvvr_texture_data* textures, uint32_t texture_count,
+                         const hvvr_mesh_data* meshes, const hvvr_transform* transforms, uint32_t mesh_count,
+                         const hvvr_light_union* lights, uint32_t light_count) {
+    if (!path || (texture_count && !textures) || (mesh_count && (!meshes || !transforms)) || (light_count && !lights))
         return fail(HVVR_ERR_INVALID, "NULL argument");
+    for (uint32_t n = 0; n < texture_count; n++) {
+        if (!texelBytes(textures[n].format)) return fail(HVVR_ERR_INVALID, "texture %u: unknown format", n);
+        if (!textures[n].data && textures[n].stride_elements && textures[n].height)
+            return fail(HVVR_ERR_INVALID, "texture %u: no texels", n);
+    }
     File fl;
     fl.f = fopen(path, "wb");
     if (!fl.f) return fail(HVVR_ERR_NOT_FOUND, "cannot create scene file %s", path);
-    const BinHeader h{kBinVersion, 0, light_count, mesh_count};
-    bool ok = fl.write(&h, sizeof(h)) && fl.write(lights, size_t(light_count) * sizeof(hvvr_light_union));
+    const BinHeader h{kBinVersion, texture_count, light_count, mesh_count};
+    bool ok = fl.write(&h, sizeof(h));
+    // per texture its record and getTextureSize(stride, height, format) bytes of texels
+    for (uint32_t n = 0; ok && n < texture_count; n++) {
+        const hvvr_texture_data& t = textures[n];
+        const BinTexture bt{t.format, t.width, t.height, t.stride_elements};
+        ok = fl.write(&bt, sizeof(bt)) && fl.write(t.data, uint64_t(t.stride_elements) * t.height * texelBytes(t.format));
+    }
+    ok = ok && fl.write(lights, size_t(light_count) * sizeof(hvvr_light_union));
     for (uint32_t n = 0; ok && n < mesh_count; n++) {
         const hvvr_mesh_data& m = meshes[n];
         const BinMesh bm{transforms[n], m.vert_count, m.tri_count, m.node_count, m.material_count};

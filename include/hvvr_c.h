@@ -348,9 +348,11 @@ int hvvr_scene_file_light(const hvvr_scene_file* file, uint32_t i, hvvr_light_un
 int hvvr_scene_file_texture(const hvvr_scene_file* file, uint32_t i, uint32_t* format, uint32_t* width,
                             uint32_t* height, uint32_t* stride, const void** texels, uint64_t* bytes);
 void hvvr_scene_file_close(hvvr_scene_file* file);
-/* writes meshes (with their transforms) and lights, no textures, in the same format */
-int hvvr_scene_file_save(const char* path, const hvvr_mesh_data* meshes, const hvvr_transform* transforms,
-                         uint32_t mesh_count, const hvvr_light_union* lights, uint32_t light_count);
+/* writes textures (stride_elements * height texels each), lights and meshes (with their
+ * transforms) in the same format (saveBin) */
+int hvvr_scene_file_save(const char* path, const hvvr_texture_data* textures, uint32_t texture_count,
+                         const hvvr_mesh_data* meshes, const hvvr_transform* transforms, uint32_t mesh_count,
+                         const hvvr_light_union* lights, uint32_t light_count);
 /* sample files (loadSamples / saveSamples, libraries/hvvr/raycaster/samples.cpp:161-187):
  * {magic 0x0CD1, version 0, reserved, count} then the samples. samples == NULL: count only. */
 int hvvr_samples_load(const char* path, hvvr_sample* samples, uint32_t capacity, uint32_t* count);

@@ -649,12 +649,15 @@ extern "C" int ref_bin_save(const char* path, const hvvr_mesh_data* meshes, cons
     return model_import::saveBin(path, model) ? 0 : 1;
 }
 
-// loadBin: counts[4] = {textures, lights, meshes, total bytes of the mesh arrays}; with out != NULL
-// the lights then every mesh's transform and arrays are packed into out in file order
+// loadBin: counts[4] = {textures, lights, meshes, total bytes}; with out != NULL every texture's
+// {format, width, height, stride} and texels (getTextureSize), then the lights, then every mesh's
+// transform and arrays are packed into out in file order
 extern "C" int ref_bin_load(const char* path, uint64_t* counts, uint8_t* out) {
     model_import::Model model;
     if (!model_import::loadBin(path, model)) return 1;
     uint64_t bytes = model.lights.size() * sizeof(hvvr::LightUnion);
+    for (const auto& t : model.textures)
+        bytes += 16 + hvvr::getTextureSize(t.tex.strideElements, t.tex.height, t.tex.format);
     for (const auto& m : model.meshes)
         bytes += sizeof(hvvr::transform) + m.data.verts.size() * 32 + m.data.triShade.size() * 16 +
                  m.data.nodes.size() * 32 + m.data.materials.size() * 64;
@@ -664,6 +667,11 @@ extern "C" int ref_bin_load(const char* path, uint64_t* counts, uint8_t* out) {
     counts[3] = bytes;
     if (!out) return 0;
     auto put = [&](const void* p, size_t n) { memcpy(out, p, n); out += n; };
+    for (const auto& t : model.textures) {
+        const uint32_t rec[4] = {uint32_t(t.tex.format), t.tex.width, t.tex.height, t.tex.strideElements};
+        put(rec, sizeof(rec));
+        put(t.tex.data, hvvr::getTextureSize(t.tex.strideElements, t.tex.height, t.tex.format));
+    }
     put(model.lights.data(), model.lights.size() * sizeof(hvvr::LightUnion));
     for (const auto& m : model.meshes) {
         put(&m.transform, sizeof(hvvr::transform));

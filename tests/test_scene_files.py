@@ -60,6 +60,31 @@ def test_library_scene_file_loads_in_reference(tmp_path):
 
 
 @needs_ref
+def test_library_scene_file_with_textures_loads_in_reference(tmp_path):
+    meshes, lights = _meshes()
+    tex = [{"format": 1, "width": 7, "height": 5, "texels": scenes.texture_rgba8(7, 5, seed=2)},
+           {"format": 4, "width": 3, "height": 2, "stride": 4,
+            "texels": np.arange(4 * 2 * 4, dtype=np.float32)}]
+    path = str(tmp_path / "lib_tex.bin")
+    hv.save_scene_file(path, meshes, lights, textures=tex)
+    lib = _ref()
+    counts = np.zeros(4, np.uint64)
+    assert lib.ref_bin_load(path.encode(), counts.ctypes.data, None) == 0
+    assert counts[:3].tolist() == [2, len(lights), len(meshes)]
+    out = np.zeros(int(counts[3]), np.uint8)
+    assert lib.ref_bin_load(path.encode(), counts.ctypes.data, out.ctypes.data) == 0
+    want = b""
+    for t in tex:
+        want += np.array([t["format"], t["width"], t["height"], t.get("stride", t["width"])], np.uint32).tobytes()
+        want += np.ascontiguousarray(t["texels"]).tobytes()
+    want += b"".join(bytes(l) for l in lights) + b"".join(_mesh_bytes(m) for m in meshes)
+    assert out.tobytes() == want
+    f = hv.load_scene_file(path)
+    assert [(t["format"], t["width"], t["height"], t["stride"]) for t in f["textures"]] == [(1, 7, 5, 7), (4, 3, 2, 4)]
+    assert f["textures"][1]["texels"].tobytes() == tex[1]["texels"].tobytes()
+
+
+@needs_ref
 def test_reference_scene_file_loads_in_library(tmp_path):
     meshes, lights = _meshes()
     path = str(tmp_path / "ref.bin")
