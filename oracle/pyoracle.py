@@ -325,8 +325,9 @@ class Reference:
 
 
 class ReferenceGpu:
-    """The reference's own texture creation (CreateTexture with its mip generator) and texture
-    reads (ReadTexture) built for the GPU (oracle/_ref/libhvvr_ref_gpu.so); needs a GPU."""
+    """The reference's own texture creation (CreateTexture with its mip generator), texture reads
+    (ReadTexture) and foveated resolve kernels built for the GPU (oracle/_ref/libhvvr_ref_gpu.so);
+    needs a GPU."""
 
     def __init__(self, path=REF_GPU_SO):
         if not os.path.exists(path):
@@ -361,6 +362,27 @@ class ReferenceGpu:
                                                  C.byref(w), C.byref(h))
         if rc != 0:
             raise RuntimeError("read_level: %d" % rc)
+        return out
+
+    def foveated_resolve(self, pattern, samples_per_ring, ring_count, polar_color, polar_depth, width, height,
+                         sample_to_eye, eye_to_sample_prev, history):
+        """The reference's own resolve kernels (ComputeMoments, FoveatedPolarToScreenSpaceKernel, the two
+        SeparableFilterUsingEccentricity passes, FinishConstrastEnhancement) on the given polar textures
+        and matrices: dict of moments [rings, spr, 2, 4], result, filtered, image [h, w]."""
+        f = self.lib.ref_gpu_foveated_resolve
+        f.restype = C.c_int
+        out = {"moments": np.zeros((ring_count, samples_per_ring, 2, 4), np.uint16),
+               "result": np.zeros((height, width), np.uint32), "filtered": np.zeros((height, width), np.uint32),
+               "image": np.zeros((height, width), np.uint32)}
+        ins = [np.ascontiguousarray(polar_color, np.uint32), np.ascontiguousarray(polar_depth, np.float32),
+               np.ascontiguousarray(sample_to_eye, np.float32), np.ascontiguousarray(eye_to_sample_prev, np.float32),
+               np.ascontiguousarray(history, np.uint32)]
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        rc = f(*[C.c_float(x) for x in pattern], C.c_uint32(samples_per_ring), C.c_uint32(ring_count), p(ins[0]),
+               p(ins[1]), C.c_uint32(width), C.c_uint32(height), p(ins[2]), p(ins[3]), p(ins[4]),
+               p(out["moments"]), p(out["result"]), p(out["filtered"]), p(out["image"]))
+        if rc != 0:
+            raise RuntimeError("foveated_resolve: %d" % rc)
         return out
 
     def sample(self, ids, q):

@@ -5,10 +5,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
-#if !defined(__CUDA_ARCH__)
 #include <immintrin.h>
 #include <x86intrin.h>
-#endif
 // BMI1 lowest-bit clear (the reference's util.h), spelled out for compilers without -mbmi
 static inline uint32_t hv_blsr32(uint32_t a) { return a & (a - 1u); }
 static inline uint64_t hv_blsr64(uint64_t a) { return a & (a - 1u); }
@@ -33,3 +31,14 @@ static inline void* _aligned_malloc(size_t size, size_t alignment) {
     return p;
 }
 static inline void _aligned_free(void* p) { free(p); }
+
+// The reference writes 64-bit texels with surf2Dwrite(uint64_t) (gpu_foveated.cu:30); uint64_t is
+// unsigned long on Linux, which CUDA's surface templates do not list, so forward it as the
+// unsigned long long they accept (same bits)
+#if defined(__CUDACC__)
+#include <surface_indirect_functions.h>
+static __device__ __forceinline__ void surf2Dwrite(unsigned long val, cudaSurfaceObject_t obj, int x, int y,
+                                                   cudaSurfaceBoundaryMode mode = cudaBoundaryModeTrap) {
+    surf2Dwrite((unsigned long long)val, obj, x, y, mode);
+}
+#endif

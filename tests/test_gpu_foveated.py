@@ -108,3 +108,40 @@ def test_foveated_resolve_matches_oracle(oracle):
         hist = res
     assert (img >> 24).min() >= 254 and (img & 0xFFFFFF).any()
     rc.close()
+
+
+@pytest.mark.skipif(not __import__("pyoracle").ReferenceGpu.available(), reason="oracle/_ref GPU library not built")
+def test_foveated_resolve_against_reference_kernels():
+    """The resolve against the reference's own kernels (gpu_foveated.cu built for this GPU by
+    oracle/refshim/ref_gpu_foveated.cu) on the GPU's polar textures, matrices and history, over
+    frames with camera and gaze motion."""
+    import pyoracle
+    ref = pyoracle.ReferenceGpu()
+    sc = scene("c1")
+    rc = _foveated_rc(sc)
+    w, h = 320, 288
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h)
+    cam.set_samples(scenes.grid_samples(w, h))
+    cam.set_msaa(4)
+    polar = hv.polar_foveated_samples(hv.foveated_spec(*PATTERN))
+    spr, rings = polar["samples_per_ring"], polar["ring_count"]
+    stats = []
+    for eye, gaze in [((0.0, 2.0, 10.0), (0.0, 0.0, -1.0)), ((0.15, 2.05, 9.9), (0.02, 0.01, -1.0)),
+                      ((0.3, 2.1, 9.8), (0.05, -0.02, -1.0))]:
+        cam.set_camera_to_world(scenes.camera_transform(eye=eye, target=(0.0, 0.0, 0.0)))
+        cam.set_eye_dir(gaze)
+        rc.render()
+        s2e, e2p, res, hist = cam.foveated_resolve()
+        pcol, pdep, pmom = cam.polar_textures(spr, rings)
+        r = ref.foveated_resolve(PATTERN, spr, rings, pcol, pdep, w, h, s2e, e2p, hist)
+        dm = np.abs(pmom.astype(np.int32) - r["moments"].astype(np.int32))
+        dr = np.abs(res.view(np.uint8).astype(np.int32) - r["result"].view(np.uint8).astype(np.int32))
+        di = np.abs(cam.image.view(np.uint8).astype(np.int32) - r["image"].view(np.uint8).astype(np.int32))
+        stats.append((dm.max(), dr.max(), (dr > 1).mean(), di.mean(), (di > 1).mean()))
+    rc.close()
+    for dm_max, dr_max, dr_gt1, di_mean, di_gt1 in stats:
+        # moments (unorm16) within 1/256 of full scale; the temporally filtered result within a few
+        # LSB; the contrast-enhanced image amplifies the result's differences up to 9x
+        assert dm_max <= 512 and dr_max <= 8 and dr_gt1 <= 0.005, stats
+        assert di_mean <= 1.5 and di_gt1 <= 0.2, stats
