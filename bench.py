@@ -747,12 +747,12 @@ def foveated_setup(hv, scenes, sc, target_cuda, torch):
 def resolve_bytes(polar, pixels):
     """Compulsory HBM bytes of a frame's foveated resolve launches, per eye summed: per polar
     sample 4 B colour + 4 B depth + 8 B remap read and 8 B written to the polar textures; per
-    polar texel the moments pass reads 4 B and writes 16 B, the polar -> screen pass reads 24 B;
-    per pixel the polar -> screen pass reads 4 B of history and writes 4 B of result and 24 B of
-    eccentricity and filter weights, the vertical pass reads 24 B and writes 4 B, the horizontal
-    pass reads 32 B and writes 4 B of image."""
+    polar texel the moments pass reads 4 B and writes 16 B, the polar -> screen pass reads 24 B
+    (colour, depth, moments); per pixel the polar -> screen pass reads 4 B of history and writes
+    4 B of result, each filter pass reads 4 B and writes 4 B, and the contrast enhancement reads
+    8 B and writes 4 B of image."""
     texels = polar["samples_per_ring"] * polar["ring_count"]
-    return polar["valid"] * 24 + texels * (4 + 16 + 24) + pixels * (4 + 4 + 24 + 24 + 4 + 32 + 4)
+    return polar["valid"] * 24 + texels * (4 + 16 + 24) + pixels * (4 + 4 + 8 + 8 + 8 + 4)
 
 
 def run_foveated(args):
@@ -863,7 +863,7 @@ def run_foveated(args):
                            "launch_ms_per_frame": statistics.mean(k[0] for k in kernel_ms)},
         "intersectShadeKernel<16,FMA>": {"algorithmic_bytes": intersect_bytes(counts),
                                          "launch_ms_per_frame": statistics.mean(k[1] for k in kernel_ms)},
-        "foveated resolve (5 kernels per eye)": {"algorithmic_bytes": 2 * resolve_bytes(polar, FOV_W * FOV_H),
+        "foveated resolve (6 kernels per eye)": {"algorithmic_bytes": 2 * resolve_bytes(polar, FOV_W * FOV_H),
                                                  "launch_ms_per_frame": resolve_ms},
     }
     for name, k in kernels.items():
@@ -894,8 +894,8 @@ def run_foveated(args):
                                [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
                                 (4, "resolve"), (5, "total")]},
         # per frame (ncu launch list): block cull, tile order, tile cull + retry pass + intersect
-        # (2 parts), 5 resolve kernels per eye
-        "gpu_launches": args.steps * 18,
+        # (2 parts), 6 resolve kernels per eye
+        "gpu_launches": args.steps * 20,
         "clocks": ck,
     }
     if rank == 0:

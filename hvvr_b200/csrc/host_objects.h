@@ -74,6 +74,28 @@ struct DevBuf {
     }
 };
 
+// A 2D CUDA array with a texture object (reads) and a surface object (writes), made as the
+// reference's createEmptyTexture makes one (libraries/hvvr/raycaster/texture.cu:283-321):
+// normalized coordinates, the given addressing per axis (clamp on the third) and filter.
+struct TexArray {
+    cudaArray_t array = nullptr;
+    cudaTextureObject_t tex = 0;
+    cudaSurfaceObject_t surf = 0;
+    uint32_t width = 0, height = 0, texelBytes = 0;
+    TexArray() = default;
+    TexArray(const TexArray&) = delete;
+    TexArray& operator=(const TexArray&) = delete;
+    ~TexArray() { release(); }
+    void release();
+    int create(uint32_t w, uint32_t h, const cudaChannelFormatDesc& channels, uint32_t texelBytes,
+               cudaTextureReadMode readMode, bool srgb, cudaTextureAddressMode addrX, cudaTextureAddressMode addrY,
+               bool linear);
+    // all texels zero
+    int clear(cudaStream_t st);
+    // the texels as rows of width * texelBytes bytes (synchronous)
+    int download(void* dst, cudaStream_t st) const;
+};
+
 } // namespace hvb
 
 // the object structs below are the C ABI's opaque types (global namespace)
@@ -144,12 +166,10 @@ struct hvvr_camera {
     DevBuf<float> tmax;               // [padded] view depth of subsample 0
     float eyeToWorld[16] = {};        // the last frame's batch-to-world matrix and cull planes
     float cullPlanes[4][4] = {};
-    // foveated resolve: polar textures, screen planes (fovResult[fovCur] is written by the next
+    // foveated resolve: polar textures, screen textures (fovResult[fovCur] is written by the next
     // frame, the other one holds the previous frame's result), the temporal history matrices
     // and the last frame's resolve matrices
-    DevBuf<uint32_t> polarColor, fovResult[2], fovFiltered;
-    DevBuf<float> polarDepth, fovEcc;
-    DevBuf<ushort4> moments;
+    TexArray polarRaw, polarDepth, moment1, moment2, fovResult[2], fovFilterV, fovFilterH;
     FoveaDev fovStatic{};             // buffers, sizes and mapping constants (no per-frame fields)
     uint32_t fovCur = 0;
     float worldToEyePrev[16] = {};

@@ -168,38 +168,6 @@ void lensTable(uint32_t n, float* out) {
         }
 }
 
-float srgbToLinear(float x) {
-    return (x <= 0.04045f) ? x * (1.0f / 12.92f) : float(pow(double((x + .055f) * (1.0f / 1.055f)), double(2.4f)));
-}
-
-float linearToSrgb(float x) {
-    return (x <= 0.0031308f) ? (x * 12.92f) : (float(pow(double(x), double(1.0f / 2.4f))) * 1.055f - .055f);
-}
-
-uint32_t srgbEncodeByte(float x) {
-    const float v = linearToSrgb(x) * 255.0f;
-    if (!(v > 0.0f)) return 0;  // negative and NaN: the device conversion saturates to 0
-    return v >= 4294967296.0f ? 0xffffffffu : uint32_t(v);
-}
-
-void colorTables(float dec[256], float thr[256]) {
-    for (int b = 0; b < 256; b++) dec[b] = srgbToLinear(float(b) / 255.0f);
-    // srgbEncodeByte is non-decreasing in x (pow is monotone on floats, both branches give
-    // byte 10 around the switch at 0.0031308), and non-negative floats order like their bits
-    thr[0] = -INFINITY;
-    for (uint32_t k = 1; k < 256; k++) {
-        uint32_t lo = 0, hi = 0x3f810000u;  // encode(0) = 0 < k <= encode(1.0078)
-        while (lo < hi) {
-            const uint32_t mid = lo + (hi - lo) / 2;
-            float x;
-            memcpy(&x, &mid, 4);
-            if (srgbEncodeByte(x) >= k) hi = mid;
-            else lo = mid + 1;
-        }
-        memcpy(&thr[k], &lo, 4);
-    }
-}
-
 void buildSampleSetup(const hvvr_sample* samples, uint32_t count, uint32_t split, const hvvr_float_rect& vp,
                       const hvvr_thin_lens& lens, float fovXDeg, float fovYDeg, uint32_t width, uint32_t height,
                       SampleSetup& out) {

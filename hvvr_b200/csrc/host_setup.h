@@ -54,16 +54,6 @@ void naiveCluster(std::vector<T>& v, size_t k, X x, Y y) {
 // depth-of-field lens positions for rate n: [4 tiles][n subsamples][128 samples] x 2 floats
 void lensTable(uint32_t n, float* out);
 
-// sRgbToLinear / linearToSRgb (libraries/hvvr/shared/util_graphics.h:16-33) with pow
-// evaluated in double and rounded to float
-float srgbToLinear(float x);
-float linearToSrgb(float x);
-// ToColor4Unorm8SRgb's channel byte: uint32_t(linearToSRgb(x) * 255.0f), saturating
-uint32_t srgbEncodeByte(float x);
-// the foveated resolve's colour tables: dec[b] = sRgbToLinear(b / 255.0f); thr[k] (k = 1..255)
-// the least non-negative float x with srgbEncodeByte(x) >= k (thr[0] = -inf)
-void colorTables(float dec[256], float thr[256]);
-
 struct SampleSetup {
     uint32_t blocks = 0, tiles = 0, padded = 0, valid = 0;
     std::vector<Rays4> tileRays, blockRays; // camera space

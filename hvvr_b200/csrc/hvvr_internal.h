@@ -120,21 +120,18 @@ struct CameraDev {
 };
 
 // The foveated resolve of one view (polar sample texture -> screen image, with temporal
-// reprojection and eccentricity-dependent contrast enhancement). Buffers in HBM:
-//   polar textures [rings][samplesPerRing]: colour (RGBA8 sRGB), view depth, moments
-//   (first and second, RGBA16 unorm each, interleaved: ushort4 pairs)
-//   screen planes [height][width]: this frame's temporally filtered image and the previous
-//   frame's (RGBA8 sRGB), the vertical filter pass (RGBA8 sRGB), the eccentricity and the five
-//   filter weights pow(1 - |R| / 5.1, sqrt(eccentricity)), R = 1..5, of each pixel
+// reprojection and eccentricity-dependent contrast enhancement). Every texture is a CUDA array
+// with a texture object for reads and a surface object for writes:
+//   polar textures [rings][samplesPerRing]: colour (RGBA8 sRGB), view depth (float), first and
+//   second moments (RGBA16 unorm each)
+//   screen textures [height][width] (RGBA8 sRGB): this frame's temporally filtered result and the
+//   previous frame's, the vertical filter pass and the full (vertical then horizontal) filter
 struct FoveaDev {
     const uint2* remap;        // [valid] polar texel (azimuth index, ring) of each sample
-    uint32_t* polarColor;      // [rings * spr]
-    float* polarDepth;         // [rings * spr]
-    ushort4* moments;          // [rings * spr * 2]
-    uint32_t* result;          // [h * w] written this frame
-    const uint32_t* history;   // [h * w] the previous frame's result
-    uint32_t* filtered;        // [h * w]
-    float* ecc;                // [6][h * w]: eccentricity, then weights R = 1..5
+    cudaTextureObject_t rawTex, depthTex, m1Tex, m2Tex;
+    cudaSurfaceObject_t rawSurf, depthSurf, m1Surf, m2Surf;
+    cudaTextureObject_t resultTex, prevTex, filterVTex, filterHTex; // result: written this frame
+    cudaSurfaceObject_t resultSurf, filterVSurf, filterHSurf;
     uint32_t* image;           // nullptr: the view has no foveated resolve
     uint32_t imageStride, width, height;
     uint32_t spr, rings, valid;
@@ -234,8 +231,6 @@ cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);
 // the launch shapes): scatter to the polar textures, moments, polar -> screen with temporal
 // reprojection, two eccentricity filter passes and contrast enhancement into fov.image
 cudaError_t launchFoveatedResolve(const FrameDev& fr, uint32_t view, const FoveaDev& fov, cudaStream_t st);
-// sRGB byte -> linear decode table and the 255 linear -> sRGB byte encode thresholds
-cudaError_t uploadColorTables(const float* decode256, const float* thresholds256, cudaStream_t st);
 // writes v to *dst with a one-thread kernel (no host memory involved; capturable)
 cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st);
 

@@ -299,23 +299,6 @@ void resetFoveatedHistory(hvvr_camera* cam) {
     memcpy(cam->eyePrevToSamplePrev, id, sizeof(id));
 }
 
-// the resolve's sRGB tables, once per device
-int ensureColorTables(cudaStream_t st) {
-    static std::mutex mu;
-    static bool uploaded[64] = {};
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return fail(HVVR_ERR_INVALID, "device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (uploaded[dev]) return HVVR_OK;
-    float dec[256], thr[256];
-    colorTables(dec, thr);
-    CUDA_TRY(uploadColorTables(dec, thr, st));
-    CUDA_TRY(cudaStreamSynchronize(st)); // the host tables go out of scope
-    uploaded[dev] = true;
-    return HVVR_OK;
-}
-
 // A camera of a foveated-polar raycaster (renderFoveatedPolarSpaceCudaReconstruct,
 // libraries/hvvr/raycaster/render.cpp:454-492): traversal and shading run on the raycaster's
 // polar sample set in eye space; the camera's own samples only bound the screen (sampleBounds,
@@ -363,26 +346,39 @@ int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st) {
     FoveaDev& fv = cam->fovStatic;
     fv = FoveaDev{};
     if (w && h) {
-        TRY(ensureColorTables(st));
-        const size_t texels = size_t(ps.samplesPerRing) * ps.ringCount, npix = size_t(w) * h;
-        TRY(cam->polarColor.alloc(texels));
-        TRY(cam->polarDepth.alloc(texels));
-        TRY(cam->moments.alloc(2 * texels));
-        for (int k = 0; k < 2; k++) {
-            TRY(cam->fovResult[k].alloc(npix));
-            CUDA_TRY(cudaMemsetAsync(cam->fovResult[k].p, 0, npix * 4, st));
-        }
-        TRY(cam->fovFiltered.alloc(npix));
-        TRY(cam->fovEcc.alloc(6 * npix));
-        CUDA_TRY(cudaMemsetAsync(cam->polarColor.p, 0, texels * 4, st));
-        CUDA_TRY(cudaMemsetAsync(cam->polarDepth.p, 0, texels * 4, st));
+        const size_t npix = size_t(w) * h;
+        const uint32_t spr = ps.samplesPerRing, rings = ps.ringCount;
+        const cudaChannelFormatDesc rgba8 = cudaCreateChannelDesc(8, 8, 8, 8, cudaChannelFormatKindUnsigned);
+        const cudaChannelFormatDesc rgba16 = cudaCreateChannelDesc(16, 16, 16, 16, cudaChannelFormatKindUnsigned);
+        const cudaChannelFormatDesc r32f = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+        const cudaTextureAddressMode wrap = cudaAddressModeWrap, clamp = cudaAddressModeClamp;
+        // polar textures: wrap in azimuth, clamp in eccentricity; depth point-sampled
+        TRY(cam->polarRaw.create(spr, rings, rgba8, 4, cudaReadModeNormalizedFloat, true, wrap, clamp, true));
+        TRY(cam->polarDepth.create(spr, rings, r32f, 4, cudaReadModeElementType, false, wrap, clamp, false));
+        TRY(cam->moment1.create(spr, rings, rgba16, 8, cudaReadModeNormalizedFloat, false, wrap, clamp, true));
+        TRY(cam->moment2.create(spr, rings, rgba16, 8, cudaReadModeNormalizedFloat, false, wrap, clamp, true));
+        // screen textures (createImageSizedTexture: clamp, linear)
+        for (int k = 0; k < 2; k++)
+            TRY(cam->fovResult[k].create(w, h, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
+        TRY(cam->fovFilterV.create(w, h, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
+        TRY(cam->fovFilterH.create(w, h, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
+        for (TexArray* t : {&cam->polarRaw, &cam->polarDepth, &cam->moment1, &cam->moment2, &cam->fovResult[0],
+                            &cam->fovResult[1], &cam->fovFilterV, &cam->fovFilterH})
+            TRY(t->clear(st));
         if (cpuTarget) TRY(cam->image.alloc(npix));
         fv.remap = cam->polarRemap.p;
-        fv.polarColor = cam->polarColor.p;
-        fv.polarDepth = cam->polarDepth.p;
-        fv.moments = cam->moments.p;
-        fv.filtered = cam->fovFiltered.p;
-        fv.ecc = cam->fovEcc.p;
+        fv.rawTex = cam->polarRaw.tex;
+        fv.rawSurf = cam->polarRaw.surf;
+        fv.depthTex = cam->polarDepth.tex;
+        fv.depthSurf = cam->polarDepth.surf;
+        fv.m1Tex = cam->moment1.tex;
+        fv.m1Surf = cam->moment1.surf;
+        fv.m2Tex = cam->moment2.tex;
+        fv.m2Surf = cam->moment2.surf;
+        fv.filterVTex = cam->fovFilterV.tex;
+        fv.filterVSurf = cam->fovFilterV.surf;
+        fv.filterHTex = cam->fovFilterH.tex;
+        fv.filterHSurf = cam->fovFilterH.surf;
         fv.image = cpuTarget ? cam->image.p : static_cast<uint32_t*>(cam->target.data);
         fv.imageStride = cpuTarget ? w : (cam->target.stride ? uint32_t(cam->target.stride) : w);
         fv.width = w;
@@ -473,7 +469,7 @@ size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa) {
         size_t b = size_t(d.tiles) * (sizeof(Rays4) + sizeof(TileList) + 4) +
                    size_t(d.blocks) * (sizeof(Rays4) + kBlockStack * sizeof(StackEntry) + 4) +
                    size_t(d.padded) * (48 + 8 + 4 + 4);
-        b += size_t(f.spr) * f.rings * (4 + 4 + 16) + size_t(f.width) * f.height * (4 * 3 + 24);
+        b += size_t(f.spr) * f.rings * (4 + 4 + 8 + 8) + size_t(f.width) * f.height * (4 * 4);
         if (cam->target.memory_type == HVVR_MEMORY_CPU) b += size_t(f.width) * f.height * 4;
         if (cam->capture & HVVR_CAPTURE_HITS) b += size_t(d.padded) * msaa * 8;
         return b;
@@ -938,8 +934,9 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
                                      cm->eyePrevToSamplePrev, v.fov.sampleToEye, v.fov.eyeToSamplePrev);
                 memcpy(cm->lastSampleToEye, v.fov.sampleToEye, sizeof(cm->lastSampleToEye));
                 memcpy(cm->lastEyeToSamplePrev, v.fov.eyeToSamplePrev, sizeof(cm->lastEyeToSamplePrev));
-                v.fov.result = cm->fovResult[cm->fovCur].p;
-                v.fov.history = cm->fovResult[cm->fovCur ^ 1u].p;
+                v.fov.resultTex = cm->fovResult[cm->fovCur].tex;
+                v.fov.resultSurf = cm->fovResult[cm->fovCur].surf;
+                v.fov.prevTex = cm->fovResult[cm->fovCur ^ 1u].tex;
                 cm->fovCur ^= 1u;
             }
         }
@@ -1803,10 +1800,10 @@ int hvvr_camera_read_foveated_resolve(const hvvr_camera* cam, float* sample_to_e
     if (!cam->foveated || !cam->fovStatic.image) return fail(HVVR_ERR_STATE, "not a foveated camera with a render target");
     if (sample_to_eye9) memcpy(sample_to_eye9, cam->lastSampleToEye, 9 * 4);
     if (eye_to_sample_prev16) memcpy(eye_to_sample_prev16, cam->lastEyeToSamplePrev, 16 * 4);
-    const size_t npix = size_t(cam->fovStatic.width) * cam->fovStatic.height;
-    // the last frame wrote fovResult[fovCur ^ 1] and read fovResult[fovCur]
-    if (result) CUDA_TRY(cudaMemcpy(result, cam->fovResult[cam->fovCur ^ 1u].p, npix * 4, cudaMemcpyDeviceToHost));
-    if (history) CUDA_TRY(cudaMemcpy(history, cam->fovResult[cam->fovCur].p, npix * 4, cudaMemcpyDeviceToHost));
+    // the last frame wrote fovResult[fovCur ^ 1] and read fovResult[fovCur] (legacy default
+    // stream: ordered after the frame's work)
+    if (result) TRY(cam->fovResult[cam->fovCur ^ 1u].download(result, 0));
+    if (history) TRY(cam->fovResult[cam->fovCur].download(history, 0));
     return HVVR_OK;
 }
 
@@ -1814,9 +1811,18 @@ int hvvr_camera_read_polar_textures(const hvvr_camera* cam, uint32_t* color, flo
     TRY(requireRendered(cam));
     if (!cam->foveated || !cam->fovStatic.image) return fail(HVVR_ERR_STATE, "not a foveated camera with a render target");
     const size_t texels = size_t(cam->fovStatic.spr) * cam->fovStatic.rings;
-    if (color) CUDA_TRY(cudaMemcpy(color, cam->polarColor.p, texels * 4, cudaMemcpyDeviceToHost));
-    if (depth) CUDA_TRY(cudaMemcpy(depth, cam->polarDepth.p, texels * 4, cudaMemcpyDeviceToHost));
-    if (moments) CUDA_TRY(cudaMemcpy(moments, cam->moments.p, texels * 16, cudaMemcpyDeviceToHost));
+    if (color) TRY(cam->polarRaw.download(color, 0));
+    if (depth) TRY(cam->polarDepth.download(depth, 0));
+    if (moments) {
+        // [texel][first, second][rgba] from the two RGBA16 textures
+        std::vector<uint64_t> m1(texels), m2(texels);
+        TRY(cam->moment1.download(m1.data(), 0));
+        TRY(cam->moment2.download(m2.data(), 0));
+        for (size_t k = 0; k < texels; k++) {
+            memcpy(moments + 8 * k, &m1[k], 8);
+            memcpy(moments + 8 * k + 4, &m2[k], 8);
+        }
+    }
     return HVVR_OK;
 }
 

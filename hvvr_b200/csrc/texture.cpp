@@ -108,6 +108,61 @@ int uploadTableNow(hvvr_raycaster* rc) {
 
 } // namespace
 
+void TexArray::release() {
+    if (tex) cudaDestroyTextureObject(tex);
+    if (surf) cudaDestroySurfaceObject(surf);
+    if (array) cudaFreeArray(array);
+    tex = 0;
+    surf = 0;
+    array = nullptr;
+    width = height = texelBytes = 0;
+}
+
+int TexArray::create(uint32_t w, uint32_t h, const cudaChannelFormatDesc& channels, uint32_t bytes,
+                     cudaTextureReadMode readMode, bool srgb, cudaTextureAddressMode addrX,
+                     cudaTextureAddressMode addrY, bool linear) {
+    release();
+    CUDA_TRY(cudaMallocArray(&array, &channels, w, h, cudaArraySurfaceLoadStore));
+    width = w;
+    height = h;
+    texelBytes = bytes;
+    cudaResourceDesc res;
+    memset(&res, 0, sizeof(res));
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = array;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = addrX;
+    td.addressMode[1] = addrY;
+    td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = linear ? cudaFilterModeLinear : cudaFilterModePoint;
+    td.readMode = readMode;
+    td.normalizedCoords = 1;
+    td.sRGB = srgb ? 1 : 0;
+    CUDA_TRY(cudaCreateTextureObject(&tex, &res, &td, nullptr));
+    CUDA_TRY(cudaCreateSurfaceObject(&surf, &res));
+    return HVVR_OK;
+}
+
+int TexArray::clear(cudaStream_t st) {
+    if (!array) return HVVR_OK;
+    const size_t row = size_t(width) * texelBytes;
+    DevBuf<uint8_t> zeros;
+    TRY(zeros.alloc(row * height));
+    CUDA_TRY(cudaMemsetAsync(zeros.p, 0, row * height, st));
+    CUDA_TRY(cudaMemcpy2DToArrayAsync(array, 0, 0, zeros.p, row, row, height, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return HVVR_OK;
+}
+
+int TexArray::download(void* dst, cudaStream_t st) const {
+    if (!array) return fail(HVVR_ERR_STATE, "no texture");
+    const size_t row = size_t(width) * texelBytes;
+    CUDA_TRY(cudaMemcpy2DFromArrayAsync(dst, row, array, 0, 0, row, height, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return HVVR_OK;
+}
+
 int uploadTextureTable(hvvr_raycaster* rc, cudaStream_t st) {
     std::vector<unsigned long long> table(rc->nextTextureId, 0ull);
     for (const auto& t : rc->textures) table[t->id] = t->object;

@@ -62,10 +62,15 @@ def test_foveated_eye_space_render_matches_oracle(oracle, msaa, fp_mode):
 
 def test_foveated_resolve_matches_oracle(oracle):
     """The resolve (polar textures, moments, temporal reprojection, eccentricity filters,
-    contrast enhancement) over frames with camera and gaze motion: each frame's temporally
-    filtered result and final image against the oracle run on the GPU's own sample colours and
-    view depths, with the GPU's previous result as the history. The per-frame matrices the GPU
-    used must equal the host entry's (pinned against the reference by the CPU tests)."""
+    contrast enhancement) over frames with camera and gaze motion, against the oracle run on the
+    GPU's own sample colours and view depths with the GPU's previous result as the history. The
+    GPU resolves through the texture unit with fast math, as the reference does (bit-exact against
+    the reference's kernels, test below); the oracle restates it with a software texture unit and
+    IEEE math, so the comparison is held to the bounds the texture unit's rounding allows: polar
+    colour within 1 LSB, moments within 1/64 of full scale, the temporally filtered result within
+    a few LSB, and the contrast-enhanced image (which scales the result's differences up to 9x)
+    on average within 1.5 LSB. The per-frame matrices the GPU used must equal the host entry's
+    (pinned against the reference by the CPU tests)."""
     sc = scene("c1")
     rc = _foveated_rc(sc)
     w, h = 320, 288
@@ -100,11 +105,16 @@ def test_foveated_resolve_matches_oracle(oracle):
         fo = oracle.foveated_resolve(PATTERN, polar, colors[:valid], depth[:valid], w, h, s2e, e2p, hist)
         img = cam.image
         pcol, _, pmom = cam.polar_textures(polar["samples_per_ring"], polar["ring_count"])
-        # bit-exact: every division is IEEE on the GPU and acos/atan2/log/cos/sin/pow are
-        # evaluated in double and rounded to float on both sides
-        for name, got, want in (("polar colour", pcol, fo["polar_color"]), ("moments", pmom, fo["moments"]),
-                                ("result", res, fo["result"]), ("image", img, fo["image"])):
-            assert np.array_equal(got, want), (name, int(np.count_nonzero(got != want)))
+        def diff(a, b):
+            if a.dtype == np.uint16:
+                return np.abs(a.astype(np.int32) - b.astype(np.int32))
+            return np.abs(a.view(np.uint8).astype(np.int32) - b.view(np.uint8).astype(np.int32))
+        dc, dm, dr, di = (diff(pcol, fo["polar_color"]), diff(pmom, fo["moments"]), diff(res, fo["result"]),
+                          diff(img, fo["image"]))
+        assert dc.max() <= 1, ("polar colour", int(dc.max()))
+        assert dm.max() <= 1024, ("moments", int(dm.max()))
+        assert dr.max() <= 8 and (dr > 1).mean() <= 0.005, ("result", int(dr.max()), float((dr > 1).mean()))
+        assert di.mean() <= 1.5 and (di > 1).mean() <= 0.2, ("image", float(di.mean()), float((di > 1).mean()))
         hist = res
     assert (img >> 24).min() >= 254 and (img & 0xFFFFFF).any()
     rc.close()
@@ -114,7 +124,8 @@ def test_foveated_resolve_matches_oracle(oracle):
 def test_foveated_resolve_against_reference_kernels():
     """The resolve against the reference's own kernels (gpu_foveated.cu built for this GPU by
     oracle/refshim/ref_gpu_foveated.cu) on the GPU's polar textures, matrices and history, over
-    frames with camera and gaze motion."""
+    frames with camera and gaze motion: moments, temporally filtered result and final image
+    bit-exact."""
     import pyoracle
     ref = pyoracle.ReferenceGpu()
     sc = scene("c1")
@@ -141,7 +152,4 @@ def test_foveated_resolve_against_reference_kernels():
         stats.append((dm.max(), dr.max(), (dr > 1).mean(), di.mean(), (di > 1).mean()))
     rc.close()
     for dm_max, dr_max, dr_gt1, di_mean, di_gt1 in stats:
-        # moments (unorm16) within 1/256 of full scale; the temporally filtered result within a few
-        # LSB; the contrast-enhanced image amplifies the result's differences up to 9x
-        assert dm_max <= 512 and dr_max <= 8 and dr_gt1 <= 0.005, stats
-        assert di_mean <= 1.5 and di_gt1 <= 0.2, stats
+        assert dm_max == 0 and dr_max == 0 and di_mean == 0, stats
