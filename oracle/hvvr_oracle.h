@@ -81,6 +81,8 @@ typedef struct {
     float* tile_rays;          /* [tiles*24] camera-space corner rays {origin[4][3], dir[4][3]} */
     uint32_t status;           /* nonzero if a capacity was exceeded */
     float* tmax;               /* [padded] view depth of subsample 0's hit (TMaxBuffer), +inf on a miss */
+    float* tile_frusta;        /* [tiles*24] world-space SimpleRayFrustum {origins[4], directions[4]}
+                                  (written by the reference harness) */
 } oracle_frame_out;
 
 /* The foveated path's frame: given batch-space (eye-space) beams and tile/block frusta, the

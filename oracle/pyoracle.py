@@ -34,7 +34,7 @@ class FrameOut(C.Structure):
                 ("hit_ids", C.c_void_p), ("depth", C.c_void_p), ("depth64", C.c_void_p), ("gb_n", C.c_void_p),
                 ("gb_tri", C.c_void_p), ("gb_mask", C.c_void_p), ("colors", C.c_void_p), ("image", C.c_void_p),
                 ("remap", C.c_void_p), ("beams", C.c_void_p), ("nodes", C.c_void_p), ("tris", C.c_void_p),
-                ("tile_rays", C.c_void_p), ("status", C.c_uint32), ("tmax", C.c_void_p)]
+                ("tile_rays", C.c_void_p), ("status", C.c_uint32), ("tmax", C.c_void_p), ("tile_frusta", C.c_void_p)]
 
 
 class FovIn(C.Structure):
@@ -136,6 +136,8 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
         alloc("tris", (len(scene.tri_shade), 9), np.float32, "tris")
     if "tmax" in want:
         alloc("tmax", padded, np.float32, "tmax")
+    if "tile_frusta" in want:
+        alloc("tile_frusta", (tiles, 24), np.float32, "tile_frusta")
     if beams_in is None:
         rc = fn(C.byref(fin), C.byref(out))
     else:
@@ -383,6 +385,32 @@ class ReferenceGpu:
                p(out["moments"]), p(out["result"]), p(out["filtered"]), p(out["image"]))
         if rc != 0:
             raise RuntimeError("foveated_resolve: %d" % rc)
+        return out
+
+    def intersect_resolve(self, msaa, frame, scene, cam_xf):
+        """The reference's IntersectKernel + ResolveKernel on a reference-harness frame's beams, world
+        tile frusta, tile lists and triangles (render(..., want=("beams", "tile_frusta", "lists",
+        "scene"))) and the scene's shading arrays: dict of gb_tri, gb_mask [padded, msaa], colors,
+        tmax [padded]."""
+        f = self.lib.ref_gpu_intersect_resolve
+        f.restype = C.c_int
+        padded, tiles = frame.padded, frame.tiles
+        out = {"gb_tri": np.full((padded, msaa), 0xFFFFFFFF, np.uint32), "gb_mask": np.zeros((padded, msaa), np.uint32),
+               "colors": np.zeros(padded, np.uint32), "tmax": np.zeros(padded, np.float32)}
+        keep = [np.ascontiguousarray(frame.beams, np.float32), np.ascontiguousarray(frame.tile_frusta, np.float32),
+                np.ascontiguousarray(frame.tile_counts, np.uint32), np.ascontiguousarray(frame.tile_indices, np.uint32),
+                np.ascontiguousarray(frame.tris, np.float32), np.ascontiguousarray(scene.tri_shade),
+                np.ascontiguousarray(scene.verts), np.ascontiguousarray(scene.materials)]
+        lights = (_abi.LightUnion * max(1, len(scene.lights)))(*scene.lights)
+        xf = _abi.Transform()
+        C.memmove(C.byref(xf), C.byref(cam_xf), C.sizeof(xf))
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        rc = f(C.c_uint32(msaa), p(keep[0]), C.c_uint32(padded), p(keep[1]), C.c_uint32(tiles), p(keep[2]), p(keep[3]),
+               p(keep[4]), p(keep[5]), C.c_uint32(len(keep[5])), p(keep[6]), C.c_uint32(len(keep[6])), p(keep[7]),
+               C.c_uint32(len(keep[7])), C.cast(lights, C.c_void_p), C.c_uint32(len(scene.lights)),
+               C.cast(C.byref(xf), C.c_void_p), p(out["gb_tri"]), p(out["gb_mask"]), p(out["colors"]), p(out["tmax"]))
+        if rc != 0:
+            raise RuntimeError("intersect_resolve: %d" % rc)
         return out
 
     def sample(self, ids, q):

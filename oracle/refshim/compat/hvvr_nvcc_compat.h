@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <float.h>
 #include <immintrin.h>
 #include <x86intrin.h>
 // BMI1 lowest-bit clear (the reference's util.h), spelled out for compilers without -mbmi
@@ -41,4 +42,20 @@ static __device__ __forceinline__ void surf2Dwrite(unsigned long val, cudaSurfac
                                                    cudaSurfaceBoundaryMode mode = cudaBoundaryModeTrap) {
     surf2Dwrite((unsigned long long)val, obj, x, y, mode);
 }
+#endif
+
+// vector_math.h decodes a half on the device with __half2float({bits}). Under the CUDA 9 headers
+// the reference was written for, that braced list set the raw bits; under CUDA 11+ it selects
+// __half's integer-value constructor (bits 0x3c00 become 15360.0), so every vertex normal would
+// decode wrong. An unsigned short overload, an exact match for the braced bits, decodes them as
+// bits, as the reference intends and as its host path does (_cvtsh_ss).
+#if defined(__CUDACC__)
+#include <cuda_fp16.h>
+static __host__ __device__ __forceinline__ float hv_half2float(unsigned short bits) {
+    __half_raw r;
+    r.x = bits;
+    return __half2float(__half(r));
+}
+static __host__ __device__ __forceinline__ float hv_half2float(const __half h) { return __half2float(h); }
+#define __half2float hv_half2float
 #endif

@@ -23,9 +23,14 @@ REF_GPU_FLAGS = -gencode arch=compute_100a,code=sm_100a -use_fast_math -std=c++1
 all: _ref/libhvvr_ref.so _ref/libhvvr_ref_gpu.so
 
 _ref/libhvvr_ref_gpu.so: _ref/obj/texture.cu.o _ref/obj/gpu_image.cu.o _ref/obj/ref_gpu_harness.cu.o \
-                         _ref/obj/ref_gpu_foveated.cu.o
+                         _ref/obj/ref_gpu_foveated.cu.o _ref/obj/ref_gpu_intersect.cu.o
 	$(NVCC) -shared -gencode arch=compute_100a,code=sm_100a -o $@ $^
 _ref/obj/%.cu.o: $(RC)/%.cu refshim/compat/hvvr_nvcc_compat.h
+	@mkdir -p _ref/obj
+	$(NVCC) $(REF_GPU_FLAGS) -c $< -o $@
+# includes the reference's intersect.cu and resolve.cu to launch their kernels at every MSAA rate
+_ref/obj/ref_gpu_intersect.cu.o: refshim/ref_gpu_intersect.cu $(RC)/intersect.cu $(RC)/resolve.cu \
+                                 refshim/compat/hvvr_nvcc_compat.h
 	@mkdir -p _ref/obj
 	$(NVCC) $(REF_GPU_FLAGS) -c $< -o $@
 # includes the reference's gpu_foveated.cu to launch its resolve kernels

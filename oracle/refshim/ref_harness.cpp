@@ -228,6 +228,8 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             simple[t].directions[n] = tilesW[t].pointDir[n];
         }
     }
+    static_assert(sizeof(SimpleRayFrustum) == 96, "SimpleRayFrustum");
+    if (out->tile_frusta) memcpy(out->tile_frusta, simple.data(), size_t(tileCount) * sizeof(SimpleRayFrustum));
 
     // cullThread (RC/traversal.cpp:99-190), one block at a time
     std::vector<std::vector<uint32_t>> lists(tileCount);

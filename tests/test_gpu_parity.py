@@ -126,3 +126,40 @@ def test_thin_lens_depth_of_field(oracle, msaa, fp_mode):
     pin = render_oracle(oracle, sc, smp, w, h, msaa, cam_xf=xf, fp_mode=fp_mode)
     assert (fo.hit_ids != pin.hit_ids).any(), "the lens did not change the hits"
     rc.close()
+
+
+@pytest.mark.skipif(not __import__("pyoracle").ReferenceGpu.available(), reason="oracle/_ref GPU library not built")
+@pytest.mark.parametrize("name,w,h,msaa,kind", [("c1", 640, 480, 1, "grid"), ("c1", 640, 480, 4, "barrel"),
+                                               ("c1", 640, 480, 8, "barrel"), ("c1", 320, 240, 16, "grid"),
+                                               ("small", 256, 192, 32, "barrel")])
+def test_against_reference_kernels(name, w, h, msaa, kind):
+    """Hit IDs, coverage masks and colours against the reference's own IntersectKernel and
+    ResolveKernel built for this GPU (oracle/refshim/ref_gpu_intersect.cu), fed the reference
+    host code's beams, world tile frusta and tile lists: the compressed G-buffer (triangle, mask)
+    pairs equal on every sample of every occupied tile but at most one, and colours within 1 LSB
+    elsewhere. The reference's kernels are built with fast math; on the recorded cases one
+    subsample on an edge shared by two triangles resolves to the other triangle (recorded in the
+    design notes), in both of this library's FP modes."""
+    import pyoracle
+    from hvvr_b200 import scenes as sc_mod
+    refg, refh = pyoracle.ReferenceGpu(), pyoracle.Reference()
+    sc = scene(name)
+    smp = sc_mod.grid_samples(w, h) if kind == "grid" else sc_mod.barrel_samples(w, h)
+    xf = sc_mod.camera_transform()
+    fr = refh.render(sc, smp, xf, sc_mod.viewport_for(w, h), w, h, msaa, fp_mode=hv.HVVR_FP_STRICT, threads=8,
+                     want=("beams", "tile_frusta", "lists", "scene", "gbuffer", "colors"))
+    r = refg.intersect_resolve(msaa, fr, sc, xf)
+    n = len(smp)
+    occupied = np.nonzero(np.repeat(fr.tile_counts > 0, 128)[:n])[0]
+    for mode in (hv.HVVR_FP_FMA, hv.HVVR_FP_STRICT):
+        rc, cam = render_gpu(sc, smp, w, h, msaa, cam_xf=xf, fp_mode=mode)
+        gn, gt, gm = cam.gbuffer()
+        col = cam.sample_colors()
+        rc.close()
+        bad = [s for s in occupied if not (np.array_equal(gt[s, :gn[s]], r["gb_tri"][s, :gn[s]]) and
+                                            np.array_equal(gm[s, :gn[s]], r["gb_mask"][s, :gn[s]]))]
+        assert len(bad) <= 1, (mode, bad[:8])
+        keep = np.ones(n, bool)
+        keep[bad] = False
+        d = np.abs(col[:n].view(np.uint8).astype(np.int32) - r["colors"][:n].view(np.uint8).astype(np.int32))
+        assert d.reshape(n, 4)[keep].max() <= 1, (mode, int(d.reshape(n, 4)[keep].max()))
