@@ -162,6 +162,28 @@ def stereo_setup(hv, scenes, sc, target_cuda, torch):
     return rc, cams, images, smp, eyes
 
 
+def sample_setup_ms(hv, scenes):
+    """Wall time of one eye's sample hierarchy (SampleData: clustering, tile and block frusta,
+    beams, image remap; 1,296,000 barrel-distorted samples), built on the device and on the host
+    (Camera.prepare, which returns once the setup is on the device)."""
+    smp = scenes.barrel_samples(W, H)
+    out = {"samples": int(len(smp))}
+    for name, mode in (("device", hv.HVVR_SETUP_DEVICE), ("host", hv.HVVR_SETUP_HOST)):
+        best = None
+        for _ in range(2 if name == "device" else 1):
+            rc = hv.Raycaster(sample_setup=mode)
+            cam = rc.create_camera(scenes.viewport_for(W, H))
+            cam.set_render_target(W, H)
+            cam.set_samples(smp)
+            t0 = time.perf_counter()
+            cam.prepare()
+            dt = (time.perf_counter() - t0) * 1e3
+            rc.close()
+            best = dt if best is None else min(best, dt)
+        out[name] = best
+    return out
+
+
 def frame_counts(hv, scenes, sc):
     """Counts of one captured stereo frame (both eyes) that define the algorithmic bytes."""
     rc, cams, _, _, _ = stereo_setup(hv, scenes, sc, False, None)
@@ -347,6 +369,7 @@ def main():
 
     # end to end through the C ABI: CPU_MEMORY targets, images copied to host every frame
     rc.close()
+    setup_ms = sample_setup_ms(hv, scenes)
     rc2, cams2, _, _, _ = stereo_setup(hv, scenes, sc, False, torch)
     for _ in range(max(2, args.warmup)):
         for c, xf in zip(cams2, eyes):
@@ -399,6 +422,7 @@ def main():
         # per frame (ncu launch list): block cull, tile order, tile cull + retry pass + intersect for
         # the slowest tiles and for the rest, remap per eye
         "gpu_launches": args.steps * 10,
+        "sample_setup_ms": setup_ms,
         "clocks": ck,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

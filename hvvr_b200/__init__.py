@@ -12,7 +12,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import (HVVR_CAPTURE_HITS, HVVR_FP_FMA, HVVR_FP_STRICT, HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA,  # noqa: F401
-                   HVVR_OK, HVVR_TEXTURE_R32_FLOAT, HVVR_TEXTURE_RGBA8_UNORM, HVVR_TEXTURE_RGBA8_UNORM_SRGB,
+                   HVVR_OK, HVVR_SETUP_DEVICE, HVVR_SETUP_HOST, HVVR_TEXTURE_R32_FLOAT, HVVR_TEXTURE_RGBA8_UNORM, HVVR_TEXTURE_RGBA8_UNORM_SRGB,
                    HVVR_TEXTURE_RGBA16_FLOAT, HVVR_TEXTURE_RGBA16_UNORM, HVVR_TEXTURE_RGBA32_FLOAT,
                    HVVR_TEXTURE_R11G11B10_FLOAT)
 
@@ -68,6 +68,7 @@ _sig("hvvr_camera_set_spherical_warp", _vp, C.c_float, C.c_float)
 _sig("hvvr_camera_set_render_target", _vp, _p(_abi.ImageDesc))
 _sig("hvvr_camera_set_samples", _vp, _vp, _u32, _u32)
 _sig("hvvr_camera_set_camera_to_world", _vp, _p(_abi.Transform))
+_sig("hvvr_camera_prepare", _vp, _p(_u32))
 _sig("hvvr_camera_set_msaa", _vp, _u32)
 _sig("hvvr_camera_get_sample_count", _vp, _p(_u32))
 _sig("hvvr_camera_set_capture", _vp, _u32)
@@ -145,7 +146,7 @@ EXPORTED = [
     "hvvr_texture_read_level", "hvvr_texture_sample", "hvvr_camera_create", "hvvr_camera_destroy", "hvvr_camera_set_enabled",
     "hvvr_camera_set_viewport", "hvvr_camera_set_lens", "hvvr_camera_set_aperture", "hvvr_camera_set_focal_depth",
     "hvvr_camera_set_eye_dir", "hvvr_camera_set_spherical_warp", "hvvr_camera_set_render_target",
-    "hvvr_camera_set_samples", "hvvr_camera_set_camera_to_world", "hvvr_camera_set_msaa",
+    "hvvr_camera_set_samples", "hvvr_camera_set_camera_to_world", "hvvr_camera_prepare", "hvvr_camera_set_msaa",
     "hvvr_camera_get_sample_count", "hvvr_camera_set_capture", "hvvr_camera_get_layout",
     "hvvr_camera_read_tile_lists", "hvvr_camera_read_block_stacks", "hvvr_camera_read_hits",
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
@@ -432,6 +433,12 @@ class Camera:
     def set_viewport(self, vp):
         _check(_lib.hvvr_camera_set_viewport(self.handle, C.byref(vp)))
 
+    def prepare(self):
+        """Builds the sample setup now; returns True when it was built on the host."""
+        on_host = _u32(0)
+        _check(_lib.hvvr_camera_prepare(self.handle, C.byref(on_host)))
+        return bool(on_host.value)
+
     def set_msaa(self, rate):
         _check(_lib.hvvr_camera_set_msaa(self.handle, rate))
 
@@ -555,7 +562,7 @@ class Camera:
 class Raycaster:
     """Raycaster(const RayCasterSpecification&) (libraries/hvvr/raycaster/raycaster.h:44)."""
 
-    def __init__(self, fp_mode=HVVR_FP_FMA, tri_index_capacity=0, device=0, spec=None):
+    def __init__(self, fp_mode=HVVR_FP_FMA, tri_index_capacity=0, device=0, spec=None, sample_setup=HVVR_SETUP_DEVICE):
         """spec: a full hvvr_spec (e.g. foveated_spec(...)); otherwise the defaults with these fields"""
         if spec is None:
             spec = _abi.Spec()
@@ -563,6 +570,7 @@ class Raycaster:
             spec.fp_mode = fp_mode
             spec.tri_index_capacity = tri_index_capacity
             spec.device = device
+            spec.sample_setup = sample_setup
         h = _vp()
         _check(_lib.hvvr_raycaster_create(C.byref(spec), C.byref(h)))
         self.handle = h

@@ -21,6 +21,7 @@ HVVR_LIGHT_NONE, HVVR_LIGHT_DIRECTIONAL, HVVR_LIGHT_POINT, HVVR_LIGHT_SPOT = 0, 
 HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA = 0, 1
 HVVR_MODE_DEFERRED_MSAA_RESOLVE, HVVR_MODE_FOVEATED_POLAR = 0, 1
 HVVR_FP_FMA, HVVR_FP_STRICT = 0, 1
+HVVR_SETUP_DEVICE, HVVR_SETUP_HOST = 0, 1
 HVVR_CAPTURE_HITS = 1
 
 
@@ -97,7 +98,8 @@ class Spec(C.Structure):
                 ("foveated_degree_tracking_error", C.c_float), ("foveated_max_fov_degrees", C.c_float),
                 ("foveated_mar_slope", C.c_float), ("foveated_foveal_mar_degrees", C.c_float),
                 ("output_format", C.c_uint32), ("output_to_3d_api", C.c_uint32),
-                ("fp_mode", C.c_uint32), ("tri_index_capacity", C.c_uint64), ("device", C.c_int)]
+                ("fp_mode", C.c_uint32), ("tri_index_capacity", C.c_uint64), ("device", C.c_int),
+                ("sample_setup", C.c_uint32)]
 
 
 class TileCullArgs(C.Structure):

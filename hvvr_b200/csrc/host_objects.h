@@ -139,6 +139,7 @@ struct hvvr_camera {
     uint32_t msaa = 16;
     uint32_t capture = 0;
     bool setupDirty = true;
+    bool setupOnHost = false;         // the current sample setup was built on the host
     bool rendered = false;
     bool hidden = false;              // a server's camera: rendered only by batches that name it
     uint64_t setupGen = 0;            // process-unique id of the current sample setup and buffers

@@ -23,6 +23,7 @@
 
 #include "foveated.h"
 #include "host_objects.h"
+#include "sample_setup.h"
 
 using namespace hvb;
 
@@ -246,13 +247,37 @@ int setupCamera(hvvr_camera* cam, cudaStream_t st) {
     if (cam->samples.empty()) return fail(HVVR_ERR_STATE, "camera has no samples");
     if (cam->rc->spec.mode == HVVR_MODE_FOVEATED_POLAR) return setupFoveatedCamera(cam, st);
     const uint32_t w = cam->target.width, h = cam->target.height;
-    buildSampleSetup(cam->samples.data(), uint32_t(cam->samples.size()), cam->split, cam->viewport, cam->lens,
-                     cam->fovX, cam->fovY, w, h, cam->setup);
+    // the sample hierarchy: on the device unless the spec asks for the host, the spherical
+    // mapping is on (its sin/cos follow the host's libm), or two samples share a position
+    bool host = cam->rc->spec.sample_setup == HVVR_SETUP_HOST || cam->fovX > 0.0f;
+    if (!host) {
+        DeviceSampleSetup ds{&cam->tileRays, &cam->blockRays, &cam->beams, &cam->remap};
+        TRY(buildSampleSetupDevice(cam->samples.data(), uint32_t(cam->samples.size()), cam->split, cam->viewport,
+                                   cam->lens, w, h, ds, st, host));
+        if (!host) {
+            cam->setup = SampleSetup{};
+            cam->setup.blocks = ds.blocks;
+            cam->setup.tiles = ds.tiles;
+            cam->setup.padded = ds.padded;
+            cam->setup.valid = ds.valid;
+        }
+    }
+    if (host) {
+        buildSampleSetup(cam->samples.data(), uint32_t(cam->samples.size()), cam->split, cam->viewport, cam->lens,
+                         cam->fovX, cam->fovY, w, h, cam->setup);
+        SampleSetup& hs = cam->setup;
+        TRY(cam->tileRays.upload(hs.tileRays.data(), hs.tileRays.size(), st));
+        TRY(cam->blockRays.upload(hs.blockRays.data(), hs.blockRays.size(), st));
+        TRY(cam->beams.upload(hs.beams.data(), hs.beams.size() / 4, st));
+        TRY(cam->remap.upload(hs.remap.data(), hs.remap.size(), st));
+        CUDA_TRY(cudaStreamSynchronize(st));  // the host arrays are released next
+        hs.tileRays = {};
+        hs.blockRays = {};
+        hs.beams = {};
+        hs.remap = {};
+    }
+    cam->setupOnHost = host;
     const SampleSetup& ss = cam->setup;
-    TRY(cam->tileRays.upload(ss.tileRays.data(), ss.tileRays.size(), st));
-    TRY(cam->blockRays.upload(ss.blockRays.data(), ss.blockRays.size(), st));
-    TRY(cam->beams.upload(ss.beams.data(), ss.beams.size() / 4, st));
-    TRY(cam->remap.upload(ss.remap.data(), ss.remap.size(), st));
     TRY(cam->blockStacks.alloc(size_t(ss.blocks) * kBlockStack));
     TRY(cam->blockSizes.alloc(ss.blocks));
     TRY(cam->tileLists.alloc(ss.tiles));
@@ -475,8 +500,8 @@ size_t cameraBytes(const hvvr_camera* cam, uint32_t msaa) {
         return b;
     }
     const SampleSetup& ss = cam->setup;
-    size_t b = ss.tileRays.size() * sizeof(Rays4) + ss.blockRays.size() * sizeof(Rays4) + ss.beams.size() * 4 +
-               ss.remap.size() * 4;
+    size_t b = cam->tileRays.n * sizeof(Rays4) + cam->blockRays.n * sizeof(Rays4) + cam->beams.n * sizeof(float4) +
+               cam->remap.n * 4;
     b += size_t(ss.blocks) * kBlockStack * sizeof(StackEntry) + size_t(ss.blocks) * 4;
     b += size_t(ss.tiles) * (sizeof(TileList) + 4) + size_t(ss.padded) * 4;
     if (cam->target.memory_type == HVVR_MEMORY_CPU) b += size_t(cam->target.width) * cam->target.height * 4;
@@ -522,16 +547,17 @@ int cloneCamera(const hvvr_camera* src, hvvr_camera** out) {
     c->xf = src->xf;
     c->msaa = src->msaa;
     c->setup = src->setup;
+    c->setupOnHost = src->setupOnHost;
     const SampleSetup& ss = c->setup;
     const cudaStream_t st = src->rc->stream;
-    TRY(c->tileRays.alloc(ss.tileRays.size()));
-    TRY(c->blockRays.alloc(ss.blockRays.size()));
-    TRY(c->beams.alloc(ss.beams.size() / 4));
-    TRY(c->remap.alloc(ss.remap.size()));
-    CUDA_TRY(cudaMemcpyAsync(c->tileRays.p, src->tileRays.p, ss.tileRays.size() * sizeof(Rays4), cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(c->blockRays.p, src->blockRays.p, ss.blockRays.size() * sizeof(Rays4), cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(c->beams.p, src->beams.p, ss.beams.size() * 4, cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(c->remap.p, src->remap.p, ss.remap.size() * 4, cudaMemcpyDeviceToDevice, st));
+    TRY(c->tileRays.alloc(src->tileRays.n));
+    TRY(c->blockRays.alloc(src->blockRays.n));
+    TRY(c->beams.alloc(src->beams.n));
+    TRY(c->remap.alloc(src->remap.n));
+    CUDA_TRY(cudaMemcpyAsync(c->tileRays.p, src->tileRays.p, src->tileRays.n * sizeof(Rays4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->blockRays.p, src->blockRays.p, src->blockRays.n * sizeof(Rays4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->beams.p, src->beams.p, src->beams.n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->remap.p, src->remap.p, src->remap.n * 4, cudaMemcpyDeviceToDevice, st));
     TRY(c->blockStacks.alloc(size_t(ss.blocks) * kBlockStack));
     TRY(c->blockSizes.alloc(ss.blocks));
     TRY(c->tileLists.alloc(ss.tiles));
@@ -1027,6 +1053,8 @@ int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out) {
     if (s.mode != HVVR_MODE_DEFERRED_MSAA_RESOLVE && s.mode != HVVR_MODE_FOVEATED_POLAR)
         return fail(HVVR_ERR_INVALID, "unknown mode");
     if (s.fp_mode != HVVR_FP_FMA && s.fp_mode != HVVR_FP_STRICT) return fail(HVVR_ERR_INVALID, "bad fp_mode");
+    if (s.sample_setup != HVVR_SETUP_DEVICE && s.sample_setup != HVVR_SETUP_HOST)
+        return fail(HVVR_ERR_INVALID, "bad sample_setup");
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) return fail(HVVR_ERR_CUDA, "no CUDA device available");
@@ -1741,11 +1769,22 @@ int hvvr_camera_read_sample_colors(const hvvr_camera* cam, uint32_t* rgba) {
     return HVVR_OK;
 }
 
+int hvvr_camera_prepare(hvvr_camera* cam, uint32_t* on_host) {
+    CAM_CHECK(cam);
+    CUDA_TRY(cudaSetDevice(cam->rc->spec.device));
+    if (cam->setupDirty) {
+        TRY(setupCamera(cam, cam->rc->stream));
+        CUDA_TRY(cudaStreamSynchronize(cam->rc->stream));
+    }
+    if (on_host) *on_host = cam->setupOnHost ? 1u : 0u;
+    return HVVR_OK;
+}
+
 int hvvr_camera_read_sample_remap(const hvvr_camera* cam, int32_t* remap, uint64_t count) {
     CAM_CHECK(cam);
     if (cam->setupDirty) return fail(HVVR_ERR_STATE, "sample setup not built yet (render once first)");
-    if (!remap || count < cam->setup.remap.size()) return fail(HVVR_ERR_INVALID, "remap buffer too small");
-    memcpy(remap, cam->setup.remap.data(), cam->setup.remap.size() * 4);
+    if (!remap || count < cam->remap.n) return fail(HVVR_ERR_INVALID, "remap buffer too small");
+    if (cam->remap.n) CUDA_TRY(cudaMemcpy(remap, cam->remap.p, cam->remap.n * 4, cudaMemcpyDeviceToHost));
     return HVVR_OK;
 }
 
@@ -1759,7 +1798,9 @@ int hvvr_camera_read_beams(const hvvr_camera* cam, float* beams9) {
         memcpy(beams9, ps.beams.data(), ps.beams.size() * sizeof(PolarBeam));
         return HVVR_OK;
     }
-    for (size_t i = 0; i < cam->setup.padded; i++) memcpy(beams9 + 9 * i, &cam->setup.beams[12 * i], 9 * 4);
+    std::vector<float4> b(cam->beams.n);
+    CUDA_TRY(cudaMemcpy(b.data(), cam->beams.p, b.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < cam->setup.padded; i++) memcpy(beams9 + 9 * i, &b[3 * i], 9 * 4);
     return HVVR_OK;
 }
 

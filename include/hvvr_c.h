@@ -145,7 +145,13 @@ typedef struct {
     uint32_t fp_mode;             /* HVVR_FP_FMA (reference kernel comments) or HVVR_FP_STRICT (no FMA in edge tests) */
     uint64_t tri_index_capacity;  /* triangle-index pool shared by the raycaster's cameras, entries; 0 = default (128M as the reference) */
     int device;                   /* CUDA device ordinal */
+    uint32_t sample_setup;        /* HVVR_SETUP_DEVICE (default) or HVVR_SETUP_HOST: where a camera's sample hierarchy is built */
 } hvvr_spec;
+/* The sample hierarchy (SampleData: clustering, tile and block frusta, beams, image remap) is built
+ * on the device when the samples' positions are distinct and not NaN and the spherical mapping is
+ * off: the reference's clustering sorts are then order-unique and the result equals the host
+ * build bit for bit. Otherwise, and with HVVR_SETUP_HOST, it is built on the host. */
+enum { HVVR_SETUP_DEVICE = 0, HVVR_SETUP_HOST = 1 };
 
 typedef struct hvvr_raycaster hvvr_raycaster;
 typedef struct hvvr_camera hvvr_camera;
@@ -238,6 +244,10 @@ int hvvr_camera_set_render_target(hvvr_camera* cam, const hvvr_image_desc* targe
 int hvvr_camera_set_samples(hvvr_camera* cam, const hvvr_sample* samples, uint32_t count, uint32_t split_color_samples);
 /* setCameraToWorld(const transform&) (camera.h:99; camera.cpp:174-176) */
 int hvvr_camera_set_camera_to_world(hvvr_camera* cam, const hvvr_transform* xf);
+/* Builds the camera's sample setup now (the reference's setSamples builds SampleData at once;
+ * otherwise this happens at the camera's first render) and returns when it is on the device.
+ * on_host (may be NULL): 1 when the hierarchy was built on the host (see hvvr_spec.sample_setup). */
+int hvvr_camera_prepare(hvvr_camera* cam, uint32_t* on_host);
 /* MSAA rate in {1,2,4,8,16,32}; the reference fixes it at compile time
  * (libraries/hvvr/raycaster/raycaster_common.h:27). Default 16. */
 int hvvr_camera_set_msaa(hvvr_camera* cam, uint32_t rate);
