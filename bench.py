@@ -39,7 +39,7 @@ CROP_ROWS = (540, 660)  # bounded CPU sample: a 120-row band across the middle o
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="hvvr_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -93,10 +93,18 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: begin the timed region once it samples
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
+        """The samples' summary, or {} when nvidia-smi gave none."""
         if not self.proc:
-            return None
+            return {}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -110,7 +118,7 @@ class Clocks:
                     rows.append(parts)
         os.unlink(self.path)
         if not rows:
-            return None
+            return {}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         reasons = set()
         for r in rows:
