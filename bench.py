@@ -43,8 +43,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="hvvr_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="stereo", choices=["stereo", "batched", "served", "foveated"],
-                    help="stereo: the headline 2x1080x1200 frame; batched: 64 views over 4 scenes, batched vs plain; "
+    ap.add_argument("--workload", default="stereo", choices=["stereo", "batched", "served", "foveated", "c1"],
+                    help="stereo: the headline 2x1080x1200 frame; c1: one 640x480 1xMSAA grid view of the 57k-triangle "
+                         "scene; batched: 64 views over 4 scenes, batched vs plain; "
                          "served: Poisson request arrivals against the render server; foveated: polar foveated "
                          "stereo, 16xMSAA, resolved to 1440x1600 per eye, gaze in a 10-degree saccade")
     ap.add_argument("--rates", default="100,250,500,1000,2000,5000,10000,20000", help="served: arrival rates, req/s")
@@ -328,6 +329,9 @@ def main():
     if args.workload == "foveated":
         run_foveated(args)
         return
+    if args.workload == "c1":
+        run_c1(args)
+        return
     import numpy as np
     import torch
     import hvvr_b200 as hv
@@ -442,6 +446,58 @@ def main():
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def run_c1(args):
+    """The small configuration: one 640x480 grid view (1xMSAA) of the 57,344-triangle scene,
+    rendered into device memory; one step = one frame. Single GPU."""
+    import numpy as np
+    import torch
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    torch.cuda.set_device(0)
+    sc = scenes.scene_c1()
+    hv.generate_topology(sc)
+    w, h = 640, 480
+    rc = hv.Raycaster()
+    rc.create_model(sc)
+    for light in sc.lights:
+        rc.create_light(light)
+    img = torch.zeros((h, w), dtype=torch.int32, device="cuda")
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h, device_ptr=img.data_ptr())
+    cam.set_samples(scenes.grid_samples(w, h))
+    cam.set_camera_to_world(scenes.camera_transform())
+    cam.set_msaa(1)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = ctypes_stream(stream)
+    for _ in range(args.warmup):
+        rc.render(stream=sp)
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    frame_ms = []
+    for i in range(args.steps):
+        flush.fill_(i & 0xff)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        rc.render(stream=sp)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        frame_ms.append(s0.elapsed_time(s1))
+    ck = clocks.stop()
+    rc.close()
+    ms = statistics.mean(frame_ms)
+    print(json.dumps({
+        "metric": "vis+shade Gsamples/s", "value": w * h / (ms * 1e-3) / 1e9, "unit": "Gsamples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_frame_ms": statistics.median(frame_ms),
+        "p99_frame_ms": float(np.percentile(frame_ms, 99)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural 57,344-triangle scene, grid samples)",
+        "config": {"workload": "640x480 grid 1xMSAA, 57,344-triangle scene, one frame per step",
+                   "l2": "flushed between frames (256 MiB write, untimed)"},
+        "gpu_launches": args.steps * 9, "clocks": ck}))
 
 
 def run_batched(args):
