@@ -203,3 +203,44 @@ def test_wide_formats_level0_and_reads():
             rc.create_texture(np.zeros((4, 4, 4), np.uint8), 99)
     finally:
         rc.close()
+
+
+def test_textured_and_untextured_scenes_in_one_batch():
+    """A frame batch over two raycasters, one with textures: each view reads its own scene's
+    texture table, so every camera's image equals its raycaster rendering alone."""
+    sc, texels, fmts = _textured_scene(4)
+    plain = scene("c1")
+    w, h = 128, 96
+    smp = scenes.barrel_samples(w, h)
+
+    def build(s, textured):
+        rc = hv.Raycaster()
+        rc.create_model(s)
+        for light in s.lights:
+            rc.create_light(light)
+        if textured:
+            for t, f in zip(texels, fmts):
+                rc.create_texture(t, f)
+        cam = rc.create_camera(scenes.viewport_for(w, h))
+        cam.set_render_target(w, h)
+        cam.set_samples(smp)
+        cam.set_camera_to_world(scenes.camera_transform(eye=(0.8, 1.6, 7.5), target=(0.0, 0.0, -1.0)))
+        cam.set_msaa(4)
+        return rc, cam
+
+    alone = []
+    for s, textured in ((sc, True), (plain, False)):
+        rc, cam = build(s, textured)
+        rc.render()
+        rc.synchronize()
+        alone.append(cam.image.copy())
+        rc.close()
+    rcs = [build(sc, True), build(plain, False)]
+    batch = hv.Batch([r for r, _ in rcs])
+    batch.render()
+    batch.synchronize()
+    for (rc, cam), want in zip(rcs, alone):
+        assert np.array_equal(cam.image, want)
+    batch.close()
+    for rc, _ in rcs:
+        rc.close()
