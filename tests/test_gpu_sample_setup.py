@@ -87,3 +87,25 @@ def test_duplicate_positions_take_the_host_build():
     b = _render(sc, smp, w, h, 4, hv.HVVR_SETUP_HOST)
     assert a["on_host"] and b["on_host"]
     assert np.array_equal(a["remap"], b["remap"]) and np.array_equal(a["hits"], b["hits"])
+
+
+def test_prepare_errors_and_reuse():
+    """prepare() without samples is an error; a second prepare() reuses the setup; new samples
+    rebuild it; the spherical mapping takes the host build."""
+    rc = hv.Raycaster()
+    cam = rc.create_camera(scenes.viewport_for(64, 48))
+    cam.set_render_target(64, 48)
+    with pytest.raises(hv.HvvrError):
+        cam.prepare()
+    cam.set_samples(scenes.grid_samples(64, 48))
+    assert cam.prepare() is False
+    b0 = cam.beams()
+    assert cam.prepare() is False
+    assert np.array_equal(cam.beams(), b0)
+    cam.set_samples(scenes.barrel_samples(64, 48))
+    assert cam.prepare() is False
+    assert not np.array_equal(cam.beams(), b0)
+    _check = hv._check
+    _check(hv._lib.hvvr_camera_set_spherical_warp(cam.handle, hv.C.c_float(90.0), hv.C.c_float(70.0)))
+    assert cam.prepare() is True
+    rc.close()
