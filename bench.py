@@ -301,9 +301,28 @@ def cpu_baseline(sc):
     impl.render(sc, crop, xf, scenes.viewport_for(W, H), W, H, MSAA, fp_mode=hv.HVVR_FP_STRICT, threads=cores,
                 want=("colors",))
     dt = time.perf_counter() - t0
+    # one core, over the first eighth of the crop's rows
+    rows1 = (CROP_ROWS[0], CROP_ROWS[0] + (CROP_ROWS[1] - CROP_ROWS[0]) // 8)
+    crop1 = smp[(smp["pixel"][:, 1] >= rows1[0]) & (smp["pixel"][:, 1] < rows1[1])]
+    t1 = time.perf_counter()
+    impl.render(sc, crop1, xf, scenes.viewport_for(W, H), W, H, MSAA, fp_mode=hv.HVVR_FP_STRICT, threads=1,
+                want=("colors",))
+    dt1 = time.perf_counter() - t1
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
     return {"value": len(crop) / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": kind,
             "sample": "%d samples (rows %d-%d of the left eye), traversal+intersect+shade, %.1f s" %
-                      (len(crop), CROP_ROWS[0], CROP_ROWS[1], dt)}
+                      (len(crop), CROP_ROWS[0], CROP_ROWS[1], dt),
+            "one_core": {"value": len(crop1) / dt1 / 1e9, "unit": "Gsamples/s",
+                         "sample": "%d samples (rows %d-%d), %.1f s" % (len(crop1), rows1[0], rows1[1], dt1)},
+            "cpu_model": model}
 
 
 def main():
