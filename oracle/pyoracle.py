@@ -413,6 +413,22 @@ class ReferenceGpu:
             raise RuntimeError("intersect_resolve: %d" % rc)
         return out
 
+    def foveated_scatter(self, samples_per_ring, ring_count, colors, tmax, remap):
+        """The reference's RemapPolarFoveatedKernel: sample colours and view depths [valid] scattered
+        by remap [valid, 2] into the polar textures; returns (colour [rings, spr], depth [rings, spr])."""
+        f = self.lib.ref_gpu_foveated_scatter
+        f.restype = C.c_int
+        c = np.ascontiguousarray(colors, np.uint32)
+        t = np.ascontiguousarray(tmax, np.float32)
+        r = np.ascontiguousarray(remap, np.uint32)
+        col = np.zeros((ring_count, samples_per_ring), np.uint32)
+        dep = np.zeros((ring_count, samples_per_ring), np.float32)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        rc = f(C.c_uint32(samples_per_ring), C.c_uint32(ring_count), C.c_uint32(len(c)), p(c), p(t), p(r), p(col), p(dep))
+        if rc != 0:
+            raise RuntimeError("foveated_scatter: %d" % rc)
+        return col, dep
+
     def sample(self, ids, q):
         """ReadTexture through the reference's atlas: ids [n], q [n, 6] -> [n, 4] float32"""
         ids = np.ascontiguousarray(ids, np.uint32)

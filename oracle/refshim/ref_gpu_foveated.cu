@@ -1,17 +1,21 @@
 // GPU-side harness around the reference's own foveated resolve kernels (libraries/hvvr/raycaster/
 // gpu_foveated.cu: ComputeMoments, FoveatedPolarToScreenSpaceKernel, SeparableFilterUsingEccentricity,
 // FinishConstrastEnhancement), built with nvcc for sm_100a into oracle/_ref/libhvvr_ref_gpu.so.
-// Test infrastructure only. The kernels are compiled from the reference's source file, included
+// Test infrastructure only. The kernels are compiled from the reference's source files (and
+// RemapPolarFoveatedKernel from remap.cu), included
 // here so that this translation unit can instantiate and launch them the way
 // GPUCamera::foveatedPolarToScreenSpace (gpu_foveated.cu:335-375) does, on textures made by the
 // reference's createEmptyTexture with the formats and addressing of GPUCamera's foveated setup
 // (gpu_camera.cu:170-230).
 #include "gpu_foveated.cu"
+#include "remap.cu"
 
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
+
+#include <vector>
 
 namespace hvvr {
 // Setup-time functions GPUCamera methods in gpu_foveated.cu refer to; the harness launches the
@@ -58,6 +62,52 @@ extern "C" {
 // [height][width] (RGBA8 sRGB). Outputs: the moments [rings][samplesPerRing][2][4] (unorm16), the
 // temporally filtered result texture and the first (vertical) filter pass [height][width]
 // (RGBA8 sRGB), and the final image [height][width].
+int ref_gpu_foveated_resolve(float degreeTrackingError, float maxFovDegrees, float marSlope, float fovealMarDegrees,
+                             uint32_t samplesPerRing, uint32_t ringCount, const uint32_t* polarColor,
+                             const float* polarDepth, uint32_t width, uint32_t height, const float* sampleToEye9,
+                             const float* eyeToSamplePrev16, const uint32_t* history, uint16_t* moments,
+                             uint32_t* result, uint32_t* filtered, uint32_t* image);
+
+// RemapPolarFoveatedKernel (remap.cu:126-141) as GPUCamera::remapPolarFoveated launches it: the
+// sample colours (RGBA8 sRGB) and view depths [valid] scattered by remap [valid] (x, y) into
+// polar textures [ringCount][samplesPerRing] made as GPUCamera's (initially zero), read back into
+// polarColor and polarDepth. valid must equal samplesPerRing * ringCount (the polar set fills its
+// texture).
+int ref_gpu_foveated_scatter(uint32_t samplesPerRing, uint32_t ringCount, uint32_t valid, const uint32_t* colors,
+                             const float* tmax, const uint32_t* remap, uint32_t* polarColor, float* polarDepth) {
+    using namespace hvvr;
+    if (size_t(valid) != size_t(samplesPerRing) * ringCount) return -1;
+    Texture2D raw = createEmptyTexture(samplesPerRing, ringCount, TextureFormat::r8g8b8a8_unorm_srgb,
+                                       cudaAddressModeWrap, cudaAddressModeClamp, true);
+    Texture2D depth = createEmptyTexture(samplesPerRing, ringCount, TextureFormat::r32_float, cudaAddressModeWrap,
+                                         cudaAddressModeClamp, false);
+    const size_t n = valid;
+    std::vector<uint32_t> zeros(n, 0u);
+    cudaError_t e = upload(raw, zeros.data(), 4);
+    if (e == cudaSuccess) e = upload(depth, zeros.data(), 4);
+    uint32_t *dColors = nullptr, *dRemap = nullptr;
+    float* dTmax = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dColors, n * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dTmax, n * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dRemap, n * 8);
+    if (e == cudaSuccess) e = cudaMemcpy(dColors, colors, n * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dTmax, tmax, n * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dRemap, remap, n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        KernelDim dim = KernelDim(valid, CUDA_GROUP_SIZE);
+        RemapPolarFoveatedKernel<<<dim.grid, dim.block>>>(dColors, dTmax, (vector2ui*)dRemap, raw, depth, n);
+        e = cudaDeviceSynchronize();
+    }
+    if (e == cudaSuccess) e = download(polarColor, raw, 4);
+    if (e == cudaSuccess) e = download(polarDepth, depth, 4);
+    cudaFree(dColors);
+    cudaFree(dTmax);
+    cudaFree(dRemap);
+    release(raw);
+    release(depth);
+    return int(e);
+}
+
 int ref_gpu_foveated_resolve(float degreeTrackingError, float maxFovDegrees, float marSlope, float fovealMarDegrees,
                              uint32_t samplesPerRing, uint32_t ringCount, const uint32_t* polarColor,
                              const float* polarDepth, uint32_t width, uint32_t height, const float* sampleToEye9,

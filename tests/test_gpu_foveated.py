@@ -124,7 +124,8 @@ def test_foveated_resolve_matches_oracle(oracle):
 def test_foveated_resolve_against_reference_kernels():
     """The resolve against the reference's own kernels (gpu_foveated.cu built for this GPU by
     oracle/refshim/ref_gpu_foveated.cu) on the GPU's polar textures, matrices and history, over
-    frames with camera and gaze motion: moments, temporally filtered result and final image
+    frames with camera and gaze motion: the polar textures (RemapPolarFoveatedKernel on the frame's
+    sample colours and view depths), moments, temporally filtered result and final image
     bit-exact."""
     import pyoracle
     ref = pyoracle.ReferenceGpu()
@@ -145,6 +146,13 @@ def test_foveated_resolve_against_reference_kernels():
         rc.render()
         s2e, e2p, res, hist = cam.foveated_resolve()
         pcol, pdep, pmom = cam.polar_textures(spr, rings)
+        if polar["valid"] == spr * rings:
+            # the scatter: RemapPolarFoveatedKernel on the frame's sample colours and view depths
+            _, _, depth = cam.foveated_frame()
+            rcol, rdep = ref.foveated_scatter(spr, rings, cam.sample_colors()[:polar["valid"]],
+                                              depth[:polar["valid"]], polar["remap"][:polar["valid"]])
+            assert np.array_equal(pcol, rcol)
+            assert np.array_equal(pdep.view(np.uint32), rdep.view(np.uint32))
         r = ref.foveated_resolve(PATTERN, spr, rings, pcol, pdep, w, h, s2e, e2p, hist)
         dm = np.abs(pmom.astype(np.int32) - r["moments"].astype(np.int32))
         dr = np.abs(res.view(np.uint8).astype(np.int32) - r["result"].view(np.uint8).astype(np.int32))
