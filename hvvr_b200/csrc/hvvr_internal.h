@@ -225,7 +225,7 @@ cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStric
 // occRank of every thin-lens view (one block per view; pinhole views are skipped)
 cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
-cudaError_t launchRefit(const SceneDev& s, cudaStream_t st);
+cudaError_t launchRefit(const SceneDev& s, bool fma, cudaStream_t st);
 cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);
 // the foveated resolve of view `view` of the frame (fov: the host copy of its FoveaDev, for
 // the launch shapes): scatter to the polar textures, moments, polar -> screen with temporal

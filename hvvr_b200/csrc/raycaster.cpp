@@ -815,7 +815,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
             rc->refitDirty = true;
         }
         if (rc->scene.nodeCount && rc->refitDirty) {
-            CUDA_TRY(launchRefit(rc->scene, st));
+            CUDA_TRY(launchRefit(rc->scene, rc->spec.fp_mode == HVVR_FP_FMA, st));
             rc->refitDirty = false;
         }
     }

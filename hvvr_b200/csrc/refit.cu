@@ -28,6 +28,18 @@ __device__ __forceinline__ uint32_t ifloatFlip(uint32_t f) {
     return f ^ mask;
 }
 
+// matrix4x4 * vector4(p, 1), one output component: the columns summed left to right, or, for the
+// fused mode, as the reference's GPU build (nvcc, -use_fast_math) contracts that sum in
+// SceneTransformVerticesKernel (gpu_scene_state.cu:118): the first column's product fused into the
+// rounded second one, the third fused into that, then the fourth (times w = 1) added. Matched
+// bit for bit against that kernel's output on rotated and scaled models.
+template <bool Fma>
+__device__ __forceinline__ float xformRow(const Mat4& M, int r, float x, float y, float z) {
+    if (Fma) return fmaf(M.m[3][r], 1.0f, fmaf(M.m[2][r], z, fmaf(M.m[0][r], x, M.m[1][r] * y)));
+    return M.m[0][r] * x + M.m[1][r] * y + M.m[2][r] * z + M.m[3][r] * 1.0f;
+}
+
+template <bool Fma>
 __global__ void transformVertsKernel(const float4* __restrict__ in, float4* __restrict__ out,
                                      const uint32_t* __restrict__ vertModel, const Mat4* __restrict__ xf,
                                      uint32_t count) {
@@ -35,8 +47,9 @@ __global__ void transformVertsKernel(const float4* __restrict__ in, float4* __re
     if (i >= count) return;
     const float4 a = in[2 * size_t(i)], b = in[2 * size_t(i) + 1];
     const Mat4 M = xf[vertModel[i]];
-    const float w = M.m[0][3] * a.x + M.m[1][3] * a.y + M.m[2][3] * a.z + M.m[3][3] * 1.0f;
-    const F3 p = xformPoint(M, f3(a.x, a.y, a.z));
+    const float w = xformRow<Fma>(M, 3, a.x, a.y, a.z);
+    const F3 p = f3(xformRow<Fma>(M, 0, a.x, a.y, a.z), xformRow<Fma>(M, 1, a.x, a.y, a.z),
+                    xformRow<Fma>(M, 2, a.x, a.y, a.z));
     const float iw = 1.0f / w;
     const uint32_t n01 = __float_as_uint(a.w), n23 = __float_as_uint(b.x);
     const F3 n = f3(__half2float(__ushort_as_half((unsigned short)(n01 & 0xffffu))),
@@ -120,10 +133,10 @@ __global__ void internalRefitKernel(Node* nodes, const uint32_t* __restrict__ st
 
 } // namespace
 
-cudaError_t launchRefit(const SceneDev& s, cudaStream_t st) {
+cudaError_t launchRefit(const SceneDev& s, bool fma, cudaStream_t st) {
     if (s.vertCount) {
-        transformVertsKernel<<<(s.vertCount + 255) / 256, 256, 0, st>>>(s.vertsIn, s.verts, s.vertModel, s.modelToWorld,
-                                                                         s.vertCount);
+        auto k = fma ? transformVertsKernel<true> : transformVertsKernel<false>;
+        k<<<(s.vertCount + 255) / 256, 256, 0, st>>>(s.vertsIn, s.verts, s.vertModel, s.modelToWorld, s.vertCount);
     }
     if (s.triCount) {
         precomputeTrisKernel<<<(s.triCount + 255) / 256, 256, 0, st>>>(s.triShade, s.verts, s.tris, s.triCount);

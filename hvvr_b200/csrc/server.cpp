@@ -224,7 +224,7 @@ int applyUpdates(hvvr_server* s, std::vector<std::unique_ptr<Update>>& ups) {
         if (std::find(touched.begin(), touched.end(), u->rc) == touched.end()) touched.push_back(u->rc);
     }
     for (hvvr_raycaster* rc : touched) {
-        CUDA_TRY(launchRefit(rc->scene, s->updateStream));
+        CUDA_TRY(launchRefit(rc->scene, rc->spec.fp_mode == HVVR_FP_FMA, s->updateStream));
         rc->refitDirty = false;
     }
     CUDA_TRY(cudaEventRecord(s->updateEv, s->updateStream));
@@ -433,7 +433,7 @@ int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr
             rc->refitDirty = true;
         }
         if (rc->scene.nodeCount && rc->refitDirty) {
-            CUDA_TRY(launchRefit(rc->scene, rc->stream));
+            CUDA_TRY(launchRefit(rc->scene, rc->spec.fp_mode == HVVR_FP_FMA, rc->stream));
             rc->refitDirty = false;
         }
         CUDA_TRY(cudaStreamSynchronize(rc->stream));

@@ -71,6 +71,16 @@ inline V4 mul(const M4& m, V4 v) {
               m.m0.z * v.x + m.m1.z * v.y + m.m2.z * v.z + m.m3.z * v.w,
               m.m0.w * v.x + m.m1.w * v.y + m.m2.w * v.z + m.m3.w * v.w};
 }
+// mul(m, v) as the reference's GPU build (nvcc, -use_fast_math) contracts it in
+// SceneTransformVerticesKernel (RC/gpu_scene_state.cu:118): per component, the first column's
+// product fused into the rounded second one, then the third and fourth fused in turn
+inline V4 mulFma(const M4& m, V4 v) {
+    auto row = [&](float a, float b, float c, float d) {
+        return fmaf(d, v.w, fmaf(c, v.z, fmaf(a, v.x, b * v.y)));
+    };
+    return V4{row(m.m0.x, m.m1.x, m.m2.x, m.m3.x), row(m.m0.y, m.m1.y, m.m2.y, m.m3.y),
+              row(m.m0.z, m.m1.z, m.m2.z, m.m3.z), row(m.m0.w, m.m1.w, m.m2.w, m.m3.w)};
+}
 inline M3 m3of(const M4& m) { return M3{mk(m.m0.x, m.m0.y, m.m0.z), mk(m.m1.x, m.m1.y, m.m1.z), mk(m.m2.x, m.m2.y, m.m2.z)}; }
 
 // matrix4x4(const transform&) = matrix4x4(matrix3x3(rotation) * scale, translation)
@@ -195,7 +205,8 @@ void refitScene(const oracle_frame_in* in, Scene& s) {
     for (size_t i = 0; i < s.verts.size(); i++) {
         const M4& t = modelToWorld[s.vertModel[i]];
         const hvvr_shading_vertex& v = s.verts[i];
-        V4 fp = mul(t, V4{v.pos.x, v.pos.y, v.pos.z, 1.0f});
+        const V4 vp = V4{v.pos.x, v.pos.y, v.pos.z, 1.0f};
+        V4 fp = in->fp_mode == HVVR_FP_FMA ? mulFma(t, vp) : mul(t, vp);
         V3 p = mk(fp.x, fp.y, fp.z) * (1.0f / fp.w);
         s.world[i].pos = hvvr_vec3{p.x, p.y, p.z};
         V3 n = mk(halfToFloat(v.normal[0]), halfToFloat(v.normal[1]), halfToFloat(v.normal[2]));

@@ -429,6 +429,28 @@ class ReferenceGpu:
             raise RuntimeError("foveated_scatter: %d" % rc)
         return col, dep
 
+    def scene_update(self, nodes, verts, vert_model, transforms, tri_shade):
+        """The reference's scene update kernels (SceneTransformVerticesKernel, SceneRefitPreKernel,
+        ScenePrecomputeTrianglesKernel, SceneRefitIntFixupKernel, SceneRefitNodeMultiPassKernel) on a
+        BVH (its child and leaf data), the untransformed vertices, each vertex's model and the model
+        transforms: returns (world vertices, precomputed triangles [t, 9], refit nodes)."""
+        f = self.lib.ref_gpu_scene_update
+        f.restype = C.c_int
+        n = np.ascontiguousarray(nodes, _abi.NODE_DTYPE)
+        v = np.ascontiguousarray(verts, _abi.VERTEX_DTYPE)
+        vm = np.ascontiguousarray(vert_model, np.uint32)
+        xf = (_abi.Transform * len(transforms))(*transforms)
+        ts = np.ascontiguousarray(tri_shade)
+        world = np.zeros_like(v)
+        tris = np.zeros((len(ts), 9), np.float32)
+        out = np.zeros_like(n)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        rc = f(p(n), C.c_uint32(len(n)), p(v), C.c_uint32(len(v)), p(vm), C.cast(xf, C.c_void_p),
+               C.c_uint32(len(transforms)), p(ts), C.c_uint32(len(ts)), p(world), p(tris), p(out))
+        if rc != 0:
+            raise RuntimeError("scene_update: %d" % rc)
+        return world, tris, out
+
     def sample(self, ids, q):
         """ReadTexture through the reference's atlas: ids [n], q [n, 6] -> [n, 4] float32"""
         ids = np.ascontiguousarray(ids, np.uint32)

@@ -23,7 +23,8 @@ REF_GPU_FLAGS = -gencode arch=compute_100a,code=sm_100a -use_fast_math -std=c++1
 all: _ref/libhvvr_ref.so _ref/libhvvr_ref_gpu.so
 
 _ref/libhvvr_ref_gpu.so: _ref/obj/texture.cu.o _ref/obj/gpu_image.cu.o _ref/obj/ref_gpu_harness.cu.o \
-                         _ref/obj/ref_gpu_foveated.cu.o _ref/obj/ref_gpu_intersect.cu.o
+                         _ref/obj/ref_gpu_foveated.cu.o _ref/obj/ref_gpu_intersect.cu.o \
+                         _ref/obj/ref_gpu_scene.cu.o
 	$(NVCC) -shared -gencode arch=compute_100a,code=sm_100a -o $@ $^
 _ref/obj/%.cu.o: $(RC)/%.cu refshim/compat/hvvr_nvcc_compat.h
 	@mkdir -p _ref/obj
@@ -37,6 +38,11 @@ _ref/obj/ref_gpu_intersect.cu.o: refshim/ref_gpu_intersect.cu $(RC)/intersect.cu
 _ref/obj/ref_gpu_foveated.cu.o: refshim/ref_gpu_foveated.cu $(RC)/gpu_foveated.cu refshim/compat/hvvr_nvcc_compat.h
 	@mkdir -p _ref/obj
 	$(NVCC) $(REF_GPU_FLAGS) -c $< -o $@
+# includes the reference's gpu_scene_state.cu to launch its scene update kernels
+# (its bvh_node.h declares structs inside an anonymous union, which gcc takes with -fpermissive)
+_ref/obj/ref_gpu_scene.cu.o: refshim/ref_gpu_scene.cu $(RC)/gpu_scene_state.cu refshim/compat/hvvr_nvcc_compat.h
+	@mkdir -p _ref/obj
+	$(NVCC) $(REF_GPU_FLAGS) -Xcompiler -fpermissive -c $< -o $@
 _ref/obj/ref_gpu_harness.cu.o: refshim/ref_gpu_harness.cu refshim/compat/hvvr_nvcc_compat.h
 	@mkdir -p _ref/obj
 	$(NVCC) $(REF_GPU_FLAGS) -c $< -o $@
