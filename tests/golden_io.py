@@ -11,9 +11,11 @@ GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    """The render fixtures (the polar_* fixtures hold sample sets only)."""
+    """The render fixtures (the polar_* fixtures hold sample sets only, the scene_update_* ones
+    world-space vertex positions)."""
     return sorted(n for n in (os.path.splitext(os.path.basename(p))[0]
-                              for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))) if not n.startswith("polar_"))
+                              for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+                  if not n.startswith(("polar_", "scene_update_")))
 
 
 def load(name):
