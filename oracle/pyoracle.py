@@ -312,6 +312,11 @@ class Reference:
         out["history"] = (w2ep, ep2sp)
         return out
 
+    def session(self, scene, samples, viewport, width, height, msaa, lens=(0.0, 1.0)):
+        """A camera kept across frames: scene upload, refit and sample setup once, then
+        ``frame(cam_xf, threads)`` per frame (see RefSession)."""
+        return RefSession(self.lib, scene, samples, viewport, width, height, msaa, lens)
+
     def generate_topology(self, scene):
         """GenerateTopology on copies of the scene arrays; returns (verts, tri_shade, nodes)."""
         verts = scene.verts.copy()
@@ -324,6 +329,67 @@ class Reference:
         if rc != 0:
             raise RuntimeError("GenerateTopology failed: %d" % rc)
         return verts, tris, nodes[: cnt.value].copy()
+
+
+class RefSession:
+    """The reference's per-frame path for one camera over a scene, as its Raycaster runs it frame
+    after frame: ref_session_create uploads and refits the scene and builds the camera's SampleData
+    once; each frame() transforms the frusta to world space, traverses the blocks and tiles on
+    ``threads`` threads (cullThread), runs the intersect/shade code per tile on the same threads and
+    remaps the colours into the image."""
+
+    def __init__(self, lib, scene, samples, viewport, width, height, msaa, lens):
+        if scene.nodes is None:
+            raise ValueError("scene has no topology")
+        lib.ref_session_create.argtypes = [C.POINTER(FrameIn), C.POINTER(C.c_void_p)]
+        lib.ref_session_create.restype = C.c_int
+        lib.ref_session_frame.argtypes = [C.c_void_p, C.POINTER(_abi.Transform), C.c_uint32, C.c_void_p, C.c_void_p]
+        lib.ref_session_frame.restype = C.c_int
+        lib.ref_session_destroy.argtypes = [C.c_void_p]
+        lib.ref_session_destroy.restype = None
+        self.lib = lib
+        self._keep = (scene, samples)
+        md = _abi.MeshData(_abi.ptr(scene.verts), len(scene.verts), _abi.ptr(scene.tri_shade), len(scene.tri_shade),
+                           _abi.ptr(scene.nodes), len(scene.nodes), _abi.ptr(scene.materials), len(scene.materials))
+        self._mds = (_abi.MeshData * 1)(md)
+        self._xfs = (_abi.Transform * 1)(_abi.transform())
+        self._lights = (_abi.LightUnion * len(scene.lights))(*scene.lights)
+        fin = FrameIn()
+        fin.model_count = 1
+        fin.models = self._mds
+        fin.model_xf = self._xfs
+        fin.lights = self._lights
+        fin.light_count = len(scene.lights)
+        fin.viewport = viewport
+        fin.lens = _abi.ThinLens(*lens)
+        fin.samples = _abi.ptr(samples)
+        fin.sample_count = len(samples)
+        fin.split_color_samples = 1
+        fin.width, fin.height = width, height
+        fin.msaa = msaa
+        fin.fp_mode = _abi.HVVR_FP_STRICT
+        self.handle = C.c_void_p()
+        rc = lib.ref_session_create(C.byref(fin), C.byref(self.handle))
+        if rc != 0:
+            raise RuntimeError("ref_session_create failed: %d" % rc)
+        _, _, self.padded = layout(len(samples))
+        self.colors = np.zeros(self.padded, np.uint32)
+        self.image = np.zeros((height, width), np.uint32)
+
+    def frame(self, cam_xf, threads):
+        rc = self.lib.ref_session_frame(self.handle, C.byref(cam_xf), threads, self.colors.ctypes.data,
+                                        self.image.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("ref_session_frame failed: %d" % rc)
+        return self.image
+
+    def close(self):
+        if self.handle:
+            self.lib.ref_session_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        self.close()
 
 
 class ReferenceGpu:

@@ -1,7 +1,8 @@
 # Compiles the reference's own sources, unmodified and in place, plus the harness in this
 # directory into _ref/libhvvr_ref.so. Test infrastructure only: run from oracle/ by the
-# oracle Makefile when the reference tree is present. Output goes to _ref/ (git-ignored).
-REF_ROOT ?= /root/reference
+# oracle Makefile when the reference tree is present (REF_ROOT: from the environment, else the
+# reference checkout beside the repository). Output goes to _ref/ (git-ignored).
+REF_ROOT ?= $(abspath $(CURDIR)/../../reference)
 RC = $(REF_ROOT)/libraries/hvvr/raycaster
 SH = $(REF_ROOT)/libraries/hvvr/shared
 SS = $(REF_ROOT)/libraries/hvvr/samples_shared

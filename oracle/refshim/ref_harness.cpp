@@ -39,6 +39,7 @@
 #include "../hvvr_oracle.h"
 
 #include <atomic>
+#include <memory>
 #include <functional>
 #include <random>
 #include <thread>
@@ -119,15 +120,43 @@ extern "C" int ref_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_c
     return 0;
 }
 
-extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
-    MxcsrScope mx;
+namespace {
+
+// What the reference keeps from one frame to the next: the uploaded and refit scene
+// (Raycaster::buildScene / GPUSceneState, RC/scene_update.cpp:22-143, RC/gpu_scene_state.cu), its
+// lighting environment, and a camera's SampleData (Camera::setSamples, RC/camera.cpp:104-164).
+struct RefSession {
+    uint32_t N = 1, width = 0, height = 0, split = 1;
+    ThinLens lens{0.0f, 1.0f};
+    DynamicArray<BVHNode> nodes;
+    std::vector<ShadingVertex> world;
+    std::vector<PrecomputedTriangleIntersect> tris;
+    std::vector<PrecomputedTriangleShade> triShade;
+    std::vector<SimpleMaterial> materials;
+    LightingEnvironment env;
+    std::unique_ptr<SampleData> sd;
+    uint32_t textureCount = 0;
+    hv_texture_hook_fn textureSample = nullptr;
+    void* textureCtx = nullptr;
+};
+
+// scene upload and refit, lighting environment and sample set of one camera
+int refSetup(const oracle_frame_in* in, oracle_frame_out* out, RefSession& S) {
     if (in->model_count != 1 || in->sample_count == 0) return 1; // harness covers single-model scenes
-    const uint32_t N = in->msaa;
-    out->status = 0;
     const hvvr_mesh_data& md = in->models[0];
+    S.N = in->msaa;
+    S.width = in->width;
+    S.height = in->height;
+    S.split = in->split_color_samples;
+    S.lens = ThinLens{in->lens.radius, in->lens.focal_distance};
+    S.textureCount = in->texture_count;
+    S.textureSample = in->texture_sample;
+    S.textureCtx = in->texture_ctx;
+    S.materials.assign((const SimpleMaterial*)md.materials, (const SimpleMaterial*)md.materials + md.material_count);
 
     // scene build for one model (RC/scene_update.cpp:86-101 with offsets 0, no root fix-up)
-    DynamicArray<BVHNode> nodes(md.node_count);
+    S.nodes = DynamicArray<BVHNode>(md.node_count);
+    DynamicArray<BVHNode>& nodes = S.nodes;
     memset(nodes.data(), 0, md.node_count * sizeof(BVHNode));
     for (uint32_t n = 0; n < md.node_count; n++) {
         const TopologyNode& tn = ((const TopologyNode*)md.nodes)[n];
@@ -141,7 +170,8 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
     }
     // refit (restatement of RC/gpu_scene_state.cu:88-375 with the reference's types and operators)
     matrix4x4 modelToWorld = matrix4x4(*(const transform*)&in->model_xf[0]);
-    std::vector<ShadingVertex> world(md.vert_count);
+    S.world.resize(md.vert_count);
+    std::vector<ShadingVertex>& world = S.world;
     for (uint32_t i = 0; i < md.vert_count; i++) {
         ShadingVertex vertex = ((const ShadingVertex*)md.verts)[i];
         vector4 fp = modelToWorld * vector4(vertex.pos, 1.0);
@@ -149,7 +179,8 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
         vertex.normal = vector4h(normalize(matrix3x3(modelToWorld) * vector3(vertex.normal)));
         world[i] = vertex;
     }
-    const PrecomputedTriangleShade* triShade = (const PrecomputedTriangleShade*)md.tri_shade;
+    S.triShade.assign((const PrecomputedTriangleShade*)md.tri_shade, (const PrecomputedTriangleShade*)md.tri_shade + md.tri_count);
+    const PrecomputedTriangleShade* triShade = S.triShade.data();
     std::vector<uint32_t> triToNodeChild(md.tri_count, 0);
     for (int64_t n = int64_t(md.node_count) - 1; n >= 0; --n) {
         for (int k = 3; k >= 0; k--) {
@@ -160,7 +191,8 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
         }
     }
     std::vector<uint32_t> flip(size_t(md.node_count) * 24, FloatFlip(0xff800000));
-    std::vector<PrecomputedTriangleIntersect> tris(md.tri_count);
+    S.tris.resize(md.tri_count);
+    std::vector<PrecomputedTriangleIntersect>& tris = S.tris;
     for (uint32_t i = 0; i < md.tri_count; i++) {
         vector3 v0 = world[triShade[i].indices[0]].pos, v1 = world[triShade[i].indices[1]].pos,
                 v2 = world[triShade[i].indices[2]].pos;
@@ -202,22 +234,45 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
     if (out->nodes) memcpy(out->nodes, nodes.data(), md.node_count * sizeof(BVHNode));
     if (out->tris) memcpy(out->tris, tris.data(), md.tri_count * sizeof(PrecomputedTriangleIntersect));
 
+    // lighting environment (GPUSceneState::updateLighting, RC/gpu_scene_state.cu:47-81)
+    LightingEnvironment& env = S.env;
+    memset(&env, 0, sizeof(env));
+    for (uint32_t i = 0; i < in->light_count; i++) {
+        const LightUnion& l = ((const LightUnion*)in->lights)[i];
+        if (l.type == LightType::directional && env.directionalLightCount < int(MAX_DIRECTIONAL_LIGHTS))
+            env.directionalLights[env.directionalLightCount++] = l.directional;
+        else if (l.type == LightType::point && env.pointLightCount < int(MAX_POINT_LIGHTS))
+            env.pointLights[env.pointLightCount++] = l.point;
+        else if (l.type == LightType::spot && env.spotLightCount < int(MAX_SPOT_LIGHTS))
+            env.spotLights[env.spotLightCount++] = l.spot;
+    }
     // samples: the reference's SampleData with Camera::getSampleToCamera (RC/camera.cpp:167-171)
     const FloatRect vp(vector2(in->viewport.lower.x, in->viewport.lower.y), vector2(in->viewport.upper.x, in->viewport.upper.y));
     matrix3x3 sampleToCamera(vector3(vp.upper.x - vp.lower.x, 0, 0), vector3(0, vp.lower.y - vp.upper.y, 0),
                              vector3(vp.lower.x, vp.upper.y, -1));
-    ThinLens lens{in->lens.radius, in->lens.focal_distance};
-    SampleData sd((const Sample*)in->samples, in->sample_count, in->split_color_samples,
-                  Sample2Dto3DMappingSettings(sampleToCamera, lens), in->width, in->height);
+    S.sd.reset(new SampleData((const Sample*)in->samples, in->sample_count, in->split_color_samples,
+                              Sample2Dto3DMappingSettings(sampleToCamera, S.lens), in->width, in->height));
+    const SampleData& sd = *S.sd;
+    const uint32_t padded = uint32_t(sd.samples.directionalBeams.size());
+    if (out->remap) memcpy(out->remap, sd.imageLocationToSampleIndex.data(), sd.imageLocationToSampleIndex.size() * 4);
+    if (out->beams) memcpy(out->beams, sd.samples.directionalBeams.data(), size_t(padded) * sizeof(DirectionalBeam));
+    return 0;
+}
+
+// one frame of a camera: world-space frusta, traversal, intersect, G-buffer, shading, remap
+int refFrame(RefSession& S, const hvvr_transform& camXf, uint32_t threads, oracle_frame_out* out) {
+    out->status = 0;
+    const SampleData& sd = *S.sd;
     const BeamBatch& batch = sd.samples;
+    const uint32_t N = S.N;
+    const uint32_t nt = threads ? threads : 1;
+    const LightingEnvironment& env = S.env;
     uint32_t blockCount = uint32_t(batch.blockFrusta3D.size());
     uint32_t tileCount = uint32_t(batch.tileFrusta3D.size());
     uint32_t padded = uint32_t(batch.directionalBeams.size());
-    if (out->remap) memcpy(out->remap, sd.imageLocationToSampleIndex.data(), sd.imageLocationToSampleIndex.size() * 4);
-    if (out->beams) memcpy(out->beams, batch.directionalBeams.data(), size_t(padded) * sizeof(DirectionalBeam));
 
     // per-frame transform (transformHierarchyCameraToWorld without cull planes, RC/render.cpp:293-310)
-    matrix4x4 cameraToWorld = matrix4x4(*(const transform*)&in->cam_xf);
+    matrix4x4 cameraToWorld = matrix4x4(*(const transform*)&camXf);
     DynamicArray<Frustum> blocksW(blockCount), tilesW(tileCount);
     std::vector<SimpleRayFrustum> simple(tileCount);
     for (uint32_t b = 0; b < blockCount; b++) blocksW[b] = frustumTransform(batch.blockFrusta3D[b], cameraToWorld);
@@ -231,57 +286,59 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
     static_assert(sizeof(SimpleRayFrustum) == 96, "SimpleRayFrustum");
     if (out->tile_frusta) memcpy(out->tile_frusta, simple.data(), size_t(tileCount) * sizeof(SimpleRayFrustum));
 
-    // cullThread (RC/traversal.cpp:99-190), one block at a time
+    // cullThread (RC/traversal.cpp:99-190): the blocks are traversed on `threads` threads, each
+    // taking the next block (a tile's list depends only on its block, so the lists are the same
+    // for any assignment of blocks to threads)
     std::vector<std::vector<uint32_t>> lists(tileCount);
-    std::vector<uint32_t> scratch(1 << 20);
-    for (uint32_t b = 0; b < blockCount; b++) {
-        BlockFrame blockFrame;
-        uint32_t stackSize = traverseBlocks(blockFrame, nodes.data(), blocksW[b]);
-        if (out->block_sizes) out->block_sizes[b] = stackSize;
-        if (!stackSize) {
-            if (out->block_entries) memset(out->block_entries + size_t(b) * 64 * 3, 0, 64 * 3 * 4);
-            continue;
-        }
-        blockFrame.sort(stackSize);
-        if (out->block_entries) {
-            for (uint32_t i = 0; i < 64; i++) {
-                uint32_t* dst = out->block_entries + (size_t(b) * 64 + i) * 3;
-                if (i < stackSize) {
-                    dst[0] = fbits(blockFrame.sortedStack[i].tMin);
-                    dst[1] = blockFrame.sortedStack[i].mask;
-                    dst[2] = uint32_t(blockFrame.sortedStack[i].node - nodes.data());
-                } else {
-                    dst[0] = dst[1] = dst[2] = 0;
+    std::atomic<uint32_t> nextBlock(0);
+    auto cullWorker = [&]() {
+        MxcsrScope mxc;
+        std::vector<uint32_t> scratch(1 << 20);
+        for (;;) {
+            const uint32_t b = nextBlock.fetch_add(1);
+            if (b >= blockCount) break;
+            BlockFrame blockFrame;
+            uint32_t stackSize = traverseBlocks(blockFrame, S.nodes.data(), blocksW[b]);
+            if (out->block_sizes) out->block_sizes[b] = stackSize;
+            if (!stackSize) {
+                if (out->block_entries) memset(out->block_entries + size_t(b) * 64 * 3, 0, 64 * 3 * 4);
+                continue;
+            }
+            blockFrame.sort(stackSize);
+            if (out->block_entries) {
+                for (uint32_t i = 0; i < 64; i++) {
+                    uint32_t* dst = out->block_entries + (size_t(b) * 64 + i) * 3;
+                    if (i < stackSize) {
+                        dst[0] = fbits(blockFrame.sortedStack[i].tMin);
+                        dst[1] = blockFrame.sortedStack[i].mask;
+                        dst[2] = uint32_t(blockFrame.sortedStack[i].node - S.nodes.data());
+                    } else {
+                        dst[0] = dst[1] = dst[2] = 0;
+                    }
                 }
             }
+            for (uint32_t ti = 0; ti < TILES_PER_BLOCK; ti++) {
+                uint32_t tile = b * TILES_PER_BLOCK + ti;
+                TileFrame tileFrame;
+                for (uint32_t slot = 0; slot != stackSize; ++slot)
+                    store(&(tileFrame.stack + slot)->tMin, load_m128(&(blockFrame.sortedStack + slot)->tMin));
+                uint32_t count = traverseTiles(scratch.data(), uint32_t(scratch.size()), tileFrame, stackSize, tilesW[tile]);
+                lists[tile].assign(scratch.begin(), scratch.begin() + count);
+            }
         }
-        for (uint32_t ti = 0; ti < TILES_PER_BLOCK; ti++) {
-            uint32_t tile = b * TILES_PER_BLOCK + ti;
-            TileFrame tileFrame;
-            for (uint32_t slot = 0; slot != stackSize; ++slot)
-                store(&(tileFrame.stack + slot)->tMin, load_m128(&(blockFrame.sortedStack + slot)->tMin));
-            uint32_t count = traverseTiles(scratch.data(), uint32_t(scratch.size()), tileFrame, stackSize, tilesW[tile]);
-            lists[tile].assign(scratch.begin(), scratch.begin() + count);
-        }
+    };
+    {
+        std::vector<std::thread> cullPool;
+        for (uint32_t t = 1; t < nt; t++) cullPool.emplace_back(cullWorker);
+        cullWorker();
+        for (auto& th : cullPool) th.join();
     }
 
-    // lighting environment (GPUSceneState::updateLighting, RC/gpu_scene_state.cu:47-81)
-    LightingEnvironment env;
-    memset(&env, 0, sizeof(env));
-    for (uint32_t i = 0; i < in->light_count; i++) {
-        const LightUnion& l = ((const LightUnion*)in->lights)[i];
-        if (l.type == LightType::directional && env.directionalLightCount < int(MAX_DIRECTIONAL_LIGHTS))
-            env.directionalLights[env.directionalLightCount++] = l.directional;
-        else if (l.type == LightType::point && env.pointLightCount < int(MAX_POINT_LIGHTS))
-            env.pointLights[env.pointLightCount++] = l.point;
-        else if (l.type == LightType::spot && env.spotLightCount < int(MAX_SPOT_LIGHTS))
-            env.spotLights[env.spotLightCount++] = l.spot;
-    }
-    const SimpleMaterial* materials = (const SimpleMaterial*)md.materials;
+    const SimpleMaterial* materials = S.materials.data();
     // material textures: the texture object of id i is i, and ReadTexture's tex2DGrad goes to the
     // frame's texture sampler
-    hv_texture_hook = in->texture_count ? in->texture_sample : nullptr;
-    hv_texture_hook_ctx = in->texture_ctx;
+    hv_texture_hook = S.textureCount ? S.textureSample : nullptr;
+    hv_texture_hook_ctx = S.textureCtx;
     std::vector<cudaTextureObject_t> textureObjects(SimpleMaterial::maxTextureCount);
     for (uint32_t i = 0; i < SimpleMaterial::maxTextureCount; i++) textureObjects[i] = cudaTextureObject_t(i);
     vector3 cameraPos = vector3(cameraToWorld.m3);
@@ -292,13 +349,13 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
 
     // depth of field: the lens table of GPUCamera::initLookupTables (RC/gpu_camera.cu:59-88) and the
     // occupied-tile index the intersect/resolve kernels run under (tileIndexRemapOccupied)
-    const bool dof = in->lens.radius > 0.0f;
+    const bool dof = S.lens.radius > 0.0f;
     std::vector<vector2> lensTab;
     std::vector<uint32_t> occRank(tileCount, 0);
     alignas(CameraBeams) unsigned char cbStorage[sizeof(CameraBeams)];
     memset(cbStorage, 0, sizeof(cbStorage));
     CameraBeams& cameraBeams = *reinterpret_cast<CameraBeams*>(cbStorage); // TileData<true>::load reads .lens only
-    cameraBeams.lens = lens;
+    cameraBeams.lens = S.lens;
     if (dof) {
         std::uniform_real_distribution<float> uniformRandomDist(0.0f, 1.0f);
         std::mt19937 generator;
@@ -350,7 +407,7 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             if (dof) tileDoF.load(cameraBeams, cameraToWorld,
                                   matrix3x3(cameraToWorld) * batch.directionalBeams[base + TILE_SIZE / 2]);
             for (uint32_t idx : list) {
-                const PrecomputedTriangleIntersect& tri = tris[idx];
+                const PrecomputedTriangleIntersect& tri = S.tris[idx];
                 if (!planes.test(tri)) continue;
                 if (dof) {
                     IntersectTriangleTile<true> tt;
@@ -374,7 +431,7 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                 // IntersectSamples (RC/intersect.cu:117-168)
                 vector3 centerDir = normalize(sample.centerRay);
                 float zed = dot(matrix3x3(cameraToWorld) * vector3(0, 0, -1.0f), centerDir);
-                vector3 lensCenterToFocalCenter = (lens.focalDistance / zed) * centerDir;
+                vector3 lensCenterToFocalCenter = (S.lens.focalDistance / zed) * centerDir;
                 float tmaxv[32];
                 uint32_t hit[32];
                 for (uint32_t i = 0; i < N; i++) { tmaxv[i] = FLT_MAX; hit[i] = ~0u; }
@@ -443,7 +500,7 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                     vector3 b, bOffX, bOffY;
                     if (dof) {
                         IntersectTriangleTile<true> tt;
-                        tt.setup(tris[triIndex], cameraPos, tileDoF.lensU, tileDoF.lensV);
+                        tt.setup(S.tris[triIndex], cameraPos, tileDoF.lensU, tileDoF.lensV);
                         IntersectTriangleThreadDoF th(tt, lensCenterToFocalCenter);
                         th.calcUVW(tt, lensCenterToFocalCenter, tileDoF.lensU, tileDoF.lensV, centroidLensUV,
                                    centroidDirUV, b);
@@ -456,7 +513,7 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                                    bOffY);
                     } else {
                         IntersectTriangleTile<false> tt;
-                        tt.setup(tris[triIndex], cameraPos);
+                        tt.setup(S.tris[triIndex], cameraPos);
                         IntersectTriangleThread th(tt, sample.centerRay, sample.du, sample.dv);
                         th.calcUVW(tt, centroidAlpha, b);
                         vector2 alpha_dX = centroidAlpha + vector2(1.0f, 0.0f);
@@ -464,12 +521,12 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
                         vector2 alpha_dY = centroidAlpha + vector2(0.0f, 1.0f);
                         th.calcUVW(tt, alpha_dY, bOffY);
                     }
-                    InterpolatedVertex vI = interpolate(world.data(), triShade[triIndex], b);
-                    InterpolatedVertex vInterpX = interpolate(world.data(), triShade[triIndex], bOffX);
-                    InterpolatedVertex vInterpY = interpolate(world.data(), triShade[triIndex], bOffY);
+                    InterpolatedVertex vI = interpolate(S.world.data(), S.triShade[triIndex], b);
+                    InterpolatedVertex vInterpX = interpolate(S.world.data(), S.triShade[triIndex], bOffX);
+                    InterpolatedVertex vInterpY = interpolate(S.world.data(), S.triShade[triIndex], bOffY);
                     vector2 dUVdX = vInterpX.uv - vI.uv;
                     vector2 dUVdY = vInterpY.uv - vI.uv;
-                    vector4 shaded = GGXShade(triShade[triIndex].material, vI, dUVdX, dUVdY, cameraPos, materials,
+                    vector4 shaded = GGXShade(S.triShade[triIndex].material, vI, dUVdX, dUVdY, cameraPos, materials,
                                               textureObjects.data(), env);
                     result += shaded * float(__builtin_popcount(sampleMask));
                 }
@@ -479,7 +536,6 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
             }
         }
     };
-    uint32_t nt = in->threads ? in->threads : 1;
     std::vector<std::thread> pool;
     for (uint32_t t = 1; t < nt; t++) pool.emplace_back(worker);
     worker();
@@ -496,14 +552,52 @@ extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
     out->tile_total = total;
     if (out->colors) memcpy(out->colors, colors.data(), size_t(padded) * 4);
     if (out->image) {
-        for (uint32_t y = 0; y < in->height; y++)
-            for (uint32_t x = 0; x < in->width; x++) {
-                int32_t o = sd.imageLocationToSampleIndex[size_t(y) * in->width + x];
-                if (o >= 0 && in->split_color_samples == 1) out->image[size_t(y) * in->width + x] = colors[o];
+        for (uint32_t y = 0; y < S.height; y++)
+            for (uint32_t x = 0; x < S.width; x++) {
+                int32_t o = sd.imageLocationToSampleIndex[size_t(y) * S.width + x];
+                if (o >= 0 && S.split == 1) out->image[size_t(y) * S.width + x] = colors[o];
             }
     }
     return 0;
 }
+
+} // namespace
+
+
+extern "C" int ref_render(const oracle_frame_in* in, oracle_frame_out* out) {
+    MxcsrScope mx;
+    RefSession S;
+    const int rc = refSetup(in, out, S);
+    if (rc) return rc;
+    return refFrame(S, in->cam_xf, in->threads, out);
+}
+
+// A camera kept across frames, as the reference's Raycaster keeps it: ref_session_create does the
+// scene upload and the sample setup once; each ref_session_frame renders one frame (frusta to
+// world, traversal, intersect and shading on `threads` threads, remap) into colors [padded] and
+// image [height*width] (either may be NULL).
+extern "C" int ref_session_create(const oracle_frame_in* in, void** session) {
+    MxcsrScope mx;
+    std::unique_ptr<RefSession> S(new RefSession());
+    oracle_frame_out none;
+    memset(&none, 0, sizeof(none));
+    const int rc = refSetup(in, &none, *S);
+    if (rc) return rc;
+    *session = S.release();
+    return 0;
+}
+
+extern "C" int ref_session_frame(void* session, const hvvr_transform* cam_xf, uint32_t threads, uint32_t* colors,
+                                 uint32_t* image) {
+    MxcsrScope mx;
+    oracle_frame_out out;
+    memset(&out, 0, sizeof(out));
+    out.colors = colors;
+    out.image = image;
+    return refFrame(*static_cast<RefSession*>(session), *cam_xf, threads, &out);
+}
+
+extern "C" void ref_session_destroy(void* session) { delete static_cast<RefSession*>(session); }
 
 // ------------------------------------------------------------------ foveated sample set
 // polarSpaceFoveatedSetup's sample-set part (libraries/hvvr/raycaster/foveated.cpp:47-110):
