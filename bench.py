@@ -50,6 +50,11 @@ def parse():
     ap.add_argument("--rates", default="100,250,500,1000,2000,5000,10000,20000", help="served: arrival rates, req/s")
     ap.add_argument("--seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--views", type=int, default=64)
+    ap.add_argument("--max-batch-views", type=int, default=64, help="served: views per throughput batch")
+    ap.add_argument("--served-cull-cap", type=int, default=3,
+                    help="served: throughput batches' tile-cull CTAs per SM (0 = no cap)")
+    ap.add_argument("--latency-frames", type=int, default=500,
+                    help="stereo: frames of the p50/p99 latency run after the timed steps")
     ap.add_argument("--profile", action="store_true",
                     help="case for ncu: the stereo frame (or with --workload foveated the foveated frame), 3 frames")
     return ap.parse_args()
@@ -62,15 +67,6 @@ def load_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def committed_traffic():
-    """DRAM bytes per frame of each kernel, scaled from the committed ncu captures, if present."""
-    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
-    return None
 
 
 class Clocks:
@@ -199,8 +195,9 @@ def frame_counts(hv, scenes, sc):
         c.set_capture(hv.HVVR_CAPTURE_HITS)
     rc.render()
     rc.render()
+    ctr = rc.counters()
     out = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0,
-           "tested_entries": int(rc.counters()[4])}
+           "tested_entries": int(ctr[4]), "tested_warp_entries": int(ctr[5]), "longest_tile_node_visits": 0}
     for cam in cams:
         blocks, tiles, padded, msaa = cam.layout()
         n, tri, mask = cam.gbuffer()
@@ -208,7 +205,9 @@ def frame_counts(hv, scenes, sc):
         out["tiles"] += tiles
         out["list_entries"] += cam.list_total()
         out["unique_hits"] += int(((tri != 0xFFFFFFFF) & (mask != 0)).sum())
-        out["node_visits"] += int(cam.tile_costs().astype(np.int64).sum())
+        costs = cam.tile_costs().astype(np.int64)
+        out["node_visits"] += int(costs.sum())
+        out["longest_tile_node_visits"] = max(out["longest_tile_node_visits"], int(costs.max()))
     rc.close()
     return out
 
@@ -221,20 +220,22 @@ def intersect_bytes(c):
 
 
 def intersect_flops(c, msaa):
-    """FP32 operations of a frame's intersect tests: every list entry that passes the per-tile tests
-    is tested against the 128 samples of its tile, 72 flops of per-(sample, triangle) setup
-    (IntersectTriangleThread + GetDifferentials) and 16 per subsample (7 FMA + 2 adds)."""
-    return c["tested_entries"] * 128 * (72 + 16 * msaa)
+    """FP32 operations of a frame's executed intersect tests: every (warp of 32 samples, surviving
+    list entry) pair whose tests ran (counted on the device; pairs the per-warp depth bound skips are
+    not counted), 72 flops of per-(sample, triangle) setup (IntersectTriangleThread +
+    GetDifferentials) and 16 per subsample test (7 FMA + 2 adds) per sample."""
+    return c["tested_warp_entries"] * 32 * (72 + 16 * msaa)
 
 
 def fp32_line(c, msaa, launch_ms, sm_mhz):
-    """achieved FP32 rate of the intersect launches against the FP32 peak at the sampled SM clock
-    (148 SMs x 128 FP32 lanes x 2 flops per FMA: a nominal figure; no FP32 peak is measured)"""
+    """achieved FP32 rate of the intersect launch (timed alone) against the FP32 peak at the sampled
+    SM clock (148 SMs x 128 FP32 lanes x 2 flops per FMA: a nominal figure; no FP32 peak is measured)"""
     flops = intersect_flops(c, msaa)
     peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     achieved = flops / (launch_ms * 1e-3) / 1e12
-    return {"flops_per_frame": flops, "achieved_tflops": achieved, "peak_tflops": peak, "frac": achieved / peak,
-            "peak_source": "nominal at %.0f MHz" % sm_mhz}
+    return {"flops_per_launch": flops, "launch_ms": launch_ms, "achieved_tflops": achieved, "peak_tflops": peak,
+            "frac": achieved / peak, "peak_source": "nominal at %.0f MHz" % sm_mhz,
+            "counted": "executed subsample tests only (device counter)"}
 
 
 def cull_bytes(c):
@@ -445,10 +446,18 @@ def main():
         ends[i].record(stream)
         torch.cuda.synchronize()
     torch.cuda.synchronize()
+    frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    # frame latency over a longer run of the same frames (p50/p99 over args.latency_frames), still
+    # inside the clock sampling window
+    lat_ms = frame_latencies(rc, sp, stream, flush, args.latency_frames)
     ck = clocks.stop()
     rc.synchronize()
-    kernel_ms, stage_ms = launch_times(rc, cams[0], lambda k: rc.render(stream=sp), flush)
-    frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    # the pipeline's span and the stages, from frames with per-launch events
+    _, stage_ms = launch_times(rc, cams[0], lambda k: rc.render(stream=sp), flush)
+    parts = rc.part_times()
+    span = parts[2 * 3 + 1]  # rate class 3 (8x MSAA), the pipelined part
+    # each kernel alone: one launch over all tiles of the frame, serial on one stream
+    kernel_ms, _ = launch_times(rc, cams[0], lambda k: rc.render(stream=sp), flush, pipeline=0, heavy_divisor=0)
     total_ms = max_over_ranks(sum(frame_ms), dist, "cuda")
     ms_per_step = total_ms / args.steps
     value = replica_throughput(samples_per_frame, args.steps, total_ms * 1e-3, world)
@@ -477,35 +486,47 @@ def main():
     cull_ms = statistics.mean(k[0] for k in kernel_ms)
     isect_ms = statistics.mean(k[1] for k in kernel_ms)
     kernels = {
-        "tileCullKernel": {"algorithmic_bytes": cull_bytes(counts), "launch_ms_per_frame": cull_ms},
-        "intersectShadeKernel<8,FMA>": {"algorithmic_bytes": intersect_bytes(counts), "launch_ms_per_frame": isect_ms},
+        "tileCullKernel": {"algorithmic_bytes": cull_bytes(counts), "launch_ms": cull_ms},
+        "intersectShadeKernel<8,FMA>": {"algorithmic_bytes": intersect_bytes(counts), "launch_ms": isect_ms},
     }
-    tr = committed_traffic()
     for name, k in kernels.items():
-        k["achieved_gbs"] = k["algorithmic_bytes"] / (k["launch_ms_per_frame"] * 1e-3) / 1e9
+        k["achieved_gbs"] = k["algorithmic_bytes"] / (k["launch_ms"] * 1e-3) / 1e9
         k["frac"] = k["achieved_gbs"] / peak
-        k["traffic"] = (tr or {}).get(name)
-    dom = max(kernels, key=lambda n: kernels[n]["launch_ms_per_frame"])
+    dom = max(kernels, key=lambda n: kernels[n]["launch_ms"])
+    fp32 = fp32_line(counts, MSAA, isect_ms, ck.get("sm_mhz") or 1965.0)
     line = {
         "metric": "vis+shade Gsamples/s", "value": value, "unit": "Gsamples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-        "p50_frame_ms": statistics.median(frame_ms), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
+        "p50_frame_ms": float(np.percentile(lat_ms, 50)), "p99_frame_ms": float(np.percentile(lat_ms, 99)),
+        "latency_frames": len(lat_ms),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded procedural 995k-triangle scene, barrel-distorted sample set)",
         "config": stereo_config(world),
         "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 2 * 32,
                 "d2h_bytes_per_step": 2 * W * H * 4},
         "roofline": {"bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": kernels[dom]["frac"], "traffic": kernels[dom]["traffic"], "kernel": dom,
-                     "per_frame": "launches of one stereo frame; bytes and times summed over them",
+                     "frac": kernels[dom]["frac"], "traffic": None, "kernel": dom,
+                     "launch_ms": kernels[dom]["launch_ms"],
+                     "timed": "each kernel alone: one launch over all 20,352 tiles of the stereo frame, serial on one "
+                              "stream (pipeline off, no heavy split), per-launch CUDA events on that stream, mean of "
+                              "5 frames after the timed ones",
+                     "traffic_source": "null here: DRAM bytes per launch are in the committed ncu summaries under "
+                                       "profiles/ (the BVH and the shared list triangles stay in L2, so DRAM traffic is "
+                                       "far below the algorithmic bytes)",
+                     "binding_bound": "neither kernel is HBM-bound: the tile cull is latency-bound (dependent node "
+                                      "visits, see critical_path) and the intersect FP32-issue-bound (see fp32)",
                      "peak_source": peak_kind, "kernels": kernels, "counts": counts},
-        "fp32": fp32_line(counts, MSAA, isect_ms, ck.get("sm_mhz") or 1965.0),
+        "fp32": fp32,
+        "critical_path": {"pipeline_span_ms": float(span[2] - span[0]) if span[0] >= 0 else None,
+                          "longest_tile_node_visits": counts["longest_tile_node_visits"],
+                          "note": "the frame ends when the longest tiles' dependent node visits and their shading "
+                                  "end; span measured with per-launch events (which cost device time)"},
         "stage_ms_per_frame": {k: statistics.mean(s[i] for s in stage_ms) for i, k in
                                [(1, "block_cull"), (2, "first_tile_cull"), (3, "rest_of_cull_and_intersect_shade"),
                                 (4, "remap"), (5, "total")]},
-        # per frame (ncu launch list): block cull, tile order, tile cull + retry pass + intersect for
-        # the slowest tiles and for the rest, remap per eye
-        "gpu_launches": args.steps * 10,
+        # per frame: block cull, tile order, tile cull, pipelined intersect/shade, retry cull, retry-list
+        # shade, remap per eye
+        "gpu_launches": args.steps * 8,
         "sample_setup_ms": setup_ms,
         "clocks": ck,
     }
@@ -699,9 +720,10 @@ def run_served(args):
     """Render server under open-loop Poisson arrivals. Six resident scenes (about 100k to 4M
     triangles); request mix: view templates per scene drawn from {256x256, 640x480,
     1080x1200 barrel, foveated 300k-1.2M} with MSAA {1,4,8,16}, plus 5% stereo requests (two
-    1080x1200 barrel 8xMSAA eyes on the 1M scene, 64 mm IPD). HBM budget 120 GiB. Arrivals
-    that find BACKLOG requests already waiting are shed (counted). Latency = output ready -
-    submit, on the server's clock. Then a sample of requests is rendered again by the plain
+    1080x1200 barrel 8xMSAA eyes on the 1M scene, 64 mm IPD) submitted as the latency class.
+    HBM budget 120 GiB. Arrivals that find BACKLOG requests already waiting are shed (counted).
+    Latency = output ready - submit, on the server's clock (a stereo pair: both eyes), reported
+    over all requests and per class. Then a sample of requests is rendered again by the plain
     path (a single-view batch) and compared image for image."""
     import torch
     import hvvr_b200 as hv
@@ -717,8 +739,9 @@ def run_served(args):
         for l in sc.lights:
             rc.create_light(l)
         rcs.append(rc)
-    srv = hv.Server(rcs, hv.server_config(slots=3, max_batch_views=64, slot_list_capacity=512 << 20,
-                                          hbm_budget_bytes=120 << 30))
+    srv = hv.Server(rcs, hv.server_config(slots=3, max_batch_views=args.max_batch_views, slot_list_capacity=512 << 20,
+                                          hbm_budget_bytes=120 << 30, latency_slots=1,
+                                          tile_cull_ctas_per_sm=args.served_cull_cap))
     rng = np.random.default_rng(5)
     tmpl = []  # (view id, width, height, samples, scene, spec)
     for si in range(len(scs)):
@@ -760,6 +783,7 @@ def run_served(args):
         start = time.perf_counter()
         next_t = start + rng.exponential(1.0 / rate)
         lat, qwait, service = [], [], []
+        lat_class = {"stereo": [], "other": []}
         done_samples = 0
         group_done = {}
         end_arrivals = start + args.seconds
@@ -774,7 +798,7 @@ def run_served(args):
                     if rng.uniform() < 0.05:
                         g = ("s", arrivals)
                         for xf in eyes:
-                            rid = srv.submit(stereo_vid, 8, xf, device_ptr=out_ptr(stereo_vid, W, H))
+                            rid = srv.submit(stereo_vid, 8, xf, device_ptr=out_ptr(stereo_vid, W, H), priority=1)
                             groups[rid] = g
                             submitted_samples[rid] = W * H
                         group_done[g] = [2, 0.0]
@@ -799,6 +823,7 @@ def run_served(args):
                 gd[1] = max(gd[1], c.done_ms - c.submit_ms)
                 if gd[0] == 0:
                     lat.append(gd[1])
+                    lat_class["stereo" if g[0] == "s" else "other"].append(gd[1])
                     del group_done[g]
             if now >= end_arrivals and pending == 0:
                 break
@@ -812,6 +837,10 @@ def run_served(args):
                 "throughput_req_s": len(lat) / wall,
                 "p50_latency_ms": float(np.percentile(lat, 50)) if lat else None,
                 "p99_latency_ms": float(np.percentile(lat, 99)) if lat else None,
+                "per_class": {k: {"requests": len(v), "p50_latency_ms": float(np.percentile(v, 50)) if v else None,
+                                  "p99_latency_ms": float(np.percentile(v, 99)) if v else None,
+                                  "max_latency_ms": float(max(v)) if v else None}
+                              for k, v in lat_class.items()},
                 "p50_queue_ms": float(np.percentile(qwait, 50)) if qwait else None,
                 "p50_service_ms": float(np.percentile(service, 50)) if service else None,
                 "p99_service_ms": float(np.percentile(service, 99)) if service else None,
@@ -855,8 +884,10 @@ def run_served(args):
         "dtype": "f32", "data": "synthetic (6 seeded procedural scenes, grid/barrel/foveated sample sets)",
         "config": {"workload": "render server: 6 resident scenes (0.1M-4.1M tris), %d view templates + stereo "
                                "2x1080x1200 8xMSAA (5%% of requests), Poisson arrivals %s req/s for %.1f s each, "
-                               "120 GiB HBM budget, 3 slots x 64 views, backlog limit %d, instances pre-warmed" %
-                               (len(tmpl), args.rates, args.seconds, BACKLOG),
+                               "120 GiB HBM budget, 3 throughput slots x %d views + 1 latency slot (stereo pairs as "
+                               "the latency class), throughput tile-cull cap %d CTAs/SM, backlog limit %d, instances "
+                               "pre-warmed" % (len(tmpl), args.rates, args.seconds, args.max_batch_views,
+                                               args.served_cull_cap, BACKLOG),
                    "l2": "inputs larger than L2"},
         "sweep": sweep, "served_vs_plain_image_match": "%d/%d" % (matches, checks),
         "host_setup_s": setup_s, "clocks": ck,
@@ -992,7 +1023,9 @@ def run_foveated(args):
         for c in cams:
             c.set_eye_dir(saccade(frame + k))
         rc.render(stream=sp)
-    kernel_ms, stage_ms = launch_times(rc, cams[0], fov_frame, flush)
+    _, stage_ms = launch_times(rc, cams[0], fov_frame, flush)
+    # each kernel alone: one launch over all tiles, serial on one stream
+    kernel_ms, _ = launch_times(rc, cams[0], fov_frame, flush, pipeline=0, heavy_divisor=0)
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = max_over_ranks(sum(frame_ms), dist, "cuda")
     value = replica_throughput(samples_per_frame, args.steps, total_ms * 1e-3, world)
@@ -1115,13 +1148,18 @@ def run_profile_case_foveated():
     rc.close()
 
 
-def launch_times(rc, cam, render, flush, frames=5):
+def launch_times(rc, cam, render, flush, frames=5, **cfg):
     """Per-launch device times of the workload's frames: the timed frames run without per-launch
     events (they cost device time), so these come from `frames` more frames of the same workload
-    rendered right after them with config.timing = 1 (L2 flushed before each, as in the timed
-    loop). Returns ([cull, intersect, block cull, remap/resolve] ms, camera stage ms) per frame."""
+    rendered right after them with config.timing = 1 and the given config changes (L2 flushed
+    before each, as in the timed loop; one untimed frame first when the config changes). Returns
+    ([cull, intersect, block cull, remap/resolve] ms, camera stage ms) per frame."""
     import torch
-    rc.set_batch_config(timing=1)
+    saved = rc.batch_config()
+    rc.set_batch_config(timing=1, **cfg)
+    if cfg:
+        render(0)
+        torch.cuda.synchronize()
     kernel_ms, stage_ms = [], []
     for k in range(frames):
         flush.fill_(k & 0xff)
@@ -1129,8 +1167,24 @@ def launch_times(rc, cam, render, flush, frames=5):
         torch.cuda.synchronize()
         kernel_ms.append([float(x) for x in rc.kernel_times()])
         stage_ms.append([float(x) for x in cam.timings()])
-    rc.set_batch_config(timing=0)
+    rc.set_batch_config(saved)
     return kernel_ms, stage_ms
+
+
+def frame_latencies(rc, sp, stream, flush, frames):
+    """Device times of `frames` consecutive frames (L2 flushed before each, untimed), in ms."""
+    import torch
+    if frames <= 0:
+        return []
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(frames)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(frames)]
+    for i in range(frames):
+        flush.fill_(i & 0xff)
+        starts[i].record(stream)
+        rc.render(stream=sp)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
 
 def ctypes_stream(stream):

@@ -86,6 +86,7 @@ _sig("hvvr_scene_get_counts", _vp, _p(_u32), _p(_u32), _p(_u32))
 _sig("hvvr_scene_read_nodes", _vp, _vp)
 _sig("hvvr_scene_read_triangles", _vp, _vp)
 _sig("hvvr_generate_topology", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32))
+_sig("hvvr_generate_topology_device", _vp, _u32, _vp, _u32, _vp, _u32, _p(_u32), _vp)
 _sig("hvvr_grid_samples", _u32, _u32, _vp)
 _sig("hvvr_scene_file_load", C.c_char_p, _p(_vp))
 _sig("hvvr_scene_file_counts", _vp, _p(_u32), _p(_u32), _p(_u32))
@@ -151,7 +152,8 @@ EXPORTED = [
     "hvvr_camera_read_tile_lists", "hvvr_camera_read_block_stacks", "hvvr_camera_read_hits",
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
-    "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_grid_samples",
+    "hvvr_scene_read_nodes", "hvvr_scene_read_triangles", "hvvr_generate_topology", "hvvr_generate_topology_device",
+    "hvvr_grid_samples",
     "hvvr_polar_foveated_layout", "hvvr_polar_foveated_samples", "hvvr_scene_file_load", "hvvr_scene_file_counts",
     "hvvr_scene_file_mesh", "hvvr_scene_file_light", "hvvr_scene_file_texture", "hvvr_scene_file_close",
     "hvvr_scene_file_save", "hvvr_samples_load", "hvvr_samples_save",
@@ -191,6 +193,18 @@ def generate_topology(scene):
     cnt = _u32(0)
     _check(_lib.hvvr_generate_topology(scene.verts.ctypes.data, len(scene.verts), scene.tri_shade.ctypes.data,
                                        len(scene.tri_shade), nodes.ctypes.data, len(nodes), C.byref(cnt)))
+    scene.nodes = nodes[: cnt.value].copy()
+    return scene
+
+
+def generate_topology_device(scene, stream=None):
+    """The device BVH build (hvvr_generate_topology_device): builds scene.nodes on the GPU and
+    reorders scene.tri_shade in place (vertices keep their order)."""
+    nodes = np.zeros(len(scene.tri_shade) + 4, dtype=_abi.TOPO_DTYPE)
+    cnt = _u32(0)
+    _check(_lib.hvvr_generate_topology_device(scene.verts.ctypes.data, len(scene.verts), scene.tri_shade.ctypes.data,
+                                              len(scene.tri_shade), nodes.ctypes.data, len(nodes), C.byref(cnt),
+                                              stream))
     scene.nodes = nodes[: cnt.value].copy()
     return scene
 
@@ -677,9 +691,9 @@ class Raycaster:
 
     def counters(self):
         """the last frame's counters: list pool entries, retried tiles, status, views, list entries
-        that passed the intersect's per-tile tests"""
-        t = np.zeros(5, dtype=np.uint64)
-        _check(_lib.hvvr_raycaster_read_counters(self.handle, t.ctypes.data, 5))
+        that passed the intersect's per-tile tests, (warp, entry) pairs whose subsample tests ran"""
+        t = np.zeros(6, dtype=np.uint64)
+        _check(_lib.hvvr_raycaster_read_counters(self.handle, t.ctypes.data, 6))
         return t
 
     def part_times(self):
@@ -850,10 +864,11 @@ class Server:
     def prewarm(self, view, count):
         _check(_lib.hvvr_server_prewarm(self.handle, view, count))
 
-    def submit(self, view, msaa, camera_to_world, output=None, device_ptr=None, tag=0):
-        """output: a (height, width) uint32 numpy array (CPU), or device_ptr for CUDA memory"""
+    def submit(self, view, msaa, camera_to_world, output=None, device_ptr=None, tag=0, priority=0):
+        """output: a (height, width) uint32 numpy array (CPU), or device_ptr for CUDA memory;
+        priority 1: the latency class (rendered at once on a latency slot)"""
         r = _abi.Request()
-        r.view, r.msaa, r.camera_to_world, r.tag = view, msaa, camera_to_world, tag
+        r.view, r.msaa, r.camera_to_world, r.tag, r.priority = view, msaa, camera_to_world, tag, priority
         if device_ptr is not None:
             r.memory_type, r.output = HVVR_MEMORY_CUDA, device_ptr
         else:

@@ -22,6 +22,7 @@ HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA = 0, 1
 HVVR_MODE_DEFERRED_MSAA_RESOLVE, HVVR_MODE_FOVEATED_POLAR = 0, 1
 HVVR_FP_FMA, HVVR_FP_STRICT = 0, 1
 HVVR_SETUP_DEVICE, HVVR_SETUP_HOST = 0, 1
+HVVR_BVH_HOST, HVVR_BVH_DEVICE = 0, 1
 HVVR_CAPTURE_HITS = 1
 
 
@@ -99,7 +100,7 @@ class Spec(C.Structure):
                 ("foveated_mar_slope", C.c_float), ("foveated_foveal_mar_degrees", C.c_float),
                 ("output_format", C.c_uint32), ("output_to_3d_api", C.c_uint32),
                 ("fp_mode", C.c_uint32), ("tri_index_capacity", C.c_uint64), ("device", C.c_int),
-                ("sample_setup", C.c_uint32)]
+                ("sample_setup", C.c_uint32), ("bvh_build", C.c_uint32)]
 
 
 class TileCullArgs(C.Structure):
@@ -113,23 +114,25 @@ class BatchConfig(C.Structure):
     """hvvr_batch_config: knobs of a frame batch (set by hand or by hvvr_batch_autotune)."""
     _fields_ = [("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32), ("tri_index_capacity", C.c_uint64),
                 ("use_graph", C.c_uint32), ("frame_ms", C.c_float), ("tile_stack_entries", C.c_uint32),
-                ("timing", C.c_uint32)]
+                ("timing", C.c_uint32), ("pipeline", C.c_uint32), ("tile_cull_ctas_per_sm", C.c_uint32)]
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch_views", C.c_uint32),
                 ("slot_list_capacity", C.c_uint64), ("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32),
-                ("min_batch_views", C.c_uint32), ("max_wait_ms", C.c_float)]
+                ("min_batch_views", C.c_uint32), ("max_wait_ms", C.c_float), ("latency_slots", C.c_uint32),
+                ("tile_cull_ctas_per_sm", C.c_uint32)]
 
 
 class Request(C.Structure):
     _fields_ = [("view", C.c_uint32), ("msaa", C.c_uint32), ("camera_to_world", Transform),
-                ("memory_type", C.c_uint32), ("output", C.c_void_p), ("tag", C.c_uint64)]
+                ("memory_type", C.c_uint32), ("output", C.c_void_p), ("tag", C.c_uint64), ("priority", C.c_uint32)]
 
 
 class Completion(C.Structure):
     _fields_ = [("id", C.c_uint64), ("tag", C.c_uint64), ("status", C.c_int), ("batch_views", C.c_uint32),
-                ("submit_ms", C.c_double), ("dispatch_ms", C.c_double), ("done_ms", C.c_double)]
+                ("submit_ms", C.c_double), ("dispatch_ms", C.c_double), ("done_ms", C.c_double),
+                ("priority", C.c_uint32)]
 
 
 class ServerStats(C.Structure):

@@ -1,13 +1,13 @@
 // foveated_resolve.cu - the foveated resolve: polar sample texture -> screen image.
 //
-// The reference's resolve, pass for pass (GPUCamera::remapPolarFoveated and
+// The reference's resolve (GPUCamera::remapPolarFoveated and
 // ::foveatedPolarToScreenSpace, libraries/hvvr/raycaster/remap.cu:143-156 and
 // gpu_foveated.cu:335-375):
 //   polarScatterKernel     RemapPolarFoveatedKernel          remap.cu:126-141
 //   momentsKernel          ComputeMoments                    gpu_foveated.cu:124-139, 159-172
 //   polarToScreenKernel    FoveatedPolarToScreenSpaceKernel  gpu_foveated.cu:36-122, 141-157, 174-249
-//   eccFilterKernel x2     SeparableFilterUsingEccentricity  gpu_foveated.cu:251-294 (vertical, then horizontal)
-//   enhanceContrastKernel  FinishConstrastEnhancement        gpu_foveated.cu:296-333
+//   filterEnhanceKernel    SeparableFilterUsingEccentricity  gpu_foveated.cu:251-294 (vertical, then horizontal)
+//                          and FinishConstrastEnhancement    gpu_foveated.cu:296-333, fused (below)
 //
 // Every texture is a CUDA array read through a texture object and written through a surface
 // object, made with the reference's texture setup (createEmptyTexture, texture.cu:283-321, with
@@ -244,18 +244,18 @@ __global__ void __launch_bounds__(256) polarToScreenKernel(const ViewDev* views,
     surf2Dwrite(encodeSrgb(surfaceResult), f.resultSurf, int(i * 4), int(j));
 }
 
-// SeparableFilterUsingEccentricity: 11 taps along (sx, sy), clamped at the image edges, with
-// weights pow(1 - |R| / 5.1, sqrt(eccentricity)). Pass 0 filters this frame's result vertically
-// into filterV, pass 1 filterV horizontally into filterH (the textures come from the view table,
-// so a replayed graph follows the per-frame result buffer).
-__global__ void __launch_bounds__(256) eccFilterKernel(const ViewDev* views, uint32_t view, int pass) {
-    const FoveaDev& f = views[view].fov;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= f.width || j >= f.height) return;
-    const int sx = pass ? 1 : 0, sy = pass ? 0 : 1;
-    const cudaTextureObject_t input = pass ? f.filterVTex : f.resultTex;
-    const cudaSurfaceObject_t output = pass ? f.filterHSurf : f.filterVSurf;
-    const float eccentricity = pixelEccentricity(f, i, j);
+// The texture unit's value for an RGBA8 sRGB texel read at its centre, per 8-bit code: .x/.y/.z the
+// sRGB decode of the code in the red/green/blue channel, .w the linear alpha (read once per
+// camera from a 256-texel texture made like the screen textures, decodeTableKernel)
+__device__ __forceinline__ V4 decodeTexel(const float4* table, uint32_t c) {
+    return V4{table[c & 0xFFu].x, table[(c >> 8) & 0xFFu].y, table[(c >> 16) & 0xFFu].z, table[c >> 24].w};
+}
+
+// SeparableFilterUsingEccentricity at pixel (i, j): 11 taps along (sx, sy), clamped at the image
+// edges, with weights pow(1 - |R| / 5.1, sqrt(eccentricity)); tap(x, y) is the input value there
+template <class Tap>
+__device__ __forceinline__ uint32_t eccFilter(const FoveaDev& f, uint32_t i, uint32_t j, int sx, int sy,
+                                              float eccentricity, Tap tap) {
     const int filterRadius = 5;
     V4 valueSum{0.0f, 0.0f, 0.0f, 0.0f};
     float weightSum = 0.0f;
@@ -265,30 +265,65 @@ __global__ void __launch_bounds__(256) eccFilterKernel(const ViewDev* views, uin
         const int ty = clampi(int(j) + R * sy, 0, int(f.height) - 1);
         const float normDist = fabsf(float(R)) / float(filterRadius + 0.1);
         const float weight = powf(1.0f - normDist, sqrtf(eccentricity));
-        valueSum = valueSum + texelFetch(input, f.width, f.height, tx, ty) * weight;
+        valueSum = valueSum + tap(tx, ty) * weight;
         weightSum += weight;
     }
-    surf2Dwrite(encodeSrgb(divs(valueSum, weightSum)), output, int(i * 4), int(j));
+    return encodeSrgb(divs(valueSum, weightSum));
 }
 
-// FinishConstrastEnhancement with enhanceContrast (gpu_foveated.cu:296-333): sigma = 8 max(0.001,
-// t^2), f_e = 1 (gpu_camera.cu:181)
-__global__ void __launch_bounds__(256) enhanceContrastKernel(const ViewDev* views, uint32_t view) {
+// The vertical eccentricity filter, the horizontal one and FinishConstrastEnhancement with
+// enhanceContrast (gpu_foveated.cu:251-333; sigma = 8 max(0.001, t^2), f_e = 1, gpu_camera.cu:181)
+// in one pass over a tile of 64 x 4 pixels. The reference writes each filter pass to an RGBA8 sRGB
+// texture and the next pass reads it at texel centres; here the vertical pass's encoded values for
+// the tile and a 5-column halo on each side stay in shared memory, and the horizontal pass and the
+// enhancement decode the encoded values through the texture unit's own decode table, so every
+// value equals what the texture reads return. The result texture (this frame's temporal result,
+// the next frame's history) is still read through its texture object.
+constexpr int kFeW = 64, kFeH = 4, kFeRadius = 5, kFeHaloW = kFeW + 2 * kFeRadius;
+
+__global__ void __launch_bounds__(kFeW * kFeH) filterEnhanceKernel(const ViewDev* views, uint32_t view) {
     const FoveaDev& f = views[view].fov;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    __shared__ float4 table[256];
+    __shared__ uint32_t vq[kFeH][kFeHaloW];
+    const uint32_t tid = threadIdx.y * kFeW + threadIdx.x;
+    table[tid] = f.srgbDecode[tid];
+    const int x0 = int(blockIdx.x) * kFeW, y0 = int(blockIdx.y) * kFeH;
+    // vertical pass of this frame's result over the tile and its halo columns
+    for (uint32_t p = tid; p < uint32_t(kFeH * kFeHaloW); p += kFeW * kFeH) {
+        const int r = int(p) / kFeHaloW, c = int(p) % kFeHaloW;
+        const int j = y0 + r;
+        if (j >= int(f.height)) continue;
+        const uint32_t ic = uint32_t(clampi(x0 - kFeRadius + c, 0, int(f.width) - 1));
+        const float eccentricity = pixelEccentricity(f, ic, uint32_t(j));
+        vq[r][c] = eccFilter(f, ic, uint32_t(j), 0, 1, eccentricity, [&](int tx, int ty) {
+            return texelFetch(f.resultTex, f.width, f.height, tx, ty);
+        });
+    }
+    __syncthreads();
+    const uint32_t i = uint32_t(x0) + threadIdx.x, j = uint32_t(y0) + threadIdx.y;
     if (i >= f.width || j >= f.height) return;
     const float eccentricity = pixelEccentricity(f, i, j);
+    // horizontal pass, reading the vertical pass's encoded values as the texture would return them
+    const uint32_t hq = eccFilter(f, i, j, 1, 0, eccentricity, [&](int tx, int ty) {
+        return decodeTexel(table, vq[ty - y0][tx - (x0 - kFeRadius)]);
+    });
     float sigma = 8.0f;
     const float t = eccentricity * f.invMaxEcc;
     sigma *= fmaxf(0.001f, clampf(t * t, 0.f, 1.f));
     const V4 pix = texelFetch(f.resultTex, f.width, f.height, int(i), int(j));
-    const V4 pmean = texelFetch(f.filterHTex, f.width, f.height, int(i), int(j));
+    const V4 pmean = decodeTexel(table, hq);
     const float f_e = 1.0f;
     const float cScale = 1.f + sigma * f_e;
     const V4 scaled = pmean + (pix - pmean) * cScale;
     const V4 r{clampf(scaled.x, 0.0f, 1.0f), clampf(scaled.y, 0.0f, 1.0f), clampf(scaled.z, 0.0f, 1.0f),
                clampf(scaled.w, 0.0f, 1.0f)};
     f.image[size_t(f.imageStride) * j + i] = encodeSrgb(r);
+}
+
+// The decode table of filterEnhanceKernel: texel i of `codes` holds (i, i, i, i).
+__global__ void decodeTableKernel(cudaTextureObject_t codes, float4* out) {
+    const uint32_t i = threadIdx.x;
+    out[i] = tex2D<float4>(codes, (float(i) + 0.5f) / 256.0f, 0.5f);
 }
 
 } // namespace
@@ -302,9 +337,13 @@ cudaError_t launchFoveatedResolve(const FrameDev& fr, uint32_t view, const Fovea
     polarScatterKernel<<<(fov.valid + 255) / 256, 256, 0, st>>>(fr.views, view);
     momentsKernel<<<polar, blk, 0, st>>>(fr.views, view);
     polarToScreenKernel<<<screen, blk, 0, st>>>(fr.views, view);
-    eccFilterKernel<<<screen, blk, 0, st>>>(fr.views, view, 0);
-    eccFilterKernel<<<screen, blk, 0, st>>>(fr.views, view, 1);
-    enhanceContrastKernel<<<screen, blk, 0, st>>>(fr.views, view);
+    const dim3 fe((fov.width + kFeW - 1) / kFeW, (fov.height + kFeH - 1) / kFeH);
+    filterEnhanceKernel<<<fe, dim3(kFeW, kFeH), 0, st>>>(fr.views, view);
+    return cudaGetLastError();
+}
+
+cudaError_t launchSrgbDecodeTable(cudaTextureObject_t codes, float4* out, cudaStream_t st) {
+    decodeTableKernel<<<1, 256, 0, st>>>(codes, out);
     return cudaGetLastError();
 }
 

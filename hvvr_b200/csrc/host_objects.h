@@ -170,7 +170,8 @@ struct hvvr_camera {
     // foveated resolve: polar textures, screen textures (fovResult[fovCur] is written by the next
     // frame, the other one holds the previous frame's result), the temporal history matrices
     // and the last frame's resolve matrices
-    TexArray polarRaw, polarDepth, moment1, moment2, fovResult[2], fovFilterV, fovFilterH;
+    TexArray polarRaw, polarDepth, moment1, moment2, fovResult[2];
+    DevBuf<float4> fovDecode;      // [256] the texture unit's read of each RGBA8 sRGB code
     FoveaDev fovStatic{};             // buffers, sizes and mapping constants (no per-frame fields)
     uint32_t fovCur = 0;
     float worldToEyePrev[16] = {};
@@ -188,6 +189,9 @@ struct hvvr_batch {
     bool fixedViews = false;          // renders exactly `cams` (else every enabled camera of rcs)
     std::vector<hvvr_camera*> cams;
     bool internal = false;            // a raycaster's own batch
+    // side-stream priorities: 0 = the slowest tiles' parts at the greatest priority, the rest at the
+    // default; 1 = every part at the greatest priority; 2 = every part at the least priority
+    int streamPriorities = 0;
     bool detached = false;            // one of its raycasters was destroyed
     hvvr_batch_config cfg{};
     // layout of the current frame
@@ -203,7 +207,7 @@ struct hvvr_batch {
     bool fpStrict = false;
     bool costValid = false;           // every view's tileCost holds a previous frame's counts
     DevBuf<ViewDev> viewsDev;
-    DevBuf<uint32_t> blockView, order, retry, pool, chunkNext, counters;
+    DevBuf<uint32_t> blockView, order, retry, ready, pool, chunkNext, counters;
     uint32_t poolChunks = 0;
     ViewDev* hostViews[2] = {};       // pinned staging of the per-frame view table
     size_t hostViewsCap = 0;
@@ -217,6 +221,7 @@ struct hvvr_batch {
     cudaEvent_t ev[6] = {};
     cudaEvent_t kev[2 * kRateClasses][3] = {}; // per side stream: before tile cull, after it, after intersect
     bool kevUsed[2 * kRateClasses] = {};
+    bool kevPipelined[2 * kRateClasses] = {}; // the part ran as a cull -> shade pipeline (kev[1] == kev[2])
     bool stageTimes = false;          // ev[1..4] and kev were recorded by the last frame
     cudaGraphExec_t graph = nullptr;
     std::vector<uint64_t> graphKey;

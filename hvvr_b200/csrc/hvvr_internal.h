@@ -29,7 +29,14 @@ enum : uint32_t {
     kStatusStackOverflow = 2u,  // tile traversal stack exhausted
     kStatusBadLeaf = 4u,        // a passing leaf had an empty/inverted triangle range
     kStatusRefitTimeout = 8u,   // refit walked more levels than the tree has
+    kStatusPipelineTimeout = 16u, // a pipelined shade CTA gave up waiting for its tile's list
+    kStatusBadInput = 32u,      // caller-supplied cull inputs out of range (hvvr_tile_cull_static)
 };
+
+// A pipelined rate class publishes each culled tile into a ready slot; the slot holds the global
+// tile index, with kReadyRetry set when the tile's traversal stack overflowed and the retry pass
+// culls and shades it instead. kReadyEmpty marks a slot not yet published.
+enum : uint32_t { kReadyEmpty = 0xffffffffu, kReadyRetry = 0x80000000u };
 
 // BVHNode (libraries/hvvr/raycaster/bvh_node.h:17-36), 128 bytes
 struct alignas(128) Node {
@@ -125,13 +132,14 @@ struct CameraDev {
 //   polar textures [rings][samplesPerRing]: colour (RGBA8 sRGB), view depth (float), first and
 //   second moments (RGBA16 unorm each)
 //   screen textures [height][width] (RGBA8 sRGB): this frame's temporally filtered result and the
-//   previous frame's, the vertical filter pass and the full (vertical then horizontal) filter
+//   previous frame's (the filter passes and the contrast enhancement run fused, in shared memory)
 struct FoveaDev {
     const uint2* remap;        // [valid] polar texel (azimuth index, ring) of each sample
     cudaTextureObject_t rawTex, depthTex, m1Tex, m2Tex;
     cudaSurfaceObject_t rawSurf, depthSurf, m1Surf, m2Surf;
-    cudaTextureObject_t resultTex, prevTex, filterVTex, filterHTex; // result: written this frame
-    cudaSurfaceObject_t resultSurf, filterVSurf, filterHSurf;
+    cudaTextureObject_t resultTex, prevTex; // result: written this frame
+    cudaSurfaceObject_t resultSurf;
+    const float4* srgbDecode;  // [256] the texture unit's read of an RGBA8 sRGB texel per 8-bit code
     uint32_t* image;           // nullptr: the view has no foveated resolve
     uint32_t imageStride, width, height;
     uint32_t spr, rings, valid;
@@ -190,6 +198,8 @@ struct FrameDev {
     uint32_t* counters = nullptr;      // [0] chunk allocator, [1] status bits, [2 + 3k ..] per-launch queues
     uint32_t* order = nullptr;         // [tiles] tile order: grouped by rate, then longest first
     uint32_t* retry = nullptr;         // [tiles] tiles whose traversal stack overflowed, per range
+    uint32_t* ready = nullptr;         // [tiles] ready slots of the pipelined rate classes (kReadyEmpty at frame start)
+    uint32_t cullCtasPerSm = 0;        // cap on the persistent tile cull's resident CTAs per SM (0: occupancy)
 };
 
 
@@ -200,12 +210,17 @@ int setLastError(int code, const char* msg);
 enum : uint32_t { kRateClasses = 12 };
 // counters: [0] chunk allocator, [1] status, then per tile-cull launch k (2 per rate class)
 // three words at kQueueBase + 3k: work-queue head, retry count, retry-queue head
-// then one word counting the list entries that survive the intersect's per-tile tests
+// then one word counting the list entries that survive the intersect's per-tile tests, one counting
+// the (warp, surviving entry) pairs whose subsample tests ran (the rest were skipped by the per-warp
+// depth bound), then per launch part k (2 per rate class) the ready-slot tail of its cull -> shade
+// pipeline
 enum : uint32_t {
     kQueueBase = 2,
     kQueueWords = 3,
     kSurvivorWord = kQueueBase + kQueueWords * 2 * kRateClasses,
-    kCounterWords = kSurvivorWord + 1
+    kTestedWord = kSurvivorWord + 1,
+    kPipeBase = kTestedWord + 1,
+    kCounterWords = kPipeBase + 2 * kRateClasses
 };
 
 // kernel launchers (defined in the .cu files); each returns cudaGetLastError()
@@ -215,13 +230,31 @@ cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st);
 cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st);
 // tile cull / intersect-shade of the global tiles order[first, first + count) (order ==
 // nullptr: tiles first..first+count-1). queues: kQueueWords zeroed words of this launch
-// (concurrent launches need their own). warps = tile-cull warps per CTA (2, 4 or 8). Tiles
+// (concurrent launches need their own). warps = tile-cull warps per CTA (1, 2, 4 or 8). Tiles
 // whose traversal stack outgrows stackLimit (0 = kTileStack; at least 8) are
 // culled again by a second launch with a 4096-entry stack.
 cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
                            uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st);
 cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, bool dof, const uint32_t* order,
                                  uint32_t first, uint32_t count, cudaStream_t st);
+// The cull -> shade pipeline of one part of a pinhole rate class over the global tiles
+// order[first, first + count), on one stream: the tile cull publishes every finished tile into fr.ready[first + i]
+// (i = the order of completion; pipe[0] counts them), and the shade launch - started while the
+// cull runs (programmatic dependent launch, once every cull CTA is resident) - shades slot i as
+// soon as it is published (pipe[1] hands out the slots; a wait gives up after about a second and
+// sets kStatusPipelineTimeout). Tiles whose stack outgrew stackLimit are then culled again with a
+// 4096-entry stack and shaded by a third launch over the retry list. queues: kQueueWords zeroed
+// words; pipe: 1 zeroed word; fr.ready[first, first + count) must hold kReadyEmpty.
+// the two passes of launchTileCull on their own: the main pass (which, given ready and readyTail,
+// publishes each finished tile as the pipeline describes) and the retry pass
+cudaError_t launchTileCullMain(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                               uint32_t* queues, uint32_t warps, uint32_t stackLimit, uint32_t* ready,
+                               uint32_t* readyTail, cudaStream_t st);
+cudaError_t launchTileCullRetryPass(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                                    uint32_t* queues, cudaStream_t st);
+cudaError_t launchCullShadePipeline(const FrameDev& fr, uint32_t msaa, bool fpStrict, uint32_t first, uint32_t count,
+                                    uint32_t* queues, uint32_t* pipe, uint32_t warps, uint32_t stackLimit,
+                                    cudaStream_t st);
 // occRank of every thin-lens view (one block per view; pinhole views are skipped)
 cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
@@ -231,6 +264,9 @@ cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);
 // the launch shapes): scatter to the polar textures, moments, polar -> screen with temporal
 // reprojection, two eccentricity filter passes and contrast enhancement into fov.image
 cudaError_t launchFoveatedResolve(const FrameDev& fr, uint32_t view, const FoveaDev& fov, cudaStream_t st);
+// out[256] <- the texture unit's value of a texel holding (i, i, i, i), read at its centre from
+// codes (a 256 x 1 RGBA8 texture made like the foveated screen textures)
+cudaError_t launchSrgbDecodeTable(cudaTextureObject_t codes, float4* out, cudaStream_t st);
 // writes v to *dst with a one-thread kernel (no host memory involved; capturable)
 cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st);
 

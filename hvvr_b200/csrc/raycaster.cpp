@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <iterator>
 #include <cmath>
 #include <atomic>
 #include <mutex>
@@ -385,11 +386,22 @@ int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st) {
         // screen textures (createImageSizedTexture: clamp, linear)
         for (int k = 0; k < 2; k++)
             TRY(cam->fovResult[k].create(w, h, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
-        TRY(cam->fovFilterV.create(w, h, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
-        TRY(cam->fovFilterH.create(w, h, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
         for (TexArray* t : {&cam->polarRaw, &cam->polarDepth, &cam->moment1, &cam->moment2, &cam->fovResult[0],
-                            &cam->fovResult[1], &cam->fovFilterV, &cam->fovFilterH})
+                            &cam->fovResult[1]})
             TRY(t->clear(st));
+        // the texture unit's read of each 8-bit code of a screen texture (for the fused filter and
+        // contrast pass): a 256-texel texture made like the screen textures, texel i = (i, i, i, i)
+        {
+            TexArray codes;
+            TRY(codes.create(256, 1, rgba8, 4, cudaReadModeNormalizedFloat, true, clamp, clamp, true));
+            uint32_t texels[256];
+            for (uint32_t i = 0; i < 256; i++) texels[i] = i * 0x01010101u;
+            CUDA_TRY(cudaMemcpy2DToArrayAsync(codes.array, 0, 0, texels, sizeof(texels), sizeof(texels), 1,
+                                              cudaMemcpyHostToDevice, st));
+            TRY(cam->fovDecode.alloc(256));
+            CUDA_TRY(launchSrgbDecodeTable(codes.tex, cam->fovDecode.p, st));
+            CUDA_TRY(cudaStreamSynchronize(st)); // before the probe texture and the host texels go
+        }
         if (cpuTarget) TRY(cam->image.alloc(npix));
         fv.remap = cam->polarRemap.p;
         fv.rawTex = cam->polarRaw.tex;
@@ -400,10 +412,7 @@ int setupFoveatedCamera(hvvr_camera* cam, cudaStream_t st) {
         fv.m1Surf = cam->moment1.surf;
         fv.m2Tex = cam->moment2.tex;
         fv.m2Surf = cam->moment2.surf;
-        fv.filterVTex = cam->fovFilterV.tex;
-        fv.filterVSurf = cam->fovFilterV.surf;
-        fv.filterHTex = cam->fovFilterH.tex;
-        fv.filterHSurf = cam->fovFilterH.surf;
+        fv.srgbDecode = cam->fovDecode.p;
         fv.image = cpuTarget ? cam->image.p : static_cast<uint32_t*>(cam->target.data);
         fv.imageStride = cpuTarget ? w : (cam->target.stride ? uint32_t(cam->target.stride) : w);
         fv.width = w;
@@ -600,16 +609,19 @@ void batchConfigDefault(hvvr_batch_config* c) {
     c->frame_ms = 0.0f;
     c->tile_stack_entries = 0;
     c->timing = 0;
+    c->pipeline = 1;
+    c->tile_cull_ctas_per_sm = 0;
 }
 
 int checkConfig(const hvvr_batch_config& c) {
-    if (c.tile_cull_warps != 2 && c.tile_cull_warps != 4 && c.tile_cull_warps != 8)
-        return fail(HVVR_ERR_INVALID, "tile_cull_warps must be 2, 4 or 8");
+    if (c.tile_cull_warps != 1 && c.tile_cull_warps != 2 && c.tile_cull_warps != 4 && c.tile_cull_warps != 8)
+        return fail(HVVR_ERR_INVALID, "tile_cull_warps must be 1, 2, 4 or 8");
     const uint64_t chunks = (c.tri_index_capacity + kChunk - 1) / kChunk;
     if (c.tri_index_capacity == 0 || chunks > 0xfffffff0ull) return fail(HVVR_ERR_INVALID, "bad tri_index_capacity");
     if (c.tile_stack_entries && (c.tile_stack_entries < 8 || c.tile_stack_entries > kTileStack))
         return fail(HVVR_ERR_INVALID, "tile_stack_entries must be 0 or in [8, 256]");
     if (c.timing > 1) return fail(HVVR_ERR_INVALID, "timing must be 0 or 1");
+    if (c.pipeline > 1) return fail(HVVR_ERR_INVALID, "pipeline must be 0 or 1");
     return HVVR_OK;
 }
 
@@ -623,9 +635,11 @@ int batchResources(hvvr_batch* b) {
     if (!b->forkEv) {
         int leastPriority = 0, greatestPriority = 0;
         CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+        const int heavyPrio = b->streamPriorities == 2 ? leastPriority : greatestPriority;
+        const int restPrio = b->streamPriorities == 1 ? greatestPriority : leastPriority;
         for (uint32_t r = 0; r < kRateClasses; r++) {
-            CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r], cudaStreamNonBlocking, greatestPriority));
-            CUDA_TRY(cudaStreamCreateWithFlags(&b->side[2 * r + 1], cudaStreamNonBlocking));
+            CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r], cudaStreamNonBlocking, heavyPrio));
+            CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r + 1], cudaStreamNonBlocking, restPrio));
         }
         CUDA_TRY(cudaEventCreateWithFlags(&b->rankEv, cudaEventDisableTiming));
         for (auto& e : b->cullEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -682,6 +696,8 @@ int checkStatus(const hvvr_batch* b) {
                     b->poolChunks);
     if (s & kStatusStackOverflow) return fail(HVVR_ERR_OVERFLOW, "tile traversal stack exhausted");
     if (s & kStatusBadLeaf) return fail(HVVR_ERR_INVALID, "BVH leaf with an empty triangle range passed the cull");
+    if (s & kStatusPipelineTimeout)
+        return fail(HVVR_ERR_TIMEOUT, "intersect/shade gave up waiting for a tile's list (cull -> shade pipeline)");
     return HVVR_OK;
 }
 
@@ -702,15 +718,18 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
     const bool stages = b->cfg.timing != 0;
     CUDA_TRY(recordStage(b->ev[0], st, capturing));
     CUDA_TRY(cudaMemsetAsync(fr.counters, 0, kCounterWords * sizeof(uint32_t), st));
+    if (b->cfg.pipeline && fr.tiles) CUDA_TRY(cudaMemsetAsync(fr.ready, 0xff, size_t(fr.tiles) * sizeof(uint32_t), st));
     CUDA_TRY(launchBlockCull(fr, st));
     if (stages) CUDA_TRY(recordStage(b->ev[1], st, capturing));
     CUDA_TRY(launchTileOrder(fr, st));
     CUDA_TRY(cudaEventRecord(b->forkEv, st));
     bool first = true;
     for (auto& u : b->kevUsed) u = false;
-    // Pinhole classes: tile cull then intersect on the same stream, per part. Thin-lens
-    // classes (one part each) need the occupied-tile ranks of the whole view, so all their
-    // culls finish before one rank launch, and their intersects follow it.
+    for (auto& u : b->kevPipelined) u = false;
+    // Pinhole classes: per part, tile cull then intersect on the part's stream, or (config.pipeline)
+    // one cull -> shade pipeline per part. Thin-lens classes (one part each) need the occupied-tile
+    // ranks of the whole view, so all their culls finish before one rank launch, and their
+    // intersects follow it.
     for (uint32_t r = 0; r < kRateClasses; r++) {
         const uint32_t n = b->rateTiles[r];
         if (!n) continue;
@@ -723,6 +742,23 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
             cudaStream_t ps = b->side[k];
             CUDA_TRY(cudaStreamWaitEvent(ps, b->forkEv, 0));
             if (stages) CUDA_TRY(recordStage(b->kev[k][0], ps, capturing));
+            if (!lens && b->cfg.pipeline) {
+                CUDA_TRY(launchCullShadePipeline(fr, msaa, b->fpStrict, p0, pn, fr.counters + kQueueBase + kQueueWords * k,
+                                                 fr.counters + kPipeBase + k, b->cfg.tile_cull_warps,
+                                                 b->cfg.tile_stack_entries, ps));
+                // the cull and the shade overlap: one event marks the end of both (and of the retry
+                // passes); no event sits between the two launches, which would serialise them
+                if (stages) {
+                    CUDA_TRY(recordStage(b->kev[k][1], ps, capturing));
+                    CUDA_TRY(recordStage(b->kev[k][2], ps, capturing));
+                    if (part == 1 && first) CUDA_TRY(recordStage(b->ev[2], ps, capturing));
+                }
+                b->kevUsed[k] = true;
+                b->kevPipelined[k] = true;
+                CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
+                CUDA_TRY(cudaStreamWaitEvent(st, b->doneEv[k], 0));
+                continue;
+            }
             CUDA_TRY(launchTileCull(fr, fr.order, p0, pn, fr.counters + kQueueBase + kQueueWords * k,
                                     b->cfg.tile_cull_warps, b->cfg.tile_stack_entries, ps));
             if (stages) CUDA_TRY(recordStage(b->kev[k][1], ps, capturing));
@@ -782,6 +818,7 @@ int reserveBatch(hvvr_batch* b, size_t tiles, size_t blocks, size_t views) {
     TRY(b->blockView.ensure(blocks));
     TRY(b->order.ensure(tiles));
     TRY(b->retry.ensure(tiles));
+    TRY(b->ready.ensure(tiles));
     TRY(b->viewsDev.ensure(views));
     if (b->hostViewsCap < views) {
         for (int k = 0; k < 2; k++) {
@@ -984,11 +1021,14 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     fr.counters = b->counters.p;
     fr.order = b->order.p;
     fr.retry = b->retry.p;
+    fr.ready = b->ready.p;
+    fr.cullCtasPerSm = b->cfg.tile_cull_ctas_per_sm;
     if (b->cfg.use_graph && b->costValid && capturable) {
         std::vector<uint64_t> gkey = b->layoutKey;
         const uint64_t extra[] = {b->cfg.tile_cull_warps, b->cfg.heavy_divisor, b->poolChunks, strict ? 1u : 0u,
-                                  uint64_t(uintptr_t(st)), b->cfg.tile_stack_entries, b->cfg.timing};
-        gkey.insert(gkey.end(), extra, extra + 7);
+                                  uint64_t(uintptr_t(st)), b->cfg.tile_stack_entries, b->cfg.timing,
+                                  b->cfg.pipeline, b->cfg.tile_cull_ctas_per_sm};
+        gkey.insert(gkey.end(), std::begin(extra), std::end(extra));
         if (!b->graph || gkey != b->graphKey) {
             dropGraph(b);
             CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
@@ -1055,6 +1095,7 @@ int hvvr_raycaster_create(const hvvr_spec* spec, hvvr_raycaster** out) {
     if (s.fp_mode != HVVR_FP_FMA && s.fp_mode != HVVR_FP_STRICT) return fail(HVVR_ERR_INVALID, "bad fp_mode");
     if (s.sample_setup != HVVR_SETUP_DEVICE && s.sample_setup != HVVR_SETUP_HOST)
         return fail(HVVR_ERR_INVALID, "bad sample_setup");
+    if (s.bvh_build != HVVR_BVH_HOST && s.bvh_build != HVVR_BVH_DEVICE) return fail(HVVR_ERR_INVALID, "bad bvh_build");
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) return fail(HVVR_ERR_CUDA, "no CUDA device available");
@@ -1264,6 +1305,12 @@ int kernelTimes(const hvvr_batch* b, float* ms4) {
     float cull = 0.0f, isect = 0.0f, t = 0.0f;
     for (uint32_t k = 0; k < 2 * kRateClasses; k++) {
         if (!b->kevUsed[k]) continue;
+        if (b->kevPipelined[k]) {
+            // cull and shade overlap: the span of the pipeline counts as intersect/shade time
+            CUDA_TRY(cudaEventElapsedTime(&t, b->kev[k][0], b->kev[k][2]));
+            isect += t;
+            continue;
+        }
         CUDA_TRY(cudaEventElapsedTime(&t, b->kev[k][0], b->kev[k][1]));
         cull += t;
         CUDA_TRY(cudaEventElapsedTime(&t, b->kev[k][1], b->kev[k][2]));
@@ -1283,9 +1330,9 @@ static int frameCounters(const hvvr_batch* b, uint64_t* out, uint32_t count) {
     CUDA_TRY(cudaEventSynchronize(b->ev[5]));
     uint64_t retried = 0;
     for (uint32_t k = 0; k < 2 * kRateClasses; k++) retried += b->hostCounters[kQueueBase + kQueueWords * k + 1];
-    const uint64_t v[5] = {uint64_t(std::min(b->hostCounters[0], b->poolChunks)) * kChunk, retried, b->hostCounters[1],
-                           b->views.size(), b->hostCounters[kSurvivorWord]};
-    for (uint32_t i = 0; i < count; i++) out[i] = i < 5 ? v[i] : 0u;
+    const uint64_t v[6] = {uint64_t(std::min(b->hostCounters[0], b->poolChunks)) * kChunk, retried, b->hostCounters[1],
+                           b->views.size(), b->hostCounters[kSurvivorWord], b->hostCounters[kTestedWord]};
+    for (uint32_t i = 0; i < count; i++) out[i] = i < 6 ? v[i] : 0u;
     return HVVR_OK;
 }
 
@@ -1298,6 +1345,7 @@ static int partTimes(const hvvr_batch* b, float* ms72) {
         o[0] = o[1] = o[2] = -1.0f;
         if (!b->kevUsed[k]) continue;
         for (int i = 0; i < 3; i++) CUDA_TRY(cudaEventElapsedTime(&o[i], b->ev[0], b->kev[k][i]));
+        if (b->kevPipelined[k]) o[1] = -1.0f; // the cull's own end is not observed in a pipeline
     }
     return HVVR_OK;
 }
@@ -1352,11 +1400,16 @@ int hvvr_batch_autotune(hvvr_batch* b, uint32_t frames, hvvr_batch_config* out) 
     hvvr_batch_config best = base;
     float bestMs = INFINITY;
     uint32_t maxChunks = 0;
-    for (uint32_t warps : {2u, 4u, 8u}) {
-        for (uint32_t div : {0u, 16u, 8u, 4u}) {
+    // per cull CTA width: the cull -> shade pipeline, and the split path with each heavy share
+    // (heavy_divisor 0 = no split); the pipeline does not use the heavy share
+    struct Candidate { uint32_t pipeline, div; };
+    const Candidate candidates[] = {{1u, base.heavy_divisor}, {0u, 0u}, {0u, 16u}, {0u, 8u}, {0u, 4u}};
+    for (uint32_t warps : {1u, 2u, 4u, 8u}) {
+        for (const Candidate& cand : candidates) {
             b->cfg = base;
             b->cfg.tile_cull_warps = warps;
-            b->cfg.heavy_divisor = div;
+            b->cfg.pipeline = cand.pipeline;
+            b->cfg.heavy_divisor = cand.div;
             std::vector<float> ms;
             for (uint32_t f = 0; f <= frames; f++) {
                 int r = renderBatch(b, st);
@@ -1402,8 +1455,15 @@ int hvvr_model_create(hvvr_raycaster* rc, const hvvr_mesh_data* mesh, hvvr_model
     } else {
         std::vector<hvvr_topology_node> nodes(size_t(mesh->tri_count) + 4);
         uint32_t count = 0;
-        TRY(hvvr_generate_topology(m->verts.data(), uint32_t(m->verts.size()), m->triShade.data(),
-                                   uint32_t(m->triShade.size()), nodes.data(), uint32_t(nodes.size()), &count));
+        if (rc->spec.bvh_build == HVVR_BVH_DEVICE) {
+            CUDA_TRY(cudaSetDevice(rc->spec.device));
+            TRY(hvvr_generate_topology_device(m->verts.data(), uint32_t(m->verts.size()), m->triShade.data(),
+                                              uint32_t(m->triShade.size()), nodes.data(), uint32_t(nodes.size()), &count,
+                                              rc->stream));
+        } else {
+            TRY(hvvr_generate_topology(m->verts.data(), uint32_t(m->verts.size()), m->triShade.data(),
+                                       uint32_t(m->triShade.size()), nodes.data(), uint32_t(nodes.size()), &count));
+        }
         nodes.resize(count);
         m->nodes = std::move(nodes);
     }

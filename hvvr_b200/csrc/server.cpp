@@ -15,6 +15,12 @@
 //     runs are rendered by the next one, overlapping on the device. An idle GPU takes any
 //     request at once; with a batch in flight the next one waits for min_batch_views requests
 //     or for its oldest request to have waited max_wait_ms.
+//   * latency class - requests with priority 1 (the two eyes of a stereo frame, say) go to the
+//     latency slots: dispatched as soon as one is free, never held back to fill a batch, on
+//     streams of the GPU's highest priority while the throughput slots run at its lowest, so
+//     their CTAs are scheduled ahead of the throughput batches' pending ones. A cap on the
+//     throughput slots' persistent tile-cull CTAs (tile_cull_ctas_per_sm) keeps SMs free for
+//     them while a long throughput cull runs.
 //     When the budget is short, idle instances of other templates are freed first.
 //   * completion - a slot whose end event has fired returns its instances to the pools and its
 //     requests to the completion queue (CPU outputs are copied out of pinned staging first).
@@ -52,6 +58,7 @@ struct Template {
 struct Instance {
     hvvr_camera* cam = nullptr;
     uint32_t tmpl = 0;
+    uint32_t width = 0, height = 0; // the template's image size (read without the server lock)
     DevBuf<uint32_t> image;         // device image the remap writes for CPU outputs
     uint32_t* staging = nullptr;    // pinned copy of image for CPU outputs (made on first use)
     size_t bytes = 0;
@@ -79,6 +86,7 @@ struct Slot {
     cudaEvent_t done = nullptr;
     std::vector<Request*> reqs;
     bool busy = false;
+    bool latency = false;           // renders only latency-class requests, at the highest priority
 };
 
 } // namespace
@@ -153,6 +161,8 @@ Instance* makeInstance(hvvr_server* s, uint32_t t) {
     cam->hidden = true;
     inst->cam = cam;
     inst->tmpl = t;
+    inst->width = tp.width;
+    inst->height = tp.height;
     if (inst->image.alloc(size_t(tp.width) * tp.height) != HVVR_OK) {
         hvvr_camera_destroy(cam->rc, cam);
         return nullptr;
@@ -187,6 +197,7 @@ void complete(hvvr_server* s, Request* r, int status) {
     c.dispatch_ms = r->dispatchMs;
     c.done_ms = r->doneMs;
     c.batch_views = r->batchViews;
+    c.priority = r->r.priority;
     std::lock_guard<std::mutex> lock(s->mu);
     s->completions.push_back(c);
     if (status == HVVR_OK) s->stats.completed++;
@@ -205,10 +216,13 @@ void finishSlot(hvvr_server* s, Slot& sl) {
     }
     for (Request* r : sl.reqs) {
         Instance* in = r->inst;
-        const Template& tp = s->templates[in->tmpl];
         if (st == HVVR_OK && r->r.memory_type == HVVR_MEMORY_CPU)
-            memcpy(r->r.output, in->staging, size_t(tp.width) * tp.height * 4);
-        s->templates[in->tmpl].freeList.push_back(in);
+            memcpy(r->r.output, in->staging, size_t(in->width) * in->height * 4);
+        {
+            // the template table may grow on other threads (hvvr_server_add_view)
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->templates[in->tmpl].freeList.push_back(in);
+        }
         complete(s, r, st);
     }
     sl.reqs.clear();
@@ -233,13 +247,27 @@ int applyUpdates(hvvr_server* s, std::vector<std::unique_ptr<Update>>& ups) {
     return HVVR_OK;
 }
 
-// forms and launches one batch on slot sl from the pending requests; false if none admitted
+// whether slot sl may render request r: a latency slot takes the latency class only; a throughput
+// slot takes the throughput class, and the latency class too when the server has no latency slots
+bool slotTakes(const hvvr_server* s, const Slot& sl, const Request* r) {
+    const bool urgent = r->r.priority != 0;
+    if (sl.latency) return urgent;
+    return !urgent || s->cfg.latency_slots == 0;
+}
+
+// forms and launches one batch on slot sl from the pending requests (latency class first, then in
+// arrival order); false if none admitted
 bool dispatch(hvvr_server* s, Slot& sl) {
     std::vector<Request*> take;
     {
         std::lock_guard<std::mutex> lock(s->mu);
+        std::stable_partition(s->pending.begin(), s->pending.end(), [](const Request* r) { return r->r.priority != 0; });
         for (auto it = s->pending.begin(); it != s->pending.end() && take.size() < s->cfg.max_batch_views;) {
             Request* r = *it;
+            if (!slotTakes(s, sl, r)) {
+                ++it;
+                continue;
+            }
             Instance* in = takeInstance(s, r->r.view);
             if (!in) {
                 ++it;
@@ -256,9 +284,13 @@ bool dispatch(hvvr_server* s, Slot& sl) {
     hvvr_batch* b = sl.batch.get();
     // frame buffers sized once for the largest batch the templates allow, so that no batch
     // reallocates (a free synchronises the device behind the other slots)
-    if (s->reservedFor != s->templates.size()) {
-        size_t maxTiles = 0;
+    size_t tmplCount = 0, maxTiles = 0;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        tmplCount = s->templates.size();
         for (const Template& t : s->templates) maxTiles = std::max<size_t>(maxTiles, t.proto->dev.tiles);
+    }
+    if (s->reservedFor != tmplCount) {
         const size_t tiles = maxTiles * s->cfg.max_batch_views;
         for (Slot& o : s->slots)
             if (!o.busy || &o == &sl) {
@@ -267,14 +299,14 @@ bool dispatch(hvvr_server* s, Slot& sl) {
             }
         bool all = true;
         for (Slot& o : s->slots) all = all && o.batch->order.n >= tiles;
-        if (all) s->reservedFor = s->templates.size();
+        if (all) s->reservedFor = tmplCount;
     }
     b->cams.clear();
     const double now = s->nowMs();
     for (Request* r : take) {
         Instance* in = r->inst;
         hvvr_camera* c = in->cam;
-        const Template& tp = s->templates[in->tmpl];
+        const Instance& tp = *in; // width and height of the template
         if (r->r.memory_type == HVVR_MEMORY_CPU && !in->staging &&
             cudaMallocHost((void**)&in->staging, size_t(tp.width) * tp.height * 4) != cudaSuccess) {
             cudaGetLastError();
@@ -305,7 +337,7 @@ bool dispatch(hvvr_server* s, Slot& sl) {
     if (rc == HVVR_OK) {
         for (Request* r : take) {
             if (r->r.memory_type != HVVR_MEMORY_CPU) continue;
-            const Template& tp = s->templates[r->inst->tmpl];
+            const Instance& tp = *r->inst;
             if (!r->inst->staging) {
                 rc = fail(HVVR_ERR_OOM, "pinned staging allocation failed");
                 break;
@@ -319,7 +351,10 @@ bool dispatch(hvvr_server* s, Slot& sl) {
     if (rc != HVVR_OK) {
         cudaStreamSynchronize(sl.stream);
         for (Request* r : take) {
-            s->templates[r->inst->tmpl].freeList.push_back(r->inst);
+            {
+                std::lock_guard<std::mutex> lock(s->mu);
+                s->templates[r->inst->tmpl].freeList.push_back(r->inst);
+            }
             complete(s, r, rc);
         }
         return true;
@@ -362,17 +397,30 @@ void workerLoop(hvvr_server* s) {
                 progress = true;
             }
         } else {
+            // latency slots first: a latency-class request goes out as soon as one is free
             for (Slot& sl : s->slots) {
-                if (sl.busy) continue;
+                if (sl.busy || !sl.latency) continue;
+                if (dispatch(s, sl)) progress = true;
+                else break;
+            }
+            for (Slot& sl : s->slots) {
+                if (sl.busy || sl.latency) continue;
                 // an idle GPU takes any request; with a batch in flight, gather a fuller batch
                 // unless the oldest request has waited max_wait_ms
                 bool busyNow = false;
-                for (const Slot& o : s->slots) busyNow = busyNow || o.busy;
+                for (const Slot& o : s->slots) busyNow = busyNow || (o.busy && !o.latency);
                 if (busyNow) {
                     std::lock_guard<std::mutex> lock(s->mu);
-                    if (s->pending.empty()) break;
-                    const double waited = s->nowMs() - s->pending.front()->submitMs;
-                    if (s->pending.size() < s->cfg.min_batch_views && waited < s->cfg.max_wait_ms) break;
+                    size_t eligible = 0;
+                    double oldest = -1.0;
+                    for (const Request* r : s->pending)
+                        if (slotTakes(s, sl, r)) {
+                            if (oldest < 0.0) oldest = r->submitMs;
+                            eligible++;
+                        }
+                    if (!eligible) break;
+                    const double waited = s->nowMs() - oldest;
+                    if (eligible < s->cfg.min_batch_views && waited < s->cfg.max_wait_ms) break;
                 }
                 if (dispatch(s, sl)) progress = true;
                 else break;
@@ -405,6 +453,8 @@ void hvvr_server_config_default(hvvr_server_config* cfg) {
     cfg->heavy_divisor = 8;
     cfg->min_batch_views = 8;
     cfg->max_wait_ms = 2.0f;
+    cfg->latency_slots = 1;
+    cfg->tile_cull_ctas_per_sm = 0;
 }
 
 int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr_server_config* cfg,
@@ -416,6 +466,7 @@ int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr
     hvvr_server_config_default(&s->cfg);
     if (cfg) s->cfg = *cfg;
     if (s->cfg.slots < 1 || s->cfg.slots > 8) return fail(HVVR_ERR_INVALID, "slots must be 1..8");
+    if (s->cfg.latency_slots > 4) return fail(HVVR_ERR_INVALID, "latency_slots must be 0..4");
     if (s->cfg.max_batch_views < 1) return fail(HVVR_ERR_INVALID, "max_batch_views must be >= 1");
     for (uint32_t i = 0; i < count; i++) {
         hvvr_raycaster* rc = scenes[i];
@@ -446,19 +497,29 @@ int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr
     bc.heavy_divisor = s->cfg.heavy_divisor;
     bc.tri_index_capacity = s->cfg.slot_list_capacity;
     TRY(checkConfig(bc));
-    s->slots.resize(s->cfg.slots);
-    for (Slot& sl : s->slots) {
+    int leastPriority = 0, greatestPriority = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+    const uint32_t slotCount = s->cfg.slots + s->cfg.latency_slots;
+    s->slots.resize(slotCount);
+    for (uint32_t i = 0; i < slotCount; i++) {
+        Slot& sl = s->slots[i];
+        sl.latency = i >= s->cfg.slots;
         sl.batch = std::make_unique<hvvr_batch>();
         sl.batch->cfg = bc;
+        // throughput slots leave SMs free for latency-class launches when asked to
+        if (!sl.latency) sl.batch->cfg.tile_cull_ctas_per_sm = s->cfg.tile_cull_ctas_per_sm;
         sl.batch->fixedViews = true;
         sl.batch->internal = true;
         sl.batch->rcs = s->scenes;
-        CUDA_TRY(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+        // with latency slots, their launches go ahead of the throughput slots' pending CTAs
+        sl.batch->streamPriorities = s->cfg.latency_slots == 0 ? 0 : (sl.latency ? 1 : 2);
+        const int prio = s->cfg.latency_slots == 0 ? leastPriority : (sl.latency ? greatestPriority : leastPriority);
+        CUDA_TRY(cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio));
         CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
     }
     CUDA_TRY(cudaStreamCreateWithFlags(&s->updateStream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&s->updateEv, cudaEventDisableTiming));
-    s->poolBytes = size_t(s->cfg.slots) * size_t(bc.tri_index_capacity) * 4 * (kChunk + 1) / kChunk;
+    s->poolBytes = size_t(slotCount) * size_t(bc.tri_index_capacity) * 4 * (kChunk + 1) / kChunk;
     if (s->poolBytes > s->cfg.hbm_budget_bytes)
         return fail(HVVR_ERR_INVALID, "the slots' triangle-list pools alone exceed the HBM budget");
     s->memUsed = s->poolBytes;
@@ -554,6 +615,7 @@ int hvvr_server_submit(hvvr_server* s, const hvvr_request* req, uint64_t* id) {
     if (!req->output) return fail(HVVR_ERR_INVALID, "NULL output");
     if (req->msaa != 1 && req->msaa != 2 && req->msaa != 4 && req->msaa != 8 && req->msaa != 16 && req->msaa != 32)
         return fail(HVVR_ERR_INVALID, "MSAA rate must be 1, 2, 4, 8, 16 or 32");
+    if (req->priority > 1) return fail(HVVR_ERR_INVALID, "priority must be 0 (throughput) or 1 (latency)");
     std::lock_guard<std::mutex> lock(s->mu);
     if (req->view >= s->templates.size()) return fail(HVVR_ERR_INVALID, "unknown view %u", req->view);
     if (s->templates[req->view].instBytes + s->poolBytes > s->cfg.hbm_budget_bytes)

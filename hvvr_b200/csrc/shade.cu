@@ -13,11 +13,16 @@
 // TestTriangleFrustaUVW; libraries/hvvr/raycaster/prim_tests.h:18-164); survivors are compacted
 // into shared memory in list order with warp ballots, and every thread then tests its
 // sample's N subsamples against them in that order, so depth ties resolve as in the reference.
+#include <algorithm>
+
 #include "dev_common.cuh"
 
 namespace hvb {
 
 __constant__ float2 cMsaa[6][32]; // unit offsets for rates 1,2,4,8,16,32
+// the same offsets split by axis, so that subsamples 2k and 2k+1 read as one 64-bit pair
+__constant__ __align__(8) float cMsaaX[6][32];
+__constant__ __align__(8) float cMsaaY[6][32];
 
 namespace {
 
@@ -97,6 +102,83 @@ __device__ __forceinline__ bool threadTest(const TriThread& th, float t, float a
     if (test < 0) return false;
     depth = t * (1.0f / denom);
     return true;
+}
+
+// Packed FP32 (sm_100 f32x2): two floats in one 64-bit register pair, each lane an ordinary IEEE
+// single-precision operation (round to nearest, flush to zero like every other operation here), so
+// a packed result equals the two scalar results bit for bit.
+typedef unsigned long long P2;
+__device__ __forceinline__ P2 pk(float lo, float hi) {
+    P2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(P2 v, float& lo, float& hi) { asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v)); }
+__device__ __forceinline__ P2 fma2(P2 a, P2 b, P2 c) {
+    P2 r;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ P2 mul2(P2 a, P2 b) {
+    P2 r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ P2 add2(P2 a, P2 b) {
+    P2 r;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ P2 sub2(P2 a, P2 b) {
+    P2 r;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// a triangle's per-thread setup with every value duplicated into both lanes of a pair
+struct TriThread2 {
+    P2 dc, vc, wc, ddx, ddy, dvx, dvy, dwx, dwy, t;
+};
+__device__ __forceinline__ TriThread2 pairSetup(const TriThread& th, float t) {
+    return TriThread2{pk(th.dc, th.dc),   pk(th.vc, th.vc),   pk(th.wc, th.wc),   pk(th.ddx, th.ddx),
+                      pk(th.ddy, th.ddy), pk(th.dvx, th.dvx), pk(th.dvy, th.dvy), pk(th.dwx, th.dwx),
+                      pk(th.dwy, th.dwy), pk(t, t)};
+}
+
+// threadTest for subsamples 2k and 2k+1 at once (ax, ay: their unit offsets as pairs), with the
+// scalar test's operations in its order: denom, depthDelta, v, w as FMA chains (FMA) or as rounded
+// products and sums (STRICT), u = (denom - v) - w, the sign-bit test and the depth update.
+template <bool FMA>
+__device__ __forceinline__ void threadTest2(const TriThread2& p, float t, P2 ax, P2 ay, float& depth0, float& depth1,
+                                            uint32_t& hit0, uint32_t& hit1, uint32_t idx) {
+    const P2 depth = pk(depth0, depth1);
+    P2 denom, dd, v, w;
+    if (FMA) {
+        denom = fma2(p.ddy, ay, fma2(p.ddx, ax, p.dc));
+        dd = fma2(depth, denom, p.t); // p.t holds -t in FMA mode
+        v = fma2(p.dvy, ay, fma2(p.dvx, ax, p.vc));
+        w = fma2(p.dwy, ay, fma2(p.dwx, ax, p.wc));
+    } else {
+        denom = add2(add2(p.dc, mul2(p.ddx, ax)), mul2(p.ddy, ay));
+        dd = sub2(mul2(depth, denom), p.t);
+        v = add2(add2(p.vc, mul2(p.dvx, ax)), mul2(p.dvy, ay));
+        w = add2(add2(p.wc, mul2(p.dwx, ax)), mul2(p.dwy, ay));
+    }
+    const P2 u = sub2(sub2(denom, v), w);
+    float den0, den1, dd0, dd1, u0, u1, v0, v1, w0, w1;
+    upk(denom, den0, den1);
+    upk(dd, dd0, dd1);
+    upk(u, u0, u1);
+    upk(v, v0, v1);
+    upk(w, w0, w1);
+    if ((__float_as_int(dd0) | __float_as_int(u0) | __float_as_int(v0) | __float_as_int(w0)) >= 0) {
+        depth0 = t * (1.0f / den0);
+        hit0 = idx;
+    }
+    if ((__float_as_int(dd1) | __float_as_int(u1) | __float_as_int(v1) | __float_as_int(w1)) >= 0) {
+        depth1 = t * (1.0f / den1);
+        hit1 = idx;
+    }
 }
 
 // IntersectTriangleThread::calcUVW (prim_tests.h:233-245)
@@ -369,18 +451,45 @@ struct ShadeSmem {
 // the 16xMSAA foveated frame than 4 CTAs at 107 registers without spills)
 template <uint32_t N> struct MinCtas { static constexpr int v = N <= 8 ? 7 : (N == 16 ? 5 : 4); };
 
+// Where a shade launch takes its tiles from; item i of the launch is
+//   kFromOrder: order[first + i] (order == nullptr: first + i), i < count;
+//   kFromReady: the tile published in ready[first + i] by the concurrent tile cull, waited for;
+//   kFromList:  list[first + i], for i < *listCount (the retry list, counted on the device).
+struct ShadeSource {
+    const uint32_t* order;
+    const uint32_t* ready;
+    const uint32_t* list;
+    const uint32_t* listCount;
+    uint32_t first, count;
+};
+
+// Waits (one thread) until the tile cull publishes a ready slot. A wait that runs past about a
+// second gives up: it sets kStatusPipelineTimeout and returns kReadyEmpty, whose kReadyRetry bit
+// makes the caller skip the slot.
+__device__ uint32_t waitReady(const uint32_t* slot, uint32_t* counters) {
+    for (uint32_t i = 0;; i++) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(slot) : "memory");
+        if (v != kReadyEmpty) return v;
+        if (i >= (1u << 20)) {
+            atomicOr(&counters[1], kStatusPipelineTimeout);
+            return kReadyEmpty;
+        }
+        __nanosleep(i < 32 ? 128 : 1024);
+    }
+}
+
+// One tile: intersect, G-buffer grouping, shading and resolve of its 128 samples. The tile's
+// list (TileList, chunk links, pool entries) is read through L2 (ld.cg): in a pipelined launch
+// another SM wrote it while this launch was running.
 template <uint32_t N, bool FMA>
-__global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel(FrameDev fr, const uint32_t* __restrict__ order,
-                                                                  uint32_t first) {
-    __shared__ ShadeSmem sm;
-    __shared__ LightEnvDev env;
-    __shared__ Mat4 M;
-    const uint32_t gt = order ? order[first + blockIdx.x] : first + blockIdx.x;
+__device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, ShadeSmem& sm, LightEnvDev& env, Mat4& M) {
     const ViewDev& V = fr.views[fr.viewCount == 1 ? 0u : __ldg(fr.blockView + gt / kTilesPerBlock)];
     const uint32_t tile = gt - V.tileStart;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sid = tile * kTileSize + tid;
-    const TileList L = V.tileLists[tile];
+    const uint2 lw = __ldcg(reinterpret_cast<const uint2*>(V.tileLists + tile));
+    const TileList L{lw.x, lw.y};
     if (L.count == 0) {
         // ClearEmptyKernel (resolve.cu:527-542)
         V.colors[sid] = 0xFF000000u;
@@ -445,16 +554,16 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
 
     uint32_t chunk = L.first;
     uint32_t remaining = L.count;
-    uint32_t survivors = 0;
+    uint32_t survivors = 0, tested = 0;
     while (remaining > 0 && chunk < fr.poolChunks) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
-        const uint32_t nextChunk = fr.chunkNext[chunk];
+        const uint32_t nextChunk = __ldcg(fr.chunkNext + chunk);
         bool keep = false;
         uint32_t idx = 0;
         float t = 0.0f, nlen = 0.0f;
         F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0), nrm = f3(0, 0, 0);
         if (tid < n) {
-            idx = fr.pool[size_t(chunk) * kChunk + tid];
+            idx = __ldcg(fr.pool + size_t(chunk) * kChunk + tid);
             const TriGeom tri = loadTri(viewPtr(V.tris), idx);
             // FrustumPlanes::test
             bool in = true;
@@ -515,6 +624,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         for (uint32_t j = 0; j < total; j++) {
             const float4 a0 = sm.te0[j], a1 = sm.te1[j];
             if (__all_sync(kFull, a0.w > laneBound * a1.w)) continue;
+            ++tested;
             const float4 a2 = sm.tvr[j], a3 = sm.tn[j];
             const F3 je0 = f3(a0.x, a0.y, a0.z);
             const F3 je1 = f3(a1.x, a1.y, a1.z);
@@ -522,10 +632,18 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
             const float jt = a0.w;
             const uint32_t jidx = __float_as_uint(a2.w);
             const TriThread th = threadSetupN(f3(a3.x, a3.y, a3.z), je0, je1, jvr, c, du, dv);
+            if (N == 1) {
+                const float2 a = cMsaa[rate][0];
+                if (threadTest<FMA>(th, jt, a.x, a.y, tmax[0])) hit[0] = jidx;
+            } else {
+                // subsamples in pairs on the packed FP32 path
+                const TriThread2 p = pairSetup(th, FMA ? -jt : jt);
 #pragma unroll
-            for (uint32_t i = 0; i < N; i++) {
-                const float2 a = cMsaa[rate][i];
-                if (threadTest<FMA>(th, jt, a.x, a.y, tmax[i])) hit[i] = jidx;
+                for (uint32_t i = 0; i + 1 < N; i += 2) {
+                    const P2 ax = *reinterpret_cast<const P2*>(&cMsaaX[rate][i]);
+                    const P2 ay = *reinterpret_cast<const P2*>(&cMsaaY[rate][i]);
+                    threadTest2<FMA>(p, jt, ax, ay, tmax[i], tmax[i + 1], hit[i], hit[i + 1], jidx);
+                }
             }
         }
         __syncthreads();
@@ -534,6 +652,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
     }
 
     if (tid == 0 && survivors) atomicAdd(&fr.counters[kSurvivorWord], survivors);
+    if (lane == 0 && tested) atomicAdd(&fr.counters[kTestedWord], tested);
     if (uint32_t* hitOut = viewPtr(V.hitIds)) {
         float* depthOut = viewPtr(V.depth);
 #pragma unroll
@@ -612,6 +731,34 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
     }
     const float sN = 1.0f / float(N);
     viewPtr(V.colors)[sid] = packColor(f3(aces(rx * sN), aces(ry * sN), aces(rz * sN)));
+}
+
+// SRC selects where the launch's tiles come from (ShadeSource): kFromOrder and kFromReady run one
+// tile per CTA; kFromList walks the list with a grid-stride loop.
+enum : int { kFromOrder = 0, kFromReady = 1, kFromList = 2 };
+
+template <uint32_t N, bool FMA, int SRC>
+__global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel(FrameDev fr, ShadeSource src) {
+    __shared__ ShadeSmem sm;
+    __shared__ LightEnvDev env;
+    __shared__ Mat4 M;
+    if constexpr (SRC == kFromOrder) {
+        const uint32_t gt = src.order ? src.order[src.first + blockIdx.x] : src.first + blockIdx.x;
+        shadeTile<N, FMA>(fr, gt, sm, env, M);
+    } else if constexpr (SRC == kFromReady) {
+        __shared__ uint32_t readyTile;
+        if (threadIdx.x == 0) readyTile = waitReady(src.ready + src.first + blockIdx.x, fr.counters);
+        __syncthreads();
+        const uint32_t gt = readyTile;
+        if (gt & kReadyRetry) return; // culled and shaded by the retry passes (or the wait gave up)
+        shadeTile<N, FMA>(fr, gt, sm, env, M);
+    } else {
+        const uint32_t count = *src.listCount;
+        for (uint32_t item = blockIdx.x; item < count; item += gridDim.x) {
+            shadeTile<N, FMA>(fr, src.list[src.first + item], sm, env, M);
+            __syncthreads();
+        }
+    }
 }
 
 // ------------------------------------------------------------------ thin lens (depth of field)
@@ -919,10 +1066,49 @@ cudaError_t launchRate(const FrameDev& fr, bool fpStrict, bool dof, const uint32
         if (fpStrict) intersectShadeDofKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
         else intersectShadeDofKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
     } else {
-        if (fpStrict) intersectShadeKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
-        else intersectShadeKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
+        const ShadeSource src{order, nullptr, nullptr, nullptr, first, count};
+        if (fpStrict) intersectShadeKernel<N, false, kFromOrder><<<count, kTileSize, 0, st>>>(fr, src);
+        else intersectShadeKernel<N, true, kFromOrder><<<count, kTileSize, 0, st>>>(fr, src);
     }
     return cudaGetLastError();
+}
+
+// The cull -> shade pipeline of one rate class (launchCullShadePipeline).
+template <uint32_t N, bool FMA>
+cudaError_t launchPipelineRate(const FrameDev& fr, uint32_t first, uint32_t count, uint32_t* queues, uint32_t* pipe,
+                               uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
+    cudaError_t e = launchTileCullMain(fr, fr.order, first, count, queues, warps, stackLimit, fr.ready, pipe, st);
+    if (e != cudaSuccess) return e;
+    // CTA i shades the i-th tile the cull finishes; the launch may start once every cull CTA runs
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(count);
+    cfg.blockDim = dim3(kTileSize);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const ShadeSource ready{nullptr, fr.ready, nullptr, nullptr, first, count};
+    if ((e = cudaLaunchKernelEx(&cfg, intersectShadeKernel<N, FMA, kFromReady>, fr, ready)) != cudaSuccess) return e;
+    // tiles whose stack outgrew the main pass: culled again, then shaded by a small grid that walks
+    // the retry list (its length is only known on the device)
+    if ((e = launchTileCullRetryPass(fr, fr.order, first, count, queues, st)) != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t grid = std::min<uint32_t>(count, uint32_t(2 * (sms > 0 ? sms : 148)));
+    const ShadeSource retried{nullptr, nullptr, fr.retry, queues + 1, first, count};
+    intersectShadeKernel<N, FMA, kFromList><<<grid, kTileSize, 0, st>>>(fr, retried);
+    return cudaGetLastError();
+}
+
+template <uint32_t N>
+cudaError_t launchPipelineFp(const FrameDev& fr, bool fpStrict, uint32_t first, uint32_t count, uint32_t* queues,
+                             uint32_t* pipe, uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
+    return fpStrict ? launchPipelineRate<N, false>(fr, first, count, queues, pipe, warps, stackLimit, st)
+                    : launchPipelineRate<N, true>(fr, first, count, queues, pipe, warps, stackLimit, st);
 }
 
 // RemapKernel (libraries/hvvr/raycaster/remap.cu:35-77) for split-colour 1, 2 (pentile) and 3
@@ -964,6 +1150,22 @@ cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStric
     }
 }
 
+cudaError_t launchCullShadePipeline(const FrameDev& fr, uint32_t msaa, bool fpStrict, uint32_t first, uint32_t count,
+                                    uint32_t* queues, uint32_t* pipe, uint32_t warps, uint32_t stackLimit,
+                                    cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    if (!fr.ready) return cudaErrorInvalidValue;
+    switch (msaa) {
+    case 1: return launchPipelineFp<1>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 2: return launchPipelineFp<2>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 4: return launchPipelineFp<4>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 8: return launchPipelineFp<8>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 16: return launchPipelineFp<16>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 32: return launchPipelineFp<32>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st) {
     if (!c.image || !c.remap || c.width == 0 || c.height == 0) return cudaSuccess;
     const dim3 block(16, 8);
@@ -983,8 +1185,19 @@ cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st) {
     case 32: idx = 5; break;
     default: return cudaErrorInvalidValue;
     }
-    return cudaMemcpyToSymbolAsync(cMsaa, offsets, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
-                                   cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpyToSymbolAsync(cMsaa, offsets, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
+                                            cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    // the per-axis copies (pageable host staging: the copy completes before the call returns)
+    float xs[32], ys[32];
+    for (uint32_t i = 0; i < n; i++) {
+        xs[i] = offsets[2 * i];
+        ys[i] = offsets[2 * i + 1];
+    }
+    e = cudaMemcpyToSymbolAsync(cMsaaX, xs, n * sizeof(float), size_t(idx) * 32 * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbolAsync(cMsaaY, ys, n * sizeof(float), size_t(idx) * 32 * sizeof(float), cudaMemcpyHostToDevice,
+                                   st);
 }
 
 } // namespace hvb

@@ -19,12 +19,17 @@
 //
 // In host code gScratch names a host-side shadow, not device memory, so its device address
 // is looked up with cudaGetSymbolAddress once per device, on the first call made with that
-// device current. Make that first call on each device before any stream capture starts.
+// device current. Make that first call on each device before any stream capture starts. The
+// address is cached for the life of the process: a cudaDeviceReset (which also ends every other
+// object of the library on that device) leaves the cache stale, so do not reset a device that the
+// library is using. Every call is synchronous: it checks the caller's inputs and reads the status
+// back, waiting for the stream each time.
 //
 // The cull itself is the tileCullKernel of the render path (traverse.cu), given a one-view
 // table written into the scratch by a one-thread kernel and pointed at the scratch pool;
 // a one-block scan and a per-tile gather then copy the chunked lists into the caller's
 // flat output in tile order. Nothing here calls cudaMalloc, cudaFree or an allocating library.
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -119,6 +124,35 @@ __global__ void gatherLists(const uint32_t* __restrict__ scratch, uint32_t tiles
     }
 }
 
+// The cull trusts its inputs (the render path builds them itself); this entry point takes them
+// from the caller, so they are checked first, one thread per node and per block: every internal
+// child of a node must lie after it and inside the node array (the depth-first layout the render
+// path checks when it builds a scene), every block-stack size must be at most kBlockStack, and every
+// block-stack entry must name a node inside the array. Any violation sets kStatusBadInput.
+__global__ void checkInputs(const Node* __restrict__ nodes, uint32_t nodeCount, const StackEntry* __restrict__ stacks,
+                            const uint32_t* __restrict__ sizes, uint32_t blocks, uint32_t* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    if (i < nodeCount) {
+        const uint32_t leafMask = nodes[i].leafMask;
+        for (uint32_t k = 0; k < 4; k++) {
+            if ((leafMask >> k) & 1u) continue;
+            const uint64_t c = uint64_t(i) + nodes[i].tri[k + 1];
+            if (c <= i || c >= nodeCount) bad = true;
+        }
+    }
+    if (i < blocks) {
+        const uint32_t n = sizes[i];
+        if (n > kBlockStack) {
+            bad = true;
+        } else {
+            for (uint32_t j = 0; j < n; j++)
+                if (stacks[size_t(i) * kBlockStack + j].node >= nodeCount) bad = true;
+        }
+    }
+    if (bad) atomicOr(status, kStatusBadInput);
+}
+
 std::mutex gSetupMutex;
 uint32_t* gScratchAddr[64] = {};
 
@@ -178,6 +212,19 @@ extern "C" int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* 
     fr.retry = scratch + kOffRetry;
     if ((e = cudaMemsetAsync(scratch + kOffCounters, 0, 8 * sizeof(uint32_t), st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "clearing the scratch counters failed", e);
+    {
+        const uint32_t n = std::max(args->node_count, fr.blocks);
+        checkInputs<<<(n + 255) / 256, 256, 0, st>>>(v.nodes, args->node_count, v.blockStacks, v.blockSizes, fr.blocks,
+                                                     scratch + kOffCounters + 1);
+        uint32_t bad = 0;
+        if ((e = cudaGetLastError()) != cudaSuccess) return failStatic(HVVR_ERR_CUDA, "input check launch failed", e);
+        if ((e = cudaMemcpyAsync(&bad, scratch + kOffCounters + 1, sizeof(bad), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return failStatic(HVVR_ERR_CUDA, "input check failed", e);
+        if (bad & kStatusBadInput)
+            return failStatic(HVVR_ERR_INVALID, "malformed input: a block-stack size above 64, or a node index or child "
+                                                "offset outside node_count");
+    }
     if ((e = launchWriteView(v, reinterpret_cast<ViewDev*>(scratch + kOffView), st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "view setup launch failed", e);
     if ((e = launchTileCull(fr, nullptr, 0, tiles, scratch + kOffCounters + 4, 4, 0, st)) != cudaSuccess)

@@ -17,6 +17,7 @@
 // test is exactly the reference's lane arithmetic (explicit fmaf where it uses
 // _mm256_fmadd_ps, IEEE single ops elsewhere) and the stacks evolve identically.
 #include <algorithm>
+#include <mutex>
 
 #include "dev_common.cuh"
 
@@ -507,6 +508,8 @@ struct TileCullArgs {
     uint32_t* retryCount;  // number of such tiles, zero at launch
     uint32_t* retryQueue;  // work-queue head of the retry pass, zero at launch
     uint32_t stackLimit;   // entries the main pass may use (<= kTileStack)
+    uint32_t* ready;       // pipelined: ready slots, slot first + i for the i-th finished tile (else nullptr)
+    uint32_t* readyTail;   // pipelined: finished tiles so far, zero at launch
 };
 
 // traverseTiles for one tile of view V (tile = view-local index); returns the node visits.
@@ -683,11 +686,17 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
 
 // Persistent warps pull tiles from a queue (longest-first when an order is given), so a
 // few long horizon tiles overlap with the rest instead of holding a CTA slot each.
+// (W = 1: one warp per CTA, so a warp that runs out of tiles frees its registers at once; the
+// bound asks for the 20 resident warps per SM that the wider CTAs reach)
 template <int W>
-__global__ void __launch_bounds__(W * 32) tileCullKernel(TileCullArgs a) {
+__global__ void __launch_bounds__(W * 32, W == 1 ? 20 : 1) tileCullKernel(TileCullArgs a) {
     __shared__ TileSmemT<kTileStack> smem[W];
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     TileSmemT<kTileStack>& s = smem[warp];
+    // A launch that follows this one with programmatic serialization (the pipelined shade) may be
+    // scheduled once every CTA of this grid has started: its CTAs wait for tiles that only this
+    // grid's warps publish, so they must never keep a cull CTA from becoming resident.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     for (;;) {
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(a.queue, 1u);
@@ -702,6 +711,17 @@ __global__ void __launch_bounds__(W * 32) tileCullKernel(TileCullArgs a) {
         if (lane == 0) {
             V.tileCost[tile] = visits;
             if (overflow) a.retry[a.first + atomicAdd(a.retryCount, 1u)] = gt;
+        }
+        if (a.ready) {
+            // publish: every lane's list writes (pool chunks, links, the tile's TileList) are made
+            // visible device-wide before lane 0 releases the slot
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) {
+                const uint32_t pos = atomicAdd(a.readyTail, 1u);
+                const uint32_t val = gt | (overflow ? kReadyRetry : 0u);
+                asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.ready + a.first + pos), "r"(val) : "memory");
+            }
         }
         __syncwarp();
     }
@@ -794,32 +814,42 @@ __global__ void __launch_bounds__(1024) occupiedRankKernel(FrameDev fr) {
 
 struct DeviceLimits {
     int sms = 0;
-    int ctasPerSm[9] = {};
+    int ctasPerSm[9] = {};  // indexed by warps per CTA
     bool retryReady = false;
 };
+
+// per-device launch limits, filled on first use; host threads rendering on different streams
+// may get here together, so the first use of a device is serialised
+std::mutex gLimitsMutex;
 
 DeviceLimits& limits() {
     static DeviceLimits perDevice[64];
     int dev = 0;
     cudaGetDevice(&dev);
     DeviceLimits& d = perDevice[dev < 0 || dev >= 64 ? 0 : dev];
+    std::lock_guard<std::mutex> lock(gLimitsMutex);
     if (!d.sms) {
-        cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
-        if (d.sms < 1) d.sms = 1;
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        d.sms = sms < 1 ? 1 : sms;
     }
     return d;
 }
 
 template <int W>
-cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, cudaStream_t st) {
+cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, uint32_t capPerSm, cudaStream_t st) {
     DeviceLimits& d = limits();
-    if (!d.ctasPerSm[W]) {
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tileCullKernel<W>, W * 32, 0);
-        d.ctasPerSm[W] = occ < 1 ? 1 : occ;
+    {
+        std::lock_guard<std::mutex> lock(gLimitsMutex);
+        if (!d.ctasPerSm[W]) {
+            int occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tileCullKernel<W>, W * 32, 0);
+            d.ctasPerSm[W] = occ < 1 ? 1 : occ;
+        }
     }
     const uint32_t needed = (count + W - 1) / W;
-    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(d.sms * d.ctasPerSm[W]));
+    const uint32_t perSm = capPerSm ? std::min<uint32_t>(capPerSm, uint32_t(d.ctasPerSm[W])) : uint32_t(d.ctasPerSm[W]);
+    const uint32_t grid = std::min<uint32_t>(needed, uint32_t(d.sms) * perSm);
     tileCullKernel<W><<<grid, W * 32, 0, st>>>(a);
     return cudaGetLastError();
 }
@@ -829,11 +859,14 @@ cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, cudaStream_t 
 cudaError_t launchTileCullRetry(const TileCullArgs& a, cudaStream_t st) {
     DeviceLimits& d = limits();
     const size_t smem = sizeof(TileSmemT<kRetryStack>);
-    if (!d.retryReady) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(tileCullRetryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) return e;
-        d.retryReady = true;
+    {
+        std::lock_guard<std::mutex> lock(gLimitsMutex);
+        if (!d.retryReady) {
+            const cudaError_t e =
+                cudaFuncSetAttribute(tileCullRetryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (e != cudaSuccess) return e;
+            d.retryReady = true;
+        }
     }
     tileCullRetryKernel<<<d.sms, 32, smem, st>>>(a);
     return cudaGetLastError();
@@ -853,22 +886,36 @@ cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
-                           uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
+cudaError_t launchTileCullMain(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                               uint32_t* queues, uint32_t warps, uint32_t stackLimit, uint32_t* ready,
+                               uint32_t* readyTail, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     if (stackLimit == 0 || stackLimit > kTileStack) stackLimit = kTileStack;
     if (stackLimit < 8) return cudaErrorInvalidValue;
     const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
-                         order, first, count, queues, fr.retry, queues + 1, queues + 2, stackLimit};
-    cudaError_t e;
+                         order, first, count, queues, fr.retry, queues + 1, queues + 2, stackLimit, ready, readyTail};
     switch (warps) {
-    case 2: e = launchTileCullW<2>(a, count, st); break;
-    case 4: e = launchTileCullW<4>(a, count, st); break;
-    case 8: e = launchTileCullW<8>(a, count, st); break;
+    case 1: return launchTileCullW<1>(a, count, fr.cullCtasPerSm, st);
+    case 2: return launchTileCullW<2>(a, count, fr.cullCtasPerSm, st);
+    case 4: return launchTileCullW<4>(a, count, fr.cullCtasPerSm, st);
+    case 8: return launchTileCullW<8>(a, count, fr.cullCtasPerSm, st);
     default: return cudaErrorInvalidValue;
     }
-    if (e != cudaSuccess) return e;
+}
+
+cudaError_t launchTileCullRetryPass(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                                    uint32_t* queues, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
+                         order, first, count, queues, fr.retry, queues + 1, queues + 2, kTileStack, nullptr, nullptr};
     return launchTileCullRetry(a, st);
+}
+
+cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
+                           uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
+    const cudaError_t e = launchTileCullMain(fr, order, first, count, queues, warps, stackLimit, nullptr, nullptr, st);
+    if (e != cudaSuccess) return e;
+    return launchTileCullRetryPass(fr, order, first, count, queues, st);
 }
 
 cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st) {

@@ -146,7 +146,11 @@ typedef struct {
     uint64_t tri_index_capacity;  /* triangle-index pool shared by the raycaster's cameras, entries; 0 = default (128M as the reference) */
     int device;                   /* CUDA device ordinal */
     uint32_t sample_setup;        /* HVVR_SETUP_DEVICE (default) or HVVR_SETUP_HOST: where a camera's sample hierarchy is built */
+    uint32_t bvh_build;           /* for models created without topology: HVVR_BVH_HOST (default; GenerateTopology's
+                                     SAH build, the reference's triangle IDs) or HVVR_BVH_DEVICE
+                                     (hvvr_generate_topology_device) */
 } hvvr_spec;
+enum { HVVR_BVH_HOST = 0, HVVR_BVH_DEVICE = 1 };
 /* The sample hierarchy (SampleData: clustering, tile and block frusta, beams, image remap) is built
  * on the device when the samples' positions are distinct and not NaN and the spherical mapping is
  * off: the reference's clustering sorts are then order-unique and the result equals the host
@@ -335,6 +339,17 @@ int hvvr_scene_read_triangles(hvvr_raycaster* rc, float* tris9);
 int hvvr_generate_topology(hvvr_shading_vertex* verts, uint32_t vert_count, hvvr_tri_shade* tri_shade,
                            uint32_t tri_count, hvvr_topology_node* nodes_out, uint32_t nodes_capacity,
                            uint32_t* node_count);
+/* No counterpart in the reference (whose only build is GenerateTopology's host SAH build): a linear
+ * BVH built on the GPU in milliseconds - 30-bit Morton codes of the triangle centroids, a stable
+ * radix sort, the binary radix tree of the codes, leaves of at most 4 triangles, collapse to 4-wide
+ * nodes (leaf slots first) and the depth-first TopologyNode layout. A different topology from
+ * hvvr_generate_topology (more node visits and list entries per frame), the same rendered image up
+ * to ties between coincident triangles. Reorders tri_shade in place (vertices keep their order) and
+ * writes node_count nodes (capacity >= tri_count); host arrays in and out, the build runs on stream
+ * of the current device and the call returns when it is done. */
+int hvvr_generate_topology_device(const hvvr_shading_vertex* verts, uint32_t vert_count, hvvr_tri_shade* tri_shade,
+                                  uint32_t tri_count, hvvr_topology_node* nodes_out, uint32_t nodes_capacity,
+                                  uint32_t* node_count, void* stream);
 /* getGridSamples(width, height) (libraries/hvvr/raycaster/samples.cpp:21-42) */
 int hvvr_grid_samples(uint32_t width, uint32_t height, hvvr_sample* out);
 
@@ -391,7 +406,7 @@ int hvvr_polar_foveated_samples(const hvvr_spec* spec, float* beams9, uint32_t* 
  * that rendered it last. Destroy batches before their raycasters; a batch whose raycaster
  * was destroyed returns HVVR_ERR_STATE. */
 typedef struct {
-    uint32_t tile_cull_warps;     /* warps per CTA of the tile-cull work queue: 2, 4 or 8 */
+    uint32_t tile_cull_warps;     /* warps per CTA of the tile-cull work queue: 1, 2, 4 or 8 */
     uint32_t heavy_divisor;       /* 1/heavy_divisor of each rate's tiles (last frame's slowest) are
                                      culled and shaded on their own stream; 0 = no split */
     uint64_t tri_index_capacity;  /* triangle-list pool entries shared by all views */
@@ -402,6 +417,13 @@ typedef struct {
     uint32_t timing;              /* 1: record per-stage and per-launch events (the stage, kernel and
                                      part read-backs); they cost device time (about 0.4 ms of a 6 ms
                                      stereo frame). 0 (default): the frame's start and end only */
+    uint32_t pipeline;            /* 1 (default): each part of a pinhole rate class runs its tile cull
+                                     and its intersect/shade as one pipeline - a tile is shaded as soon
+                                     as its list is complete, while other tiles are still being culled.
+                                     0: the cull of a part finishes before its intersect/shade starts */
+    uint32_t tile_cull_ctas_per_sm; /* cap on the persistent tile cull's resident CTAs per SM (0 = as many
+                                     as fit): leaves room on every SM for other work (the intersect of
+                                     finished tiles, another batch's launches) */
 } hvvr_batch_config;
 void hvvr_batch_config_default(hvvr_batch_config* cfg);
 int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,
@@ -418,15 +440,17 @@ int hvvr_batch_synchronize(hvvr_batch* batch);
 int hvvr_batch_get_config(const hvvr_batch* batch, hvvr_batch_config* cfg);
 int hvvr_batch_set_config(hvvr_batch* batch, const hvvr_batch_config* cfg);
 /* Autotuner: renders `frames` timed frames (after one warm-up) for each tile_cull_warps in
- * {2,4,8} x heavy_divisor in {0,16,8,4}, keeps the fastest, then sizes the pool to 1.25x the
- * largest list total seen (at least 1M entries). Writes the chosen config to *out. */
+ * {1,2,4,8} x (pipeline 1 with the configured heavy_divisor, or pipeline 0 with heavy_divisor in
+ * {0,16,8,4}), keeps the fastest, then sizes the pool to 1.25x the largest list total seen (at
+ * least 1M entries). Writes the chosen config to *out. */
 int hvvr_batch_autotune(hvvr_batch* batch, uint32_t frames, hvvr_batch_config* out);
 /* device ms of the last frame: [0] total; [1] block cull, [2] first tile cull, [3] rest of
  * cull + intersect/shade, [4] remap + copies - stages are 0 unless config.timing is 1 */
 int hvvr_batch_read_timings(const hvvr_batch* batch, float* ms5);
 /* device ms of the last frame's launches, summed over the launches of the frame (launches on
  * different streams overlap, so the sum can exceed the frame time): [0] tile cull, [1]
- * intersect/shade, [2] block cull, [3] remap. Needs config.timing = 1 for that frame. */
+ * intersect/shade, [2] block cull, [3] remap. A pipelined class counts the span of its cull and
+ * shade as intersect/shade time. Needs config.timing = 1 for that frame. */
 int hvvr_batch_read_kernel_times(const hvvr_batch* batch, float* ms4);
 int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
 /* the configuration of the batch behind hvvr_raycaster_render (default: hvvr_batch_config_default
@@ -436,7 +460,9 @@ int hvvr_raycaster_set_batch_config(hvvr_raycaster* rc, const hvvr_batch_config*
 /* The last frame's launch timeline per part: rate class r (log2 MSAA, + 6 for thin-lens views)
  * runs as part 2r (its slowest tiles by the previous frame's cost, on a high-priority stream)
  * and part 2r+1 (the rest). ms72[3 * part + i] = tile cull start, tile cull end, intersect/shade
- * end, in ms from the frame start; -1 for parts that did not run. Needs config.timing = 1. */
+ * end, in ms from the frame start; -1 for parts that did not run. In a pipelined part
+ * (config.pipeline) the tile cull end reads -1 (the cull and the shade overlap).
+ * Needs config.timing = 1. */
 int hvvr_batch_read_part_times(const hvvr_batch* batch, float* ms72);
 int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72);
 /* counters of the last frame: [0] list-pool entries taken (whole chunks), [1] tiles culled
@@ -445,7 +471,10 @@ int hvvr_batch_read_stats(const hvvr_batch* batch, uint64_t* out4);
 /* The last frame's counters, out[0..count): [0] triangle-list pool entries used (whole chunks),
  * [1] tiles culled again with the 4096-entry stack, [2] status bits, [3] views, [4] list entries
  * that passed the intersect's per-tile tests (frustum planes, ray-origin side, corner-ray
- * barycentrics) and were tested against every sample of the tile; later indices read 0. */
+ * barycentrics), [5] (warp of 32 samples, passing entry) pairs whose subsample tests ran (the
+ * intersect skips a pair when a depth bound proves that no subsample of the warp can hit the
+ * triangle, so [5] x 32 samples x msaa is the number of subsample tests executed, at most
+ * [4] x 4 warps); later indices read 0. */
 int hvvr_batch_read_counters(const hvvr_batch* batch, uint64_t* out, uint32_t count);
 int hvvr_raycaster_read_counters(const hvvr_raycaster* rc, uint64_t* out, uint32_t count);
 
@@ -474,6 +503,11 @@ typedef struct {
     uint32_t min_batch_views;     /* with a batch in flight, wait for this many requests (default 8) ... */
     float max_wait_ms;            /* ... or until the oldest has waited this long (default 2 ms);
                                      an idle GPU takes any request at once */
+    uint32_t latency_slots;       /* slots (0..4, default 1) that render only latency-class requests
+                                     (hvvr_request.priority 1), at once and on the GPU's highest stream
+                                     priority; the `slots` throughput slots then run at its lowest */
+    uint32_t tile_cull_ctas_per_sm; /* as hvvr_batch_config, for the throughput slots (default 0; with
+                                     latency slots, a cap keeps SMs free for latency-class launches) */
 } hvvr_server_config;
 typedef struct {
     uint32_t view;                /* from hvvr_server_add_view */
@@ -482,12 +516,16 @@ typedef struct {
     uint32_t memory_type;         /* HVVR_MEMORY_CPU or HVVR_MEMORY_CUDA */
     void* output;                 /* width x height RGBA8 (sRGB) pixels, row stride = width */
     uint64_t tag;                 /* returned with the completion */
+    uint32_t priority;            /* 0: throughput class (batched); 1: latency class (e.g. the eyes of a
+                                     stereo frame): dispatched ahead of the throughput class on a
+                                     latency slot, never held back to fill a batch */
 } hvvr_request;
 typedef struct {
     uint64_t id, tag;
     int status;                   /* HVVR_OK, or the error of the batch that rendered it */
     uint32_t batch_views;         /* views in that batch */
     double submit_ms, dispatch_ms, done_ms; /* server clock (ms since creation); done = output ready */
+    uint32_t priority;            /* the request's class */
 } hvvr_completion;
 typedef struct {
     uint64_t submitted, completed, failed, batches, queued, in_flight;
@@ -526,7 +564,10 @@ int hvvr_server_get_stats(hvvr_server* server, hvvr_server_stats* out);
  * list entries and rejects larger work with HVVR_ERR_INVALID / HVVR_ERR_OVERFLOW.
  * Calls share that area: calls whose GPU work overlaps race and must be serialised by the caller.
  * The first call on each device looks up the area's device address; make it before any stream
- * capture begins. The call waits for its own work (stream sync) to report the status.
+ * capture begins (the address stays cached until the process exits: do not cudaDeviceReset a
+ * device the library uses). Every call is synchronous: it checks the inputs on the device (block
+ * sizes at most 64, node indices and child offsets inside node_count; HVVR_ERR_INVALID otherwise)
+ * and waits for its own work on the stream to report the status.
  * Output: counts[tile_count] and, when total <= capacity, the lists concatenated in tile order
  * in indices[] - the same lists as hvvr_camera_read_tile_lists for the same frame. */
 typedef struct {

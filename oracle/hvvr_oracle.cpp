@@ -1895,3 +1895,218 @@ void oracle_texture_table_set(uint32_t n, const uint32_t* ids, const float* q, c
 uint32_t oracle_texture_table_missing(void) { return gTexMissing.load(); }
 
 } // extern "C"
+
+// ------------------------------------------------------------------ device BVH build (restated)
+// The linear BVH build of the library's bvh_device.cu, step for step on the CPU. It has no
+// counterpart in the reference, whose GenerateTopology (libraries/hvvr/shared/bvh.cpp:542-556) is a
+// host SAH build; the output uses the reference's TopologyNode layout (leaf slots before internal
+// slots, so that leaf slot k spans [data[k], data[k+1])) and its depth-first node order.
+namespace {
+
+constexpr uint32_t kLbvhLeafTris = 4;
+
+inline uint32_t spreadBits10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+inline uint32_t quantize10(float c, float lo, float scale) {
+    float q = (c - lo) * scale;
+    q = q > 0.0f ? q : 0.0f;
+    q = q < 1023.0f ? q : 1023.0f;
+    return uint32_t(q);
+}
+
+struct LbvhTree {
+    std::vector<uint32_t> keys;              // sorted Morton codes
+    std::vector<uint32_t> order;             // sorted position -> triangle
+    std::vector<uint32_t> left, right;       // internal node children (bit 31: a sorted position, i.e. a single triangle)
+    std::vector<uint32_t> first, last;       // internal node ranges
+};
+
+inline int lbvhDelta(const LbvhTree& t, int i, int j) {
+    const int n = int(t.keys.size());
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = t.keys[size_t(i)], b = t.keys[size_t(j)];
+    if (a == b) return 32 + __builtin_clz(uint32_t(i) ^ uint32_t(j));
+    return __builtin_clz(a ^ b);
+}
+
+// the binary radix tree of the sorted keys (one internal node per i in [0, n-2])
+void lbvhRadixTree(LbvhTree& t) {
+    const int n = int(t.keys.size());
+    t.left.assign(size_t(n > 1 ? n - 1 : 0), 0u);
+    t.right = t.left;
+    t.first = t.left;
+    t.last = t.left;
+    for (int i = 0; i + 1 < n; i++) {
+        const int d = lbvhDelta(t, i, i + 1) - lbvhDelta(t, i, i - 1) > 0 ? 1 : -1;
+        const int dmin = lbvhDelta(t, i, i - d);
+        int lmax = 2;
+        while (lbvhDelta(t, i, i + lmax * d) > dmin) lmax *= 2;
+        int l = 0;
+        for (int s = lmax / 2; s >= 1; s /= 2)
+            if (lbvhDelta(t, i, i + (l + s) * d) > dmin) l += s;
+        const int j = i + l * d;
+        const int dnode = lbvhDelta(t, i, j);
+        int s = 0;
+        for (int div = 2;; div *= 2) {
+            const int step = (l + div - 1) / div;
+            if (lbvhDelta(t, i, i + (s + step) * d) > dnode) s += step;
+            if (step <= 1) break;
+        }
+        const int gamma = i + s * d + (d < 0 ? -1 : 0);
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        t.left[size_t(i)] = lo == gamma ? (0x80000000u | uint32_t(gamma)) : uint32_t(gamma);
+        t.right[size_t(i)] = hi == gamma + 1 ? (0x80000000u | uint32_t(gamma + 1)) : uint32_t(gamma + 1);
+        t.first[size_t(i)] = uint32_t(lo);
+        t.last[size_t(i)] = uint32_t(hi);
+    }
+}
+
+struct LbvhEntry {
+    uint32_t node;      // internal node id, or bit 31 + sorted position for a single triangle
+    uint32_t lo, hi;    // sorted range [lo, hi]
+    uint32_t count() const { return hi - lo + 1; }
+    bool internal() const { return count() > kLbvhLeafTris; }
+};
+
+LbvhEntry lbvhEntry(const LbvhTree& t, uint32_t c) {
+    if (c & 0x80000000u) return LbvhEntry{c, c & 0x7fffffffu, c & 0x7fffffffu};
+    return LbvhEntry{c, t.first[c], t.last[c]};
+}
+
+// the 4-wide node of internal node x: its two children, the child with the most triangles
+// expanded until there are four or none can be, then leaf slots before internal slots
+int lbvhCollapse(const LbvhTree& t, uint32_t x, LbvhEntry* out) {
+    LbvhEntry e[4];
+    int n = 2;
+    e[0] = lbvhEntry(t, t.left[x]);
+    e[1] = lbvhEntry(t, t.right[x]);
+    while (n < 4) {
+        int best = -1;
+        for (int k = 0; k < n; k++)
+            if (e[k].internal() && (best < 0 || e[k].count() > e[best].count())) best = k;
+        if (best < 0) break;
+        const uint32_t id = e[best].node;
+        for (int k = n; k > best + 1; k--) e[k] = e[k - 1];
+        e[best] = lbvhEntry(t, t.left[id]);
+        e[best + 1] = lbvhEntry(t, t.right[id]);
+        n++;
+    }
+    int m = 0;
+    for (int k = 0; k < n; k++)
+        if (!e[k].internal()) out[m++] = e[k];
+    const int leaves = m;
+    for (int k = 0; k < n; k++)
+        if (e[k].internal()) out[m++] = e[k];
+    (void)leaves;
+    return n;
+}
+
+struct LbvhWriter {
+    const LbvhTree& t;
+    const hvvr_tri_shade* tris;
+    hvvr_tri_shade* trisOut;
+    hvvr_topology_node* nodes;
+    uint32_t capacity, nodeCount = 0, triCount = 0;
+    bool overflow = false;
+
+    // writes the node of entry list e[0, n) (n <= 4) at the next index; returns its index
+    uint32_t emit(const LbvhEntry* e, int n) {
+        const uint32_t index = nodeCount++;
+        if (index >= capacity) {
+            overflow = true;
+            return index;
+        }
+        hvvr_topology_node out{};
+        out.leaf_mask = 0;
+        out.data[0] = triCount;
+        uint32_t children[4];
+        int internalCount = 0;
+        for (int k = 0; k < 4; k++) {
+            if (k >= n) { // empty leaf slot
+                out.leaf_mask |= 1u << k;
+                out.data[1 + k] = triCount;
+                continue;
+            }
+            if (e[k].internal()) {
+                children[internalCount++] = uint32_t(k);
+                continue;
+            }
+            out.leaf_mask |= 1u << k;
+            for (uint32_t p = e[k].lo; p <= e[k].hi; p++) trisOut[triCount++] = tris[t.order[p]];
+            out.data[1 + k] = triCount;
+        }
+        nodes[index] = out;
+        for (int c = 0; c < internalCount; c++) {
+            const int k = int(children[c]);
+            LbvhEntry sub[4];
+            const int m = lbvhCollapse(t, e[k].node, sub);
+            const uint32_t child = emit(sub, m);
+            if (!overflow) nodes[index].data[1 + k] = child - index;
+        }
+        return index;
+    }
+};
+
+} // namespace
+
+extern "C" int oracle_lbvh_build(const hvvr_shading_vertex* verts, uint32_t vert_count, const hvvr_tri_shade* tris,
+                                 uint32_t tri_count, hvvr_tri_shade* tris_out, hvvr_topology_node* nodes_out,
+                                 uint32_t capacity, uint32_t* node_count) {
+    if (!verts || !tris || !tris_out || !nodes_out || !node_count || tri_count == 0) return 1;
+    for (uint32_t i = 0; i < tri_count; i++)
+        for (int k = 0; k < 3; k++)
+            if (tris[i].indices[k] >= vert_count) return 1;
+    // centroids (IEEE single, no contraction) and their bounds
+    std::vector<float> cen(size_t(tri_count) * 3);
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = 0; i < tri_count; i++) {
+        const hvvr_vec3& a = verts[tris[i].indices[0]].pos;
+        const hvvr_vec3& b = verts[tris[i].indices[1]].pos;
+        const hvvr_vec3& c = verts[tris[i].indices[2]].pos;
+        const float v[3] = {((a.x + b.x) + c.x) * (1.0f / 3.0f), ((a.y + b.y) + c.y) * (1.0f / 3.0f),
+                            ((a.z + b.z) + c.z) * (1.0f / 3.0f)};
+        for (int k = 0; k < 3; k++) {
+            cen[size_t(i) * 3 + k] = v[k];
+            lo[k] = v[k] < lo[k] ? v[k] : lo[k];
+            hi[k] = v[k] > hi[k] ? v[k] : hi[k];
+        }
+    }
+    float scale[3];
+    for (int k = 0; k < 3; k++) {
+        const float ext = hi[k] - lo[k];
+        scale[k] = ext > 0.0f ? 1024.0f / ext : 0.0f;
+    }
+    LbvhTree t;
+    std::vector<uint32_t> codes(tri_count);
+    for (uint32_t i = 0; i < tri_count; i++) {
+        const float* c = &cen[size_t(i) * 3];
+        codes[i] = (spreadBits10(quantize10(c[0], lo[0], scale[0])) << 2) |
+                   (spreadBits10(quantize10(c[1], lo[1], scale[1])) << 1) |
+                   spreadBits10(quantize10(c[2], lo[2], scale[2]));
+    }
+    t.order.resize(tri_count);
+    for (uint32_t i = 0; i < tri_count; i++) t.order[i] = i;
+    std::stable_sort(t.order.begin(), t.order.end(), [&](uint32_t a, uint32_t b) { return codes[a] < codes[b]; });
+    t.keys.resize(tri_count);
+    for (uint32_t i = 0; i < tri_count; i++) t.keys[i] = codes[t.order[i]];
+    lbvhRadixTree(t);
+    LbvhWriter w{t, tris, tris_out, nodes_out, capacity};
+    LbvhEntry root[4];
+    int n;
+    if (tri_count <= kLbvhLeafTris) {
+        root[0] = LbvhEntry{0x80000000u, 0, tri_count - 1};
+        n = 1;
+    } else {
+        n = lbvhCollapse(t, 0, root);
+    }
+    w.emit(root, n);
+    *node_count = w.nodeCount;
+    return w.overflow ? 2 : 0;
+}

@@ -134,6 +134,15 @@ typedef struct {
 } oracle_fov_out;
 int oracle_foveated_resolve(const oracle_fov_in* in, oracle_fov_out* out);
 
+/* The library's device BVH build (hvvr_generate_topology_device), restated: centroids, 30-bit
+ * Morton codes over the centroid bounds, a stable sort, the binary radix tree of the sorted codes,
+ * leaves of at most 4 triangles, collapse to 4-wide nodes (expanding the child with the most
+ * triangles, leaf slots first), depth-first layout. Writes the nodes and the triangles in leaf
+ * order (vertices are not reordered); returns 0, or 1 for bad arguments / 2 when capacity is short. */
+int oracle_lbvh_build(const hvvr_shading_vertex* verts, uint32_t vert_count, const hvvr_tri_shade* tris,
+                      uint32_t tri_count, hvvr_tri_shade* tris_out, hvvr_topology_node* nodes_out,
+                      uint32_t capacity, uint32_t* node_count);
+
 #ifdef __cplusplus
 }
 #endif

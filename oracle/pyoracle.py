@@ -67,17 +67,27 @@ class Frame:
 def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi.HVVR_FP_FMA, lens=(0.0, 1.0),
          threads=None, split=1, want=("lists", "hits", "colors", "image", "blocks", "gbuffer", "scene", "beams"),
          model_xf=None, tile_capacity=None, beams_in=None, textures=0, sampler=None):
-    if scene.nodes is None:
+    # one scene, or a list of scenes (models of one raycaster, merged under root fix-up nodes as
+    # Raycaster::buildScene does) with a list of model transforms; the lights are the first scene's
+    models = list(scene) if isinstance(scene, (list, tuple)) else [scene]
+    if any(m.nodes is None for m in models):
         raise ValueError("scene has no topology")
+    if isinstance(model_xf, (list, tuple)):
+        model_xfs = list(model_xf)
+    else:
+        model_xfs = [model_xf if model_xf is not None else _abi.transform()] * len(models)
     n = len(samples) if beams_in is None else len(beams_in["beams"])
     blocks, tiles, padded = layout(n)
-    md = _abi.MeshData(_abi.ptr(scene.verts), len(scene.verts), _abi.ptr(scene.tri_shade), len(scene.tri_shade),
-                       _abi.ptr(scene.nodes), len(scene.nodes), _abi.ptr(scene.materials), len(scene.materials))
-    mds = (_abi.MeshData * 1)(md)
-    xfs = (_abi.Transform * 1)(model_xf if model_xf is not None else _abi.transform())
-    lights = (_abi.LightUnion * len(scene.lights))(*scene.lights)
+    mds = (_abi.MeshData * len(models))(*[
+        _abi.MeshData(_abi.ptr(m.verts), len(m.verts), _abi.ptr(m.tri_shade), len(m.tri_shade), _abi.ptr(m.nodes),
+                      len(m.nodes), _abi.ptr(m.materials), len(m.materials)) for m in models])
+    xfs = (_abi.Transform * len(models))(*model_xfs)
+    lights = (_abi.LightUnion * len(models[0].lights))(*models[0].lights)
+    node_total = sum(len(m.nodes) for m in models) + ((len(models) + 1) // 3 if len(models) > 1 else 0)
+    tri_total = sum(len(m.tri_shade) for m in models)
+    scene = models[0]
     fin = FrameIn()
-    fin.model_count = 1
+    fin.model_count = len(models)
     fin.models = mds
     fin.model_xf = xfs
     fin.lights = lights
@@ -132,8 +142,8 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
     if "tile_rays" in want:
         alloc("tile_rays", (tiles, 24), np.float32, "tile_rays")
     if "scene" in want:
-        alloc("nodes", len(scene.nodes), _abi.NODE_DTYPE, "nodes")
-        alloc("tris", (len(scene.tri_shade), 9), np.float32, "tris")
+        alloc("nodes", node_total, _abi.NODE_DTYPE, "nodes")
+        alloc("tris", (tri_total, 9), np.float32, "tris")
     if "tmax" in want:
         alloc("tmax", padded, np.float32, "tmax")
     if "tile_frusta" in want:
@@ -244,6 +254,22 @@ class Oracle:
         if f(C.byref(fi), C.byref(fo)) != 0:
             raise RuntimeError("oracle_foveated_resolve failed")
         return out
+
+    def lbvh_build(self, scene):
+        """The device BVH build restated (oracle_lbvh_build): (tri_shade in leaf order, nodes)."""
+        f = self.lib.oracle_lbvh_build
+        f.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                      C.POINTER(C.c_uint32)]
+        f.restype = C.c_int
+        n = len(scene.tri_shade)
+        tris = np.zeros_like(scene.tri_shade)
+        nodes = np.zeros(n + 4, dtype=_abi.TOPO_DTYPE)
+        cnt = C.c_uint32(0)
+        rc = f(scene.verts.ctypes.data, len(scene.verts), scene.tri_shade.ctypes.data, n, tris.ctypes.data,
+               nodes.ctypes.data, len(nodes), C.byref(cnt))
+        if rc != 0:
+            raise RuntimeError("oracle_lbvh_build failed: %d" % rc)
+        return tris, nodes[: cnt.value].copy()
 
     def msaa_offsets(self, n):
         o = np.zeros((n, 2), dtype=np.float32)

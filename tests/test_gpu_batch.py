@@ -133,16 +133,20 @@ def test_animated_refit_matches_oracle(oracle):
     rc.close()
 
 
-def test_stack_retry_pass_matches_oracle(oracle):
+@pytest.mark.parametrize("pipeline", [1, 0])
+def test_stack_retry_pass_matches_oracle(oracle, pipeline):
     """A 16-entry main-pass stack sends every tile whose sorted stack grows deeper to the retry
-    pass (4096 entries); the lists, hits and colours must not change."""
+    pass (4096 entries); the lists, hits and colours must not change. With the cull -> shade
+    pipeline the retried tiles are skipped by the pipelined shade and shaded by the retry list's
+    own launch."""
     sc = scene("c1")
     w, h = 320, 288
     rc = _make_rc(sc)
     cam, smp = _add_cam(rc, w, h, "barrel", 4)
     xf = scenes.camera_transform(eye=(3.0, 1.2, 6.0), target=(-2.0, 0.3, -1.0))
     cam.set_camera_to_world(xf)
-    batch = hv.Batch(cameras=[cam], config=hv.batch_config(tile_stack_entries=16, tri_index_capacity=1 << 22))
+    batch = hv.Batch(cameras=[cam], config=hv.batch_config(tile_stack_entries=16, tri_index_capacity=1 << 22,
+                                                           pipeline=pipeline))
     for _ in range(3):
         batch.render()
         st = batch.stats()
@@ -150,6 +154,46 @@ def test_stack_retry_pass_matches_oracle(oracle):
         _check_view(oracle, sc, cam, smp, w, h, 4, xf)
     batch.close()
     rc.close()
+
+
+@pytest.mark.parametrize("use_graph", [1, 0])
+def test_pipelined_and_split_frames_agree(oracle, use_graph):
+    """The cull -> shade pipeline (default) against the split path (heavy part on its own stream,
+    cull before shade) on a frame batch with three MSAA rates over two scenes, over three frames
+    (the second and later ones cull in the previous frame's cost order): identical lists, hits
+    and colours, and both equal to the oracle."""
+    sa, sb = scene("c1"), scene("small")
+    rc_a, rc_b = _make_rc(sa), _make_rc(sb)
+    views = [(rc_a, sa, 256, 224, "barrel", 8), (rc_a, sa, 192, 160, "grid", 1), (rc_b, sb, 160, 176, "barrel", 4)]
+    cams = []
+    for k, (rc, sc, w, h, kind, msaa) in enumerate(views):
+        cam, smp = _add_cam(rc, w, h, kind, msaa)
+        xf = scenes.camera_transform(eye=(0.4 * k, 2.0, 10.0), target=(0.0, 0.2 * k, 0.0))
+        cam.set_camera_to_world(xf)
+        cams.append((cam, sc, smp, w, h, msaa, xf))
+    results = {}
+    for pipeline in (1, 0):
+        batch = hv.Batch([rc_a, rc_b], hv.batch_config(use_graph=use_graph, tri_index_capacity=1 << 22,
+                                                       pipeline=pipeline, timing=1, tile_cull_warps=1 + pipeline))
+        for frame in range(3):
+            batch.render()
+            assert batch.stats()["status"] == 0
+        parts = batch.part_times()
+        assert parts is not None
+        out = []
+        for cam, sc, smp, w, h, msaa, xf in cams:
+            counts, idx = cam.tile_lists()
+            ids, depth = cam.hits()
+            out.append((counts, idx, ids, depth, cam.sample_colors()))
+            if pipeline:  # read while the batch that holds the lists is open
+                _check_view(oracle, sc, cam, smp, w, h, msaa, xf)
+        results[pipeline] = out
+        batch.close()
+    for a, b in zip(results[1], results[0]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    rc_a.close()
+    rc_b.close()
 
 
 def test_batch_mixes_thin_lens_and_pinhole_views(oracle):

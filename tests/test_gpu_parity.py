@@ -137,9 +137,11 @@ def test_against_reference_kernels(name, w, h, msaa, kind):
     ResolveKernel built for this GPU (oracle/refshim/ref_gpu_intersect.cu), fed the reference
     host code's beams, world tile frusta and tile lists: the compressed G-buffer (triangle, mask)
     pairs equal on every sample of every occupied tile but at most one, and colours within 1 LSB
-    elsewhere. The reference's kernels are built with fast math; on the recorded cases one
-    subsample on an edge shared by two triangles resolves to the other triangle (recorded in the
-    design notes), in both of this library's FP modes."""
+    elsewhere. The reference's kernels are built with fast math (nvcc contracts their products
+    into FMAs where it chooses); on three of these cases one subsample on an edge shared by two
+    triangles resolves to the other triangle - C1 barrel MSAA 4 sample 217585 subsample 3, C1 barrel
+    MSAA 8 sample 235826 subsample 0, the small scene MSAA 32 sample 41379 subsample 7 - in both of
+    this library's FP modes."""
     import pyoracle
     from hvvr_b200 import scenes as sc_mod
     refg, refh = pyoracle.ReferenceGpu(), pyoracle.Reference()
@@ -163,3 +165,74 @@ def test_against_reference_kernels(name, w, h, msaa, kind):
         keep[bad] = False
         d = np.abs(col[:n].view(np.uint8).astype(np.int32) - r["colors"][:n].view(np.uint8).astype(np.int32))
         assert d.reshape(n, 4)[keep].max() <= 1, (mode, int(d.reshape(n, 4)[keep].max()))
+
+
+def _split_samples(w, h, split, seed):
+    """split copies of a jittered grid, each copy jittered again (one per colour channel)"""
+    rng = np.random.default_rng(seed)
+    base = scenes.grid_samples(w, h)
+    base["position"] += rng.uniform(-0.4, 0.4, (len(base), 2)).astype(np.float32) / np.array([w, h], np.float32)
+    smp = np.repeat(base, split)
+    smp["position"] += rng.uniform(-0.1, 0.1, (len(smp), 2)).astype(np.float32) / np.array([w, h], np.float32)
+    return smp
+
+
+@pytest.mark.parametrize("split", [2, 3])
+def test_split_color_images_match_oracle(oracle, split):
+    """Split-colour sample sets (Camera::setSamples with splitColorSamples 2 or 3; the remap of
+    RC/remap.cu:35-124 packs the channels of 2 (pentile) or 3 samples into one pixel): hits, colours
+    and the remapped image against the oracle."""
+    sc = scene("small")
+    w, h = 200, 160
+    smp = _split_samples(w, h, split, 40 + split)
+    rc, cam = render_gpu(sc, smp, w, h, 4, split=split)
+    fo = render_oracle(oracle, sc, smp, w, h, 4, split=split)
+    _compare(cam, rc, fo, 4)
+    assert np.array_equal(cam.sample_remap(split), fo.remap)
+    img = cam.image
+    d = np.abs(img.view(np.uint8).astype(np.int32) - fo.image.view(np.uint8).astype(np.int32))
+    assert d.max() <= 1 and (img != 0).any()
+    rc.close()
+
+
+def test_five_models_under_root_fixup_nodes(oracle):
+    """Five models in one raycaster, each with its own transform: Raycaster::buildScene merges them
+    under two levels of root fix-up nodes (RC/scene_update.cpp:22-143); the merged BVH after refit,
+    the triangles, the lists, hits and colours must equal the oracle's merge of the same models."""
+    parts = [scenes.make_scene(10, 60, seed=30 + k) for k in range(5)]
+    for p in parts:
+        hv.generate_topology(p)
+    xfs = []
+    for k in range(5):
+        a = 0.3 * k
+        rot = (0.0, float(np.sin(a / 2)), 0.0, float(np.cos(a / 2)))
+        xfs.append(_abi_transform(rot, (-8.0 + 4.0 * k, 0.2 * k, -2.0 * (k % 2)), 0.6 + 0.1 * k))
+    rc = hv.Raycaster()
+    for p, xf in zip(parts, xfs):
+        m = rc.create_model(p)
+        m.set_transform(xf)
+    for l in parts[0].lights:
+        rc.create_light(l)
+    w, h = 320, 240
+    smp = scenes.barrel_samples(w, h)
+    cam_xf = scenes.camera_transform(eye=(0.0, 6.0, 14.0), target=(0.0, 0.0, 0.0))
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h)
+    cam.set_samples(smp)
+    cam.set_camera_to_world(cam_xf)
+    cam.set_msaa(4)
+    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+    rc.render()
+    fo = oracle.render(parts, smp, cam_xf, scenes.viewport_for(w, h), w, h, 4, model_xf=xfs)
+    assert len(rc.scene_nodes()) == sum(len(p.nodes) for p in parts) + 2
+    _compare(cam, rc, fo, 4)
+    ids, _ = cam.hits()
+    tri_base = np.cumsum([0] + [len(p.tri_shade) for p in parts])
+    hit_models = set(np.searchsorted(tri_base, ids[ids != 0xFFFFFFFF], side="right") - 1)
+    assert len(hit_models) >= 3, hit_models
+    rc.close()
+
+
+def _abi_transform(rot, trans, scale):
+    from hvvr_b200 import _abi
+    return _abi.transform(rot, trans, scale)

@@ -98,7 +98,7 @@ def test_tight_budget_evicts_and_completes():
     pools = 2 * cap * 4 * 129 // 128
     budget = pools + (3 << 20)  # room for two of these small views at a time, not all four
     srv = hv.Server(rcs, hv.server_config(slots=2, max_batch_views=4, slot_list_capacity=cap,
-                                          hbm_budget_bytes=budget))
+                                          hbm_budget_bytes=budget, latency_slots=0))
     ids = []
     for si, kind, w, h in _templates():
         smp, vp = _samples(kind, w, h)
@@ -201,3 +201,49 @@ def test_polar_foveated_requests_same_alone_in_mix_and_direct():
         assert np.array_equal(cam.image, mix[k][1]), "request %d differs from a direct render" % k
         cam.set_enabled(False)
     rc.close()
+
+
+def test_latency_class_jumps_a_busy_mix(oracle):
+    """A stereo pair submitted as the latency class (priority 1) behind a queue of throughput
+    requests is dispatched at once on the latency slot, both eyes in one batch, while throughput
+    requests are still waiting; each eye's image equals the oracle's (and its completion says which
+    class it was)."""
+    scs = [scene("c1"), scene("small")]
+    rcs = [_rc(s) for s in scs]
+    srv = hv.Server(rcs, hv.server_config(slots=2, max_batch_views=4, slot_list_capacity=1 << 22, latency_slots=1,
+                                          tile_cull_ctas_per_sm=3))
+    tmpl = []
+    for si, kind, w, h in _templates():
+        smp, vp = _samples(kind, w, h)
+        tmpl.append((srv.add_view(si, vp, smp, w, h), w, h))
+    sw, sh = 320, 352
+    ssmp = scenes.barrel_samples(sw, sh)
+    stereo = srv.add_view(0, scenes.viewport_for(sw, sh), ssmp, sw, sh)
+    rng = np.random.default_rng(9)
+    for k in range(32):
+        vid, w, h = tmpl[k % len(tmpl)]
+        xf = scenes.camera_transform(eye=(float(rng.uniform(-4, 4)), 2.0, 9.0))
+        srv.submit(vid, 16, xf, output=np.zeros((h, w), dtype=np.uint32), tag=k)
+    eyes = scenes.stereo_eyes(0.064)
+    outs = []
+    for e, xf in enumerate(eyes):
+        out = np.zeros((sh, sw), dtype=np.uint32)
+        outs.append((srv.submit(stereo, 8, xf, output=out, tag=1000 + e, priority=1), out, xf))
+    done = _drain(srv, 34)
+    assert all(c.status == 0 for c in done.values())
+    thr = [c for c in done.values() if c.priority == 0]
+    lat = [done[rid] for rid, _, _ in outs]
+    assert all(c.priority == 1 for c in lat) and len(thr) == 32
+    assert all(c.batch_views <= 2 for c in lat)
+    # dispatched ahead of throughput requests submitted before them
+    assert max(c.dispatch_ms for c in lat) < max(c.dispatch_ms for c in thr)
+    for rid, out, xf in outs:
+        fo = render_oracle(oracle, scs[0], ssmp, sw, sh, 8, cam_xf=xf)
+        d = np.abs(out.view(np.uint8).astype(np.int32) - fo.image.view(np.uint8).astype(np.int32))
+        assert d.max() <= 1
+    # a bad class is refused
+    with pytest.raises(hv.HvvrError):
+        srv.submit(stereo, 8, eyes[0], output=np.zeros((sh, sw), dtype=np.uint32), priority=2)
+    srv.close()
+    for rc in rcs:
+        rc.close()
