@@ -14,7 +14,8 @@ from . import _abi
 from ._abi import (HVVR_CAPTURE_HITS, HVVR_FP_FMA, HVVR_FP_STRICT, HVVR_MEMORY_CPU, HVVR_MEMORY_CUDA,  # noqa: F401
                    HVVR_OK, HVVR_SETUP_DEVICE, HVVR_SETUP_HOST, HVVR_TEXTURE_R32_FLOAT, HVVR_TEXTURE_RGBA8_UNORM, HVVR_TEXTURE_RGBA8_UNORM_SRGB,
                    HVVR_TEXTURE_RGBA16_FLOAT, HVVR_TEXTURE_RGBA16_UNORM, HVVR_TEXTURE_RGBA32_FLOAT,
-                   HVVR_TEXTURE_R11G11B10_FLOAT)
+                   HVVR_TEXTURE_R11G11B10_FLOAT, HVVR_MSAA_SPIRAL, HVVR_MSAA_ROTATED_GRID, HVVR_BVH_HOST,
+                   HVVR_BVH_DEVICE)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("HVVR_B200_LIB") or os.path.join(_HERE, "_lib", "libhvvr_b200.so")
@@ -70,6 +71,7 @@ _sig("hvvr_camera_set_samples", _vp, _vp, _u32, _u32)
 _sig("hvvr_camera_set_camera_to_world", _vp, _p(_abi.Transform))
 _sig("hvvr_camera_prepare", _vp, _p(_u32))
 _sig("hvvr_camera_set_msaa", _vp, _u32)
+_sig("hvvr_camera_set_msaa_pattern", _vp, _u32)
 _sig("hvvr_camera_get_sample_count", _vp, _p(_u32))
 _sig("hvvr_camera_set_capture", _vp, _u32)
 _sig("hvvr_camera_get_layout", _vp, _p(_u32), _p(_u32), _p(_u32), _p(_u32))
@@ -148,7 +150,7 @@ EXPORTED = [
     "hvvr_camera_set_viewport", "hvvr_camera_set_lens", "hvvr_camera_set_aperture", "hvvr_camera_set_focal_depth",
     "hvvr_camera_set_eye_dir", "hvvr_camera_set_spherical_warp", "hvvr_camera_set_render_target",
     "hvvr_camera_set_samples", "hvvr_camera_set_camera_to_world", "hvvr_camera_prepare", "hvvr_camera_set_msaa",
-    "hvvr_camera_get_sample_count", "hvvr_camera_set_capture", "hvvr_camera_get_layout",
+    "hvvr_camera_get_sample_count", "hvvr_camera_set_capture", "hvvr_camera_get_layout", "hvvr_camera_set_msaa_pattern",
     "hvvr_camera_read_tile_lists", "hvvr_camera_read_block_stacks", "hvvr_camera_read_hits",
     "hvvr_camera_read_gbuffer", "hvvr_camera_read_sample_colors", "hvvr_camera_read_sample_remap",
     "hvvr_camera_read_beams", "hvvr_camera_read_timings", "hvvr_camera_read_list_total", "hvvr_scene_get_counts",
@@ -453,6 +455,10 @@ class Camera:
         _check(_lib.hvvr_camera_prepare(self.handle, C.byref(on_host)))
         return bool(on_host.value)
 
+    def set_msaa_pattern(self, pattern):
+        """HVVR_MSAA_SPIRAL (the reference's, default) or HVVR_MSAA_ROTATED_GRID"""
+        _check(_lib.hvvr_camera_set_msaa_pattern(self.handle, pattern))
+
     def set_msaa(self, rate):
         _check(_lib.hvvr_camera_set_msaa(self.handle, rate))
 
@@ -697,10 +703,10 @@ class Raycaster:
         return t
 
     def part_times(self):
-        """the last frame's timeline per launch part [24, 3]: tile cull start, tile cull end,
+        """the last frame's timeline per launch part [36, 3]: tile cull start, tile cull end,
         intersect end (ms from the frame start, -1 where the part did not run); part 2r holds
         rate class r's slowest tiles, 2r+1 the rest"""
-        t = np.zeros((24, 3), dtype=np.float32)
+        t = np.zeros((36, 3), dtype=np.float32)
         _check(_lib.hvvr_raycaster_read_part_times(self.handle, t.ctypes.data))
         return t
 
@@ -796,8 +802,8 @@ class Batch:
         return t
 
     def part_times(self):
-        """the last frame's timeline per launch part [24, 3] (see Raycaster.part_times)"""
-        t = np.zeros((24, 3), dtype=np.float32)
+        """the last frame's timeline per launch part [36, 3] (see Raycaster.part_times)"""
+        t = np.zeros((36, 3), dtype=np.float32)
         _check(_lib.hvvr_batch_read_part_times(self.handle, t.ctypes.data))
         return t
 

@@ -23,6 +23,7 @@ HVVR_MODE_DEFERRED_MSAA_RESOLVE, HVVR_MODE_FOVEATED_POLAR = 0, 1
 HVVR_FP_FMA, HVVR_FP_STRICT = 0, 1
 HVVR_SETUP_DEVICE, HVVR_SETUP_HOST = 0, 1
 HVVR_BVH_HOST, HVVR_BVH_DEVICE = 0, 1
+HVVR_MSAA_SPIRAL, HVVR_MSAA_ROTATED_GRID = 0, 1
 HVVR_CAPTURE_HITS = 1
 
 

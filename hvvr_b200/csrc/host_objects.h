@@ -137,6 +137,7 @@ struct hvvr_camera {
     uint32_t split = 1;
     hvvr_transform xf{};
     uint32_t msaa = 16;
+    uint32_t msaaPattern = 0;       // HVVR_MSAA_SPIRAL or HVVR_MSAA_ROTATED_GRID
     uint32_t capture = 0;
     bool setupDirty = true;
     bool setupOnHost = false;         // the current sample setup was built on the host

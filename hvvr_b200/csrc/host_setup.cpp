@@ -144,6 +144,20 @@ void msaaOffsets(uint32_t n, float* out) {
     }
 }
 
+// The alternative pattern (no counterpart in the reference): an n-rooks lattice, subsample i in
+// column i and row (k i) mod n of an n x n grid over [-1, 1]^2 (k = 1, 3, 5, 9, 19 for
+// n = 2, 4, 8, 16, 32: one subsample per row and column, the rows spread), scaled by 1/sqrt(2) into
+// the unit disk the spiral fills; rate 1 is the sample's centre.
+void msaaOffsetsRotatedGrid(uint32_t n, float* out) {
+    const uint32_t k = n == 2 ? 1u : n == 4 ? 3u : n == 8 ? 5u : n == 16 ? 9u : n == 32 ? 19u : 0u;
+    for (uint32_t i = 0; i < n; i++) {
+        const float x = float(2 * i + 1) / float(n) - 1.0f;
+        const float y = float(2 * ((k * i) % n) + 1) / float(n) - 1.0f;
+        out[2 * i + 0] = x * 0.70710677f;
+        out[2 * i + 1] = y * 0.70710677f;
+    }
+}
+
 // GPUCamera::initLookupTables (libraries/hvvr/raycaster/gpu_camera.cu:59-88): for each of the 4
 // table tiles and 128 samples one random rotation (std::mt19937, default seed, drawn through
 // uniform_real_distribution<float> and scaled by Tau), and subsample i of that sample takes the

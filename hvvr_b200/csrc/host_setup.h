@@ -27,6 +27,8 @@ Mat4 transformToMatrix(const hvvr_transform& t);
 
 // getSubsampleUnitOffset<N> with JITTER_SAMPLES=0 (libraries/hvvr/raycaster/gpu_samples.h:35-61)
 void msaaOffsets(uint32_t n, float* out2n);
+// the rotated-grid (n-rooks) alternative, same layout
+void msaaOffsetsRotatedGrid(uint32_t n, float* out2n);
 // naiveXYCluster (libraries/hvvr/raycaster/sample_clustering.h:17-49): stratified sorts into k
 // blocks of kBlockSize and tiles of kTileSize; x(p), y(p) give a point's 2D position
 template <class T, class X, class Y>

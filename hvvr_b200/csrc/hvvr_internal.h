@@ -174,7 +174,7 @@ struct ViewDev {
     uint32_t* hitIds;                // nullptr unless capturing
     float* depth;
     uint32_t tileStart, blockStart;  // first global tile / block
-    uint32_t msaa, rateIdx;          // rate; its class: log2(msaa), + 6 for a thin-lens view
+    uint32_t msaa, rateIdx;          // rate; its class: log2(msaa), + 6 for a thin-lens view, + 12 for the rotated grid
     // thin lens (depth of field) when lensRadius > 0
     float lensRadius, focalDistance;
     const float2* lensPos;           // [4 tiles][msaa][128] lens positions (the reference's lookup table)
@@ -206,8 +206,9 @@ struct FrameDev {
 // records the message returned by hvvr_last_error() on this thread and returns code
 int setLastError(int code, const char* msg);
 
-// rate classes: log2(msaa) for pinhole views, 6 + log2(msaa) for thin-lens views
-enum : uint32_t { kRateClasses = 12 };
+// rate classes: log2(msaa) for pinhole views (spiral pattern), 6 + log2(msaa) for thin-lens views,
+// 12 + log2(msaa) for pinhole views with the rotated-grid pattern
+enum : uint32_t { kRateClasses = 18 };
 // counters: [0] chunk allocator, [1] status, then per tile-cull launch k (2 per rate class)
 // three words at kQueueBase + 3k: work-queue head, retry count, retry-queue head
 // then one word counting the list entries that survive the intersect's per-tile tests, one counting
@@ -235,8 +236,9 @@ cudaError_t launchTileOrder(const FrameDev& fr, cudaStream_t st);
 // culled again by a second launch with a 4096-entry stack.
 cudaError_t launchTileCull(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
                            uint32_t* queues, uint32_t warps, uint32_t stackLimit, cudaStream_t st);
-cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, bool dof, const uint32_t* order,
-                                 uint32_t first, uint32_t count, cudaStream_t st);
+// pattern: 0 the spiral, 1 the rotated grid (pinhole only; thin lens always uses the spiral)
+cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, uint32_t pattern, bool fpStrict, bool dof,
+                                 const uint32_t* order, uint32_t first, uint32_t count, cudaStream_t st);
 // The cull -> shade pipeline of one part of a pinhole rate class over the global tiles
 // order[first, first + count), on one stream: the tile cull publishes every finished tile into fr.ready[first + i]
 // (i = the order of completion; pipe[0] counts them), and the shade launch - started while the
@@ -252,14 +254,15 @@ cudaError_t launchTileCullMain(const FrameDev& fr, const uint32_t* order, uint32
                                uint32_t* readyTail, cudaStream_t st);
 cudaError_t launchTileCullRetryPass(const FrameDev& fr, const uint32_t* order, uint32_t first, uint32_t count,
                                     uint32_t* queues, cudaStream_t st);
-cudaError_t launchCullShadePipeline(const FrameDev& fr, uint32_t msaa, bool fpStrict, uint32_t first, uint32_t count,
-                                    uint32_t* queues, uint32_t* pipe, uint32_t warps, uint32_t stackLimit,
-                                    cudaStream_t st);
+cudaError_t launchCullShadePipeline(const FrameDev& fr, uint32_t msaa, uint32_t pattern, bool fpStrict, uint32_t first,
+                                    uint32_t count, uint32_t* queues, uint32_t* pipe, uint32_t warps,
+                                    uint32_t stackLimit, cudaStream_t st);
 // occRank of every thin-lens view (one block per view; pinhole views are skipped)
 cudaError_t launchOccupiedRank(const FrameDev& fr, cudaStream_t st);
 cudaError_t launchRemap(const CameraDev& c, cudaStream_t st);
 cudaError_t launchRefit(const SceneDev& s, bool fma, cudaStream_t st);
-cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st);
+// the unit offsets of rate n for pattern 0 (spiral) or 1 (rotated grid)
+cudaError_t uploadMsaaTable(uint32_t n, uint32_t pattern, const float* offsets, cudaStream_t st);
 // the foveated resolve of view `view` of the frame (fov: the host copy of its FoveaDev, for
 // the launch shapes): scatter to the polar textures, moments, polar -> screen with temporal
 // reprojection, two eccentricity filter passes and contrast enhancement into fov.image

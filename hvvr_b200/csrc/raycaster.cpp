@@ -476,7 +476,11 @@ uint32_t rateIndex(uint32_t rate) { return rate <= 1 ? 0u : uint32_t(31 - __buil
 
 bool hasLens(const hvvr_camera* c) { return c->lens.radius > 0.0f; }
 // launches are grouped by rate class: log2(msaa), + 6 for a thin-lens view (a separate kernel)
-uint32_t rateClass(const hvvr_camera* c) { return rateIndex(c->msaa) + (hasLens(c) ? 6u : 0u); }
+// rate class: log2(msaa); + 6 for a thin-lens view; + 12 for a pinhole view with the rotated grid
+uint32_t rateClass(const hvvr_camera* c) {
+    if (hasLens(c)) return rateIndex(c->msaa) + 6u;
+    return rateIndex(c->msaa) + (c->msaaPattern == HVVR_MSAA_ROTATED_GRID ? 12u : 0u);
+}
 
 // the offset tables live in one __constant__ array per device, written once per rate
 int ensureMsaaTable(uint32_t rate, cudaStream_t st) {
@@ -490,7 +494,9 @@ int ensureMsaaTable(uint32_t rate, cudaStream_t st) {
     if (done) return HVVR_OK;
     float off[64];
     msaaOffsets(rate, off);
-    CUDA_TRY(uploadMsaaTable(rate, off, st));
+    CUDA_TRY(uploadMsaaTable(rate, 0, off, st));
+    msaaOffsetsRotatedGrid(rate, off);
+    CUDA_TRY(uploadMsaaTable(rate, 1, off, st));
     CUDA_TRY(cudaStreamSynchronize(st)); // visible before any other stream can use the rate
     done = true;
     return HVVR_OK;
@@ -733,7 +739,8 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
     for (uint32_t r = 0; r < kRateClasses; r++) {
         const uint32_t n = b->rateTiles[r];
         if (!n) continue;
-        const bool lens = r >= 6;
+        const bool lens = r >= 6 && r < 12;
+        const uint32_t pattern = r >= 12 ? 1u : 0u;
         const uint32_t rs = b->rateStart[r], heavy = lens ? 0u : heavyTiles(b, n), msaa = 1u << (r % 6);
         // part 0: last frame's slowest tiles on the high-priority stream; part 1: the rest
         for (uint32_t part = heavy ? 0u : 1u; part < 2; part++) {
@@ -743,7 +750,7 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
             CUDA_TRY(cudaStreamWaitEvent(ps, b->forkEv, 0));
             if (stages) CUDA_TRY(recordStage(b->kev[k][0], ps, capturing));
             if (!lens && b->cfg.pipeline) {
-                CUDA_TRY(launchCullShadePipeline(fr, msaa, b->fpStrict, p0, pn, fr.counters + kQueueBase + kQueueWords * k,
+                CUDA_TRY(launchCullShadePipeline(fr, msaa, pattern, b->fpStrict, p0, pn, fr.counters + kQueueBase + kQueueWords * k,
                                                  fr.counters + kPipeBase + k, b->cfg.tile_cull_warps,
                                                  b->cfg.tile_stack_entries, ps));
                 // the cull and the shade overlap: one event marks the end of both (and of the retry
@@ -767,7 +774,7 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
                 CUDA_TRY(cudaEventRecord(b->cullEv[k], ps));
                 continue;
             }
-            CUDA_TRY(launchIntersectShade(fr, msaa, b->fpStrict, false, fr.order, p0, pn, ps));
+            CUDA_TRY(launchIntersectShade(fr, msaa, pattern, b->fpStrict, false, fr.order, p0, pn, ps));
             if (stages) CUDA_TRY(recordStage(b->kev[k][2], ps, capturing));
             b->kevUsed[k] = true;
             CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
@@ -776,17 +783,17 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
         first = false;
     }
     if (b->anyLens) {
-        for (uint32_t r = 6; r < kRateClasses; r++)
+        for (uint32_t r = 6; r < 12; r++)
             if (b->rateTiles[r]) CUDA_TRY(cudaStreamWaitEvent(st, b->cullEv[2 * r + 1], 0));
         CUDA_TRY(launchOccupiedRank(fr, st));
         CUDA_TRY(cudaEventRecord(b->rankEv, st));
-        for (uint32_t r = 6; r < kRateClasses; r++) {
+        for (uint32_t r = 6; r < 12; r++) {
             const uint32_t n = b->rateTiles[r];
             if (!n) continue;
             const uint32_t k = 2 * r + 1;
             cudaStream_t ps = b->side[k];
             CUDA_TRY(cudaStreamWaitEvent(ps, b->rankEv, 0));
-            CUDA_TRY(launchIntersectShade(fr, 1u << (r % 6), b->fpStrict, true, fr.order, b->rateStart[r], n, ps));
+            CUDA_TRY(launchIntersectShade(fr, 1u << (r % 6), 0, b->fpStrict, true, fr.order, b->rateStart[r], n, ps));
             if (stages) CUDA_TRY(recordStage(b->kev[k][2], ps, capturing));
             b->kevUsed[k] = true;
             CUDA_TRY(cudaEventRecord(b->doneEv[k], ps));
@@ -1336,12 +1343,12 @@ static int frameCounters(const hvvr_batch* b, uint64_t* out, uint32_t count) {
     return HVVR_OK;
 }
 
-static int partTimes(const hvvr_batch* b, float* ms72) {
+static int partTimes(const hvvr_batch* b, float* ms108) {
     if (!b || !b->counterValid) return fail(HVVR_ERR_STATE, "no frame rendered");
     if (!b->stageTimes) return fail(HVVR_ERR_STATE, "the last frame was rendered without per-launch events (config.timing = 0)");
     CUDA_TRY(cudaEventSynchronize(b->ev[5]));
     for (uint32_t k = 0; k < 2 * kRateClasses; k++) {
-        float* o = ms72 + 3 * k;
+        float* o = ms108 + 3 * k;
         o[0] = o[1] = o[2] = -1.0f;
         if (!b->kevUsed[k]) continue;
         for (int i = 0; i < 3; i++) CUDA_TRY(cudaEventElapsedTime(&o[i], b->ev[0], b->kev[k][i]));
@@ -1376,14 +1383,14 @@ int hvvr_raycaster_read_counters(const hvvr_raycaster* rc, uint64_t* out, uint32
     return frameCounters(rc->own.get(), out, count);
 }
 
-int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72) {
-    if (!rc || !ms72) return fail(HVVR_ERR_INVALID, "NULL argument");
-    return partTimes(rc->own.get(), ms72);
+int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms108) {
+    if (!rc || !ms108) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return partTimes(rc->own.get(), ms108);
 }
 
-int hvvr_batch_read_part_times(const hvvr_batch* b, float* ms72) {
-    if (!ms72) return fail(HVVR_ERR_INVALID, "NULL argument");
-    return partTimes(b, ms72);
+int hvvr_batch_read_part_times(const hvvr_batch* b, float* ms108) {
+    if (!ms108) return fail(HVVR_ERR_INVALID, "NULL argument");
+    return partTimes(b, ms108);
 }
 
 int hvvr_batch_read_kernel_times(const hvvr_batch* b, float* ms4) {
@@ -1672,6 +1679,13 @@ int hvvr_camera_set_msaa(hvvr_camera* cam, uint32_t rate) {
     CAM_CHECK(cam);
     if (!validRate(rate)) return fail(HVVR_ERR_INVALID, "MSAA rate must be 1, 2, 4, 8, 16 or 32");
     cam->msaa = rate;
+    return HVVR_OK;
+}
+
+int hvvr_camera_set_msaa_pattern(hvvr_camera* cam, uint32_t pattern) {
+    if (!cam) return fail(HVVR_ERR_INVALID, "NULL camera");
+    if (pattern != HVVR_MSAA_SPIRAL && pattern != HVVR_MSAA_ROTATED_GRID) return fail(HVVR_ERR_INVALID, "unknown MSAA pattern");
+    cam->msaaPattern = pattern;
     return HVVR_OK;
 }
 int hvvr_camera_get_sample_count(const hvvr_camera* cam, uint32_t* count) {

@@ -19,10 +19,11 @@
 
 namespace hvb {
 
-__constant__ float2 cMsaa[6][32]; // unit offsets for rates 1,2,4,8,16,32
+// unit offsets for rates 1,2,4,8,16,32: rows 0-5 the spiral, rows 6-11 the rotated grid
+__constant__ float2 cMsaa[12][32];
 // the same offsets split by axis, so that subsamples 2k and 2k+1 read as one 64-bit pair
-__constant__ __align__(8) float cMsaaX[6][32];
-__constant__ __align__(8) float cMsaaY[6][32];
+__constant__ __align__(8) float cMsaaX[12][32];
+__constant__ __align__(8) float cMsaaY[12][32];
 
 namespace {
 
@@ -482,7 +483,9 @@ __device__ uint32_t waitReady(const uint32_t* slot, uint32_t* counters) {
 // One tile: intersect, G-buffer grouping, shading and resolve of its 128 samples. The tile's
 // list (TileList, chunk links, pool entries) is read through L2 (ld.cg): in a pipelined launch
 // another SM wrote it while this launch was running.
-template <uint32_t N, bool FMA>
+// ROW: the row of the offset tables (the rate's spiral row, or + 6 for the rotated grid), a
+// compile-time constant so that the offsets stay immediate constant-bank operands
+template <uint32_t N, bool FMA, int ROW>
 __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, ShadeSmem& sm, LightEnvDev& env, Mat4& M) {
     const ViewDev& V = fr.views[fr.viewCount == 1 ? 0u : __ldg(fr.blockView + gt / kTilesPerBlock)];
     const uint32_t tile = gt - V.tileStart;
@@ -505,7 +508,7 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         }
         return;
     }
-    const int rate = RateIndex<N>::v;
+    const int rate = ROW;
     for (uint32_t i = tid; i < sizeof(LightEnvDev) / 4; i += kTileSize)
         reinterpret_cast<uint32_t*>(&env)[i] = reinterpret_cast<const uint32_t*>(&V.env)[i];
     if (tid < 16) reinterpret_cast<float*>(&M)[tid] = reinterpret_cast<const float*>(&V.M)[tid];
@@ -737,25 +740,25 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
 // tile per CTA; kFromList walks the list with a grid-stride loop.
 enum : int { kFromOrder = 0, kFromReady = 1, kFromList = 2 };
 
-template <uint32_t N, bool FMA, int SRC>
+template <uint32_t N, bool FMA, int SRC, int ROW>
 __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel(FrameDev fr, ShadeSource src) {
     __shared__ ShadeSmem sm;
     __shared__ LightEnvDev env;
     __shared__ Mat4 M;
     if constexpr (SRC == kFromOrder) {
         const uint32_t gt = src.order ? src.order[src.first + blockIdx.x] : src.first + blockIdx.x;
-        shadeTile<N, FMA>(fr, gt, sm, env, M);
+        shadeTile<N, FMA, ROW>(fr, gt, sm, env, M);
     } else if constexpr (SRC == kFromReady) {
         __shared__ uint32_t readyTile;
         if (threadIdx.x == 0) readyTile = waitReady(src.ready + src.first + blockIdx.x, fr.counters);
         __syncthreads();
         const uint32_t gt = readyTile;
         if (gt & kReadyRetry) return; // culled and shaded by the retry passes (or the wait gave up)
-        shadeTile<N, FMA>(fr, gt, sm, env, M);
+        shadeTile<N, FMA, ROW>(fr, gt, sm, env, M);
     } else {
         const uint32_t count = *src.listCount;
         for (uint32_t item = blockIdx.x; item < count; item += gridDim.x) {
-            shadeTile<N, FMA>(fr, src.list[src.first + item], sm, env, M);
+            shadeTile<N, FMA, ROW>(fr, src.list[src.first + item], sm, env, M);
             __syncthreads();
         }
     }
@@ -1060,21 +1063,27 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr
 }
 
 template <uint32_t N>
-cudaError_t launchRate(const FrameDev& fr, bool fpStrict, bool dof, const uint32_t* order, uint32_t first,
-                       uint32_t count, cudaStream_t st) {
+cudaError_t launchRate(const FrameDev& fr, uint32_t pattern, bool fpStrict, bool dof, const uint32_t* order,
+                       uint32_t first, uint32_t count, cudaStream_t st) {
+    constexpr int S = RateIndex<N>::v, G = RateIndex<N>::v + 6; // spiral / rotated-grid offset rows
     if (dof) {
         if (fpStrict) intersectShadeDofKernel<N, false><<<count, kTileSize, 0, st>>>(fr, order, first);
         else intersectShadeDofKernel<N, true><<<count, kTileSize, 0, st>>>(fr, order, first);
     } else {
         const ShadeSource src{order, nullptr, nullptr, nullptr, first, count};
-        if (fpStrict) intersectShadeKernel<N, false, kFromOrder><<<count, kTileSize, 0, st>>>(fr, src);
-        else intersectShadeKernel<N, true, kFromOrder><<<count, kTileSize, 0, st>>>(fr, src);
+        if (fpStrict) {
+            if (pattern) intersectShadeKernel<N, false, kFromOrder, G><<<count, kTileSize, 0, st>>>(fr, src);
+            else intersectShadeKernel<N, false, kFromOrder, S><<<count, kTileSize, 0, st>>>(fr, src);
+        } else {
+            if (pattern) intersectShadeKernel<N, true, kFromOrder, G><<<count, kTileSize, 0, st>>>(fr, src);
+            else intersectShadeKernel<N, true, kFromOrder, S><<<count, kTileSize, 0, st>>>(fr, src);
+        }
     }
     return cudaGetLastError();
 }
 
 // The cull -> shade pipeline of one rate class (launchCullShadePipeline).
-template <uint32_t N, bool FMA>
+template <uint32_t N, bool FMA, int ROW>
 cudaError_t launchPipelineRate(const FrameDev& fr, uint32_t first, uint32_t count, uint32_t* queues, uint32_t* pipe,
                                uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
     cudaError_t e = launchTileCullMain(fr, fr.order, first, count, queues, warps, stackLimit, fr.ready, pipe, st);
@@ -1091,7 +1100,7 @@ cudaError_t launchPipelineRate(const FrameDev& fr, uint32_t first, uint32_t coun
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const ShadeSource ready{nullptr, fr.ready, nullptr, nullptr, first, count};
-    if ((e = cudaLaunchKernelEx(&cfg, intersectShadeKernel<N, FMA, kFromReady>, fr, ready)) != cudaSuccess) return e;
+    if ((e = cudaLaunchKernelEx(&cfg, intersectShadeKernel<N, FMA, kFromReady, ROW>, fr, ready)) != cudaSuccess) return e;
     // tiles whose stack outgrew the main pass: culled again, then shaded by a small grid that walks
     // the retry list (its length is only known on the device)
     if ((e = launchTileCullRetryPass(fr, fr.order, first, count, queues, st)) != cudaSuccess) return e;
@@ -1100,15 +1109,19 @@ cudaError_t launchPipelineRate(const FrameDev& fr, uint32_t first, uint32_t coun
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t grid = std::min<uint32_t>(count, uint32_t(2 * (sms > 0 ? sms : 148)));
     const ShadeSource retried{nullptr, nullptr, fr.retry, queues + 1, first, count};
-    intersectShadeKernel<N, FMA, kFromList><<<grid, kTileSize, 0, st>>>(fr, retried);
+    intersectShadeKernel<N, FMA, kFromList, ROW><<<grid, kTileSize, 0, st>>>(fr, retried);
     return cudaGetLastError();
 }
 
 template <uint32_t N>
-cudaError_t launchPipelineFp(const FrameDev& fr, bool fpStrict, uint32_t first, uint32_t count, uint32_t* queues,
-                             uint32_t* pipe, uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
-    return fpStrict ? launchPipelineRate<N, false>(fr, first, count, queues, pipe, warps, stackLimit, st)
-                    : launchPipelineRate<N, true>(fr, first, count, queues, pipe, warps, stackLimit, st);
+cudaError_t launchPipelineFp(const FrameDev& fr, uint32_t pattern, bool fpStrict, uint32_t first, uint32_t count,
+                             uint32_t* queues, uint32_t* pipe, uint32_t warps, uint32_t stackLimit, cudaStream_t st) {
+    constexpr int S = RateIndex<N>::v, G = RateIndex<N>::v + 6;
+    if (pattern)
+        return fpStrict ? launchPipelineRate<N, false, G>(fr, first, count, queues, pipe, warps, stackLimit, st)
+                        : launchPipelineRate<N, true, G>(fr, first, count, queues, pipe, warps, stackLimit, st);
+    return fpStrict ? launchPipelineRate<N, false, S>(fr, first, count, queues, pipe, warps, stackLimit, st)
+                    : launchPipelineRate<N, true, S>(fr, first, count, queues, pipe, warps, stackLimit, st);
 }
 
 // RemapKernel (libraries/hvvr/raycaster/remap.cu:35-77) for split-colour 1, 2 (pentile) and 3
@@ -1136,32 +1149,32 @@ __global__ void remapKernel(const uint32_t* __restrict__ src, const int32_t* __r
 
 } // namespace
 
-cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, bool fpStrict, bool dof, const uint32_t* order,
-                                 uint32_t first, uint32_t count, cudaStream_t st) {
+cudaError_t launchIntersectShade(const FrameDev& fr, uint32_t msaa, uint32_t pattern, bool fpStrict, bool dof,
+                                 const uint32_t* order, uint32_t first, uint32_t count, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     switch (msaa) {
-    case 1: return launchRate<1>(fr, fpStrict, dof, order, first, count, st);
-    case 2: return launchRate<2>(fr, fpStrict, dof, order, first, count, st);
-    case 4: return launchRate<4>(fr, fpStrict, dof, order, first, count, st);
-    case 8: return launchRate<8>(fr, fpStrict, dof, order, first, count, st);
-    case 16: return launchRate<16>(fr, fpStrict, dof, order, first, count, st);
-    case 32: return launchRate<32>(fr, fpStrict, dof, order, first, count, st);
+    case 1: return launchRate<1>(fr, pattern, fpStrict, dof, order, first, count, st);
+    case 2: return launchRate<2>(fr, pattern, fpStrict, dof, order, first, count, st);
+    case 4: return launchRate<4>(fr, pattern, fpStrict, dof, order, first, count, st);
+    case 8: return launchRate<8>(fr, pattern, fpStrict, dof, order, first, count, st);
+    case 16: return launchRate<16>(fr, pattern, fpStrict, dof, order, first, count, st);
+    case 32: return launchRate<32>(fr, pattern, fpStrict, dof, order, first, count, st);
     default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launchCullShadePipeline(const FrameDev& fr, uint32_t msaa, bool fpStrict, uint32_t first, uint32_t count,
-                                    uint32_t* queues, uint32_t* pipe, uint32_t warps, uint32_t stackLimit,
-                                    cudaStream_t st) {
+cudaError_t launchCullShadePipeline(const FrameDev& fr, uint32_t msaa, uint32_t pattern, bool fpStrict, uint32_t first,
+                                    uint32_t count, uint32_t* queues, uint32_t* pipe, uint32_t warps,
+                                    uint32_t stackLimit, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     if (!fr.ready) return cudaErrorInvalidValue;
     switch (msaa) {
-    case 1: return launchPipelineFp<1>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
-    case 2: return launchPipelineFp<2>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
-    case 4: return launchPipelineFp<4>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
-    case 8: return launchPipelineFp<8>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
-    case 16: return launchPipelineFp<16>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
-    case 32: return launchPipelineFp<32>(fr, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 1: return launchPipelineFp<1>(fr, pattern, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 2: return launchPipelineFp<2>(fr, pattern, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 4: return launchPipelineFp<4>(fr, pattern, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 8: return launchPipelineFp<8>(fr, pattern, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 16: return launchPipelineFp<16>(fr, pattern, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
+    case 32: return launchPipelineFp<32>(fr, pattern, fpStrict, first, count, queues, pipe, warps, stackLimit, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1174,7 +1187,7 @@ cudaError_t launchRemap(const CameraDev& c, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st) {
+cudaError_t uploadMsaaTable(uint32_t n, uint32_t pattern, const float* offsets, cudaStream_t st) {
     int idx = -1;
     switch (n) {
     case 1: idx = 0; break;
@@ -1185,6 +1198,8 @@ cudaError_t uploadMsaaTable(uint32_t n, const float* offsets, cudaStream_t st) {
     case 32: idx = 5; break;
     default: return cudaErrorInvalidValue;
     }
+    if (pattern > 1) return cudaErrorInvalidValue;
+    idx += 6 * int(pattern);
     cudaError_t e = cudaMemcpyToSymbolAsync(cMsaa, offsets, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
                                             cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;

@@ -320,6 +320,7 @@ public:
 
     // additions: the MSAA rate (1, 2, 4, 8, 16 or 32; default 16) and an eager sample setup
     void setMsaa(uint32_t rate) { check(hvvr_camera_set_msaa(_handle, rate), "Camera::setMsaa"); }
+    void setMsaaPattern(uint32_t pattern) { check(hvvr_camera_set_msaa_pattern(_handle, pattern), "Camera::setMsaaPattern"); }
     void prepare() { check(hvvr_camera_prepare(_handle, nullptr), "Camera::prepare"); }
     hvvr_camera* handle() const { return _handle; }
 

@@ -255,6 +255,14 @@ int hvvr_camera_prepare(hvvr_camera* cam, uint32_t* on_host);
 /* MSAA rate in {1,2,4,8,16,32}; the reference fixes it at compile time
  * (libraries/hvvr/raycaster/raycaster_common.h:27). Default 16. */
 int hvvr_camera_set_msaa(hvvr_camera* cam, uint32_t rate);
+/* The subsample pattern (no counterpart in the reference, which compiles in its spiral,
+ * libraries/hvvr/raycaster/gpu_samples.h:23-61): HVVR_MSAA_SPIRAL (default, the reference's) or
+ * HVVR_MSAA_ROTATED_GRID, an n-rooks lattice - subsample i in column i and row (k i) mod n of an
+ * n x n grid over the sample's [-1, 1]^2 unit offsets (k = 1, 3, 5, 9, 19 for n = 2, 4, 8, 16, 32),
+ * scaled by 1/sqrt(2) into the unit disk; at rate 1 the sample's centre. Thin-lens cameras use the
+ * spiral whatever the setting (the reference's lens table is built on it). */
+enum { HVVR_MSAA_SPIRAL = 0, HVVR_MSAA_ROTATED_GRID = 1 };
+int hvvr_camera_set_msaa_pattern(hvvr_camera* cam, uint32_t pattern);
 /* getSampleCount (camera.h:95; camera.cpp:162-164): valid (unpadded) sample count */
 int hvvr_camera_get_sample_count(const hvvr_camera* cam, uint32_t* count);
 
@@ -457,14 +465,15 @@ int hvvr_raycaster_read_kernel_times(const hvvr_raycaster* rc, float* ms4);
  * with the spec's tri_index_capacity) */
 int hvvr_raycaster_get_batch_config(hvvr_raycaster* rc, hvvr_batch_config* cfg);
 int hvvr_raycaster_set_batch_config(hvvr_raycaster* rc, const hvvr_batch_config* cfg);
-/* The last frame's launch timeline per part: rate class r (log2 MSAA, + 6 for thin-lens views)
- * runs as part 2r (its slowest tiles by the previous frame's cost, on a high-priority stream)
- * and part 2r+1 (the rest). ms72[3 * part + i] = tile cull start, tile cull end, intersect/shade
+/* The last frame's launch timeline per part: rate class r (log2 MSAA, + 6 for thin-lens views,
+ * + 12 for pinhole views with the rotated-grid pattern) runs as part 2r (its slowest tiles by the
+ * previous frame's cost, on a high-priority stream) and part 2r+1 (the rest).
+ * ms108[3 * part + i] = tile cull start, tile cull end, intersect/shade
  * end, in ms from the frame start; -1 for parts that did not run. In a pipelined part
  * (config.pipeline) the tile cull end reads -1 (the cull and the shade overlap).
  * Needs config.timing = 1. */
-int hvvr_batch_read_part_times(const hvvr_batch* batch, float* ms72);
-int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms72);
+int hvvr_batch_read_part_times(const hvvr_batch* batch, float* ms108);
+int hvvr_raycaster_read_part_times(const hvvr_raycaster* rc, float* ms108);
 /* counters of the last frame: [0] list-pool entries taken (whole chunks), [1] tiles culled
  * again with the 4096-entry stack, [2] device status bits, [3] views */
 int hvvr_batch_read_stats(const hvvr_batch* batch, uint64_t* out4);

@@ -1014,6 +1014,20 @@ extern "C" void oracle_msaa_offsets(uint32_t n, float* out) {
     }
 }
 
+// The library's alternative MSAA pattern (no counterpart in the reference, whose only pattern is
+// the spiral above): an n-rooks lattice, subsample i in column i and row (k i) mod n of an n x n
+// grid over [-1, 1]^2 (k = 1, 3, 5, 9, 19 for n = 2, 4, 8, 16, 32), scaled by 1/sqrt(2) into the
+// unit disk; n = 1 is the sample's centre.
+extern "C" void oracle_msaa_offsets_rotated_grid(uint32_t n, float* out) {
+    const uint32_t k = n == 2 ? 1u : n == 4 ? 3u : n == 8 ? 5u : n == 16 ? 9u : n == 32 ? 19u : 0u;
+    for (uint32_t i = 0; i < n; i++) {
+        const float x = float(2 * i + 1) / float(n) - 1.0f;
+        const float y = float(2 * ((k * i) % n) + 1) / float(n) - 1.0f;
+        out[2 * i + 0] = x * 0.70710677f;
+        out[2 * i + 1] = y * 0.70710677f;
+    }
+}
+
 // GPUCamera::initLookupTables (RC/gpu_camera.cu:59-88): DOF_LENS_POS_LOOKUP_TABLE_TILES (4) tiles of
 // per-sample random rotations of the spiral, subsample i taking spiral position (7 i + 7) mod n,
 // laid out [tile][subsample][sample]; std::mt19937 default seed, uniform_real_distribution<float>.
@@ -1161,7 +1175,10 @@ int renderCore(const oracle_frame_in* in, const SampleSetup& ss, const M4& c2w, 
 
     // MSAA offsets and the lighting environment (GPUSceneState::updateLighting, RC/gpu_scene_state.cu:47-81)
     std::vector<float> off(2 * N);
-    oracle_msaa_offsets(N, off.data());
+    // thin-lens views keep the spiral, which their lens table is built on
+    if (in->msaa_pattern == HVVR_MSAA_ROTATED_GRID && !(in->lens.radius > 0.0f))
+        oracle_msaa_offsets_rotated_grid(N, off.data());
+    else oracle_msaa_offsets(N, off.data());
     LightEnv env;
     for (uint32_t i = 0; i < in->light_count; i++) {
         const hvvr_light_union& l = in->lights[i];

@@ -42,6 +42,7 @@ typedef struct {
     uint32_t texture_count;
     void (*texture_sample)(void* ctx, uint32_t id, const float* q, float* rgba);
     void* texture_ctx;
+    uint32_t msaa_pattern;  /* HVVR_MSAA_SPIRAL (the reference's) or HVVR_MSAA_ROTATED_GRID */
 } oracle_frame_in;
 
 /* Texture samplers for oracle_frame_in.texture_sample (and the reference harness's texture hook).
@@ -107,6 +108,8 @@ int oracle_render(const oracle_frame_in* in, oracle_frame_out* out);
 int oracle_render_beams(const oracle_frame_in* in, const oracle_beams_in* beams, oracle_frame_out* out);
 /* MSAA unit offsets for rate n (n*2 floats), the spiral pattern of the reference */
 void oracle_msaa_offsets(uint32_t n, float* out);
+/* the library's n-rooks ("rotated grid") MSAA pattern for rate n (n*2 floats) */
+void oracle_msaa_offsets_rotated_grid(uint32_t n, float* out);
 /* depth-of-field lens positions for rate n: [4 tiles][n subsamples][128 samples] x 2 floats */
 void oracle_lens_table(uint32_t n, float* out);
 

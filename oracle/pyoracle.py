@@ -25,7 +25,8 @@ class FrameIn(C.Structure):
                 ("cam_xf", _abi.Transform), ("samples", C.c_void_p), ("sample_count", C.c_uint32),
                 ("split_color_samples", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
                 ("msaa", C.c_uint32), ("fp_mode", C.c_uint32), ("threads", C.c_uint32),
-                ("texture_count", C.c_uint32), ("texture_sample", C.c_void_p), ("texture_ctx", C.c_void_p)]
+                ("texture_count", C.c_uint32), ("texture_sample", C.c_void_p), ("texture_ctx", C.c_void_p),
+                ("msaa_pattern", C.c_uint32)]
 
 
 class FrameOut(C.Structure):
@@ -66,7 +67,7 @@ class Frame:
 
 def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi.HVVR_FP_FMA, lens=(0.0, 1.0),
          threads=None, split=1, want=("lists", "hits", "colors", "image", "blocks", "gbuffer", "scene", "beams"),
-         model_xf=None, tile_capacity=None, beams_in=None, textures=0, sampler=None):
+         model_xf=None, tile_capacity=None, beams_in=None, textures=0, sampler=None, msaa_pattern=0):
     # one scene, or a list of scenes (models of one raycaster, merged under root fix-up nodes as
     # Raycaster::buildScene does) with a list of model transforms; the lights are the first scene's
     models = list(scene) if isinstance(scene, (list, tuple)) else [scene]
@@ -106,6 +107,7 @@ def _run(fn, scene, samples, cam_xf, viewport, width, height, msaa, fp_mode=_abi
     # of a C sampler such as Oracle.hash_sampler / Oracle.table_sampler)
     fin.texture_count = textures
     fin.texture_sample = sampler
+    fin.msaa_pattern = msaa_pattern
     f = Frame()
     out = FrameOut()
     keep = []

@@ -69,3 +69,24 @@ def test_generator_is_stable():
     g, *_ = load("grid_msaa1")
     sc = scenes.make_scene(8, 40, 3)
     assert np.array_equal(sc.verts, g["in_verts"]) and np.array_equal(sc.tri_shade, g["in_tris"])
+
+
+def test_rotated_grid_offsets_are_n_rooks():
+    """The rotated-grid pattern: one subsample per column and per row of the n x n grid, inside the
+    unit disk the spiral fills, the sample's centre at rate 1."""
+    import ctypes as C
+    import pyoracle
+    lib = pyoracle.Oracle().lib
+    lib.oracle_msaa_offsets_rotated_grid.argtypes = [C.c_uint32, C.c_void_p]
+    lib.oracle_msaa_offsets_rotated_grid.restype = None
+    for n in (1, 2, 4, 8, 16, 32):
+        o = np.zeros(2 * n, np.float32)
+        lib.oracle_msaa_offsets_rotated_grid(n, o.ctypes.data)
+        xy = o.reshape(n, 2) / np.float32(0.70710677)
+        cols = np.rint((xy[:, 0] + 1) * n / 2 - 0.5).astype(int)
+        rows = np.rint((xy[:, 1] + 1) * n / 2 - 0.5).astype(int)
+        assert sorted(cols) == list(range(n)) and sorted(rows) == list(range(n))
+        assert (np.hypot(o[0::2], o[1::2]) <= 1.0).all()
+    o = np.zeros(2, np.float32)
+    lib.oracle_msaa_offsets_rotated_grid(1, o.ctypes.data)
+    assert (o == 0).all()
