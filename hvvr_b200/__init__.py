@@ -842,6 +842,10 @@ class Server:
         self.handle = h
         self.raycasters = list(raycasters)
         self.views = []
+        # CPU output arrays of requests in flight: the server writes a request's image into its
+        # array when the request completes, so the array is held here until poll() returns its
+        # completion (or the server is closed)
+        self._outputs = {}
         for r in self.raycasters:
             r.batches.append(self)  # closed before its raycasters
 
@@ -849,6 +853,7 @@ class Server:
         if self.handle:
             _check(_lib.hvvr_server_destroy(self.handle))
             self.handle = None
+            self._outputs.clear()
             for r in self.raycasters:
                 if self in r.batches:
                     r.batches.remove(self)
@@ -882,13 +887,18 @@ class Server:
             r.memory_type, r.output = HVVR_MEMORY_CPU, output.ctypes.data
         rid = C.c_uint64(0)
         _check(_lib.hvvr_server_submit(self.handle, C.byref(r), C.byref(rid)))
+        if device_ptr is None:
+            self._outputs[rid.value] = output
         return rid.value
 
     def poll(self, capacity=256, wait_ms=0.0):
         out = (_abi.Completion * capacity)()
         n = _u32(0)
         _check(_lib.hvvr_server_poll(self.handle, out, capacity, C.byref(n), C.c_double(wait_ms)))
-        return [out[i] for i in range(n.value)]
+        done = [out[i] for i in range(n.value)]
+        for c in done:
+            self._outputs.pop(c.id, None)
+        return done
 
     def update_vertices(self, model, first, count, device_ptr):
         _check(_lib.hvvr_server_update_vertices(self.handle, model.handle, first, count, _vp(device_ptr)))

@@ -21,9 +21,10 @@ namespace hvb {
 
 // unit offsets for rates 1,2,4,8,16,32: rows 0-5 the spiral, rows 6-11 the rotated grid
 __constant__ float2 cMsaa[12][32];
-// the same offsets split by axis, so that subsamples 2k and 2k+1 read as one 64-bit pair
-__constant__ __align__(8) float cMsaaX[12][32];
-__constant__ __align__(8) float cMsaaY[12][32];
+// each offset's x and y duplicated into both halves of a 64-bit pair, the operands of the packed
+// tests that run one subsample against two triangles
+__constant__ __align__(8) float2 cMsaaXX[12][32];
+__constant__ __align__(8) float2 cMsaaYY[12][32];
 
 namespace {
 
@@ -120,9 +121,17 @@ __device__ __forceinline__ P2 fma2(P2 a, P2 b, P2 c) {
     asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
     return r;
 }
+// The rounded product a*b of both lanes, written as fma(a, b, z) with z = (-0, -0): x + (-0) = x
+// for every x (zeros keep their sign), so this is exactly mul.rn.ftz. The compiler contracts a
+// packed mul.rn with the add that consumes it into one FMA, and it does the same to
+// fma(a, b, -0) when it can see the -0 (both measured on sm_100a: the uncontracted expressions
+// then round differently from their scalar forms). So z comes from constant memory that the host
+// writes at run time (cNegZero2, with the offset tables), a value the compiler cannot know: the
+// FMA stays a rounded product, and every product and sum below keeps its own rounding.
+__constant__ P2 cNegZero2;
 __device__ __forceinline__ P2 mul2(P2 a, P2 b) {
     P2 r;
-    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(cNegZero2));
     return r;
 }
 __device__ __forceinline__ P2 add2(P2 a, P2 b) {
@@ -136,32 +145,66 @@ __device__ __forceinline__ P2 sub2(P2 a, P2 b) {
     return r;
 }
 
-// a triangle's per-thread setup with every value duplicated into both lanes of a pair
-struct TriThread2 {
-    P2 dc, vc, wc, ddx, ddy, dvx, dvy, dwx, dwy, t;
+// exact negation of both lanes (a sign-bit flip, as the scalar unary minus)
+__device__ __forceinline__ P2 neg2(P2 a) { return a ^ 0x8000000080000000ull; }
+
+struct V2 {
+    P2 x, y, z;
 };
-__device__ __forceinline__ TriThread2 pairSetup(const TriThread& th, float t) {
-    return TriThread2{pk(th.dc, th.dc),   pk(th.vc, th.vc),   pk(th.wc, th.wc),   pk(th.ddx, th.ddx),
-                      pk(th.ddy, th.ddy), pk(th.dvx, th.dvx), pk(th.dvy, th.dvy), pk(th.dwx, th.dwx),
-                      pk(th.dwy, th.dwy), pk(t, t)};
+// dot3 / cross3 (same association) on two triangles at once
+__device__ __forceinline__ P2 dot2(const V2& a, const V2& b) {
+    return add2(add2(mul2(a.x, b.x), mul2(a.y, b.y)), mul2(a.z, b.z));
+}
+__device__ __forceinline__ V2 cross2(const V2& a, const V2& b) {
+    return V2{sub2(mul2(a.y, b.z), mul2(a.z, b.y)), sub2(mul2(a.z, b.x), mul2(a.x, b.z)),
+              sub2(mul2(a.x, b.y), mul2(a.y, b.x))};
 }
 
-// threadTest for subsamples 2k and 2k+1 at once (ax, ay: their unit offsets as pairs), with the
-// scalar test's operations in its order: denom, depthDelta, v, w as FMA chains (FMA) or as rounded
-// products and sums (STRICT), u = (denom - v) - w, the sign-bit test and the depth update.
+// threadSetupN for two triangles j, k (lane 0 / lane 1 of every pair) against this thread's
+// sample: nc, ndu, ndv are -c, -du, -dv duplicated into both lanes
+struct TriPair {
+    P2 dc, vc, wc, ddx, ddy, dvx, dvy, dwx, dwy;
+};
+__device__ __forceinline__ TriPair pairSetup(const V2& n, const V2& e0, const V2& e1, const V2& v0r, const V2& nc,
+                                             const V2& ndu, const V2& ndv) {
+    TriPair r;
+    r.dc = dot2(nc, n);
+    const V2 ec = cross2(nc, v0r);
+    r.vc = dot2(e1, ec);
+    r.wc = neg2(dot2(e0, ec));
+    r.ddx = dot2(ndu, n);
+    r.ddy = dot2(ndv, n);
+    const V2 cu = cross2(ndu, v0r), cv = cross2(ndv, v0r);
+    r.dvx = dot2(e1, cu);
+    r.dvy = dot2(e1, cv);
+    r.dwx = neg2(dot2(e0, cu));
+    r.dwy = neg2(dot2(e0, cv));
+    return r;
+}
+
+__device__ __forceinline__ bool signsClear(float a, float b, float c, float d) {
+    return (__float_as_int(a) | __float_as_int(b) | __float_as_int(c) | __float_as_int(d)) >= 0;
+}
+
+// threadTest of one subsample (unit offset ax, ay duplicated into both lanes) against triangles j
+// and k in that order, with the scalar test's operations in its order: denom, depthDelta, v, w as
+// FMA chains (FMA) or as rounded products and sums (STRICT), u = (denom - v) - w, the sign-bit test
+// and the depth update. Both depth deltas are formed from the depth before j; when j hits, k's is
+// formed again from the new depth, so k sees exactly the depth the sequential fold gives it.
+// tt holds (-t_j, -t_k) in FMA mode, (t_j, t_k) in STRICT mode.
 template <bool FMA>
-__device__ __forceinline__ void threadTest2(const TriThread2& p, float t, P2 ax, P2 ay, float& depth0, float& depth1,
-                                            uint32_t& hit0, uint32_t& hit1, uint32_t idx) {
-    const P2 depth = pk(depth0, depth1);
+__device__ __forceinline__ void pairTest(const TriPair& p, P2 tt, float tj, float tk, uint32_t ij, uint32_t ik,
+                                         P2 ax, P2 ay, float& depth, uint32_t& hit) {
+    const P2 d2 = pk(depth, depth);
     P2 denom, dd, v, w;
     if (FMA) {
         denom = fma2(p.ddy, ay, fma2(p.ddx, ax, p.dc));
-        dd = fma2(depth, denom, p.t); // p.t holds -t in FMA mode
+        dd = fma2(d2, denom, tt);
         v = fma2(p.dvy, ay, fma2(p.dvx, ax, p.vc));
         w = fma2(p.dwy, ay, fma2(p.dwx, ax, p.wc));
     } else {
         denom = add2(add2(p.dc, mul2(p.ddx, ax)), mul2(p.ddy, ay));
-        dd = sub2(mul2(depth, denom), p.t);
+        dd = sub2(mul2(d2, denom), tt);
         v = add2(add2(p.vc, mul2(p.dvx, ax)), mul2(p.dvy, ay));
         w = add2(add2(p.wc, mul2(p.dwx, ax)), mul2(p.dwy, ay));
     }
@@ -172,13 +215,14 @@ __device__ __forceinline__ void threadTest2(const TriThread2& p, float t, P2 ax,
     upk(u, u0, u1);
     upk(v, v0, v1);
     upk(w, w0, w1);
-    if ((__float_as_int(dd0) | __float_as_int(u0) | __float_as_int(v0) | __float_as_int(w0)) >= 0) {
-        depth0 = t * (1.0f / den0);
-        hit0 = idx;
+    if (signsClear(dd0, u0, v0, w0)) {
+        depth = tj * (1.0f / den0);
+        hit = ij;
+        dd1 = FMA ? fmaf(depth, den1, -tk) : depth * den1 - tk;
     }
-    if ((__float_as_int(dd1) | __float_as_int(u1) | __float_as_int(v1) | __float_as_int(w1)) >= 0) {
-        depth1 = t * (1.0f / den1);
-        hit1 = idx;
+    if (signsClear(dd1, u1, v1, w1)) {
+        depth = tk * (1.0f / den1);
+        hit = ik;
     }
 }
 
@@ -440,10 +484,13 @@ __device__ __forceinline__ bool uvwAllOut(const float (&ro)[4][3], const float (
 struct ShadeSmem {
     float ro[4][3], rd[4][3]; // world corner rays
     float pl[4][4];           // frustum planes
-    // the chunk's surviving triangles, one 16-byte record each (read by all threads at once):
-    // {e0, t}, {e1, |e0 x e1|} (the norm as computed in float, for the depth skip),
-    // {camPos - v0, index}, {e0 x e1, 0}
-    float4 te0[kChunk], te1[kChunk], tvr[kChunk], tn[kChunk];
+    // the chunk's surviving triangles, one array per component (a warp reads the same entry on
+    // every lane, and a pair of entries j, k loads straight into the two halves of a register
+    // pair): e0, e1, camPos - v0, e0 x e1, t, |e0 x e1| (the norm as computed in float, for the
+    // depth skip) and the triangle index
+    float g[12][kChunk];
+    float t[kChunk], nlen[kChunk];
+    uint32_t idx[kChunk];
     uint32_t warpCount[4];
 };
 
@@ -536,16 +583,29 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
     }
     const F3 camPos = f3(M.m[3][0], M.m[3][1], M.m[3][2]);
     // this thread's beam, rotated to world space (GetDirectionalSample3D, gpu_samples.h:78-82)
-    const float4* __restrict__ beams = V.beams;
-    const float4 b0 = __ldg(beams + 3 * size_t(sid) + 0);
-    const float4 b1 = __ldg(beams + 3 * size_t(sid) + 1);
-    const float4 b2 = __ldg(beams + 3 * size_t(sid) + 2);
-    const F3 c = xformDir(M, f3(b0.x, b0.y, b0.z));
-    const F3 du = xformDir(M, f3(b0.w, b1.x, b1.y));
-    const F3 dv = xformDir(M, f3(b1.z, b1.w, b2.x));
-    // Upper bound on |denom| / |e0 x e1| over this sample's subsamples: denom = -dir . n with
-    // dir = c + ax du + ay dv and |ax|,|ay| <= 1, so |denom| <= (|c| + |du| + |dv|) |n|.
-    const float dirLen = (sqrtf(dot3(c, c)) + sqrtf(dot3(du, du)) + sqrtf(dot3(dv, dv))) * 1.0001f;
+    // this thread's beam, rotated to world space (GetDirectionalSample3D, gpu_samples.h:78-82): c,
+    // du, dv; loaded again after the triangle loop so that they need no registers during it
+    auto beamDirs = [&](F3& c, F3& du, F3& dv) {
+        const float4* __restrict__ beams = V.beams;
+        const float4 b0 = __ldg(beams + 3 * size_t(sid) + 0);
+        const float4 b1 = __ldg(beams + 3 * size_t(sid) + 1);
+        const float4 b2 = __ldg(beams + 3 * size_t(sid) + 2);
+        c = xformDir(M, f3(b0.x, b0.y, b0.z));
+        du = xformDir(M, f3(b0.w, b1.x, b1.y));
+        dv = xformDir(M, f3(b1.z, b1.w, b2.x));
+    };
+    float dirLen;
+    V2 nc, ndu, ndv; // -c, -du, -dv in both lanes, for the two-triangle setup
+    {
+        F3 c, du, dv;
+        beamDirs(c, du, dv);
+        // Upper bound on |denom| / |e0 x e1| over this sample's subsamples: denom = -dir . n with
+        // dir = c + ax du + ay dv and |ax|,|ay| <= 1, so |denom| <= (|c| + |du| + |dv|) |n|.
+        dirLen = (sqrtf(dot3(c, c)) + sqrtf(dot3(du, du)) + sqrtf(dot3(dv, dv))) * 1.0001f;
+        nc = V2{pk(-c.x, -c.x), pk(-c.y, -c.y), pk(-c.z, -c.z)};
+        ndu = V2{pk(-du.x, -du.x), pk(-du.y, -du.y), pk(-du.z, -du.z)};
+        ndv = V2{pk(-dv.x, -dv.x), pk(-dv.y, -dv.y), pk(-dv.z, -dv.z)};
+    }
     float tmax[N];
     uint32_t hit[N];
 #pragma unroll
@@ -608,47 +668,68 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
             total += cw;
         }
         if (keep) {
-            sm.te0[off] = make_float4(e0.x, e0.y, e0.z, t);
-            sm.te1[off] = make_float4(e1.x, e1.y, e1.z, nlen);
-            sm.tvr[off] = make_float4(v0r.x, v0r.y, v0r.z, __uint_as_float(idx));
-            sm.tn[off] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+            sm.g[0][off] = e0.x; sm.g[1][off] = e0.y; sm.g[2][off] = e0.z;
+            sm.g[3][off] = e1.x; sm.g[4][off] = e1.y; sm.g[5][off] = e1.z;
+            sm.g[6][off] = v0r.x; sm.g[7][off] = v0r.y; sm.g[8][off] = v0r.z;
+            sm.g[9][off] = nrm.x; sm.g[10][off] = nrm.y; sm.g[11][off] = nrm.z;
+            sm.t[off] = t;
+            sm.nlen[off] = nlen;
+            sm.idx[off] = idx;
         }
         __syncthreads();
         // Depth skip. The test rejects a subsample when depth * denom < t (FMA mode, exactly;
         // STRICT mode with the product rounded, covered by the 1e-4 margin in dirLen). With
         // denom <= dirLen * |n| and depth <= laneT, t > laneT * dirLen * |n| rejects every
-        // subsample of the lane; a triangle is skipped only when that holds for all 32 lanes,
-        // so the hits are exactly those of the full loop. Misses keep laneT at FLT_MAX (no skip).
+        // subsample of the lane; a triangle is skipped only when that holds for all 32 lanes, so
+        // the hits are exactly those of the full loop. Misses keep laneT at FLT_MAX (no skip).
+        // For |n| >= 0 the rounded product is monotone in the bound, so "for all lanes" is the
+        // test against the warp's largest bound, and lane l evaluates it for survivor g + l: one
+        // ballot decides 32 survivors. The bound is taken at the start of each group of 32; depths
+        // only fall, so a bound taken earlier is larger and skips no triangle that could hit.
+        //
+        // The triangles that are not skipped are tested two at a time, in list order: j in lane 0
+        // and k in lane 1 of every packed operation (pairTest). An odd one left at the end of the
+        // chunk is tested as the pair (j, j): a second test of the same triangle on the same
+        // subsample changes nothing (it either fails or writes the same depth and index again).
         survivors += total;
-        float laneT = 0.0f;
+        uint32_t pend = ~0u; // a triangle waiting for its pair partner
+        auto testPair = [&](uint32_t j, uint32_t k) {
+            const V2 e0 = {pk(sm.g[0][j], sm.g[0][k]), pk(sm.g[1][j], sm.g[1][k]), pk(sm.g[2][j], sm.g[2][k])};
+            const V2 e1 = {pk(sm.g[3][j], sm.g[3][k]), pk(sm.g[4][j], sm.g[4][k]), pk(sm.g[5][j], sm.g[5][k])};
+            const V2 vr = {pk(sm.g[6][j], sm.g[6][k]), pk(sm.g[7][j], sm.g[7][k]), pk(sm.g[8][j], sm.g[8][k])};
+            const V2 nn = {pk(sm.g[9][j], sm.g[9][k]), pk(sm.g[10][j], sm.g[10][k]), pk(sm.g[11][j], sm.g[11][k])};
+            const float tj = sm.t[j], tk = sm.t[k];
+            const uint32_t ij = sm.idx[j], ik = sm.idx[k];
+            const TriPair tp = pairSetup(nn, e0, e1, vr, nc, ndu, ndv);
+            const P2 tt = FMA ? pk(-tj, -tk) : pk(tj, tk);
 #pragma unroll
-        for (uint32_t i = 0; i < N; i++) laneT = fmaxf(laneT, tmax[i]);
-        const float laneBound = laneT * dirLen;
-        for (uint32_t j = 0; j < total; j++) {
-            const float4 a0 = sm.te0[j], a1 = sm.te1[j];
-            if (__all_sync(kFull, a0.w > laneBound * a1.w)) continue;
-            ++tested;
-            const float4 a2 = sm.tvr[j], a3 = sm.tn[j];
-            const F3 je0 = f3(a0.x, a0.y, a0.z);
-            const F3 je1 = f3(a1.x, a1.y, a1.z);
-            const F3 jvr = f3(a2.x, a2.y, a2.z);
-            const float jt = a0.w;
-            const uint32_t jidx = __float_as_uint(a2.w);
-            const TriThread th = threadSetupN(f3(a3.x, a3.y, a3.z), je0, je1, jvr, c, du, dv);
-            if (N == 1) {
-                const float2 a = cMsaa[rate][0];
-                if (threadTest<FMA>(th, jt, a.x, a.y, tmax[0])) hit[0] = jidx;
-            } else {
-                // subsamples in pairs on the packed FP32 path
-                const TriThread2 p = pairSetup(th, FMA ? -jt : jt);
+            for (uint32_t i = 0; i < N; i++) {
+                const P2 ax = *reinterpret_cast<const P2*>(&cMsaaXX[rate][i]);
+                const P2 ay = *reinterpret_cast<const P2*>(&cMsaaYY[rate][i]);
+                pairTest<FMA>(tp, tt, tj, tk, ij, ik, ax, ay, tmax[i], hit[i]);
+            }
+        };
+        for (uint32_t g0 = 0; g0 < total; g0 += 32) {
+            float laneT = 0.0f;
 #pragma unroll
-                for (uint32_t i = 0; i + 1 < N; i += 2) {
-                    const P2 ax = *reinterpret_cast<const P2*>(&cMsaaX[rate][i]);
-                    const P2 ay = *reinterpret_cast<const P2*>(&cMsaaY[rate][i]);
-                    threadTest2<FMA>(p, jt, ax, ay, tmax[i], tmax[i + 1], hit[i], hit[i + 1], jidx);
+            for (uint32_t i = 0; i < N; i++) laneT = fmaxf(laneT, tmax[i]);
+            const float bound = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(laneT * dirLen)));
+            const uint32_t js = g0 + lane;
+            const bool skip = js < total && sm.t[js] > bound * sm.nlen[js];
+            uint32_t live = __ballot_sync(kFull, js < total && !skip);
+            tested += __popc(live);
+            while (live) {
+                const uint32_t j = g0 + uint32_t(__ffs(live) - 1);
+                live &= live - 1u;
+                if (pend == ~0u) {
+                    pend = j;
+                } else {
+                    testPair(pend, j);
+                    pend = ~0u;
                 }
             }
         }
+        if (pend != ~0u) testPair(pend, pend);
         __syncthreads();
         remaining -= n;
         chunk = nextChunk;
@@ -656,6 +737,8 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
 
     if (tid == 0 && survivors) atomicAdd(&fr.counters[kSurvivorWord], survivors);
     if (lane == 0 && tested) atomicAdd(&fr.counters[kTestedWord], tested);
+    F3 c, du, dv;
+    beamDirs(c, du, dv);
     if (uint32_t* hitOut = viewPtr(V.hitIds)) {
         float* depthOut = viewPtr(V.depth);
 #pragma unroll
@@ -1200,19 +1283,24 @@ cudaError_t uploadMsaaTable(uint32_t n, uint32_t pattern, const float* offsets, 
     }
     if (pattern > 1) return cudaErrorInvalidValue;
     idx += 6 * int(pattern);
+    // the packed products' addend (-0, -0), written with every table upload (mul2)
+    const unsigned long long negZero2 = 0x8000000080000000ull;
+    cudaError_t ez = cudaMemcpyToSymbolAsync(cNegZero2, &negZero2, sizeof(negZero2), 0, cudaMemcpyHostToDevice, st);
+    if (ez != cudaSuccess) return ez;
     cudaError_t e = cudaMemcpyToSymbolAsync(cMsaa, offsets, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
                                             cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
-    // the per-axis copies (pageable host staging: the copy completes before the call returns)
-    float xs[32], ys[32];
+    // the duplicated per-axis copies (pageable host staging: the copy completes before the call returns)
+    float2 xs[32], ys[32];
     for (uint32_t i = 0; i < n; i++) {
-        xs[i] = offsets[2 * i];
-        ys[i] = offsets[2 * i + 1];
+        xs[i] = make_float2(offsets[2 * i], offsets[2 * i]);
+        ys[i] = make_float2(offsets[2 * i + 1], offsets[2 * i + 1]);
     }
-    e = cudaMemcpyToSymbolAsync(cMsaaX, xs, n * sizeof(float), size_t(idx) * 32 * sizeof(float), cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyToSymbolAsync(cMsaaXX, xs, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
+                                cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
-    return cudaMemcpyToSymbolAsync(cMsaaY, ys, n * sizeof(float), size_t(idx) * 32 * sizeof(float), cudaMemcpyHostToDevice,
-                                   st);
+    return cudaMemcpyToSymbolAsync(cMsaaYY, ys, n * sizeof(float2), size_t(idx) * 32 * sizeof(float2),
+                                   cudaMemcpyHostToDevice, st);
 }
 
 } // namespace hvb

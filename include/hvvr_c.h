@@ -523,7 +523,9 @@ typedef struct {
     uint32_t msaa;                /* 1,2,4,8,16,32 */
     hvvr_transform camera_to_world;
     uint32_t memory_type;         /* HVVR_MEMORY_CPU or HVVR_MEMORY_CUDA */
-    void* output;                 /* width x height RGBA8 (sRGB) pixels, row stride = width */
+    void* output;                 /* width x height RGBA8 (sRGB) pixels, row stride = width; the
+                                     server writes it when the request completes, so it must stay
+                                     valid until hvvr_server_poll has returned the completion */
     uint64_t tag;                 /* returned with the completion */
     uint32_t priority;            /* 0: throughput class (batched); 1: latency class (e.g. the eyes of a
                                      stereo frame): dispatched ahead of the throughput class on a

@@ -220,10 +220,12 @@ def test_latency_class_jumps_a_busy_mix(oracle):
     ssmp = scenes.barrel_samples(sw, sh)
     stereo = srv.add_view(0, scenes.viewport_for(sw, sh), ssmp, sw, sh)
     rng = np.random.default_rng(9)
+    busy = []  # the throughput requests' outputs, alive until their completions arrive
     for k in range(32):
         vid, w, h = tmpl[k % len(tmpl)]
         xf = scenes.camera_transform(eye=(float(rng.uniform(-4, 4)), 2.0, 9.0))
-        srv.submit(vid, 16, xf, output=np.zeros((h, w), dtype=np.uint32), tag=k)
+        busy.append(np.zeros((h, w), dtype=np.uint32))
+        srv.submit(vid, 16, xf, output=busy[-1], tag=k)
     eyes = scenes.stereo_eyes(0.064)
     outs = []
     for e, xf in enumerate(eyes):
