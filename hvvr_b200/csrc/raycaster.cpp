@@ -606,9 +606,11 @@ int cloneCamera(const hvvr_camera* src, hvvr_camera** out) {
 constexpr uint32_t kSplitMinTiles = 32;
 
 void batchConfigDefault(hvvr_batch_config* c) {
-    c->tile_cull_warps = 4;
-    // 1/8 was fastest on the 1M-triangle stereo 2x1080x1200 frame (1/4 and 1/16 within 1%,
-    // no split 4.5% slower)
+    // On the 1M-triangle stereo 2x1080x1200 8xMSAA frame, one-warp cull CTAs with the slowest 1/8
+    // of the tiles as the heavy part were fastest: 5.30 ms against 5.45 with 4-warp CTAs (a warp
+    // that runs out of tiles frees its registers for the shade of finished tiles at once);
+    // heavy shares 1/4 and 1/16 were 5.55 and 5.73 ms, no split 5.97
+    c->tile_cull_warps = 1;
     c->heavy_divisor = 8;
     c->tri_index_capacity = kDefaultCapacity;
     c->use_graph = 1;

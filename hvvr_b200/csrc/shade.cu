@@ -492,7 +492,20 @@ struct ShadeSmem {
     float t[kChunk], nlen[kChunk];
     uint32_t idx[kChunk];
     uint32_t warpCount[4];
+    // the list triangles of the chunk being culled, 48 bytes per entry (three float4 rows of the
+    // triangle array), copied in by cp.async one chunk ahead; thread i writes and reads only
+    // entry i, so the copy of the next chunk can start as soon as entry i has been read
+    float4 stage[3 * kChunk];
 };
+
+// cp.async of 16 bytes, global to shared, cached in L2 only (the triangle rows are gathered once
+// per tile; neighbouring tiles share them through L2)
+__device__ __forceinline__ void cpAsync16(void* dst, const void* src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // resident CTAs per SM the register allocation must allow (7 = 72 registers per thread)
 // resident CTAs per SM: N <= 8 at 72 registers; N = 16 at 96 (a few spilled bytes, 5.5% faster on
@@ -615,19 +628,35 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
     }
     __syncthreads();
 
+    // The list is consumed chunk by chunk. Entry tid of a chunk is staged into shared memory by
+    // cp.async (the 48-byte triangle record that its index names) while the CTA is still testing
+    // the previous chunk, so the gathers overlap the subsample tests.
+    const float4* __restrict__ trisG = viewPtr(V.tris);
+    auto stage = [&](uint32_t ix) {
+        const float4* src = trisG + 3 * size_t(ix);
+        cpAsync16(&sm.stage[3 * tid + 0], src + 0);
+        cpAsync16(&sm.stage[3 * tid + 1], src + 1);
+        cpAsync16(&sm.stage[3 * tid + 2], src + 2);
+    };
     uint32_t chunk = L.first;
     uint32_t remaining = L.count;
     uint32_t survivors = 0, tested = 0;
+    uint32_t idx = 0;
+    if (chunk < fr.poolChunks && tid < (remaining < kChunk ? remaining : kChunk)) {
+        idx = __ldcg(fr.pool + size_t(chunk) * kChunk + tid);
+        stage(idx);
+    }
+    cpAsyncCommit();
     while (remaining > 0 && chunk < fr.poolChunks) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
         const uint32_t nextChunk = __ldcg(fr.chunkNext + chunk);
         bool keep = false;
-        uint32_t idx = 0;
         float t = 0.0f, nlen = 0.0f;
         F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0), nrm = f3(0, 0, 0);
+        cpAsyncWaitAll();
         if (tid < n) {
-            idx = __ldcg(fr.pool + size_t(chunk) * kChunk + tid);
-            const TriGeom tri = loadTri(viewPtr(V.tris), idx);
+            const float4 ra = sm.stage[3 * tid + 0], rb = sm.stage[3 * tid + 1], rc = sm.stage[3 * tid + 2];
+            const TriGeom tri{f3(ra.x, ra.y, ra.z), f3(ra.w, rb.x, rb.y), f3(rb.z, rb.w, rc.x)};
             // FrustumPlanes::test
             bool in = true;
 #pragma unroll
@@ -656,6 +685,11 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
                 }
             }
         }
+        // the next chunk's index of this entry (its chunk link has arrived by now)
+        const uint32_t rest = remaining - n;
+        const bool more = rest > 0 && nextChunk < fr.poolChunks;
+        uint32_t idxNext = 0;
+        if (more && tid < (rest < kChunk ? rest : kChunk)) idxNext = __ldcg(fr.pool + size_t(nextChunk) * kChunk + tid);
         const uint32_t bal = __ballot_sync(kFull, keep);
         if (lane == 0) sm.warpCount[warp] = __popc(bal);
         __syncthreads();
@@ -677,6 +711,9 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
             sm.idx[off] = idx;
         }
         __syncthreads();
+        // stage the next chunk (this thread's entry of this chunk was read above)
+        if (more && tid < (rest < kChunk ? rest : kChunk)) stage(idxNext);
+        cpAsyncCommit();
         // Depth skip. The test rejects a subsample when depth * denom < t (FMA mode, exactly;
         // STRICT mode with the product rounded, covered by the 1e-4 margin in dirLen). With
         // denom <= dirLen * |n| and depth <= laneT, t > laneT * dirLen * |n| rejects every
@@ -733,6 +770,7 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         __syncthreads();
         remaining -= n;
         chunk = nextChunk;
+        idx = idxNext;
     }
 
     if (tid == 0 && survivors) atomicAdd(&fr.counters[kSurvivorWord], survivors);

@@ -577,7 +577,9 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
             if (mask && s.mask[top] == 0u) {
                 int k = __ffs(mask) - 1;
                 if (!(mask & (mask - 1))) {
-                    node = childNode[k];
+                    // (child indices by shuffle: a register array indexed at run time would live
+                    // in local memory)
+                    node = node + __float_as_uint(__shfl_sync(kFull, v, 26 + k));
                     v = vc[0];
 #pragma unroll
                     for (int q = 1; q < 4; q++)
@@ -607,7 +609,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                         const int kk = mm ? __ffs(mm) - 1 : 0;
                         ck[i] = __uint_as_float(__float_as_uint(__shfl_sync(kFull, v, distIdx * 4 + kk)) ^ 0x80000000u);
                         ckz[i] = dazf(ck[i]);
-                        cnode[i] = childNode[kk];
+                        cnode[i] = node + __float_as_uint(__shfl_sync(kFull, v, 26 + kk));
                         if (mm) maxKey = fmaxf(maxKey, ckz[i]);
                         mm &= mm - 1;
                     }

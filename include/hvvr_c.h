@@ -414,7 +414,7 @@ int hvvr_polar_foveated_samples(const hvvr_spec* spec, float* beams9, uint32_t* 
  * that rendered it last. Destroy batches before their raycasters; a batch whose raycaster
  * was destroyed returns HVVR_ERR_STATE. */
 typedef struct {
-    uint32_t tile_cull_warps;     /* warps per CTA of the tile-cull work queue: 1, 2, 4 or 8 */
+    uint32_t tile_cull_warps;     /* warps per CTA of the tile-cull work queue: 1 (default), 2, 4 or 8 */
     uint32_t heavy_divisor;       /* 1/heavy_divisor of each rate's tiles (last frame's slowest) are
                                      culled and shaded on their own stream; 0 = no split */
     uint64_t tri_index_capacity;  /* triangle-list pool entries shared by all views */

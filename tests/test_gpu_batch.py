@@ -91,7 +91,7 @@ def test_batch_matches_single_view_and_autotune():
     ref_img = cam.image.copy()
     batch = hv.Batch([rc])
     cfg = batch.autotune(frames=2)
-    assert cfg.tile_cull_warps in (2, 4, 8) and cfg.frame_ms > 0
+    assert cfg.tile_cull_warps in (1, 2, 4, 8) and cfg.frame_ms > 0
     assert cfg.tri_index_capacity >= 1 << 20
     for _ in range(3):
         batch.render()
