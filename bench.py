@@ -973,8 +973,9 @@ def run_foveated(args):
         c.set_capture(hv.HVVR_CAPTURE_HITS)
     rc.render()
     rc.render()
+    ctr = rc.counters()
     counts = {"padded_samples": 0, "tiles": 0, "list_entries": 0, "unique_hits": 0, "node_visits": 0,
-              "tested_entries": int(rc.counters()[4])}
+              "tested_entries": int(ctr[4]), "tested_warp_entries": int(ctr[5])}
     for cam in cams:
         blocks, tiles, padded, msaa = cam.layout()
         n, tri, mask = cam.gbuffer()

@@ -213,14 +213,18 @@ __device__ __forceinline__ ChildBox childBox(float v) {
     return b;
 }
 
-// bit c set where byte c of m is all ones / nonzero
+// Bit c set where byte c of m is all ones / nonzero. Per byte, (b & 0x7f) + 0x7f sets the byte's
+// high bit exactly when its low seven bits are not all zero and never carries into the next byte
+// (at most 0xfe), so the byte tests are exact; the multiply gathers bits 7, 15, 23, 31 into bits
+// 21-24 (the partial products land on distinct bits, so nothing carries).
+__device__ __forceinline__ uint32_t gatherByteFlags(uint32_t z) { return (((z >> 7) * 0x204081u) >> 21) & 0xfu; }
 __device__ __forceinline__ uint32_t bytesAllOnes(uint32_t m) {
-    const uint32_t x = __vcmpeq4(m, 0xffffffffu);
-    return ((x >> 7) & 1u) | ((x >> 14) & 2u) | ((x >> 21) & 4u) | ((x >> 28) & 8u);
+    const uint32_t s = (~m & 0x7f7f7f7fu) + 0x7f7f7f7fu; // high bit: the byte of ~m has a low bit set
+    return gatherByteFlags(~s & m & 0x80808080u);
 }
 __device__ __forceinline__ uint32_t bytesNonZero(uint32_t m) {
-    const uint32_t x = __vcmpne4(m, 0u);
-    return ((x >> 7) & 1u) | ((x >> 14) & 2u) | ((x >> 21) & 4u) | ((x >> 28) & 8u);
+    const uint32_t s = (m & 0x7f7f7f7fu) + 0x7f7f7f7fu;
+    return gatherByteFlags((s | m) & 0x80808080u);
 }
 
 // Frustum::testBVHNodeChildren (traverse_avx.h:104-164)
