@@ -885,9 +885,9 @@ def run_served(args):
         "config": {"workload": "render server: 6 resident scenes (0.1M-4.1M tris), %d view templates + stereo "
                                "2x1080x1200 8xMSAA (5%% of requests), Poisson arrivals %s req/s for %.1f s each, "
                                "120 GiB HBM budget, 3 throughput slots x %d views + 1 latency slot (stereo pairs as "
-                               "the latency class), throughput tile-cull cap %d CTAs/SM, backlog limit %d, instances "
-                               "pre-warmed" % (len(tmpl), args.rates, args.seconds, args.max_batch_views,
-                                               args.served_cull_cap, BACKLOG),
+                               "the latency class; latency isolation: the throughput slots cull a tile per warp "
+                               "without the cull -> shade pipeline), backlog limit %d, instances "
+                               "pre-warmed" % (len(tmpl), args.rates, args.seconds, args.max_batch_views, BACKLOG),
                    "l2": "inputs larger than L2"},
         "sweep": sweep, "served_vs_plain_image_match": "%d/%d" % (matches, checks),
         "host_setup_s": setup_s, "clocks": ck,

@@ -115,14 +115,15 @@ class BatchConfig(C.Structure):
     """hvvr_batch_config: knobs of a frame batch (set by hand or by hvvr_batch_autotune)."""
     _fields_ = [("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32), ("tri_index_capacity", C.c_uint64),
                 ("use_graph", C.c_uint32), ("frame_ms", C.c_float), ("tile_stack_entries", C.c_uint32),
-                ("timing", C.c_uint32), ("pipeline", C.c_uint32), ("tile_cull_ctas_per_sm", C.c_uint32)]
+                ("timing", C.c_uint32), ("pipeline", C.c_uint32), ("tile_cull_ctas_per_sm", C.c_uint32),
+                ("tile_cull_persistent", C.c_uint32)]
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch_views", C.c_uint32),
                 ("slot_list_capacity", C.c_uint64), ("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32),
                 ("min_batch_views", C.c_uint32), ("max_wait_ms", C.c_float), ("latency_slots", C.c_uint32),
-                ("tile_cull_ctas_per_sm", C.c_uint32)]
+                ("tile_cull_ctas_per_sm", C.c_uint32), ("latency_isolation", C.c_uint32)]
 
 
 class Request(C.Structure):

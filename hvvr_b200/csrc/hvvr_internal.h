@@ -200,6 +200,7 @@ struct FrameDev {
     uint32_t* retry = nullptr;         // [tiles] tiles whose traversal stack overflowed, per range
     uint32_t* ready = nullptr;         // [tiles] ready slots of the pipelined rate classes (kReadyEmpty at frame start)
     uint32_t cullCtasPerSm = 0;        // cap on the persistent tile cull's resident CTAs per SM (0: occupancy)
+    uint32_t cullPersistent = 1;       // 0: each tile-cull warp culls one tile, and the grid covers all tiles
 };
 
 

@@ -619,6 +619,7 @@ void batchConfigDefault(hvvr_batch_config* c) {
     c->timing = 0;
     c->pipeline = 1;
     c->tile_cull_ctas_per_sm = 0;
+    c->tile_cull_persistent = 1;
 }
 
 int checkConfig(const hvvr_batch_config& c) {
@@ -630,6 +631,7 @@ int checkConfig(const hvvr_batch_config& c) {
         return fail(HVVR_ERR_INVALID, "tile_stack_entries must be 0 or in [8, 256]");
     if (c.timing > 1) return fail(HVVR_ERR_INVALID, "timing must be 0 or 1");
     if (c.pipeline > 1) return fail(HVVR_ERR_INVALID, "pipeline must be 0 or 1");
+    if (c.tile_cull_persistent > 1) return fail(HVVR_ERR_INVALID, "tile_cull_persistent must be 0 or 1");
     return HVVR_OK;
 }
 
@@ -1032,11 +1034,12 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     fr.retry = b->retry.p;
     fr.ready = b->ready.p;
     fr.cullCtasPerSm = b->cfg.tile_cull_ctas_per_sm;
+    fr.cullPersistent = b->cfg.tile_cull_persistent;
     if (b->cfg.use_graph && b->costValid && capturable) {
         std::vector<uint64_t> gkey = b->layoutKey;
         const uint64_t extra[] = {b->cfg.tile_cull_warps, b->cfg.heavy_divisor, b->poolChunks, strict ? 1u : 0u,
                                   uint64_t(uintptr_t(st)), b->cfg.tile_stack_entries, b->cfg.timing,
-                                  b->cfg.pipeline, b->cfg.tile_cull_ctas_per_sm};
+                                  b->cfg.pipeline, b->cfg.tile_cull_ctas_per_sm, b->cfg.tile_cull_persistent};
         gkey.insert(gkey.end(), std::begin(extra), std::end(extra));
         if (!b->graph || gkey != b->graphKey) {
             dropGraph(b);

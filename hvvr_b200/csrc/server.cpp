@@ -18,9 +18,10 @@
 //   * latency class - requests with priority 1 (the two eyes of a stereo frame, say) go to the
 //     latency slots: dispatched as soon as one is free, never held back to fill a batch, on
 //     streams of the GPU's highest priority while the throughput slots run at its lowest, so
-//     their CTAs are scheduled ahead of the throughput batches' pending ones. A cap on the
-//     throughput slots' persistent tile-cull CTAs (tile_cull_ctas_per_sm) keeps SMs free for
-//     them while a long throughput cull runs.
+//     their CTAs are scheduled ahead of the throughput batches' pending ones. With latency
+//     isolation (default) the throughput slots' frames cull non-persistently (a warp per tile) and
+//     without the cull -> shade pipeline, so no throughput CTA holds an SM slot for longer than one
+//     tile or waits on another CTA, and each slot one frees goes to the latency class first.
 //     When the budget is short, idle instances of other templates are freed first.
 //   * completion - a slot whose end event has fired returns its instances to the pools and its
 //     requests to the completion queue (CPU outputs are copied out of pinned staging first).
@@ -455,6 +456,7 @@ void hvvr_server_config_default(hvvr_server_config* cfg) {
     cfg->max_wait_ms = 2.0f;
     cfg->latency_slots = 1;
     cfg->tile_cull_ctas_per_sm = 0;
+    cfg->latency_isolation = 1;
 }
 
 int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr_server_config* cfg,
@@ -468,6 +470,7 @@ int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr
     if (s->cfg.slots < 1 || s->cfg.slots > 8) return fail(HVVR_ERR_INVALID, "slots must be 1..8");
     if (s->cfg.latency_slots > 4) return fail(HVVR_ERR_INVALID, "latency_slots must be 0..4");
     if (s->cfg.max_batch_views < 1) return fail(HVVR_ERR_INVALID, "max_batch_views must be >= 1");
+    if (s->cfg.latency_isolation > 1) return fail(HVVR_ERR_INVALID, "latency_isolation must be 0 or 1");
     for (uint32_t i = 0; i < count; i++) {
         hvvr_raycaster* rc = scenes[i];
         if (!rc) return fail(HVVR_ERR_INVALID, "NULL scene %u", i);
@@ -508,6 +511,12 @@ int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr
         sl.batch->cfg = bc;
         // throughput slots leave SMs free for latency-class launches when asked to
         if (!sl.latency) sl.batch->cfg.tile_cull_ctas_per_sm = s->cfg.tile_cull_ctas_per_sm;
+        // and, isolated, hold no SM slot for longer than one tile and never wait on another CTA: the
+        // block scheduler then hands every slot they free to the latency class's launches first
+        if (!sl.latency && s->cfg.latency_slots && s->cfg.latency_isolation) {
+            sl.batch->cfg.tile_cull_persistent = 0;
+            sl.batch->cfg.pipeline = 0;
+        }
         sl.batch->fixedViews = true;
         sl.batch->internal = true;
         sl.batch->rcs = s->scenes;

@@ -514,6 +514,7 @@ struct TileCullArgs {
     uint32_t stackLimit;   // entries the main pass may use (<= kTileStack)
     uint32_t* ready;       // pipelined: ready slots, slot first + i for the i-th finished tile (else nullptr)
     uint32_t* readyTail;   // pipelined: finished tiles so far, zero at launch
+    uint32_t persistent;   // 0: every warp culls one tile (the grid has a warp per tile), then exits
 };
 
 // traverseTiles for one tile of view V (tile = view-local index); returns the node visits.
@@ -691,7 +692,9 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
 }
 
 // Persistent warps pull tiles from a queue (longest-first when an order is given), so a
-// few long horizon tiles overlap with the rest instead of holding a CTA slot each.
+// few long horizon tiles overlap with the rest instead of holding a CTA slot each. Non-persistent
+// (a.persistent == 0): the grid has a warp per tile and each warp takes one tile from the same
+// queue, so the tiles still start longest-first and every CTA ends with its tile.
 // (W = 1: one warp per CTA, so a warp that runs out of tiles frees its registers at once; the
 // bound asks for the 20 resident warps per SM that the wider CTAs reach)
 template <int W>
@@ -730,6 +733,7 @@ __global__ void __launch_bounds__(W * 32, W == 1 ? 20 : 1) tileCullKernel(TileCu
             }
         }
         __syncwarp();
+        if (!a.persistent) return;
     }
 }
 
@@ -844,6 +848,10 @@ DeviceLimits& limits() {
 
 template <int W>
 cudaError_t launchTileCullW(const TileCullArgs& a, uint32_t count, uint32_t capPerSm, cudaStream_t st) {
+    if (!a.persistent) {
+        tileCullKernel<W><<<(count + W - 1) / W, W * 32, 0, st>>>(a);
+        return cudaGetLastError();
+    }
     DeviceLimits& d = limits();
     {
         std::lock_guard<std::mutex> lock(gLimitsMutex);
@@ -899,7 +907,8 @@ cudaError_t launchTileCullMain(const FrameDev& fr, const uint32_t* order, uint32
     if (stackLimit == 0 || stackLimit > kTileStack) stackLimit = kTileStack;
     if (stackLimit < 8) return cudaErrorInvalidValue;
     const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
-                         order, first, count, queues, fr.retry, queues + 1, queues + 2, stackLimit, ready, readyTail};
+                         order, first, count, queues, fr.retry, queues + 1, queues + 2, stackLimit, ready, readyTail,
+                         fr.cullPersistent ? 1u : 0u};
     switch (warps) {
     case 1: return launchTileCullW<1>(a, count, fr.cullCtasPerSm, st);
     case 2: return launchTileCullW<2>(a, count, fr.cullCtasPerSm, st);
@@ -913,7 +922,7 @@ cudaError_t launchTileCullRetryPass(const FrameDev& fr, const uint32_t* order, u
                                     uint32_t* queues, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
-                         order, first, count, queues, fr.retry, queues + 1, queues + 2, kTileStack, nullptr, nullptr};
+                         order, first, count, queues, fr.retry, queues + 1, queues + 2, kTileStack, nullptr, nullptr, 1u};
     return launchTileCullRetry(a, st);
 }
 

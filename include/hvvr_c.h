@@ -432,6 +432,11 @@ typedef struct {
     uint32_t tile_cull_ctas_per_sm; /* cap on the persistent tile cull's resident CTAs per SM (0 = as many
                                      as fit): leaves room on every SM for other work (the intersect of
                                      finished tiles, another batch's launches) */
+    uint32_t tile_cull_persistent; /* 1 (default): the tile cull's warps take tiles from its work queue
+                                     until it is empty. 0: each warp culls one tile and its CTA exits,
+                                     so the cull's CTAs are short-lived and the GPU's block scheduler
+                                     can give their SM slots to work of a higher stream priority
+                                     between tiles (a served throughput batch under a latency class) */
 } hvvr_batch_config;
 void hvvr_batch_config_default(hvvr_batch_config* cfg);
 int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,
@@ -517,6 +522,12 @@ typedef struct {
                                      priority; the `slots` throughput slots then run at its lowest */
     uint32_t tile_cull_ctas_per_sm; /* as hvvr_batch_config, for the throughput slots (default 0; with
                                      latency slots, a cap keeps SMs free for latency-class launches) */
+    uint32_t latency_isolation;   /* 1 (default): with latency slots, the throughput slots' frames run
+                                     with a non-persistent tile cull and without the cull -> shade
+                                     pipeline, so none of their CTAs holds an SM slot for longer than
+                                     one tile and none waits on another: each slot a throughput CTA
+                                     frees goes to the latency class's launches (highest stream
+                                     priority) first. 0: throughput slots keep the batch defaults */
 } hvvr_server_config;
 typedef struct {
     uint32_t view;                /* from hvvr_server_add_view */

@@ -159,9 +159,10 @@ def test_stack_retry_pass_matches_oracle(oracle, pipeline):
 @pytest.mark.parametrize("use_graph", [1, 0])
 def test_pipelined_and_split_frames_agree(oracle, use_graph):
     """The cull -> shade pipeline (default) against the split path (heavy part on its own stream,
-    cull before shade) on a frame batch with three MSAA rates over two scenes, over three frames
-    (the second and later ones cull in the previous frame's cost order): identical lists, hits
-    and colours, and both equal to the oracle."""
+    cull before shade) and against the pipeline with a non-persistent tile cull (a warp per tile,
+    as a served throughput batch runs) on a frame batch with three MSAA rates over two scenes, over
+    three frames (the second and later ones cull in the previous frame's cost order): identical
+    lists, hits and colours, and equal to the oracle."""
     sa, sb = scene("c1"), scene("small")
     rc_a, rc_b = _make_rc(sa), _make_rc(sb)
     views = [(rc_a, sa, 256, 224, "barrel", 8), (rc_a, sa, 192, 160, "grid", 1), (rc_b, sb, 160, 176, "barrel", 4)]
@@ -172,9 +173,10 @@ def test_pipelined_and_split_frames_agree(oracle, use_graph):
         cam.set_camera_to_world(xf)
         cams.append((cam, sc, smp, w, h, msaa, xf))
     results = {}
-    for pipeline in (1, 0):
+    for mode, pipeline, persistent in (("pipelined", 1, 1), ("split", 0, 1), ("one tile per warp", 1, 0)):
         batch = hv.Batch([rc_a, rc_b], hv.batch_config(use_graph=use_graph, tri_index_capacity=1 << 22,
-                                                       pipeline=pipeline, timing=1, tile_cull_warps=1 + pipeline))
+                                                       pipeline=pipeline, timing=1, tile_cull_warps=1 + pipeline,
+                                                       tile_cull_persistent=persistent))
         for frame in range(3):
             batch.render()
             assert batch.stats()["status"] == 0
@@ -185,13 +187,14 @@ def test_pipelined_and_split_frames_agree(oracle, use_graph):
             counts, idx = cam.tile_lists()
             ids, depth = cam.hits()
             out.append((counts, idx, ids, depth, cam.sample_colors()))
-            if pipeline:  # read while the batch that holds the lists is open
+            if mode == "pipelined":  # read while the batch that holds the lists is open
                 _check_view(oracle, sc, cam, smp, w, h, msaa, xf)
-        results[pipeline] = out
+        results[mode] = out
         batch.close()
-    for a, b in zip(results[1], results[0]):
-        for x, y in zip(a, b):
-            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    for other in ("split", "one tile per warp"):
+        for a, b in zip(results["pipelined"], results[other]):
+            for x, y in zip(a, b):
+                assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), other
     rc_a.close()
     rc_b.close()
 
