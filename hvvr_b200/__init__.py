@@ -125,6 +125,7 @@ _sig("hvvr_server_create", _p(_vp), _u32, _p(_abi.ServerConfig), _p(_vp))
 _sig("hvvr_server_destroy", _vp)
 _sig("hvvr_server_add_view", _vp, _u32, _p(_abi.FloatRect), _vp, _u32, _u32, _u32, _u32, _p(_u32))
 _sig("hvvr_server_submit", _vp, _p(_abi.Request), _p(C.c_uint64))
+_sig("hvvr_server_submit_group", _vp, _p(_abi.Request), _u32, _p(C.c_uint64))
 _sig("hvvr_server_prewarm", _vp, _u32, _u32)
 _sig("hvvr_server_poll", _vp, _p(_abi.Completion), _u32, _p(_u32), C.c_double)
 _sig("hvvr_server_update_vertices", _vp, _vp, _u32, _u32, _vp)
@@ -169,7 +170,7 @@ EXPORTED = [
     "hvvr_camera_read_foveated_frame", "hvvr_camera_read_foveated_resolve", "hvvr_foveated_frame_matrices",
     "hvvr_camera_read_polar_textures",
     "hvvr_server_config_default", "hvvr_server_create", "hvvr_server_destroy", "hvvr_server_add_view",
-    "hvvr_server_submit", "hvvr_server_prewarm", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
+    "hvvr_server_submit", "hvvr_server_submit_group", "hvvr_server_prewarm", "hvvr_server_poll", "hvvr_server_update_vertices", "hvvr_server_get_stats",
 ]
 
 
@@ -890,6 +891,28 @@ class Server:
         if device_ptr is None:
             self._outputs[rid.value] = output
         return rid.value
+
+    def submit_group(self, items, priority=0):
+        """Submits several requests at once (e.g. the two eyes of a stereo frame), so that they can
+        render in one batch. items: (view, msaa, camera_to_world, output or None, device_ptr or None,
+        tag) tuples. Returns their request ids."""
+        reqs = (_abi.Request * len(items))()
+        keep = []
+        for r, (view, msaa, xf, output, device_ptr, tag) in zip(reqs, items):
+            r.view, r.msaa, r.camera_to_world, r.tag, r.priority = view, msaa, xf, tag, priority
+            if device_ptr is not None:
+                r.memory_type, r.output = HVVR_MEMORY_CUDA, device_ptr
+                keep.append(None)
+            else:
+                assert output.flags["C_CONTIGUOUS"] and output.dtype == np.uint32
+                r.memory_type, r.output = HVVR_MEMORY_CPU, output.ctypes.data
+                keep.append(output)
+        ids = (C.c_uint64 * len(items))()
+        _check(_lib.hvvr_server_submit_group(self.handle, reqs, len(items), ids))
+        for i, out in zip(ids, keep):
+            if out is not None:
+                self._outputs[i] = out
+        return list(ids)
 
     def poll(self, capacity=256, wait_ms=0.0):
         out = (_abi.Completion * capacity)()

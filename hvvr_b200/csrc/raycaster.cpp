@@ -641,16 +641,32 @@ void dropGraph(hvvr_batch* b) {
     b->graphKey.clear();
 }
 
-int batchResources(hvvr_batch* b) {
-    if (!b->forkEv) {
-        int leastPriority = 0, greatestPriority = 0;
-        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+// The side streams of the rate classes that this frame renders, made on first use: the device has a
+// fixed number of hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 unless the process sets more
+// before CUDA starts) that all streams share, so a batch keeps no idle streams, and streams of
+// different priorities (a server's latency and throughput slots) share a queue as rarely as the
+// count allows.
+int ensureSideStreams(hvvr_batch* b) {
+    int leastPriority = 0, greatestPriority = 0;
+    for (uint32_t r = 0; r < kRateClasses; r++) {
+        if (!b->rateTiles[r]) continue;
+        // the heavy part's stream only where a heavy part can run
+        const bool heavy = b->cfg.heavy_divisor != 0 && !(r >= 6 && r < 12);
+        if (b->side[2 * r + 1] && (b->side[2 * r] || !heavy)) continue;
+        if (leastPriority == 0 && greatestPriority == 0)
+            CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
         const int heavyPrio = b->streamPriorities == 2 ? leastPriority : greatestPriority;
         const int restPrio = b->streamPriorities == 1 ? greatestPriority : leastPriority;
-        for (uint32_t r = 0; r < kRateClasses; r++) {
+        if (heavy && !b->side[2 * r])
             CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r], cudaStreamNonBlocking, heavyPrio));
+        if (!b->side[2 * r + 1])
             CUDA_TRY(cudaStreamCreateWithPriority(&b->side[2 * r + 1], cudaStreamNonBlocking, restPrio));
-        }
+    }
+    return HVVR_OK;
+}
+
+int batchResources(hvvr_batch* b) {
+    if (!b->forkEv) {
         CUDA_TRY(cudaEventCreateWithFlags(&b->rankEv, cudaEventDisableTiming));
         for (auto& e : b->cullEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&b->forkEv, cudaEventDisableTiming));
@@ -951,6 +967,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
         b->costValid = std::all_of(cams.begin(), cams.end(), [](const hvvr_camera* c) { return c->costFrames > 0; });
         dropGraph(b);
     }
+    TRY(ensureSideStreams(b));
     b->fpStrict = strict;
 
     // this frame's view table (transforms, scene pointers), staged in pinned memory that the

@@ -516,6 +516,9 @@ int hvvr_server_create(hvvr_raycaster* const* scenes, uint32_t count, const hvvr
         if (!sl.latency && s->cfg.latency_slots && s->cfg.latency_isolation) {
             sl.batch->cfg.tile_cull_persistent = 0;
             sl.batch->cfg.pipeline = 0;
+            // no heavy-part split (a single frame's latency device, not a batch's): one stream per
+            // rate class, so that all slots' streams fit the hardware work queues
+            sl.batch->cfg.heavy_divisor = 0;
         }
         sl.batch->fixedViews = true;
         sl.batch->internal = true;
@@ -617,29 +620,56 @@ int hvvr_server_prewarm(hvvr_server* s, uint32_t view, uint32_t count) {
     return HVVR_OK;
 }
 
-int hvvr_server_submit(hvvr_server* s, const hvvr_request* req, uint64_t* id) {
-    if (!s || !req) return fail(HVVR_ERR_INVALID, "NULL argument");
+namespace {
+
+// the checks of one request; the template checks need the server lock held
+int checkRequest(const hvvr_server* s, const hvvr_request* req) {
+    if (!req) return fail(HVVR_ERR_INVALID, "NULL request");
     if (req->memory_type != HVVR_MEMORY_CPU && req->memory_type != HVVR_MEMORY_CUDA)
         return fail(HVVR_ERR_INVALID, "output must be CPU or CUDA memory");
     if (!req->output) return fail(HVVR_ERR_INVALID, "NULL output");
     if (req->msaa != 1 && req->msaa != 2 && req->msaa != 4 && req->msaa != 8 && req->msaa != 16 && req->msaa != 32)
         return fail(HVVR_ERR_INVALID, "MSAA rate must be 1, 2, 4, 8, 16 or 32");
     if (req->priority > 1) return fail(HVVR_ERR_INVALID, "priority must be 0 (throughput) or 1 (latency)");
-    std::lock_guard<std::mutex> lock(s->mu);
     if (req->view >= s->templates.size()) return fail(HVVR_ERR_INVALID, "unknown view %u", req->view);
     if (s->templates[req->view].instBytes + s->poolBytes > s->cfg.hbm_budget_bytes)
         return fail(HVVR_ERR_OOM, "one view of this template exceeds the HBM budget");
-    auto r = std::make_unique<Request>();
-    r->id = s->nextId++;
-    r->r = *req;
-    r->submitMs = s->nowMs();
-    if (id) *id = r->id;
-    s->pending.push_back(r.get());
-    s->live[r->id] = std::move(r);
-    s->stats.submitted++;
-    s->stats.in_flight++;
+    return HVVR_OK;
+}
+
+// queues checked requests (server lock held) and wakes the worker once
+void enqueueRequests(hvvr_server* s, const hvvr_request* reqs, uint32_t count, uint64_t* ids) {
+    const double now = s->nowMs();
+    for (uint32_t i = 0; i < count; i++) {
+        auto r = std::make_unique<Request>();
+        r->id = s->nextId++;
+        r->r = reqs[i];
+        r->submitMs = now;
+        if (ids) ids[i] = r->id;
+        s->pending.push_back(r.get());
+        s->live[r->id] = std::move(r);
+        s->stats.submitted++;
+        s->stats.in_flight++;
+    }
     s->stats.queued = s->pending.size();
     s->workCv.notify_all();
+}
+
+} // namespace
+
+int hvvr_server_submit(hvvr_server* s, const hvvr_request* req, uint64_t* id) {
+    if (!s || !req) return fail(HVVR_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    TRY(checkRequest(s, req));
+    enqueueRequests(s, req, 1, id);
+    return HVVR_OK;
+}
+
+int hvvr_server_submit_group(hvvr_server* s, const hvvr_request* reqs, uint32_t count, uint64_t* ids) {
+    if (!s || (count && !reqs)) return fail(HVVR_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (uint32_t i = 0; i < count; i++) TRY(checkRequest(s, reqs + i));
+    enqueueRequests(s, reqs, count, ids);
     return HVVR_OK;
 }
 

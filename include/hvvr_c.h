@@ -522,6 +522,11 @@ typedef struct {
                                      priority; the `slots` throughput slots then run at its lowest */
     uint32_t tile_cull_ctas_per_sm; /* as hvvr_batch_config, for the throughput slots (default 0; with
                                      latency slots, a cap keeps SMs free for latency-class launches) */
+    /* Every stream of the process shares the device's hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS,
+     * 8 by default). With fewer queues than busy streams, a latency slot's launches can wait in a
+     * queue behind throughput launches whatever their stream priority: set the variable to 32 in
+     * the environment before the process first uses CUDA (stereo latency class at 500 req/s,
+     * p50/p99: 220/488 ms with 8 queues, 15/28 ms with 32). */
     uint32_t latency_isolation;   /* 1 (default): with latency slots, the throughput slots' frames run
                                      with a non-persistent tile cull and without the cull -> shade
                                      pipeline, so none of their CTAs holds an SM slot for longer than
@@ -568,6 +573,10 @@ int hvvr_server_add_view(hvvr_server* server, uint32_t scene, const hvvr_float_r
  * the device, so a warm server admits without allocating) */
 int hvvr_server_prewarm(hvvr_server* server, uint32_t view, uint32_t count);
 int hvvr_server_submit(hvvr_server* server, const hvvr_request* request, uint64_t* id);
+/* submits count requests at once (all checked first; none queued if one is refused), so the worker
+ * sees them together and can render them in one batch: the two eyes of a stereo frame submitted as
+ * one group of latency-class requests go out in one latency batch. ids[i] receives request i's id. */
+int hvvr_server_submit_group(hvvr_server* server, const hvvr_request* requests, uint32_t count, uint64_t* ids);
 /* moves up to capacity completions out; waits up to wait_ms for the first one */
 int hvvr_server_poll(hvvr_server* server, hvvr_completion* out, uint32_t capacity, uint32_t* count, double wait_ms);
 /* copies count device vertices (32 B each) now; they replace the model's vertices [first, first+count)

@@ -204,10 +204,10 @@ def test_polar_foveated_requests_same_alone_in_mix_and_direct():
 
 
 def test_latency_class_jumps_a_busy_mix(oracle):
-    """A stereo pair submitted as the latency class (priority 1) behind a queue of throughput
-    requests is dispatched at once on the latency slot, both eyes in one batch, while throughput
-    requests are still waiting; each eye's image equals the oracle's (and its completion says which
-    class it was)."""
+    """A stereo pair submitted as one group of the latency class (priority 1) behind a queue of
+    throughput requests is dispatched at once on the latency slot, both eyes in one batch, while
+    throughput requests are still waiting; each eye's image equals the oracle's (and its completion
+    says which class it was). A group with one refused request queues none of them."""
     scs = [scene("c1"), scene("small")]
     rcs = [_rc(s) for s in scs]
     srv = hv.Server(rcs, hv.server_config(slots=2, max_batch_views=4, slot_list_capacity=1 << 22, latency_slots=1,
@@ -221,31 +221,47 @@ def test_latency_class_jumps_a_busy_mix(oracle):
     stereo = srv.add_view(0, scenes.viewport_for(sw, sh), ssmp, sw, sh)
     rng = np.random.default_rng(9)
     busy = []  # the throughput requests' outputs, alive until their completions arrive
+    poses = []
     for k in range(32):
         vid, w, h = tmpl[k % len(tmpl)]
         xf = scenes.camera_transform(eye=(float(rng.uniform(-4, 4)), 2.0, 9.0))
         busy.append(np.zeros((h, w), dtype=np.uint32))
+        poses.append(xf)
         srv.submit(vid, 16, xf, output=busy[-1], tag=k)
     eyes = scenes.stereo_eyes(0.064)
-    outs = []
-    for e, xf in enumerate(eyes):
-        out = np.zeros((sh, sw), dtype=np.uint32)
-        outs.append((srv.submit(stereo, 8, xf, output=out, tag=1000 + e, priority=1), out, xf))
+    outs = [np.zeros((sh, sw), dtype=np.uint32) for _ in eyes]
+    # both eyes as one group: they reach the worker together and render in one latency batch
+    rids = srv.submit_group([(stereo, 8, xf, out, None, 1000 + e) for e, (xf, out) in enumerate(zip(eyes, outs))],
+                            priority=1)
+    outs = list(zip(rids, outs, eyes))
     done = _drain(srv, 34)
     assert all(c.status == 0 for c in done.values())
     thr = [c for c in done.values() if c.priority == 0]
     lat = [done[rid] for rid, _, _ in outs]
     assert all(c.priority == 1 for c in lat) and len(thr) == 32
-    assert all(c.batch_views <= 2 for c in lat)
+    assert all(c.batch_views == 2 for c in lat) and lat[0].dispatch_ms == lat[1].dispatch_ms
     # dispatched ahead of throughput requests submitted before them
     assert max(c.dispatch_ms for c in lat) < max(c.dispatch_ms for c in thr)
     for rid, out, xf in outs:
         fo = render_oracle(oracle, scs[0], ssmp, sw, sh, 8, cam_xf=xf)
         d = np.abs(out.view(np.uint8).astype(np.int32) - fo.image.view(np.uint8).astype(np.int32))
         assert d.max() <= 1
-    # a bad class is refused
+    # throughput requests that ran beside the latency frame: their tiles may have been left by
+    # yielding CTAs and done by the drain launches; the images are the oracle's all the same
+    for k in (0, 1, 2, 3, 5, 6):
+        si, kind, w, h = _templates()[k % len(tmpl)]
+        smp, vp = _samples(kind, w, h)
+        fo = render_oracle(oracle, scs[si], smp, w, h, 16, cam_xf=poses[k], viewport=vp)
+        d = np.abs(busy[k].view(np.uint8).astype(np.int32) - fo.image.view(np.uint8).astype(np.int32))
+        assert d.max() <= 1, k
+    # a bad class is refused, alone and inside a group (which then queues nothing)
     with pytest.raises(hv.HvvrError):
         srv.submit(stereo, 8, eyes[0], output=np.zeros((sh, sw), dtype=np.uint32), priority=2)
+    before = srv.stats()["submitted"]
+    bad = np.zeros((sh, sw), dtype=np.uint32)
+    with pytest.raises(hv.HvvrError):
+        srv.submit_group([(stereo, 8, eyes[0], bad, None, 0), (stereo, 3, eyes[1], bad, None, 0)], priority=1)
+    assert srv.stats()["submitted"] == before
     srv.close()
     for rc in rcs:
         rc.close()
