@@ -66,12 +66,18 @@ int buildScene(hvvr_raycaster* rc, std::vector<Node>& nodes, std::vector<uint4>&
     verts.clear();
     vertModel.clear();
     materials.clear();
-    if (modelCount == 0) {
+    // Models without triangles have no nodes: they take no child slot of the root fix-up nodes. A
+    // scene with no triangles at all gets one root whose four leaf slots are empty; the refit gives
+    // empty ranges -inf bounds, which fail every frustum test, so every tile's list is empty and the
+    // frame clears its samples to the background.
+    uint32_t liveCount = 0;
+    for (auto& m : rc->models) liveCount += m->nodes.empty() ? 0u : 1u;
+    if (liveCount == 0) {
         nodes.assign(1, Node{});
         nodes[0].leafMask = 0xf;
         return HVVR_OK;
     }
-    const uint32_t rootNodeCount = (modelCount + 1) / 3;
+    const uint32_t rootNodeCount = (liveCount + 1) / 3;
     size_t nc = rootNodeCount;
     for (auto& m : rc->models) nc += m->nodes.size();
     nodes.assign(nc, Node{});
@@ -128,9 +134,10 @@ int buildScene(hvvr_raycaster* rc, std::vector<Node>& nodes, std::vector<uint4>&
     if (rootNodeCount > 0) {
         std::vector<int64_t> children(rootNodeCount * 4);
         size_t w = 0;
-        for (size_t i = children.size() - modelCount - (rootNodeCount - 1); i != 0; --i) children[w++] = -1;
+        for (size_t i = children.size() - liveCount - (rootNodeCount - 1); i != 0; --i) children[w++] = -1;
         for (uint32_t i = 1; i < rootNodeCount; i++) children[w++] = i;
-        for (uint32_t mi = 0; mi < modelCount; mi++) children[w++] = viewOffsets[mi];
+        for (uint32_t mi = 0; mi < modelCount; mi++)
+            if (!rc->models[mi]->nodes.empty()) children[w++] = viewOffsets[mi];
         for (uint32_t i = 0; i < rootNodeCount; i++) {
             Node& n = nodes[i];
             n.tri[0] = 0;
@@ -1479,7 +1486,9 @@ int hvvr_model_create(hvvr_raycaster* rc, const hvvr_mesh_data* mesh, hvvr_model
     m->verts.assign(mesh->verts, mesh->verts + mesh->vert_count);
     m->triShade.assign(mesh->tri_shade, mesh->tri_shade + mesh->tri_count);
     if (mesh->materials) m->materials.assign(mesh->materials, mesh->materials + mesh->material_count);
-    if (mesh->nodes && mesh->node_count) {
+    if (mesh->tri_count == 0) {
+        // a model without triangles (MeshData may be empty): no nodes; the scene merge skips it
+    } else if (mesh->nodes && mesh->node_count) {
         m->nodes.assign(mesh->nodes, mesh->nodes + mesh->node_count);
     } else {
         std::vector<hvvr_topology_node> nodes(size_t(mesh->tri_count) + 4);

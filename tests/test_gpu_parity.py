@@ -233,6 +233,60 @@ def test_five_models_under_root_fixup_nodes(oracle):
     rc.close()
 
 
+def _empty_scene(like):
+    """A model with no triangles, vertices or materials (empty MeshData), with the lights of `like`."""
+    return scenes.Scene(like.verts[:0].copy(), like.tri_shade[:0].copy(), like.materials[:0].copy(), like.lights)
+
+
+def test_empty_models(oracle):
+    """Models without triangles: a raycaster whose only model is empty renders the background
+    (every sample 0xFF000000, every subsample a miss, status OK), and an empty model among others
+    takes no child slot of the root fix-up nodes, so the frame equals the oracle's merge of the
+    non-empty models."""
+    small = scene("small")
+    w, h = 160, 176
+    smp = scenes.barrel_samples(w, h)
+    xf = scenes.camera_transform(eye=(1.0, 2.5, 9.0), target=(0.0, 0.0, 0.0))
+    rc = hv.Raycaster()
+    rc.create_model(_empty_scene(small))
+    for l in small.lights:
+        rc.create_light(l)
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h)
+    cam.set_samples(smp)
+    cam.set_camera_to_world(xf)
+    cam.set_msaa(4)
+    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+    rc.render()
+    ids, depth = cam.hits()
+    assert (ids == 0xFFFFFFFF).all() and np.isinf(depth).all()
+    assert (cam.sample_colors() == 0xFF000000).all()
+    mapped = cam.sample_remap() >= 0
+    assert mapped.any() and (cam.image.reshape(-1)[mapped.reshape(-1)] == 0xFF000000).all()
+    rc.close()
+    parts = [scenes.make_scene(10, 60, seed=40 + k) for k in range(3)]
+    for p in parts:
+        hv.generate_topology(p)
+    xfs = [_abi_transform((0.0, 0.0, 0.0, 1.0), (-5.0 + 5.0 * k, 0.0, 0.0), 0.7) for k in range(3)]
+    rc = hv.Raycaster()
+    for p, mxf in ((parts[0], xfs[0]), (_empty_scene(parts[0]), xfs[0]), (parts[1], xfs[1]),
+                   (_empty_scene(parts[0]), xfs[0]), (parts[2], xfs[2])):
+        rc.create_model(p).set_transform(mxf)
+    for l in parts[0].lights:
+        rc.create_light(l)
+    cam = rc.create_camera(scenes.viewport_for(w, h))
+    cam.set_render_target(w, h)
+    cam.set_samples(smp)
+    cam.set_camera_to_world(xf)
+    cam.set_msaa(4)
+    cam.set_capture(hv.HVVR_CAPTURE_HITS)
+    rc.render()
+    fo = oracle.render(parts, smp, xf, scenes.viewport_for(w, h), w, h, 4, model_xf=xfs)
+    assert len(rc.scene_nodes()) == sum(len(p.nodes) for p in parts) + 1
+    _compare(cam, rc, fo, 4)
+    rc.close()
+
+
 def _abi_transform(rot, trans, scale):
     from hvvr_b200 import _abi
     return _abi.transform(rot, trans, scale)
