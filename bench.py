@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--views", type=int, default=64)
     ap.add_argument("--max-batch-views", type=int, default=64, help="served: views per throughput batch")
+    ap.add_argument("--throughput-slots", type=int, default=3, help="served: throughput batches in flight")
+    ap.add_argument("--latency-slots", type=int, default=1, help="served: latency-class slots")
     ap.add_argument("--served-cull-cap", type=int, default=3,
                     help="served: throughput batches' tile-cull CTAs per SM (0 = no cap)")
     ap.add_argument("--latency-frames", type=int, default=500,
@@ -743,9 +745,9 @@ def run_served(args):
         for l in sc.lights:
             rc.create_light(l)
         rcs.append(rc)
-    srv = hv.Server(rcs, hv.server_config(slots=3, max_batch_views=args.max_batch_views, slot_list_capacity=512 << 20,
-                                          hbm_budget_bytes=120 << 30, latency_slots=1,
-                                          tile_cull_ctas_per_sm=args.served_cull_cap))
+    srv = hv.Server(rcs, hv.server_config(slots=args.throughput_slots, max_batch_views=args.max_batch_views,
+                                          slot_list_capacity=512 << 20, hbm_budget_bytes=120 << 30,
+                                          latency_slots=args.latency_slots, tile_cull_ctas_per_sm=args.served_cull_cap))
     rng = np.random.default_rng(5)
     tmpl = []  # (view id, width, height, samples, scene, spec)
     for si in range(len(scs)):
@@ -912,10 +914,11 @@ def run_served(args):
         "dtype": "f32", "data": "synthetic (6 seeded procedural scenes, grid/barrel/foveated sample sets)",
         "config": {"workload": "render server: 6 resident scenes (0.1M-4.1M tris), %d view templates + stereo "
                                "2x1080x1200 8xMSAA (5%% of requests, each pair submitted as one group), Poisson arrivals %s req/s for %.1f s each, "
-                               "120 GiB HBM budget, 3 throughput slots x %d views + 1 latency slot (stereo pairs as "
+                               "120 GiB HBM budget, %d throughput slots x %d views + %d latency slot(s) (stereo pairs as "
                                "the latency class; latency isolation: the throughput slots cull a tile per warp "
                                "without the cull -> shade pipeline; CUDA_DEVICE_MAX_CONNECTIONS=32), backlog limit %d, instances "
-                               "pre-warmed" % (len(tmpl), args.rates, args.seconds, args.max_batch_views, BACKLOG),
+                               "pre-warmed" % (len(tmpl), args.rates, args.seconds, args.throughput_slots,
+                                               args.max_batch_views, args.latency_slots, BACKLOG),
                    "l2": "inputs larger than L2"},
         "sweep": sweep, "served_vs_plain_image_match": "%d/%d" % (matches, checks),
         "host_setup_s": setup_s, "clocks": ck,
