@@ -318,6 +318,15 @@ public:
     }
     const vector3& getTranslation() const { return static_cast<const vector3&>(_cameraToWorld.translation); }
 
+    // Camera::extractImage (camera.h:57): the reference copies the device image into a CPU_MEMORY
+    // render target here; Raycaster::render already returns with CPU targets complete, so nothing
+    // is left to do
+    void extractImage() {}
+    // Camera::advanceJitter (camera.cpp:205-209): the reference steps a per-frame jitter that only
+    // spins the MSAA pattern under JITTER_SAMPLES, which its build sets to 0
+    // (kernel_constants.h:17); the image does not depend on it
+    void advanceJitter() {}
+
     // additions: the MSAA rate (1, 2, 4, 8, 16 or 32; default 16) and an eager sample setup
     void setMsaa(uint32_t rate) { check(hvvr_camera_set_msaa(_handle, rate), "Camera::setMsaa"); }
     void setMsaaPattern(uint32_t pattern) { check(hvvr_camera_set_msaa_pattern(_handle, pattern), "Camera::setMsaaPattern"); }

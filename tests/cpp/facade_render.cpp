@@ -69,7 +69,10 @@ int main(int argc, char** argv) {
         camera->setCameraToWorld(cameraXf);
         if (camera->getSampleCount() != samples.size()) return 2;
         raycaster->render(0.0);
+        // a viewer's per-frame calls (no effect on the image here)
+        camera->advanceJitter();
         raycaster->render(1.0 / 90.0); // a second frame (scheduled by the first frame's costs)
+        camera->extractImage();
         // the error model: destroying an object the raycaster does not own is reported, not fatal
         bool threw = false;
         try {
