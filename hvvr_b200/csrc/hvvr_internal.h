@@ -163,6 +163,8 @@ struct ViewDev {
     const float4* materials;
     const unsigned long long* textures; // texture objects by id (0: none); textureCount entries
     uint32_t textureCount;
+    uint32_t prefetchNodes;          // nodes to bring into L2 at the top of the frame (0: an earlier
+                                     // view of the frame renders the same scene, or none)
     const Rays4* tileRays;
     const Rays4* blockRays;
     const float4* beams;

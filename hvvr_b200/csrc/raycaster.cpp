@@ -654,6 +654,7 @@ void dropGraph(hvvr_batch* b) {
 // different priorities (a server's latency and throughput slots) share a queue as rarely as the
 // count allows.
 int ensureSideStreams(hvvr_batch* b) {
+    if (!b->orderStream) CUDA_TRY(cudaStreamCreateWithFlags(&b->orderStream, cudaStreamNonBlocking));
     int leastPriority = 0, greatestPriority = 0;
     for (uint32_t r = 0; r < kRateClasses; r++) {
         if (!b->rateTiles[r]) continue;
@@ -677,6 +678,8 @@ int batchResources(hvvr_batch* b) {
         CUDA_TRY(cudaEventCreateWithFlags(&b->rankEv, cudaEventDisableTiming));
         for (auto& e : b->cullEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&b->forkEv, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&b->orderForkEv, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&b->orderDoneEv, cudaEventDisableTiming));
         for (auto& e : b->doneEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto& e : b->hostViewsEv) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto& e : b->ev) CUDA_TRY(cudaEventCreate(&e));
@@ -702,7 +705,8 @@ void releaseBatch(hvvr_batch* b) {
     dropGraph(b);
     for (auto& t : b->side)
         if (t) cudaStreamDestroy(t), t = nullptr;
-    for (cudaEvent_t* e : {&b->forkEv})
+    if (b->orderStream) cudaStreamDestroy(b->orderStream), b->orderStream = nullptr;
+    for (cudaEvent_t* e : {&b->forkEv, &b->orderForkEv, &b->orderDoneEv})
         if (*e) cudaEventDestroy(*e), *e = nullptr;
     for (auto& e : b->doneEv)
         if (e) cudaEventDestroy(e), e = nullptr;
@@ -752,9 +756,15 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
     CUDA_TRY(recordStage(b->ev[0], st, capturing));
     CUDA_TRY(cudaMemsetAsync(fr.counters, 0, kCounterWords * sizeof(uint32_t), st));
     if (b->cfg.pipeline && fr.tiles) CUDA_TRY(cudaMemsetAsync(fr.ready, 0xff, size_t(fr.tiles) * sizeof(uint32_t), st));
+    // the tile order reads only last frame's costs, so it runs on its own stream beside the block
+    // cull, and the tile culls wait for both
+    CUDA_TRY(cudaEventRecord(b->orderForkEv, st));
+    CUDA_TRY(cudaStreamWaitEvent(b->orderStream, b->orderForkEv, 0));
+    CUDA_TRY(launchTileOrder(fr, b->orderStream));
+    CUDA_TRY(cudaEventRecord(b->orderDoneEv, b->orderStream));
     CUDA_TRY(launchBlockCull(fr, st));
     if (stages) CUDA_TRY(recordStage(b->ev[1], st, capturing));
-    CUDA_TRY(launchTileOrder(fr, st));
+    CUDA_TRY(cudaStreamWaitEvent(st, b->orderDoneEv, 0));
     CUDA_TRY(cudaEventRecord(b->forkEv, st));
     bool first = true;
     for (auto& u : b->kevUsed) u = false;
@@ -983,6 +993,7 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     b->hostSlot ^= 1;
     if (b->hostViewsUsed[slot]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[slot]));
     ViewDev* hv = b->hostViews[slot];
+    std::vector<const Node*> prefetched;
     for (size_t i = 0; i < b->views.size(); i++) {
         const hvvr_camera* c = b->views[i].cam;
         const SceneDev& sc = c->rc->scene;
@@ -991,6 +1002,10 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
         v.M = transformToMatrix(c->xf);
         v.env = sc.env;
         v.nodes = sc.nodes;
+        if (sc.nodes && std::find(prefetched.begin(), prefetched.end(), sc.nodes) == prefetched.end()) {
+            v.prefetchNodes = sc.nodeCount;
+            prefetched.push_back(sc.nodes);
+        }
         v.tris = sc.tris;
         v.triShade = sc.triShade;
         v.verts = sc.verts;

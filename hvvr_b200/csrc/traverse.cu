@@ -309,8 +309,34 @@ __device__ __forceinline__ const ViewDev& viewOfBlock(const ViewDev* __restrict_
     return views[viewCount == 1 ? 0u : __ldg(blockView + blk)];
 }
 
+// A block walks up to a few hundred dependent node visits, each of which waits for its node's row
+// if it misses L2; so the CTAs past the block-cull CTAs first bring every scene's node array into
+// L2 (bulk prefetches of 4 KiB, issued at once; the traversing warps meet lines in flight or
+// resident, and so do the tile culls that follow).
+constexpr uint32_t kPrefetchCtas = 32, kPrefetchChunk = 4096;
+
+__device__ void prefetchSceneNodes(const FrameDev& fr, uint32_t cta) {
+    const uint32_t tid = cta * blockDim.x + threadIdx.x, threads = kPrefetchCtas * blockDim.x;
+    for (uint32_t vi = 0; vi < fr.viewCount; vi++) {
+        const ViewDev& V = fr.views[vi];
+        // whole 128-byte nodes of a 128-byte-aligned array: every chunk starts 16-byte aligned and
+        // its size is a multiple of 16
+        const size_t bytes = size_t(V.prefetchNodes) * sizeof(Node);
+        const char* base = reinterpret_cast<const char*>(V.nodes);
+        for (size_t off = size_t(tid) * kPrefetchChunk; off < bytes; off += size_t(threads) * kPrefetchChunk) {
+            const uint32_t n = uint32_t(bytes - off < kPrefetchChunk ? bytes - off : kPrefetchChunk);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(n) : "memory");
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kBlockWarps * 32) blockCullKernel(FrameDev fr) {
     __shared__ BlockSmem smem[kBlockWarps];
+    const uint32_t blockCtas = (fr.blocks + kBlockWarps - 1) / kBlockWarps;
+    if (blockIdx.x >= blockCtas) {
+        prefetchSceneNodes(fr, blockIdx.x - blockCtas);
+        return;
+    }
     const uint32_t warp = threadIdx.x >> 5, lane = laneId();
     const uint32_t gblk = blockIdx.x * kBlockWarps + warp;
     if (gblk >= fr.blocks) return;
@@ -890,7 +916,7 @@ cudaError_t launchTileCullRetry(const TileCullArgs& a, cudaStream_t st) {
 
 cudaError_t launchBlockCull(const FrameDev& fr, cudaStream_t st) {
     if (fr.blocks == 0) return cudaSuccess;
-    blockCullKernel<<<(fr.blocks + kBlockWarps - 1) / kBlockWarps, kBlockWarps * 32, 0, st>>>(fr);
+    blockCullKernel<<<(fr.blocks + kBlockWarps - 1) / kBlockWarps + kPrefetchCtas, kBlockWarps * 32, 0, st>>>(fr);
     return cudaGetLastError();
 }
 

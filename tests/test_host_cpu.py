@@ -71,3 +71,14 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(hv.HvvrError) as e:
         hv.Raycaster()
     assert e.value.code == _abi.HVVR_ERR_CUDA
+
+
+def test_batch_config_defaults():
+    """hvvr_batch_config_default: the configuration the stereo frame was tuned on (one-warp
+    persistent tile-cull CTAs, the slowest eighth of the tiles as the heavy part, the cull ->
+    shade pipeline, CUDA graph replay)."""
+    cfg = hv.batch_config()
+    assert (cfg.tile_cull_warps, cfg.heavy_divisor, cfg.pipeline, cfg.tile_cull_persistent) == (1, 8, 1, 1)
+    assert (cfg.use_graph, cfg.timing, cfg.tile_stack_entries, cfg.tile_cull_ctas_per_sm) == (1, 0, 0, 0)
+    assert C.sizeof(_abi.BatchConfig) == 48
+
