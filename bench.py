@@ -59,6 +59,9 @@ def parse():
                     help="stereo: frames of the p50/p99 latency run after the timed steps")
     ap.add_argument("--profile", action="store_true",
                     help="case for ncu: the stereo frame (or with --workload foveated the foveated frame), 3 frames")
+    ap.add_argument("--visit-clocks", action="store_true",
+                    help="per-visit phase cycles of the tile cull on the stereo frame, from the profiling build "
+                         "(make -C hvvr_b200/csrc visit-clocks); not a benchmark line")
     return ap.parse_args()
 
 
@@ -396,6 +399,9 @@ def main():
             run_profile_case_foveated()
         else:
             run_profile_case()
+        return
+    if args.visit_clocks:
+        run_visit_clocks()
         return
     if args.workload == "batched":
         run_batched(args)
@@ -1156,6 +1162,68 @@ def run_profile_case():
                           "stage_ms": [float(x) for x in cams[0].timings()],
                           "kernel_ms": [float(x) for x in rc.kernel_times()],
                           "list_entries": sum(c.list_total() for c in cams)}))
+
+
+VISIT_PHASES = ("row wait", "child test", "leaf refine + ranges", "multi-child insert", "next node", "list tail")
+
+
+def run_visit_clocks():
+    """The stereo frame rendered by the profiling build of the library, whose tile cull sums the SM
+    cycles of each tile's node visits per phase (clock64 reads that wait for each phase's result).
+    Prints one JSON line: cycles per visit by phase for all tiles, for the slowest eighth (the
+    heavy part) and for the 16 longest tiles, each from the third frame after an L2 flush."""
+    import ctypes as C
+    lib_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hvvr_b200", "_lib", "visit_clocks",
+                            "libhvvr_b200.so")
+    if not os.path.exists(lib_path):
+        sys.exit("bench.py --visit-clocks: build the profiling library first (make -C hvvr_b200/csrc visit-clocks)")
+    os.environ["HVVR_B200_LIB"] = lib_path
+    import torch
+    import hvvr_b200 as hv
+    from hvvr_b200 import scenes
+    lib = hv.lib()
+    lib.hvvr_dbg_visit_clocks.argtypes = [C.c_void_p, C.c_uint32]
+    sc = scenes.scene_c2()
+    hv.generate_topology(sc)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    with hv.Raycaster(tri_index_capacity=128 << 20) as rc:
+        rc.create_model(sc)
+        for l in sc.lights:
+            rc.create_light(l)
+        cams = []
+        for xf in scenes.stereo_eyes(IPD):
+            cam = rc.create_camera(scenes.viewport_for(W, H))
+            cam.set_render_target(W, H)
+            cam.set_samples(scenes.barrel_samples(W, H))
+            cam.set_camera_to_world(xf)
+            cam.set_msaa(MSAA)
+            cams.append(cam)
+        for _ in range(3):
+            flush.fill_(1.0)
+            rc.render()
+        rc.synchronize()
+        tiles = sum(len(c.tile_lists()[0]) for c in cams)
+        raw = np.zeros((tiles, len(VISIT_PHASES) + 1), np.uint64)
+        assert lib.hvvr_dbg_visit_clocks(raw.ctypes.data, tiles) == 0
+    cyc, visits = raw[:, :-1].astype(np.float64), raw[:, -1].astype(np.int64)
+
+    def table(sel):
+        v = max(int(visits[sel].sum()), 1)
+        per = cyc[sel].sum(axis=0) / v
+        return {"tiles": int(sel.sum()), "visits": int(visits[sel].sum()),
+                "cycles_per_visit": round(float(per.sum()), 1),
+                "phases": {name: {"cycles_per_visit": round(float(x), 1), "share": round(float(x / per.sum()), 3)}
+                           for name, x in zip(VISIT_PHASES, per)}}
+
+    order = np.argsort(-visits)
+    heavy = np.zeros(tiles, bool)
+    heavy[order[: max(1, tiles // 8)]] = True
+    top = np.zeros(tiles, bool)
+    top[order[:16]] = True
+    print(json.dumps({"visit_clocks": "tile cull, stereo 2x1080x1200 8xMSAA, 995,072 triangles, frame 3 after an L2 "
+                                      "flush, profiling build (counters add registers and spills)",
+                      "all": table(visits > 0), "slowest_eighth": table(heavy), "longest_16": table(top),
+                      "longest_tile_visits": int(visits.max())}))
 
 
 def run_profile_case_foveated():

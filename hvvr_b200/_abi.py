@@ -108,7 +108,7 @@ class TileCullArgs(C.Structure):
     """hvvr_tile_cull_args: device inputs of hvvr_tile_cull_static."""
     _fields_ = [("nodes", C.c_void_p), ("node_count", C.c_uint32), ("tile_rays", C.c_void_p),
                 ("tile_count", C.c_uint32), ("block_stacks", C.c_void_p), ("block_sizes", C.c_void_p),
-                ("camera_to_world", Transform)]
+                ("camera_to_world", Transform), ("tile_stack_entries", C.c_uint32)]
 
 
 class BatchConfig(C.Structure):

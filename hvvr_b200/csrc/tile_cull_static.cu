@@ -176,6 +176,8 @@ extern "C" int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* 
     if (args->tile_count > kMaxTiles)
         return failStatic(HVVR_ERR_INVALID, "tile_count exceeds the static scratch limit of 65536 tiles");
     if (capacity && !indices) return failStatic(HVVR_ERR_INVALID, "capacity given without an indices buffer");
+    if (args->tile_stack_entries && (args->tile_stack_entries < 8 || args->tile_stack_entries > kTileStack))
+        return failStatic(HVVR_ERR_INVALID, "tile_stack_entries must be 0 or in [8, 256]");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) return failStatic(HVVR_ERR_CUDA, "cudaGetDevice failed", e);
@@ -227,7 +229,8 @@ extern "C" int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* 
     }
     if ((e = launchWriteView(v, reinterpret_cast<ViewDev*>(scratch + kOffView), st)) != cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "view setup launch failed", e);
-    if ((e = launchTileCull(fr, nullptr, 0, tiles, scratch + kOffCounters + 4, 4, 0, st)) != cudaSuccess)
+    if ((e = launchTileCull(fr, nullptr, 0, tiles, scratch + kOffCounters + 4, 4, args->tile_stack_entries, st)) !=
+        cudaSuccess)
         return failStatic(HVVR_ERR_CUDA, "tile cull launch failed", e);
     scanCounts<<<1, 1024, 0, st>>>(scratch, tiles);
     gatherLists<<<(tiles + 7) / 8, 256, 0, st>>>(scratch, tiles, counts, indices, capacity);

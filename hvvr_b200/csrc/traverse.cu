@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <mutex>
 
+#include "../../include/hvvr_c.h"
 #include "dev_common.cuh"
 
 namespace hvb {
@@ -26,6 +27,40 @@ namespace hvb {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+
+#ifdef HVVR_VISIT_CLOCKS
+// Profiling build only (make -C hvvr_b200/csrc visit-clocks): per global tile, the SM cycles of
+// its tile-cull node visits split into phases, plus its visit count, read back through
+// hvvr_dbg_visit_clocks. The counters cost registers and instructions of their own, so the
+// phases' shares are what this build measures, not the production kernel's absolute times.
+constexpr uint32_t kVisitClockTiles = 1u << 17;
+enum : uint32_t {
+    kVcRow,    // waiting for the node's row (loaded during the previous visit)
+    kVcTest,   // child-row loads issued, child boxes shuffled, frustum plane/projection tests
+    kVcLeaf,   // refine tests of passing leaf slots and recording their triangle ranges
+    kVcInsert, // sorted insertion of two or more internal children
+    kVcNext,   // choosing the next node (one child, an inserted child, or a pop)
+    kVcTail,   // after the last visit: expanding the buffered ranges into the tile's list
+    kVcPhases
+};
+__device__ unsigned long long gVisitClocks[kVisitClockTiles][kVcPhases + 1];
+// clock64 read once dep is available: the read is predicated on a test of dep, so it waits for
+// dep's producer (the sentinel is a value none of the marked quantities takes in practice)
+__device__ __forceinline__ long long visitClock(uint32_t dep) {
+    long long t;
+    asm volatile("{ .reg .pred p; setp.ne.u32 p, %1, 0x9e3779b9; @p mov.u64 %0, %%clock64; @!p mov.u64 %0, 0; }"
+                 : "=l"(t) : "r"(dep) : "memory");
+    return t;
+}
+#define VISIT_MARK(phase, dep)                                                                                         \
+    do {                                                                                                               \
+        const long long t_ = visitClock(dep);                                                                          \
+        vcAcc[phase] += t_ - vcLast;                                                                                   \
+        vcLast = t_;                                                                                                   \
+    } while (0)
+#else
+#define VISIT_MARK(phase, dep) do { } while (0)
+#endif
 
 struct SmemFrustum {
     float tpLo[4][3], tpHi[4][3], w[4];
@@ -577,12 +612,17 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
     uint32_t visits = 0;
     const float* rows = reinterpret_cast<const float*>(nodes);
     float v = rows[size_t(node) * 32 + lane];
+#ifdef HVVR_VISIT_CLOCKS
+    long long vcAcc[kVcPhases] = {0, 0, 0, 0, 0, 0};
+    long long vcLast = visitClock(node);
+#endif
     for (;;) {
         ++visits;
         // The next visit is always one of this node's internal children or the stack entry
         // below the current one (a pop, or a push whose children all sort below it), so their
         // rows are loaded now and consumed at the end of the visit, hiding the load latency.
         const uint32_t leafMask = __float_as_uint(__shfl_sync(kFull, v, 24));
+        VISIT_MARK(kVcRow, leafMask);
         uint32_t childNode[4];
         float vc[4];
 #pragma unroll
@@ -595,6 +635,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
         const float vp = hasPop ? rows[size_t(popNode) * 32 + lane] : 0.0f;
         const ChildBox cb = childBox(v);
         uint32_t mask = testChildren(cb, t);
+        VISIT_MARK(kVcTest, mask);
         bool descend = false;
         if (mask) {
             uint32_t leaf = mask & leafMask;
@@ -602,6 +643,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                 mask &= ~refineReject(cb, t);
                 leaf = mask & leafMask;
                 if (leaf) em.addLeaves(s, v, leaf);
+                VISIT_MARK(kVcLeaf, em.rc);
                 if (em.dead) break;
             }
             mask &= ~leafMask;
@@ -615,6 +657,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
 #pragma unroll
                     for (int q = 1; q < 4; q++)
                         if (q == k) v = vc[q];
+                    VISIT_MARK(kVcNext, node);
                     continue;
                 }
                 // Insert all m >= 2 children at once. Keys are never NaN (a child that passes the
@@ -686,6 +729,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                 __syncwarp();
                 top += m - 1;
                 descend = true;
+                VISIT_MARK(kVcInsert, top);
             }
         }
         if (descend) {
@@ -697,13 +741,18 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                 if (!have && next == childNode[q] && !((leafMask >> q) & 1u)) { nv = vc[q]; have = true; }
             node = next;
             v = have ? nv : rows[size_t(node) * 32 + lane];
+            VISIT_MARK(kVcNext, node);
             continue;
         }
         if (top == 0) break;
         --top;
         node = popNode;
         v = vp;
+        VISIT_MARK(kVcNext, node);
     }
+#ifdef HVVR_VISIT_CLOCKS
+    vcLast = visitClock(top);
+#endif
     if (overflow) {
         if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
         return visits;
@@ -714,6 +763,13 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
         if (em.prev != kNoChunk) a.chunkNext[em.prev] = kNoChunk;
         V.tileLists[tile] = TileList{em.first, em.dead ? em.stored : em.total};
     }
+#ifdef HVVR_VISIT_CLOCKS
+    VISIT_MARK(kVcTail, em.total);
+    if (lane == 0 && V.tileStart + tile < kVisitClockTiles) {
+        for (uint32_t k = 0; k < kVcPhases; k++) gVisitClocks[V.tileStart + tile][k] = uint64_t(vcAcc[k]);
+        gVisitClocks[V.tileStart + tile][kVcPhases] = visits;
+    }
+#endif
     return visits;
 }
 
@@ -971,3 +1027,13 @@ cudaError_t launchWriteView(const ViewDev& v, ViewDev* dst, cudaStream_t st) {
 }
 
 } // namespace hvb
+
+#ifdef HVVR_VISIT_CLOCKS
+// profiling build only: per global tile [0, tiles), kVcPhases phase cycle sums then the visit count
+extern "C" int hvvr_dbg_visit_clocks(unsigned long long* out, uint32_t tiles) {
+    if (!out || tiles > hvb::kVisitClockTiles) return HVVR_ERR_INVALID;
+    return cudaMemcpyFromSymbol(out, hvb::gVisitClocks, size_t(tiles) * sizeof(hvb::gVisitClocks[0])) == cudaSuccess
+               ? HVVR_OK
+               : HVVR_ERR_CUDA;
+}
+#endif

@@ -609,6 +609,9 @@ typedef struct {
     const void* block_stacks;     /* device: (tile_count/64) x 64 x {float tMin; uint32_t mask; uint32_t node} */
     const uint32_t* block_sizes;  /* device: tile_count/64 sorted block-stack sizes */
     hvvr_transform camera_to_world;
+    uint32_t tile_stack_entries;  /* traversal stack of the main pass, 0 (= 256) or 8..256; tiles that
+                                     need more are culled again with 4096 entries (as
+                                     hvvr_batch_config.tile_stack_entries) */
 } hvvr_tile_cull_args;
 int hvvr_tile_cull_static(const hvvr_tile_cull_args* args, uint32_t* counts, uint32_t* indices, uint64_t capacity,
                           uint64_t* total, void* stream);

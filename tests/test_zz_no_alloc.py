@@ -7,7 +7,8 @@ library. This file checks, through the C ABI, that two calls in a row return exa
 per-tile triangle lists that the regular render path produced for the same frame (integer
 output, so the tolerance is zero), that the second call leaves the device's free memory
 unchanged (cudaMemGetInfo), that malformed inputs and work beyond the fixed limits are refused,
-and that lists longer than the fixed area are reported rather than cut.
+that the retry pass (tiles whose traversal stack outgrows the main pass's) gives the same lists
+from the fixed area, and that lists longer than the fixed area are reported rather than cut.
 It is collected last so that a run stopping at the first failure has run everything else.
 """
 import ctypes as C
@@ -101,6 +102,20 @@ def test_static_cull_matches_render_path(oracle):
     # the well-formed inputs still cull after the rejected calls
     rc_ = _call(args, C.c_void_p(d_counts.data_ptr()), C.c_void_p(d_idx.data_ptr()), cap, total)
     assert rc_ == hv.HVVR_OK and total.value == len(idx_ref)
+    # a 16-entry main-pass stack sends most tiles through the retry pass (4096-entry stacks in the
+    # same fixed area): the lists are unchanged; a stack size outside [8, 256] is refused
+    small = _abi.TileCullArgs(d_nodes.data_ptr(), len(nodes), d_rays.data_ptr(), tiles, d_stacks.data_ptr(),
+                              d_sizes.data_ptr(), xf, 16)
+    d_counts.fill_(-1)
+    d_idx.fill_(-1)
+    rc_ = _call(small, C.c_void_p(d_counts.data_ptr()), C.c_void_p(d_idx.data_ptr()), cap, total)
+    assert rc_ == hv.HVVR_OK, hv.lib().hvvr_last_error().decode()
+    assert total.value == len(idx_ref)
+    assert np.array_equal(d_counts.cpu().numpy().view(np.uint32), counts_ref)
+    assert np.array_equal(d_idx.cpu().numpy().view(np.uint32)[: total.value], idx_ref)
+    small.tile_stack_entries = 5
+    rc_ = _call(small, C.c_void_p(d_counts.data_ptr()), C.c_void_p(d_idx.data_ptr()), cap, total)
+    assert rc_ == _abi.HVVR_ERR_INVALID and b"tile_stack_entries" in hv.lib().hvvr_last_error()
     rc.close()
 
 
