@@ -688,16 +688,13 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                         mm &= mm - 1;
                     }
                 }
-                // old entries that move: those with a key below the largest child key (a top run)
-                const uint32_t region = shiftCount(top, [&](uint32_t p) { return dazf(s.tMin[p]) < maxKey; });
+                // old entries that move: those with a key below the largest child key (a top run).
+                // Lane j holds entry top-1-j of a group of 32; the first group is read once both
+                // to find the run and to move it, and the run continues into later groups only
+                // when all 32 of the first move.
                 uint32_t less[4] = {0u, 0u, 0u, 0u};
-                for (uint32_t base = 0; base < region; base += 32) {
-                    const uint32_t j = base + lane;
-                    const bool act = j < region;
-                    const uint32_t p = act ? top - 1 - j : 0u;
-                    float e = 0.0f, ez = 0.0f;
-                    uint32_t em_ = 0, en = 0;
-                    if (act) { e = s.tMin[p]; em_ = s.mask[p]; en = s.node[p]; ez = dazf(e); }
+                auto moveGroup = [&](uint32_t j, bool act, float e, float ez, uint32_t em_, uint32_t en) {
+                    const uint32_t p = top - 1 - j;
                     uint32_t d = 0;
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
@@ -708,6 +705,29 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                     __syncwarp();
                     if (act && d) { s.tMin[p + d] = e; s.mask[p + d] = em_; s.node[p + d] = en; }
                     __syncwarp();
+                };
+                uint32_t region;
+                {
+                    const bool inb = lane < top;
+                    float e = 0.0f, ez = 0.0f;
+                    uint32_t em_ = 0, en = 0;
+                    if (inb) {
+                        const uint32_t p = top - 1 - lane;
+                        e = s.tMin[p]; em_ = s.mask[p]; en = s.node[p]; ez = dazf(e);
+                    }
+                    const uint32_t b = __ballot_sync(kFull, inb && ez < maxKey);
+                    region = (b == kFull) ? 32u : uint32_t(__ffs(~b) - 1);
+                    moveGroup(lane, lane < region, e, ez, em_, en);
+                    if (region == 32u && top > 32u)
+                        region = 32u + shiftCount(top - 32u, [&](uint32_t p) { return dazf(s.tMin[p]) < maxKey; });
+                }
+                for (uint32_t base = 32; base < region; base += 32) {
+                    const uint32_t j = base + lane;
+                    const bool act = j < region;
+                    float e = 0.0f, ez = 0.0f;
+                    uint32_t em_ = 0, en = 0;
+                    if (act) { const uint32_t p = top - 1 - j; e = s.tMin[p]; em_ = s.mask[p]; en = s.node[p]; ez = dazf(e); }
+                    moveGroup(j, act, e, ez, em_, en);
                 }
                 if (lane < m) {
                     uint32_t pos = top - less[0];
