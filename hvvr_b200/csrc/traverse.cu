@@ -636,7 +636,6 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
         const ChildBox cb = childBox(v);
         uint32_t mask = testChildren(cb, t);
         VISIT_MARK(kVcTest, mask);
-        bool descend = false;
         if (mask) {
             uint32_t leaf = mask & leafMask;
             if (leaf) {
@@ -673,19 +672,18 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                     overflow = true;
                     break;
                 }
+                // the children in slot order (bit i of mask: child i is inserted); the reference
+                // inserts them in slot order, so "earlier" in the tie rule is the earlier slot
                 float ck[4], ckz[4];
-                uint32_t cnode[4];
-                float maxKey = -INFINITY;
-                {
-                    uint32_t mm = mask;
+                float maxKey = -INFINITY, minKey = INFINITY;
+                uint32_t kmin = 0;
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const int kk = mm ? __ffs(mm) - 1 : 0;
-                        ck[i] = __uint_as_float(__float_as_uint(__shfl_sync(kFull, v, distIdx * 4 + kk)) ^ 0x80000000u);
-                        ckz[i] = dazf(ck[i]);
-                        cnode[i] = node + __float_as_uint(__shfl_sync(kFull, v, 26 + kk));
-                        if (mm) maxKey = fmaxf(maxKey, ckz[i]);
-                        mm &= mm - 1;
+                for (int i = 0; i < 4; i++) {
+                    ck[i] = __uint_as_float(__float_as_uint(__shfl_sync(kFull, v, distIdx * 4 + i)) ^ 0x80000000u);
+                    ckz[i] = dazf(ck[i]);
+                    if ((mask >> i) & 1u) {
+                        maxKey = fmaxf(maxKey, ckz[i]);
+                        if (ckz[i] <= minKey) { minKey = ckz[i]; kmin = uint32_t(i); }
                     }
                 }
                 // old entries that move: those with a key below the largest child key (a top run).
@@ -698,7 +696,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                     uint32_t d = 0;
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        const bool valid = uint32_t(i) < m;
+                        const bool valid = (mask >> i) & 1u;
                         d += (act && valid && ckz[i] > ez) ? 1u : 0u;
                         less[i] += __popc(__ballot_sync(kFull, act && valid && ez < ckz[i]));
                     }
@@ -707,6 +705,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                     __syncwarp();
                 };
                 uint32_t region;
+                float oldTopKey; // key of the entry below the current one (when there is one)
                 {
                     const bool inb = lane < top;
                     float e = 0.0f, ez = 0.0f;
@@ -715,6 +714,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                         const uint32_t p = top - 1 - lane;
                         e = s.tMin[p]; em_ = s.mask[p]; en = s.node[p]; ez = dazf(e);
                     }
+                    oldTopKey = __shfl_sync(kFull, ez, 0);
                     const uint32_t b = __ballot_sync(kFull, inb && ez < maxKey);
                     region = (b == kFull) ? 32u : uint32_t(__ffs(~b) - 1);
                     moveGroup(lane, lane < region, e, ez, em_, en);
@@ -729,17 +729,17 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                     if (act) { const uint32_t p = top - 1 - j; e = s.tMin[p]; em_ = s.mask[p]; en = s.node[p]; ez = dazf(e); }
                     moveGroup(j, act, e, ez, em_, en);
                 }
-                if (lane < m) {
+                if ((mask >> lane) & 1u) { // lanes 0-3, one per inserted child
                     uint32_t pos = top - less[0];
                     float mine = ckz[0];
                     float rawk = ck[0];
-                    uint32_t nd = cnode[0];
+                    uint32_t nd = childNode[0];
 #pragma unroll
                     for (int i = 1; i < 4; i++)
-                        if (uint32_t(i) == lane) { pos = top - less[i]; mine = ckz[i]; rawk = ck[i]; nd = cnode[i]; }
+                        if (uint32_t(i) == lane) { pos = top - less[i]; mine = ckz[i]; rawk = ck[i]; nd = childNode[i]; }
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        if (uint32_t(i) >= m || uint32_t(i) == lane) continue;
+                        if (!((mask >> i) & 1u) || uint32_t(i) == lane) continue;
                         if (ckz[i] > mine || (ckz[i] == mine && uint32_t(i) < lane)) pos++;
                     }
                     s.tMin[pos] = rawk;
@@ -747,22 +747,25 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
                     s.node[pos] = nd;
                 }
                 __syncwarp();
+                const bool popNext = hasPop && oldTopKey < minKey;
                 top += m - 1;
-                descend = true;
                 VISIT_MARK(kVcInsert, top);
-            }
-        }
-        if (descend) {
-            const uint32_t next = s.node[top];
-            float nv = vp;
-            bool have = hasPop && (next == popNode);
+                // The new top entry is the next node: the old entry below the current one when its
+                // key is below every child's (it moved up by m), else the child with the smallest
+                // key, the last slot among equal ones (an old entry with an equal key stays below it).
+                if (popNext) {
+                    node = popNode;
+                    v = vp;
+                } else {
+                    node = childNode[0];
+                    v = vc[0];
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (!have && next == childNode[q] && !((leafMask >> q) & 1u)) { nv = vc[q]; have = true; }
-            node = next;
-            v = have ? nv : rows[size_t(node) * 32 + lane];
-            VISIT_MARK(kVcNext, node);
-            continue;
+                    for (uint32_t q = 1; q < 4; q++)
+                        if (q == kmin) { node = childNode[q]; v = vc[q]; }
+                }
+                VISIT_MARK(kVcNext, node);
+                continue;
+            }
         }
         if (top == 0) break;
         --top;
