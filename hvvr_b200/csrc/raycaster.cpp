@@ -993,7 +993,11 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
     b->hostSlot ^= 1;
     if (b->hostViewsUsed[slot]) CUDA_TRY(cudaEventSynchronize(b->hostViewsEv[slot]));
     ViewDev* hv = b->hostViews[slot];
+    // scenes whose BVH nodes the block-cull launch prefetches into L2, at most half of a B200's
+    // 126 MB L2 per frame (a served batch over several large scenes would only evict its own lines)
     std::vector<const Node*> prefetched;
+    size_t prefetchBytes = 0;
+    constexpr size_t kPrefetchBudget = size_t(64) << 20;
     for (size_t i = 0; i < b->views.size(); i++) {
         const hvvr_camera* c = b->views[i].cam;
         const SceneDev& sc = c->rc->scene;
@@ -1002,9 +1006,11 @@ int renderBatch(hvvr_batch* b, cudaStream_t st, bool skipScenes) {
         v.M = transformToMatrix(c->xf);
         v.env = sc.env;
         v.nodes = sc.nodes;
-        if (sc.nodes && std::find(prefetched.begin(), prefetched.end(), sc.nodes) == prefetched.end()) {
+        if (sc.nodes && std::find(prefetched.begin(), prefetched.end(), sc.nodes) == prefetched.end() &&
+            prefetchBytes + size_t(sc.nodeCount) * sizeof(Node) <= kPrefetchBudget) {
             v.prefetchNodes = sc.nodeCount;
             prefetched.push_back(sc.nodes);
+            prefetchBytes += size_t(sc.nodeCount) * sizeof(Node);
         }
         v.tris = sc.tris;
         v.triShade = sc.triShade;
