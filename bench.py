@@ -1165,13 +1165,17 @@ def run_profile_case():
 
 
 VISIT_PHASES = ("row wait", "child test", "leaf refine + ranges", "multi-child insert", "next node", "list tail")
+SHADE_PHASES = ("setup", "chunk: staged triangles, tile tests, compaction", "chunk: depth skip, subsample tests",
+                "outputs, G-buffer, shading")
 
 
 def run_visit_clocks():
     """The stereo frame rendered by the profiling build of the library, whose tile cull sums the SM
-    cycles of each tile's node visits per phase (clock64 reads that wait for each phase's result).
-    Prints one JSON line: cycles per visit by phase for all tiles, for the slowest eighth (the
-    heavy part) and for the 16 longest tiles, each from the third frame after an L2 flush."""
+    cycles of each tile's node visits per phase (clock64 reads that wait for each phase's result)
+    and whose intersect/shade sums its CTA's cycles per phase. Prints one JSON line: cycles per
+    visit by phase for all tiles, for the slowest eighth (the heavy part) and for the 16 longest
+    tiles, and the intersect/shade cycles per tile by phase for the same sets, each from the third
+    frame after an L2 flush."""
     import ctypes as C
     lib_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hvvr_b200", "_lib", "visit_clocks",
                             "libhvvr_b200.so")
@@ -1183,6 +1187,7 @@ def run_visit_clocks():
     from hvvr_b200 import scenes
     lib = hv.lib()
     lib.hvvr_dbg_visit_clocks.argtypes = [C.c_void_p, C.c_uint32]
+    lib.hvvr_dbg_shade_clocks.argtypes = [C.c_void_p, C.c_uint32]
     sc = scenes.scene_c2()
     hv.generate_topology(sc)
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
@@ -1205,7 +1210,10 @@ def run_visit_clocks():
         tiles = sum(len(c.tile_lists()[0]) for c in cams)
         raw = np.zeros((tiles, len(VISIT_PHASES) + 1), np.uint64)
         assert lib.hvvr_dbg_visit_clocks(raw.ctypes.data, tiles) == 0
+        sraw = np.zeros((tiles, len(SHADE_PHASES) + 2), np.uint64)
+        assert lib.hvvr_dbg_shade_clocks(sraw.ctypes.data, tiles) == 0
     cyc, visits = raw[:, :-1].astype(np.float64), raw[:, -1].astype(np.int64)
+    scyc, entries = sraw[:, :len(SHADE_PHASES)].astype(np.float64), sraw[:, -1].astype(np.int64)
 
     def table(sel):
         v = max(int(visits[sel].sum()), 1)
@@ -1215,15 +1223,29 @@ def run_visit_clocks():
                 "phases": {name: {"cycles_per_visit": round(float(x), 1), "share": round(float(x / per.sum()), 3)}
                            for name, x in zip(VISIT_PHASES, per)}}
 
+    def shade_table(sel):
+        sel = sel & (entries > 0)
+        n = max(int(sel.sum()), 1)
+        per = scyc[sel].sum(axis=0) / n
+        return {"tiles": int(sel.sum()), "list_entries_per_tile": round(float(entries[sel].sum()) / n, 1),
+                "cycles_per_tile": round(float(per.sum()), 1),
+                "phases": {name: {"cycles_per_tile": round(float(x), 1), "share": round(float(x / per.sum()), 3)}
+                           for name, x in zip(SHADE_PHASES, per)}}
+
     order = np.argsort(-visits)
     heavy = np.zeros(tiles, bool)
     heavy[order[: max(1, tiles // 8)]] = True
     top = np.zeros(tiles, bool)
     top[order[:16]] = True
+    stop = np.zeros(tiles, bool)
+    stop[np.argsort(-scyc.sum(axis=1))[:16]] = True
     print(json.dumps({"visit_clocks": "tile cull, stereo 2x1080x1200 8xMSAA, 995,072 triangles, frame 3 after an L2 "
                                       "flush, profiling build (counters add registers and spills)",
                       "all": table(visits > 0), "slowest_eighth": table(heavy), "longest_16": table(top),
-                      "longest_tile_visits": int(visits.max())}))
+                      "longest_tile_visits": int(visits.max()),
+                      "shade_clocks": {"all": shade_table(np.ones(tiles, bool)), "slowest_eighth": shade_table(heavy),
+                                       "longest_16_shades": shade_table(stop),
+                                       "longest_shade_cycles": round(float(scyc.sum(axis=1).max()), 1)}}))
 
 
 def run_profile_case_foveated():

@@ -57,6 +57,18 @@ __device__ __forceinline__ float dazf(float f) {
 
 __device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
 
+#ifdef HVVR_VISIT_CLOCKS
+// Profiling build only (make -C hvvr_b200/csrc visit-clocks): clock64 read once dep is available.
+// The read is predicated on a test of dep, so it waits for dep's producer (the sentinel is a value
+// none of the marked quantities takes in practice).
+__device__ __forceinline__ long long phaseClock(uint32_t dep) {
+    long long t;
+    asm volatile("{ .reg .pred p; setp.ne.u32 p, %1, 0x9e3779b9; @p mov.u64 %0, %%clock64; @!p mov.u64 %0, 0; }"
+                 : "=l"(t) : "r"(dep) : "memory");
+    return t;
+}
+#endif
+
 // ReadTexture (libraries/hvvr/raycaster/shading.h:45-47): one gradient read through a texture
 // object made as the reference makes its material textures (texture.cu:234-265)
 __device__ __forceinline__ float4 readTexture(cudaTextureObject_t t, float u, float v, float2 ddx, float2 ddy) {

@@ -15,6 +15,7 @@
 // sample's N subsamples against them in that order, so depth ties resolve as in the reference.
 #include <algorithm>
 
+#include "../../include/hvvr_c.h"
 #include "dev_common.cuh"
 
 namespace hvb {
@@ -29,6 +30,29 @@ __constant__ __align__(8) float2 cMsaaYY[12][32];
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+
+#ifdef HVVR_VISIT_CLOCKS
+// Profiling build only (make -C hvvr_b200/csrc visit-clocks): per global tile, the SM cycles that
+// thread 0 of its intersect/shade CTA spends in each phase (the CTA's barriers make thread 0's
+// clock the CTA's), its chunk count and its list length, read back through hvvr_dbg_shade_clocks.
+constexpr uint32_t kShadeClockTiles = 1u << 17;
+enum : uint32_t {
+    kScSetup, // view, frustum planes, beams, first chunk staged
+    kScCull,  // per chunk: staged triangles arrive, per-triangle tile tests, survivor compaction
+    kScTest,  // per chunk: depth skip and the packed subsample tests, next chunk staged
+    kScShade, // hit and depth outputs, G-buffer grouping, shading, resolve
+    kScPhases
+};
+__device__ unsigned long long gShadeClocks[kShadeClockTiles][kScPhases + 2];
+#define SHADE_MARK(phase, dep)                                                                                         \
+    do {                                                                                                               \
+        const long long t_ = phaseClock(dep);                                                                          \
+        scAcc[phase] += t_ - scLast;                                                                                   \
+        scLast = t_;                                                                                                   \
+    } while (0)
+#else
+#define SHADE_MARK(phase, dep) do { } while (0)
+#endif
 
 template <uint32_t N> struct RateIndex;
 template <> struct RateIndex<1> { static constexpr int v = 0; };
@@ -568,6 +592,11 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         }
         return;
     }
+#ifdef HVVR_VISIT_CLOCKS
+    long long scAcc[kScPhases] = {0, 0, 0, 0};
+    long long scLast = phaseClock(L.count);
+    uint32_t scChunks = 0;
+#endif
     const int rate = ROW;
     for (uint32_t i = tid; i < sizeof(LightEnvDev) / 4; i += kTileSize)
         reinterpret_cast<uint32_t*>(&env)[i] = reinterpret_cast<const uint32_t*>(&V.env)[i];
@@ -627,6 +656,7 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         hit[i] = ~0u;
     }
     __syncthreads();
+    SHADE_MARK(kScSetup, L.first);
 
     // The list is consumed chunk by chunk. Entry tid of a chunk is staged into shared memory by
     // cp.async (the 48-byte triangle record that its index names) while the CTA is still testing
@@ -711,6 +741,7 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
             sm.idx[off] = idx;
         }
         __syncthreads();
+        SHADE_MARK(kScCull, total);
         // stage the next chunk (this thread's entry of this chunk was read above)
         if (more && tid < (rest < kChunk ? rest : kChunk)) stage(idxNext);
         cpAsyncCommit();
@@ -771,6 +802,10 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         remaining -= n;
         chunk = nextChunk;
         idx = idxNext;
+        SHADE_MARK(kScTest, remaining);
+#ifdef HVVR_VISIT_CLOCKS
+        ++scChunks;
+#endif
     }
 
     if (tid == 0 && survivors) atomicAdd(&fr.counters[kSurvivorWord], survivors);
@@ -855,6 +890,15 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
     }
     const float sN = 1.0f / float(N);
     viewPtr(V.colors)[sid] = packColor(f3(aces(rx * sN), aces(ry * sN), aces(rz * sN)));
+#ifdef HVVR_VISIT_CLOCKS
+    __syncthreads();
+    SHADE_MARK(kScShade, gi);
+    if (tid == 0 && gt < kShadeClockTiles) {
+        for (uint32_t k = 0; k < kScPhases; k++) gShadeClocks[gt][k] = uint64_t(scAcc[k]);
+        gShadeClocks[gt][kScPhases] = scChunks;
+        gShadeClocks[gt][kScPhases + 1] = L.count;
+    }
+#endif
 }
 
 // SRC selects where the launch's tiles come from (ShadeSource): kFromOrder and kFromReady run one
@@ -1342,3 +1386,15 @@ cudaError_t uploadMsaaTable(uint32_t n, uint32_t pattern, const float* offsets, 
 }
 
 } // namespace hvb
+
+#ifdef HVVR_VISIT_CLOCKS
+// profiling build only: per global tile [0, tiles), kScPhases phase cycle sums of the intersect/shade
+// CTA's thread 0, then its chunk count and list length
+extern "C" int hvvr_dbg_shade_clocks(unsigned long long* out, uint32_t tiles) {
+    if (!out || tiles > hvb::kShadeClockTiles) return HVVR_ERR_INVALID;
+    return cudaMemcpyFromSymbol(out, hvb::gShadeClocks, size_t(tiles) * sizeof(hvb::gShadeClocks[0])) == cudaSuccess
+               ? HVVR_OK
+               : HVVR_ERR_CUDA;
+}
+#endif
+

@@ -44,17 +44,9 @@ enum : uint32_t {
     kVcPhases
 };
 __device__ unsigned long long gVisitClocks[kVisitClockTiles][kVcPhases + 1];
-// clock64 read once dep is available: the read is predicated on a test of dep, so it waits for
-// dep's producer (the sentinel is a value none of the marked quantities takes in practice)
-__device__ __forceinline__ long long visitClock(uint32_t dep) {
-    long long t;
-    asm volatile("{ .reg .pred p; setp.ne.u32 p, %1, 0x9e3779b9; @p mov.u64 %0, %%clock64; @!p mov.u64 %0, 0; }"
-                 : "=l"(t) : "r"(dep) : "memory");
-    return t;
-}
 #define VISIT_MARK(phase, dep)                                                                                         \
     do {                                                                                                               \
-        const long long t_ = visitClock(dep);                                                                          \
+        const long long t_ = phaseClock(dep);                                                                          \
         vcAcc[phase] += t_ - vcLast;                                                                                   \
         vcLast = t_;                                                                                                   \
     } while (0)
@@ -614,7 +606,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
     float v = rows[size_t(node) * 32 + lane];
 #ifdef HVVR_VISIT_CLOCKS
     long long vcAcc[kVcPhases] = {0, 0, 0, 0, 0, 0};
-    long long vcLast = visitClock(node);
+    long long vcLast = phaseClock(node);
 #endif
     for (;;) {
         ++visits;
@@ -774,7 +766,7 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
         VISIT_MARK(kVcNext, node);
     }
 #ifdef HVVR_VISIT_CLOCKS
-    vcLast = visitClock(top);
+    vcLast = phaseClock(top);
 #endif
     if (overflow) {
         if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
