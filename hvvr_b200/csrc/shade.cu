@@ -215,6 +215,11 @@ __device__ __forceinline__ bool signsClear(float a, float b, float c, float d) {
 // FMA chains (FMA) or as rounded products and sums (STRICT), u = (denom - v) - w, the sign-bit test
 // and the depth update. Both depth deltas are formed from the depth before j; when j hits, k's is
 // formed again from the new depth, so k sees exactly the depth the sequential fold gives it.
+// The depth of a hit, t / denom as the reference computes it (t times the IEEE reciprocal). Out of
+// line: it runs only on a hit, and one copy of the division replaces one per unrolled subsample
+// test, which keeps the pair-test loop small in the instruction cache.
+__device__ __noinline__ float hitDepth(float t, float denom) { return t * (1.0f / denom); }
+
 // tt holds (-t_j, -t_k) in FMA mode, (t_j, t_k) in STRICT mode.
 template <bool FMA>
 __device__ __forceinline__ void pairTest(const TriPair& p, P2 tt, float tj, float tk, uint32_t ij, uint32_t ik,
@@ -240,12 +245,12 @@ __device__ __forceinline__ void pairTest(const TriPair& p, P2 tt, float tj, floa
     upk(v, v0, v1);
     upk(w, w0, w1);
     if (signsClear(dd0, u0, v0, w0)) {
-        depth = tj * (1.0f / den0);
+        depth = hitDepth(tj, den0);
         hit = ij;
         dd1 = FMA ? fmaf(depth, den1, -tk) : depth * den1 - tk;
     }
     if (signsClear(dd1, u1, v1, w1)) {
-        depth = tk * (1.0f / den1);
+        depth = hitDepth(tk, den1);
         hit = ik;
     }
 }
