@@ -108,28 +108,6 @@ __device__ __forceinline__ TriThread threadSetup(F3 e0, F3 e1, F3 v0r, F3 c, F3 
     return threadSetupN(cross3(e0, e1), e0, e1, v0r, c, du, dv);
 }
 
-// IntersectTriangleThread::test (prim_tests.h:192-231)
-template <bool FMA>
-__device__ __forceinline__ bool threadTest(const TriThread& th, float t, float ax, float ay, float& depth) {
-    float denom, depthDelta, v, w;
-    if (FMA) {
-        denom = fmaf(th.ddy, ay, fmaf(th.ddx, ax, th.dc));
-        depthDelta = fmaf(depth, denom, -t);
-        v = fmaf(th.dvy, ay, fmaf(th.dvx, ax, th.vc));
-        w = fmaf(th.dwy, ay, fmaf(th.dwx, ax, th.wc));
-    } else {
-        denom = th.dc + th.ddx * ax + th.ddy * ay;
-        depthDelta = depth * denom - t;
-        v = th.vc + th.dvx * ax + th.dvy * ay;
-        w = th.wc + th.dwx * ax + th.dwy * ay;
-    }
-    const float u = denom - v - w;
-    const int test = __float_as_int(depthDelta) | __float_as_int(u) | __float_as_int(v) | __float_as_int(w);
-    if (test < 0) return false;
-    depth = t * (1.0f / denom);
-    return true;
-}
-
 // Packed FP32 (sm_100 f32x2): two floats in one 64-bit register pair, each lane an ordinary IEEE
 // single-precision operation (round to nearest, flush to zero like every other operation here), so
 // a packed result equals the two scalar results bit for bit.
@@ -210,16 +188,17 @@ __device__ __forceinline__ bool signsClear(float a, float b, float c, float d) {
     return (__float_as_int(a) | __float_as_int(b) | __float_as_int(c) | __float_as_int(d)) >= 0;
 }
 
-// threadTest of one subsample (unit offset ax, ay duplicated into both lanes) against triangles j
-// and k in that order, with the scalar test's operations in its order: denom, depthDelta, v, w as
-// FMA chains (FMA) or as rounded products and sums (STRICT), u = (denom - v) - w, the sign-bit test
-// and the depth update. Both depth deltas are formed from the depth before j; when j hits, k's is
-// formed again from the new depth, so k sees exactly the depth the sequential fold gives it.
 // The depth of a hit, t / denom as the reference computes it (t times the IEEE reciprocal). Out of
 // line: it runs only on a hit, and one copy of the division replaces one per unrolled subsample
 // test, which keeps the pair-test loop small in the instruction cache.
 __device__ __noinline__ float hitDepth(float t, float denom) { return t * (1.0f / denom); }
 
+// IntersectTriangleThread::test (prim_tests.h:192-231) of one subsample (unit offset ax, ay
+// duplicated into both lanes) against triangles j and k in that order, with the scalar test's
+// operations in its order: denom, depthDelta, v, w as FMA chains (FMA) or as rounded products and
+// sums (STRICT), u = (denom - v) - w, the sign-bit test and the depth update. Both depth deltas are
+// formed from the depth before j; when j hits, k's is formed again from the new depth, so k sees
+// exactly the depth the sequential fold gives it.
 // tt holds (-t_j, -t_k) in FMA mode, (t_j, t_k) in STRICT mode.
 template <bool FMA>
 __device__ __forceinline__ void pairTest(const TriPair& p, P2 tt, float tj, float tk, uint32_t ij, uint32_t ik,
@@ -1147,7 +1126,7 @@ __global__ void __launch_bounds__(kTileSize) intersectShadeDofKernel(FrameDev fr
                 // NaN fails (a padding sample's zero beam normalises to NaN; the sign-bit test alone
                 // would depend on which NaN the hardware produces)
                 if (test >= 0 && u == u && depthDelta == depthDelta) {
-                    tmax[i] = t * (1.0f / denom);
+                    tmax[i] = hitDepth(t, denom);
                     hit[i] = jidx;
                 }
             }
