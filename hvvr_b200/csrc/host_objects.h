@@ -219,8 +219,7 @@ struct hvvr_batch {
     bool counterValid = false;
     cudaStream_t side[2 * kRateClasses] = {}; // per rate class: [2r] heavy tiles (high priority), [2r+1] the rest
     cudaEvent_t forkEv = nullptr, rankEv = nullptr, doneEv[2 * kRateClasses] = {}, cullEv[2 * kRateClasses] = {};
-    cudaStream_t orderStream = nullptr;        // the tile order, beside the block cull
-    cudaEvent_t orderForkEv = nullptr, orderDoneEv = nullptr;
+    cudaEvent_t orderForkEv = nullptr, orderDoneEv = nullptr; // the tile order, beside the block cull
     cudaEvent_t ev[6] = {};
     cudaEvent_t kev[2 * kRateClasses][3] = {}; // per side stream: before tile cull, after it, after intersect
     bool kevUsed[2 * kRateClasses] = {};

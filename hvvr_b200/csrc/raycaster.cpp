@@ -654,7 +654,6 @@ void dropGraph(hvvr_batch* b) {
 // different priorities (a server's latency and throughput slots) share a queue as rarely as the
 // count allows.
 int ensureSideStreams(hvvr_batch* b) {
-    if (!b->orderStream) CUDA_TRY(cudaStreamCreateWithFlags(&b->orderStream, cudaStreamNonBlocking));
     int leastPriority = 0, greatestPriority = 0;
     for (uint32_t r = 0; r < kRateClasses; r++) {
         if (!b->rateTiles[r]) continue;
@@ -705,7 +704,6 @@ void releaseBatch(hvvr_batch* b) {
     dropGraph(b);
     for (auto& t : b->side)
         if (t) cudaStreamDestroy(t), t = nullptr;
-    if (b->orderStream) cudaStreamDestroy(b->orderStream), b->orderStream = nullptr;
     for (cudaEvent_t* e : {&b->forkEv, &b->orderForkEv, &b->orderDoneEv})
         if (*e) cudaEventDestroy(*e), *e = nullptr;
     for (auto& e : b->doneEv)
@@ -756,15 +754,27 @@ int enqueueFrame(hvvr_batch* b, const FrameDev& fr, cudaStream_t st, bool captur
     CUDA_TRY(recordStage(b->ev[0], st, capturing));
     CUDA_TRY(cudaMemsetAsync(fr.counters, 0, kCounterWords * sizeof(uint32_t), st));
     if (b->cfg.pipeline && fr.tiles) CUDA_TRY(cudaMemsetAsync(fr.ready, 0xff, size_t(fr.tiles) * sizeof(uint32_t), st));
-    // the tile order reads only last frame's costs, so it runs on its own stream beside the block
-    // cull, and the tile culls wait for both
-    CUDA_TRY(cudaEventRecord(b->orderForkEv, st));
-    CUDA_TRY(cudaStreamWaitEvent(b->orderStream, b->orderForkEv, 0));
-    CUDA_TRY(launchTileOrder(fr, b->orderStream));
-    CUDA_TRY(cudaEventRecord(b->orderDoneEv, b->orderStream));
+    // The tile order reads only last frame's costs, so it runs beside the block cull, and the tile
+    // culls wait for both. It borrows the side stream of the first rate class (heavy part's if
+    // there is one): idle at the top of the frame, it has the priority the batch gives its culls
+    // (a latency-class batch's order must not queue behind other batches' work), and it adds no
+    // stream to share the device's hardware queues.
+    cudaStream_t os = st;
+    for (uint32_t r = 0; r < kRateClasses; r++) {
+        if (!b->rateTiles[r]) continue;
+        cudaStream_t c = b->side[2 * r] ? b->side[2 * r] : b->side[2 * r + 1];
+        if (c) os = c;
+        break;
+    }
+    if (os != st) {
+        CUDA_TRY(cudaEventRecord(b->orderForkEv, st));
+        CUDA_TRY(cudaStreamWaitEvent(os, b->orderForkEv, 0));
+    }
+    CUDA_TRY(launchTileOrder(fr, os));
+    if (os != st) CUDA_TRY(cudaEventRecord(b->orderDoneEv, os));
     CUDA_TRY(launchBlockCull(fr, st));
     if (stages) CUDA_TRY(recordStage(b->ev[1], st, capturing));
-    CUDA_TRY(cudaStreamWaitEvent(st, b->orderDoneEv, 0));
+    if (os != st) CUDA_TRY(cudaStreamWaitEvent(st, b->orderDoneEv, 0));
     CUDA_TRY(cudaEventRecord(b->forkEv, st));
     bool first = true;
     for (auto& u : b->kevUsed) u = false;
