@@ -614,9 +614,10 @@ constexpr uint32_t kSplitMinTiles = 32;
 
 void batchConfigDefault(hvvr_batch_config* c) {
     // On the 1M-triangle stereo 2x1080x1200 8xMSAA frame, one-warp cull CTAs with the slowest 1/8
-    // of the tiles as the heavy part were fastest: 5.30 ms against 5.45 with 4-warp CTAs (a warp
-    // that runs out of tiles frees its registers for the shade of finished tiles at once);
-    // heavy shares 1/4 and 1/16 were 5.55 and 5.73 ms, no split 5.97
+    // of the tiles as the heavy part, cull -> shade pipeline on, were fastest: 4.92 ms against 5.50
+    // with 2-warp CTAs (a warp that runs out of tiles frees its registers for the shade of finished
+    // tiles at once); heavy shares 1/4, 1/6, 1/12 and 1/16 were 5.17, 5.05, 5.19 and 5.3-5.4 ms;
+    // without the pipeline 5.99
     c->tile_cull_warps = 1;
     c->heavy_divisor = 8;
     c->tri_index_capacity = kDefaultCapacity;
