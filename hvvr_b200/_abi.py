@@ -116,7 +116,7 @@ class BatchConfig(C.Structure):
     _fields_ = [("tile_cull_warps", C.c_uint32), ("heavy_divisor", C.c_uint32), ("tri_index_capacity", C.c_uint64),
                 ("use_graph", C.c_uint32), ("frame_ms", C.c_float), ("tile_stack_entries", C.c_uint32),
                 ("timing", C.c_uint32), ("pipeline", C.c_uint32), ("tile_cull_ctas_per_sm", C.c_uint32),
-                ("tile_cull_persistent", C.c_uint32)]
+                ("tile_cull_persistent", C.c_uint32), ("stream_tiles", C.c_uint32)]
 
 
 class ServerConfig(C.Structure):

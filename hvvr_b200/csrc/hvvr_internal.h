@@ -22,6 +22,12 @@ enum : uint32_t { kTileStack = 256 };
 // triangle indices move between traversal and intersection in chunks of one intersect batch
 enum : uint32_t { kChunk = 128 };
 enum : uint32_t { kNoChunk = 0xffffffffu };
+// Streamed tiles (the first tiles of a pipelined launch's queue, its longest): the list is
+// published after its first chunk and its shade follows the chunks as they are linked. A chunk's
+// link reads kChunkPending until the next chunk is linked (kNoChunk after the last one), the
+// tile's TileList reads count kCountStreaming until the list is complete, and the last chunk's
+// unused entries hold kNoTriangle.
+enum : uint32_t { kChunkPending = 0xfffffffeu, kCountStreaming = 0xffffffffu, kNoTriangle = 0xffffffffu };
 
 // device status bits (OR-ed into a per-frame word)
 enum : uint32_t {
@@ -203,6 +209,7 @@ struct FrameDev {
     uint32_t* ready = nullptr;         // [tiles] ready slots of the pipelined rate classes (kReadyEmpty at frame start)
     uint32_t cullCtasPerSm = 0;        // cap on the persistent tile cull's resident CTAs per SM (0: occupancy)
     uint32_t cullPersistent = 1;       // 0: each tile-cull warp culls one tile, and the grid covers all tiles
+    uint32_t streamTiles = 0;          // pipelined launches: the first streamTiles tiles of the queue stream
 };
 
 

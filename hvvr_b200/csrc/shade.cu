@@ -500,6 +500,8 @@ struct ShadeSmem {
     float t[kChunk], nlen[kChunk];
     uint32_t idx[kChunk];
     uint32_t warpCount[4];
+    uint2 list;    // the tile's TileList as thread 0 read it
+    uint32_t link; // a streamed list's next chunk, as thread 0 waited for it
     // the list triangles of the chunk being culled, 48 bytes per entry (three float4 rows of the
     // triangle array), copied in by cp.async one chunk ahead; thread i writes and reads only
     // entry i, so the copy of the next chunk can start as soon as entry i has been read
@@ -548,18 +550,47 @@ __device__ uint32_t waitReady(const uint32_t* slot, uint32_t* counters) {
     }
 }
 
+// Waits (one thread) until a streamed list's chunk is linked to its successor (or marked as the
+// last); gives up like waitReady, returning kNoChunk.
+__device__ uint32_t waitChunkLink(const uint32_t* link, uint32_t* counters) {
+    for (uint32_t i = 0;; i++) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(link) : "memory");
+        if (v != kChunkPending) return v;
+        if (i >= (1u << 20)) {
+            atomicOr(&counters[1], kStatusPipelineTimeout);
+            return kNoChunk;
+        }
+        __nanosleep(i < 32 ? 128 : 1024);
+    }
+}
+
 // One tile: intersect, G-buffer grouping, shading and resolve of its 128 samples. The tile's
 // list (TileList, chunk links, pool entries) is read through L2 (ld.cg): in a pipelined launch
 // another SM wrote it while this launch was running.
 // ROW: the row of the offset tables (the rate's spiral row, or + 6 for the rotated grid), a
 // compile-time constant so that the offsets stay immediate constant-bank operands
-template <uint32_t N, bool FMA, int ROW>
+// STREAM: the tile may come from a pipelined launch, whose longest tiles stream their lists.
+template <uint32_t N, bool FMA, int ROW, bool STREAM = false>
 __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, ShadeSmem& sm, LightEnvDev& env, Mat4& M) {
     const ViewDev& V = fr.views[fr.viewCount == 1 ? 0u : __ldg(fr.blockView + gt / kTilesPerBlock)];
     const uint32_t tile = gt - V.tileStart;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sid = tile * kTileSize + tid;
-    const uint2 lw = __ldcg(reinterpret_cast<const uint2*>(V.tileLists + tile));
+    uint2 lw;
+    if constexpr (STREAM) {
+        // (read once, with acquire, for the whole CTA: a streamed tile's list may be completed while
+        // the CTA reads it, and every thread must take the same path)
+        if (tid == 0) {
+            unsigned long long l;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(l) : "l"(V.tileLists + tile) : "memory");
+            sm.list = make_uint2(uint32_t(l), uint32_t(l >> 32));
+        }
+        __syncthreads();
+        lw = sm.list;
+    } else {
+        lw = __ldcg(reinterpret_cast<const uint2*>(V.tileLists + tile));
+    }
     const TileList L{lw.x, lw.y};
     if (L.count == 0) {
         // ClearEmptyKernel (resolve.cu:527-542)
@@ -652,23 +683,27 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         cpAsync16(&sm.stage[3 * tid + 1], src + 1);
         cpAsync16(&sm.stage[3 * tid + 2], src + 2);
     };
+    // A streamed list (the cull published the tile after its first chunk) is walked as its chunks
+    // are linked: each chunk is taken whole (its unused entries, in the last chunk, hold
+    // kNoTriangle), and the next one is staged once this one's link is set.
+    const bool streamed = STREAM && L.count == kCountStreaming;
     uint32_t chunk = L.first;
-    uint32_t remaining = L.count;
+    uint32_t remaining = streamed ? kChunk + 1 : L.count;
     uint32_t survivors = 0, tested = 0;
     uint32_t idx = 0;
     if (chunk < fr.poolChunks && tid < (remaining < kChunk ? remaining : kChunk)) {
         idx = __ldcg(fr.pool + size_t(chunk) * kChunk + tid);
-        stage(idx);
+        if (!STREAM || idx != kNoTriangle) stage(idx);
     }
     cpAsyncCommit();
     while (remaining > 0 && chunk < fr.poolChunks) {
         const uint32_t n = remaining < kChunk ? remaining : kChunk;
-        const uint32_t nextChunk = __ldcg(fr.chunkNext + chunk);
+        uint32_t nextChunk = streamed ? kChunkPending : __ldcg(fr.chunkNext + chunk);
         bool keep = false;
         float t = 0.0f, nlen = 0.0f;
         F3 e0 = f3(0, 0, 0), e1 = f3(0, 0, 0), v0r = f3(0, 0, 0), nrm = f3(0, 0, 0);
         cpAsyncWaitAll();
-        if (tid < n) {
+        if (tid < n && (!STREAM || idx != kNoTriangle)) {
             const float4 ra = sm.stage[3 * tid + 0], rb = sm.stage[3 * tid + 1], rc = sm.stage[3 * tid + 2];
             const TriGeom tri{f3(ra.x, ra.y, ra.z), f3(ra.w, rb.x, rb.y), f3(rb.z, rb.w, rc.x)};
             // FrustumPlanes::test
@@ -701,7 +736,7 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         }
         // the next chunk's index of this entry (its chunk link has arrived by now)
         const uint32_t rest = remaining - n;
-        const bool more = rest > 0 && nextChunk < fr.poolChunks;
+        const bool more = !streamed && rest > 0 && nextChunk < fr.poolChunks;
         uint32_t idxNext = 0;
         if (more && tid < (rest < kChunk ? rest : kChunk)) idxNext = __ldcg(fr.pool + size_t(nextChunk) * kChunk + tid);
         const uint32_t bal = __ballot_sync(kFull, keep);
@@ -783,6 +818,19 @@ __device__ __forceinline__ void shadeTile(const FrameDev& fr, uint32_t gt, Shade
         }
         if (pend != ~0u) testPair(pend, pend);
         __syncthreads();
+        if (STREAM && streamed) {
+            if (tid == 0) sm.link = waitChunkLink(fr.chunkNext + chunk, fr.counters);
+            __syncthreads();
+            nextChunk = sm.link;
+            if (nextChunk < fr.poolChunks) {
+                idxNext = __ldcg(fr.pool + size_t(nextChunk) * kChunk + tid);
+                if (idxNext != kNoTriangle) stage(idxNext);
+                remaining = n + kChunk + 1; // after this chunk: a whole chunk and an unknown rest
+            } else {
+                remaining = n; // the list's end: the loop stops
+            }
+            cpAsyncCommit();
+        }
         remaining -= n;
         chunk = nextChunk;
         idx = idxNext;
@@ -903,7 +951,7 @@ __global__ void __launch_bounds__(kTileSize, MinCtas<N>::v) intersectShadeKernel
         __syncthreads();
         const uint32_t gt = readyTile;
         if (gt & kReadyRetry) return; // culled and shaded by the retry passes (or the wait gave up)
-        shadeTile<N, FMA, ROW>(fr, gt, sm, env, M);
+        shadeTile<N, FMA, ROW, true>(fr, gt, sm, env, M);
     } else {
         const uint32_t count = *src.listCount;
         for (uint32_t item = blockIdx.x; item < count; item += gridDim.x) {

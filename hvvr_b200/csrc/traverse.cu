@@ -450,6 +450,15 @@ struct TileSmemT {
     uint32_t rStart[kRanges], rLen[kRanges];
 };
 
+// End of a streamed tile's list: every lane's list writes are visible device-wide before lane 0
+// releases the last chunk's link as kNoChunk.
+__device__ __forceinline__ void endStream(uint32_t* lastLink) {
+    __threadfence();
+    __syncwarp();
+    if (laneId() == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(lastLink), "r"(kNoChunk) : "memory");
+    __syncwarp();
+}
+
 struct Emitter {
     uint32_t* pool;
     uint32_t* chunkNext;
@@ -457,8 +466,17 @@ struct Emitter {
     uint32_t* counters;
     uint32_t first, prev, bufCount, stored, total;
     bool dead;
+    uint32_t rc; // ranges buffered in rStart/rLen
+    // streamed tile (stream): published with its first chunk; list = its TileList, ready = the
+    // launch's ready slots, gt = the global tile index the slot carries
+    bool stream, published;
+    TileList* list;
+    uint32_t* ready;
+    uint32_t* readyTail;
+    uint32_t gt;
 
-    __device__ void flush(uint32_t* buf) {
+    // last: the list's final (partial) chunk
+    __device__ void flush(uint32_t* buf, bool last = false) {
         __syncwarp();
         uint32_t c = 0;
         if (laneId() == 0) c = atomicAdd(&counters[0], 1u);
@@ -470,7 +488,25 @@ struct Emitter {
         }
         const uint4 w = reinterpret_cast<const uint4*>(buf)[laneId()];
         reinterpret_cast<uint4*>(pool + size_t(c) * kChunk)[laneId()] = w;
-        if (laneId() == 0) {
+        if (stream && (prev != kNoChunk || !last)) {
+            // The chunk's entries and its pending link are visible device-wide before the chunk is
+            // linked to its predecessor, or, the first chunk, before the tile is published with a
+            // streaming TileList. (A list that fits one chunk is published at the end as usual.)
+            if (laneId() == 0) chunkNext[c] = kChunkPending;
+            __threadfence();
+            __syncwarp();
+            if (laneId() == 0) {
+                if (prev != kNoChunk) {
+                    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(chunkNext + prev), "r"(c) : "memory");
+                } else {
+                    *list = TileList{c, kCountStreaming};
+                    __threadfence();
+                    const uint32_t pos = atomicAdd(readyTail, 1u);
+                    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ready + pos), "r"(gt) : "memory");
+                }
+            }
+            if (prev == kNoChunk) published = true;
+        } else if (laneId() == 0) {
             if (prev != kNoChunk) chunkNext[prev] = c;
         }
         if (prev == kNoChunk) first = c;
@@ -479,8 +515,6 @@ struct Emitter {
         bufCount = 0;
         __syncwarp();
     }
-
-    uint32_t rc; // ranges buffered in rStart/rLen
 
     // Records the triangle ranges of the passing leaf slots of one node, in slot order (leaf
     // slot k covers [tri[k], tri[k+1]) = words 25+k, 26+k of the node; v holds word l of the
@@ -568,13 +602,14 @@ struct TileCullArgs {
     uint32_t* ready;       // pipelined: ready slots, slot first + i for the i-th finished tile (else nullptr)
     uint32_t* readyTail;   // pipelined: finished tiles so far, zero at launch
     uint32_t persistent;   // 0: every warp culls one tile (the grid has a warp per tile), then exits
+    uint32_t streamTiles;  // with ready: queue positions below this stream their lists (else 0)
 };
 
 // traverseTiles for one tile of view V (tile = view-local index); returns the node visits.
 // overflow: the sorted stack needed more than S entries; the tile's list is left empty.
 template <uint32_t S>
 __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t tile, TileSmemT<S>& s,
-                             bool& overflow) {
+                             bool& overflow, bool stream = false, uint32_t gt = 0, bool* published = nullptr) {
     overflow = false;
     const uint32_t lane = laneId();
     const Node* __restrict__ nodes = V.nodes;
@@ -598,7 +633,9 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
     __syncwarp();
     const LaneTest t = loadLaneTest(s.f);
     const int distIdx = s.f.distIdx;
-    Emitter em{a.pool, a.chunkNext, a.poolChunks, a.counters, kNoChunk, kNoChunk, 0, 0, 0, false, 0};
+    Emitter em{a.pool, a.chunkNext, a.poolChunks, a.counters, kNoChunk, kNoChunk, 0, 0, 0, false, 0,
+               stream && a.ready != nullptr, false, V.tileLists + tile, a.ready ? a.ready + a.first : nullptr,
+               a.readyTail, gt};
     uint32_t top = stackSize - 1;
     uint32_t node = s.node[top];
     uint32_t visits = 0;
@@ -769,12 +806,32 @@ __device__ uint32_t cullTile(const TileCullArgs& a, const ViewDev& V, uint32_t t
     vcLast = phaseClock(top);
 #endif
     if (overflow) {
+        // (a streamed tile's shade ends its chunk walk here; the retry passes cull and shade the
+        // tile again after it)
+        if (published) *published = em.published;
+        if (em.published) endStream(a.chunkNext + em.prev);
         if (lane == 0) V.tileLists[tile] = TileList{kNoChunk, 0};
         return visits;
     }
     if (!em.dead && em.rc) em.expand(s);
-    if (!em.dead && em.bufCount) em.flush(s.buf);
-    if (lane == 0) {
+    if (em.published && !em.dead && em.bufCount) {
+        // a streamed list's last chunk: its unused entries say so
+        for (uint32_t i = em.bufCount + lane; i < kChunk; i += 32) s.buf[i] = kNoTriangle;
+        __syncwarp();
+    }
+    if (!em.dead && em.bufCount) em.flush(s.buf, true);
+    // (after the last expansion, whose full chunks may have published the tile)
+    if (published) *published = em.published;
+    if (em.published) {
+        // the last chunk's end-of-list link, then the complete TileList, each after what precedes it
+        endStream(a.chunkNext + em.prev);
+        if (lane == 0) {
+            __threadfence();
+            const unsigned long long l =
+                uint64_t(em.first) | (uint64_t(em.dead ? em.stored : em.total) << 32);
+            asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(V.tileLists + tile), "l"(l) : "memory");
+        }
+    } else if (lane == 0) {
         if (em.prev != kNoChunk) a.chunkNext[em.prev] = kNoChunk;
         V.tileLists[tile] = TileList{em.first, em.dead ? em.stored : em.total};
     }
@@ -812,13 +869,13 @@ __global__ void __launch_bounds__(W * 32, W == 1 ? 20 : 1) tileCullKernel(TileCu
         const ViewDev& V = viewOfBlock(a.views, a.blockView, a.viewCount, gt / kTilesPerBlock);
         const uint32_t tile = gt - V.tileStart;
         __syncwarp();
-        bool overflow;
-        const uint32_t visits = cullTile(a, V, tile, s, overflow);
+        bool overflow, published = false;
+        const uint32_t visits = cullTile(a, V, tile, s, overflow, w < a.streamTiles, gt, &published);
         if (lane == 0) {
             V.tileCost[tile] = visits;
             if (overflow) a.retry[a.first + atomicAdd(a.retryCount, 1u)] = gt;
         }
-        if (a.ready) {
+        if (a.ready && !published) {
             // publish: every lane's list writes (pool chunks, links, the tile's TileList) are made
             // visible device-wide before lane 0 releases the slot
             __threadfence();
@@ -1005,7 +1062,7 @@ cudaError_t launchTileCullMain(const FrameDev& fr, const uint32_t* order, uint32
     if (stackLimit < 8) return cudaErrorInvalidValue;
     const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
                          order, first, count, queues, fr.retry, queues + 1, queues + 2, stackLimit, ready, readyTail,
-                         fr.cullPersistent ? 1u : 0u};
+                         fr.cullPersistent ? 1u : 0u, ready ? fr.streamTiles : 0u};
     switch (warps) {
     case 1: return launchTileCullW<1>(a, count, fr.cullCtasPerSm, st);
     case 2: return launchTileCullW<2>(a, count, fr.cullCtasPerSm, st);
@@ -1019,7 +1076,8 @@ cudaError_t launchTileCullRetryPass(const FrameDev& fr, const uint32_t* order, u
                                     uint32_t* queues, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     const TileCullArgs a{fr.views, fr.blockView, fr.viewCount, fr.pool, fr.chunkNext, fr.poolChunks, fr.counters,
-                         order, first, count, queues, fr.retry, queues + 1, queues + 2, kTileStack, nullptr, nullptr, 1u};
+                         order, first, count, queues, fr.retry, queues + 1, queues + 2, kTileStack, nullptr, nullptr, 1u,
+                         0u};
     return launchTileCullRetry(a, st);
 }
 

@@ -437,6 +437,12 @@ typedef struct {
                                      so the cull's CTAs are short-lived and the GPU's block scheduler
                                      can give their SM slots to work of a higher stream priority
                                      between tiles (a served throughput batch under a latency class) */
+    uint32_t stream_tiles;        /* with pipeline: the first stream_tiles tiles of each rate class's
+                                     first part (its longest, in last frame's order) publish their
+                                     lists chunk by chunk, and their intersect/shade follows the
+                                     chunks while the cull is still producing them (default 400).
+                                     0: every tile is published when its list is complete. The
+                                     images are the same */
 } hvvr_batch_config;
 void hvvr_batch_config_default(hvvr_batch_config* cfg);
 int hvvr_batch_create(hvvr_raycaster* const* raycasters, uint32_t count, const hvvr_batch_config* cfg,

@@ -159,8 +159,9 @@ def test_stack_retry_pass_matches_oracle(oracle, pipeline):
 @pytest.mark.parametrize("use_graph", [1, 0])
 def test_pipelined_and_split_frames_agree(oracle, use_graph):
     """The cull -> shade pipeline (default) against the split path (heavy part on its own stream,
-    cull before shade) and against the pipeline with a non-persistent tile cull (a warp per tile,
-    as a served throughput batch runs) on a frame batch with three MSAA rates over two scenes, over
+    cull before shade), against the pipeline with a non-persistent tile cull (a warp per tile,
+    as a served throughput batch runs) and against the pipeline with every tile streaming its list
+    chunk by chunk to its shade, on a frame batch with three MSAA rates over two scenes, over
     three frames (the second and later ones cull in the previous frame's cost order): identical
     lists, hits and colours, and equal to the oracle."""
     sa, sb = scene("c1"), scene("small")
@@ -173,10 +174,11 @@ def test_pipelined_and_split_frames_agree(oracle, use_graph):
         cam.set_camera_to_world(xf)
         cams.append((cam, sc, smp, w, h, msaa, xf))
     results = {}
-    for mode, pipeline, persistent in (("pipelined", 1, 1), ("split", 0, 1), ("one tile per warp", 1, 0)):
+    modes = (("pipelined", 1, 1, 0), ("split", 0, 1, 0), ("one tile per warp", 1, 0, 0), ("streamed", 1, 1, 1 << 20))
+    for mode, pipeline, persistent, stream in modes:
         batch = hv.Batch([rc_a, rc_b], hv.batch_config(use_graph=use_graph, tri_index_capacity=1 << 22,
                                                        pipeline=pipeline, timing=1, tile_cull_warps=1 + pipeline,
-                                                       tile_cull_persistent=persistent))
+                                                       tile_cull_persistent=persistent, stream_tiles=stream))
         for frame in range(3):
             batch.render()
             assert batch.stats()["status"] == 0
@@ -191,7 +193,9 @@ def test_pipelined_and_split_frames_agree(oracle, use_graph):
                 _check_view(oracle, sc, cam, smp, w, h, msaa, xf)
         results[mode] = out
         batch.close()
-    for other in ("split", "one tile per warp"):
+    # streaming starts at a list's second chunk: some tiles here have more than one
+    assert max(int(o[0].max()) for o in results["streamed"]) > 128
+    for other in ("split", "one tile per warp", "streamed"):
         for a, b in zip(results["pipelined"], results[other]):
             for x, y in zip(a, b):
                 assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), other

@@ -80,5 +80,6 @@ def test_batch_config_defaults():
     cfg = hv.batch_config()
     assert (cfg.tile_cull_warps, cfg.heavy_divisor, cfg.pipeline, cfg.tile_cull_persistent) == (1, 8, 1, 1)
     assert (cfg.use_graph, cfg.timing, cfg.tile_stack_entries, cfg.tile_cull_ctas_per_sm) == (1, 0, 0, 0)
+    assert cfg.stream_tiles == 400
     assert C.sizeof(_abi.BatchConfig) == 48
 
