@@ -214,7 +214,7 @@ int buildSampleSetupDevice(const hvvr_sample* samples, uint32_t count, uint32_t 
     TRY(perm[1].alloc(count));
     TRY(flags.alloc(1));
     CUDA_TRY(cudaMemsetAsync(flags.p, 0, 4, st));
-    // round 1: the whole set by (y, x)
+    // sort 1 of naiveXYCluster: the whole set by (y, x)
     keysKernel<<<grid(count, 256), 256, 0, st>>>(dSamples.p, nullptr, count, kKeyYX, keys[0].p, flags.p);
     iotaKernel<<<grid(count, 256), 256, 0, st>>>(perm[0].p, count);
     size_t tempBytes = 0;
@@ -232,7 +232,7 @@ int buildSampleSetupDevice(const hvvr_sample* samples, uint32_t count, uint32_t 
         needsHost = true;
         return HVVR_OK;
     }
-    // rounds 2-4: fixed-size runs of the current order, sorted within each run
+    // sorts 2-4: fixed-size runs of the current order, sorted within each run
     uint32_t cur = 1;  // perm[cur] holds the order
     auto round = [&](size_t run, uint32_t mode) -> int {
         std::vector<int> begins, ends;

@@ -241,7 +241,7 @@ def make_lights(rng):
     return lights
 
 
-# ---------------------------------------------------------------- BASELINE configurations
+# ---------------------------------------------------------------- the benchmark configurations (C1-C5)
 def scene_c1(seed=1):
     """128x128-quad heightfield (32,768 tris) + 2,048 boxes (24,576 tris): 57,344 triangles."""
     return make_scene(128, 2048, seed)
