@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import hvvr_b200 as hv
-from hvvr_b200 import scenes
+from hvvr_b200 import _abi, scenes
 
 from helpers import list_mismatch, render_oracle, scene
 
@@ -239,3 +239,30 @@ def test_batch_mixes_thin_lens_and_pinhole_views(oracle):
     batch.close()
     rc_a.close()
     rc_b.close()
+
+
+@pytest.mark.parametrize("stream", [0, 1 << 20])
+def test_list_pool_overflow_is_reported(oracle, stream):
+    """Tile lists that outgrow the triangle-index pool are reported (HVVR_ERR_OVERFLOW) instead of
+    being returned cut, with the cull -> shade pipeline and with every tile streaming its list (a
+    streamed list ends after its last stored chunk, and its shade ends there with it); a batch with
+    a pool large enough then renders the same view exactly."""
+    sc = scene("c1")
+    rc = _make_rc(sc)
+    w, h = 256, 224
+    cam, smp = _add_cam(rc, w, h, "barrel", 8)
+    xf = scenes.camera_transform(eye=(0.0, 2.0, 10.0), target=(0.0, 0.0, 0.0))
+    cam.set_camera_to_world(xf)
+    small = hv.Batch(cameras=[cam], config=hv.batch_config(tri_index_capacity=4096, stream_tiles=stream))
+    with pytest.raises(hv.HvvrError) as err:
+        small.render()
+        small.synchronize()
+    assert err.value.code == _abi.HVVR_ERR_OVERFLOW
+    small.close()
+    big = hv.Batch(cameras=[cam], config=hv.batch_config(tri_index_capacity=1 << 22, stream_tiles=stream))
+    for _ in range(2):
+        big.render()
+    big.synchronize()
+    _check_view(oracle, sc, cam, smp, w, h, 8, xf)
+    big.close()
+    rc.close()
